@@ -1,0 +1,456 @@
+#!/usr/bin/env python
+"""Benchmark of the per-subgraph APSP solve path on B200.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl fap|reference]
+
+One step = one full APSP solve of the workload (every part's SSSP, Floyd and
+min-plus; every distance entry written to HBM).  Default workload: the
+114,599-vertex road-shaped graph (integer weights 1..1000), K=128 parts.
+
+Arms
+  fap (default)  the CUDA path.  `value` = APSP entries/s of the batched form
+                 with inputs resident in HBM, timed with CUDA events on the
+                 library's stream (max over ranks); `plain` = the same for the
+                 one-launch-sequence-per-part form; `e2e` = the public API with
+                 host inputs and every block read back to pinned host memory.
+  reference      the reference's own CPU path (oracle/_ref/fap_ref built from
+                 the reference sources; the C restatement when that binary is
+                 absent) on this host's cores, one process per core like the
+                 reference's MPI driver, each step a bounded sample of parts.
+
+With N>1 (torchrun) the parts are sharded across ranks (no data-path
+collective; the reference's MPI task split); rank 0 prints the JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "APSP entries/sec, batched vs plain form on 1 B200 (bit-exact int32); p50/p99 latency"
+UNIT = "entries/s"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["fap", "reference"], default="fap")
+    ap.add_argument("--workload", default="road114k")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--plain-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-procs", type=int, default=0, help="0 = min(cores, memory bound)")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# helpers
+# ---------------------------------------------------------------------------
+def read_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def read_traffic(workload, kernel):
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    return d.get(workload, {}).get(kernel)
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for nm, v in zip(names, parts[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", str(rank)))
+    return rank, world, local
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference's CPU path, one process per core
+# ---------------------------------------------------------------------------
+def cpu_procs(requested):
+    cores = os.cpu_count() or 1
+    avail_gb = 8.0
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    avail_gb = int(line.split()[1]) / 1e6
+    except OSError:
+        pass
+    cap = max(1, int(avail_gb * 0.5 / 1.0))   # ~1 GB per process (block + path)
+    p = min(cores, cap, 64)
+    if requested:
+        p = min(p, requested)
+    return max(1, p)
+
+
+def run_reference_sample(wl, parts_per_proc, procs, timeout=900):
+    """Runs the reference CPU path on `procs` concurrent processes, process i
+    solving parts_per_proc[i] in order.  Returns (kind, per-process list of
+    (part, rows, entries, seconds))."""
+    from oracle import oracle as O
+    kind = "reference" if O.ref_available() else "port"
+    env = dict(os.environ, OMP_NUM_THREADS="1")
+    if kind == "reference":
+        cmds = [[O.REF_BIN, "--dir", wl.root, "-f", wl.name, "-k", str(wl.K),
+                 "-direct", str(int(wl.edges.directed)), "-weight", str(int(wl.edges.weighted)),
+                 "--parts", ",".join(map(str, pp)), "--quiet"] for pp in parts_per_proc]
+    else:
+        script = os.path.join(ROOT, "oracle", "port_cli.py")
+        cmds = [[sys.executable, script, "--dir", wl.root, "-f", wl.name, "-k", str(wl.K),
+                 "-direct", str(int(wl.edges.directed)), "-weight", str(int(wl.edges.weighted)),
+                 "--parts", ",".join(map(str, pp))] for pp in parts_per_proc]
+    ps = [subprocess.Popen(c, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True, env=env)
+          for c in cmds]
+    out = []
+    for p in ps:
+        so, se = p.communicate(timeout=timeout)
+        if p.returncode != 0:
+            raise RuntimeError(f"CPU baseline process failed: {se[-500:]}")
+        rec = [json.loads(x) for x in so.splitlines() if x.startswith("{")]
+        out.append([(r["part"], r["rows"], r["entries"], r["seconds"]) for r in rec
+                    if r.get("event") == "part"])
+    return kind, out
+
+
+def sample_parts(K, count, seed):
+    rng = np.random.default_rng(seed)
+    return [int(x) + 1 for x in rng.permutation(K)[:count]]
+
+
+# ---------------------------------------------------------------------------
+# reference arm
+# ---------------------------------------------------------------------------
+def main_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from fastapsp_b200 import workloads
+    wl = workloads.load(args.workload)
+    P = cpu_procs(args.cpu_procs)
+    steps = args.warmup + args.steps
+    need = P * steps
+    order = [int(x) + 1 for x in np.random.default_rng(7).permutation(wl.K)]
+    order = (order * (need // wl.K + 1))[:need]
+    per = [order[i::P] for i in range(P)]
+    kind, res = run_reference_sample(wl, per, P)
+    tot_entries, tot_time, step_ms = 0, 0.0, []
+    for s in range(args.warmup, steps):
+        ent = sum(r[s][2] for r in res)
+        sec = max(r[s][3] for r in res)
+        tot_entries += ent
+        tot_time += sec
+        step_ms.append(sec * 1e3)
+    value = tot_entries / tot_time
+    sample = (f"{args.steps} timed steps x {P} processes x 1 part "
+              f"({wl.name}, K={wl.K}); step time = slowest process")
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": float(np.mean(step_ms)), "higher_is_better": True,
+        "impl": "reference", "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": {**wl.describe(), "mode": "reference CPU path"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": P, "kind": kind,
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# fap arm
+# ---------------------------------------------------------------------------
+def main_fap(args):
+    import torch
+    import torch.distributed as dist
+
+    from fastapsp_b200 import FAP_DTYPE_F32, FAP_MODE_BATCHED, FAP_MODE_PLAIN, Context, DeviceGraph
+    from fastapsp_b200 import workloads
+    from fastapsp_b200.sharding import rows_of, shard_parts
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def allmax(x):
+        if world == 1:
+            return float(x)
+        t = torch.tensor([float(x)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def allsum(x):
+        if world == 1:
+            return float(x)
+        t = torch.tensor([float(x)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    wl = workloads.load(args.workload)
+    n = wl.n
+    vn, vo, bn = wl.ver_num, wl.ver_offset, wl.bdy_num
+    mine = shard_parts(vn, bn, n, world)[rank]
+    my_rows = rows_of(mine, vn)
+    my_entries = my_rows * n
+    total_entries = allsum(my_entries)
+    ro, col, w = wl.csr()
+    gid = wl.graph.getGraphId()
+    st2ed = wl.graph.getMapping()
+
+    ctx = Context(local)
+    ctx.use_torch_stream()
+    stream = torch.cuda.current_stream()
+    dg = DeviceGraph(ctx, ro, col, w)
+    dtype = dg.dtype
+    dg.set_parts(wl.K, gid, st2ed, vn, vo, bn)
+    dg.reserve(0 if world == 1 else my_rows)
+    relax_peak = ctx.relax_peak(dtype)
+    hbm_peak, peak_kind = read_peaks()
+
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+
+    # ---- batched, device-resident inputs ----
+    for _ in range(args.warmup):
+        dg.solve(mine, FAP_MODE_BATCHED, check_errors=False)
+    dg.check()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    step_ms, stages = [], []
+    launches = 0
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        dg.solve(mine, FAP_MODE_BATCHED, check_errors=False)
+        e1.record(stream)
+        e1.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+        stages.append(dg.last_timing())
+        launches += dg.last_launches()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    dg.check()
+    my_ms = float(np.sum(step_ms))
+    max_ms = allmax(my_ms)
+    ms_per_step = max_ms / args.steps
+    value = total_entries * args.steps / (max_ms * 1e-3)
+    st = np.mean(np.stack(stages), 0)  # [sssp, gather, floyd, minplus, total]
+
+    # ---- plain form ----
+    plain_ms = []
+    for i in range(1 + args.plain_steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        dg.solve(mine, FAP_MODE_PLAIN, check_errors=False)
+        e1.record(stream)
+        e1.synchronize()
+        if i > 0:
+            plain_ms.append(e0.elapsed_time(e1))
+    dg.check()
+    plain_max = allmax(float(np.sum(plain_ms))) if plain_ms else float("nan")
+    plain_value = total_entries * len(plain_ms) / (plain_max * 1e-3) if plain_ms else None
+
+    # ---- roofline figures per stage (algorithmic work of one launch) ----
+    m_arcs = int(ro[-1])
+    srcs = int(sum(int(bn[p]) for p in mine))
+    sssp_bytes = srcs * (4 * (n + 1) + 8 * m_arcs + 4 * n)
+    floyd_relax = float(sum(float(vn[p]) ** 3 for p in mine))
+    mp_relax = float(sum(float(vn[p] - bn[p]) * float(bn[p]) * n for p in mine))
+    mp_bytes = float(sum(4.0 * ((vn[p] - bn[p]) * n + (vn[p] - bn[p]) * bn[p] + bn[p] * n)
+                         for p in mine))
+    stage_roof = {
+        "sssp": {"ms": float(st[0]), "bytes": sssp_bytes,
+                 "achieved_gbs": sssp_bytes / (st[0] * 1e-3) / 1e9},
+        "gather": {"ms": float(st[1])},
+        "floyd": {"ms": float(st[2]), "relax": floyd_relax,
+                  "achieved_grelax_s": floyd_relax / (st[2] * 1e-3) / 1e9},
+        "minplus": {"ms": float(st[3]), "bytes": mp_bytes, "relax": mp_relax,
+                    "achieved_gbs": mp_bytes / (st[3] * 1e-3) / 1e9,
+                    "achieved_grelax_s": mp_relax / (st[3] * 1e-3) / 1e9},
+    }
+    peak_grelax = relax_peak / 1e9
+    dom = max(("sssp", "floyd", "minplus"), key=lambda k: stage_roof[k]["ms"])
+    if dom == "floyd":
+        a = stage_roof["floyd"]["achieved_grelax_s"]
+        roof = {"kernel": "floyd_part_kernel", "bound": "dpx", "achieved": a,
+                "peak": peak_grelax, "unit": "Grelax/s", "frac": a / peak_grelax,
+                "peak_source": "measured relaxation microbenchmark (fap_measure_relax_peak)",
+                "traffic": read_traffic(wl.name, "floyd_part_kernel")}
+    else:
+        kern = "sssp_bitmap_kernel" if dom == "sssp" else "minplus_part_kernel"
+        a = stage_roof[dom]["achieved_gbs"]
+        roof = {"kernel": kern, "bound": "hbm", "achieved": a, "peak": hbm_peak, "unit": "GB/s",
+                "frac": a / hbm_peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                "traffic": read_traffic(wl.name, kern)}
+    stage_roof["floyd"]["frac_of_relax_peak"] = stage_roof["floyd"]["achieved_grelax_s"] / peak_grelax
+    stage_roof["minplus"]["frac_of_relax_peak"] = (stage_roof["minplus"]["achieved_grelax_s"]
+                                                   / peak_grelax)
+    stage_roof["minplus"]["frac_of_hbm"] = stage_roof["minplus"]["achieved_gbs"] / hbm_peak
+    stage_roof["sssp"]["frac_of_hbm"] = stage_roof["sssp"]["achieved_gbs"] / hbm_peak
+
+    # ---- e2e through the public API: host inputs in, every block out ----
+    del dg
+    torch.cuda.synchronize()
+    max_rows = int(max(vn[p] for p in mine))
+    host_buf = torch.empty((max_rows, n), dtype=torch.float32, pin_memory=True)
+    hb = host_buf.numpy()
+    pin = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory().numpy()
+           for k, v in dict(ro=ro, col=col, w=w.astype(np.float32), gid=gid, st2ed=st2ed,
+                            vn=vn, vo=vo, bn=bn).items()}
+    h2d = sum(a.nbytes for a in pin.values())
+    d2h = my_rows * n * 4
+    e2e_s = []
+    for i in range(1 + args.e2e_steps):
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        g2 = DeviceGraph(ctx, pin["ro"], pin["col"], pin["w"])
+        g2.set_parts(wl.K, pin["gid"], pin["st2ed"], pin["vn"], pin["vo"], pin["bn"])
+        g2.reserve(my_rows)
+        g2.solve(mine, FAP_MODE_BATCHED)
+        for p in mine:
+            g2.copy_block(p, out_dtype=FAP_DTYPE_F32, out=hb[:int(vn[p])])
+        t1 = time.perf_counter()
+        del g2
+        if i > 0:
+            e2e_s.append(t1 - t0)
+    e2e_max = allmax(float(np.sum(e2e_s)))
+    e2e_value = total_entries * len(e2e_s) / e2e_max
+
+    # ---- CPU baseline (rank 0, N=1 only) ----
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        P = cpu_procs(args.cpu_procs)
+        parts = sample_parts(wl.K, P, seed=11)
+        kind, res = run_reference_sample(wl, [[p] for p in parts], P)
+        ent = sum(r[0][2] for r in res)
+        sec = max(r[0][3] for r in res)
+        cpu = {"value": ent / sec, "unit": UNIT, "cores": P, "kind": kind,
+               "sample": f"{P} parts of {wl.name} (K={wl.K}), one process per core, "
+                         f"1 thread each; time = slowest process ({sec:.2f} s)"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "int32" if dtype == 0 else "f32",
+            "data": "synthetic: seeded road-shaped graph (EMST + nearest-neighbour edges, "
+                    "uniform points), int weights U[1,1000]",
+            "config": {**wl.describe(), "mode": "batched", "parallelism": f"parts sharded x{world}",
+                       "l2": "256 MB buffer written between timed steps (outside the events); "
+                             f"each step also writes {4 * n * n / 1e9:.1f} GB of output"},
+            "plain": {"value": plain_value, "ms_per_step": plain_max / max(len(plain_ms), 1),
+                      "steps": len(plain_ms)},
+            "batched_over_plain": (value / plain_value) if plain_value else None,
+            "stages_ms": {"sssp": float(st[0]), "gather": float(st[1]), "floyd": float(st[2]),
+                          "minplus": float(st[3]), "total": float(st[4])},
+            "roofline": roof, "stage_roofline": stage_roof,
+            "relax_peak_grelax_s": peak_grelax,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h), "steps": len(e2e_s),
+                    "s_per_step": e2e_max / max(len(e2e_s), 1)},
+            "gpu_launches": int(launches),
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        main_reference(args)
+    else:
+        main_fap(args)
+
+
+if __name__ == "__main__":
+    main()

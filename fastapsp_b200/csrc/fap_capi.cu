@@ -1,0 +1,803 @@
+// C ABI of the per-subgraph solve path: device-resident graph state and the
+// per-part pipeline (reference fapGraph::run, fap/fap.cpp:92-181), in a plain
+// (one launch sequence per part) and a batched (one launch per stage for all
+// requested parts) form.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "fap_b200.h"
+#include "fap_common.cuh"
+#include "fap_internal.h"
+
+using namespace fapb;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define FAP_CK(call)                                                                     \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess) {                                                             \
+      if (e_ == cudaErrorMemoryAllocation) {                                             \
+        cudaGetLastError();                                                              \
+        return fail(FAP_ERR_NOMEM, "%s: %s", #call, cudaGetErrorString(e_));             \
+      }                                                                                  \
+      return fail(FAP_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_));                \
+    }                                                                                    \
+  } while (0)
+
+#define FAP_TRY(expr)         \
+  do {                        \
+    int r_ = (expr);          \
+    if (r_ != FAP_OK) return r_; \
+  } while (0)
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+  int ensure(size_t want) {
+    if (want <= bytes) return FAP_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    if (want == 0) return FAP_OK;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      p = nullptr;
+      return fail(FAP_ERR_NOMEM, "cudaMalloc(%zu bytes): %s", want, cudaGetErrorString(e));
+    }
+    bytes = want;
+    return FAP_OK;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  template <typename T>
+  T *as() const { return reinterpret_cast<T *>(p); }
+};
+
+// RAII: make the context's device current for the duration of a call.
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+}  // namespace
+
+struct fap_ctx {
+  int device = 0;
+  int sm_count = 0;
+  cudaStream_t stream = nullptr;
+  cudaStream_t own = nullptr;
+  cudaEvent_t ev[6] = {};
+  DevBuf scratch;     // fap_op_floyd padding copy
+  DevBuf status;      // int device status for device-pointer ops
+  DevBuf sink;        // microbenchmark sink
+  int64_t launches = 0;
+};
+
+struct fap_dgraph {
+  fap_ctx *ctx = nullptr;
+  int32_t n = 0;
+  int64_t m = 0;
+  int dtype = FAP_DTYPE_F32;
+  DevBuf ro, col, w;
+  // partition
+  int32_t K = 0;
+  std::vector<int32_t> gid, st2ed, ed2st, vnum, voff, bnum;
+  DevBuf d_gid, d_st2ed, d_ed2st;
+  // output
+  int64_t ldD = 0;
+  int64_t max_rows = 0;
+  DevBuf D;
+  std::vector<int64_t> row_base;  // per part (1..K), -1 = not resident
+  // batch state
+  DevBuf F, d_parts, d_work, d_src, d_srcrows, d_status, d_checks, staging;
+  std::vector<PartDesc> parts;
+  std::vector<MPWork> work;
+  std::vector<int32_t> src;
+  std::vector<int64_t> srcrows;
+  std::vector<int32_t> part_src_off, part_work_off;  // per batch index, size nparts+1
+  std::vector<int32_t> last_ids;
+  int64_t f_elems = 0;
+  int max_ldf = 0, max_b = 0, max_s = 0;
+  // tuning
+  double sssp_delta = -1.0;  // <0: automatic
+  int64_t sssp_max_rounds = -1;  // <0: 8n + 1024
+  // last solve
+  int last_mode = -1;
+  float timing[5] = {-1, -1, -1, -1, -1};
+  int64_t launches = 0;
+};
+
+// ---------------------------------------------------------------------------
+// misc
+// ---------------------------------------------------------------------------
+extern "C" const char *fap_last_error(void) { return g_err.c_str(); }
+extern "C" int fap_version(void) { return 0x000100; }
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+extern "C" int fap_ctx_create(int device, fap_ctx **out) {
+  if (!out) return fail(FAP_ERR_INVALID, "fap_ctx_create: out is NULL");
+  *out = nullptr;
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    return fail(FAP_ERR_CUDA, "no CUDA device available (%s)", cudaGetErrorString(e));
+  }
+  if (device < 0 || device >= count) return fail(FAP_ERR_INVALID, "device %d out of range", device);
+  DeviceGuard g(device);
+  fap_ctx *c = new fap_ctx();
+  c->device = device;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) {
+    delete c;
+    return fail(FAP_ERR_CUDA, "cudaGetDeviceProperties failed");
+  }
+  if (prop.major < 10) {
+    delete c;
+    return fail(FAP_ERR_CUDA, "device %d is sm_%d%d; this library is built for sm_100a", device,
+                prop.major, prop.minor);
+  }
+  c->sm_count = prop.multiProcessorCount;
+  if (cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return fail(FAP_ERR_CUDA, "cudaStreamCreate failed");
+  }
+  c->stream = c->own;
+  for (auto &ev : c->ev) cudaEventCreate(&ev);
+  if (c->status.ensure(sizeof(int)) != FAP_OK) {
+    fap_ctx_destroy(c);
+    return FAP_ERR_NOMEM;
+  }
+  *out = c;
+  return FAP_OK;
+}
+
+extern "C" int fap_ctx_destroy(fap_ctx *c) {
+  if (!c) return FAP_OK;
+  DeviceGuard g(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  c->scratch.release();
+  c->status.release();
+  c->sink.release();
+  for (auto &ev : c->ev)
+    if (ev) cudaEventDestroy(ev);
+  if (c->own) cudaStreamDestroy(c->own);
+  delete c;
+  return FAP_OK;
+}
+
+extern "C" int fap_ctx_set_stream(fap_ctx *c, void *stream) {
+  if (!c) return fail(FAP_ERR_INVALID, "ctx is NULL");
+  c->stream = stream ? reinterpret_cast<cudaStream_t>(stream) : c->own;
+  return FAP_OK;
+}
+
+extern "C" int fap_ctx_get_stream(fap_ctx *c, void **stream) {
+  if (!c || !stream) return fail(FAP_ERR_INVALID, "NULL argument");
+  *stream = reinterpret_cast<void *>(c->stream);
+  return FAP_OK;
+}
+
+extern "C" int fap_ctx_sync(fap_ctx *c) {
+  if (!c) return fail(FAP_ERR_INVALID, "ctx is NULL");
+  DeviceGuard g(c->device);
+  FAP_CK(cudaStreamSynchronize(c->stream));
+  return FAP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// graph
+// ---------------------------------------------------------------------------
+extern "C" int fap_graph_create(fap_ctx *ctx, int32_t n, int64_t m, const int32_t *row_offset,
+                                const int32_t *col_val, const float *weight, int dtype,
+                                fap_dgraph **out) {
+  if (!ctx || !out) return fail(FAP_ERR_INVALID, "NULL argument");
+  *out = nullptr;
+  if (n <= 0) return fail(FAP_ERR_INVALID, "n must be positive (got %d)", n);
+  if (m < 0 || (m > 0 && (!col_val || !weight)) || !row_offset)
+    return fail(FAP_ERR_INVALID, "bad CSR arguments");
+  if (m > INT32_MAX) return fail(FAP_ERR_INVALID, "m exceeds int32 edge indexing");
+  if (row_offset[0] != 0) return fail(FAP_ERR_INVALID, "row_offset[0] must be 0");
+  for (int32_t v = 0; v < n; v++)
+    if (row_offset[v + 1] < row_offset[v]) return fail(FAP_ERR_INVALID, "row_offset not monotone at %d", v);
+  const int64_t used = row_offset[n];
+  if (used > m) return fail(FAP_ERR_INVALID, "row_offset[n]=%lld exceeds m=%lld", (long long)used, (long long)m);
+  bool integral = true;
+  for (int64_t e = 0; e < used; e++) {
+    if (col_val[e] < 0 || col_val[e] >= n)
+      return fail(FAP_ERR_INVALID, "col_val[%lld]=%d out of range", (long long)e, col_val[e]);
+    const float x = weight[e];
+    if (!(x >= 0.0f) || !std::isfinite(x))
+      return fail(FAP_ERR_INVALID, "weight[%lld] must be finite and non-negative", (long long)e);
+    if (x != std::floor(x) || x > (float)FAP_MAX_INT_WEIGHT) integral = false;
+  }
+  int dt = dtype;
+  if (dt == FAP_DTYPE_AUTO) dt = integral ? FAP_DTYPE_I32 : FAP_DTYPE_F32;
+  if (dt == FAP_DTYPE_I32 && !integral)
+    return fail(FAP_ERR_RANGE, "int32 distances need integral weights <= %d", FAP_MAX_INT_WEIGHT);
+  if (dt != FAP_DTYPE_I32 && dt != FAP_DTYPE_F32) return fail(FAP_ERR_INVALID, "bad dtype %d", dtype);
+
+  DeviceGuard g(ctx->device);
+  fap_dgraph *G = new fap_dgraph();
+  G->ctx = ctx;
+  G->n = n;
+  G->m = used;
+  G->dtype = dt;
+  G->ldD = round_up(n, kLdAlign);
+  auto cleanup = [&](int rc) {
+    fap_graph_destroy(G);
+    return rc;
+  };
+  int rc;
+  if ((rc = G->ro.ensure((size_t)(n + 1) * 4)) != FAP_OK) return cleanup(rc);
+  if ((rc = G->col.ensure((size_t)std::max<int64_t>(used, 1) * 4)) != FAP_OK) return cleanup(rc);
+  if ((rc = G->w.ensure((size_t)std::max<int64_t>(used, 1) * 4)) != FAP_OK) return cleanup(rc);
+  cudaError_t e = cudaMemcpy(G->ro.p, row_offset, (size_t)(n + 1) * 4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && used > 0)
+    e = cudaMemcpy(G->col.p, col_val, (size_t)used * 4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && used > 0) {
+    if (dt == FAP_DTYPE_I32) {
+      std::vector<int32_t> wi((size_t)used);
+      for (int64_t i = 0; i < used; i++) wi[i] = (int32_t)weight[i];
+      e = cudaMemcpy(G->w.p, wi.data(), (size_t)used * 4, cudaMemcpyHostToDevice);
+    } else {
+      e = cudaMemcpy(G->w.p, weight, (size_t)used * 4, cudaMemcpyHostToDevice);
+    }
+  }
+  if (e != cudaSuccess) return cleanup(fail(FAP_ERR_CUDA, "CSR upload: %s", cudaGetErrorString(e)));
+  if ((rc = G->d_status.ensure(sizeof(int))) != FAP_OK) return cleanup(rc);
+  cudaMemset(G->d_status.p, 0, sizeof(int));
+  *out = G;
+  return FAP_OK;
+}
+
+extern "C" int fap_graph_destroy(fap_dgraph *G) {
+  if (!G) return FAP_OK;
+  DeviceGuard g(G->ctx->device);
+  cudaStreamSynchronize(G->ctx->stream);
+  for (DevBuf *b : {&G->ro, &G->col, &G->w, &G->d_gid, &G->d_st2ed, &G->d_ed2st, &G->D, &G->F,
+                    &G->d_parts, &G->d_work, &G->d_src, &G->d_srcrows, &G->d_status,
+                    &G->d_checks, &G->staging})
+    b->release();
+  delete G;
+  return FAP_OK;
+}
+
+extern "C" int fap_graph_dtype(const fap_dgraph *G) { return G ? G->dtype : FAP_ERR_INVALID; }
+
+extern "C" int fap_graph_set_parts(fap_dgraph *G, int32_t K, const int32_t *graph_id,
+                                   const int32_t *st2ed, const int32_t *ver_num,
+                                   const int32_t *ver_offset, const int32_t *bdy_num) {
+  if (!G || !graph_id || !st2ed || !ver_num || !ver_offset || !bdy_num)
+    return fail(FAP_ERR_INVALID, "NULL argument");
+  const int32_t n = G->n;
+  if (K < 1 || K > n) return fail(FAP_ERR_PARTITION, "K=%d must be in [1, n=%d]", K, n);
+  std::vector<int32_t> ed2st(n, -1);
+  for (int32_t i = 0; i < n; i++) {
+    const int32_t v = st2ed[i];
+    if (v < 0 || v >= n || ed2st[v] != -1) return fail(FAP_ERR_PARTITION, "st2ed is not a permutation");
+    ed2st[v] = i;
+    if (graph_id[v] < 1 || graph_id[v] > K)
+      return fail(FAP_ERR_PARTITION, "graph_id[%d]=%d outside 1..K", v, graph_id[v]);
+  }
+  int64_t off = 0;
+  for (int32_t p = 1; p <= K; p++) {
+    if (ver_offset[p] != off) return fail(FAP_ERR_PARTITION, "ver_offset[%d] inconsistent", p);
+    if (ver_num[p] < 0 || bdy_num[p] < 0 || bdy_num[p] > ver_num[p])
+      return fail(FAP_ERR_PARTITION, "part %d counts inconsistent", p);
+    for (int32_t i = 0; i < ver_num[p]; i++)
+      if (graph_id[st2ed[off + i]] != p) return fail(FAP_ERR_PARTITION, "part %d block holds a foreign vertex", p);
+    off += ver_num[p];
+  }
+  if (off != n) return fail(FAP_ERR_PARTITION, "part sizes sum to %lld, not n", (long long)off);
+  DeviceGuard g(G->ctx->device);
+  G->K = K;
+  G->gid.assign(graph_id, graph_id + n);
+  G->st2ed.assign(st2ed, st2ed + n);
+  G->ed2st = std::move(ed2st);
+  G->vnum.assign(ver_num, ver_num + K + 1);
+  G->voff.assign(ver_offset, ver_offset + K + 1);
+  G->bnum.assign(bdy_num, bdy_num + K + 1);
+  G->row_base.assign(K + 1, -1);
+  G->last_ids.clear();
+  FAP_TRY(G->d_gid.ensure((size_t)n * 4));
+  FAP_TRY(G->d_st2ed.ensure((size_t)n * 4));
+  FAP_TRY(G->d_ed2st.ensure((size_t)n * 4));
+  FAP_CK(cudaMemcpy(G->d_gid.p, G->gid.data(), (size_t)n * 4, cudaMemcpyHostToDevice));
+  FAP_CK(cudaMemcpy(G->d_st2ed.p, G->st2ed.data(), (size_t)n * 4, cudaMemcpyHostToDevice));
+  FAP_CK(cudaMemcpy(G->d_ed2st.p, G->ed2st.data(), (size_t)n * 4, cudaMemcpyHostToDevice));
+  return FAP_OK;
+}
+
+extern "C" int fap_graph_reserve(fap_dgraph *G, int64_t max_rows) {
+  if (!G) return fail(FAP_ERR_INVALID, "NULL graph");
+  if (max_rows <= 0 || max_rows > G->n) max_rows = G->n;
+  DeviceGuard g(G->ctx->device);
+  cudaStreamSynchronize(G->ctx->stream);
+  const size_t bytes = (size_t)max_rows * (size_t)G->ldD * 4;
+  if (G->D.bytes < bytes) {
+    G->D.release();
+    FAP_TRY(G->D.ensure(bytes));
+  }
+  G->max_rows = max_rows;
+  std::fill(G->row_base.begin(), G->row_base.end(), -1);
+  G->last_ids.clear();
+  return FAP_OK;
+}
+
+namespace {
+
+// Builds (or reuses) the batch descriptors for the requested parts.
+int prepare_batch(fap_dgraph *G, const std::vector<int32_t> &ids) {
+  const bool same = (ids == G->last_ids);
+  if (same) return FAP_OK;
+  const int64_t n = G->n;
+  const bool full = (G->max_rows == n);
+  // rows
+  std::vector<int64_t> base(ids.size());
+  int64_t next = 0;
+  for (size_t i = 0; i < ids.size(); i++) {
+    const int32_t p = ids[i];
+    if (full) {
+      base[i] = G->voff[p];
+    } else {
+      base[i] = next;
+      next += G->vnum[p];
+    }
+  }
+  if (!full && next > G->max_rows)
+    return fail(FAP_ERR_NOMEM, "requested parts need %lld rows, %lld reserved", (long long)next,
+                (long long)G->max_rows);
+  G->parts.clear();
+  G->work.clear();
+  G->src.clear();
+  G->srcrows.clear();
+  G->part_src_off.assign(1, 0);
+  G->part_work_off.assign(1, 0);
+  int64_t foff = 0;
+  G->max_ldf = 0;
+  G->max_b = 0;
+  G->max_s = 0;
+  for (size_t i = 0; i < ids.size(); i++) {
+    const int32_t p = ids[i];
+    PartDesc d{};
+    d.part = p;
+    d.start = G->voff[p];
+    d.s = G->vnum[p];
+    d.b = G->bnum[p];
+    d.row_base = base[i];
+    d.ldf = (int32_t)round_up(std::max(d.s, 1), kFloydTile);
+    d.f_off = foff;
+    foff += (int64_t)d.ldf * d.ldf;
+    G->max_ldf = std::max(G->max_ldf, d.ldf);
+    G->max_b = std::max(G->max_b, d.b);
+    G->max_s = std::max(G->max_s, d.s);
+    G->parts.push_back(d);
+    for (int32_t k = 0; k < d.b; k++) {
+      G->src.push_back(G->st2ed[d.start + k]);
+      G->srcrows.push_back(d.row_base + k);
+    }
+    G->part_src_off.push_back((int32_t)G->src.size());
+    for (int32_t m0 = 0; m0 < d.s - d.b; m0 += kMinplusBM) G->work.push_back(MPWork{(int32_t)i, m0});
+    G->part_work_off.push_back((int32_t)G->work.size());
+  }
+  G->f_elems = foff;
+  FAP_TRY(G->F.ensure((size_t)std::max<int64_t>(foff, 1) * 4));
+  FAP_TRY(G->d_parts.ensure(std::max<size_t>(G->parts.size(), 1) * sizeof(PartDesc)));
+  FAP_TRY(G->d_work.ensure(std::max<size_t>(G->work.size(), 1) * sizeof(MPWork)));
+  FAP_TRY(G->d_src.ensure(std::max<size_t>(G->src.size(), 1) * 4));
+  FAP_TRY(G->d_srcrows.ensure(std::max<size_t>(G->srcrows.size(), 1) * 8));
+  cudaStream_t st = G->ctx->stream;
+  FAP_CK(cudaStreamSynchronize(st));
+  FAP_CK(cudaMemcpy(G->d_parts.p, G->parts.data(), G->parts.size() * sizeof(PartDesc), cudaMemcpyHostToDevice));
+  if (!G->work.empty())
+    FAP_CK(cudaMemcpy(G->d_work.p, G->work.data(), G->work.size() * sizeof(MPWork), cudaMemcpyHostToDevice));
+  if (!G->src.empty()) {
+    FAP_CK(cudaMemcpy(G->d_src.p, G->src.data(), G->src.size() * 4, cudaMemcpyHostToDevice));
+    FAP_CK(cudaMemcpy(G->d_srcrows.p, G->srcrows.data(), G->srcrows.size() * 8, cudaMemcpyHostToDevice));
+  }
+  // Rows of other parts may have been overwritten by this batch.
+  std::fill(G->row_base.begin(), G->row_base.end(), -1);
+  G->last_ids = ids;
+  return FAP_OK;
+}
+
+template <typename T>
+T sssp_delta_for(const fap_dgraph *G) {
+  if (G->sssp_delta > 0) {
+    const double d = std::min<double>(G->sssp_delta, (double)Dist<T>::inf());
+    return (T)d;
+  }
+  return Dist<T>::inf();  // plain frontier Bellman-Ford
+}
+
+template <typename T>
+int run_solve(fap_dgraph *G, int mode) {
+  fap_ctx *c = G->ctx;
+  cudaStream_t st = c->stream;
+  const int np = (int)G->parts.size();
+  const T *w = G->w.as<const T>();
+  T *D = G->D.as<T>();
+  T *F = G->F.as<T>();
+  const int32_t *ro = G->ro.as<const int32_t>(), *col = G->col.as<const int32_t>();
+  const PartDesc *dp = G->d_parts.as<const PartDesc>();
+  const MPWork *dw = G->d_work.as<const MPWork>();
+  const int32_t *src = G->d_src.as<const int32_t>();
+  const int64_t *srow = G->d_srcrows.as<const int64_t>();
+  const int32_t *gid = G->d_gid.as<const int32_t>(), *st2ed = G->d_st2ed.as<const int32_t>(),
+                *ed2st = G->d_ed2st.as<const int32_t>();
+  int *status = G->d_status.as<int>();
+  const T delta = sssp_delta_for<T>(G);
+  const int64_t max_rounds = G->sssp_max_rounds > 0 ? G->sssp_max_rounds : 8 * (int64_t)G->n + 1024;
+  int64_t L = 0;
+  FAP_CK(cudaMemsetAsync(status, 0, sizeof(int), st));
+  for (int i = 0; i < 5; i++) G->timing[i] = -1.0f;
+  if (mode == FAP_MODE_BATCHED) {
+    FAP_CK(cudaEventRecord(c->ev[0], st));
+    FAP_CK(launch_sssp<T>(ro, col, w, G->n, src, srow, (int)G->src.size(), D, G->ldD, G->ldD,
+                          delta, max_rounds, status, st, &L));
+    FAP_CK(cudaEventRecord(c->ev[1], st));
+    FAP_CK(launch_gather<T>(dp, np, G->max_ldf, ro, col, w, gid, st2ed, ed2st, D, G->ldD, F, st, &L));
+    FAP_CK(cudaEventRecord(c->ev[2], st));
+    FAP_CK(launch_floyd_parts<T>(dp, np, F, D, G->ldD, st2ed, st, &L));
+    FAP_CK(cudaEventRecord(c->ev[3], st));
+    FAP_CK(launch_minplus_parts<T>(dp, dw, (int)G->work.size(), G->n, F, D, G->ldD, gid, ed2st, st, &L));
+    FAP_CK(cudaEventRecord(c->ev[4], st));
+  } else {
+    FAP_CK(cudaEventRecord(c->ev[0], st));
+    for (int i = 0; i < np; i++) {
+      const PartDesc &d = G->parts[i];
+      const int s0 = G->part_src_off[i], s1 = G->part_src_off[i + 1];
+      const int w0 = G->part_work_off[i], w1 = G->part_work_off[i + 1];
+      FAP_CK(launch_sssp<T>(ro, col, w, G->n, src + s0, srow + s0, s1 - s0, D, G->ldD, G->ldD,
+                            delta, max_rounds, status, st, &L));
+      FAP_CK(launch_gather<T>(dp + i, 1, d.ldf, ro, col, w, gid, st2ed, ed2st, D, G->ldD, F, st, &L));
+      FAP_CK(launch_floyd_matrix<T>(F + d.f_off, d.ldf, d.ldf / kFloydTile, st, &L));
+      FAP_CK(launch_bdy_scatter<T>(dp + i, 1, F, D, G->ldD, st2ed, d.b, d.s, st, &L));
+      FAP_CK(launch_minplus_parts<T>(dp, dw + w0, w1 - w0, G->n, F, D, G->ldD, gid, ed2st, st, &L));
+    }
+    FAP_CK(cudaEventRecord(c->ev[4], st));
+  }
+  G->launches = L;
+  c->launches += L;
+  return FAP_OK;
+}
+
+int read_status(fap_dgraph *G) {
+  int h = 0;
+  FAP_CK(cudaMemcpy(&h, G->d_status.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (h == kDevSsspRoundLimit)
+    return fail(FAP_ERR_NOT_CONVERGED, "SSSP hit its round bound");
+  if (h != kDevOk) return fail(FAP_ERR_DEVICE, "device-side error %d", h);
+  return FAP_OK;
+}
+
+}  // namespace
+
+extern "C" int fap_solve(fap_dgraph *G, const int32_t *parts, int32_t count, int mode) {
+  if (!G) return fail(FAP_ERR_INVALID, "NULL graph");
+  if (G->K == 0) return fail(FAP_ERR_STATE, "fap_solve before fap_graph_set_parts");
+  if (mode != FAP_MODE_PLAIN && mode != FAP_MODE_BATCHED) return fail(FAP_ERR_INVALID, "bad mode %d", mode);
+  std::vector<int32_t> ids;
+  if (parts == nullptr) {
+    for (int32_t p = 1; p <= G->K; p++) ids.push_back(p);
+  } else {
+    if (count < 0) return fail(FAP_ERR_INVALID, "negative count");
+    std::vector<char> seen(G->K + 1, 0);
+    for (int32_t i = 0; i < count; i++) {
+      const int32_t p = parts[i];
+      if (p < 1 || p > G->K) return fail(FAP_ERR_INVALID, "part id %d outside 1..%d", p, G->K);
+      if (seen[p]) return fail(FAP_ERR_INVALID, "part id %d requested twice", p);
+      seen[p] = 1;
+      ids.push_back(p);
+    }
+  }
+  if (ids.empty()) return FAP_OK;
+  DeviceGuard g(G->ctx->device);
+  if (G->max_rows == 0) FAP_TRY(fap_graph_reserve(G, 0));
+  FAP_TRY(prepare_batch(G, ids));
+  int rc = (G->dtype == FAP_DTYPE_I32) ? run_solve<int32_t>(G, mode) : run_solve<float>(G, mode);
+  if (rc != FAP_OK) return rc;
+  for (const PartDesc &d : G->parts) G->row_base[d.part] = d.row_base;
+  G->last_mode = mode;
+  return FAP_OK;
+}
+
+extern "C" int fap_graph_check(fap_dgraph *G) {
+  if (!G) return fail(FAP_ERR_INVALID, "NULL graph");
+  DeviceGuard g(G->ctx->device);
+  FAP_CK(cudaStreamSynchronize(G->ctx->stream));
+  FAP_TRY(read_status(G));
+  return FAP_OK;
+}
+
+extern "C" int fap_graph_last_timing(fap_dgraph *G, float *ms5) {
+  if (!G || !ms5) return fail(FAP_ERR_INVALID, "NULL argument");
+  for (int i = 0; i < 5; i++) ms5[i] = -1.0f;
+  if (G->last_mode < 0) return fail(FAP_ERR_STATE, "no solve yet");
+  DeviceGuard g(G->ctx->device);
+  fap_ctx *c = G->ctx;
+  FAP_CK(cudaEventSynchronize(c->ev[4]));
+  float t;
+  FAP_CK(cudaEventElapsedTime(&t, c->ev[0], c->ev[4]));
+  ms5[4] = t;
+  if (G->last_mode == FAP_MODE_BATCHED) {
+    for (int i = 0; i < 4; i++) {
+      FAP_CK(cudaEventElapsedTime(&t, c->ev[i], c->ev[i + 1]));
+      ms5[i] = t;
+    }
+  }
+  for (int i = 0; i < 5; i++) G->timing[i] = ms5[i];
+  return FAP_OK;
+}
+
+extern "C" int fap_graph_last_launches(fap_dgraph *G, int64_t *count) {
+  if (!G || !count) return fail(FAP_ERR_INVALID, "NULL argument");
+  *count = G->launches;
+  return FAP_OK;
+}
+
+extern "C" int fap_graph_block(fap_dgraph *G, int32_t part, void **dev_ptr, int64_t *rows,
+                               int64_t *ld) {
+  if (!G || !dev_ptr || !rows || !ld) return fail(FAP_ERR_INVALID, "NULL argument");
+  if (part < 1 || part > G->K) return fail(FAP_ERR_INVALID, "part %d outside 1..%d", part, G->K);
+  if (G->row_base[part] < 0) return fail(FAP_ERR_STATE, "part %d is not resident", part);
+  *dev_ptr = G->D.as<char>() + (size_t)G->row_base[part] * G->ldD * 4;
+  *rows = G->vnum[part];
+  *ld = G->ldD;
+  return FAP_OK;
+}
+
+extern "C" int fap_graph_copy_block(fap_dgraph *G, int32_t part, void *host, int out_dtype) {
+  if (!G || !host) return fail(FAP_ERR_INVALID, "NULL argument");
+  void *dp;
+  int64_t rows, ld;
+  FAP_TRY(fap_graph_block(G, part, &dp, &rows, &ld));
+  DeviceGuard g(G->ctx->device);
+  cudaStream_t st = G->ctx->stream;
+  const int64_t n = G->n;
+  if (rows == 0) return FAP_OK;
+  if (out_dtype == G->dtype) {
+    FAP_CK(cudaMemcpy2DAsync(host, (size_t)n * 4, dp, (size_t)ld * 4, (size_t)n * 4, (size_t)rows,
+                             cudaMemcpyDeviceToHost, st));
+  } else if (G->dtype == FAP_DTYPE_I32 && out_dtype == FAP_DTYPE_F32) {
+    FAP_TRY(G->staging.ensure((size_t)rows * n * 4));
+    int64_t L = 0;
+    FAP_CK(launch_i32_to_f32(reinterpret_cast<const int32_t *>(dp), rows, n, ld,
+                             G->staging.as<float>(), st, &L));
+    FAP_CK(cudaMemcpyAsync(host, G->staging.p, (size_t)rows * n * 4, cudaMemcpyDeviceToHost, st));
+  } else {
+    return fail(FAP_ERR_INVALID, "cannot copy %s distances as int32",
+                G->dtype == FAP_DTYPE_F32 ? "float" : "?");
+  }
+  FAP_CK(cudaStreamSynchronize(st));
+  FAP_TRY(read_status(G));
+  return FAP_OK;
+}
+
+extern "C" int fap_graph_block_checksums(fap_dgraph *G, int32_t part, uint64_t *host_out) {
+  if (!G || !host_out) return fail(FAP_ERR_INVALID, "NULL argument");
+  if (G->dtype != FAP_DTYPE_I32) return fail(FAP_ERR_INVALID, "checksums need the int32 path");
+  void *dp;
+  int64_t rows, ld;
+  FAP_TRY(fap_graph_block(G, part, &dp, &rows, &ld));
+  if (rows == 0) return FAP_OK;
+  DeviceGuard g(G->ctx->device);
+  cudaStream_t st = G->ctx->stream;
+  FAP_TRY(G->d_checks.ensure((size_t)rows * 8));
+  int64_t L = 0;
+  FAP_CK(launch_row_checksums(reinterpret_cast<const int32_t *>(dp), rows, G->n, ld,
+                              G->d_checks.as<uint64_t>(), st, &L));
+  FAP_CK(cudaMemcpyAsync(host_out, G->d_checks.p, (size_t)rows * 8, cudaMemcpyDeviceToHost, st));
+  FAP_CK(cudaStreamSynchronize(st));
+  FAP_TRY(read_status(G));
+  return FAP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// device-pointer operators
+// ---------------------------------------------------------------------------
+namespace {
+int read_ctx_status(fap_ctx *c) {
+  int h = 0;
+  FAP_CK(cudaMemcpyAsync(&h, c->status.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  FAP_CK(cudaStreamSynchronize(c->stream));
+  if (h == kDevSsspRoundLimit) return fail(FAP_ERR_NOT_CONVERGED, "SSSP hit its round bound");
+  if (h != kDevOk) return fail(FAP_ERR_DEVICE, "device-side error %d", h);
+  return FAP_OK;
+}
+}  // namespace
+
+extern "C" int fap_op_sssp(fap_ctx *c, int dtype, int32_t n, int64_t m, const int32_t *row_offset,
+                           const int32_t *col_val, const void *weight, const int32_t *sources,
+                           int32_t num_sources, void *out, int64_t ld_out) {
+  if (!c || !row_offset || (m > 0 && (!col_val || !weight)) || (num_sources > 0 && (!sources || !out)))
+    return fail(FAP_ERR_INVALID, "NULL argument");
+  if (n <= 0 || m < 0 || num_sources < 0 || ld_out < n) return fail(FAP_ERR_INVALID, "bad sizes");
+  if ((size_t)ceil_div(n, 32) * 8 > 227 * 1024)
+    return fail(FAP_ERR_INVALID, "n=%d exceeds the shared-memory frontier limit", n);
+  DeviceGuard g(c->device);
+  FAP_CK(cudaMemsetAsync(c->status.p, 0, sizeof(int), c->stream));
+  int64_t L = 0;
+  const int64_t rounds = 8 * (int64_t)n + 1024;
+  if (dtype == FAP_DTYPE_I32) {
+    FAP_CK(launch_sssp<int32_t>(row_offset, col_val, (const int32_t *)weight, n, sources, nullptr,
+                                num_sources, (int32_t *)out, ld_out, n, kInfI32, rounds,
+                                c->status.as<int>(), c->stream, &L));
+  } else if (dtype == FAP_DTYPE_F32) {
+    FAP_CK(launch_sssp<float>(row_offset, col_val, (const float *)weight, n, sources, nullptr,
+                              num_sources, (float *)out, ld_out, n, kInfF32, rounds,
+                              c->status.as<int>(), c->stream, &L));
+  } else {
+    return fail(FAP_ERR_INVALID, "bad dtype %d", dtype);
+  }
+  c->launches += L;
+  return read_ctx_status(c);
+}
+
+extern "C" int fap_op_floyd(fap_ctx *c, int dtype, int32_t s, void *mat, int64_t ld) {
+  if (!c || (s > 0 && !mat)) return fail(FAP_ERR_INVALID, "NULL argument");
+  if (s < 0 || ld < s) return fail(FAP_ERR_INVALID, "bad sizes");
+  if (s == 0) return FAP_OK;
+  if (dtype != FAP_DTYPE_I32 && dtype != FAP_DTYPE_F32) return fail(FAP_ERR_INVALID, "bad dtype");
+  DeviceGuard g(c->device);
+  cudaStream_t st = c->stream;
+  const int64_t ldp = round_up(s, kFloydTile);
+  FAP_TRY(c->scratch.ensure((size_t)ldp * ldp * 4));
+  int64_t L = 0;
+  // padded copy: sentinel everywhere, then the matrix
+  if (dtype == FAP_DTYPE_I32)
+    FAP_CK(launch_fill<int32_t>(c->scratch.as<int32_t>(), ldp, ldp, ldp, kInfI32, st, &L));
+  else
+    FAP_CK(launch_fill<float>(c->scratch.as<float>(), ldp, ldp, ldp, kInfF32, st, &L));
+  FAP_CK(cudaMemcpy2DAsync(c->scratch.p, (size_t)ldp * 4, mat, (size_t)ld * 4, (size_t)s * 4, (size_t)s,
+                           cudaMemcpyDeviceToDevice, st));
+  if (dtype == FAP_DTYPE_I32)
+    FAP_CK(launch_floyd_matrix<int32_t>(c->scratch.as<int32_t>(), ldp, (int)(ldp / kFloydTile), st, &L));
+  else
+    FAP_CK(launch_floyd_matrix<float>(c->scratch.as<float>(), ldp, (int)(ldp / kFloydTile), st, &L));
+  FAP_CK(cudaMemcpy2DAsync(mat, (size_t)ld * 4, c->scratch.p, (size_t)ldp * 4, (size_t)s * 4, (size_t)s,
+                           cudaMemcpyDeviceToDevice, st));
+  FAP_CK(cudaStreamSynchronize(st));
+  c->launches += L;
+  return FAP_OK;
+}
+
+extern "C" int fap_op_minplus(fap_ctx *c, int dtype, int32_t M, int32_t N, int32_t K, const void *A,
+                              int64_t lda, const void *B, int64_t ldb, void *C, int64_t ldc) {
+  if (!c) return fail(FAP_ERR_INVALID, "NULL ctx");
+  if (M < 0 || N < 0 || K < 0) return fail(FAP_ERR_INVALID, "negative size");
+  if (M == 0 || N == 0) return FAP_OK;
+  if (!C || (K > 0 && (!A || !B))) return fail(FAP_ERR_INVALID, "NULL matrix");
+  if (ldc < N || (K > 0 && (lda < K || ldb < N))) return fail(FAP_ERR_INVALID, "bad leading dimension");
+  DeviceGuard g(c->device);
+  int64_t L = 0;
+  if (dtype == FAP_DTYPE_I32)
+    FAP_CK(launch_minplus_generic<int32_t>(M, N, K, (const int32_t *)A, lda, (const int32_t *)B, ldb,
+                                           (int32_t *)C, ldc, c->stream, &L));
+  else if (dtype == FAP_DTYPE_F32)
+    FAP_CK(launch_minplus_generic<float>(M, N, K, (const float *)A, lda, (const float *)B, ldb,
+                                         (float *)C, ldc, c->stream, &L));
+  else
+    return fail(FAP_ERR_INVALID, "bad dtype %d", dtype);
+  FAP_CK(cudaStreamSynchronize(c->stream));
+  c->launches += L;
+  return FAP_OK;
+}
+
+extern "C" int fap_measure_relax_peak(fap_ctx *c, int dtype, double *relax_per_s) {
+  if (!c || !relax_per_s) return fail(FAP_ERR_INVALID, "NULL argument");
+  DeviceGuard g(c->device);
+  cudaStream_t st = c->stream;
+  FAP_TRY(c->sink.ensure(64));
+  const int blocks = c->sm_count * 8;
+  const int iters = 4096;
+  double count = 0;
+  float best = 1e30f;
+  for (int rep = 0; rep < 4; rep++) {
+    FAP_CK(cudaEventRecord(c->ev[0], st));
+    if (dtype == FAP_DTYPE_I32)
+      FAP_CK(launch_relax_peak<int32_t>(c->sink.as<int32_t>(), blocks, iters, st, &count));
+    else
+      FAP_CK(launch_relax_peak<float>(c->sink.as<float>(), blocks, iters, st, &count));
+    FAP_CK(cudaEventRecord(c->ev[1], st));
+    FAP_CK(cudaEventSynchronize(c->ev[1]));
+    float t;
+    FAP_CK(cudaEventElapsedTime(&t, c->ev[0], c->ev[1]));
+    if (rep > 0) best = std::min(best, t);
+  }
+  *relax_per_s = count / (best * 1e-3);
+  return FAP_OK;
+}
+
+extern "C" int fap_graph_sssp_rows(fap_dgraph *G, const int32_t *sources, int32_t count,
+                                   float *host_out) {
+  if (!G || (count > 0 && (!sources || !host_out))) return fail(FAP_ERR_INVALID, "NULL argument");
+  if (count < 0) return fail(FAP_ERR_INVALID, "negative count");
+  if (count == 0) return FAP_OK;
+  for (int32_t i = 0; i < count; i++)
+    if (sources[i] < 0 || sources[i] >= G->n) return fail(FAP_ERR_INVALID, "source %d out of range", sources[i]);
+  DeviceGuard g(G->ctx->device);
+  cudaStream_t st = G->ctx->stream;
+  const int64_t n = G->n;
+  DevBuf srcs, rows;
+  FAP_TRY(srcs.ensure((size_t)count * 4));
+  FAP_TRY(rows.ensure((size_t)count * n * 4));
+  int rc = FAP_OK;
+  int64_t L = 0;
+  const int64_t rounds = G->sssp_max_rounds > 0 ? G->sssp_max_rounds : 8 * n + 1024;
+  do {
+    cudaError_t e = cudaMemcpyAsync(srcs.p, sources, (size_t)count * 4, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(G->d_status.p, 0, sizeof(int), st);
+    if (e == cudaSuccess) {
+      if (G->dtype == FAP_DTYPE_I32)
+        e = launch_sssp<int32_t>(G->ro.as<int32_t>(), G->col.as<int32_t>(), G->w.as<int32_t>(), G->n,
+                                 srcs.as<int32_t>(), nullptr, count, rows.as<int32_t>(), n, n,
+                                 sssp_delta_for<int32_t>(G), rounds, G->d_status.as<int>(), st, &L);
+      else
+        e = launch_sssp<float>(G->ro.as<int32_t>(), G->col.as<int32_t>(), G->w.as<float>(), G->n,
+                               srcs.as<int32_t>(), nullptr, count, rows.as<float>(), n, n,
+                               sssp_delta_for<float>(G), rounds, G->d_status.as<int>(), st, &L);
+    }
+    if (e == cudaSuccess && G->dtype == FAP_DTYPE_I32)
+      e = launch_i32_to_f32(rows.as<int32_t>(), count, n, n, rows.as<float>(), st, &L);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(host_out, rows.p, (size_t)count * n * 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+      rc = fail(FAP_ERR_CUDA, "fap_graph_sssp_rows: %s", cudaGetErrorString(e));
+      break;
+    }
+    rc = read_status(G);
+  } while (0);
+  srcs.release();
+  rows.release();
+  G->ctx->launches += L;
+  return rc;
+}
+
+extern "C" int fap_graph_set_param(fap_dgraph *G, const char *key, double value) {
+  if (!G || !key) return fail(FAP_ERR_INVALID, "NULL argument");
+  if (std::strcmp(key, "sssp_delta") == 0) {
+    G->sssp_delta = (value > 0 && value < 1e8) ? value : -1.0;
+    return FAP_OK;
+  }
+  if (std::strcmp(key, "sssp_max_rounds") == 0) {
+    G->sssp_max_rounds = value >= 1 ? (int64_t)value : -1;
+    return FAP_OK;
+  }
+  return fail(FAP_ERR_INVALID, "unknown parameter '%s'", key);
+}

@@ -1,0 +1,440 @@
+// Kernels and launchers of the per-subgraph solve path (sm_100a).
+//
+// Stage map (reference fapGraph::run, fap/fap.cpp:92-181):
+//   stage 1   boundary SSSP            sssp_bitmap_kernel        (sssp.cuh)
+//   stage 2.1 Floyd matrix build       gather_kernel             (util_Myalgorithm.h:30-73)
+//   stage 2.2 Floyd-Warshall           floyd_part_kernel / floyd_phase*_kernel (floyd.cuh)
+//   stage 3.1 thin matrix              read in place from F      (util_Myalgorithm.h:88-95)
+//   stage 3.2 min-plus                 minplus_part_kernel       (minplus.h:51-65)
+//   stage 3.3 decode                   fused into the min-plus epilogue (inner rows) and
+//                                      the Floyd epilogue (boundary rows)
+//                                                                (util_Myalgorithm.h:75-86)
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "fap_common.cuh"
+#include "fap_internal.h"
+#include "floyd.cuh"
+#include "minplus_tile.cuh"
+#include "sssp.cuh"
+
+namespace fapb {
+
+using MPCfg32 = TileCfg<int32_t, kMinplusBM, kMinplusBN, 16, 8, 8>;
+
+template <typename T>
+using MPCfg = TileCfg<T, kMinplusBM, kMinplusBN, 16, 8, 8>;
+
+// ---------------------------------------------------------------------------
+// Stage 2.1: build each part's padded Floyd matrix.
+// CTA (i, pidx): row i of part pidx.  Inner rows take the part's own edges
+// in CSR order, a later duplicate overwriting an earlier one (resolved by
+// keeping the largest edge index per column), then a zero diagonal.
+// Boundary rows copy the SSSP row restricted to the part's columns.
+// Padding rows/columns hold the sentinel.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256)
+    gather_kernel(const PartDesc *__restrict__ parts, const int32_t *__restrict__ row_offset,
+                  const int32_t *__restrict__ col, const T *__restrict__ w,
+                  const int32_t *__restrict__ graph_id, const int32_t *__restrict__ st2ed,
+                  const int32_t *__restrict__ ed2st, const T *__restrict__ D, int64_t ldD,
+                  T *__restrict__ F) {
+  extern __shared__ int32_t winner[];
+  const PartDesc pd = parts[blockIdx.y];
+  const int i = blockIdx.x;
+  if (i >= pd.ldf) return;
+  const T inf = Dist<T>::inf();
+  T *Fi = F + pd.f_off + (int64_t)i * pd.ldf;
+  if (i >= pd.s) {
+    for (int j = threadIdx.x; j < pd.ldf; j += blockDim.x) Fi[j] = inf;
+    return;
+  }
+  if (i < pd.b) {
+    const T *Si = D + (pd.row_base + i) * ldD;
+    for (int j = threadIdx.x; j < pd.ldf; j += blockDim.x) {
+      T v = inf;
+      if (j < pd.s) v = (j == i) ? T(0) : Si[__ldg(st2ed + pd.start + j)];
+      Fi[j] = v;
+    }
+    return;
+  }
+  for (int j = threadIdx.x; j < pd.s; j += blockDim.x) winner[j] = -1;
+  __syncthreads();
+  const int v = st2ed[pd.start + i];
+  const int e0 = row_offset[v], e1 = row_offset[v + 1];
+  for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+    const int nb = __ldg(col + e);
+    if (__ldg(graph_id + nb) != pd.part) continue;
+    const int j = __ldg(ed2st + nb) - pd.start;
+    if (j >= 0 && j < pd.s) atomicMax(&winner[j], e);
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < pd.ldf; j += blockDim.x) {
+    T val = inf;
+    if (j < pd.s) {
+      if (j == i) val = T(0);
+      else if (winner[j] >= 0) val = __ldg(w + winner[j]);
+    }
+    Fi[j] = val;
+  }
+}
+
+template <typename T>
+cudaError_t launch_gather(const PartDesc *parts, int nparts, int max_ldf, const int32_t *row_offset,
+                          const int32_t *col, const T *w, const int32_t *graph_id,
+                          const int32_t *st2ed, const int32_t *ed2st, const T *D, int64_t ldD,
+                          T *F, cudaStream_t stream, int64_t *launches) {
+  if (nparts <= 0) return cudaSuccess;
+  size_t smem = (size_t)max_ldf * sizeof(int32_t);
+  auto kern = gather_kernel<T>;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  kern<<<dim3(max_ldf, nparts), 256, smem, stream>>>(parts, row_offset, col, w, graph_id, st2ed,
+                                                     ed2st, D, ldD, F);
+  *launches += 1;
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Stage 1 launcher
+// ---------------------------------------------------------------------------
+template <typename T>
+cudaError_t launch_sssp(const int32_t *row_offset, const int32_t *col, const T *w, int n,
+                        const int32_t *sources, const int64_t *out_rows, int num_sources, T *out,
+                        int64_t ld, int64_t init_cols, T delta, int64_t max_rounds, int *status,
+                        cudaStream_t stream, int64_t *launches) {
+  if (num_sources <= 0) return cudaSuccess;
+  size_t smem = sssp_smem_bytes(n);
+  auto kern = sssp_bitmap_kernel<T>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  kern<<<num_sources, kSsspThreads, smem, stream>>>(row_offset, col, w, n, sources, out_rows,
+                                                     num_sources, out, ld, init_cols, delta,
+                                                     max_rounds, status);
+  *launches += 1;
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Stage 2.2: Floyd-Warshall
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS)
+    floyd_part_kernel(const PartDesc *__restrict__ parts, T *F, T *D, int64_t ldD,
+                      const int32_t *__restrict__ st2ed) {
+  extern __shared__ __align__(16) unsigned char fp_smem_raw[];
+  T *smem = reinterpret_cast<T *>(fp_smem_raw);
+  const PartDesc pd = parts[blockIdx.x];
+  T *mat = F + pd.f_off;
+  floyd_close_cta<T, kFloydTile>(mat, pd.ldf, pd.ldf / kFloydTile, smem);
+  // Decode of the boundary rows (util_Myalgorithm.h:75-86 for rows < b).
+  const int64_t cnt = (int64_t)pd.b * pd.s;
+  for (int64_t t = threadIdx.x; t < cnt; t += blockDim.x) {
+    const int i = (int)(t / pd.s), j = (int)(t % pd.s);
+    D[(pd.row_base + i) * ldD + st2ed[pd.start + j]] = mat[(int64_t)i * pd.ldf + j];
+  }
+}
+
+template <typename T>
+cudaError_t launch_floyd_parts(const PartDesc *parts, int nparts, T *F, T *D, int64_t ldD,
+                               const int32_t *st2ed, cudaStream_t stream, int64_t *launches) {
+  if (nparts <= 0) return cudaSuccess;
+  const size_t smem = FloydCfg<T, kFloydTile>::SMEM_ELEMS * sizeof(T);
+  auto kern = floyd_part_kernel<T>;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  kern<<<nparts, FloydCfg<T, kFloydTile>::THREADS, smem, stream>>>(parts, F, D, ldD, st2ed);
+  *launches += 1;
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_floyd_matrix(T *mat, int64_t ld, int nb, cudaStream_t stream,
+                                int64_t *launches) {
+  using FC = FloydCfg<T, kFloydTile>;
+  const size_t smem = FC::SMEM_ELEMS * sizeof(T);
+  for (int kb = 0; kb < nb; kb++) {
+    floyd_phase1_kernel<T, kFloydTile><<<1, FC::THREADS, smem, stream>>>(mat, ld, kb);
+    *launches += 1;
+    if (nb > 1) {
+      floyd_phase2_kernel<T, kFloydTile><<<2 * (nb - 1), FC::THREADS, smem, stream>>>(mat, ld, kb, nb);
+      floyd_phase3_kernel<T, kFloydTile><<<(nb - 1) * (nb - 1), FC::THREADS, smem, stream>>>(mat, ld, kb, nb);
+      *launches += 2;
+    }
+  }
+  return cudaGetLastError();
+}
+
+template <typename T>
+__global__ void bdy_scatter_kernel(const PartDesc *__restrict__ parts, const T *__restrict__ F,
+                                   T *D, int64_t ldD, const int32_t *__restrict__ st2ed) {
+  const PartDesc pd = parts[blockIdx.y];
+  const int i = blockIdx.x;
+  if (i >= pd.b) return;
+  const T *Fi = F + pd.f_off + (int64_t)i * pd.ldf;
+  T *Di = D + (pd.row_base + i) * ldD;
+  for (int j = threadIdx.x; j < pd.s; j += blockDim.x) Di[st2ed[pd.start + j]] = Fi[j];
+}
+
+template <typename T>
+cudaError_t launch_bdy_scatter(const PartDesc *parts, int nparts, const T *F, T *D, int64_t ldD,
+                               const int32_t *st2ed, int max_b, int max_s, cudaStream_t stream,
+                               int64_t *launches) {
+  if (nparts <= 0 || max_b <= 0) return cudaSuccess;
+  (void)max_s;
+  bdy_scatter_kernel<T><<<dim3(max_b, nparts), 256, 0, stream>>>(parts, F, D, ldD, st2ed);
+  *launches += 1;
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Stage 3: min-plus merge with the fused decode of own-part columns.
+// grid (ldD / BN, nwork): CTA (x, y) computes rows work[y].m0 .. +BM of the
+// part's inner block against columns x*BN .. +BN.
+//   R[i][j] = min(INF, min_{k<b} F[b+i][k] + S[k][j])   (S = the part's
+//   boundary rows of D), then for own-part columns j the closed Floyd value
+//   F[b+i][ed2st[j]-start] replaces it, as the reference's decode does.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(MPCfg<T>::THREADS)
+    minplus_part_kernel(const PartDesc *__restrict__ parts, const MPWork *__restrict__ work, int n,
+                        const T *__restrict__ F, T *D, int64_t ldD,
+                        const int32_t *__restrict__ graph_id, const int32_t *__restrict__ ed2st) {
+  using C = MPCfg<T>;
+  extern __shared__ __align__(16) unsigned char mp_smem_raw[];
+  T *smem = reinterpret_cast<T *>(mp_smem_raw);
+  const MPWork wk = work[blockIdx.y];
+  const PartDesc pd = parts[wk.pidx];
+  const int n0 = blockIdx.x * C::BN;
+  const int M = pd.s - pd.b, K = pd.b;
+  const T *A = F + pd.f_off + (int64_t)pd.b * pd.ldf;
+  const T *B = D + pd.row_base * ldD;
+  T *Cm = D + (pd.row_base + pd.b) * ldD;
+  T acc[C::TM][C::TN];
+  acc_fill<T, C>(acc, Dist<T>::inf());
+  minplus_tile<T, C, true, true>(A, pd.ldf, B, ldD, wk.m0, n0, M, (int)ldD, K, acc, smem);
+
+  const int tid = threadIdx.x, ty = tid / C::TX, tx = tid % C::TX;
+  // Own-part columns of this thread (fused decode).
+  int own[C::TN];
+  bool any_own = false;
+#pragma unroll
+  for (int gj = 0; gj < C::GN; gj++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int c = n0 + tile_col<C>(tx, gj, q);
+      int o = -1;
+      if (c < n && __ldg(graph_id + c) == pd.part) o = __ldg(ed2st + c) - pd.start;
+      own[4 * gj + q] = o;
+      any_own |= (o >= 0);
+    }
+  using V = typename Vec4<T>::type;
+#pragma unroll
+  for (int gi = 0; gi < C::GM; gi++)
+#pragma unroll
+    for (int l = 0; l < 4; l++) {
+      const int r = wk.m0 + tile_row<C>(ty, gi, l);
+      if (r >= M) continue;
+      if (any_own) {
+        const T *Fr = F + pd.f_off + (int64_t)(pd.b + r) * pd.ldf;
+#pragma unroll
+        for (int j = 0; j < C::TN; j++)
+          if (own[j] >= 0) acc[4 * gi + l][j] = Fr[own[j]];
+      }
+      T *dst = Cm + (int64_t)r * ldD + n0;
+#pragma unroll
+      for (int gj = 0; gj < C::GN; gj++) {
+        V v;
+        v.x = acc[4 * gi + l][4 * gj + 0];
+        v.y = acc[4 * gi + l][4 * gj + 1];
+        v.z = acc[4 * gi + l][4 * gj + 2];
+        v.w = acc[4 * gi + l][4 * gj + 3];
+        __stcs(reinterpret_cast<V *>(dst + tile_col<C>(tx, gj, 0)), v);
+      }
+    }
+}
+
+template <typename T>
+cudaError_t launch_minplus_parts(const PartDesc *parts, const MPWork *work, int nwork, int n,
+                                 const T *F, T *D, int64_t ldD, const int32_t *graph_id,
+                                 const int32_t *ed2st, cudaStream_t stream, int64_t *launches) {
+  if (nwork <= 0) return cudaSuccess;
+  using C = MPCfg<T>;
+  const size_t smem = C::SMEM_ELEMS * sizeof(T);
+  dim3 grid((unsigned)(ldD / C::BN), (unsigned)nwork);
+  minplus_part_kernel<T><<<grid, C::THREADS, smem, stream>>>(parts, work, n, F, D, ldD, graph_id,
+                                                             ed2st);
+  *launches += 1;
+  return cudaGetLastError();
+}
+
+// Generic C = min(INF, A (x) B), any sizes and alignments.
+template <typename T, bool VEC_B>
+__global__ void __launch_bounds__(MPCfg<T>::THREADS)
+    minplus_generic_kernel(int M, int N, int K, const T *__restrict__ A, int64_t lda,
+                           const T *__restrict__ B, int64_t ldb, T *__restrict__ Cp, int64_t ldc) {
+  using C = MPCfg<T>;
+  extern __shared__ __align__(16) unsigned char mg_smem_raw[];
+  T *smem = reinterpret_cast<T *>(mg_smem_raw);
+  const int m0 = blockIdx.y * C::BM, n0 = blockIdx.x * C::BN;
+  T acc[C::TM][C::TN];
+  acc_fill<T, C>(acc, Dist<T>::inf());
+  minplus_tile<T, C, VEC_B, true>(A, lda, B, ldb, m0, n0, M, N, K, acc, smem);
+  acc_store<T, C, false>(acc, Cp, ldc, m0, n0, M, N);
+}
+
+template <typename T>
+cudaError_t launch_minplus_generic(int M, int N, int K, const T *A, int64_t lda, const T *B,
+                                   int64_t ldb, T *C, int64_t ldc, cudaStream_t stream,
+                                   int64_t *launches) {
+  if (M <= 0 || N <= 0) return cudaSuccess;
+  using Cf = MPCfg<T>;
+  const size_t smem = Cf::SMEM_ELEMS * sizeof(T);
+  dim3 grid((unsigned)ceil_div(N, Cf::BN), (unsigned)ceil_div(M, Cf::BM));
+  // Vector B loads need 16-byte rows and whole 4-vectors inside each row.
+  const bool vec = (ldb % 4 == 0) && (N % 4 == 0) && ((uintptr_t)B % 16 == 0);
+  if (vec)
+    minplus_generic_kernel<T, true><<<grid, Cf::THREADS, smem, stream>>>(M, N, K, A, lda, B, ldb, C, ldc);
+  else
+    minplus_generic_kernel<T, false><<<grid, Cf::THREADS, smem, stream>>>(M, N, K, A, lda, B, ldb, C, ldc);
+  *launches += 1;
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Utilities
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void fill_kernel(T *p, int64_t rows, int64_t cols, int64_t ld, T v) {
+  const int64_t total = rows * cols;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = t / cols, c = t % cols;
+    p[r * ld + c] = v;
+  }
+}
+
+template <typename T>
+cudaError_t launch_fill(T *p, int64_t rows, int64_t cols, int64_t ld, T v, cudaStream_t stream,
+                        int64_t *launches) {
+  if (rows <= 0 || cols <= 0) return cudaSuccess;
+  const int64_t total = rows * cols;
+  const int blocks = (int)std::min<int64_t>(ceil_div(total, 256), 148 * 32);
+  fill_kernel<T><<<blocks, 256, 0, stream>>>(p, rows, cols, ld, v);
+  *launches += 1;
+  return cudaGetLastError();
+}
+
+__global__ void row_checksum_kernel(const int32_t *__restrict__ D, int64_t n, int64_t ld,
+                                    uint64_t *__restrict__ out) {
+  const int64_t r = blockIdx.x;
+  const uint32_t *row = reinterpret_cast<const uint32_t *>(D + r * ld);
+  uint64_t acc = 0;
+  for (int64_t j = threadIdx.x; j < n; j += blockDim.x)
+    acc += (uint64_t)__ldg(row + j) * (uint64_t)(2 * j + 1);
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  __shared__ uint64_t part[32];
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    uint64_t v = (threadIdx.x < (blockDim.x >> 5)) ? part[threadIdx.x] : 0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (threadIdx.x == 0) out[r] = v;
+  }
+}
+
+cudaError_t launch_row_checksums(const int32_t *D, int64_t rows, int64_t n, int64_t ld,
+                                 uint64_t *out, cudaStream_t stream, int64_t *launches) {
+  if (rows <= 0) return cudaSuccess;
+  row_checksum_kernel<<<(unsigned)rows, 256, 0, stream>>>(D, n, ld, out);
+  *launches += 1;
+  return cudaGetLastError();
+}
+
+__global__ void i32_to_f32_kernel(const int32_t *__restrict__ src, int64_t rows, int64_t n,
+                                  int64_t ld, float *__restrict__ dst) {
+  const int64_t total = rows * n;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = t / n, c = t % n;
+    dst[t] = (float)src[r * ld + c];
+  }
+}
+
+cudaError_t launch_i32_to_f32(const int32_t *src, int64_t rows, int64_t n, int64_t ld, float *dst,
+                              cudaStream_t stream, int64_t *launches) {
+  if (rows <= 0 || n <= 0) return cudaSuccess;
+  const int blocks = (int)std::min<int64_t>(ceil_div(rows * n, 256), 148 * 32);
+  i32_to_f32_kernel<<<blocks, 256, 0, stream>>>(src, rows, n, ld, dst);
+  *launches += 1;
+  return cudaGetLastError();
+}
+
+// Relaxation throughput: 64 independent-ish accumulators per thread, every
+// relaxation's add input changes each iteration so nothing can be hoisted.
+template <typename T>
+__global__ void __launch_bounds__(256) relax_peak_kernel(T *sink, int iters, T seed) {
+  T acc[8][8], b[8];
+#pragma unroll
+  for (int j = 0; j < 8; j++) b[j] = seed + T((threadIdx.x + j) & 7);
+#pragma unroll
+  for (int i = 0; i < 8; i++)
+#pragma unroll
+    for (int j = 0; j < 8; j++) acc[i][j] = seed * T(i + 1) + T(j + threadIdx.x % 5);
+  for (int it = 0; it < iters; it++) {
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+#pragma unroll
+      for (int j = 0; j < 8; j++) acc[i][j] = Dist<T>::relax(acc[i][j], b[j], acc[(i + 1) & 7][j]);
+  }
+  T s = T(0);
+#pragma unroll
+  for (int i = 0; i < 8; i++)
+#pragma unroll
+    for (int j = 0; j < 8; j++) s = Dist<T>::min(s, acc[i][j]);
+  if (s == T(-12345)) sink[0] = s;  // never true; keeps the loop live
+  if (threadIdx.x == 0 && blockIdx.x == 0) sink[1] = s;
+}
+
+template <typename T>
+cudaError_t launch_relax_peak(T *sink, int blocks, int iters, cudaStream_t stream,
+                              double *relax_count) {
+  relax_peak_kernel<T><<<blocks, 256, 0, stream>>>(sink, iters, T(3));
+  *relax_count = (double)blocks * 256.0 * (double)iters * 64.0;
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Explicit instantiations
+// ---------------------------------------------------------------------------
+#define FAPB_INSTANTIATE(T)                                                                       \
+  template cudaError_t launch_sssp<T>(const int32_t *, const int32_t *, const T *, int,           \
+                                      const int32_t *, const int64_t *, int, T *, int64_t,        \
+                                      int64_t, T, int64_t, int *, cudaStream_t, int64_t *);       \
+  template cudaError_t launch_gather<T>(const PartDesc *, int, int, const int32_t *,              \
+                                        const int32_t *, const T *, const int32_t *,              \
+                                        const int32_t *, const int32_t *, const T *, int64_t, T *, \
+                                        cudaStream_t, int64_t *);                                 \
+  template cudaError_t launch_floyd_parts<T>(const PartDesc *, int, T *, T *, int64_t,            \
+                                             const int32_t *, cudaStream_t, int64_t *);           \
+  template cudaError_t launch_floyd_matrix<T>(T *, int64_t, int, cudaStream_t, int64_t *);        \
+  template cudaError_t launch_bdy_scatter<T>(const PartDesc *, int, const T *, T *, int64_t,      \
+                                             const int32_t *, int, int, cudaStream_t, int64_t *); \
+  template cudaError_t launch_minplus_parts<T>(const PartDesc *, const MPWork *, int, int,        \
+                                               const T *, T *, int64_t, const int32_t *,          \
+                                               const int32_t *, cudaStream_t, int64_t *);         \
+  template cudaError_t launch_minplus_generic<T>(int, int, int, const T *, int64_t, const T *,    \
+                                                 int64_t, T *, int64_t, cudaStream_t, int64_t *); \
+  template cudaError_t launch_fill<T>(T *, int64_t, int64_t, int64_t, T, cudaStream_t, int64_t *); \
+  template cudaError_t launch_relax_peak<T>(T *, int, int, cudaStream_t, double *);
+
+FAPB_INSTANTIATE(int32_t)
+FAPB_INSTANTIATE(float)
+
+}  // namespace fapb

@@ -1,0 +1,644 @@
+// Host side of the drop-in fap::fapGraph (include/fap/fap.h): graph IO,
+// METIS partitioning, boundary detection and renumbering stay on the host,
+// exactly as the reference does them, and stages 1-3 go to the GPU through
+// the C ABI (include/fap_b200.h).
+//
+// Reference behaviour reproduced here (Liu-xiandong/FastAPSP):
+//   readVerEdges / readMatFile   fap/utils/readMatFile.h:36-173
+//   Graph_decomposition          fap/utils/readIdFile.h:71-132
+//   findBoundry                  fap/utils/util_preprocess.h:32-58
+//   sort_and_encode              fap/utils/util_preprocess.h:73-106
+//   fapGraph                     fap/fap.cpp:27-277
+#include "fap/fap.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <ctime>
+#include <fstream>
+#include <map>
+#include <string>
+#include <unordered_set>
+#include <vector>
+
+#include "fap_b200.h"
+#include "fap_host.h"
+
+// METIS 5 k-way partitioner.  The CUDA toolkit's libmetis_static.a is linked
+// into this library; it uses 64-bit idx_t.
+extern "C" int METIS_PartGraphKway(int64_t *nvtxs, int64_t *ncon, int64_t *xadj, int64_t *adjncy,
+                                   int64_t *vwgt, int64_t *vsize, int64_t *adjwgt, int64_t *nparts,
+                                   float *tpwgts, float *ubvec, int64_t *options, int64_t *edgecut,
+                                   int64_t *part);
+
+namespace fap {
+
+namespace {
+
+constexpr int kMetisOk = 1;
+
+[[noreturn]] void raise(int code, const std::string &msg) { throw fapError(code, msg); }
+
+void check(int rc, const char *what) {
+  if (rc != FAP_OK) raise(rc, std::string(what) + ": " + fap_last_error());
+}
+
+std::string mtx_path(const std::string &name, bool directed, bool weighted) {
+  const char *kind = !directed ? (weighted ? "weight-undirected" : "unweight-undirected")
+                               : (weighted ? "weight-directed" : "unweight-directed");
+  return std::string("graph/") + kind + "/" + name + ".mtx";
+}
+
+// MatrixMarket reader with the reference's CSR layout: every input line a b
+// [w] inserts a->b (and b->a when undirected); a vertex's adjacency lists its
+// insertions newest first (the reference prepends to a linked list per
+// vertex, readMatFile.h:30-34,150-162).  Ids are 1-based in the file.
+// Weights are |w| as float32, or 1 when unweighted.
+struct MtxGraph {
+  int32_t n = 0;
+  int64_t m_decl = 0;  // declared arcs (2x lines when undirected)
+  std::vector<int32_t> adj_size, row_offset, col_val;
+  std::vector<float> weight;
+};
+
+MtxGraph read_mtx(const std::string &path, bool directed, bool weighted) {
+  std::ifstream in(path);
+  if (!in) raise(FAP_ERR_IO, "cannot open graph file " + path);
+  while (in.peek() == '%') in.ignore(2048, '\n');
+  long long n = 0, t = 0, m = 0;
+  if (!(in >> n >> t >> m) || n <= 0 || m < 0 || n > INT32_MAX)
+    raise(FAP_ERR_IO, "malformed MatrixMarket header in " + path);
+  MtxGraph g;
+  g.n = (int32_t)n;
+  g.m_decl = directed ? m : 2 * m;
+  if (g.m_decl > INT32_MAX) raise(FAP_ERR_IO, "too many edges in " + path);
+  std::vector<int32_t> src, dst;
+  std::vector<float> w;
+  src.reserve(g.m_decl);
+  dst.reserve(g.m_decl);
+  w.reserve(g.m_decl);
+  long long a, b;
+  double c;
+  auto push = [&](long long x, long long y, float wt) {
+    if ((int64_t)src.size() >= g.m_decl) raise(FAP_ERR_IO, "more edge lines than declared in " + path);
+    src.push_back((int32_t)x);
+    dst.push_back((int32_t)y);
+    w.push_back(wt);
+  };
+  for (;;) {
+    if (!(in >> a >> b)) break;
+    float wt = 1.0f;
+    if (weighted) {
+      if (!(in >> c)) raise(FAP_ERR_IO, "missing weight in " + path);
+      wt = static_cast<float>(std::fabs(c));
+    }
+    if (a < 1 || a > n || b < 1 || b > n) raise(FAP_ERR_IO, "vertex id out of range in " + path);
+    a--;
+    b--;
+    push(a, b, wt);
+    if (!directed) push(b, a, wt);
+  }
+  const int64_t used = (int64_t)src.size();
+  g.adj_size.assign(n, 0);
+  g.row_offset.assign(n + 1, 0);
+  g.col_val.assign(g.m_decl, 0);
+  g.weight.assign(g.m_decl, 0.0f);
+  for (int64_t i = 0; i < used; i++) g.adj_size[src[i]]++;
+  for (int32_t v = 0; v < n; v++) g.row_offset[v + 1] = g.row_offset[v] + g.adj_size[v];
+  // newest insertion first within each vertex
+  std::vector<int32_t> fill(g.row_offset.begin(), g.row_offset.end() - 1);
+  for (int64_t i = used - 1; i >= 0; i--) {
+    const int32_t u = src[i];
+    g.col_val[fill[u]] = dst[i];
+    g.weight[fill[u]] = w[i];
+    fill[u]++;
+  }
+  return g;
+}
+
+// METIS k-way partition with default options; returns 1-based part ids.
+// Directed graphs are symmetrised first (self-loops dropped), with the
+// reference's containers so that the adjacency order METIS sees is the same
+// (readIdFile.h:78-104).  The reference lists only vertices that have an
+// edge, which misaligns xadj when some vertex has none; here such vertices
+// get an empty adjacency instead.
+std::vector<int> metis_partition(int32_t n, int64_t edges, const std::vector<int32_t> &adj_size,
+                                 const std::vector<int32_t> &row_offset,
+                                 const std::vector<int32_t> &col_val, bool directed, int32_t K) {
+  std::vector<int> id(n, 1);
+  if (K == 1) return id;
+  std::vector<int64_t> xadj(1, 0), adjncy;
+  if (directed) {
+    std::map<int, std::unordered_set<int>> sym;
+    for (int v = 0; v < n; v++) {
+      for (int i = 0; i < adj_size[v]; i++) {
+        const int u = col_val[row_offset[v] + i];
+        if (u == v) continue;
+        sym[v].insert(u);
+        sym[u].insert(v);
+      }
+    }
+    for (int v = 0; v < n; v++) {
+      auto it = sym.find(v);
+      if (it != sym.end())
+        for (int u : it->second) adjncy.push_back(u);
+      xadj.push_back((int64_t)adjncy.size());
+    }
+  } else {
+    xadj.assign(row_offset.begin(), row_offset.end());
+    adjncy.assign(col_val.begin(), col_val.begin() + std::max<int64_t>(edges, row_offset[n]));
+  }
+  if (adjncy.empty()) adjncy.push_back(0);
+  int64_t nv = n, ncon = 1, np = K, objval = 0;
+  std::vector<int64_t> part(n, 0);
+  const int ret = METIS_PartGraphKway(&nv, &ncon, xadj.data(), adjncy.data(), nullptr, nullptr,
+                                      nullptr, &np, nullptr, nullptr, nullptr, &objval, part.data());
+  if (ret != kMetisOk) raise(FAP_ERR_PARTITION, "METIS_PartGraphKway failed");
+  for (int32_t i = 0; i < n; i++) {
+    if (part[i] < 0 || part[i] >= K) raise(FAP_ERR_PARTITION, "METIS returned an invalid part id");
+    id[i] = (int)part[i] + 1;
+  }
+  return id;
+}
+
+struct DenseNode {
+  int v;
+  int GraphId;
+  int isBound;
+};
+
+// Part ascending, boundary vertices first within a part (util_preprocess.h:66-71).
+bool node_order(const DenseNode &a, const DenseNode &b) {
+  if (a.GraphId == b.GraphId) return a.isBound > b.isBound;
+  return a.GraphId < b.GraphId;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// construction
+// ---------------------------------------------------------------------------
+void fapGraph::init_storage() {
+  graph_id.assign(num_vertexs, 0);
+  st2ed.assign(num_vertexs, 0);
+  ed2st.assign(num_vertexs, 0);
+  C_BlockVer_num.assign(K + 1, 0);
+  C_BlockVer_offset.assign(K + 1, 0);
+  C_BlockBdy_num.assign(K + 1, 0);
+  C_BlockBdy_offset.assign(K + 1, 0);
+}
+
+fapGraph::fapGraph(std::string input_graph, bool directed, bool weight, int32_t K) {
+  if (K < 1) raise(FAP_ERR_INVALID, "K must be >= 1");
+  this->input_graph = input_graph;
+  this->directed = directed;
+  this->weighted = weight;
+  MtxGraph g = read_mtx(mtx_path(input_graph, directed, weight), directed, weight);
+  if (K > g.n) raise(FAP_ERR_INVALID, "K exceeds the number of vertices");
+  num_vertexs = g.n;
+  num_edges = (int32_t)g.m_decl;
+  this->K = K;
+  adj_size = std::move(g.adj_size);
+  row_offset = std::move(g.row_offset);
+  col_val = std::move(g.col_val);
+  this->weight = std::move(g.weight);
+  init_storage();
+  graph_id = metis_partition(num_vertexs, num_edges, adj_size, row_offset, col_val, directed, K);
+  for (int i = 0; i < num_vertexs; i++) BlockVer[graph_id[i]].push_back(i);
+}
+
+fapGraph::fapGraph(int32_t n, int64_t m, std::vector<int32_t> ro, std::vector<int32_t> cv,
+                   std::vector<float> w, int32_t K)
+    : fapGraph(n, m, std::move(ro), std::move(cv), std::move(w), K, false) {}
+
+fapGraph::fapGraph(int32_t n, int64_t m, std::vector<int32_t> ro, std::vector<int32_t> cv,
+                   std::vector<float> w, int32_t K, bool directed) {
+  if (n <= 0 || K < 1 || K > n) raise(FAP_ERR_INVALID, "need n > 0 and 1 <= K <= n");
+  if ((int64_t)ro.size() != (int64_t)n + 1 || ro[0] != 0 || ro[n] > m || (int64_t)cv.size() < ro[n] ||
+      (int64_t)w.size() < ro[n])
+    raise(FAP_ERR_INVALID, "inconsistent CSR");
+  num_vertexs = n;
+  num_edges = (int32_t)m;
+  this->K = K;
+  this->directed = directed;
+  weighted = true;
+  row_offset = std::move(ro);
+  col_val = std::move(cv);
+  weight = std::move(w);
+  col_val.resize(std::max<int64_t>(m, row_offset[n]), 0);
+  weight.resize(std::max<int64_t>(m, row_offset[n]), 0.0f);
+  adj_size.assign(n, 0);
+  for (int32_t v = 0; v < n; v++) {
+    if (row_offset[v + 1] < row_offset[v]) raise(FAP_ERR_INVALID, "row_offset not monotone");
+    adj_size[v] = row_offset[v + 1] - row_offset[v];
+  }
+  for (int64_t e = 0; e < row_offset[n]; e++)
+    if (col_val[e] < 0 || col_val[e] >= n) raise(FAP_ERR_INVALID, "col_val out of range");
+  init_storage();
+  graph_id = metis_partition(num_vertexs, num_edges, adj_size, row_offset, col_val, directed, K);
+  for (int i = 0; i < num_vertexs; i++) BlockVer[graph_id[i]].push_back(i);
+}
+
+fapGraph::~fapGraph() {
+  if (dg_) fap_graph_destroy(dg_);
+  if (ctx_) fap_ctx_destroy(ctx_);
+}
+
+void fapGraph::setPartition(const std::vector<int32_t> &gid) {
+  if ((int32_t)gid.size() != num_vertexs) raise(FAP_ERR_PARTITION, "partition size != n");
+  for (int32_t v : gid)
+    if (v < 1 || v > K) raise(FAP_ERR_PARTITION, "partition id outside 1..K");
+  graph_id.assign(gid.begin(), gid.end());
+  BlockVer.clear();
+  for (int i = 0; i < num_vertexs; i++) BlockVer[graph_id[i]].push_back(i);
+  partition_injected_ = true;
+  prepared_ = false;
+}
+
+void fapGraph::setDevice(int device) { device_ = device; }
+void fapGraph::setDtype(int dtype) { dtype_ = dtype; }
+void fapGraph::setMode(SolveMode mode) { mode_ = mode; }
+
+int fapGraph::getDtype() {
+  ensure_device();
+  return fap_graph_dtype(dg_);
+}
+
+// ---------------------------------------------------------------------------
+// preCondition: boundary flags + renumbering (util_preprocess.h:32-106)
+// ---------------------------------------------------------------------------
+void fapGraph::preCondition() {
+  const int n = num_vertexs;
+  isBoundry.clear();
+  BlockBoundary.clear();
+  std::vector<char> bdy(n, 0);
+  for (int v = 0; v < n; v++) {
+    for (int e = row_offset[v]; e < row_offset[v] + adj_size[v]; e++) {
+      const int u = col_val[e];
+      if (graph_id[u] != graph_id[v]) {
+        bdy[v] = 1;
+        bdy[u] = 1;
+      }
+    }
+  }
+  for (int v = 0; v < n; v++) {
+    isBoundry[v] = bdy[v];
+    if (bdy[v]) BlockBoundary[graph_id[v]].push_back(v);
+  }
+  std::vector<DenseNode> nodes(n);
+  for (int v = 0; v < n; v++) nodes[v] = DenseNode{v, graph_id[v], (int)bdy[v]};
+  std::sort(nodes.begin(), nodes.end(), node_order);
+  for (int i = 0; i < n; i++) {
+    st2ed[i] = nodes[i].v;
+    ed2st[nodes[i].v] = i;
+  }
+  int cnt = 0;
+  max_subgraph_vertexs = 0;
+  for (int p = 1; p <= K; p++) {
+    C_BlockVer_offset[p] = cnt;
+    C_BlockVer_num[p] = (int)BlockVer[p].size();
+    C_BlockBdy_offset[p] = cnt;
+    C_BlockBdy_num[p] = (int)BlockBoundary[p].size();
+    cnt += (int)BlockVer[p].size();
+    max_subgraph_vertexs = std::max(max_subgraph_vertexs, C_BlockVer_num[p]);
+  }
+  is_split = (num_vertexs > max_vertexs_num_limit);
+  prepared_ = true;
+  if (dg_) {
+    check(fap_graph_set_parts(dg_, K, graph_id.data(), st2ed.data(), C_BlockVer_num.data(),
+                              C_BlockVer_offset.data(), C_BlockBdy_num.data()),
+          "fap_graph_set_parts");
+  }
+}
+
+bool fapGraph::isSplit() { return is_split; }
+std::vector<int> fapGraph::getGraphId() { return graph_id; }
+
+// ---------------------------------------------------------------------------
+// GPU plumbing
+// ---------------------------------------------------------------------------
+void fapGraph::ensure_device() {
+  if (!ctx_) check(fap_ctx_create(device_, &ctx_), "fap_ctx_create");
+  if (!dg_) {
+    check(fap_graph_create(ctx_, num_vertexs, row_offset[num_vertexs], row_offset.data(),
+                           col_val.data(), weight.data(), dtype_, &dg_),
+          "fap_graph_create");
+    if (prepared_)
+      check(fap_graph_set_parts(dg_, K, graph_id.data(), st2ed.data(), C_BlockVer_num.data(),
+                                C_BlockVer_offset.data(), C_BlockBdy_num.data()),
+            "fap_graph_set_parts");
+  }
+}
+
+void fapGraph::run_parts(const std::vector<int32_t> &ids) {
+  check(fap_solve(dg_, ids.data(), (int32_t)ids.size(), static_cast<int>(mode_)), "fap_solve");
+  check(fap_graph_check(dg_), "fap_graph_check");
+}
+
+void fapGraph::copy_block(int32_t id, float *dst) {
+  check(fap_graph_copy_block(dg_, id, dst, FAP_DTYPE_F32), "fap_graph_copy_block");
+}
+
+int32_t fapGraph::solve(bool path_needed) {
+  if (!prepared_) raise(FAP_ERR_STATE, "solve before preCondition");
+  is_path_needed = path_needed;
+  ensure_device();
+  const int64_t n = num_vertexs;
+  dist.assign((size_t)(n * n), 0.0f);
+  path.assign((size_t)(n * n), -1);
+  std::vector<int32_t> all;
+  for (int32_t p = 1; p <= K; p++) all.push_back(p);
+  run_parts(all);
+  for (int32_t p = 1; p <= K; p++) copy_block(p, dist.data() + (size_t)C_BlockVer_offset[p] * n);
+  return 0;
+}
+
+int32_t fapGraph::solveSubGraph(int32_t id, bool path_needed) {
+  if (!prepared_) raise(FAP_ERR_STATE, "solveSubGraph before preCondition");
+  if (id < 1 || id > K) return -1;
+  is_path_needed = path_needed;
+  ensure_device();
+  const int64_t n = num_vertexs;
+  void *dp;
+  int64_t rows, ld;
+  if (fap_graph_block(dg_, id, &dp, &rows, &ld) != FAP_OK) {
+    if (mode_ == SolveMode::Batched) {
+      // Solve every part once (blocks stay resident); later calls only copy.
+      std::vector<int32_t> all;
+      for (int32_t p = 1; p <= K; p++) all.push_back(p);
+      if (fap_solve(dg_, all.data(), (int32_t)all.size(), FAP_MODE_BATCHED) != FAP_OK) {
+        // Not enough room for every block: solve this part alone.
+        run_parts({id});
+      } else {
+        check(fap_graph_check(dg_), "fap_graph_check");
+      }
+    } else {
+      run_parts({id});
+    }
+  }
+  subgraph_dist.resize((size_t)C_BlockVer_num[id] * n);
+  subgraph_path.assign((size_t)C_BlockVer_num[id] * n, -1);
+  current_subgraph_id = id;
+  copy_block(id, subgraph_dist.data());
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// getters
+// ---------------------------------------------------------------------------
+std::vector<int32_t> fapGraph::getMapping() { return st2ed; }
+
+std::vector<float> fapGraph::getAllDistance() {
+  if (is_split) raise(FAP_ERR_STATE, "getAllDistance on a split graph");
+  return dist;
+}
+
+std::vector<int32_t> fapGraph::getAllPath() {
+  if (is_split) raise(FAP_ERR_STATE, "getAllPath on a split graph");
+  return path;
+}
+
+std::vector<int32_t> fapGraph::getSubGraphIndex(int32_t id) {
+  if (id < 1 || id > K) raise(FAP_ERR_INVALID, "part id out of range");
+  const int off = C_BlockVer_offset[id], size = C_BlockVer_num[id];
+  return std::vector<int32_t>(st2ed.begin() + off, st2ed.begin() + off + size);
+}
+
+int32_t fapGraph::getCurrentSubGraphId() { return current_subgraph_id; }
+
+std::vector<float> fapGraph::getSubGraphDistance(int32_t id) {
+  if (id != current_subgraph_id) raise(FAP_ERR_STATE, "part is not the current one");
+  return subgraph_dist;
+}
+
+std::vector<int32_t> fapGraph::getSubGraphPath(int32_t id) {
+  if (id != current_subgraph_id) raise(FAP_ERR_STATE, "part is not the current one");
+  return subgraph_path;
+}
+
+std::vector<float> fapGraph::getDistanceFromOnePoint(int32_t v) {
+  if (v < 0 || v >= num_vertexs) raise(FAP_ERR_INVALID, "vertex out of range");
+  if (graph_id[v] != current_subgraph_id) raise(FAP_ERR_STATE, "vertex is not in the current part");
+  const int64_t n = num_vertexs;
+  const int64_t row = ed2st[v] - C_BlockVer_offset[current_subgraph_id];
+  return std::vector<float>(subgraph_dist.begin() + row * n, subgraph_dist.begin() + (row + 1) * n);
+}
+
+std::vector<int32_t> fapGraph::getPathFromOnePoint(int32_t v) {
+  if (v < 0 || v >= num_vertexs) raise(FAP_ERR_INVALID, "vertex out of range");
+  if (graph_id[v] != current_subgraph_id) raise(FAP_ERR_STATE, "vertex is not in the current part");
+  const int64_t n = num_vertexs;
+  const int64_t row = ed2st[v] - C_BlockVer_offset[current_subgraph_id];
+  return std::vector<int32_t>(subgraph_path.begin() + row * n, subgraph_path.begin() + (row + 1) * n);
+}
+
+float fapGraph::getDistanceP2P(int32_t from, int32_t to) {
+  if (from < 0 || from >= num_vertexs || to < 0 || to >= num_vertexs)
+    raise(FAP_ERR_INVALID, "vertex out of range");
+  const int64_t n = num_vertexs;
+  if (!dist.empty()) return dist[(size_t)ed2st[from] * n + to];
+  if (graph_id[from] != current_subgraph_id) solveSubGraph(graph_id[from]);
+  const int64_t row = ed2st[from] - C_BlockVer_offset[current_subgraph_id];
+  return subgraph_dist[(size_t)row * n + to];
+}
+
+std::vector<int32_t> fapGraph::getPathP2P(int32_t from, int32_t to) {
+  raise(FAP_ERR_STATE, "paths are not computed by this build (distances only)");
+  (void)from;
+  (void)to;
+}
+
+bool fapGraph::check_result(float *d, int *p, int *source, int source_num, int vertexs, int *,
+                            int *, int *, float *, int *) {
+  (void)p;
+  if (source_num <= 0 || vertexs != num_vertexs) return false;
+  ensure_device();
+  unsigned int seed = (unsigned int)time(nullptr);
+  const int cases = 20, cols = 10;
+  std::vector<int32_t> rows_idx(cases), srcs(cases);
+  for (int c = 0; c < cases; c++) {
+    rows_idx[c] = rand_r(&seed) % source_num;
+    srcs[c] = source[rows_idx[c]];
+  }
+  std::vector<float> ref((size_t)cases * vertexs);
+  check(fap_graph_sssp_rows(dg_, srcs.data(), cases, ref.data()), "fap_graph_sssp_rows");
+  const float big = 1e8f / 10;
+  for (int c = 0; c < cases; c++) {
+    for (int k = 0; k < cols; k++) {
+      const int des = rand_r(&seed) % vertexs;
+      const float now = d[(size_t)rows_idx[c] * vertexs + des];
+      const float want = ref[(size_t)c * vertexs + des];
+      if (now > big && want > big) continue;
+      if (std::fabs(now - want) > 1e-5f) return false;
+    }
+  }
+  return true;
+}
+
+}  // namespace fap
+
+// ---------------------------------------------------------------------------
+// C wrappers of fap::fapGraph (for FFI callers, e.g. the Python mirror)
+// ---------------------------------------------------------------------------
+namespace {
+thread_local std::string h_err;
+int h_fail(const fap::fapError &e) {
+  h_err = e.what();
+  return e.code() < 0 ? e.code() : FAP_ERR_INVALID;
+}
+int h_fail_std(const std::exception &e) {
+  h_err = e.what();
+  return FAP_ERR_INVALID;
+}
+}  // namespace
+
+#define FAPH_BODY(...)                         \
+  try {                                        \
+    __VA_ARGS__;                               \
+    return FAP_OK;                             \
+  } catch (const fap::fapError &e) {           \
+    return h_fail(e);                          \
+  } catch (const std::bad_alloc &) {           \
+    h_err = "host allocation failed";          \
+    return FAP_ERR_NOMEM;                      \
+  } catch (const std::exception &e) {          \
+    return h_fail_std(e);                      \
+  }
+
+extern "C" {
+
+const char *fap_host_last_error(void) { return h_err.c_str(); }
+
+int fap_host_from_mtx(const char *name, int directed, int weighted, int K, fap::fapGraph **out) {
+  if (!name || !out) return FAP_ERR_INVALID;
+  FAPH_BODY(*out = new fap::fapGraph(std::string(name), directed != 0, weighted != 0, K))
+}
+
+int fap_host_from_csr(int32_t n, int64_t m, const int32_t *ro, const int32_t *col, const float *w,
+                      int K, int directed, fap::fapGraph **out) {
+  if (!ro || !out || (m > 0 && (!col || !w))) return FAP_ERR_INVALID;
+  FAPH_BODY({
+    std::vector<int32_t> r(ro, ro + n + 1), c(col, col + m);
+    std::vector<float> ww(w, w + m);
+    *out = new fap::fapGraph(n, m, std::move(r), std::move(c), std::move(ww), K, directed != 0);
+  })
+}
+
+int fap_host_destroy(fap::fapGraph *g) {
+  delete g;
+  return FAP_OK;
+}
+
+int fap_host_set_partition(fap::fapGraph *g, const int32_t *gid) {
+  FAPH_BODY(g->setPartition(std::vector<int32_t>(gid, gid + g->num_vertexs)))
+}
+
+int fap_host_set_options(fap::fapGraph *g, int device, int dtype, int mode) {
+  FAPH_BODY({
+    g->setDevice(device);
+    g->setDtype(dtype);
+    g->setMode(mode == 0 ? fap::SolveMode::Plain : fap::SolveMode::Batched);
+  })
+}
+
+int fap_host_precondition(fap::fapGraph *g) { FAPH_BODY(g->preCondition()) }
+
+int fap_host_is_split(fap::fapGraph *g) { return g->isSplit() ? 1 : 0; }
+
+int fap_host_dtype(fap::fapGraph *g) {
+  try {
+    return g->getDtype();
+  } catch (const fap::fapError &e) {
+    return h_fail(e);
+  }
+}
+
+// sizes: [n, m_decl, K, stored arcs]
+int fap_host_sizes(fap::fapGraph *g, int64_t *out4) {
+  out4[0] = g->num_vertexs;
+  out4[1] = g->num_edges;
+  out4[2] = g->getK();
+  out4[3] = g->row_offset.empty() ? 0 : g->row_offset.back();
+  return FAP_OK;
+}
+
+int fap_host_csr(fap::fapGraph *g, int32_t *ro, int32_t *col, float *w) {
+  const int64_t used = g->row_offset.back();
+  std::memcpy(ro, g->row_offset.data(), (g->num_vertexs + 1) * sizeof(int32_t));
+  std::memcpy(col, g->col_val.data(), used * sizeof(int32_t));
+  std::memcpy(w, g->weight.data(), used * sizeof(float));
+  return FAP_OK;
+}
+
+int fap_host_graph_id(fap::fapGraph *g, int32_t *out) {
+  auto v = g->getGraphId();
+  std::memcpy(out, v.data(), v.size() * sizeof(int32_t));
+  return FAP_OK;
+}
+
+int fap_host_mapping(fap::fapGraph *g, int32_t *out) {
+  auto v = g->getMapping();
+  std::memcpy(out, v.data(), v.size() * sizeof(int32_t));
+  return FAP_OK;
+}
+
+// ver_num, ver_offset, bdy_num: K+1 entries each
+int fap_host_parts(fap::fapGraph *g, int32_t *vnum, int32_t *voff, int32_t *bnum) {
+  const int K = g->getK();
+  std::memcpy(vnum, g->getBlockVerNum().data(), (K + 1) * sizeof(int32_t));
+  std::memcpy(voff, g->getBlockVerOffset().data(), (K + 1) * sizeof(int32_t));
+  std::memcpy(bnum, g->getBlockBdyNum().data(), (K + 1) * sizeof(int32_t));
+  return FAP_OK;
+}
+
+int fap_host_solve(fap::fapGraph *g, int path_needed) { FAPH_BODY(g->solve(path_needed != 0)) }
+
+int fap_host_solve_subgraph(fap::fapGraph *g, int id, int path_needed) {
+  FAPH_BODY({
+    if (g->solveSubGraph(id, path_needed != 0) != 0) throw fap::fapError(FAP_ERR_INVALID, "bad part id");
+  })
+}
+
+int fap_host_current_subgraph(fap::fapGraph *g) { return g->getCurrentSubGraphId(); }
+
+int fap_host_subgraph_distance(fap::fapGraph *g, int id, float *out) {
+  FAPH_BODY({
+    auto v = g->getSubGraphDistance(id);
+    std::memcpy(out, v.data(), v.size() * sizeof(float));
+  })
+}
+
+int fap_host_all_distance(fap::fapGraph *g, float *out) {
+  FAPH_BODY({
+    auto v = g->getAllDistance();
+    std::memcpy(out, v.data(), v.size() * sizeof(float));
+  })
+}
+
+int fap_host_distance_from_one_point(fap::fapGraph *g, int v, float *out) {
+  FAPH_BODY({
+    auto r = g->getDistanceFromOnePoint(v);
+    std::memcpy(out, r.data(), r.size() * sizeof(float));
+  })
+}
+
+int fap_host_distance_p2p(fap::fapGraph *g, int from, int to, float *out) {
+  FAPH_BODY(*out = g->getDistanceP2P(from, to))
+}
+
+int fap_host_check_result(fap::fapGraph *g, int id, int *ok) {
+  FAPH_BODY({
+    auto d = g->getSubGraphDistance(id);
+    auto src = g->getSubGraphIndex(id);
+    *ok = g->check_result(d.data(), nullptr, src.data(), (int)src.size(), g->num_vertexs, nullptr,
+                          nullptr, nullptr, nullptr, nullptr)
+              ? 1
+              : 0;
+  })
+}
+
+fap_dgraph *fap_host_device_graph(fap::fapGraph *g) { return g->deviceGraph(); }
+
+}  // extern "C"

@@ -1,0 +1,97 @@
+// Internal host-side interface between the C ABI (fap_capi.cu) and the
+// kernel launchers (fap_device.cu).  Not installed.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace fapb {
+
+// One part of a solve batch.  All offsets are in elements.
+struct PartDesc {
+  int32_t part;      // 1-based part id
+  int32_t start;     // first sorted position of the part
+  int32_t s;         // vertices in the part
+  int32_t b;         // boundary vertices (sorted first)
+  int64_t row_base;  // first output row of the part's block
+  int64_t f_off;     // offset of the part's padded Floyd matrix in the F arena
+  int32_t ldf;       // padded Floyd leading dimension (multiple of kFloydTile)
+  int32_t pad_;
+};
+
+// One min-plus work row: BM output rows of one part (index into the batch).
+struct MPWork {
+  int32_t pidx;
+  int32_t m0;
+};
+
+constexpr int kFloydTile = 128;
+constexpr int kMinplusBM = 128;
+constexpr int kMinplusBN = 128;
+constexpr int kLdAlign = 128;  // output leading dimension multiple (= kMinplusBN)
+
+// Launchers.  T is int32_t or float.  All asynchronous on `stream`; each
+// returns the cudaError_t of its launch(es) and adds the number of kernel
+// launches it issued to *launches.
+template <typename T>
+cudaError_t launch_sssp(const int32_t *row_offset, const int32_t *col, const T *w, int n,
+                        const int32_t *sources, const int64_t *out_rows, int num_sources, T *out,
+                        int64_t ld, int64_t init_cols, T delta, int64_t max_rounds, int *status,
+                        cudaStream_t stream, int64_t *launches);
+
+template <typename T>
+cudaError_t launch_gather(const PartDesc *parts, int nparts, int max_ldf, const int32_t *row_offset,
+                          const int32_t *col, const T *w, const int32_t *graph_id,
+                          const int32_t *st2ed, const int32_t *ed2st, const T *D, int64_t ldD,
+                          T *F, cudaStream_t stream, int64_t *launches);
+
+// Batched: one CTA per part closes its matrix and writes its boundary rows'
+// own-part columns back into D.
+template <typename T>
+cudaError_t launch_floyd_parts(const PartDesc *parts, int nparts, T *F, T *D, int64_t ldD,
+                               const int32_t *st2ed, cudaStream_t stream, int64_t *launches);
+
+// Plain: one padded matrix (ld multiple of kFloydTile, nb = ld / kFloydTile
+// tiles per side), one launch per phase per pivot block.
+template <typename T>
+cudaError_t launch_floyd_matrix(T *mat, int64_t ld, int nb, cudaStream_t stream,
+                                int64_t *launches);
+
+// Boundary rows of the listed parts: F[i][j] -> D[row_base+i][st2ed[start+j]].
+template <typename T>
+cudaError_t launch_bdy_scatter(const PartDesc *parts, int nparts, const T *F, T *D, int64_t ldD,
+                               const int32_t *st2ed, int max_b, int max_s, cudaStream_t stream,
+                               int64_t *launches);
+
+// Min-plus merge of the inner rows of the batch's parts, with the own-part
+// columns taken from the closed Floyd matrices (fused decode).
+template <typename T>
+cudaError_t launch_minplus_parts(const PartDesc *parts, const MPWork *work, int nwork, int n,
+                                 const T *F, T *D, int64_t ldD, const int32_t *graph_id,
+                                 const int32_t *ed2st, cudaStream_t stream, int64_t *launches);
+
+// Generic C = min(INF, A (x) B).
+template <typename T>
+cudaError_t launch_minplus_generic(int M, int N, int K, const T *A, int64_t lda, const T *B,
+                                   int64_t ldb, T *C, int64_t ldc, cudaStream_t stream,
+                                   int64_t *launches);
+
+// Fill rows x cols of a row-major matrix with v.
+template <typename T>
+cudaError_t launch_fill(T *p, int64_t rows, int64_t cols, int64_t ld, T v, cudaStream_t stream,
+                        int64_t *launches);
+
+// Per-row checksums (int32 data).
+cudaError_t launch_row_checksums(const int32_t *D, int64_t rows, int64_t n, int64_t ld,
+                                 uint64_t *out, cudaStream_t stream, int64_t *launches);
+
+// int32 -> float copy of a rows x n block into a dense buffer.
+cudaError_t launch_i32_to_f32(const int32_t *src, int64_t rows, int64_t n, int64_t ld, float *dst,
+                              cudaStream_t stream, int64_t *launches);
+
+// Relaxation-throughput microbenchmark; returns relaxations performed.
+template <typename T>
+cudaError_t launch_relax_peak(T *sink, int blocks, int iters, cudaStream_t stream,
+                              double *relax_count);
+
+}  // namespace fapb

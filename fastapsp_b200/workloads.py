@@ -1,0 +1,54 @@
+"""Benchmark workloads: seeded synthetic graphs of the named shapes, written
+as MatrixMarket and loaded through the drop-in fapGraph (host IO, METIS,
+boundary detection and renumbering)."""
+from __future__ import annotations
+
+import os
+import tempfile
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import generators as G
+from .graph import fapGraph
+
+
+@dataclass
+class Workload:
+    name: str
+    K: int
+    edges: G.EdgeList
+    root: str           # directory holding graph/<kind>/<name>.mtx
+    graph: fapGraph     # after preCondition
+    n: int
+    ver_num: np.ndarray
+    ver_offset: np.ndarray
+    bdy_num: np.ndarray
+
+    @property
+    def entries(self) -> int:
+        return self.n * self.n
+
+    def csr(self):
+        return self.graph.csr()
+
+    def describe(self) -> dict:
+        vn, bn = self.ver_num[1:], self.bdy_num[1:]
+        return {"workload": self.name, "n": self.n, "arcs": int(self.graph.csr()[0][-1]),
+                "K": self.K, "directed": self.edges.directed,
+                "avg_degree": round(float(self.graph.csr()[0][-1]) / self.n, 3),
+                "part_size": [int(vn.min()), int(np.median(vn)), int(vn.max())],
+                "boundary": [int(bn.min()), int(np.median(bn)), int(bn.max()), int(bn.sum())]}
+
+
+def load(name: str, root: str | None = None) -> Workload:
+    spec = G.WORKLOADS[name]
+    el = spec["make"]()
+    root = root or tempfile.mkdtemp(prefix="fap_wl_")
+    path = G.mtx_path(root, name, el.directed, el.weighted)
+    if not os.path.exists(path):
+        G.write_mtx(el, root, name)
+    g = fapGraph(name, el.directed, el.weighted, spec["K"], root=root)
+    g.preCondition()
+    vn, vo, bn = g.partInfo()
+    return Workload(name, spec["K"], el, root, g, g.num_vertexs, vn, vo, bn)

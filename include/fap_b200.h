@@ -1,0 +1,176 @@
+/*
+ * fap_b200.h -- C ABI of the B200 (sm_100a) per-subgraph APSP solve path.
+ *
+ * Every function returns an int status (FAP_OK = 0, negative on error; the
+ * message is in fap_last_error(), per host thread).  Nothing calls exit().
+ * Handles are not thread-safe: use one fap_ctx per host thread.
+ *
+ * The path replaces the reference's kernel ABI
+ *   fap/kernel/cuda/cuda_kernel.h:21-24  handle_boundry_Nvidia_GPU  (stage 1, SSSP)
+ *   fap/kernel/cuda/cuda_kernel.h:29     floyd_GPU_Nvidia_path      (stage 2, Floyd)
+ *   fap/kernel/cuda/cuda_kernel.h:41-42  minplus_NVIDIA_path        (stage 3, min-plus)
+ * and the per-part driver fapGraph::run (fap/fap.cpp:92-181) that calls them
+ * with the host gather/scatter of fap/utils/util_Myalgorithm.h:30-95.
+ * Those three legacy symbols, with their exact C++ signatures, are exported
+ * as well (include/fap_legacy_kernel.h).
+ *
+ * Layout conventions
+ *   - Vertex ids are 0-based int32.  Part ids in this ABI are 1-based, like
+ *     the reference's graph_id (fap/utils/readIdFile.h:127-131).
+ *   - The distance output of a graph is one row-major matrix with n rows and
+ *     a leading dimension ld >= n (padded to a multiple of 128 elements).
+ *     Row r is the vertex at sorted position r (st2ed[r]); column j is
+ *     vertex j.  Part p owns rows ver_offset[p] .. ver_offset[p]+ver_num[p]-1,
+ *     its boundary vertices first: exactly the reference's solve() layout
+ *     (fap/fap.cpp:184-194).
+ *   - Unreachable pairs hold the sentinel 1e8 (100000000 as int32).
+ */
+#ifndef FAP_B200_H_
+#define FAP_B200_H_
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define FAP_API __attribute__((visibility("default")))
+#else
+#define FAP_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define FAP_OK 0
+#define FAP_ERR_INVALID (-1)     /* bad argument */
+#define FAP_ERR_CUDA (-2)        /* CUDA runtime error */
+#define FAP_ERR_NOMEM (-3)       /* device or host allocation failed / too large */
+#define FAP_ERR_STATE (-4)       /* call out of order (e.g. solve before parts) */
+#define FAP_ERR_NOT_CONVERGED (-5) /* SSSP hit its round bound */
+#define FAP_ERR_RANGE (-6)       /* int32 path requested but weights not integral/in range */
+#define FAP_ERR_IO (-7)          /* graph file missing or malformed */
+#define FAP_ERR_PARTITION (-8)   /* METIS failed or partition invalid */
+#define FAP_ERR_DEVICE (-9)      /* a kernel reported a device-side error */
+
+/* ---- distance types ---- */
+#define FAP_DTYPE_AUTO (-1) /* int32 when every weight is an integer <= FAP_MAX_INT_WEIGHT */
+#define FAP_DTYPE_I32 0
+#define FAP_DTYPE_F32 1
+#define FAP_MAX_INT_WEIGHT 1000000
+
+/* ---- solve forms ---- */
+#define FAP_MODE_PLAIN 0   /* one launch sequence per part */
+#define FAP_MODE_BATCHED 1 /* every stage of every requested part in one launch */
+
+#define FAP_INF_I32 100000000
+#define FAP_INF_F32 1e8f
+
+typedef struct fap_ctx fap_ctx;
+typedef struct fap_dgraph fap_dgraph;
+
+/* Last error message of the calling host thread ("" if none). */
+FAP_API const char *fap_last_error(void);
+/* ABI version: 0xMMmmpp. */
+FAP_API int fap_version(void);
+
+/* ---- context: one CUDA device + one stream ---- */
+FAP_API int fap_ctx_create(int device, fap_ctx **out);
+FAP_API int fap_ctx_destroy(fap_ctx *ctx);
+/* Use an external cudaStream_t (passed as void*); NULL = the context's own stream. */
+FAP_API int fap_ctx_set_stream(fap_ctx *ctx, void *stream);
+FAP_API int fap_ctx_get_stream(fap_ctx *ctx, void **stream);
+FAP_API int fap_ctx_sync(fap_ctx *ctx);
+
+/* ---- device-resident graph ----
+ * Uploads the CSR (row_offset[n+1], col_val[m], weight[m] as the reference's
+ * float weights, fap/fap.h:69-74).  dtype: FAP_DTYPE_AUTO / I32 / F32.
+ * Host pointers; copied before return. */
+FAP_API int fap_graph_create(fap_ctx *ctx, int32_t n, int64_t m, const int32_t *row_offset,
+                     const int32_t *col_val, const float *weight, int dtype,
+                     fap_dgraph **out);
+FAP_API int fap_graph_destroy(fap_dgraph *g);
+FAP_API int fap_graph_dtype(const fap_dgraph *g);
+
+/* Sets the partition and renumbering produced on the host by findBoundry +
+ * sort_and_encode (fap/utils/util_preprocess.h:32-106):
+ *   graph_id[n]  1-based part of every vertex,
+ *   st2ed[n]     vertex at each sorted position,
+ *   ver_num[K+1], ver_offset[K+1], bdy_num[K+1]  per part, index 1..K.
+ * Checks that they are consistent.  Host pointers. */
+FAP_API int fap_graph_set_parts(fap_dgraph *g, int32_t K, const int32_t *graph_id,
+                        const int32_t *st2ed, const int32_t *ver_num,
+                        const int32_t *ver_offset, const int32_t *bdy_num);
+
+/* Reserves the output matrix for at most max_rows rows (0 = all n rows).
+ * When max_rows < n, each fap_solve call may only request parts whose rows
+ * fit; their blocks are packed from row 0 in request order. */
+FAP_API int fap_graph_reserve(fap_dgraph *g, int64_t max_rows);
+
+/* Solves the listed parts (1-based ids; parts == NULL means 1..K) into the
+ * device-resident output.  mode: FAP_MODE_PLAIN or FAP_MODE_BATCHED.
+ * Asynchronous on the context stream; errors from the device are reported by
+ * fap_graph_check (or any call that synchronises). */
+FAP_API int fap_solve(fap_dgraph *g, const int32_t *parts, int32_t count, int mode);
+
+/* Synchronises and returns FAP_OK or the device-side error of the last solve. */
+FAP_API int fap_graph_check(fap_dgraph *g);
+
+/* Where part p's block lives: device pointer to its first row, rows, leading
+ * dimension (elements).  Valid until the next fap_solve that reuses rows. */
+FAP_API int fap_graph_block(fap_dgraph *g, int32_t part, void **dev_ptr, int64_t *rows, int64_t *ld);
+
+/* Copies part p's block to host memory as a dense rows x n matrix of
+ * out_dtype (FAP_DTYPE_F32 gives the reference's float values; I32 requires
+ * the int32 path).  Synchronous. */
+FAP_API int fap_graph_copy_block(fap_dgraph *g, int32_t part, void *host, int out_dtype);
+
+/* Per-row checksums of part p's block (int32 path only):
+ * sum_j uint32(d[r][j]) * (2j+1) mod 2^64, j < n.  host_out[rows]. */
+FAP_API int fap_graph_block_checksums(fap_dgraph *g, int32_t part, uint64_t *host_out);
+
+/* Shortest-distance rows from arbitrary sources over the graph's CSR
+ * (distance-row requests, self-checks).  Host sources[count]; host
+ * out[count * n] receives float distances (the reference's type). */
+FAP_API int fap_graph_sssp_rows(fap_dgraph *g, const int32_t *sources, int32_t count, float *host_out);
+
+/* Tuning knobs: "sssp_delta" (bucket width of the near/far SSSP; <= 0 or
+ * >= 1e8 means plain frontier Bellman-Ford); "sssp_max_rounds" (round bound
+ * after which a source gives up and the solve reports
+ * FAP_ERR_NOT_CONVERGED; <= 0 restores the default 8n + 1024). */
+FAP_API int fap_graph_set_param(fap_dgraph *g, const char *key, double value);
+
+/* Device time (ms) of the stages of the last fap_solve, measured with events
+ * on the context stream: [sssp, gather, floyd, minplus, total]. */
+FAP_API int fap_graph_last_timing(fap_dgraph *g, float *ms5);
+
+/* Number of kernels the last fap_solve launched. */
+FAP_API int fap_graph_last_launches(fap_dgraph *g, int64_t *count);
+
+/* ---- device-pointer operators (the three stages on their own) ----
+ * All pointers are device pointers; run on the context stream. */
+
+/* Stage 1: one shortest-path row per source over the CSR.  out row i
+ * (out + i*ld_out) receives the distances from sources[i] to every vertex.
+ * weight is int32* for FAP_DTYPE_I32, float* for FAP_DTYPE_F32. */
+FAP_API int fap_op_sssp(fap_ctx *ctx, int dtype, int32_t n, int64_t m, const int32_t *row_offset,
+                const int32_t *col_val, const void *weight, const int32_t *sources,
+                int32_t num_sources, void *out, int64_t ld_out);
+
+/* Stage 2: in-place Floyd-Warshall closure of an s x s matrix (leading
+ * dimension ld).  The whole GPU works on the one matrix. */
+FAP_API int fap_op_floyd(fap_ctx *ctx, int dtype, int32_t s, void *mat, int64_t ld);
+
+/* Stage 3: C[i][j] = min(1e8, min_k A[i][k] + B[k][j]) for an M x N result,
+ * inner dimension K (row-major, leading dimensions lda, ldb, ldc). */
+FAP_API int fap_op_minplus(fap_ctx *ctx, int dtype, int32_t M, int32_t N, int32_t K,
+                   const void *A, int64_t lda, const void *B, int64_t ldb, void *C,
+                   int64_t ldc);
+
+/* Measured relaxation throughput of this device (relaxations/s) for the
+ * given dtype, from a register-resident microbenchmark. */
+FAP_API int fap_measure_relax_peak(fap_ctx *ctx, int dtype, double *relax_per_s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FAP_B200_H_ */

@@ -1,0 +1,54 @@
+/*
+ * fap_legacy_kernel.h -- the reference's CUDA kernel ABI, re-implemented on
+ * the B200 path so that the reference's own host code (fap/fap.cpp built with
+ * -DWITH_CUDA) links against this library unchanged.
+ *
+ * Signatures and C++ linkage are exactly those of
+ * fap/kernel/cuda/cuda_kernel.h:21-24, :29 and :41-42 (Liu-xiandong/FastAPSP).
+ * All pointers are host pointers; calls are synchronous, like the reference.
+ *
+ * Behaviour:
+ *   - distances are computed on the GPU in int32 when every input value is an
+ *     integer (bit-exact with the reference's float results while finite
+ *     distances stay below 2^24), else in float32;
+ *   - the predecessor outputs (path, res_path) are not computed by this build
+ *     and are left unchanged; the reference's CUDA SSSP also leaves them
+ *     unset (fap/kernel/cuda/batch_sssp.cu:222-281);
+ *   - on an error the outputs are left unchanged, a message goes to stderr
+ *     and fap_legacy_last_status() returns the FAP_ERR_* code (the reference
+ *     calls exit(EXIT_FAILURE) instead).
+ */
+#ifndef FAP_LEGACY_KERNEL_H_
+#define FAP_LEGACY_KERNEL_H_
+
+#if defined(__GNUC__)
+#define FAP_LEGACY_API __attribute__((visibility("default")))
+#else
+#define FAP_LEGACY_API
+#endif
+
+/* Stage 1: shortest-distance rows from st2ed[offset .. offset+bdy_num-1]
+ * into subGraph[bdy_num x vertexs].  Replaces cuda_kernel.h:21-24. */
+FAP_LEGACY_API void handle_boundry_Nvidia_GPU(float *subGraph, int vertexs, int edges, int bdy_num,
+                               int *adj_size, int *row_offset, int *col_val, float *weight,
+                               int *st2ed, int offset);
+
+/* Stage 2: in-place Floyd-Warshall of arc[num_node x num_node].
+ * Replaces cuda_kernel.h:29. */
+FAP_LEGACY_API void floyd_GPU_Nvidia_path(int num_node, float *arc, int *path);
+
+/* Stage 3: res[m x n] = min(1e8, min_k mat1[m x k] + mat2[k x n]).
+ * Replaces cuda_kernel.h:41-42. */
+FAP_LEGACY_API void minplus_NVIDIA_path(float *mat1, float *mat2, int *mat2_path, float *res, int *res_path,
+                         int m, int n, int k);
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+/* Status of the calling thread's last legacy call (FAP_OK or FAP_ERR_*). */
+FAP_LEGACY_API int fap_legacy_last_status(void);
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FAP_LEGACY_KERNEL_H_ */

@@ -1,0 +1,252 @@
+"""Oracle for the per-subgraph solve path -- TEST INFRASTRUCTURE ONLY.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
+module, and only as the checker or as the timed CPU baseline.  The product
+(fastapsp_b200) never imports it.
+
+Two oracles live here:
+
+* the restatement ("port"): oracle/fap_oracle.c, a C restatement of the
+  reference's CPU path, built as oracle/liboracle_port.so and called through
+  ctypes below; plus numpy restatements of the host preprocessing
+  (restate_boundary, restate_encode_classes);
+* the reference itself ("ref"): oracle/_ref/fap_ref, the reference's own
+  fap/fap.cpp compiled from its sources by oracle/Makefile, driven per part
+  through fapGraph::run (fap/fap.cpp:92-181).
+
+The port is pinned against the reference by tests/test_oracle.py and by the
+committed fixtures under tests/golden/ (made by tests/golden/make_golden.py
+from oracle/_ref).
+"""
+from __future__ import annotations
+
+import ctypes
+import json
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_SO = os.path.join(HERE, "liboracle_port.so")
+REF_BIN = os.path.join(HERE, "_ref", "fap_ref")
+MAXVALUE = np.float32(1e8)  # fap/utils/parameter.h:26
+
+
+# --------------------------------------------------------------------------
+# Reading the reference's CSR / partition / renumbering
+# --------------------------------------------------------------------------
+
+@dataclass
+class Meta:
+    """The reference's fapGraph state after preCondition (fap/fap.h:24-76):
+    CSR, 1-based graph_id, st2ed/ed2st and per-part counts (index 1..K)."""
+    n: int
+    m: int
+    K: int
+    row_offset: np.ndarray
+    col_val: np.ndarray
+    weight: np.ndarray
+    graph_id: np.ndarray
+    st2ed: np.ndarray
+    ed2st: np.ndarray
+    ver_num: np.ndarray
+    ver_offset: np.ndarray
+    bdy_num: np.ndarray
+
+
+def read_meta(path: str) -> Meta:
+    """Parse the binary written by fap_ref --meta (see dump_meta there)."""
+    raw = np.fromfile(path, dtype=np.int32)
+    n, m, K = (int(x) for x in raw[:3])
+    o = 3
+
+    def take(cnt, dt=np.int32):
+        nonlocal o
+        a = raw[o:o + cnt].copy()
+        o += cnt
+        return a.view(dt) if dt is not np.int32 else a
+
+    ro = take(n + 1)
+    col = take(m)
+    w = take(m, np.float32)
+    gid = take(n)
+    st2ed = take(n)
+    ed2st = take(n)
+    vn = take(K + 1)
+    vo = take(K + 1)
+    bn = take(K + 1)
+    assert o == raw.size, "meta file size mismatch"
+    return Meta(n, m, K, ro, col, w, gid, st2ed, ed2st, vn, vo, bn)
+
+
+# --------------------------------------------------------------------------
+# The C restatement
+# --------------------------------------------------------------------------
+
+_port = None
+
+
+def port_lib():
+    global _port
+    if _port is None:
+        if not os.path.exists(PORT_SO):
+            subprocess.run(["make", "-C", HERE, "port"], check=True,
+                           stdout=subprocess.DEVNULL)
+        lib = ctypes.CDLL(PORT_SO)
+        P = ctypes.c_void_p
+        I = ctypes.c_int
+        lib.fo_run_part.argtypes = [I, P, P, P, P, P, P, I, I, I, P]
+        lib.fo_run_part.restype = I
+        lib.fo_dijkstra_path.argtypes = [I, I, P, P, P, P, P]
+        lib.fo_dijkstra_path.restype = None
+        lib.fo_floyd.argtypes = [I, P]
+        lib.fo_floyd.restype = None
+        _port = lib
+    return _port
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def port_run_part(row_offset, col, weight, graph_id, st2ed, ed2st,
+                  start: int, s: int, bdy: int) -> np.ndarray:
+    """Solve one part with the C restatement of fapGraph::run; returns the
+    s x n float32 block (row r = vertex st2ed[start + r], column = vertex id)."""
+    n = int(row_offset.shape[0]) - 1
+    ro = np.ascontiguousarray(row_offset, np.int32)
+    cv = np.ascontiguousarray(col, np.int32)
+    w = np.ascontiguousarray(weight, np.float32)
+    gid = np.ascontiguousarray(graph_id, np.int32)
+    s2e = np.ascontiguousarray(st2ed, np.int32)
+    e2s = np.ascontiguousarray(ed2st, np.int32)
+    out = np.empty((s, n), np.float32)
+    rc = port_lib().fo_run_part(n, _p(ro), _p(cv), _p(w), _p(gid), _p(s2e), _p(e2s),
+                                int(start), int(s), int(bdy), _p(out))
+    if rc != 0:
+        raise MemoryError("oracle part solve failed")
+    return out
+
+
+def port_dijkstra(row_offset, col, weight, src: int) -> np.ndarray:
+    n = int(row_offset.shape[0]) - 1
+    ro = np.ascontiguousarray(row_offset, np.int32)
+    cv = np.ascontiguousarray(col, np.int32)
+    w = np.ascontiguousarray(weight, np.float32)
+    d = np.empty(n, np.float32)
+    port_lib().fo_dijkstra_path(int(src), n, _p(ro), _p(cv), _p(w), _p(d), None)
+    return d
+
+
+def port_floyd(mat: np.ndarray) -> np.ndarray:
+    m = np.ascontiguousarray(mat, np.float32).copy()
+    port_lib().fo_floyd(int(m.shape[0]), _p(m))
+    return m
+
+
+def port_solve_meta(meta: Meta, parts=None) -> dict:
+    """Solve the given 1-based parts of a Meta with the restatement."""
+    out = {}
+    parts = range(1, meta.K + 1) if parts is None else parts
+    for p in parts:
+        out[p] = port_run_part(meta.row_offset, meta.col_val, meta.weight, meta.graph_id,
+                               meta.st2ed, meta.ed2st, int(meta.ver_offset[p]),
+                               int(meta.ver_num[p]), int(meta.bdy_num[p]))
+    return out
+
+
+# --------------------------------------------------------------------------
+# numpy restatements of the host preprocessing
+# --------------------------------------------------------------------------
+
+def restate_boundary(row_offset, col, graph_id) -> np.ndarray:
+    """Boundary flags.  Follows fap/utils/util_preprocess.h:32-58
+    (findBoundry): both endpoints of every out-edge whose endpoints lie in
+    different parts are boundary."""
+    n = row_offset.shape[0] - 1
+    src = np.repeat(np.arange(n), np.diff(row_offset))
+    cross = graph_id[src] != graph_id[col]
+    flag = np.zeros(n, bool)
+    flag[src[cross]] = True
+    flag[col[cross]] = True
+    return flag
+
+
+def restate_encode_classes(graph_id, is_bdy, K):
+    """What sort_and_encode (fap/utils/util_preprocess.h:73-106) guarantees,
+    independent of how std::sort orders ties: per part p = 1..K the
+    offset/count of its contiguous block, boundary vertices first, and the
+    vertex set of every (part, boundary) class."""
+    ver_num = np.zeros(K + 1, np.int64)
+    bdy_num = np.zeros(K + 1, np.int64)
+    np.add.at(ver_num, graph_id, 1)
+    np.add.at(bdy_num, graph_id[is_bdy], 1)
+    ver_off = np.zeros(K + 1, np.int64)
+    ver_off[1:] = np.concatenate([[0], np.cumsum(ver_num[1:])[:-1]])
+    return ver_num, ver_off, bdy_num
+
+
+def check_encoding(st2ed, graph_id, is_bdy, K) -> None:
+    """Assert st2ed is a permutation placing each part contiguously in part
+    order, boundary vertices first (the sort_and_encode contract)."""
+    n = graph_id.shape[0]
+    assert sorted(st2ed.tolist()) == list(range(n))
+    vn, vo, bn = restate_encode_classes(graph_id, is_bdy, K)
+    for p in range(1, K + 1):
+        seg = st2ed[vo[p]:vo[p] + vn[p]]
+        assert np.all(graph_id[seg] == p)
+        assert np.all(is_bdy[seg[:bn[p]]])
+        assert not np.any(is_bdy[seg[bn[p]:]])
+
+
+# --------------------------------------------------------------------------
+# The reference binary
+# --------------------------------------------------------------------------
+
+def ref_available() -> bool:
+    return os.path.exists(REF_BIN)
+
+
+def run_ref(workdir: str, name: str, directed: bool, weighted: bool, K: int, *,
+            parts="all", meta_out: str | None = None, dist_out: str | None = None,
+            threads: int | None = None, partition_file: str | None = None,
+            timeout: float | None = None) -> list:
+    """Run the reference's CPU path (oracle/_ref/fap_ref) and return its JSON
+    event lines."""
+    if not ref_available():
+        raise FileNotFoundError(REF_BIN)
+    cmd = [REF_BIN, "--dir", workdir, "-f", name, "-k", str(K),
+           "-direct", str(int(directed)), "-weight", str(int(weighted)),
+           "--parts", parts if isinstance(parts, str) else ",".join(map(str, parts))]
+    if meta_out:
+        cmd += ["--meta", os.path.abspath(meta_out)]
+    if dist_out:
+        cmd += ["--dist", os.path.abspath(dist_out)]
+    env = dict(os.environ)
+    if threads:
+        env["OMP_NUM_THREADS"] = str(threads)
+    if partition_file:
+        env["FAP_PARTITION_FILE"] = os.path.abspath(partition_file)
+    r = subprocess.run(cmd, check=True, capture_output=True, text=True, env=env,
+                       timeout=timeout)
+    return [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
+
+
+# --------------------------------------------------------------------------
+# Comparison helpers
+# --------------------------------------------------------------------------
+
+def to_i32(block_f32: np.ndarray) -> np.ndarray:
+    """Reference float distances on integer weights -> int32 (exact while the
+    finite distances stay below 2^24); the sentinel 1e8 maps to 100000000."""
+    return block_f32.astype(np.int64).astype(np.int32)
+
+
+def row_checksums(block_i32: np.ndarray) -> np.ndarray:
+    """Per-row checksum: sum_j uint32(v[j]) * (2j + 1) mod 2^64."""
+    b = np.ascontiguousarray(block_i32).view(np.uint32).astype(np.uint64)
+    wts = (2 * np.arange(b.shape[1], dtype=np.uint64) + 1)
+    with np.errstate(over="ignore"):
+        return (b * wts[None, :]).sum(axis=1, dtype=np.uint64)

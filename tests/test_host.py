@@ -1,0 +1,100 @@
+"""Host half of the drop-in fapGraph (no GPU needed): MatrixMarket reading,
+METIS partition, boundary detection and renumbering must reproduce the
+reference's CSR, graph_id and st2ed exactly (golden fixtures made by the
+reference itself)."""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+from conftest import golden_names, load_golden, write_golden_mtx
+from fastapsp_b200 import FapError, fapGraph
+from fastapsp_b200 import _lib as L
+
+
+def _host_graph(case, tmp):
+    write_golden_mtx(case, tmp)
+    g = fapGraph(case["name"], bool(case["directed"]), bool(case["weighted"]), int(case["K"]),
+                 root=tmp)
+    if case["injected_partition"]:
+        gid0 = (np.arange(case["n"], dtype=np.int64) * case["K"] // case["n"]).astype(np.int32)
+        g.setPartition(gid0 + 1)
+    g.preCondition()
+    return g
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_csr_partition_renumbering_match_reference(name):
+    case = load_golden(name)
+    with tempfile.TemporaryDirectory() as tmp:
+        g = _host_graph(case, tmp)
+        ro, col, w = g.csr()
+        assert g.num_vertexs == case["n"]
+        assert g.num_edges == case["m"]
+        np.testing.assert_array_equal(ro, case["row_offset"])
+        used = case["row_offset"][-1]
+        np.testing.assert_array_equal(col, case["col_val"][:used])
+        np.testing.assert_array_equal(w, case["weight"][:used])
+        np.testing.assert_array_equal(g.getGraphId(), case["graph_id"])
+        np.testing.assert_array_equal(g.getMapping(), case["st2ed"])
+        vn, vo, bn = g.partInfo()
+        np.testing.assert_array_equal(vn[1:], case["ver_num"][1:])
+        np.testing.assert_array_equal(vo[1:], case["ver_offset"][1:])
+        np.testing.assert_array_equal(bn[1:], case["bdy_num"][1:])
+        assert g.isSplit() == (case["n"] > 20000)
+        for p in range(1, case["K"] + 1):
+            idx = g.getSubGraphIndex(p)
+            np.testing.assert_array_equal(idx, case["st2ed"][vo[p]:vo[p] + vn[p]])
+
+
+def test_metadata_constructor_matches_file_constructor():
+    case = load_golden("road300_k6")
+    with tempfile.TemporaryDirectory() as tmp:
+        a = _host_graph(case, tmp)
+    ro, col, w = a.csr()
+    b = fapGraph.from_csr(case["n"], case["m"], ro, col, w, int(case["K"]))
+    b.preCondition()
+    np.testing.assert_array_equal(a.getGraphId(), b.getGraphId())
+    np.testing.assert_array_equal(a.getMapping(), b.getMapping())
+
+
+def test_missing_file_raises_io_error():
+    with tempfile.TemporaryDirectory() as tmp:
+        with pytest.raises(FapError) as e:
+            fapGraph("nope", False, False, 4, root=tmp)
+        assert e.value.code == L.FAP_ERR_IO
+
+
+def test_bad_k_and_bad_partition():
+    case = load_golden("grid12_k4")
+    with tempfile.TemporaryDirectory() as tmp:
+        write_golden_mtx(case, tmp)
+        with pytest.raises(FapError):
+            fapGraph(case["name"], False, False, 0, root=tmp)
+        g = fapGraph(case["name"], False, False, 4, root=tmp)
+        with pytest.raises(FapError):
+            g.setPartition(np.zeros(case["n"], np.int32))      # ids must be 1..K
+        with pytest.raises(FapError):
+            g.setPartition(np.ones(case["n"] - 1, np.int32))   # wrong length
+
+
+def test_malformed_mtx():
+    with tempfile.TemporaryDirectory() as tmp:
+        d = os.path.join(tmp, "graph", "unweight-undirected")
+        os.makedirs(d)
+        with open(os.path.join(d, "bad.mtx"), "w") as f:
+            f.write("3 3 2\n1 2\n2 9\n")   # vertex 9 out of range
+        with pytest.raises(FapError) as e:
+            fapGraph("bad", False, False, 2, root=tmp)
+        assert e.value.code == L.FAP_ERR_IO
+
+
+def test_solve_before_precondition_is_an_error():
+    case = load_golden("grid12_k4")
+    with tempfile.TemporaryDirectory() as tmp:
+        write_golden_mtx(case, tmp)
+        g = fapGraph(case["name"], False, False, 4, root=tmp)
+        with pytest.raises(FapError) as e:
+            g.solveSubGraph(1)
+        assert e.value.code == L.FAP_ERR_STATE
