@@ -363,19 +363,18 @@ int32_t fapGraph::solveSubGraph(int32_t id, bool path_needed) {
   const int64_t n = num_vertexs;
   void *dp;
   int64_t rows, ld;
-  if (fap_graph_block(dg_, id, &dp, &rows, &ld) != FAP_OK) {
-    if (mode_ == SolveMode::Batched) {
-      // Solve every part once (blocks stay resident); later calls only copy.
-      std::vector<int32_t> all;
-      for (int32_t p = 1; p <= K; p++) all.push_back(p);
-      if (fap_solve(dg_, all.data(), (int32_t)all.size(), FAP_MODE_BATCHED) != FAP_OK) {
-        // Not enough room for every block: solve this part alone.
-        run_parts({id});
-      } else {
-        check(fap_graph_check(dg_), "fap_graph_check");
-      }
-    } else {
+  if (mode_ == SolveMode::Plain) {
+    // Plain form: every call solves its part with its own launch sequence.
+    run_parts({id});
+  } else if (fap_graph_block(dg_, id, &dp, &rows, &ld) != FAP_OK) {
+    // Batched form: solve every part once (blocks stay resident in HBM);
+    // later calls only copy.  Without room for every block, solve this part.
+    std::vector<int32_t> all;
+    for (int32_t p = 1; p <= K; p++) all.push_back(p);
+    if (fap_solve(dg_, all.data(), (int32_t)all.size(), FAP_MODE_BATCHED) != FAP_OK) {
       run_parts({id});
+    } else {
+      check(fap_graph_check(dg_), "fap_graph_check");
     }
   }
   subgraph_dist.resize((size_t)C_BlockVer_num[id] * n);
