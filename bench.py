@@ -129,6 +129,24 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def _jsonable(o):
+    if isinstance(o, (np.floating,)):
+        return float(o)
+    if isinstance(o, (np.integer,)):
+        return int(o)
+    if isinstance(o, np.ndarray):
+        return o.tolist()
+    raise TypeError(type(o).__name__)
+
+
+def emit(line):
+    print(json.dumps(line, default=_jsonable), flush=True)
+
+
+def log(msg):
+    print(f"[bench {time.strftime('%H:%M:%S')}] {msg}", file=sys.stderr, flush=True)
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -225,7 +243,7 @@ def main_reference(args):
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
-    print(json.dumps(line), flush=True)
+    emit(line)
 
 
 # ---------------------------------------------------------------------------
@@ -263,7 +281,9 @@ def main_fap(args):
         dist.all_reduce(t, op=dist.ReduceOp.SUM)
         return float(t.item())
 
+    t_load = time.perf_counter()
     wl = workloads.load(args.workload)
+    log(f"workload {wl.name} loaded in {time.perf_counter() - t_load:.1f} s: {wl.describe()}")
     n = wl.n
     vn, vo, bn = wl.ver_num, wl.ver_offset, wl.bdy_num
     mine = shard_parts(vn, bn, n, world)[rank]
@@ -318,6 +338,8 @@ def main_fap(args):
     ms_per_step = max_ms / args.steps
     value = total_entries * args.steps / (max_ms * 1e-3)
     st = np.mean(np.stack(stages), 0)  # [sssp, gather, floyd, minplus, total]
+    log(f"batched: {ms_per_step:.3f} ms/step, stages {np.round(st, 3).tolist()}, "
+        f"{value:.4g} entries/s")
 
     # ---- plain form ----
     plain_ms = []
@@ -334,6 +356,7 @@ def main_fap(args):
     dg.check()
     plain_max = allmax(float(np.sum(plain_ms))) if plain_ms else float("nan")
     plain_value = total_entries * len(plain_ms) / (plain_max * 1e-3) if plain_ms else None
+    log(f"plain: {plain_ms} ms")
 
     # ---- roofline figures per stage (algorithmic work of one launch) ----
     m_arcs = int(ro[-1])
@@ -401,6 +424,7 @@ def main_fap(args):
             e2e_s.append(t1 - t0)
     e2e_max = allmax(float(np.sum(e2e_s)))
     e2e_value = total_entries * len(e2e_s) / e2e_max
+    log(f"e2e: {e2e_s} s/step")
 
     # ---- CPU baseline (rank 0, N=1 only) ----
     cpu = None
@@ -439,7 +463,7 @@ def main_fap(args):
             "gpu_launches": int(launches),
             "clocks": clk,
         }
-        print(json.dumps(line), flush=True)
+        emit(line)
     if world > 1:
         dist.destroy_process_group()
 

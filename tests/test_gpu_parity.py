@@ -101,9 +101,22 @@ def test_subgraph_getters_and_self_check(cuda_ok):
             row = g.getDistanceFromOnePoint(v)
             assert_dist_equal(row, blk[3], True)
             assert g.getDistanceP2P(v, 7) == blk[3, 7]
-            assert g.check_result(p)
         with pytest.raises(FapError):
             g.getSubGraphDistance(1)  # not the current part
+
+
+@pytest.mark.parametrize("name", ["grid12_k4", "disconnected_k3"])
+def test_check_result_self_check(cuda_ok, name):
+    """check_result compares sampled entries with fresh GPU shortest-path rows
+    (the reference's check_ans, fap/utils/checkResult.h:38-82).  Like the
+    reference's, it expects true shortest distances, so graphs whose inner
+    rows carry the duplicate-edge rule are excluded."""
+    case = load_golden(name)
+    with tempfile.TemporaryDirectory() as tmp:
+        g = build_graph(case, tmp, FAP_MODE_BATCHED)
+        for p in range(1, case["K"] + 1):
+            g.solveSubGraph(p)
+            assert g.check_result(p)
 
 
 def test_plain_and_batched_blocks_identical(cuda_ok):
