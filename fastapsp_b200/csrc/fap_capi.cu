@@ -102,6 +102,8 @@ struct fap_ctx {
   DevBuf status;      // int device status for device-pointer ops
   DevBuf sink;        // microbenchmark sink
   int64_t launches = 0;
+  int graphs = 0;             // live fap_dgraph objects created on this context
+  bool destroy_pending = false;  // fap_ctx_destroy called while graphs were live
 };
 
 struct fap_dgraph {
@@ -185,8 +187,8 @@ extern "C" int fap_ctx_create(int device, fap_ctx **out) {
   return FAP_OK;
 }
 
-extern "C" int fap_ctx_destroy(fap_ctx *c) {
-  if (!c) return FAP_OK;
+namespace {
+void ctx_release(fap_ctx *c) {
   DeviceGuard g(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   c->scratch.release();
@@ -196,6 +198,19 @@ extern "C" int fap_ctx_destroy(fap_ctx *c) {
     if (ev) cudaEventDestroy(ev);
   if (c->own) cudaStreamDestroy(c->own);
   delete c;
+}
+}  // namespace
+
+// A context outlives its graphs: with graphs still alive the release is
+// deferred until the last of them is destroyed, so callers (and garbage
+// collectors) may destroy the two in either order.
+extern "C" int fap_ctx_destroy(fap_ctx *c) {
+  if (!c) return FAP_OK;
+  if (c->graphs > 0) {
+    c->destroy_pending = true;
+    return FAP_OK;
+  }
+  ctx_release(c);
   return FAP_OK;
 }
 
@@ -253,6 +268,7 @@ extern "C" int fap_graph_create(fap_ctx *ctx, int32_t n, int64_t m, const int32_
   DeviceGuard g(ctx->device);
   fap_dgraph *G = new fap_dgraph();
   G->ctx = ctx;
+  ctx->graphs++;
   G->n = n;
   G->m = used;
   G->dtype = dt;
@@ -286,13 +302,18 @@ extern "C" int fap_graph_create(fap_ctx *ctx, int32_t n, int64_t m, const int32_
 
 extern "C" int fap_graph_destroy(fap_dgraph *G) {
   if (!G) return FAP_OK;
-  DeviceGuard g(G->ctx->device);
-  cudaStreamSynchronize(G->ctx->stream);
-  for (DevBuf *b : {&G->ro, &G->col, &G->w, &G->d_gid, &G->d_st2ed, &G->d_ed2st, &G->D, &G->F,
-                    &G->d_parts, &G->d_work, &G->d_src, &G->d_srcrows, &G->d_status,
-                    &G->d_checks, &G->staging})
-    b->release();
+  fap_ctx *c = G->ctx;
+  {
+    DeviceGuard g(c->device);
+    cudaStreamSynchronize(c->stream);
+    for (DevBuf *b : {&G->ro, &G->col, &G->w, &G->d_gid, &G->d_st2ed, &G->d_ed2st, &G->D, &G->F,
+                      &G->d_parts, &G->d_work, &G->d_src, &G->d_srcrows, &G->d_status,
+                      &G->d_checks, &G->staging})
+      b->release();
+  }
   delete G;
+  c->graphs--;
+  if (c->destroy_pending && c->graphs == 0) ctx_release(c);
   return FAP_OK;
 }
 

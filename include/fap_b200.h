@@ -73,7 +73,9 @@ FAP_API const char *fap_last_error(void);
 /* ABI version: 0xMMmmpp. */
 FAP_API int fap_version(void);
 
-/* ---- context: one CUDA device + one stream ---- */
+/* ---- context: one CUDA device + one stream ----
+ * Destroying a context whose graphs are still alive defers its release
+ * until the last of those graphs is destroyed. */
 FAP_API int fap_ctx_create(int device, fap_ctx **out);
 FAP_API int fap_ctx_destroy(fap_ctx *ctx);
 /* Use an external cudaStream_t (passed as void*); NULL = the context's own stream. */
