@@ -385,7 +385,7 @@ def main_fap(args):
                 "peak_source": "measured relaxation microbenchmark (fap_measure_relax_peak)",
                 "traffic": read_traffic(wl.name, "floyd_part_kernel")}
     else:
-        kern = "sssp_bitmap_kernel" if dom == "sssp" else "minplus_part_kernel"
+        kern = "sssp_frontier_kernel" if dom == "sssp" else "minplus_part_kernel"
         a = stage_roof[dom]["achieved_gbs"]
         roof = {"kernel": kern, "bound": "hbm", "achieved": a, "peak": hbm_peak, "unit": "GB/s",
                 "frac": a / hbm_peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",

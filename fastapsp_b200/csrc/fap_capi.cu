@@ -112,6 +112,11 @@ struct fap_dgraph {
   int64_t m = 0;
   int dtype = FAP_DTYPE_F32;
   DevBuf ro, col, w;
+  std::vector<int32_t> h_ro, h_col;
+  std::vector<uint32_t> h_w;      // weight bits as uploaded (int32 or float)
+  double mean_w = 1.0;
+  // CSR relabelled into sorted-position order (SSSP work space)
+  DevBuf ro_s, col_s, w_s, sssp_scratch;
   // partition
   int32_t K = 0;
   std::vector<int32_t> gid, st2ed, ed2st, vnum, voff, bnum;
@@ -284,15 +289,22 @@ extern "C" int fap_graph_create(fap_ctx *ctx, int32_t n, int64_t m, const int32_
   cudaError_t e = cudaMemcpy(G->ro.p, row_offset, (size_t)(n + 1) * 4, cudaMemcpyHostToDevice);
   if (e == cudaSuccess && used > 0)
     e = cudaMemcpy(G->col.p, col_val, (size_t)used * 4, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess && used > 0) {
+  G->h_ro.assign(row_offset, row_offset + n + 1);
+  G->h_col.assign(col_val, col_val + used);
+  G->h_w.resize((size_t)used);
+  double wsum = 0.0;
+  for (int64_t i = 0; i < used; i++) {
+    wsum += weight[i];
     if (dt == FAP_DTYPE_I32) {
-      std::vector<int32_t> wi((size_t)used);
-      for (int64_t i = 0; i < used; i++) wi[i] = (int32_t)weight[i];
-      e = cudaMemcpy(G->w.p, wi.data(), (size_t)used * 4, cudaMemcpyHostToDevice);
+      const int32_t wi = (int32_t)weight[i];
+      std::memcpy(&G->h_w[i], &wi, 4);
     } else {
-      e = cudaMemcpy(G->w.p, weight, (size_t)used * 4, cudaMemcpyHostToDevice);
+      std::memcpy(&G->h_w[i], &weight[i], 4);
     }
   }
+  G->mean_w = used > 0 ? std::max(wsum / (double)used, 1e-30) : 1.0;
+  if (e == cudaSuccess && used > 0)
+    e = cudaMemcpy(G->w.p, G->h_w.data(), (size_t)used * 4, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return cleanup(fail(FAP_ERR_CUDA, "CSR upload: %s", cudaGetErrorString(e)));
   if ((rc = G->d_status.ensure(sizeof(int))) != FAP_OK) return cleanup(rc);
   cudaMemset(G->d_status.p, 0, sizeof(int));
@@ -306,9 +318,9 @@ extern "C" int fap_graph_destroy(fap_dgraph *G) {
   {
     DeviceGuard g(c->device);
     cudaStreamSynchronize(c->stream);
-    for (DevBuf *b : {&G->ro, &G->col, &G->w, &G->d_gid, &G->d_st2ed, &G->d_ed2st, &G->D, &G->F,
-                      &G->d_parts, &G->d_work, &G->d_src, &G->d_srcrows, &G->d_status,
-                      &G->d_checks, &G->staging})
+    for (DevBuf *b : {&G->ro, &G->col, &G->w, &G->ro_s, &G->col_s, &G->w_s, &G->sssp_scratch,
+                      &G->d_gid, &G->d_st2ed, &G->d_ed2st, &G->D, &G->F, &G->d_parts, &G->d_work,
+                      &G->d_src, &G->d_srcrows, &G->d_status, &G->d_checks, &G->staging})
       b->release();
   }
   delete G;
@@ -360,6 +372,26 @@ extern "C" int fap_graph_set_parts(fap_dgraph *G, int32_t K, const int32_t *grap
   FAP_CK(cudaMemcpy(G->d_gid.p, G->gid.data(), (size_t)n * 4, cudaMemcpyHostToDevice));
   FAP_CK(cudaMemcpy(G->d_st2ed.p, G->st2ed.data(), (size_t)n * 4, cudaMemcpyHostToDevice));
   FAP_CK(cudaMemcpy(G->d_ed2st.p, G->ed2st.data(), (size_t)n * 4, cudaMemcpyHostToDevice));
+  // SSSP work space: the CSR relabelled into sorted positions, so that
+  // vertices of one part (geometrically compact) sit next to each other.
+  const int64_t m = G->m;
+  std::vector<int32_t> ro_s((size_t)n + 1, 0), col_s((size_t)std::max<int64_t>(m, 1));
+  std::vector<uint32_t> w_s((size_t)std::max<int64_t>(m, 1));
+  for (int32_t i = 0; i < n; i++) {
+    const int32_t v = G->st2ed[i];
+    ro_s[i + 1] = ro_s[i] + (G->h_ro[v + 1] - G->h_ro[v]);
+    int32_t pos = ro_s[i];
+    for (int32_t e = G->h_ro[v]; e < G->h_ro[v + 1]; e++, pos++) {
+      col_s[pos] = G->ed2st[G->h_col[e]];
+      w_s[pos] = G->h_w[e];
+    }
+  }
+  FAP_TRY(G->ro_s.ensure((size_t)(n + 1) * 4));
+  FAP_TRY(G->col_s.ensure(col_s.size() * 4));
+  FAP_TRY(G->w_s.ensure(w_s.size() * 4));
+  FAP_CK(cudaMemcpy(G->ro_s.p, ro_s.data(), (size_t)(n + 1) * 4, cudaMemcpyHostToDevice));
+  FAP_CK(cudaMemcpy(G->col_s.p, col_s.data(), col_s.size() * 4, cudaMemcpyHostToDevice));
+  FAP_CK(cudaMemcpy(G->w_s.p, w_s.data(), w_s.size() * 4, cudaMemcpyHostToDevice));
   return FAP_OK;
 }
 
@@ -428,7 +460,7 @@ int prepare_batch(fap_dgraph *G, const std::vector<int32_t> &ids) {
     G->max_s = std::max(G->max_s, d.s);
     G->parts.push_back(d);
     for (int32_t k = 0; k < d.b; k++) {
-      G->src.push_back(G->st2ed[d.start + k]);
+      G->src.push_back(d.start + k);  // sorted position = SSSP work-space id
       G->srcrows.push_back(d.row_base + k);
     }
     G->part_src_off.push_back((int32_t)G->src.size());
@@ -441,6 +473,8 @@ int prepare_batch(fap_dgraph *G, const std::vector<int32_t> &ids) {
   FAP_TRY(G->d_work.ensure(std::max<size_t>(G->work.size(), 1) * sizeof(MPWork)));
   FAP_TRY(G->d_src.ensure(std::max<size_t>(G->src.size(), 1) * 4));
   FAP_TRY(G->d_srcrows.ensure(std::max<size_t>(G->srcrows.size(), 1) * 8));
+  FAP_TRY(G->sssp_scratch.ensure(
+      (size_t)std::max(sssp_scratch_rows(G->n, (int)G->src.size()), 1) * (size_t)G->n * 4));
   cudaStream_t st = G->ctx->stream;
   FAP_CK(cudaStreamSynchronize(st));
   FAP_CK(cudaMemcpy(G->d_parts.p, G->parts.data(), G->parts.size() * sizeof(PartDesc), cudaMemcpyHostToDevice));
@@ -456,13 +490,15 @@ int prepare_batch(fap_dgraph *G, const std::vector<int32_t> &ids) {
   return FAP_OK;
 }
 
+// Bucket width of the near/far SSSP: the tuned value when set, else 64 mean
+// edge weights (wide enough that a bucket is finished in a few rounds, narrow
+// enough to keep re-relaxations near Dijkstra's count on road-like graphs).
 template <typename T>
 T sssp_delta_for(const fap_dgraph *G) {
-  if (G->sssp_delta > 0) {
-    const double d = std::min<double>(G->sssp_delta, (double)Dist<T>::inf());
-    return (T)d;
-  }
-  return Dist<T>::inf();  // plain frontier Bellman-Ford
+  double d = G->sssp_delta > 0 ? G->sssp_delta : 64.0 * G->mean_w;
+  d = std::min<double>(d, (double)Dist<T>::inf());
+  if (Dist<T>::kDtype == FAP_DTYPE_I32) d = std::max(1.0, std::floor(d));
+  return (T)d;
 }
 
 template <typename T>
@@ -474,6 +510,9 @@ int run_solve(fap_dgraph *G, int mode) {
   T *D = G->D.as<T>();
   T *F = G->F.as<T>();
   const int32_t *ro = G->ro.as<const int32_t>(), *col = G->col.as<const int32_t>();
+  const int32_t *ro_s = G->ro_s.as<const int32_t>(), *col_s = G->col_s.as<const int32_t>();
+  const T *w_s = G->w_s.as<const T>();
+  T *scratch = G->sssp_scratch.as<T>();
   const PartDesc *dp = G->d_parts.as<const PartDesc>();
   const MPWork *dw = G->d_work.as<const MPWork>();
   const int32_t *src = G->d_src.as<const int32_t>();
@@ -488,8 +527,8 @@ int run_solve(fap_dgraph *G, int mode) {
   for (int i = 0; i < 5; i++) G->timing[i] = -1.0f;
   if (mode == FAP_MODE_BATCHED) {
     FAP_CK(cudaEventRecord(c->ev[0], st));
-    FAP_CK(launch_sssp<T>(ro, col, w, G->n, src, srow, (int)G->src.size(), D, G->ldD, G->ldD,
-                          delta, max_rounds, status, st, &L));
+    FAP_CK(launch_sssp<T>(ro_s, col_s, w_s, G->n, src, srow, (int)G->src.size(), D, G->ldD, G->ldD,
+                          ed2st, scratch, delta, max_rounds, status, st, &L));
     FAP_CK(cudaEventRecord(c->ev[1], st));
     FAP_CK(launch_gather<T>(dp, np, G->max_ldf, ro, col, w, gid, st2ed, ed2st, D, G->ldD, F, st, &L));
     FAP_CK(cudaEventRecord(c->ev[2], st));
@@ -503,8 +542,8 @@ int run_solve(fap_dgraph *G, int mode) {
       const PartDesc &d = G->parts[i];
       const int s0 = G->part_src_off[i], s1 = G->part_src_off[i + 1];
       const int w0 = G->part_work_off[i], w1 = G->part_work_off[i + 1];
-      FAP_CK(launch_sssp<T>(ro, col, w, G->n, src + s0, srow + s0, s1 - s0, D, G->ldD, G->ldD,
-                            delta, max_rounds, status, st, &L));
+      FAP_CK(launch_sssp<T>(ro_s, col_s, w_s, G->n, src + s0, srow + s0, s1 - s0, D, G->ldD,
+                            G->ldD, ed2st, scratch, delta, max_rounds, status, st, &L));
       FAP_CK(launch_gather<T>(dp + i, 1, d.ldf, ro, col, w, gid, st2ed, ed2st, D, G->ldD, F, st, &L));
       FAP_CK(launch_floyd_matrix<T>(F + d.f_off, d.ldf, d.ldf / kFloydTile, st, &L));
       FAP_CK(launch_bdy_scatter<T>(dp + i, 1, F, D, G->ldD, st2ed, d.b, d.s, st, &L));
@@ -676,11 +715,13 @@ extern "C" int fap_op_sssp(fap_ctx *c, int dtype, int32_t n, int64_t m, const in
   const int64_t rounds = 8 * (int64_t)n + 1024;
   if (dtype == FAP_DTYPE_I32) {
     FAP_CK(launch_sssp<int32_t>(row_offset, col_val, (const int32_t *)weight, n, sources, nullptr,
-                                num_sources, (int32_t *)out, ld_out, n, kInfI32, rounds,
+                                num_sources, (int32_t *)out, ld_out, n, nullptr, nullptr, kInfI32,
+                                rounds,
                                 c->status.as<int>(), c->stream, &L));
   } else if (dtype == FAP_DTYPE_F32) {
     FAP_CK(launch_sssp<float>(row_offset, col_val, (const float *)weight, n, sources, nullptr,
-                              num_sources, (float *)out, ld_out, n, kInfF32, rounds,
+                              num_sources, (float *)out, ld_out, n, nullptr, nullptr, kInfF32,
+                              rounds,
                               c->status.as<int>(), c->stream, &L));
   } else {
     return fail(FAP_ERR_INVALID, "bad dtype %d", dtype);
@@ -764,6 +805,37 @@ extern "C" int fap_measure_relax_peak(fap_ctx *c, int dtype, double *relax_per_s
   return FAP_OK;
 }
 
+namespace {
+// Distance rows from original-id sources into rows (count x n, dense).  Uses
+// the relabelled work space when the partition is known.
+template <typename T>
+cudaError_t sssp_rows_launch(fap_dgraph *G, const int32_t *h_sources, int32_t count, DevBuf &srcs,
+                             DevBuf &rows, DevBuf &scratch, int64_t *L) {
+  cudaStream_t st = G->ctx->stream;
+  const int64_t n = G->n;
+  const int64_t rounds = G->sssp_max_rounds > 0 ? G->sssp_max_rounds : 8 * n + 1024;
+  const bool relabel = G->K > 0;
+  std::vector<int32_t> work(h_sources, h_sources + count);
+  if (relabel)
+    for (auto &x : work) x = G->ed2st[x];
+  cudaError_t e = cudaMemcpyAsync(srcs.p, work.data(), (size_t)count * 4, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(G->d_status.p, 0, sizeof(int), st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return e;
+  if (relabel) {
+    if (scratch.ensure((size_t)std::max(sssp_scratch_rows(G->n, count), 1) * n * 4) != FAP_OK)
+      return cudaErrorMemoryAllocation;
+    return launch_sssp<T>(G->ro_s.as<int32_t>(), G->col_s.as<int32_t>(), G->w_s.as<T>(), G->n,
+                          srcs.as<int32_t>(), nullptr, count, rows.as<T>(), n, n,
+                          G->d_ed2st.as<int32_t>(), scratch.as<T>(), sssp_delta_for<T>(G), rounds,
+                          G->d_status.as<int>(), st, L);
+  }
+  return launch_sssp<T>(G->ro.as<int32_t>(), G->col.as<int32_t>(), G->w.as<T>(), G->n,
+                        srcs.as<int32_t>(), nullptr, count, rows.as<T>(), n, n, nullptr, nullptr,
+                        sssp_delta_for<T>(G), rounds, G->d_status.as<int>(), st, L);
+}
+}  // namespace
+
 extern "C" int fap_graph_sssp_rows(fap_dgraph *G, const int32_t *sources, int32_t count,
                                    float *host_out) {
   if (!G || (count > 0 && (!sources || !host_out))) return fail(FAP_ERR_INVALID, "NULL argument");
@@ -774,38 +846,31 @@ extern "C" int fap_graph_sssp_rows(fap_dgraph *G, const int32_t *sources, int32_
   DeviceGuard g(G->ctx->device);
   cudaStream_t st = G->ctx->stream;
   const int64_t n = G->n;
-  DevBuf srcs, rows;
-  FAP_TRY(srcs.ensure((size_t)count * 4));
-  FAP_TRY(rows.ensure((size_t)count * n * 4));
+  DevBuf srcs, rows, scratch;
   int rc = FAP_OK;
   int64_t L = 0;
-  const int64_t rounds = G->sssp_max_rounds > 0 ? G->sssp_max_rounds : 8 * n + 1024;
   do {
-    cudaError_t e = cudaMemcpyAsync(srcs.p, sources, (size_t)count * 4, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(G->d_status.p, 0, sizeof(int), st);
-    if (e == cudaSuccess) {
-      if (G->dtype == FAP_DTYPE_I32)
-        e = launch_sssp<int32_t>(G->ro.as<int32_t>(), G->col.as<int32_t>(), G->w.as<int32_t>(), G->n,
-                                 srcs.as<int32_t>(), nullptr, count, rows.as<int32_t>(), n, n,
-                                 sssp_delta_for<int32_t>(G), rounds, G->d_status.as<int>(), st, &L);
-      else
-        e = launch_sssp<float>(G->ro.as<int32_t>(), G->col.as<int32_t>(), G->w.as<float>(), G->n,
-                               srcs.as<int32_t>(), nullptr, count, rows.as<float>(), n, n,
-                               sssp_delta_for<float>(G), rounds, G->d_status.as<int>(), st, &L);
-    }
+    if ((rc = srcs.ensure((size_t)count * 4)) != FAP_OK) break;
+    if ((rc = rows.ensure((size_t)count * n * 4)) != FAP_OK) break;
+    cudaError_t e = (G->dtype == FAP_DTYPE_I32)
+                        ? sssp_rows_launch<int32_t>(G, sources, count, srcs, rows, scratch, &L)
+                        : sssp_rows_launch<float>(G, sources, count, srcs, rows, scratch, &L);
     if (e == cudaSuccess && G->dtype == FAP_DTYPE_I32)
       e = launch_i32_to_f32(rows.as<int32_t>(), count, n, n, rows.as<float>(), st, &L);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(host_out, rows.p, (size_t)count * n * 4, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) {
-      rc = fail(FAP_ERR_CUDA, "fap_graph_sssp_rows: %s", cudaGetErrorString(e));
+      cudaGetLastError();
+      rc = fail(e == cudaErrorMemoryAllocation ? FAP_ERR_NOMEM : FAP_ERR_CUDA,
+                "fap_graph_sssp_rows: %s", cudaGetErrorString(e));
       break;
     }
     rc = read_status(G);
   } while (0);
   srcs.release();
   rows.release();
+  scratch.release();
   G->ctx->launches += L;
   return rc;
 }

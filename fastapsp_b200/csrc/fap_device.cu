@@ -1,7 +1,7 @@
 // Kernels and launchers of the per-subgraph solve path (sm_100a).
 //
 // Stage map (reference fapGraph::run, fap/fap.cpp:92-181):
-//   stage 1   boundary SSSP            sssp_bitmap_kernel        (sssp.cuh)
+//   stage 1   boundary SSSP            sssp_frontier_kernel      (sssp.cuh)
 //   stage 2.1 Floyd matrix build       gather_kernel             (util_Myalgorithm.h:30-73)
 //   stage 2.2 Floyd-Warshall           floyd_part_kernel / floyd_phase*_kernel (floyd.cuh)
 //   stage 3.1 thin matrix              read in place from F      (util_Myalgorithm.h:88-95)
@@ -102,19 +102,45 @@ cudaError_t launch_gather(const PartDesc *parts, int nparts, int max_ldf, const 
 // ---------------------------------------------------------------------------
 // Stage 1 launcher
 // ---------------------------------------------------------------------------
+namespace {
+int sssp_resident_ctas(int n) {
+  static int cached_n = -1, cached = 0;
+  if (n == cached_n) return cached;
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const size_t smem = sssp_smem_bytes(n);
+  cudaFuncSetAttribute(sssp_frontier_kernel<int32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaFuncSetAttribute(sssp_frontier_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sssp_frontier_kernel<int32_t>, kSsspThreads, smem);
+  cudaGetLastError();
+  cached_n = n;
+  cached = std::max(1, per_sm) * std::max(1, sms);
+  return cached;
+}
+}  // namespace
+
+int sssp_scratch_rows(int n, int num_sources) {
+  return std::max(0, std::min(num_sources, sssp_resident_ctas(n)));
+}
+
 template <typename T>
 cudaError_t launch_sssp(const int32_t *row_offset, const int32_t *col, const T *w, int n,
                         const int32_t *sources, const int64_t *out_rows, int num_sources, T *out,
-                        int64_t ld, int64_t init_cols, T delta, int64_t max_rounds, int *status,
-                        cudaStream_t stream, int64_t *launches) {
+                        int64_t ld, int64_t init_cols, const int32_t *perm_out, T *scratch,
+                        T delta, int64_t max_rounds, int *status, cudaStream_t stream,
+                        int64_t *launches) {
   if (num_sources <= 0) return cudaSuccess;
-  size_t smem = sssp_smem_bytes(n);
-  auto kern = sssp_bitmap_kernel<T>;
+  const size_t smem = sssp_smem_bytes(n);
+  auto kern = sssp_frontier_kernel<T>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  kern<<<num_sources, kSsspThreads, smem, stream>>>(row_offset, col, w, n, sources, out_rows,
-                                                     num_sources, out, ld, init_cols, delta,
-                                                     max_rounds, status);
+  // With a relabelled work space every CTA needs a scratch row, so the grid
+  // is the resident CTA count and CTAs loop over sources.
+  const int grid = perm_out ? sssp_scratch_rows(n, num_sources) : num_sources;
+  kern<<<grid, kSsspThreads, smem, stream>>>(row_offset, col, w, n, sources, out_rows, num_sources,
+                                             out, ld, init_cols, perm_out, scratch, delta,
+                                             max_rounds, status);
   *launches += 1;
   return cudaGetLastError();
 }
@@ -416,7 +442,8 @@ cudaError_t launch_relax_peak(T *sink, int blocks, int iters, cudaStream_t strea
 #define FAPB_INSTANTIATE(T)                                                                       \
   template cudaError_t launch_sssp<T>(const int32_t *, const int32_t *, const T *, int,           \
                                       const int32_t *, const int64_t *, int, T *, int64_t,        \
-                                      int64_t, T, int64_t, int *, cudaStream_t, int64_t *);       \
+                                      int64_t, const int32_t *, T *, T, int64_t, int *,           \
+                                      cudaStream_t, int64_t *);                                   \
   template cudaError_t launch_gather<T>(const PartDesc *, int, int, const int32_t *,              \
                                         const int32_t *, const T *, const int32_t *,              \
                                         const int32_t *, const int32_t *, const T *, int64_t, T *, \

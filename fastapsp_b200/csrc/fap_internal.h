@@ -33,11 +33,19 @@ constexpr int kLdAlign = 128;  // output leading dimension multiple (= kMinplusB
 // Launchers.  T is int32_t or float.  All asynchronous on `stream`; each
 // returns the cudaError_t of its launch(es) and adds the number of kernel
 // launches it issued to *launches.
+// Stage 1.  row_offset/col/w/sources are in work space; with perm_out
+// (original vertex -> work id) the CTAs compute in `scratch` (sssp_scratch_rows
+// rows of n) and write out[v] = dist[perm_out[v]].
 template <typename T>
 cudaError_t launch_sssp(const int32_t *row_offset, const int32_t *col, const T *w, int n,
                         const int32_t *sources, const int64_t *out_rows, int num_sources, T *out,
-                        int64_t ld, int64_t init_cols, T delta, int64_t max_rounds, int *status,
-                        cudaStream_t stream, int64_t *launches);
+                        int64_t ld, int64_t init_cols, const int32_t *perm_out, T *scratch,
+                        T delta, int64_t max_rounds, int *status, cudaStream_t stream,
+                        int64_t *launches);
+
+// Rows of scratch the relabelled SSSP needs (= CTAs it launches) for
+// num_sources sources on this device.
+int sssp_scratch_rows(int n, int num_sources);
 
 template <typename T>
 cudaError_t launch_gather(const PartDesc *parts, int nparts, int max_ldf, const int32_t *row_offset,
