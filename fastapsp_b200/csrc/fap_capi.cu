@@ -132,13 +132,16 @@ struct fap_dgraph {
   std::vector<MPWork> work;
   std::vector<int32_t> src;
   std::vector<int64_t> srcrows;
-  std::vector<int32_t> part_src_off, part_work_off;  // per batch index, size nparts+1
+  std::vector<int32_t> part_src_off;                 // per batch index, size nparts+1
+  std::vector<int32_t> part_work_begin, part_work_end;  // per batch index, into work
+  int32_t n_thin = 0;  // work[0, n_thin) is thin-boundary work, the rest thick
   std::vector<int32_t> last_ids;
   int64_t f_elems = 0;
   int max_ldf = 0, max_b = 0, max_s = 0;
   // tuning
   double sssp_delta = -1.0;  // <0: automatic
   int64_t sssp_max_rounds = -1;  // <0: 8n + 1024
+  bool floyd_per_cta = false;     // batched Floyd: one CTA per part instead of per-tile launches
   // last solve
   int last_mode = -1;
   float timing[5] = {-1, -1, -1, -1, -1};
@@ -439,7 +442,10 @@ int prepare_batch(fap_dgraph *G, const std::vector<int32_t> &ids) {
   G->src.clear();
   G->srcrows.clear();
   G->part_src_off.assign(1, 0);
-  G->part_work_off.assign(1, 0);
+  G->part_work_begin.clear();
+  G->part_work_end.clear();
+  std::vector<MPWork> thick;
+  std::vector<char> is_thin;
   int64_t foff = 0;
   G->max_ldf = 0;
   G->max_b = 0;
@@ -464,9 +470,21 @@ int prepare_batch(fap_dgraph *G, const std::vector<int32_t> &ids) {
       G->srcrows.push_back(d.row_base + k);
     }
     G->part_src_off.push_back((int32_t)G->src.size());
-    for (int32_t m0 = 0; m0 < d.s - d.b; m0 += kMinplusBM) G->work.push_back(MPWork{(int32_t)i, m0});
-    G->part_work_off.push_back((int32_t)G->work.size());
+    const bool thin = d.b <= kThinBoundary;
+    std::vector<MPWork> &dst = thin ? G->work : thick;
+    G->part_work_begin.push_back((int32_t)dst.size());
+    for (int32_t m0 = 0; m0 < d.s - d.b; m0 += kMinplusBM) dst.push_back(MPWork{(int32_t)i, m0});
+    G->part_work_end.push_back((int32_t)dst.size());
+    is_thin.push_back(thin);
   }
+  // work = [thin parts' rows][thick parts' rows]
+  G->n_thin = (int32_t)G->work.size();
+  for (size_t i = 0; i < is_thin.size(); i++)
+    if (!is_thin[i]) {
+      G->part_work_begin[i] += G->n_thin;
+      G->part_work_end[i] += G->n_thin;
+    }
+  G->work.insert(G->work.end(), thick.begin(), thick.end());
   G->f_elems = foff;
   FAP_TRY(G->F.ensure((size_t)std::max<int64_t>(foff, 1) * 4));
   FAP_TRY(G->d_parts.ensure(std::max<size_t>(G->parts.size(), 1) * sizeof(PartDesc)));
@@ -532,22 +550,32 @@ int run_solve(fap_dgraph *G, int mode) {
     FAP_CK(cudaEventRecord(c->ev[1], st));
     FAP_CK(launch_gather<T>(dp, np, G->max_ldf, ro, col, w, gid, st2ed, ed2st, D, G->ldD, F, st, &L));
     FAP_CK(cudaEventRecord(c->ev[2], st));
-    FAP_CK(launch_floyd_parts<T>(dp, np, F, D, G->ldD, st2ed, st, &L));
+    if (G->floyd_per_cta) {
+      FAP_CK(launch_floyd_parts<T>(dp, np, F, D, G->ldD, st2ed, st, &L));
+    } else {
+      FAP_CK(launch_floyd_parts_multi<T>(dp, np, G->max_ldf, F, st, &L));
+      FAP_CK(launch_bdy_scatter<T>(dp, np, F, D, G->ldD, st2ed, G->max_b, G->max_s, st, &L));
+    }
     FAP_CK(cudaEventRecord(c->ev[3], st));
-    FAP_CK(launch_minplus_parts<T>(dp, dw, (int)G->work.size(), G->n, F, D, G->ldD, gid, ed2st, st, &L));
+    FAP_CK(launch_minplus_thin<T>(dp, dw, G->n_thin, G->n, F, D, G->ldD, gid, ed2st, st, &L));
+    FAP_CK(launch_minplus_parts<T>(dp, dw + G->n_thin, (int)G->work.size() - G->n_thin, G->n, F, D,
+                                   G->ldD, gid, ed2st, st, &L));
     FAP_CK(cudaEventRecord(c->ev[4], st));
   } else {
     FAP_CK(cudaEventRecord(c->ev[0], st));
     for (int i = 0; i < np; i++) {
       const PartDesc &d = G->parts[i];
       const int s0 = G->part_src_off[i], s1 = G->part_src_off[i + 1];
-      const int w0 = G->part_work_off[i], w1 = G->part_work_off[i + 1];
+      const int w0 = G->part_work_begin[i], w1 = G->part_work_end[i];
       FAP_CK(launch_sssp<T>(ro_s, col_s, w_s, G->n, src + s0, srow + s0, s1 - s0, D, G->ldD,
                             G->ldD, ed2st, scratch, delta, max_rounds, status, st, &L));
       FAP_CK(launch_gather<T>(dp + i, 1, d.ldf, ro, col, w, gid, st2ed, ed2st, D, G->ldD, F, st, &L));
       FAP_CK(launch_floyd_matrix<T>(F + d.f_off, d.ldf, d.ldf / kFloydTile, st, &L));
       FAP_CK(launch_bdy_scatter<T>(dp + i, 1, F, D, G->ldD, st2ed, d.b, d.s, st, &L));
-      FAP_CK(launch_minplus_parts<T>(dp, dw + w0, w1 - w0, G->n, F, D, G->ldD, gid, ed2st, st, &L));
+      if (d.b <= kThinBoundary)
+        FAP_CK(launch_minplus_thin<T>(dp, dw + w0, w1 - w0, G->n, F, D, G->ldD, gid, ed2st, st, &L));
+      else
+        FAP_CK(launch_minplus_parts<T>(dp, dw + w0, w1 - w0, G->n, F, D, G->ldD, gid, ed2st, st, &L));
     }
     FAP_CK(cudaEventRecord(c->ev[4], st));
   }
@@ -879,6 +907,10 @@ extern "C" int fap_graph_set_param(fap_dgraph *G, const char *key, double value)
   if (!G || !key) return fail(FAP_ERR_INVALID, "NULL argument");
   if (std::strcmp(key, "sssp_delta") == 0) {
     G->sssp_delta = (value > 0 && value < 1e8) ? value : -1.0;
+    return FAP_OK;
+  }
+  if (std::strcmp(key, "floyd_per_cta") == 0) {
+    G->floyd_per_cta = value != 0.0;
     return FAP_OK;
   }
   if (std::strcmp(key, "sssp_max_rounds") == 0) {

@@ -197,6 +197,75 @@ cudaError_t launch_floyd_matrix(T *mat, int64_t ld, int nb, cudaStream_t stream,
   return cudaGetLastError();
 }
 
+// Batched multi-launch form: pivot round kb of every part in three
+// launches (diagonal tiles, panel tiles, remainder tiles), so thousands of
+// tile CTAs keep every SM busy whatever the number of parts.  Parts have
+// nb_p = ldf / kFloydTile tiles per side; CTAs beyond a part's tiles exit.
+template <typename T>
+__global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS)
+    floyd_parts_phase1_kernel(const PartDesc *__restrict__ parts, T *F, int kb) {
+  extern __shared__ __align__(16) unsigned char fm_smem_raw[];
+  T *smem = reinterpret_cast<T *>(fm_smem_raw);
+  const PartDesc pd = parts[blockIdx.x];
+  if (kb >= pd.ldf / kFloydTile) return;
+  floyd_diag_close<T, kFloydTile>(F + pd.f_off, pd.ldf, kb * kFloydTile, smem);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS)
+    floyd_parts_phase2_kernel(const PartDesc *__restrict__ parts, T *F, int kb) {
+  extern __shared__ __align__(16) unsigned char fm_smem_raw[];
+  T *smem = reinterpret_cast<T *>(fm_smem_raw);
+  const PartDesc pd = parts[blockIdx.y];
+  const int nb = pd.ldf / kFloydTile;
+  int t = blockIdx.x;
+  if (kb >= nb || t >= 2 * (nb - 1)) return;
+  T *mat = F + pd.f_off;
+  if (t < nb - 1) {
+    const int j = t < kb ? t : t + 1;
+    floyd_tile_update<T, kFloydTile>(mat, pd.ldf, kb, j, kb, smem);
+  } else {
+    t -= nb - 1;
+    const int i = t < kb ? t : t + 1;
+    floyd_tile_update<T, kFloydTile>(mat, pd.ldf, i, kb, kb, smem);
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS)
+    floyd_parts_phase3_kernel(const PartDesc *__restrict__ parts, T *F, int kb) {
+  extern __shared__ __align__(16) unsigned char fm_smem_raw[];
+  T *smem = reinterpret_cast<T *>(fm_smem_raw);
+  const PartDesc pd = parts[blockIdx.y];
+  const int nb = pd.ldf / kFloydTile;
+  const int t = blockIdx.x;
+  if (kb >= nb || t >= (nb - 1) * (nb - 1)) return;
+  int i = t / (nb - 1), j = t % (nb - 1);
+  i = i < kb ? i : i + 1;
+  j = j < kb ? j : j + 1;
+  floyd_tile_update<T, kFloydTile>(F + pd.f_off, pd.ldf, i, j, kb, smem);
+}
+
+template <typename T>
+cudaError_t launch_floyd_parts_multi(const PartDesc *parts, int nparts, int max_ldf, T *F,
+                                     cudaStream_t stream, int64_t *launches) {
+  if (nparts <= 0) return cudaSuccess;
+  using FC = FloydCfg<T, kFloydTile>;
+  const size_t smem = FC::SMEM_ELEMS * sizeof(T);
+  const int nbmax = max_ldf / kFloydTile;
+  for (int kb = 0; kb < nbmax; kb++) {
+    floyd_parts_phase1_kernel<T><<<nparts, FC::THREADS, smem, stream>>>(parts, F, kb);
+    *launches += 1;
+    if (nbmax > 1) {
+      floyd_parts_phase2_kernel<T><<<dim3(2 * (nbmax - 1), nparts), FC::THREADS, smem, stream>>>(parts, F, kb);
+      floyd_parts_phase3_kernel<T><<<dim3((nbmax - 1) * (nbmax - 1), nparts), FC::THREADS, smem, stream>>>(
+          parts, F, kb);
+      *launches += 2;
+    }
+  }
+  return cudaGetLastError();
+}
+
 template <typename T>
 __global__ void bdy_scatter_kernel(const PartDesc *__restrict__ parts, const T *__restrict__ F,
                                    T *D, int64_t ldD, const int32_t *__restrict__ st2ed) {
@@ -286,6 +355,82 @@ __global__ void __launch_bounds__(MPCfg<T>::THREADS)
     }
 }
 
+// Thin-K variant (b <= kThinK): the product is store-bound, not
+// relaxation-bound, so the kernel is shaped around the stores.  A CTA owns a
+// strip of kThinCols columns (4 per thread: one 16-byte streaming store per
+// row) and a range of up to kMinplusBM rows of one part.  The part's b
+// boundary rows of the strip stay in registers for the whole CTA; the rows'
+// A values are staged in shared memory and read as broadcasts.
+constexpr int kThinK = kThinBoundary;
+constexpr int kThinCols = 4 * 256;
+
+template <typename T>
+__global__ void __launch_bounds__(256, 2)
+    minplus_thin_kernel(const PartDesc *__restrict__ parts, const MPWork *__restrict__ work, int n,
+                        const T *__restrict__ F, T *D, int64_t ldD,
+                        const int32_t *__restrict__ graph_id, const int32_t *__restrict__ ed2st) {
+  using V = typename Vec4<T>::type;
+  __shared__ __align__(16) T As[kMinplusBM][kThinK];
+  const MPWork wk = work[blockIdx.y];
+  const PartDesc pd = parts[wk.pidx];
+  const int M = pd.s - pd.b, b = pd.b;
+  const int rows = min(kMinplusBM, M - wk.m0);
+  const T inf = Dist<T>::inf();
+  // stage A rows (F[b + m0 + r][0..b-1]) in shared memory, sentinel-padded
+  const T *A = F + pd.f_off + (int64_t)(pd.b + wk.m0) * pd.ldf;
+  for (int t = threadIdx.x; t < kMinplusBM * kThinK; t += blockDim.x) {
+    const int r = t / kThinK, k = t % kThinK;
+    As[r][k] = (r < rows && k < b) ? __ldg(A + (int64_t)r * pd.ldf + k) : inf;
+  }
+  const int64_t c0 = (int64_t)blockIdx.x * kThinCols + 4 * threadIdx.x;
+  const bool live = c0 < ldD;
+  // the strip of the b boundary rows (S = D rows row_base .. row_base+b-1)
+  T sv[kThinK][4];
+#pragma unroll
+  for (int k = 0; k < kThinK; k++) {
+    if (live && k < b) {
+      const V v = __ldg(reinterpret_cast<const V *>(D + (pd.row_base + k) * ldD + c0));
+      sv[k][0] = v.x; sv[k][1] = v.y; sv[k][2] = v.z; sv[k][3] = v.w;
+    } else {
+      sv[k][0] = sv[k][1] = sv[k][2] = sv[k][3] = inf;
+    }
+  }
+  int own[4];
+  bool any_own = false;
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int64_t c = c0 + q;
+    int o = -1;
+    if (live && c < n && __ldg(graph_id + c) == pd.part) o = __ldg(ed2st + c) - pd.start;
+    own[q] = o;
+    any_own |= (o >= 0);
+  }
+  __syncthreads();
+  if (!live) return;
+  T *Cm = D + (pd.row_base + pd.b + wk.m0) * ldD + c0;
+  const T *Fr = F + pd.f_off + (int64_t)(pd.b + wk.m0) * pd.ldf;
+#pragma unroll 2
+  for (int r = 0; r < rows; r++) {
+    T acc[4] = {inf, inf, inf, inf};
+#pragma unroll
+    for (int k = 0; k < kThinK; k++) {
+      if (k < b) {
+        const T a = As[r][k];
+#pragma unroll
+        for (int q = 0; q < 4; q++) acc[q] = Dist<T>::relax(a, sv[k][q], acc[q]);
+      }
+    }
+    if (any_own) {
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+        if (own[q] >= 0) acc[q] = Fr[(int64_t)r * pd.ldf + own[q]];
+    }
+    V v;
+    v.x = acc[0]; v.y = acc[1]; v.z = acc[2]; v.w = acc[3];
+    __stcs(reinterpret_cast<V *>(Cm + (int64_t)r * ldD), v);
+  }
+}
+
 template <typename T>
 cudaError_t launch_minplus_parts(const PartDesc *parts, const MPWork *work, int nwork, int n,
                                  const T *F, T *D, int64_t ldD, const int32_t *graph_id,
@@ -296,6 +441,17 @@ cudaError_t launch_minplus_parts(const PartDesc *parts, const MPWork *work, int 
   dim3 grid((unsigned)(ldD / C::BN), (unsigned)nwork);
   minplus_part_kernel<T><<<grid, C::THREADS, smem, stream>>>(parts, work, n, F, D, ldD, graph_id,
                                                              ed2st);
+  *launches += 1;
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_minplus_thin(const PartDesc *parts, const MPWork *work, int nwork, int n,
+                                const T *F, T *D, int64_t ldD, const int32_t *graph_id,
+                                const int32_t *ed2st, cudaStream_t stream, int64_t *launches) {
+  if (nwork <= 0) return cudaSuccess;
+  dim3 grid((unsigned)ceil_div(ldD, kThinCols), (unsigned)nwork);
+  minplus_thin_kernel<T><<<grid, 256, 0, stream>>>(parts, work, n, F, D, ldD, graph_id, ed2st);
   *launches += 1;
   return cudaGetLastError();
 }
@@ -451,11 +607,16 @@ cudaError_t launch_relax_peak(T *sink, int blocks, int iters, cudaStream_t strea
   template cudaError_t launch_floyd_parts<T>(const PartDesc *, int, T *, T *, int64_t,            \
                                              const int32_t *, cudaStream_t, int64_t *);           \
   template cudaError_t launch_floyd_matrix<T>(T *, int64_t, int, cudaStream_t, int64_t *);        \
+  template cudaError_t launch_floyd_parts_multi<T>(const PartDesc *, int, int, T *, cudaStream_t, \
+                                                   int64_t *);                                    \
   template cudaError_t launch_bdy_scatter<T>(const PartDesc *, int, const T *, T *, int64_t,      \
                                              const int32_t *, int, int, cudaStream_t, int64_t *); \
   template cudaError_t launch_minplus_parts<T>(const PartDesc *, const MPWork *, int, int,        \
                                                const T *, T *, int64_t, const int32_t *,          \
                                                const int32_t *, cudaStream_t, int64_t *);         \
+  template cudaError_t launch_minplus_thin<T>(const PartDesc *, const MPWork *, int, int,         \
+                                              const T *, T *, int64_t, const int32_t *,           \
+                                              const int32_t *, cudaStream_t, int64_t *);          \
   template cudaError_t launch_minplus_generic<T>(int, int, int, const T *, int64_t, const T *,    \
                                                  int64_t, T *, int64_t, cudaStream_t, int64_t *); \
   template cudaError_t launch_fill<T>(T *, int64_t, int64_t, int64_t, T, cudaStream_t, int64_t *); \

@@ -59,6 +59,12 @@ template <typename T>
 cudaError_t launch_floyd_parts(const PartDesc *parts, int nparts, T *F, T *D, int64_t ldD,
                                const int32_t *st2ed, cudaStream_t stream, int64_t *launches);
 
+// Batched, multi-launch: every part's pivot round in three launches
+// (3 x max_ldf/kFloydTile launches in all); no boundary-row decode.
+template <typename T>
+cudaError_t launch_floyd_parts_multi(const PartDesc *parts, int nparts, int max_ldf, T *F,
+                                     cudaStream_t stream, int64_t *launches);
+
 // Plain: one padded matrix (ld multiple of kFloydTile, nb = ld / kFloydTile
 // tiles per side), one launch per phase per pivot block.
 template <typename T>
@@ -77,6 +83,14 @@ template <typename T>
 cudaError_t launch_minplus_parts(const PartDesc *parts, const MPWork *work, int nwork, int n,
                                  const T *F, T *D, int64_t ldD, const int32_t *graph_id,
                                  const int32_t *ed2st, cudaStream_t stream, int64_t *launches);
+
+// Same for parts with at most kThinBoundary boundary vertices (store-bound
+// shape).  Work rows must belong to such parts.
+constexpr int kThinBoundary = 16;
+template <typename T>
+cudaError_t launch_minplus_thin(const PartDesc *parts, const MPWork *work, int nwork, int n,
+                                const T *F, T *D, int64_t ldD, const int32_t *graph_id,
+                                const int32_t *ed2st, cudaStream_t stream, int64_t *launches);
 
 // Generic C = min(INF, A (x) B).
 template <typename T>

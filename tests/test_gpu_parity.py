@@ -135,6 +135,11 @@ def test_plain_and_batched_blocks_identical(cuda_ok):
         for x, y in zip(a, b):
             np.testing.assert_array_equal(x, y)
         np.testing.assert_array_equal(np.concatenate(a), case["row_checksums"])
+        dg.set_param("floyd_per_cta", 1)   # the one-CTA-per-part Floyd form
+        dg.solve(mode=FAP_MODE_BATCHED)
+        c = [dg.block_checksums(p) for p in range(1, case["K"] + 1)]
+        np.testing.assert_array_equal(np.concatenate(c), case["row_checksums"])
+        dg.set_param("floyd_per_cta", 0)
         # packed placement: only part 5 and 2, in a 2-part row budget
         dg.reserve(int(case["ver_num"][5] + case["ver_num"][2]))
         dg.solve([5, 2], mode=FAP_MODE_BATCHED)
