@@ -343,7 +343,7 @@ def main_fap(args):
 
     # ---- plain form ----
     plain_ms = []
-    for i in range(1 + args.plain_steps):
+    for i in range(1 + args.plain_steps if args.plain_steps > 0 else 0):
         flush.zero_()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
@@ -408,7 +408,7 @@ def main_fap(args):
     h2d = sum(a.nbytes for a in pin.values())
     d2h = my_rows * n * 4
     e2e_s = []
-    for i in range(1 + args.e2e_steps):
+    for i in range(1 + args.e2e_steps if args.e2e_steps > 0 else 0):
         torch.cuda.synchronize()
         barrier()
         t0 = time.perf_counter()
@@ -423,7 +423,7 @@ def main_fap(args):
         if i > 0:
             e2e_s.append(t1 - t0)
     e2e_max = allmax(float(np.sum(e2e_s)))
-    e2e_value = total_entries * len(e2e_s) / e2e_max
+    e2e_value = total_entries * len(e2e_s) / e2e_max if e2e_s else None
     log(f"e2e: {e2e_s} s/step")
 
     # ---- CPU baseline (rank 0, N=1 only) ----

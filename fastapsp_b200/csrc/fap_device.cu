@@ -370,12 +370,17 @@ __global__ void __launch_bounds__(256, 2)
                         const T *__restrict__ F, T *D, int64_t ldD,
                         const int32_t *__restrict__ graph_id, const int32_t *__restrict__ ed2st) {
   using V = typename Vec4<T>::type;
+  constexpr int kOwnMax = 32;  // own-part columns of a strip staged in shared memory
   __shared__ __align__(16) T As[kMinplusBM][kThinK];
+  __shared__ T Own[kMinplusBM][kOwnMax];
+  __shared__ int32_t own_col[kOwnMax];
+  __shared__ int s_nown;
   const MPWork wk = work[blockIdx.y];
   const PartDesc pd = parts[wk.pidx];
   const int M = pd.s - pd.b, b = pd.b;
   const int rows = min(kMinplusBM, M - wk.m0);
   const T inf = Dist<T>::inf();
+  if (threadIdx.x == 0) s_nown = 0;
   // stage A rows (F[b + m0 + r][0..b-1]) in shared memory, sentinel-padded
   const T *A = F + pd.f_off + (int64_t)(pd.b + wk.m0) * pd.ldf;
   for (int t = threadIdx.x; t < kMinplusBM * kThinK; t += blockDim.x) {
@@ -395,20 +400,38 @@ __global__ void __launch_bounds__(256, 2)
       sv[k][0] = sv[k][1] = sv[k][2] = sv[k][3] = inf;
     }
   }
-  int own[4];
+  // Own-part columns: their values come from the closed Floyd matrix (the
+  // reference's decode).  Register them and stage F[b+m0+r][j] for every row
+  // so that the row loop never waits on a gather.
+  int slot[4];
+  int jloc[4];
   bool any_own = false;
+  __syncthreads();
 #pragma unroll
   for (int q = 0; q < 4; q++) {
     const int64_t c = c0 + q;
-    int o = -1;
-    if (live && c < n && __ldg(graph_id + c) == pd.part) o = __ldg(ed2st + c) - pd.start;
-    own[q] = o;
-    any_own |= (o >= 0);
+    slot[q] = -1;
+    jloc[q] = -1;
+    if (live && c < n && __ldg(graph_id + c) == pd.part) {
+      jloc[q] = __ldg(ed2st + c) - pd.start;
+      const int sl = atomicAdd(&s_nown, 1);
+      if (sl < kOwnMax) {
+        own_col[sl] = jloc[q];
+        slot[q] = sl;
+      }
+      any_own = true;
+    }
+  }
+  __syncthreads();
+  const int nown = min(s_nown, kOwnMax);
+  const T *Fr = F + pd.f_off + (int64_t)(pd.b + wk.m0) * pd.ldf;
+  for (int t = threadIdx.x; t < rows * nown; t += blockDim.x) {
+    const int r = t / nown, o = t % nown;
+    Own[r][o] = __ldg(Fr + (int64_t)r * pd.ldf + own_col[o]);
   }
   __syncthreads();
   if (!live) return;
   T *Cm = D + (pd.row_base + pd.b + wk.m0) * ldD + c0;
-  const T *Fr = F + pd.f_off + (int64_t)(pd.b + wk.m0) * pd.ldf;
 #pragma unroll 2
   for (int r = 0; r < rows; r++) {
     T acc[4] = {inf, inf, inf, inf};
@@ -422,8 +445,10 @@ __global__ void __launch_bounds__(256, 2)
     }
     if (any_own) {
 #pragma unroll
-      for (int q = 0; q < 4; q++)
-        if (own[q] >= 0) acc[q] = Fr[(int64_t)r * pd.ldf + own[q]];
+      for (int q = 0; q < 4; q++) {
+        if (slot[q] >= 0) acc[q] = Own[r][slot[q]];
+        else if (jloc[q] >= 0) acc[q] = Fr[(int64_t)r * pd.ldf + jloc[q]];  // beyond kOwnMax
+      }
     }
     V v;
     v.x = acc[0]; v.y = acc[1]; v.z = acc[2]; v.w = acc[3];

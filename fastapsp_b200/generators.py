@@ -205,6 +205,8 @@ WORKLOADS = {
     "grid64": dict(make=lambda: grid_graph(64, 64, drop_frac=0.02, seed=1), K=8),
     # 114,599-vertex road-shaped graph, int weights in [1,1000], K=128
     "road114k": dict(make=lambda: road_graph(114599, seed=2), K=128),
+    # profiling-size stand-in for road114k: same part size (~830 vertices)
+    "road20k": dict(make=lambda: road_graph(20000, seed=9), K=24),
     # 512x512 grid + 1% long-range edges, int weights in [1,100], K=256
     "grid512": dict(make=lambda: grid_graph(512, 512, extra_frac=0.01, wmin=1, wmax=100,
                                             seed=3), K=256),
