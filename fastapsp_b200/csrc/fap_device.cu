@@ -128,7 +128,7 @@ template <typename T>
 cudaError_t launch_sssp(const int32_t *row_offset, const int32_t *col, const T *w, int n,
                         const int32_t *sources, const int64_t *out_rows, int num_sources, T *out,
                         int64_t ld, int64_t init_cols, const int32_t *perm_out, T *scratch,
-                        T delta, int64_t max_rounds, int *status, cudaStream_t stream,
+                        T delta, int chain, int64_t max_rounds, int *status, cudaStream_t stream,
                         int64_t *launches) {
   if (num_sources <= 0) return cudaSuccess;
   const size_t smem = sssp_smem_bytes(n);
@@ -140,7 +140,7 @@ cudaError_t launch_sssp(const int32_t *row_offset, const int32_t *col, const T *
   const int grid = perm_out ? sssp_scratch_rows(n, num_sources) : num_sources;
   kern<<<grid, kSsspThreads, smem, stream>>>(row_offset, col, w, n, sources, out_rows, num_sources,
                                              out, ld, init_cols, perm_out, scratch, delta,
-                                             max_rounds, status);
+                                             chain, max_rounds, status);
   *launches += 1;
   return cudaGetLastError();
 }
@@ -357,102 +357,151 @@ __global__ void __launch_bounds__(MPCfg<T>::THREADS)
 
 // Thin-K variant (b <= kThinK): the product is store-bound, not
 // relaxation-bound, so the kernel is shaped around the stores.  A CTA owns a
-// strip of kThinCols columns (4 per thread: one 16-byte streaming store per
-// row) and a range of up to kMinplusBM rows of one part.  The part's b
-// boundary rows of the strip stay in registers for the whole CTA; the rows'
-// A values are staged in shared memory and read as broadcasts.
+// strip of kThinCols columns (8 per thread: two 16-byte streaming stores per
+// row) and up to kMinplusBM rows of one part.  The part's b boundary rows of
+// the strip stay in registers; the rows' A values are staged in shared memory
+// and read as 16-byte broadcasts.  The relaxation loop is instantiated for
+// every exact b (a uniform switch per CTA), so no relaxation or branch is
+// spent on padding.  Own-part columns (the reference's decode) are staged in
+// shared memory once per CTA.
 constexpr int kThinK = kThinBoundary;
-constexpr int kThinCols = 4 * 256;
+constexpr int kThinThreads = 256;
+constexpr int kThinCols = 8 * kThinThreads;
+constexpr int kThinOwnMax = 64;
 
 template <typename T>
-__global__ void __launch_bounds__(256, 2)
+struct ThinShared {
+  __align__(16) T As[kMinplusBM][kThinK];
+  T Own[kMinplusBM][kThinOwnMax];
+  int32_t own_col[kThinOwnMax];
+  int nown;
+};
+
+// Columns c0 .. c0+4*G-1 of rows [0, rows) of the part: G groups of 4
+// columns (16 bytes each), B relaxations per output.
+template <typename T, int B, int G>
+__device__ __forceinline__ void thin_rows(ThinShared<T> &sh, const PartDesc &pd, int rows,
+                                          int64_t c0, const T *__restrict__ D, int64_t ldD,
+                                          T *Cm, const int (&own)[8], bool any_own, const T *Fr,
+                                          int goff) {
+  using V = typename Vec4<T>::type;
+  const T inf = Dist<T>::inf();
+  T sv[B > 0 ? B : 1][4 * G];
+#pragma unroll
+  for (int k = 0; k < B; k++)
+#pragma unroll
+    for (int g = 0; g < G; g++) {
+      const V v = __ldg(reinterpret_cast<const V *>(D + (pd.row_base + k) * ldD + c0 + 4 * g));
+      sv[k][4 * g + 0] = v.x; sv[k][4 * g + 1] = v.y; sv[k][4 * g + 2] = v.z; sv[k][4 * g + 3] = v.w;
+    }
+#pragma unroll 2
+  for (int r = 0; r < rows; r++) {
+    T acc[4 * G];
+#pragma unroll
+    for (int q = 0; q < 4 * G; q++) acc[q] = inf;
+#pragma unroll
+    for (int k4 = 0; k4 < (B + 3) / 4; k4++) {
+      const V a4 = *reinterpret_cast<const V *>(&sh.As[r][4 * k4]);
+      const T av[4] = {a4.x, a4.y, a4.z, a4.w};
+#pragma unroll
+      for (int kk = 0; kk < 4; kk++)
+        if (4 * k4 + kk < B) {
+#pragma unroll
+          for (int q = 0; q < 4 * G; q++) acc[q] = Dist<T>::relax(av[kk], sv[4 * k4 + kk][q], acc[q]);
+        }
+    }
+    if (any_own) {
+#pragma unroll
+      for (int q = 0; q < 4 * G; q++) {
+        const int o = own[goff + q];  // -1, or (part-local column << 7) | (staged slot + 1)
+        if (o >= 0) {
+          const int sl = (o & 127) - 1;
+          acc[q] = sl >= 0 ? sh.Own[r][sl] : Fr[(int64_t)r * pd.ldf + (o >> 7)];
+        }
+      }
+    }
+#pragma unroll
+    for (int g = 0; g < G; g++) {
+      V v;
+      v.x = acc[4 * g + 0]; v.y = acc[4 * g + 1]; v.z = acc[4 * g + 2]; v.w = acc[4 * g + 3];
+      __stcs(reinterpret_cast<V *>(Cm + (int64_t)r * ldD + 4 * g), v);
+    }
+  }
+}
+
+template <typename T, int B>
+__device__ __forceinline__ void thin_dispatch(ThinShared<T> &sh, const PartDesc &pd, int rows,
+                                              int64_t c0, bool two, const T *D, int64_t ldD,
+                                              T *Cm, const int (&own)[8], bool any_own,
+                                              const T *Fr) {
+  if (B <= 6) {
+    if (two) thin_rows<T, B, 2>(sh, pd, rows, c0, D, ldD, Cm, own, any_own, Fr, 0);
+    else thin_rows<T, B, 1>(sh, pd, rows, c0, D, ldD, Cm, own, any_own, Fr, 0);
+  } else {
+    // 8 columns as two passes of 4 keep the boundary strip within registers
+    thin_rows<T, B, 1>(sh, pd, rows, c0, D, ldD, Cm, own, any_own, Fr, 0);
+    if (two) thin_rows<T, B, 1>(sh, pd, rows, c0 + 4, D, ldD, Cm + 4, own, any_own, Fr, 4);
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThinThreads, 2)
     minplus_thin_kernel(const PartDesc *__restrict__ parts, const MPWork *__restrict__ work, int n,
                         const T *__restrict__ F, T *D, int64_t ldD,
                         const int32_t *__restrict__ graph_id, const int32_t *__restrict__ ed2st) {
-  using V = typename Vec4<T>::type;
-  constexpr int kOwnMax = 32;  // own-part columns of a strip staged in shared memory
-  __shared__ __align__(16) T As[kMinplusBM][kThinK];
-  __shared__ T Own[kMinplusBM][kOwnMax];
-  __shared__ int32_t own_col[kOwnMax];
-  __shared__ int s_nown;
+  __shared__ ThinShared<T> sh;
   const MPWork wk = work[blockIdx.y];
   const PartDesc pd = parts[wk.pidx];
   const int M = pd.s - pd.b, b = pd.b;
   const int rows = min(kMinplusBM, M - wk.m0);
   const T inf = Dist<T>::inf();
-  if (threadIdx.x == 0) s_nown = 0;
-  // stage A rows (F[b + m0 + r][0..b-1]) in shared memory, sentinel-padded
+  if (threadIdx.x == 0) sh.nown = 0;
   const T *A = F + pd.f_off + (int64_t)(pd.b + wk.m0) * pd.ldf;
   for (int t = threadIdx.x; t < kMinplusBM * kThinK; t += blockDim.x) {
     const int r = t / kThinK, k = t % kThinK;
-    As[r][k] = (r < rows && k < b) ? __ldg(A + (int64_t)r * pd.ldf + k) : inf;
+    sh.As[r][k] = (r < rows && k < b) ? __ldg(A + (int64_t)r * pd.ldf + k) : inf;
   }
-  const int64_t c0 = (int64_t)blockIdx.x * kThinCols + 4 * threadIdx.x;
+  const int64_t c0 = (int64_t)blockIdx.x * kThinCols + 8 * threadIdx.x;
   const bool live = c0 < ldD;
-  // the strip of the b boundary rows (S = D rows row_base .. row_base+b-1)
-  T sv[kThinK][4];
-#pragma unroll
-  for (int k = 0; k < kThinK; k++) {
-    if (live && k < b) {
-      const V v = __ldg(reinterpret_cast<const V *>(D + (pd.row_base + k) * ldD + c0));
-      sv[k][0] = v.x; sv[k][1] = v.y; sv[k][2] = v.z; sv[k][3] = v.w;
-    } else {
-      sv[k][0] = sv[k][1] = sv[k][2] = sv[k][3] = inf;
-    }
-  }
-  // Own-part columns: their values come from the closed Floyd matrix (the
-  // reference's decode).  Register them and stage F[b+m0+r][j] for every row
-  // so that the row loop never waits on a gather.
-  int slot[4];
-  int jloc[4];
+  const bool two = c0 + 4 < ldD;  // ldD is a multiple of 4: 4 or 8 live columns
+  int own[8];
   bool any_own = false;
   __syncthreads();
 #pragma unroll
-  for (int q = 0; q < 4; q++) {
+  for (int q = 0; q < 8; q++) {
     const int64_t c = c0 + q;
-    slot[q] = -1;
-    jloc[q] = -1;
+    own[q] = -1;
     if (live && c < n && __ldg(graph_id + c) == pd.part) {
-      jloc[q] = __ldg(ed2st + c) - pd.start;
-      const int sl = atomicAdd(&s_nown, 1);
-      if (sl < kOwnMax) {
-        own_col[sl] = jloc[q];
-        slot[q] = sl;
+      const int j = __ldg(ed2st + c) - pd.start;
+      const int sl = atomicAdd(&sh.nown, 1);
+      int staged = 0;
+      if (sl < kThinOwnMax) {
+        sh.own_col[sl] = j;
+        staged = sl + 1;
       }
+      own[q] = (j << 7) | staged;
       any_own = true;
     }
   }
   __syncthreads();
-  const int nown = min(s_nown, kOwnMax);
+  const int nown = min(sh.nown, kThinOwnMax);
   const T *Fr = F + pd.f_off + (int64_t)(pd.b + wk.m0) * pd.ldf;
   for (int t = threadIdx.x; t < rows * nown; t += blockDim.x) {
     const int r = t / nown, o = t % nown;
-    Own[r][o] = __ldg(Fr + (int64_t)r * pd.ldf + own_col[o]);
+    sh.Own[r][o] = __ldg(Fr + (int64_t)r * pd.ldf + sh.own_col[o]);
   }
   __syncthreads();
   if (!live) return;
   T *Cm = D + (pd.row_base + pd.b + wk.m0) * ldD + c0;
-#pragma unroll 2
-  for (int r = 0; r < rows; r++) {
-    T acc[4] = {inf, inf, inf, inf};
-#pragma unroll
-    for (int k = 0; k < kThinK; k++) {
-      if (k < b) {
-        const T a = As[r][k];
-#pragma unroll
-        for (int q = 0; q < 4; q++) acc[q] = Dist<T>::relax(a, sv[k][q], acc[q]);
-      }
-    }
-    if (any_own) {
-#pragma unroll
-      for (int q = 0; q < 4; q++) {
-        if (slot[q] >= 0) acc[q] = Own[r][slot[q]];
-        else if (jloc[q] >= 0) acc[q] = Fr[(int64_t)r * pd.ldf + jloc[q]];  // beyond kOwnMax
-      }
-    }
-    V v;
-    v.x = acc[0]; v.y = acc[1]; v.z = acc[2]; v.w = acc[3];
-    __stcs(reinterpret_cast<V *>(Cm + (int64_t)r * ldD), v);
+  switch (b) {
+#define FAPB_THIN_CASE(NB) \
+  case NB: thin_dispatch<T, NB>(sh, pd, rows, c0, two, D, ldD, Cm, own, any_own, Fr); break;
+    FAPB_THIN_CASE(0) FAPB_THIN_CASE(1) FAPB_THIN_CASE(2) FAPB_THIN_CASE(3) FAPB_THIN_CASE(4)
+    FAPB_THIN_CASE(5) FAPB_THIN_CASE(6) FAPB_THIN_CASE(7) FAPB_THIN_CASE(8) FAPB_THIN_CASE(9)
+    FAPB_THIN_CASE(10) FAPB_THIN_CASE(11) FAPB_THIN_CASE(12) FAPB_THIN_CASE(13)
+    FAPB_THIN_CASE(14) FAPB_THIN_CASE(15) FAPB_THIN_CASE(16)
+#undef FAPB_THIN_CASE
+    default: break;
   }
 }
 
@@ -476,7 +525,7 @@ cudaError_t launch_minplus_thin(const PartDesc *parts, const MPWork *work, int n
                                 const int32_t *ed2st, cudaStream_t stream, int64_t *launches) {
   if (nwork <= 0) return cudaSuccess;
   dim3 grid((unsigned)ceil_div(ldD, kThinCols), (unsigned)nwork);
-  minplus_thin_kernel<T><<<grid, 256, 0, stream>>>(parts, work, n, F, D, ldD, graph_id, ed2st);
+  minplus_thin_kernel<T><<<grid, kThinThreads, 0, stream>>>(parts, work, n, F, D, ldD, graph_id, ed2st);
   *launches += 1;
   return cudaGetLastError();
 }
@@ -623,7 +672,7 @@ cudaError_t launch_relax_peak(T *sink, int blocks, int iters, cudaStream_t strea
 #define FAPB_INSTANTIATE(T)                                                                       \
   template cudaError_t launch_sssp<T>(const int32_t *, const int32_t *, const T *, int,           \
                                       const int32_t *, const int64_t *, int, T *, int64_t,        \
-                                      int64_t, const int32_t *, T *, T, int64_t, int *,           \
+                                      int64_t, const int32_t *, T *, T, int, int64_t, int *,      \
                                       cudaStream_t, int64_t *);                                   \
   template cudaError_t launch_gather<T>(const PartDesc *, int, int, const int32_t *,              \
                                         const int32_t *, const T *, const int32_t *,              \

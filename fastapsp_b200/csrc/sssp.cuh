@@ -19,6 +19,10 @@
 //     atomics of a 4-edge group in flight at once; vertices with more than
 //     kHeavyDeg edges are expanded by a whole warp (lane-strided, coalesced
 //     column/weight reads).
+//   - Chains: a thread that improves a near neighbour expands it at once
+//     (up to `chain` hops per round) instead of leaving it for the next
+//     round, so a hop along a path costs one load + atomic latency rather
+//     than a whole round.
 //   - Order: near/far (delta stepping).  A frontier vertex whose distance is
 //     not below the threshold stays in the bitmap; when no near vertex is
 //     left, the threshold moves to (smallest far distance + delta).
@@ -86,6 +90,47 @@ __device__ __forceinline__ int block_excl_scan(int x, int *warp_tmp, int *total)
   return warp_tmp[wid] + inc - x;
 }
 
+// Relaxes edges [e0, e1) of a light vertex at distance du.  One improved
+// neighbour inside the current bucket may be handed back in *next / *dnext
+// (chain-following: the caller expands it at once instead of a round later);
+// every other improved neighbour gets its frontier bit.  Returns whether a bit
+// was set.
+template <typename T>
+__device__ __forceinline__ bool relax_edges_chain(const int32_t *__restrict__ col,
+                                                  const T *__restrict__ w, int e0, int e1, T du,
+                                                  T *dist, uint32_t *nb, T thresh, bool may_chain,
+                                                  int *next, T *dnext) {
+  bool any = false;
+  *next = -1;
+  for (int e = e0; e < e1; e += 4) {
+    int v[4];
+    T nd[4], cur[4], old[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int ek = e + k;
+      v[k] = ek < e1 ? __ldg(col + ek) : -1;
+      nd[k] = ek < e1 ? du + __ldg(w + ek) : du;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) cur[k] = v[k] >= 0 ? ld_relaxed(dist + v[k]) : du;
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+      old[k] = (v[k] >= 0 && nd[k] < cur[k]) ? Dist<T>::atomic_min(dist + v[k], nd[k]) : nd[k];
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+      if (nd[k] < old[k]) {
+        if (may_chain && *next < 0 && nd[k] < thresh) {
+          *next = v[k];
+          *dnext = nd[k];
+        } else {
+          atomicOr(nb + (v[k] >> 5), 1u << (v[k] & 31));
+          any = true;
+        }
+      }
+  }
+  return any;
+}
+
 // Relaxes edges [e0, e1) of a vertex at distance du; sets the frontier bit
 // of every improved neighbour.  Returns whether anything improved.
 template <typename T>
@@ -127,7 +172,7 @@ __global__ void __launch_bounds__(kSsspThreads)
                          const T *__restrict__ w, int n, const int32_t *__restrict__ sources,
                          const int64_t *__restrict__ out_rows, int num_sources, T *out, int64_t ld,
                          int64_t init_cols, const int32_t *__restrict__ perm_out, T *scratch,
-                         T delta, int64_t max_rounds, int *status) {
+                         T delta, int chain, int64_t max_rounds, int *status) {
   extern __shared__ uint32_t sm_bits[];
   __shared__ int32_t s_minfar[3];
   __shared__ int s_warp[kSsspThreads / 32];
@@ -202,15 +247,25 @@ __global__ void __launch_bounds__(kSsspThreads)
             far = 1;
             continue;
           }
-          const int e0 = __ldg(row_offset + u), e1 = __ldg(row_offset + u + 1);
-          if (e1 - e0 > kHeavyDeg) {
-            const int h = atomicAdd(&s_nheavy, 1);
-            if (h < kHeavyList) {
-              heavy[h] = u;
-              continue;
+          // Expand u, then follow improved near neighbours in this thread.
+          int x = u;
+          T dx = du;
+          for (int hop = 0;; hop++) {
+            const int e0 = __ldg(row_offset + x), e1 = __ldg(row_offset + x + 1);
+            if (e1 - e0 > kHeavyDeg) {
+              const int h = atomicAdd(&s_nheavy, 1);
+              if (h < kHeavyList) {
+                heavy[h] = x;
+                break;
+              }
             }
+            int nx;
+            T dn;
+            any |= relax_edges_chain<T>(col, w, e0, e1, dx, dist, nb, thresh, hop < chain, &nx, &dn);
+            if (nx < 0) break;
+            x = nx;
+            dx = dn;
           }
-          any |= relax_edges<T>(col, w, e0, e1, 1, du, dist, nb);
         }
         __syncthreads();
         // Heavy vertices: one warp each, lanes stride over the edges.

@@ -140,7 +140,9 @@ FAP_API int fap_graph_sssp_rows(fap_dgraph *g, const int32_t *sources, int32_t c
  * after which a source gives up and the solve reports
  * FAP_ERR_NOT_CONVERGED; <= 0 restores the default 8n + 1024);
  * "floyd_per_cta" (non-zero: the batched Floyd closes each part's matrix
- * with one CTA instead of per-tile launches across all parts). */
+ * with one CTA instead of per-tile launches across all parts);
+ * "sssp_chain" (hops a thread may follow within one SSSP round; 0 turns
+ * chain-following off; default 32). */
 FAP_API int fap_graph_set_param(fap_dgraph *g, const char *key, double value);
 
 /* Device time (ms) of the stages of the last fap_solve, measured with events
