@@ -142,7 +142,7 @@ struct fap_dgraph {
   double sssp_delta = -1.0;  // <0: automatic
   int64_t sssp_max_rounds = -1;  // <0: 8n + 1024
   bool floyd_per_cta = false;     // batched Floyd: one CTA per part instead of per-tile launches
-  int sssp_chain = 32;            // SSSP chain-following budget (hops per thread per round)
+  int sssp_chain = 0;             // SSSP chain-following budget (hops per thread per round)
   // last solve
   int last_mode = -1;
   float timing[5] = {-1, -1, -1, -1, -1};
@@ -911,7 +911,7 @@ extern "C" int fap_graph_set_param(fap_dgraph *G, const char *key, double value)
     return FAP_OK;
   }
   if (std::strcmp(key, "sssp_chain") == 0) {
-    G->sssp_chain = value >= 0 ? (int)value : 32;
+    G->sssp_chain = value >= 0 ? (int)value : 0;
     return FAP_OK;
   }
   if (std::strcmp(key, "floyd_per_cta") == 0) {
