@@ -133,8 +133,10 @@ struct fap_dgraph {
   std::vector<int32_t> src;
   std::vector<int64_t> srcrows;
   std::vector<int32_t> part_src_off;                 // per batch index, size nparts+1
-  std::vector<int32_t> part_work_begin, part_work_end;  // per batch index, into work
-  int32_t n_thin = 0;  // work[0, n_thin) is thin-boundary work, the rest thick
+  std::vector<int32_t> part_work_begin, part_work_end;  // per batch index, into work (thick parts)
+  std::vector<int32_t> thin;      // batch indices of thin-boundary parts
+  std::vector<int32_t> thin_pos;  // per batch index: position in thin, or -1
+  DevBuf d_thin;
   std::vector<int32_t> last_ids;
   int64_t f_elems = 0;
   int max_ldf = 0, max_b = 0, max_s = 0;
@@ -322,7 +324,7 @@ extern "C" int fap_graph_destroy(fap_dgraph *G) {
   {
     DeviceGuard g(c->device);
     cudaStreamSynchronize(c->stream);
-    for (DevBuf *b : {&G->ro, &G->col, &G->w, &G->ro_s, &G->col_s, &G->w_s, &G->sssp_scratch,
+    for (DevBuf *b : {&G->ro, &G->col, &G->w, &G->ro_s, &G->col_s, &G->w_s, &G->sssp_scratch, &G->d_thin,
                       &G->d_gid, &G->d_st2ed, &G->d_ed2st, &G->D, &G->F, &G->d_parts, &G->d_work,
                       &G->d_src, &G->d_srcrows, &G->d_status, &G->d_checks, &G->staging})
       b->release();
@@ -445,8 +447,8 @@ int prepare_batch(fap_dgraph *G, const std::vector<int32_t> &ids) {
   G->part_src_off.assign(1, 0);
   G->part_work_begin.clear();
   G->part_work_end.clear();
-  std::vector<MPWork> thick;
-  std::vector<char> is_thin;
+  G->thin.clear();
+  G->thin_pos.clear();
   int64_t foff = 0;
   G->max_ldf = 0;
   G->max_b = 0;
@@ -471,25 +473,21 @@ int prepare_batch(fap_dgraph *G, const std::vector<int32_t> &ids) {
       G->srcrows.push_back(d.row_base + k);
     }
     G->part_src_off.push_back((int32_t)G->src.size());
-    const bool thin = d.b <= kThinBoundary;
-    std::vector<MPWork> &dst = thin ? G->work : thick;
-    G->part_work_begin.push_back((int32_t)dst.size());
-    for (int32_t m0 = 0; m0 < d.s - d.b; m0 += kMinplusBM) dst.push_back(MPWork{(int32_t)i, m0});
-    G->part_work_end.push_back((int32_t)dst.size());
-    is_thin.push_back(thin);
-  }
-  // work = [thin parts' rows][thick parts' rows]
-  G->n_thin = (int32_t)G->work.size();
-  for (size_t i = 0; i < is_thin.size(); i++)
-    if (!is_thin[i]) {
-      G->part_work_begin[i] += G->n_thin;
-      G->part_work_end[i] += G->n_thin;
+    G->part_work_begin.push_back((int32_t)G->work.size());
+    if (d.b <= kThinBoundary) {
+      G->thin_pos.push_back((int32_t)G->thin.size());
+      G->thin.push_back((int32_t)i);
+    } else {
+      G->thin_pos.push_back(-1);
+      for (int32_t m0 = 0; m0 < d.s - d.b; m0 += kMinplusBM) G->work.push_back(MPWork{(int32_t)i, m0});
     }
-  G->work.insert(G->work.end(), thick.begin(), thick.end());
+    G->part_work_end.push_back((int32_t)G->work.size());
+  }
   G->f_elems = foff;
   FAP_TRY(G->F.ensure((size_t)std::max<int64_t>(foff, 1) * 4));
   FAP_TRY(G->d_parts.ensure(std::max<size_t>(G->parts.size(), 1) * sizeof(PartDesc)));
   FAP_TRY(G->d_work.ensure(std::max<size_t>(G->work.size(), 1) * sizeof(MPWork)));
+  FAP_TRY(G->d_thin.ensure(std::max<size_t>(G->thin.size(), 1) * 4));
   FAP_TRY(G->d_src.ensure(std::max<size_t>(G->src.size(), 1) * 4));
   FAP_TRY(G->d_srcrows.ensure(std::max<size_t>(G->srcrows.size(), 1) * 8));
   FAP_TRY(G->sssp_scratch.ensure(
@@ -499,6 +497,8 @@ int prepare_batch(fap_dgraph *G, const std::vector<int32_t> &ids) {
   FAP_CK(cudaMemcpy(G->d_parts.p, G->parts.data(), G->parts.size() * sizeof(PartDesc), cudaMemcpyHostToDevice));
   if (!G->work.empty())
     FAP_CK(cudaMemcpy(G->d_work.p, G->work.data(), G->work.size() * sizeof(MPWork), cudaMemcpyHostToDevice));
+  if (!G->thin.empty())
+    FAP_CK(cudaMemcpy(G->d_thin.p, G->thin.data(), G->thin.size() * 4, cudaMemcpyHostToDevice));
   if (!G->src.empty()) {
     FAP_CK(cudaMemcpy(G->d_src.p, G->src.data(), G->src.size() * 4, cudaMemcpyHostToDevice));
     FAP_CK(cudaMemcpy(G->d_srcrows.p, G->srcrows.data(), G->srcrows.size() * 8, cudaMemcpyHostToDevice));
@@ -558,9 +558,10 @@ int run_solve(fap_dgraph *G, int mode) {
       FAP_CK(launch_bdy_scatter<T>(dp, np, F, D, G->ldD, st2ed, G->max_b, G->max_s, st, &L));
     }
     FAP_CK(cudaEventRecord(c->ev[3], st));
-    FAP_CK(launch_minplus_thin<T>(dp, dw, G->n_thin, G->n, F, D, G->ldD, gid, ed2st, st, &L));
-    FAP_CK(launch_minplus_parts<T>(dp, dw + G->n_thin, (int)G->work.size() - G->n_thin, G->n, F, D,
-                                   G->ldD, gid, ed2st, st, &L));
+    FAP_CK(launch_minplus_thin<T>(dp, G->d_thin.as<int32_t>(), (int)G->thin.size(), G->n, F, D,
+                                  G->ldD, gid, ed2st, st, &L));
+    FAP_CK(launch_minplus_parts<T>(dp, dw, (int)G->work.size(), G->n, F, D, G->ldD, gid, ed2st, st,
+                                   &L));
     FAP_CK(cudaEventRecord(c->ev[4], st));
   } else {
     FAP_CK(cudaEventRecord(c->ev[0], st));
@@ -573,8 +574,9 @@ int run_solve(fap_dgraph *G, int mode) {
       FAP_CK(launch_gather<T>(dp + i, 1, d.ldf, ro, col, w, gid, st2ed, ed2st, D, G->ldD, F, st, &L));
       FAP_CK(launch_floyd_matrix<T>(F + d.f_off, d.ldf, d.ldf / kFloydTile, st, &L));
       FAP_CK(launch_bdy_scatter<T>(dp + i, 1, F, D, G->ldD, st2ed, d.b, d.s, st, &L));
-      if (d.b <= kThinBoundary)
-        FAP_CK(launch_minplus_thin<T>(dp, dw + w0, w1 - w0, G->n, F, D, G->ldD, gid, ed2st, st, &L));
+      if (G->thin_pos[i] >= 0)
+        FAP_CK(launch_minplus_thin<T>(dp, G->d_thin.as<int32_t>() + G->thin_pos[i], 1, G->n, F, D,
+                                      G->ldD, gid, ed2st, st, &L));
       else
         FAP_CK(launch_minplus_parts<T>(dp, dw + w0, w1 - w0, G->n, F, D, G->ldD, gid, ed2st, st, &L));
     }

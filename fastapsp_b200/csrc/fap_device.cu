@@ -357,16 +357,19 @@ __global__ void __launch_bounds__(MPCfg<T>::THREADS)
 
 // Thin-K variant (b <= kThinK): the product is store-bound, not
 // relaxation-bound, so the kernel is shaped around the stores.  A CTA owns a
-// strip of kThinCols columns (8 per thread: two 16-byte streaming stores per
-// row) and up to kMinplusBM rows of one part.  The part's b boundary rows of
-// the strip stay in registers; the rows' A values are staged in shared memory
-// and read as 16-byte broadcasts.  The relaxation loop is instantiated for
-// every exact b (a uniform switch per CTA), so no relaxation or branch is
-// spent on padding.  Own-part columns (the reference's decode) are staged in
-// shared memory once per CTA.
+// strip of kThinCols columns of one part and walks all of the part's inner
+// rows.  Each thread owns two groups of 4 columns, kThinCols/2 apart, so
+// that every warp-wide 16-byte store covers 512 contiguous bytes (whole
+// sectors; a half-written sector would be read back from DRAM).  The part's
+// b boundary rows of the strip stay in registers for the whole CTA; each
+// block of kMinplusBM rows stages its A values and its own-part (decode)
+// values in shared memory.  The relaxation loop is instantiated for every
+// exact b (a uniform switch per CTA), so no relaxation or branch is spent on
+// padding.
 constexpr int kThinK = kThinBoundary;
 constexpr int kThinThreads = 256;
 constexpr int kThinCols = 8 * kThinThreads;
+constexpr int kThinHalf = kThinCols / 2;
 constexpr int kThinOwnMax = 64;
 
 template <typename T>
@@ -377,13 +380,13 @@ struct ThinShared {
   int nown;
 };
 
-// Columns c0 .. c0+4*G-1 of rows [0, rows) of the part: G groups of 4
-// columns (16 bytes each), B relaxations per output.
+// Rows [0, M) of the part's inner block for the thread's columns
+// c0 + {0..3} (g = 0) and c0 + kThinHalf + {0..3} (g = 1); B relaxations per
+// output.  G = 1 handles only group g0.
 template <typename T, int B, int G>
-__device__ __forceinline__ void thin_rows(ThinShared<T> &sh, const PartDesc &pd, int rows,
-                                          int64_t c0, const T *__restrict__ D, int64_t ldD,
-                                          T *Cm, const int (&own)[8], bool any_own, const T *Fr,
-                                          int goff) {
+__device__ __forceinline__ void thin_rows(ThinShared<T> &sh, const PartDesc &pd, int M, int64_t c0,
+                                          const T *__restrict__ F, T *D, int64_t ldD, const int (&own)[8], bool any_own,
+                                          int g0, const bool (&live)[2]) {
   using V = typename Vec4<T>::type;
   const T inf = Dist<T>::inf();
   T sv[B > 0 ? B : 1][4 * G];
@@ -391,87 +394,105 @@ __device__ __forceinline__ void thin_rows(ThinShared<T> &sh, const PartDesc &pd,
   for (int k = 0; k < B; k++)
 #pragma unroll
     for (int g = 0; g < G; g++) {
-      const V v = __ldg(reinterpret_cast<const V *>(D + (pd.row_base + k) * ldD + c0 + 4 * g));
+      const int gg = g0 + g;
+      V v;
+      if (live[gg]) v = __ldg(reinterpret_cast<const V *>(D + (pd.row_base + k) * ldD + c0 + gg * kThinHalf));
+      else v.x = v.y = v.z = v.w = inf;
       sv[k][4 * g + 0] = v.x; sv[k][4 * g + 1] = v.y; sv[k][4 * g + 2] = v.z; sv[k][4 * g + 3] = v.w;
     }
-#pragma unroll 2
-  for (int r = 0; r < rows; r++) {
-    T acc[4 * G];
-#pragma unroll
-    for (int q = 0; q < 4 * G; q++) acc[q] = inf;
-#pragma unroll
-    for (int k4 = 0; k4 < (B + 3) / 4; k4++) {
-      const V a4 = *reinterpret_cast<const V *>(&sh.As[r][4 * k4]);
-      const T av[4] = {a4.x, a4.y, a4.z, a4.w};
-#pragma unroll
-      for (int kk = 0; kk < 4; kk++)
-        if (4 * k4 + kk < B) {
-#pragma unroll
-          for (int q = 0; q < 4 * G; q++) acc[q] = Dist<T>::relax(av[kk], sv[4 * k4 + kk][q], acc[q]);
-        }
+  const T *Fp = F + pd.f_off;
+  for (int m0 = 0; m0 < M; m0 += kMinplusBM) {
+    const int rows = min(kMinplusBM, M - m0);
+    const T *Fr = Fp + (int64_t)(pd.b + m0) * pd.ldf;
+    // stage this block's A values and own-part values
+    __syncthreads();
+    for (int t = threadIdx.x; t < kMinplusBM * kThinK; t += blockDim.x) {
+      const int r = t / kThinK, k = t % kThinK;
+      sh.As[r][k] = (r < rows && k < B) ? __ldg(Fr + (int64_t)r * pd.ldf + k) : inf;
     }
-    if (any_own) {
+    const int nown = min(sh.nown, kThinOwnMax);
+    for (int t = threadIdx.x; t < rows * nown; t += blockDim.x) {
+      const int r = t / nown, o = t % nown;
+      sh.Own[r][o] = __ldg(Fr + (int64_t)r * pd.ldf + sh.own_col[o]);
+    }
+    __syncthreads();
+    T *Cm = D + (pd.row_base + pd.b + m0) * ldD + c0;
+#pragma unroll 2
+    for (int r = 0; r < rows; r++) {
+      T acc[4 * G];
 #pragma unroll
-      for (int q = 0; q < 4 * G; q++) {
-        const int o = own[goff + q];  // -1, or (part-local column << 7) | (staged slot + 1)
-        if (o >= 0) {
-          const int sl = (o & 127) - 1;
-          acc[q] = sl >= 0 ? sh.Own[r][sl] : Fr[(int64_t)r * pd.ldf + (o >> 7)];
+      for (int q = 0; q < 4 * G; q++) acc[q] = inf;
+#pragma unroll
+      for (int k4 = 0; k4 < (B + 3) / 4; k4++) {
+        const V a4 = *reinterpret_cast<const V *>(&sh.As[r][4 * k4]);
+        const T av[4] = {a4.x, a4.y, a4.z, a4.w};
+#pragma unroll
+        for (int kk = 0; kk < 4; kk++)
+          if (4 * k4 + kk < B) {
+#pragma unroll
+            for (int q = 0; q < 4 * G; q++)
+              acc[q] = Dist<T>::relax(av[kk], sv[4 * k4 + kk][q], acc[q]);
+          }
+      }
+      if (any_own) {
+#pragma unroll
+        for (int q = 0; q < 4 * G; q++) {
+          const int o = own[4 * g0 + q];  // -1, or (part-local column << 7) | (slot + 1)
+          if (o >= 0) {
+            const int sl = (o & 127) - 1;
+            acc[q] = sl >= 0 ? sh.Own[r][sl] : Fr[(int64_t)r * pd.ldf + (o >> 7)];
+          }
         }
       }
-    }
 #pragma unroll
-    for (int g = 0; g < G; g++) {
-      V v;
-      v.x = acc[4 * g + 0]; v.y = acc[4 * g + 1]; v.z = acc[4 * g + 2]; v.w = acc[4 * g + 3];
-      __stcs(reinterpret_cast<V *>(Cm + (int64_t)r * ldD + 4 * g), v);
+      for (int g = 0; g < G; g++) {
+        const int gg = g0 + g;
+        if (live[gg]) {
+          V v;
+          v.x = acc[4 * g + 0]; v.y = acc[4 * g + 1]; v.z = acc[4 * g + 2]; v.w = acc[4 * g + 3];
+          __stcs(reinterpret_cast<V *>(Cm + (int64_t)r * ldD + gg * kThinHalf), v);
+        }
+      }
     }
   }
 }
 
 template <typename T, int B>
-__device__ __forceinline__ void thin_dispatch(ThinShared<T> &sh, const PartDesc &pd, int rows,
-                                              int64_t c0, bool two, const T *D, int64_t ldD,
-                                              T *Cm, const int (&own)[8], bool any_own,
-                                              const T *Fr) {
+__device__ __forceinline__ void thin_dispatch(ThinShared<T> &sh, const PartDesc &pd, int M,
+                                              int64_t c0, const T *F, T *D, int64_t ldD,
+                                              const int (&own)[8], bool any_own,
+                                              const bool (&live)[2]) {
   if (B <= 6) {
-    if (two) thin_rows<T, B, 2>(sh, pd, rows, c0, D, ldD, Cm, own, any_own, Fr, 0);
-    else thin_rows<T, B, 1>(sh, pd, rows, c0, D, ldD, Cm, own, any_own, Fr, 0);
+    thin_rows<T, B, 2>(sh, pd, M, c0, F, D, ldD, own, any_own, 0, live);
   } else {
-    // 8 columns as two passes of 4 keep the boundary strip within registers
-    thin_rows<T, B, 1>(sh, pd, rows, c0, D, ldD, Cm, own, any_own, Fr, 0);
-    if (two) thin_rows<T, B, 1>(sh, pd, rows, c0 + 4, D, ldD, Cm + 4, own, any_own, Fr, 4);
+    // the two column groups in two passes keep the boundary strip in registers
+    thin_rows<T, B, 1>(sh, pd, M, c0, F, D, ldD, own, any_own, 0, live);
+    thin_rows<T, B, 1>(sh, pd, M, c0, F, D, ldD, own, any_own, 1, live);
   }
 }
 
+// grid (ceil(ldD / kThinCols), number of thin parts); blockIdx.y indexes
+// thin_parts (batch indices).
 template <typename T>
 __global__ void __launch_bounds__(kThinThreads, 2)
-    minplus_thin_kernel(const PartDesc *__restrict__ parts, const MPWork *__restrict__ work, int n,
-                        const T *__restrict__ F, T *D, int64_t ldD,
+    minplus_thin_kernel(const PartDesc *__restrict__ parts, const int32_t *__restrict__ thin_parts,
+                        int n, const T *__restrict__ F, T *D, int64_t ldD,
                         const int32_t *__restrict__ graph_id, const int32_t *__restrict__ ed2st) {
   __shared__ ThinShared<T> sh;
-  const MPWork wk = work[blockIdx.y];
-  const PartDesc pd = parts[wk.pidx];
-  const int M = pd.s - pd.b, b = pd.b;
-  const int rows = min(kMinplusBM, M - wk.m0);
-  const T inf = Dist<T>::inf();
+  const PartDesc pd = parts[thin_parts[blockIdx.y]];
+  const int M = pd.s - pd.b;
+  if (M <= 0) return;
   if (threadIdx.x == 0) sh.nown = 0;
-  const T *A = F + pd.f_off + (int64_t)(pd.b + wk.m0) * pd.ldf;
-  for (int t = threadIdx.x; t < kMinplusBM * kThinK; t += blockDim.x) {
-    const int r = t / kThinK, k = t % kThinK;
-    sh.As[r][k] = (r < rows && k < b) ? __ldg(A + (int64_t)r * pd.ldf + k) : inf;
-  }
-  const int64_t c0 = (int64_t)blockIdx.x * kThinCols + 8 * threadIdx.x;
-  const bool live = c0 < ldD;
-  const bool two = c0 + 4 < ldD;  // ldD is a multiple of 4: 4 or 8 live columns
+  const int64_t c0 = (int64_t)blockIdx.x * kThinCols + 4 * threadIdx.x;
+  const bool live[2] = {c0 < ldD, c0 + kThinHalf < ldD};  // ldD is a multiple of 4
   int own[8];
   bool any_own = false;
   __syncthreads();
 #pragma unroll
   for (int q = 0; q < 8; q++) {
-    const int64_t c = c0 + q;
+    const int64_t c = c0 + (q >> 2) * kThinHalf + (q & 3);
     own[q] = -1;
-    if (live && c < n && __ldg(graph_id + c) == pd.part) {
+    if (live[q >> 2] && c < n && __ldg(graph_id + c) == pd.part) {
       const int j = __ldg(ed2st + c) - pd.start;
       const int sl = atomicAdd(&sh.nown, 1);
       int staged = 0;
@@ -483,19 +504,9 @@ __global__ void __launch_bounds__(kThinThreads, 2)
       any_own = true;
     }
   }
-  __syncthreads();
-  const int nown = min(sh.nown, kThinOwnMax);
-  const T *Fr = F + pd.f_off + (int64_t)(pd.b + wk.m0) * pd.ldf;
-  for (int t = threadIdx.x; t < rows * nown; t += blockDim.x) {
-    const int r = t / nown, o = t % nown;
-    sh.Own[r][o] = __ldg(Fr + (int64_t)r * pd.ldf + sh.own_col[o]);
-  }
-  __syncthreads();
-  if (!live) return;
-  T *Cm = D + (pd.row_base + pd.b + wk.m0) * ldD + c0;
-  switch (b) {
+  switch (pd.b) {
 #define FAPB_THIN_CASE(NB) \
-  case NB: thin_dispatch<T, NB>(sh, pd, rows, c0, two, D, ldD, Cm, own, any_own, Fr); break;
+  case NB: thin_dispatch<T, NB>(sh, pd, M, c0, F, D, ldD, own, any_own, live); break;
     FAPB_THIN_CASE(0) FAPB_THIN_CASE(1) FAPB_THIN_CASE(2) FAPB_THIN_CASE(3) FAPB_THIN_CASE(4)
     FAPB_THIN_CASE(5) FAPB_THIN_CASE(6) FAPB_THIN_CASE(7) FAPB_THIN_CASE(8) FAPB_THIN_CASE(9)
     FAPB_THIN_CASE(10) FAPB_THIN_CASE(11) FAPB_THIN_CASE(12) FAPB_THIN_CASE(13)
@@ -520,12 +531,13 @@ cudaError_t launch_minplus_parts(const PartDesc *parts, const MPWork *work, int 
 }
 
 template <typename T>
-cudaError_t launch_minplus_thin(const PartDesc *parts, const MPWork *work, int nwork, int n,
+cudaError_t launch_minplus_thin(const PartDesc *parts, const int32_t *thin_parts, int nthin, int n,
                                 const T *F, T *D, int64_t ldD, const int32_t *graph_id,
                                 const int32_t *ed2st, cudaStream_t stream, int64_t *launches) {
-  if (nwork <= 0) return cudaSuccess;
-  dim3 grid((unsigned)ceil_div(ldD, kThinCols), (unsigned)nwork);
-  minplus_thin_kernel<T><<<grid, kThinThreads, 0, stream>>>(parts, work, n, F, D, ldD, graph_id, ed2st);
+  if (nthin <= 0) return cudaSuccess;
+  dim3 grid((unsigned)ceil_div(ldD, kThinCols), (unsigned)nthin);
+  minplus_thin_kernel<T><<<grid, kThinThreads, 0, stream>>>(parts, thin_parts, n, F, D, ldD,
+                                                            graph_id, ed2st);
   *launches += 1;
   return cudaGetLastError();
 }
@@ -688,7 +700,7 @@ cudaError_t launch_relax_peak(T *sink, int blocks, int iters, cudaStream_t strea
   template cudaError_t launch_minplus_parts<T>(const PartDesc *, const MPWork *, int, int,        \
                                                const T *, T *, int64_t, const int32_t *,          \
                                                const int32_t *, cudaStream_t, int64_t *);         \
-  template cudaError_t launch_minplus_thin<T>(const PartDesc *, const MPWork *, int, int,         \
+  template cudaError_t launch_minplus_thin<T>(const PartDesc *, const int32_t *, int, int,        \
                                               const T *, T *, int64_t, const int32_t *,           \
                                               const int32_t *, cudaStream_t, int64_t *);          \
   template cudaError_t launch_minplus_generic<T>(int, int, int, const T *, int64_t, const T *,    \

@@ -85,10 +85,10 @@ cudaError_t launch_minplus_parts(const PartDesc *parts, const MPWork *work, int 
                                  const int32_t *ed2st, cudaStream_t stream, int64_t *launches);
 
 // Same for parts with at most kThinBoundary boundary vertices (store-bound
-// shape).  Work rows must belong to such parts.
+// shape): thin_parts[0..nthin) are batch indices of such parts.
 constexpr int kThinBoundary = 16;
 template <typename T>
-cudaError_t launch_minplus_thin(const PartDesc *parts, const MPWork *work, int nwork, int n,
+cudaError_t launch_minplus_thin(const PartDesc *parts, const int32_t *thin_parts, int nthin, int n,
                                 const T *F, T *D, int64_t ldD, const int32_t *graph_id,
                                 const int32_t *ed2st, cudaStream_t stream, int64_t *launches);
 
