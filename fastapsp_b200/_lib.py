@@ -30,6 +30,7 @@ FAP_DTYPE_I32 = 0
 FAP_DTYPE_F32 = 1
 FAP_MODE_PLAIN = 0
 FAP_MODE_BATCHED = 1
+FAP_NOALLOC_FLOYD_MAX = 1024
 FAP_INF_I32 = 100000000
 FAP_INF_F32 = 1e8
 
@@ -84,6 +85,8 @@ _SIGS = {
     "fap_op_floyd": (INT, [P, INT, I32, P, I64]),
     "fap_op_minplus": (INT, [P, INT, I32, I32, I32, P, I64, P, I64, P, I64]),
     "fap_measure_relax_peak": (INT, [P, INT, ctypes.POINTER(DBL)]),
+    "fap_floyd_noalloc": (INT, [INT, I32, P, I64, P]),
+    "fap_floyd_noalloc_last_error": (ctypes.c_char_p, []),
     "fap_legacy_last_status": (INT, []),
     "fap_host_last_error": (ctypes.c_char_p, []),
     "fap_host_from_mtx": (INT, [ctypes.c_char_p, INT, INT, INT, PP]),

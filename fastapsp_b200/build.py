@@ -33,7 +33,7 @@ METIS_A = os.path.join(CUDA_LIB, "libmetis_static.a")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fvisibility=hidden",
           "-I" + INCLUDE, "-I" + CSRC]
-SOURCES = ["fap_device.cu", "fap_capi.cu", "fap_legacy.cu", "fap_host.cpp"]
+SOURCES = ["fap_device.cu", "fap_capi.cu", "fap_legacy.cu", "fap_noalloc.cu", "fap_host.cpp"]
 HEADERS = ["fap_common.cuh", "minplus_tile.cuh", "floyd.cuh", "sssp.cuh", "fap_internal.h"]
 
 

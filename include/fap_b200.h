@@ -172,6 +172,31 @@ FAP_API int fap_op_minplus(fap_ctx *ctx, int dtype, int32_t M, int32_t N, int32_
                    const void *A, int64_t lda, const void *B, int64_t ldb, void *C,
                    int64_t ldc);
 
+/* ---- allocation-free closure (no counterpart in the reference) ----
+ * For callers that may not allocate device memory when they need a closure:
+ * a host framework that owns the GPU's memory through its own pool (a
+ * database or serving plugin), or a latency-sensitive path where cudaMalloc /
+ * cudaFree would implicitly synchronise the device.  Same result as
+ * fap_op_floyd (in-place Floyd-Warshall of an s x s device matrix, leading
+ * dimension ld, dtype FAP_DTYPE_I32 or FAP_DTYPE_F32), but it allocates
+ * nothing and needs no fap_ctx: its padded working copy lives in one 4 MiB
+ * device array built into the library, which every GPU that loads the
+ * library keeps until the process exits.
+ *   - s is limited to FAP_NOALLOC_FLOYD_MAX; larger sizes return
+ *     FAP_ERR_RANGE before any GPU work.
+ *   - Work is queued on `stream` (a cudaStream_t; NULL = the legacy default
+ *     stream) and the call returns without waiting: synchronise the stream
+ *     before reading mat.
+ *   - Every call on a device uses the same array, so calls whose GPU work
+ *     overlaps (different streams, or host threads, on one device) race and
+ *     corrupt each other: serialise them.
+ *   - The first call on a device looks up the array's device address; make
+ *     that first call before any stream capture.
+ * Messages: fap_floyd_noalloc_last_error(). */
+#define FAP_NOALLOC_FLOYD_MAX 1024
+FAP_API int fap_floyd_noalloc(int dtype, int32_t s, void *mat, int64_t ld, void *stream);
+FAP_API const char *fap_floyd_noalloc_last_error(void);
+
 /* Measured relaxation throughput of this device (relaxations/s) for the
  * given dtype, from a register-resident microbenchmark. */
 FAP_API int fap_measure_relax_peak(fap_ctx *ctx, int dtype, double *relax_per_s);
