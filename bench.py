@@ -255,7 +255,7 @@ def main_fap(args):
 
     from fastapsp_b200 import FAP_DTYPE_F32, FAP_MODE_BATCHED, FAP_MODE_PLAIN, Context, DeviceGraph
     from fastapsp_b200 import workloads
-    from fastapsp_b200.sharding import rows_of, shard_parts
+    from fastapsp_b200.sharding import reduce_over_ranks, rows_of, shard_parts
 
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
@@ -268,18 +268,10 @@ def main_fap(args):
             dist.barrier()
 
     def allmax(x):
-        if world == 1:
-            return float(x)
-        t = torch.tensor([float(x)], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_over_ranks(x, "max", device="cuda")
 
     def allsum(x):
-        if world == 1:
-            return float(x)
-        t = torch.tensor([float(x)], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return float(t.item())
+        return reduce_over_ranks(x, "sum", device="cuda")
 
     t_load = time.perf_counter()
     wl = workloads.load(args.workload)
@@ -385,7 +377,9 @@ def main_fap(args):
                 "peak_source": "measured relaxation microbenchmark (fap_measure_relax_peak)",
                 "traffic": read_traffic(wl.name, "floyd_part_kernel")}
     else:
-        kern = "sssp_frontier_kernel" if dom == "sssp" else "minplus_part_kernel"
+        thin_only = all(int(bn[p]) <= 16 for p in mine)
+        kern = ("sssp_frontier_kernel" if dom == "sssp" else
+                "minplus_thin_kernel" if thin_only else "minplus_part_kernel")
         a = stage_roof[dom]["achieved_gbs"]
         roof = {"kernel": kern, "bound": "hbm", "achieved": a, "peak": hbm_peak, "unit": "GB/s",
                 "frac": a / hbm_peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",

@@ -41,3 +41,16 @@ def shard_parts(ver_num: Sequence[int], bdy_num: Sequence[int], n: int, world: i
 
 def rows_of(parts: Sequence[int], ver_num: Sequence[int]) -> int:
     return int(sum(int(ver_num[p]) for p in parts))
+
+
+def reduce_over_ranks(x: float, op: str = "max", device=None) -> float:
+    """Max or sum of a scalar over all ranks of the default process group
+    (identity without one).  `device` is where the reduction tensor lives
+    (a CUDA device for NCCL, None/CPU for gloo)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
