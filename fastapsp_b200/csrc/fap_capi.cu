@@ -449,8 +449,11 @@ int prepare_batch(fap_dgraph *G, const std::vector<int32_t> &ids) {
   G->part_work_end.clear();
   G->thin.clear();
   G->thin_pos.clear();
+  // Floyd arena: equal padded squares (one tensor map describes all parts)
+  int32_t ldf = kFloydTile;
+  for (int32_t p : ids) ldf = std::max<int32_t>(ldf, (int32_t)round_up(std::max(G->vnum[p], 1), kFloydTile));
   int64_t foff = 0;
-  G->max_ldf = 0;
+  G->max_ldf = ldf;
   G->max_b = 0;
   G->max_s = 0;
   for (size_t i = 0; i < ids.size(); i++) {
@@ -461,10 +464,9 @@ int prepare_batch(fap_dgraph *G, const std::vector<int32_t> &ids) {
     d.s = G->vnum[p];
     d.b = G->bnum[p];
     d.row_base = base[i];
-    d.ldf = (int32_t)round_up(std::max(d.s, 1), kFloydTile);
+    d.ldf = ldf;
     d.f_off = foff;
     foff += (int64_t)d.ldf * d.ldf;
-    G->max_ldf = std::max(G->max_ldf, d.ldf);
     G->max_b = std::max(G->max_b, d.b);
     G->max_s = std::max(G->max_s, d.s);
     G->parts.push_back(d);
@@ -552,16 +554,17 @@ int run_solve(fap_dgraph *G, int mode) {
     FAP_CK(launch_gather<T>(dp, np, G->max_ldf, ro, col, w, gid, st2ed, ed2st, D, G->ldD, F, st, &L));
     FAP_CK(cudaEventRecord(c->ev[2], st));
     if (G->floyd_per_cta) {
-      FAP_CK(launch_floyd_parts<T>(dp, np, F, D, G->ldD, st2ed, st, &L));
+      FAP_CK(launch_floyd_parts<T>(dp, np, F, G->max_ldf, D, G->ldD, st2ed, status, st, &L));
     } else {
-      FAP_CK(launch_floyd_parts_multi<T>(dp, np, G->max_ldf, F, st, &L));
+      FAP_CK(launch_floyd_parts_multi<T>(dp, np, (int)ceil_div(G->max_s, kFloydTile), F, G->max_ldf,
+                                         status, st, &L));
       FAP_CK(launch_bdy_scatter<T>(dp, np, F, D, G->ldD, st2ed, G->max_b, G->max_s, st, &L));
     }
     FAP_CK(cudaEventRecord(c->ev[3], st));
     FAP_CK(launch_minplus_thin<T>(dp, G->d_thin.as<int32_t>(), (int)G->thin.size(), G->n, F, D,
                                   G->ldD, gid, ed2st, st, &L));
-    FAP_CK(launch_minplus_parts<T>(dp, dw, (int)G->work.size(), G->n, F, D, G->ldD, gid, ed2st, st,
-                                   &L));
+    FAP_CK(launch_minplus_parts<T>(dp, np, dw, (int)G->work.size(), G->n, F, G->max_ldf, D, G->ldD,
+                                   G->max_rows, gid, ed2st, status, st, &L));
     FAP_CK(cudaEventRecord(c->ev[4], st));
   } else {
     FAP_CK(cudaEventRecord(c->ev[0], st));
@@ -572,13 +575,14 @@ int run_solve(fap_dgraph *G, int mode) {
       FAP_CK(launch_sssp<T>(ro_s, col_s, w_s, G->n, src + s0, srow + s0, s1 - s0, D, G->ldD,
                             G->ldD, ed2st, scratch, delta, G->sssp_chain, max_rounds, status, st, &L));
       FAP_CK(launch_gather<T>(dp + i, 1, d.ldf, ro, col, w, gid, st2ed, ed2st, D, G->ldD, F, st, &L));
-      FAP_CK(launch_floyd_matrix<T>(F + d.f_off, d.ldf, d.ldf / kFloydTile, st, &L));
+      FAP_CK(launch_floyd_matrix<T>(F + d.f_off, d.ldf, (int)ceil_div(d.s, kFloydTile), status, st, &L));
       FAP_CK(launch_bdy_scatter<T>(dp + i, 1, F, D, G->ldD, st2ed, d.b, d.s, st, &L));
       if (G->thin_pos[i] >= 0)
         FAP_CK(launch_minplus_thin<T>(dp, G->d_thin.as<int32_t>() + G->thin_pos[i], 1, G->n, F, D,
                                       G->ldD, gid, ed2st, st, &L));
       else
-        FAP_CK(launch_minplus_parts<T>(dp, dw + w0, w1 - w0, G->n, F, D, G->ldD, gid, ed2st, st, &L));
+        FAP_CK(launch_minplus_parts<T>(dp, np, dw + w0, w1 - w0, G->n, F, G->max_ldf, D, G->ldD,
+                                       G->max_rows, gid, ed2st, status, st, &L));
     }
     FAP_CK(cudaEventRecord(c->ev[4], st));
   }
@@ -592,6 +596,7 @@ int read_status(fap_dgraph *G) {
   FAP_CK(cudaMemcpy(&h, G->d_status.p, sizeof(int), cudaMemcpyDeviceToHost));
   if (h == kDevSsspRoundLimit)
     return fail(FAP_ERR_NOT_CONVERGED, "SSSP hit its round bound");
+  if (h == kDevTmaTimeout) return fail(FAP_ERR_DEVICE, "a TMA tile load did not complete in time");
   if (h != kDevOk) return fail(FAP_ERR_DEVICE, "device-side error %d", h);
   return FAP_OK;
 }
@@ -769,6 +774,7 @@ extern "C" int fap_op_floyd(fap_ctx *c, int dtype, int32_t s, void *mat, int64_t
   DeviceGuard g(c->device);
   cudaStream_t st = c->stream;
   const int64_t ldp = round_up(s, kFloydTile);
+  FAP_CK(cudaMemsetAsync(c->status.p, 0, sizeof(int), st));
   FAP_TRY(c->scratch.ensure((size_t)ldp * ldp * 4));
   int64_t L = 0;
   // padded copy: sentinel everywhere, then the matrix
@@ -779,14 +785,15 @@ extern "C" int fap_op_floyd(fap_ctx *c, int dtype, int32_t s, void *mat, int64_t
   FAP_CK(cudaMemcpy2DAsync(c->scratch.p, (size_t)ldp * 4, mat, (size_t)ld * 4, (size_t)s * 4, (size_t)s,
                            cudaMemcpyDeviceToDevice, st));
   if (dtype == FAP_DTYPE_I32)
-    FAP_CK(launch_floyd_matrix<int32_t>(c->scratch.as<int32_t>(), ldp, (int)(ldp / kFloydTile), st, &L));
+    FAP_CK(launch_floyd_matrix<int32_t>(c->scratch.as<int32_t>(), ldp, (int)(ldp / kFloydTile),
+                                        c->status.as<int>(), st, &L));
   else
-    FAP_CK(launch_floyd_matrix<float>(c->scratch.as<float>(), ldp, (int)(ldp / kFloydTile), st, &L));
+    FAP_CK(launch_floyd_matrix<float>(c->scratch.as<float>(), ldp, (int)(ldp / kFloydTile),
+                                      c->status.as<int>(), st, &L));
   FAP_CK(cudaMemcpy2DAsync(mat, (size_t)ld * 4, c->scratch.p, (size_t)ldp * 4, (size_t)s * 4, (size_t)s,
                            cudaMemcpyDeviceToDevice, st));
-  FAP_CK(cudaStreamSynchronize(st));
   c->launches += L;
-  return FAP_OK;
+  return read_ctx_status(c);
 }
 
 extern "C" int fap_op_minplus(fap_ctx *c, int dtype, int32_t M, int32_t N, int32_t K, const void *A,

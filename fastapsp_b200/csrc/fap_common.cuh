@@ -62,6 +62,7 @@ enum DevStatus : int {
   kDevOk = 0,
   kDevSsspRoundLimit = 1,   // SSSP did not converge within its round bound
   kDevBadIndex = 2,         // an input index was out of range (skipped)
+  kDevTmaTimeout = 3,       // a TMA stage never completed (bounded wait gave up)
 };
 
 __device__ inline void set_status(int *status, int code) {

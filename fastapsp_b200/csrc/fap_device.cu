@@ -18,8 +18,60 @@
 #include "floyd.cuh"
 #include "minplus_tile.cuh"
 #include "sssp.cuh"
+#include "tma.cuh"
+#include "tma_tile.cuh"
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
 
 namespace fapb {
+
+// ---------------------------------------------------------------------------
+// Tensor maps (host).  cuTensorMapEncodeTiled comes from the driver through
+// the runtime's entry-point query, so the library needs no link-time
+// dependency on libcuda.
+// ---------------------------------------------------------------------------
+namespace {
+PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    else
+      cudaGetLastError();
+  }
+  return fn;
+}
+}  // namespace
+
+cudaError_t make_tmap_3d(CUtensorMap *map, const void *base, bool is_float, uint64_t d0, uint64_t d1,
+                         uint64_t d2, uint32_t box0, uint32_t box1) {
+  auto enc = tmap_encoder();
+  if (!enc) return cudaErrorNotSupported;
+  const cuuint64_t dims[3] = {d0, d1, d2};
+  const cuuint64_t strides[2] = {d0 * 4, d0 * d1 * 4};
+  const cuuint32_t box[3] = {box0, box1, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r = enc(map, is_float ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_INT32, 3,
+                         const_cast<void *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+template <typename T>
+cudaError_t make_arena_tmaps(const T *F, int64_t ld, int nparts, CUtensorMap *mapA, CUtensorMap *mapB) {
+  using TC = typename FloydCfg<T, kFloydTile>::TC;
+  const bool f = Dist<T>::kDtype == FAP_DTYPE_F32;
+  cudaError_t e = make_tmap_3d(mapA, F, f, ld, ld, nparts, TC::BK, TC::BM);
+  if (e == cudaSuccess) e = make_tmap_3d(mapB, F, f, ld, ld, nparts, TC::BN, TC::BK);
+  return e;
+}
 
 using MPCfg32 = TileCfg<int32_t, kMinplusBM, kMinplusBN, 16, 8, 8>;
 
@@ -149,14 +201,20 @@ cudaError_t launch_sssp(const int32_t *row_offset, const int32_t *col, const T *
 // Stage 2.2: Floyd-Warshall
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS)
+__global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS, 2)
     floyd_part_kernel(const PartDesc *__restrict__ parts, T *F, T *D, int64_t ldD,
-                      const int32_t *__restrict__ st2ed) {
-  extern __shared__ __align__(16) unsigned char fp_smem_raw[];
-  T *smem = reinterpret_cast<T *>(fp_smem_raw);
+                      const int32_t *__restrict__ st2ed, const __grid_constant__ CUtensorMap mapA,
+                      const __grid_constant__ CUtensorMap mapB, int *status) {
+  using TC = typename FloydCfg<T, kFloydTile>::TC;
+  extern __shared__ __align__(128) unsigned char fp_smem_raw[];
+  auto sm = tma_smem_init<T, TC>(fp_smem_raw);
   const PartDesc pd = parts[blockIdx.x];
   T *mat = F + pd.f_off;
-  floyd_close_cta<T, kFloydTile>(mat, pd.ldf, pd.ldf / kFloydTile, smem);
+  const int nb = (int)ceil_div(pd.s, kFloydTile);
+  if (!floyd_close_cta<T, kFloydTile>(&mapA, &mapB, blockIdx.x, mat, pd.ldf, nb, sm)) {
+    if (threadIdx.x == 0) set_status(status, kDevTmaTimeout);
+    return;
+  }
   // Decode of the boundary rows (util_Myalgorithm.h:75-86 for rows < b).
   const int64_t cnt = (int64_t)pd.b * pd.s;
   for (int64_t t = threadIdx.x; t < cnt; t += blockDim.x) {
@@ -166,31 +224,95 @@ __global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS)
 }
 
 template <typename T>
-cudaError_t launch_floyd_parts(const PartDesc *parts, int nparts, T *F, T *D, int64_t ldD,
-                               const int32_t *st2ed, cudaStream_t stream, int64_t *launches) {
+cudaError_t launch_floyd_parts(const PartDesc *parts, int nparts, T *F, int64_t ld, T *D,
+                               int64_t ldD, const int32_t *st2ed, int *status, cudaStream_t stream,
+                               int64_t *launches) {
   if (nparts <= 0) return cudaSuccess;
-  const size_t smem = FloydCfg<T, kFloydTile>::SMEM_ELEMS * sizeof(T);
+  CUtensorMap mapA, mapB;
+  cudaError_t e = make_arena_tmaps<T>(F, ld, nparts, &mapA, &mapB);
+  if (e != cudaSuccess) return e;
+  const size_t smem = FloydCfg<T, kFloydTile>::SMEM_BYTES;
   auto kern = floyd_part_kernel<T>;
-  if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-  }
-  kern<<<nparts, FloydCfg<T, kFloydTile>::THREADS, smem, stream>>>(parts, F, D, ldD, st2ed);
+  e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  kern<<<nparts, FloydCfg<T, kFloydTile>::THREADS, smem, stream>>>(parts, F, D, ldD, st2ed, mapA, mapB,
+                                                                   status);
   *launches += 1;
   return cudaGetLastError();
 }
 
+// One matrix (leading dimension ld, a multiple of kFloydTile, padded with the
+// sentinel to nb tiles per side), one launch per phase per pivot block.
 template <typename T>
-cudaError_t launch_floyd_matrix(T *mat, int64_t ld, int nb, cudaStream_t stream,
+__global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS, 2)
+    floyd_mat_phase1_kernel(T *mat, int64_t ld, int kb) {
+  using TC = typename FloydCfg<T, kFloydTile>::TC;
+  extern __shared__ __align__(128) unsigned char fq_smem_raw[];
+  auto sm = tma_smem_init<T, TC>(fq_smem_raw);
+  floyd_diag_close<T, kFloydTile>(mat, ld, kb * kFloydTile, sm.ring);
+}
+
+// blockIdx.x in [0, 2*(nb-1)): first nb-1 are row-panel tiles, rest column.
+template <typename T>
+__global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS, 2)
+    floyd_mat_phase2_kernel(T *mat, int64_t ld, int kb, int nb,
+                            const __grid_constant__ CUtensorMap mapA,
+                            const __grid_constant__ CUtensorMap mapB, int *status) {
+  using TC = typename FloydCfg<T, kFloydTile>::TC;
+  extern __shared__ __align__(128) unsigned char fq_smem_raw[];
+  auto sm = tma_smem_init<T, TC>(fq_smem_raw);
+  int t = blockIdx.x;
+  bool ok;
+  if (t < nb - 1) {
+    const int j = t < kb ? t : t + 1;
+    ok = floyd_tile_update<T, kFloydTile>(&mapA, &mapB, 0, mat, ld, kb, j, kb, sm);
+  } else {
+    t -= nb - 1;
+    const int i = t < kb ? t : t + 1;
+    ok = floyd_tile_update<T, kFloydTile>(&mapA, &mapB, 0, mat, ld, i, kb, kb, sm);
+  }
+  if (!ok && threadIdx.x == 0 && status) set_status(status, kDevTmaTimeout);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS, 2)
+    floyd_mat_phase3_kernel(T *mat, int64_t ld, int kb, int nb,
+                            const __grid_constant__ CUtensorMap mapA,
+                            const __grid_constant__ CUtensorMap mapB, int *status) {
+  using TC = typename FloydCfg<T, kFloydTile>::TC;
+  extern __shared__ __align__(128) unsigned char fq_smem_raw[];
+  auto sm = tma_smem_init<T, TC>(fq_smem_raw);
+  const int t = blockIdx.x;
+  int i = t / (nb - 1), j = t % (nb - 1);
+  i = i < kb ? i : i + 1;
+  j = j < kb ? j : j + 1;
+  if (!floyd_tile_update<T, kFloydTile>(&mapA, &mapB, 0, mat, ld, i, j, kb, sm) && threadIdx.x == 0 &&
+      status)
+    set_status(status, kDevTmaTimeout);
+}
+
+template <typename T>
+cudaError_t launch_floyd_matrix(T *mat, int64_t ld, int nb, int *status, cudaStream_t stream,
                                 int64_t *launches) {
   using FC = FloydCfg<T, kFloydTile>;
-  const size_t smem = FC::SMEM_ELEMS * sizeof(T);
+  if (nb <= 0) return cudaSuccess;
+  CUtensorMap mapA, mapB;
+  cudaError_t e = make_arena_tmaps<T>(mat, ld, 1, &mapA, &mapB);
+  if (e != cudaSuccess) return e;
+  const size_t smem = FC::SMEM_BYTES;
+  for (auto k : {(const void *)floyd_mat_phase1_kernel<T>, (const void *)floyd_mat_phase2_kernel<T>,
+                 (const void *)floyd_mat_phase3_kernel<T>}) {
+    e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
   for (int kb = 0; kb < nb; kb++) {
-    floyd_phase1_kernel<T, kFloydTile><<<1, FC::THREADS, smem, stream>>>(mat, ld, kb);
+    floyd_mat_phase1_kernel<T><<<1, FC::THREADS, smem, stream>>>(mat, ld, kb);
     *launches += 1;
     if (nb > 1) {
-      floyd_phase2_kernel<T, kFloydTile><<<2 * (nb - 1), FC::THREADS, smem, stream>>>(mat, ld, kb, nb);
-      floyd_phase3_kernel<T, kFloydTile><<<(nb - 1) * (nb - 1), FC::THREADS, smem, stream>>>(mat, ld, kb, nb);
+      floyd_mat_phase2_kernel<T><<<2 * (nb - 1), FC::THREADS, smem, stream>>>(mat, ld, kb, nb, mapA, mapB,
+                                                                             status);
+      floyd_mat_phase3_kernel<T><<<(nb - 1) * (nb - 1), FC::THREADS, smem, stream>>>(mat, ld, kb, nb, mapA,
+                                                                                    mapB, status);
       *launches += 2;
     }
   }
@@ -199,67 +321,87 @@ cudaError_t launch_floyd_matrix(T *mat, int64_t ld, int nb, cudaStream_t stream,
 
 // Batched multi-launch form: pivot round kb of every part in three
 // launches (diagonal tiles, panel tiles, remainder tiles), so thousands of
-// tile CTAs keep every SM busy whatever the number of parts.  Parts have
-// nb_p = ldf / kFloydTile tiles per side; CTAs beyond a part's tiles exit.
+// tile CTAs keep every SM busy whatever the number of parts.  Part z has
+// nb_z = ceil(s_z / kFloydTile) tiles per side in an arena of equal squares;
+// CTAs beyond a part's tiles exit.
 template <typename T>
-__global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS)
+__global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS, 2)
     floyd_parts_phase1_kernel(const PartDesc *__restrict__ parts, T *F, int kb) {
-  extern __shared__ __align__(16) unsigned char fm_smem_raw[];
-  T *smem = reinterpret_cast<T *>(fm_smem_raw);
+  using TC = typename FloydCfg<T, kFloydTile>::TC;
+  extern __shared__ __align__(128) unsigned char fm_smem_raw[];
   const PartDesc pd = parts[blockIdx.x];
-  if (kb >= pd.ldf / kFloydTile) return;
-  floyd_diag_close<T, kFloydTile>(F + pd.f_off, pd.ldf, kb * kFloydTile, smem);
+  if (kb >= (int)ceil_div(pd.s, kFloydTile)) return;
+  auto sm = tma_smem_init<T, TC>(fm_smem_raw);
+  floyd_diag_close<T, kFloydTile>(F + pd.f_off, pd.ldf, kb * kFloydTile, sm.ring);
 }
 
 template <typename T>
-__global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS)
-    floyd_parts_phase2_kernel(const PartDesc *__restrict__ parts, T *F, int kb) {
-  extern __shared__ __align__(16) unsigned char fm_smem_raw[];
-  T *smem = reinterpret_cast<T *>(fm_smem_raw);
+__global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS, 2)
+    floyd_parts_phase2_kernel(const PartDesc *__restrict__ parts, T *F, int kb,
+                              const __grid_constant__ CUtensorMap mapA,
+                              const __grid_constant__ CUtensorMap mapB, int *status) {
+  using TC = typename FloydCfg<T, kFloydTile>::TC;
+  extern __shared__ __align__(128) unsigned char fm_smem_raw[];
   const PartDesc pd = parts[blockIdx.y];
-  const int nb = pd.ldf / kFloydTile;
+  const int nb = (int)ceil_div(pd.s, kFloydTile);
   int t = blockIdx.x;
   if (kb >= nb || t >= 2 * (nb - 1)) return;
+  auto sm = tma_smem_init<T, TC>(fm_smem_raw);
   T *mat = F + pd.f_off;
+  bool ok;
   if (t < nb - 1) {
     const int j = t < kb ? t : t + 1;
-    floyd_tile_update<T, kFloydTile>(mat, pd.ldf, kb, j, kb, smem);
+    ok = floyd_tile_update<T, kFloydTile>(&mapA, &mapB, blockIdx.y, mat, pd.ldf, kb, j, kb, sm);
   } else {
     t -= nb - 1;
     const int i = t < kb ? t : t + 1;
-    floyd_tile_update<T, kFloydTile>(mat, pd.ldf, i, kb, kb, smem);
+    ok = floyd_tile_update<T, kFloydTile>(&mapA, &mapB, blockIdx.y, mat, pd.ldf, i, kb, kb, sm);
   }
+  if (!ok && threadIdx.x == 0) set_status(status, kDevTmaTimeout);
 }
 
 template <typename T>
-__global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS)
-    floyd_parts_phase3_kernel(const PartDesc *__restrict__ parts, T *F, int kb) {
-  extern __shared__ __align__(16) unsigned char fm_smem_raw[];
-  T *smem = reinterpret_cast<T *>(fm_smem_raw);
+__global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS, 2)
+    floyd_parts_phase3_kernel(const PartDesc *__restrict__ parts, T *F, int kb,
+                              const __grid_constant__ CUtensorMap mapA,
+                              const __grid_constant__ CUtensorMap mapB, int *status) {
+  using TC = typename FloydCfg<T, kFloydTile>::TC;
+  extern __shared__ __align__(128) unsigned char fm_smem_raw[];
   const PartDesc pd = parts[blockIdx.y];
-  const int nb = pd.ldf / kFloydTile;
+  const int nb = (int)ceil_div(pd.s, kFloydTile);
   const int t = blockIdx.x;
   if (kb >= nb || t >= (nb - 1) * (nb - 1)) return;
+  auto sm = tma_smem_init<T, TC>(fm_smem_raw);
   int i = t / (nb - 1), j = t % (nb - 1);
   i = i < kb ? i : i + 1;
   j = j < kb ? j : j + 1;
-  floyd_tile_update<T, kFloydTile>(F + pd.f_off, pd.ldf, i, j, kb, smem);
+  if (!floyd_tile_update<T, kFloydTile>(&mapA, &mapB, blockIdx.y, F + pd.f_off, pd.ldf, i, j, kb, sm) &&
+      threadIdx.x == 0)
+    set_status(status, kDevTmaTimeout);
 }
 
 template <typename T>
-cudaError_t launch_floyd_parts_multi(const PartDesc *parts, int nparts, int max_ldf, T *F,
-                                     cudaStream_t stream, int64_t *launches) {
-  if (nparts <= 0) return cudaSuccess;
+cudaError_t launch_floyd_parts_multi(const PartDesc *parts, int nparts, int max_nb, T *F, int64_t ld,
+                                     int *status, cudaStream_t stream, int64_t *launches) {
+  if (nparts <= 0 || max_nb <= 0) return cudaSuccess;
   using FC = FloydCfg<T, kFloydTile>;
-  const size_t smem = FC::SMEM_ELEMS * sizeof(T);
-  const int nbmax = max_ldf / kFloydTile;
-  for (int kb = 0; kb < nbmax; kb++) {
+  CUtensorMap mapA, mapB;
+  cudaError_t e = make_arena_tmaps<T>(F, ld, nparts, &mapA, &mapB);
+  if (e != cudaSuccess) return e;
+  const size_t smem = FC::SMEM_BYTES;
+  for (auto k : {(const void *)floyd_parts_phase1_kernel<T>, (const void *)floyd_parts_phase2_kernel<T>,
+                 (const void *)floyd_parts_phase3_kernel<T>}) {
+    e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  for (int kb = 0; kb < max_nb; kb++) {
     floyd_parts_phase1_kernel<T><<<nparts, FC::THREADS, smem, stream>>>(parts, F, kb);
     *launches += 1;
-    if (nbmax > 1) {
-      floyd_parts_phase2_kernel<T><<<dim3(2 * (nbmax - 1), nparts), FC::THREADS, smem, stream>>>(parts, F, kb);
-      floyd_parts_phase3_kernel<T><<<dim3((nbmax - 1) * (nbmax - 1), nparts), FC::THREADS, smem, stream>>>(
-          parts, F, kb);
+    if (max_nb > 1) {
+      floyd_parts_phase2_kernel<T><<<dim3(2 * (max_nb - 1), nparts), FC::THREADS, smem, stream>>>(
+          parts, F, kb, mapA, mapB, status);
+      floyd_parts_phase3_kernel<T><<<dim3((max_nb - 1) * (max_nb - 1), nparts), FC::THREADS, smem, stream>>>(
+          parts, F, kb, mapA, mapB, status);
       *launches += 2;
     }
   }
@@ -297,23 +439,31 @@ cudaError_t launch_bdy_scatter(const PartDesc *parts, int nparts, const T *F, T 
 //   F[b+i][ed2st[j]-start] replaces it, as the reference's decode does.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(MPCfg<T>::THREADS)
+__global__ void __launch_bounds__(MPCfg<T>::THREADS, 2)
     minplus_part_kernel(const PartDesc *__restrict__ parts, const MPWork *__restrict__ work, int n,
                         const T *__restrict__ F, T *D, int64_t ldD,
-                        const int32_t *__restrict__ graph_id, const int32_t *__restrict__ ed2st) {
+                        const int32_t *__restrict__ graph_id, const int32_t *__restrict__ ed2st,
+                        const __grid_constant__ CUtensorMap mapF, const __grid_constant__ CUtensorMap mapD,
+                        int *status) {
   using C = MPCfg<T>;
-  extern __shared__ __align__(16) unsigned char mp_smem_raw[];
-  T *smem = reinterpret_cast<T *>(mp_smem_raw);
+  using TC = typename FloydCfg<T, kFloydTile>::TC;
+  extern __shared__ __align__(128) unsigned char mp_smem_raw[];
+  auto sm = tma_smem_init<T, TC>(mp_smem_raw);
   const MPWork wk = work[blockIdx.y];
   const PartDesc pd = parts[wk.pidx];
   const int n0 = blockIdx.x * C::BN;
   const int M = pd.s - pd.b, K = pd.b;
-  const T *A = F + pd.f_off + (int64_t)pd.b * pd.ldf;
-  const T *B = D + pd.row_base * ldD;
   T *Cm = D + (pd.row_base + pd.b) * ldD;
   T acc[C::TM][C::TN];
   acc_fill<T, C>(acc, Dist<T>::inf());
-  minplus_tile<T, C, true, true>(A, pd.ldf, B, ldD, wk.m0, n0, M, (int)ldD, K, acc, smem);
+  // A = F rows b+m0.. of part wk.pidx (columns 0..b-1); B = D rows
+  // row_base..row_base+b-1 (the part's boundary rows).  Rows and columns past
+  // the part's extent are never stored; k past b is never read.
+  if (!tma_minplus_tile<T, TC>(&mapF, 0, pd.b + wk.m0, wk.pidx, &mapD, n0, (int)pd.row_base, 0, K, acc,
+                               sm)) {
+    if (threadIdx.x == 0) set_status(status, kDevTmaTimeout);
+    return;
+  }
 
   const int tid = threadIdx.x, ty = tid / C::TX, tx = tid % C::TX;
   // Own-part columns of this thread (fused decode).
@@ -517,15 +667,24 @@ __global__ void __launch_bounds__(kThinThreads, 2)
 }
 
 template <typename T>
-cudaError_t launch_minplus_parts(const PartDesc *parts, const MPWork *work, int nwork, int n,
-                                 const T *F, T *D, int64_t ldD, const int32_t *graph_id,
-                                 const int32_t *ed2st, cudaStream_t stream, int64_t *launches) {
+cudaError_t launch_minplus_parts(const PartDesc *parts, int nparts, const MPWork *work, int nwork, int n,
+                                 const T *F, int64_t ldf, T *D, int64_t ldD, int64_t drows,
+                                 const int32_t *graph_id, const int32_t *ed2st, int *status,
+                                 cudaStream_t stream, int64_t *launches) {
   if (nwork <= 0) return cudaSuccess;
   using C = MPCfg<T>;
-  const size_t smem = C::SMEM_ELEMS * sizeof(T);
+  using TC = typename FloydCfg<T, kFloydTile>::TC;
+  const bool f = Dist<T>::kDtype == FAP_DTYPE_F32;
+  CUtensorMap mapF, mapD;
+  cudaError_t e = make_tmap_3d(&mapF, F, f, ldf, ldf, nparts, TC::BK, TC::BM);
+  if (e == cudaSuccess) e = make_tmap_3d(&mapD, D, f, ldD, drows, 1, TC::BN, TC::BK);
+  if (e != cudaSuccess) return e;
+  const size_t smem = TC::SMEM_BYTES;
+  auto kern = minplus_part_kernel<T>;
+  e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
   dim3 grid((unsigned)(ldD / C::BN), (unsigned)nwork);
-  minplus_part_kernel<T><<<grid, C::THREADS, smem, stream>>>(parts, work, n, F, D, ldD, graph_id,
-                                                             ed2st);
+  kern<<<grid, C::THREADS, smem, stream>>>(parts, work, n, F, D, ldD, graph_id, ed2st, mapF, mapD, status);
   *launches += 1;
   return cudaGetLastError();
 }
@@ -690,16 +849,17 @@ cudaError_t launch_relax_peak(T *sink, int blocks, int iters, cudaStream_t strea
                                         const int32_t *, const T *, const int32_t *,              \
                                         const int32_t *, const int32_t *, const T *, int64_t, T *, \
                                         cudaStream_t, int64_t *);                                 \
-  template cudaError_t launch_floyd_parts<T>(const PartDesc *, int, T *, T *, int64_t,            \
-                                             const int32_t *, cudaStream_t, int64_t *);           \
-  template cudaError_t launch_floyd_matrix<T>(T *, int64_t, int, cudaStream_t, int64_t *);        \
-  template cudaError_t launch_floyd_parts_multi<T>(const PartDesc *, int, int, T *, cudaStream_t, \
-                                                   int64_t *);                                    \
+  template cudaError_t launch_floyd_parts<T>(const PartDesc *, int, T *, int64_t, T *, int64_t,   \
+                                             const int32_t *, int *, cudaStream_t, int64_t *);    \
+  template cudaError_t launch_floyd_matrix<T>(T *, int64_t, int, int *, cudaStream_t, int64_t *); \
+  template cudaError_t launch_floyd_parts_multi<T>(const PartDesc *, int, int, T *, int64_t, int *, \
+                                                   cudaStream_t, int64_t *);                      \
   template cudaError_t launch_bdy_scatter<T>(const PartDesc *, int, const T *, T *, int64_t,      \
                                              const int32_t *, int, int, cudaStream_t, int64_t *); \
-  template cudaError_t launch_minplus_parts<T>(const PartDesc *, const MPWork *, int, int,        \
-                                               const T *, T *, int64_t, const int32_t *,          \
-                                               const int32_t *, cudaStream_t, int64_t *);         \
+  template cudaError_t launch_minplus_parts<T>(const PartDesc *, int, const MPWork *, int, int,   \
+                                               const T *, int64_t, T *, int64_t, int64_t,         \
+                                               const int32_t *, const int32_t *, int *,           \
+                                               cudaStream_t, int64_t *);                          \
   template cudaError_t launch_minplus_thin<T>(const PartDesc *, const int32_t *, int, int,        \
                                               const T *, T *, int64_t, const int32_t *,           \
                                               const int32_t *, cudaStream_t, int64_t *);          \

@@ -53,22 +53,26 @@ cudaError_t launch_gather(const PartDesc *parts, int nparts, int max_ldf, const 
                           const int32_t *st2ed, const int32_t *ed2st, const T *D, int64_t ldD,
                           T *F, cudaStream_t stream, int64_t *launches);
 
+// The Floyd arena F holds the batch's parts as equal padded squares of
+// leading dimension ld (a multiple of kFloydTile), part i at i * ld * ld.
+
 // Batched: one CTA per part closes its matrix and writes its boundary rows'
 // own-part columns back into D.
 template <typename T>
-cudaError_t launch_floyd_parts(const PartDesc *parts, int nparts, T *F, T *D, int64_t ldD,
-                               const int32_t *st2ed, cudaStream_t stream, int64_t *launches);
+cudaError_t launch_floyd_parts(const PartDesc *parts, int nparts, T *F, int64_t ld, T *D,
+                               int64_t ldD, const int32_t *st2ed, int *status, cudaStream_t stream,
+                               int64_t *launches);
 
 // Batched, multi-launch: every part's pivot round in three launches
-// (3 x max_ldf/kFloydTile launches in all); no boundary-row decode.
+// (3 x max_nb launches in all); no boundary-row decode.
 template <typename T>
-cudaError_t launch_floyd_parts_multi(const PartDesc *parts, int nparts, int max_ldf, T *F,
-                                     cudaStream_t stream, int64_t *launches);
+cudaError_t launch_floyd_parts_multi(const PartDesc *parts, int nparts, int max_nb, T *F, int64_t ld,
+                                     int *status, cudaStream_t stream, int64_t *launches);
 
-// Plain: one padded matrix (ld multiple of kFloydTile, nb = ld / kFloydTile
-// tiles per side), one launch per phase per pivot block.
+// Plain: one padded matrix (ld a multiple of kFloydTile, nb tiles per side
+// in use), one launch per phase per pivot block.  status may be null.
 template <typename T>
-cudaError_t launch_floyd_matrix(T *mat, int64_t ld, int nb, cudaStream_t stream,
+cudaError_t launch_floyd_matrix(T *mat, int64_t ld, int nb, int *status, cudaStream_t stream,
                                 int64_t *launches);
 
 // Boundary rows of the listed parts: F[i][j] -> D[row_base+i][st2ed[start+j]].
@@ -79,10 +83,13 @@ cudaError_t launch_bdy_scatter(const PartDesc *parts, int nparts, const T *F, T 
 
 // Min-plus merge of the inner rows of the batch's parts, with the own-part
 // columns taken from the closed Floyd matrices (fused decode).
+// (F is the batch's Floyd arena with leading dimension ldf and nparts parts;
+// D has drows rows.)
 template <typename T>
-cudaError_t launch_minplus_parts(const PartDesc *parts, const MPWork *work, int nwork, int n,
-                                 const T *F, T *D, int64_t ldD, const int32_t *graph_id,
-                                 const int32_t *ed2st, cudaStream_t stream, int64_t *launches);
+cudaError_t launch_minplus_parts(const PartDesc *parts, int nparts, const MPWork *work, int nwork, int n,
+                                 const T *F, int64_t ldf, T *D, int64_t ldD, int64_t drows,
+                                 const int32_t *graph_id, const int32_t *ed2st, int *status,
+                                 cudaStream_t stream, int64_t *launches);
 
 // Same for parts with at most kThinBoundary boundary vertices (store-bound
 // shape): thin_parts[0..nthin) are batch indices of such parts.

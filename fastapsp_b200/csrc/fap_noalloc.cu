@@ -72,7 +72,8 @@ cudaError_t noalloc_run(T *scratch, int32_t s, T *mat, int64_t ld, cudaStream_t 
   if (e == cudaSuccess)
     e = cudaMemcpy2DAsync(scratch, (size_t)ldp * sizeof(T), mat, (size_t)ld * sizeof(T),
                           (size_t)s * sizeof(T), (size_t)s, cudaMemcpyDeviceToDevice, st);
-  if (e == cudaSuccess) e = launch_floyd_matrix<T>(scratch, ldp, (int)(ldp / kFloydTile), st, &launches);
+  if (e == cudaSuccess)
+    e = launch_floyd_matrix<T>(scratch, ldp, (int)(ldp / kFloydTile), nullptr, st, &launches);
   if (e == cudaSuccess)
     e = cudaMemcpy2DAsync(mat, (size_t)ld * sizeof(T), scratch, (size_t)ldp * sizeof(T),
                           (size_t)s * sizeof(T), (size_t)s, cudaMemcpyDeviceToDevice, st);

@@ -4,9 +4,11 @@
 // 32x32 tile per CTA, one element per thread, 2 launches per pivot) and the
 // CPU floyd_CPU_path (fap/kernel/floyd.h:38-49).
 //
-// The matrix is padded to a multiple of TILE in both dimensions with the
-// sentinel (padding never improves a real entry), so no tile needs bounds
-// checks.  Per pivot block kb:
+// The matrices live in an arena of equal-sized padded squares (leading
+// dimension ld, a multiple of TILE, part z at offset z * ld * ld), padded with
+// the sentinel (padding never improves a real entry), so no tile needs bounds
+// checks and one 3-D tensor map (column, row, part) describes every part.
+// Per pivot block kb:
 //   phase 1  close the diagonal tile D[kb][kb] with TILE sequential steps;
 //            each thread keeps its TMxTN entries in registers and only the
 //            pivot row/column of a step go through shared memory.
@@ -15,39 +17,42 @@
 //            Because D*[kb][kb] is closed, one min-plus product gives what
 //            TILE sequential pivot steps give.
 //   phase 3  D[I][J] = min(D[I][J], D[I][kb] (x) D[kb][J])
-// Phases 2 and 3 run on the register-tiled min-plus engine.
+// Phases 2 and 3 run on the TMA-fed tile engine (tma_tile.cuh).
 //
-// Two drivers use the same phases:
-//   floyd_part_kernel   one CTA closes one part's whole matrix (every part of
-//                       a batch in one launch, no inter-CTA synchronisation);
-//   floyd_*_phase       one launch per phase, tiles spread over the GPU (one
-//                       matrix at a time: the plain form and fap_op_floyd).
+// Drivers:
+//   floyd_close_cta      one CTA closes one part's whole matrix;
+//   floyd_*_phase kernels one launch per phase, tiles across the GPU.
 #pragma once
 
 #include "minplus_tile.cuh"
+#include "tma_tile.cuh"
 
 namespace fapb {
 
+constexpr int kFloydStages = 4;
+
 template <typename T, int TILE>
 struct FloydCfg {
-  using C = TileCfg<T, TILE, TILE, 16, 8, 8>;
+  using C = TileCfg<T, TILE, TILE, 16, 8, 8>;                 // register layout
+  using TC = TmaTileCfg<T, TILE, TILE, 16, kFloydStages>;      // phase 2/3 engine
   static constexpr int THREADS = C::THREADS;
-  // phase-1 pivot row/column buffers (double-buffered) + min-plus staging
-  static constexpr int P1_ELEMS = 4 * TILE;
-  static constexpr int SMEM_ELEMS = (C::SMEM_ELEMS > P1_ELEMS ? C::SMEM_ELEMS : P1_ELEMS);
+  static_assert(TC::THREADS == C::THREADS, "same thread layout");
+  static constexpr int P1_BYTES = 4 * TILE * (int)sizeof(T);
+  static constexpr int SMEM_BYTES = TC::SMEM_BYTES;
+  static_assert(P1_BYTES <= TC::RING_BYTES, "phase-1 buffers fit in the ring");
 };
 
-// Phase 1 on the tile at (r0, r0) of a padded matrix.  Block-wide; all
-// threads of the CTA must call it.
+// Phase 1 on the tile at (r0, r0) of a padded matrix.  Block-wide; `buf`
+// holds 4*TILE elements of shared memory.
 template <typename T, int TILE>
-__device__ __forceinline__ void floyd_diag_close(T *mat, int64_t ld, int r0, T *smem) {
+__device__ __forceinline__ void floyd_diag_close(T *mat, int64_t ld, int r0, T *buf) {
   using C = typename FloydCfg<T, TILE>::C;
   const int tid = threadIdx.x, ty = tid / C::TX, tx = tid % C::TX;
   T acc[C::TM][C::TN];
   acc_load<T, C, true>(acc, mat, ld, r0, r0, 0, 0);
   for (int k = 0; k < TILE; k++) {
-    T *rowbuf0 = smem + (k & 1) * TILE;
-    T *colbuf0 = smem + 2 * TILE + (k & 1) * TILE;
+    T *rowbuf0 = buf + (k & 1) * TILE;
+    T *colbuf0 = buf + 2 * TILE + (k & 1) * TILE;
     // publish the current pivot row k and pivot column k (all register
     // indices compile-time; the owner test selects the live copy)
     const int kg = k / (TILE / C::GM), kl = k % 4, kt = (k % (TILE / C::GM)) / 4;
@@ -97,77 +102,45 @@ __device__ __forceinline__ void floyd_diag_close(T *mat, int64_t ld, int r0, T *
   __syncthreads();
 }
 
-// Phase 2/3 on one tile: D[ti][tj] = min(D[ti][tj], D[ti][tk] (x) D[tk][tj]).
-// Tile coordinates are in units of TILE.  Block-wide.
+// Phase 2/3 on one tile of part z: D[ti][tj] = min(D[ti][tj], D[ti][tk] (x)
+// D[tk][tj]).  mat is the part's matrix (ld = arena leading dimension);
+// mapA/mapB describe the arena with TILE x 16 and 16 x TILE boxes.
+// Block-wide; false if a TMA stage never completed.
 template <typename T, int TILE>
-__device__ __forceinline__ void floyd_tile_update(T *mat, int64_t ld, int ti, int tj, int tk,
-                                                  T *smem) {
+__device__ __forceinline__ bool floyd_tile_update(const CUtensorMap *mapA, const CUtensorMap *mapB,
+                                                  int z, T *mat, int64_t ld, int ti, int tj, int tk,
+                                                  TmaSmem<T, typename FloydCfg<T, TILE>::TC> &sm) {
   using C = typename FloydCfg<T, TILE>::C;
+  using TC = typename FloydCfg<T, TILE>::TC;
   T acc[C::TM][C::TN];
-  const int64_t r0 = (int64_t)ti * TILE, c0 = (int64_t)tj * TILE, k0 = (int64_t)tk * TILE;
+  const int64_t r0 = (int64_t)ti * TILE, c0 = (int64_t)tj * TILE;
   acc_load<T, C, true>(acc, mat + r0 * ld + c0, ld, 0, 0, 0, 0);
-  minplus_tile<T, C, true, false>(mat + r0 * ld + k0, ld, mat + k0 * ld + c0, ld, 0, 0, TILE, TILE,
-                           TILE, acc, smem);
-  acc_store<T, C, true>(acc, mat + r0 * ld + c0, ld, 0, 0, 0, 0);
+  const bool ok = tma_minplus_tile<T, TC>(mapA, tk * TILE, ti * TILE, z, mapB, tj * TILE, tk * TILE,
+                                          z, TILE, acc, sm);
+  if (ok) acc_store<T, C, true>(acc, mat + r0 * ld + c0, ld, 0, 0, 0, 0);
+  return ok;
 }
 
-// Closes one padded matrix (nb x nb tiles) with the calling CTA.
+// Closes one padded matrix (nb x nb tiles) of part z with the calling CTA.
 template <typename T, int TILE>
-__device__ void floyd_close_cta(T *mat, int64_t ld, int nb, T *smem) {
-  for (int kb = 0; kb < nb; kb++) {
-    floyd_diag_close<T, TILE>(mat, ld, kb * TILE, smem);
-    for (int j = 0; j < nb; j++)
-      if (j != kb) floyd_tile_update<T, TILE>(mat, ld, kb, j, kb, smem);
-    for (int i = 0; i < nb; i++)
-      if (i != kb) floyd_tile_update<T, TILE>(mat, ld, i, kb, kb, smem);
+__device__ bool floyd_close_cta(const CUtensorMap *mapA, const CUtensorMap *mapB, int z, T *mat,
+                                int64_t ld, int nb, TmaSmem<T, typename FloydCfg<T, TILE>::TC> &sm) {
+  bool ok = true;
+  for (int kb = 0; kb < nb && ok; kb++) {
+    floyd_diag_close<T, TILE>(mat, ld, kb * TILE, sm.ring);
+    for (int j = 0; j < nb && ok; j++)
+      if (j != kb) ok = floyd_tile_update<T, TILE>(mapA, mapB, z, mat, ld, kb, j, kb, sm);
+    for (int i = 0; i < nb && ok; i++)
+      if (i != kb) ok = floyd_tile_update<T, TILE>(mapA, mapB, z, mat, ld, i, kb, kb, sm);
     __syncthreads();
-    for (int i = 0; i < nb; i++) {
+    for (int i = 0; i < nb && ok; i++) {
       if (i == kb) continue;
-      for (int j = 0; j < nb; j++)
-        if (j != kb) floyd_tile_update<T, TILE>(mat, ld, i, j, kb, smem);
+      for (int j = 0; j < nb && ok; j++)
+        if (j != kb) ok = floyd_tile_update<T, TILE>(mapA, mapB, z, mat, ld, i, j, kb, sm);
     }
     __syncthreads();
   }
-}
-
-// ---- multi-launch form: one matrix, tiles across the GPU ----
-
-template <typename T, int TILE>
-__global__ void __launch_bounds__(FloydCfg<T, TILE>::THREADS)
-    floyd_phase1_kernel(T *mat, int64_t ld, int kb) {
-  extern __shared__ __align__(16) unsigned char fl_smem_raw[];
-  T *smem = reinterpret_cast<T *>(fl_smem_raw);
-  floyd_diag_close<T, TILE>(mat, ld, kb * TILE, smem);
-}
-
-// blockIdx.x in [0, 2*(nb-1)): first nb-1 are row-panel tiles, rest column.
-template <typename T, int TILE>
-__global__ void __launch_bounds__(FloydCfg<T, TILE>::THREADS)
-    floyd_phase2_kernel(T *mat, int64_t ld, int kb, int nb) {
-  extern __shared__ __align__(16) unsigned char fl_smem_raw[];
-  T *smem = reinterpret_cast<T *>(fl_smem_raw);
-  int t = blockIdx.x;
-  if (t < nb - 1) {
-    const int j = t < kb ? t : t + 1;
-    floyd_tile_update<T, TILE>(mat, ld, kb, j, kb, smem);
-  } else {
-    t -= nb - 1;
-    const int i = t < kb ? t : t + 1;
-    floyd_tile_update<T, TILE>(mat, ld, i, kb, kb, smem);
-  }
-}
-
-// blockIdx.x over the (nb-1)^2 remainder tiles.
-template <typename T, int TILE>
-__global__ void __launch_bounds__(FloydCfg<T, TILE>::THREADS)
-    floyd_phase3_kernel(T *mat, int64_t ld, int kb, int nb) {
-  extern __shared__ __align__(16) unsigned char fl_smem_raw[];
-  T *smem = reinterpret_cast<T *>(fl_smem_raw);
-  const int t = blockIdx.x;
-  int i = t / (nb - 1), j = t % (nb - 1);
-  i = i < kb ? i : i + 1;
-  j = j < kb ? j : j + 1;
-  floyd_tile_update<T, TILE>(mat, ld, i, j, kb, smem);
+  return ok;
 }
 
 }  // namespace fapb

@@ -1,0 +1,79 @@
+// Tensor Memory Accelerator (TMA) helpers for sm_100a: mbarrier wrappers,
+// tiled bulk tensor loads into shared memory (no multicast), and a bounded
+// wait that reports a timeout instead of spinning forever.
+#pragma once
+
+#include <cuda.h>
+#include <stdint.h>
+
+#include "fap_common.cuh"
+
+namespace fapb {
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+// Makes initialised mbarriers visible to the async (TMA) proxy.
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Orders this thread's generic-proxy shared-memory accesses before later
+// async-proxy (TMA) accesses.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Orders this thread's earlier generic-proxy accesses (shared and global)
+// before later async-proxy (TMA) accesses, e.g. a tile this CTA just stored
+// and now loads with TMA.
+__device__ __forceinline__ void fence_proxy_async_all() {
+  asm volatile("fence.proxy.async;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Waits for the phase with the given parity to complete; gives up after a
+// bounded number of polls (each poll may suspend the thread briefly) and
+// returns false.
+constexpr uint32_t kMbarPollLimit = 1u << 26;
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+  for (uint32_t i = 0; i < kMbarPollLimit; i++)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+// 3-D tiled load of one box into shared memory; completion is counted on
+// `bar` in bytes.  The destination is this CTA's own shared memory; no
+// multicast.  The innermost coordinate x must be a multiple of 4 (16 bytes of
+// 32-bit elements): callers only pass multiples of their 16-element chunks.
+__device__ __forceinline__ void tma_load_3d(void *smem_dst, const CUtensorMap *map, int x, int y, int z,
+                                            uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(smem_dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+
+}  // namespace fapb
