@@ -145,6 +145,14 @@ struct fap_dgraph {
   int64_t sssp_max_rounds = -1;  // <0: 8n + 1024
   bool floyd_per_cta = false;     // batched Floyd: one CTA per part instead of per-tile launches
   int sssp_chain = 0;             // SSSP chain-following budget (hops per thread per round)
+  // CUDA graph of the batched launch sequence (replayed while nothing that
+  // it captured changes: batch, buffers, parameters, stream)
+  bool use_graph = true;
+  uint64_t epoch = 1;
+  cudaGraphExec_t gexec = nullptr;
+  uint64_t gexec_epoch = 0;
+  cudaStream_t gexec_stream = nullptr;
+  int64_t gexec_launches = 0;
   // last solve
   int last_mode = -1;
   float timing[5] = {-1, -1, -1, -1, -1};
@@ -324,6 +332,7 @@ extern "C" int fap_graph_destroy(fap_dgraph *G) {
   {
     DeviceGuard g(c->device);
     cudaStreamSynchronize(c->stream);
+    if (G->gexec) cudaGraphExecDestroy(G->gexec);
     for (DevBuf *b : {&G->ro, &G->col, &G->w, &G->ro_s, &G->col_s, &G->w_s, &G->sssp_scratch, &G->d_thin,
                       &G->d_gid, &G->d_st2ed, &G->d_ed2st, &G->D, &G->F, &G->d_parts, &G->d_work,
                       &G->d_src, &G->d_srcrows, &G->d_status, &G->d_checks, &G->staging})
@@ -414,6 +423,7 @@ extern "C" int fap_graph_reserve(fap_dgraph *G, int64_t max_rows) {
   G->max_rows = max_rows;
   std::fill(G->row_base.begin(), G->row_base.end(), -1);
   G->last_ids.clear();
+  G->epoch++;
   return FAP_OK;
 }
 
@@ -508,6 +518,7 @@ int prepare_batch(fap_dgraph *G, const std::vector<int32_t> &ids) {
   // Rows of other parts may have been overwritten by this batch.
   std::fill(G->row_base.begin(), G->row_base.end(), -1);
   G->last_ids = ids;
+  G->epoch++;
   return FAP_OK;
 }
 
@@ -625,8 +636,40 @@ extern "C" int fap_solve(fap_dgraph *G, const int32_t *parts, int32_t count, int
   DeviceGuard g(G->ctx->device);
   if (G->max_rows == 0) FAP_TRY(fap_graph_reserve(G, 0));
   FAP_TRY(prepare_batch(G, ids));
-  int rc = (G->dtype == FAP_DTYPE_I32) ? run_solve<int32_t>(G, mode) : run_solve<float>(G, mode);
-  if (rc != FAP_OK) return rc;
+  int rc = FAP_OK;
+  cudaStream_t st = G->ctx->stream;
+  if (mode == FAP_MODE_BATCHED && G->use_graph && st != nullptr) {
+    if (!G->gexec || G->gexec_epoch != G->epoch || G->gexec_stream != st) {
+      if (G->gexec) cudaGraphExecDestroy(G->gexec);
+      G->gexec = nullptr;
+      // Capture the whole batched launch sequence once; replay it while the
+      // batch, its buffers, the parameters and the stream stay the same.
+      FAP_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      rc = (G->dtype == FAP_DTYPE_I32) ? run_solve<int32_t>(G, mode) : run_solve<float>(G, mode);
+      cudaGraph_t graph = nullptr;
+      const cudaError_t ec = cudaStreamEndCapture(st, &graph);
+      if (rc != FAP_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+      }
+      if (ec != cudaSuccess) return fail(FAP_ERR_CUDA, "stream capture: %s", cudaGetErrorString(ec));
+      const cudaError_t ei = cudaGraphInstantiate(&G->gexec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ei != cudaSuccess) {
+        G->gexec = nullptr;
+        return fail(FAP_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ei));
+      }
+      G->gexec_epoch = G->epoch;
+      G->gexec_stream = st;
+      G->gexec_launches = G->launches;
+    }
+    FAP_CK(cudaGraphLaunch(G->gexec, st));
+    G->launches = G->gexec_launches;
+    G->ctx->launches += G->launches;
+  } else {
+    rc = (G->dtype == FAP_DTYPE_I32) ? run_solve<int32_t>(G, mode) : run_solve<float>(G, mode);
+    if (rc != FAP_OK) return rc;
+  }
   for (const PartDesc &d : G->parts) G->row_base[d.part] = d.row_base;
   G->last_mode = mode;
   return FAP_OK;
@@ -915,6 +958,11 @@ extern "C" int fap_graph_sssp_rows(fap_dgraph *G, const int32_t *sources, int32_
 
 extern "C" int fap_graph_set_param(fap_dgraph *G, const char *key, double value) {
   if (!G || !key) return fail(FAP_ERR_INVALID, "NULL argument");
+  G->epoch++;  // a captured launch sequence no longer matches
+  if (std::strcmp(key, "cuda_graph") == 0) {
+    G->use_graph = value != 0.0;
+    return FAP_OK;
+  }
   if (std::strcmp(key, "sssp_delta") == 0) {
     G->sssp_delta = (value > 0 && value < 1e8) ? value : -1.0;
     return FAP_OK;

@@ -135,6 +135,15 @@ def test_plain_and_batched_blocks_identical(cuda_ok):
         for x, y in zip(a, b):
             np.testing.assert_array_equal(x, y)
         np.testing.assert_array_equal(np.concatenate(a), case["row_checksums"])
+        dg.set_param("cuda_graph", 0)      # direct launches instead of the captured graph
+        dg.solve(mode=FAP_MODE_BATCHED)
+        c0 = [dg.block_checksums(p) for p in range(1, case["K"] + 1)]
+        np.testing.assert_array_equal(np.concatenate(c0), case["row_checksums"])
+        dg.set_param("cuda_graph", 1)
+        for _ in range(2):                  # replays of the captured graph
+            dg.solve(mode=FAP_MODE_BATCHED)
+        c1 = [dg.block_checksums(p) for p in range(1, case["K"] + 1)]
+        np.testing.assert_array_equal(np.concatenate(c1), case["row_checksums"])
         dg.set_param("floyd_per_cta", 1)   # the one-CTA-per-part Floyd form
         dg.solve(mode=FAP_MODE_BATCHED)
         c = [dg.block_checksums(p) for p in range(1, case["K"] + 1)]
