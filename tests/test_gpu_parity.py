@@ -144,6 +144,8 @@ def test_plain_and_batched_blocks_identical(cuda_ok):
             dg.solve(mode=FAP_MODE_BATCHED)
         c1 = [dg.block_checksums(p) for p in range(1, case["K"] + 1)]
         np.testing.assert_array_equal(np.concatenate(c1), case["row_checksums"])
+        t = dg.last_timing()            # stage events recorded inside the graph
+        assert t[4] > 0 and np.all(t[:4] >= 0) and abs(t[:4].sum() - t[4]) < 0.05 * t[4] + 0.05
         dg.set_param("floyd_per_cta", 1)   # the one-CTA-per-part Floyd form
         dg.solve(mode=FAP_MODE_BATCHED)
         c = [dg.block_checksums(p) for p in range(1, case["K"] + 1)]
