@@ -50,6 +50,15 @@ int fail(int code, const char *fmt, ...) {
     if (r_ != FAP_OK) return r_; \
   } while (0)
 
+// Records ev on st; inside a stream capture the record becomes an event node
+// of the graph, so the host can still time the replayed stages.
+cudaError_t record_event(cudaEvent_t ev, cudaStream_t st) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) cs = cudaStreamCaptureStatusNone;
+  return cs == cudaStreamCaptureStatusActive ? cudaEventRecordWithFlags(ev, st, cudaEventRecordExternal)
+                                             : cudaEventRecord(ev, st);
+}
+
 struct DevBuf {
   void *p = nullptr;
   size_t bytes = 0;
@@ -558,12 +567,12 @@ int run_solve(fap_dgraph *G, int mode) {
   FAP_CK(cudaMemsetAsync(status, 0, sizeof(int), st));
   for (int i = 0; i < 5; i++) G->timing[i] = -1.0f;
   if (mode == FAP_MODE_BATCHED) {
-    FAP_CK(cudaEventRecordWithFlags(c->ev[0], st, cudaEventRecordExternal));
+    FAP_CK(record_event(c->ev[0], st));
     FAP_CK(launch_sssp<T>(ro_s, col_s, w_s, G->n, src, srow, (int)G->src.size(), D, G->ldD, G->ldD,
                           ed2st, scratch, delta, G->sssp_chain, max_rounds, status, st, &L));
-    FAP_CK(cudaEventRecordWithFlags(c->ev[1], st, cudaEventRecordExternal));
+    FAP_CK(record_event(c->ev[1], st));
     FAP_CK(launch_gather<T>(dp, np, G->max_ldf, ro, col, w, gid, st2ed, ed2st, D, G->ldD, F, st, &L));
-    FAP_CK(cudaEventRecordWithFlags(c->ev[2], st, cudaEventRecordExternal));
+    FAP_CK(record_event(c->ev[2], st));
     if (G->floyd_per_cta) {
       FAP_CK(launch_floyd_parts<T>(dp, np, F, G->max_ldf, D, G->ldD, st2ed, status, st, &L));
     } else {
@@ -571,14 +580,14 @@ int run_solve(fap_dgraph *G, int mode) {
                                          status, st, &L));
       FAP_CK(launch_bdy_scatter<T>(dp, np, F, D, G->ldD, st2ed, G->max_b, G->max_s, st, &L));
     }
-    FAP_CK(cudaEventRecordWithFlags(c->ev[3], st, cudaEventRecordExternal));
+    FAP_CK(record_event(c->ev[3], st));
     FAP_CK(launch_minplus_thin<T>(dp, G->d_thin.as<int32_t>(), (int)G->thin.size(), G->n, F, D,
                                   G->ldD, gid, ed2st, st, &L));
     FAP_CK(launch_minplus_parts<T>(dp, np, dw, (int)G->work.size(), G->n, F, G->max_ldf, D, G->ldD,
                                    G->max_rows, gid, ed2st, status, st, &L));
-    FAP_CK(cudaEventRecordWithFlags(c->ev[4], st, cudaEventRecordExternal));
+    FAP_CK(record_event(c->ev[4], st));
   } else {
-    FAP_CK(cudaEventRecordWithFlags(c->ev[0], st, cudaEventRecordExternal));
+    FAP_CK(record_event(c->ev[0], st));
     for (int i = 0; i < np; i++) {
       const PartDesc &d = G->parts[i];
       const int s0 = G->part_src_off[i], s1 = G->part_src_off[i + 1];
@@ -595,7 +604,7 @@ int run_solve(fap_dgraph *G, int mode) {
         FAP_CK(launch_minplus_parts<T>(dp, np, dw + w0, w1 - w0, G->n, F, G->max_ldf, D, G->ldD,
                                        G->max_rows, gid, ed2st, status, st, &L));
     }
-    FAP_CK(cudaEventRecordWithFlags(c->ev[4], st, cudaEventRecordExternal));
+    FAP_CK(record_event(c->ev[4], st));
   }
   G->launches = L;
   c->launches += L;
@@ -871,12 +880,12 @@ extern "C" int fap_measure_relax_peak(fap_ctx *c, int dtype, double *relax_per_s
   double count = 0;
   float best = 1e30f;
   for (int rep = 0; rep < 4; rep++) {
-    FAP_CK(cudaEventRecordWithFlags(c->ev[0], st, cudaEventRecordExternal));
+    FAP_CK(record_event(c->ev[0], st));
     if (dtype == FAP_DTYPE_I32)
       FAP_CK(launch_relax_peak<int32_t>(c->sink.as<int32_t>(), blocks, iters, st, &count));
     else
       FAP_CK(launch_relax_peak<float>(c->sink.as<float>(), blocks, iters, st, &count));
-    FAP_CK(cudaEventRecordWithFlags(c->ev[1], st, cudaEventRecordExternal));
+    FAP_CK(record_event(c->ev[1], st));
     FAP_CK(cudaEventSynchronize(c->ev[1]));
     float t;
     FAP_CK(cudaEventElapsedTime(&t, c->ev[0], c->ev[1]));
