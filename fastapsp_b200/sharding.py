@@ -54,3 +54,24 @@ def reduce_over_ranks(x: float, op: str = "max", device=None) -> float:
     t = torch.tensor([float(x)], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
     return float(t.item())
+
+
+def group_parts_by_rows(parts: Sequence[int], ver_num: Sequence[int], max_rows: int) -> List[List[int]]:
+    """Split `parts` (in order) into consecutive groups whose row counts fit
+    in max_rows -- the output of a graph too large for device memory is
+    produced group by group into one reserved row budget."""
+    groups: List[List[int]] = []
+    cur: List[int] = []
+    rows = 0
+    for p in parts:
+        r = int(ver_num[p])
+        if r > max_rows:
+            raise ValueError(f"part {p} has {r} rows, more than the budget of {max_rows}")
+        if cur and rows + r > max_rows:
+            groups.append(cur)
+            cur, rows = [], 0
+        cur.append(p)
+        rows += r
+    if cur:
+        groups.append(cur)
+    return groups

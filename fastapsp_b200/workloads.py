@@ -32,6 +32,21 @@ class Workload:
     def csr(self):
         return self.graph.csr()
 
+    def data_description(self) -> str:
+        info = self.edges.info
+        kind = info.get("kind")
+        if kind == "road":
+            return ("synthetic: seeded road-shaped graph (uniform points, Euclidean MST + "
+                    "nearest-neighbour edges), int weights U[1,1000]")
+        if kind == "grid":
+            return (f"synthetic: seeded {info['rows']}x{info['cols']} grid, "
+                    f"{info['drop_frac']:.0%} edges dropped, {info['extra_frac']:.0%} extra random "
+                    "edges, int weights")
+        if kind == "rmat":
+            return ("synthetic: seeded directed R-MAT (0.57, 0.19, 0.19, 0.05), self-loops dropped, "
+                    "duplicates kept, float weights log-uniform [0.01, 100]")
+        return "synthetic"
+
     def describe(self) -> dict:
         vn, bn = self.ver_num[1:], self.bdy_num[1:]
         return {"workload": self.name, "n": self.n, "arcs": int(self.graph.csr()[0][-1]),
