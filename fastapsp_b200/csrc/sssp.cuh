@@ -12,15 +12,17 @@
 //     graphs, and METIS parts are compact -- touches nearby addresses.  The
 //     CTA then works on a scratch row and finally writes the output row in
 //     original column order (out[v] = dist[ed2st[v]]).
-//   - Frontier: a work queue in shared memory, deduplicated by one bitmap of
-//     n bits ("queued").  A round processes the queue and pushes improved
-//     vertices to the other queue, so its cost follows the frontier, not n.
-//     When a queue overflows, the vertices stay marked in the bitmap and the
-//     next round collects them with a block-wide scan of the bitmap instead.
+//   - Frontier: a pair of bitmaps in shared memory (n bits each); dedup is
+//     free.  Each round compacts the set bits into a shared list with a block
+//     scan, so active vertices are spread evenly over the threads.
 //   - Expansion: a thread relaxes a light vertex's edges with all loads and
 //     atomics of a 4-edge group in flight at once; vertices with more than
 //     kHeavyDeg edges are expanded by a whole warp (lane-strided, coalesced
 //     column/weight reads).
+//   - Chains: a thread that improves a near neighbour expands it at once
+//     (up to `chain` hops per round) instead of leaving it for the next
+//     round, so a hop along a path costs one load + atomic latency rather
+//     than a whole round.
 //   - Order: near/far (delta stepping).  A frontier vertex whose distance is
 //     not below the threshold stays in the bitmap; when no near vertex is
 //     left, the threshold moves to (smallest far distance + delta).
@@ -35,13 +37,13 @@
 namespace fapb {
 
 constexpr int kSsspThreads = 256;
-constexpr int kSsspQueue = 2048;  // entries per frontier queue (two queues)
+constexpr int kSsspList = 2048;   // compacted frontier entries per pass
 constexpr int kHeavyDeg = 32;     // vertices above this degree go to a warp
 constexpr int kHeavyList = 256;
 
 // Shared-memory bytes a CTA needs for n vertices (dynamic part).
 inline size_t sssp_smem_bytes(int n) {
-  return (size_t)ceil_div(n, 32) * sizeof(uint32_t) + (2 * kSsspQueue + kHeavyList) * sizeof(int32_t);
+  return 2 * (size_t)ceil_div(n, 32) * sizeof(uint32_t) + (kSsspList + kHeavyList) * sizeof(int32_t);
 }
 
 template <typename T>
@@ -88,25 +90,53 @@ __device__ __forceinline__ int block_excl_scan(int x, int *warp_tmp, int *total)
   return warp_tmp[wid] + inc - x;
 }
 
-// Frontier push: marks v in the queued bitmap and, if it was not marked,
-// appends it to the next queue (or flags an overflow, leaving it marked).
-__device__ __forceinline__ void frontier_push(int v, uint32_t *queued, int32_t *nextq, int *ncount,
-                                              int *novf) {
-  const uint32_t bit = 1u << (v & 31);
-  if (!(atomicOr(queued + (v >> 5), bit) & bit)) {
-    const int p = atomicAdd(ncount, 1);
-    if (p < kSsspQueue) nextq[p] = v;
-    else *novf = 1;
+// Relaxes edges [e0, e1) of a light vertex at distance du.  One improved
+// neighbour inside the current bucket may be handed back in *next / *dnext
+// (chain-following: the caller expands it at once instead of a round later);
+// every other improved neighbour gets its frontier bit.  Returns whether a bit
+// was set.
+template <typename T>
+__device__ __forceinline__ bool relax_edges_chain(const int32_t *__restrict__ col,
+                                                  const T *__restrict__ w, int e0, int e1, T du,
+                                                  T *dist, uint32_t *nb, T thresh, bool may_chain,
+                                                  int *next, T *dnext) {
+  bool any = false;
+  *next = -1;
+  for (int e = e0; e < e1; e += 4) {
+    int v[4];
+    T nd[4], cur[4], old[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int ek = e + k;
+      v[k] = ek < e1 ? __ldg(col + ek) : -1;
+      nd[k] = ek < e1 ? du + __ldg(w + ek) : du;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) cur[k] = v[k] >= 0 ? ld_relaxed(dist + v[k]) : du;
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+      old[k] = (v[k] >= 0 && nd[k] < cur[k]) ? Dist<T>::atomic_min(dist + v[k], nd[k]) : nd[k];
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+      if (nd[k] < old[k]) {
+        if (may_chain && *next < 0 && nd[k] < thresh) {
+          *next = v[k];
+          *dnext = nd[k];
+        } else {
+          atomicOr(nb + (v[k] >> 5), 1u << (v[k] & 31));
+          any = true;
+        }
+      }
   }
+  return any;
 }
 
-// Relaxes edges [e0, e1) (every stride-th) of a vertex at distance du with
-// 4 loads and 4 atomics in flight; pushes every improved neighbour.  Returns
-// whether anything improved.
+// Relaxes edges [e0, e1) of a vertex at distance du; sets the frontier bit
+// of every improved neighbour.  Returns whether anything improved.
 template <typename T>
 __device__ __forceinline__ bool relax_edges(const int32_t *__restrict__ col, const T *__restrict__ w,
                                             int e0, int e1, int stride, T du, T *dist,
-                                            uint32_t *queued, int32_t *nextq, int *ncount, int *novf) {
+                                            uint32_t *nb) {
   bool any = false;
   for (int e = e0; e < e1; e += 4 * stride) {
     int v[4];
@@ -125,7 +155,7 @@ __device__ __forceinline__ bool relax_edges(const int32_t *__restrict__ col, con
 #pragma unroll
     for (int k = 0; k < 4; k++)
       if (nd[k] < old[k]) {
-        frontier_push(v[k], queued, nextq, ncount, novf);
+        atomicOr(nb + (v[k] >> 5), 1u << (v[k] & 31));
         any = true;
       }
   }
@@ -137,20 +167,19 @@ __device__ __forceinline__ bool relax_edges(const int32_t *__restrict__ col, con
 // CTA) and out[v] = dist[perm_out[v]] is written at the end; otherwise dist is
 // the output row itself.
 template <typename T>
-__global__ void __launch_bounds__(kSsspThreads, 4)
+__global__ void __launch_bounds__(kSsspThreads)
     sssp_frontier_kernel(const int32_t *__restrict__ row_offset, const int32_t *__restrict__ col,
                          const T *__restrict__ w, int n, const int32_t *__restrict__ sources,
                          const int64_t *__restrict__ out_rows, int num_sources, T *out, int64_t ld,
                          int64_t init_cols, const int32_t *__restrict__ perm_out, T *scratch,
-                         T delta, int64_t max_rounds, int *status) {
-  extern __shared__ uint32_t queued[];
+                         T delta, int chain, int64_t max_rounds, int *status) {
+  extern __shared__ uint32_t sm_bits[];
   __shared__ int32_t s_minfar[3];
   __shared__ int s_warp[kSsspThreads / 32];
   __shared__ int s_total, s_nheavy;
-  __shared__ int s_cnt[2], s_ovf[2];  // queue fill and overflow flag, by round parity
   const int nwords = (int)ceil_div(n, 32);
-  int32_t *const qbase = reinterpret_cast<int32_t *>(queued + nwords);  // two queues
-  int32_t *const heavy = qbase + 2 * kSsspQueue;
+  int32_t *act = reinterpret_cast<int32_t *>(sm_bits + 2 * nwords);
+  int32_t *heavy = act + kSsspList;
   const T inf = Dist<T>::inf();
   const int32_t inf_bits = order_bits<T>(inf + inf);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -165,119 +194,90 @@ __global__ void __launch_bounds__(kSsspThreads, 4)
     }
     const int64_t init = perm_out ? n : init_cols;
     for (int64_t v = threadIdx.x; v < init; v += blockDim.x) dist[v] = inf;
-    for (int i = threadIdx.x; i < nwords; i += blockDim.x) queued[i] = 0;
+    for (int i = threadIdx.x; i < 2 * nwords; i += blockDim.x) sm_bits[i] = 0;
     if (threadIdx.x < 3) s_minfar[threadIdx.x] = inf_bits;
     __syncthreads();
     if (threadIdx.x == 0) {
       dist[src] = T(0);
-      queued[src >> 5] = 1u << (src & 31);
-      qbase[0] = src;
-      s_cnt[0] = 1;
-      s_ovf[0] = 0;
-      s_cnt[1] = 0;
-      s_ovf[1] = 0;
+      sm_bits[src >> 5] = 1u << (src & 31);
     }
     __syncthreads();
     T thresh = delta;  // identical in every thread
+    int cur = 0;
     for (int64_t round = 0;; round++) {
       if (round >= max_rounds) {
         if (threadIdx.x == 0) set_status(status, kDevSsspRoundLimit);
         break;
       }
-      const int cur = (int)(round & 1), nxt = cur ^ 1;
       const int slot = (int)(round % 3);
       if (threadIdx.x == 0) s_minfar[(slot + 1) % 3] = inf_bits;
-      const int cnt = s_cnt[cur];
-      const bool scan = s_ovf[cur] != 0;
-      int32_t *const list = qbase + cur * kSsspQueue;
-      int32_t *const nextq = qbase + nxt * kSsspQueue;
+      uint32_t *cb = sm_bits + cur * nwords, *nb = sm_bits + (cur ^ 1) * nwords;
       int any = 0, far = 0;
       int32_t minfar = inf_bits;
-      // Expand one frontier vertex (its queued bit already cleared).
-      auto expand = [&](int u) {
-        const T du = ld_relaxed(dist + u);
-        if (!(du < thresh)) {  // far: keep it for a later bucket
-          frontier_push(u, queued, nextq, &s_cnt[nxt], &s_ovf[nxt]);
-          minfar = min(minfar, order_bits<T>(du));
-          far = 1;
-          return;
+      // Passes of at most kSsspList frontier vertices each.
+      for (;;) {
+        int cnt = 0;
+        for (int wi = threadIdx.x; wi < nwords; wi += blockDim.x) cnt += __popc(cb[wi]);
+        const int off = block_excl_scan(cnt, s_warp, &s_total);
+        const int total = s_total;
+        if (total == 0) break;
+        if (threadIdx.x == 0) s_nheavy = 0;
+        // Move the first kSsspList set bits (in thread order) to the list.
+        int pos = off;
+        for (int wi = threadIdx.x; wi < nwords && pos < kSsspList; wi += blockDim.x) {
+          uint32_t m = cb[wi];
+          if (!m) continue;
+          uint32_t taken = 0;
+          while (m && pos < kSsspList) {
+            const int b = __ffs(m) - 1;
+            m &= m - 1;
+            act[pos++] = (wi << 5) + b;
+            taken |= 1u << b;
+          }
+          cb[wi] &= ~taken;
         }
-        const int e0 = __ldg(row_offset + u), e1 = __ldg(row_offset + u + 1);
-        if (e1 - e0 > kHeavyDeg) {
-          const int h = atomicAdd(&s_nheavy, 1);
-          if (h < kHeavyList) {
-            heavy[h] = u;
-            return;
+        __syncthreads();
+        const int take = min(total, kSsspList);
+        for (int i = threadIdx.x; i < take; i += blockDim.x) {
+          const int u = act[i];
+          const T du = ld_relaxed(dist + u);
+          if (!(du < thresh)) {  // far: expand in a later bucket
+            atomicOr(nb + (u >> 5), 1u << (u & 31));
+            minfar = min(minfar, order_bits<T>(du));
+            far = 1;
+            continue;
+          }
+          // Expand u, then follow improved near neighbours in this thread.
+          int x = u;
+          T dx = du;
+          for (int hop = 0;; hop++) {
+            const int e0 = __ldg(row_offset + x), e1 = __ldg(row_offset + x + 1);
+            if (e1 - e0 > kHeavyDeg) {
+              const int h = atomicAdd(&s_nheavy, 1);
+              if (h < kHeavyList) {
+                heavy[h] = x;
+                break;
+              }
+            }
+            int nx;
+            T dn;
+            any |= relax_edges_chain<T>(col, w, e0, e1, dx, dist, nb, thresh, hop < chain, &nx, &dn);
+            if (nx < 0) break;
+            x = nx;
+            dx = dn;
           }
         }
-        any |= relax_edges<T>(col, w, e0, e1, 1, du, dist, queued, nextq, &s_cnt[nxt], &s_ovf[nxt]);
-      };
-      auto heavy_pass = [&]() {
+        __syncthreads();
+        // Heavy vertices: one warp each, lanes stride over the edges.
         const int nh = min(s_nheavy, kHeavyList);
         for (int h = wid; h < nh; h += kSsspThreads / 32) {
           const int u = heavy[h];
           const T du = ld_relaxed(dist + u);
           const int e0 = __ldg(row_offset + u), e1 = __ldg(row_offset + u + 1);
-          any |= relax_edges<T>(col, w, e0 + lane, e1, 32, du, dist, queued, nextq, &s_cnt[nxt],
-                                &s_ovf[nxt]);
-        }
-      };
-      if (!scan) {
-        // Queue round: the frontier is list[0, cnt).
-        if (threadIdx.x == 0) s_nheavy = 0;
-        __syncthreads();
-        for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
-          const int u = list[i];
-          atomicAnd(queued + (u >> 5), ~(1u << (u & 31)));
-          expand(u);
+          any |= relax_edges<T>(col, w, e0 + lane, e1, 32, du, dist, nb);
         }
         __syncthreads();
-        // every thread has read s_cnt[cur]: reset it for the round after next
-        if (threadIdx.x == 0) {
-          s_cnt[cur] = 0;
-          s_ovf[cur] = 0;
-        }
-        heavy_pass();
-      } else {
-        // Overflow round: collect every marked vertex from the bitmap, in
-        // passes of at most kSsspQueue (the current queue is reused as the
-        // list; nothing pushes into it this round).
-        for (;;) {
-          int c = 0;
-          for (int wi = threadIdx.x; wi < nwords; wi += blockDim.x) c += __popc(queued[wi]);
-          const int off = block_excl_scan(c, s_warp, &s_total);
-          const int total = s_total;
-          if (total == 0) break;
-          if (threadIdx.x == 0) s_nheavy = 0;
-          int pos = off;
-          for (int wi = threadIdx.x; wi < nwords && pos < kSsspQueue; wi += blockDim.x) {
-            uint32_t m = queued[wi];
-            if (!m) continue;
-            uint32_t taken = 0;
-            while (m && pos < kSsspQueue) {
-              const int b = __ffs(m) - 1;
-              m &= m - 1;
-              list[pos++] = (wi << 5) + b;
-              taken |= 1u << b;
-            }
-            queued[wi] &= ~taken;  // no pushes run during collection
-          }
-          __syncthreads();
-          const int take = min(total, kSsspQueue);
-          for (int i = threadIdx.x; i < take; i += blockDim.x) expand(list[i]);
-          __syncthreads();
-          heavy_pass();
-          __syncthreads();
-          // Vertices pushed during this pass are marked again; the next
-          // round picks them up (from the queue, or by another scan).
-          if (total <= kSsspQueue) break;
-          // more marked vertices than one pass: the pushes of this pass are in
-          // the bitmap as well, so keep collecting from it
-        }
-        if (threadIdx.x == 0) {
-          s_cnt[cur] = 0;
-          s_ovf[cur] = 0;
-        }
+        if (total <= kSsspList) break;
       }
       if (far) atomicMin(&s_minfar[slot], minfar);
       const int active = __syncthreads_or(any);
@@ -288,6 +288,7 @@ __global__ void __launch_bounds__(kSsspThreads, 4)
         const T mf = from_order_bits<T>(s_minfar[slot]);
         thresh = (mf >= inf - delta) ? inf + inf : mf + delta;
       }
+      cur ^= 1;
     }
     __syncthreads();
     if (perm_out) {

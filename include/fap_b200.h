@@ -141,7 +141,8 @@ FAP_API int fap_graph_sssp_rows(fap_dgraph *g, const int32_t *sources, int32_t c
  * FAP_ERR_NOT_CONVERGED; <= 0 restores the default 8n + 1024);
  * "floyd_per_cta" (non-zero: the batched Floyd closes each part's matrix
  * with one CTA instead of per-tile launches across all parts);
- * "cuda_graph" (non-zero, the default:
+ * "sssp_chain" (hops a thread may follow within one SSSP round; 0 turns
+ * chain-following off, the default); "cuda_graph" (non-zero, the default:
  * a batched solve captures its launch sequence in a CUDA graph on first use
  * and replays it while the batch, buffers, parameters and stream are
  * unchanged). */
