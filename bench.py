@@ -308,6 +308,10 @@ def main_fap(args):
     def solve_all(mode):
         for grp in groups:
             dg.solve(grp, mode, check_errors=False)
+    from fastapsp_b200 import autotune
+    tuned = autotune.tune_sssp(dg, vn, bn)
+    log(f"SSSP delta {tuned['delta']:.6g} ({'cached' if tuned['cached'] else 'tuned'}: "
+        f"{tuned['key']}, factor {tuned['factor']})")
     relax_peak = ctx.relax_peak(dtype)
     hbm_peak, peak_kind = read_peaks()
 
@@ -466,6 +470,8 @@ def main_fap(args):
             "data": wl.data_description(),
             "config": {**wl.describe(), "mode": "batched", "parallelism": f"parts sharded x{world}",
                        "groups": len(groups),
+                       "sssp_delta": {"value": tuned["delta"], "factor_of_mean_weight": tuned["factor"],
+                                      "bucket": tuned["key"], "from_cache": tuned["cached"]},
                        "l2": "256 MB buffer written between timed steps (outside the events); "
                              f"each step also writes {4 * n * n / 1e9:.1f} GB of output"},
             "plain": {"value": plain_value, "ms_per_step": plain_max / max(len(plain_ms), 1),

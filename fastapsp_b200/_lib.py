@@ -85,6 +85,8 @@ _SIGS = {
     "fap_op_floyd": (INT, [P, INT, I32, P, I64]),
     "fap_op_minplus": (INT, [P, INT, I32, I32, I32, P, I64, P, I64, P, I64]),
     "fap_measure_relax_peak": (INT, [P, INT, ctypes.POINTER(DBL)]),
+    "fap_graph_tune_sssp": (INT, [P, P, I32, I32, ctypes.POINTER(DBL), P]),
+    "fap_graph_mean_weight": (DBL, [P]),
     "fap_floyd_noalloc": (INT, [INT, I32, P, I64, P]),
     "fap_floyd_noalloc_last_error": (ctypes.c_char_p, []),
     "fap_legacy_last_status": (INT, []),

@@ -1,0 +1,85 @@
+"""Autotuner for the SSSP bucket width (delta), cached per (part size,
+boundary count) bucket.
+
+The best delta depends on the graph: on road-like graphs with deep
+shortest-path trees wide buckets win (few rounds), on small-world graphs
+narrow buckets win (fewer re-relaxations).  The tuner times the SSSP stage
+on one wave of boundary sources for delta = f x (mean edge weight), f in
+FACTORS, plus plain Bellman-Ford, and stores the winning factor (scale-free)
+under a key built from the dtype, the median part size and the median
+boundary count, each rounded to a power of two.  The cache is a JSON file:
+$FAP_TUNE_CACHE, else ~/.cache/fastapsp_b200/autotune.json.
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+import tempfile
+
+import numpy as np
+
+FACTORS = (1, 2, 4, 8, 16, 32, 64, 128, 256)
+BF = None  # factor recorded when plain Bellman-Ford wins
+
+
+def cache_path() -> str:
+    p = os.environ.get("FAP_TUNE_CACHE")
+    if p:
+        return p
+    return os.path.join(os.path.expanduser("~"), ".cache", "fastapsp_b200", "autotune.json")
+
+
+def bucket_key(ver_num, bdy_num, dtype: int) -> str:
+    vn = np.asarray(ver_num)[1:]
+    bn = np.asarray(bdy_num)[1:]
+    nsub = max(1.0, float(np.median(vn)))
+    nbdy = float(np.median(bn))
+    return (f"{'i32' if dtype == 0 else 'f32'}:nsub~2^{round(math.log2(nsub))}"
+            f":nbdy~2^{round(math.log2(nbdy + 1))}")
+
+
+def _load(path):
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def _save(path, data):
+    d = os.path.dirname(path)
+    if d:
+        os.makedirs(d, exist_ok=True)
+    fd, tmp = tempfile.mkstemp(dir=d or ".", suffix=".tmp")
+    with os.fdopen(fd, "w") as f:
+        json.dump(data, f, indent=1, sort_keys=True)
+    os.replace(tmp, path)
+
+
+def tune_sssp(dg, ver_num, bdy_num, *, path: str | None = None, force: bool = False) -> dict:
+    """Sets dg's SSSP delta from the cache, or tunes it (and caches it).
+    Returns the cache entry plus 'key', 'delta' and 'cached'."""
+    path = path or cache_path()
+    key = bucket_key(ver_num, bdy_num, dg.dtype)
+    mw = dg.mean_weight()
+    cache = _load(path)
+    entry = cache.get(key)
+    if entry is not None and not force:
+        f = entry.get("factor")
+        delta = 1e9 if f is None else f * mw
+        dg.set_param("sssp_delta", delta)
+        return {**entry, "key": key, "delta": delta, "cached": True}
+    cands = [f * mw for f in FACTORS] + [1e9]
+    best, ms = dg.tune_sssp(cands)
+    best_i = int(np.argmin(ms))
+    factor = BF if best_i == len(FACTORS) else FACTORS[best_i]
+    entry = {"factor": factor, "ms": [round(float(x), 4) for x in ms],
+             "factors": list(FACTORS) + ["bellman-ford"]}
+    cache[key] = entry
+    try:
+        _save(path, cache)
+    except OSError:
+        pass  # a read-only home: the tuned value still applies to dg
+    delta = 1e9 if factor is None else factor * mw
+    return {**entry, "key": key, "delta": delta, "cached": False}

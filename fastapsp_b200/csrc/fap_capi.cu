@@ -536,6 +536,7 @@ int prepare_batch(fap_dgraph *G, const std::vector<int32_t> &ids) {
 // enough to keep re-relaxations near Dijkstra's count on road-like graphs).
 template <typename T>
 T sssp_delta_for(const fap_dgraph *G) {
+  if (G->sssp_delta == -2.0) return Dist<T>::inf();  // tuned: plain Bellman-Ford
   double d = G->sssp_delta > 0 ? G->sssp_delta : 64.0 * G->mean_w;
   d = std::min<double>(d, (double)Dist<T>::inf());
   if (Dist<T>::kDtype == FAP_DTYPE_I32) d = std::max(1.0, std::floor(d));
@@ -990,3 +991,79 @@ extern "C" int fap_graph_set_param(fap_dgraph *G, const char *key, double value)
   }
   return fail(FAP_ERR_INVALID, "unknown parameter '%s'", key);
 }
+
+// ---------------------------------------------------------------------------
+// SSSP bucket-width tuning: times the SSSP stage on a sample of the graph's
+// boundary sources (one wave of CTAs) for each candidate delta and keeps the
+// fastest.
+// ---------------------------------------------------------------------------
+namespace {
+template <typename T>
+int tune_sssp_impl(fap_dgraph *G, const double *deltas, int32_t count, int32_t sample,
+                   double *best_delta, float *ms_out) {
+  fap_ctx *c = G->ctx;
+  cudaStream_t st = c->stream;
+  const int64_t n = G->n;
+  // boundary sources of every part, in sorted-position space
+  std::vector<int32_t> all;
+  for (int32_t p = 1; p <= G->K; p++)
+    for (int32_t k = 0; k < G->bnum[p]; k++) all.push_back(G->voff[p] + k);
+  if (all.empty()) return fail(FAP_ERR_STATE, "graph has no boundary vertices to tune on");
+  const int want = sample > 0 ? sample : sssp_scratch_rows(G->n, (int)all.size());
+  const int ns = std::max(1, std::min<int>(want, (int)all.size()));
+  std::vector<int32_t> src(ns);
+  for (int i = 0; i < ns; i++) src[i] = all[(int64_t)i * (int64_t)all.size() / ns];
+  DevBuf d_src, rows, scratch;
+  FAP_TRY(d_src.ensure((size_t)ns * 4));
+  FAP_TRY(rows.ensure((size_t)ns * n * 4));
+  FAP_TRY(scratch.ensure((size_t)std::max(sssp_scratch_rows(G->n, ns), 1) * n * 4));
+  FAP_CK(cudaMemcpy(d_src.p, src.data(), (size_t)ns * 4, cudaMemcpyHostToDevice));
+  const int64_t rounds = G->sssp_max_rounds > 0 ? G->sssp_max_rounds : 8 * n + 1024;
+  double best = -1.0;
+  float best_ms = 1e30f;
+  int64_t L = 0;
+  for (int32_t i = 0; i < count; i++) {
+    const double dd = deltas[i];
+    double d = (dd > 0 && dd < (double)Dist<T>::inf()) ? dd : (double)Dist<T>::inf();
+    if (Dist<T>::kDtype == FAP_DTYPE_I32) d = std::max(1.0, std::floor(d));
+    float t_best = 1e30f;
+    for (int rep = 0; rep < 2; rep++) {
+      FAP_CK(cudaMemsetAsync(G->d_status.p, 0, sizeof(int), st));
+      FAP_CK(cudaEventRecord(c->ev[0], st));
+      FAP_CK(launch_sssp<T>(G->ro_s.as<int32_t>(), G->col_s.as<int32_t>(), G->w_s.as<T>(), G->n,
+                            d_src.as<int32_t>(), nullptr, ns, rows.as<T>(), n, n,
+                            G->d_ed2st.as<int32_t>(), scratch.as<T>(), (T)d, G->sssp_chain, rounds,
+                            G->d_status.as<int>(), st, &L));
+      FAP_CK(cudaEventRecord(c->ev[1], st));
+      FAP_CK(cudaEventSynchronize(c->ev[1]));
+      FAP_TRY(read_status(G));
+      float t;
+      FAP_CK(cudaEventElapsedTime(&t, c->ev[0], c->ev[1]));
+      if (rep > 0 || count == 1) t_best = std::min(t_best, t);
+    }
+    if (ms_out) ms_out[i] = t_best;
+    if (t_best < best_ms) {
+      best_ms = t_best;
+      best = dd;
+    }
+  }
+  d_src.release();
+  rows.release();
+  scratch.release();
+  G->sssp_delta = (best > 0 && best < 1e8) ? best : -2.0;  // -2: plain Bellman-Ford chosen
+  G->epoch++;
+  if (best_delta) *best_delta = best;
+  return FAP_OK;
+}
+}  // namespace
+
+extern "C" int fap_graph_tune_sssp(fap_dgraph *G, const double *deltas, int32_t count, int32_t sample,
+                                   double *best_delta, float *ms_out) {
+  if (!G || !deltas || count <= 0) return fail(FAP_ERR_INVALID, "need a graph and candidate deltas");
+  if (G->K == 0) return fail(FAP_ERR_STATE, "tune before fap_graph_set_parts");
+  DeviceGuard g(G->ctx->device);
+  return G->dtype == FAP_DTYPE_I32 ? tune_sssp_impl<int32_t>(G, deltas, count, sample, best_delta, ms_out)
+                                   : tune_sssp_impl<float>(G, deltas, count, sample, best_delta, ms_out);
+}
+
+extern "C" double fap_graph_mean_weight(const fap_dgraph *G) { return G ? G->mean_w : 0.0; }

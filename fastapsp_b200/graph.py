@@ -353,6 +353,19 @@ class DeviceGraph:
     def set_param(self, key: str, value: float) -> None:
         check(lib().fap_graph_set_param(self._h, key.encode(), float(value)), "set_param")
 
+    def mean_weight(self) -> float:
+        return float(lib().fap_graph_mean_weight(self._h))
+
+    def tune_sssp(self, deltas: Sequence[float], sample: int = 0):
+        """Times the SSSP stage for each candidate bucket width and keeps the
+        fastest; returns (best_delta, ms per candidate)."""
+        d = np.ascontiguousarray(deltas, dtype=np.float64)
+        ms = np.zeros(d.shape[0], np.float32)
+        best = ctypes.c_double()
+        check(lib().fap_graph_tune_sssp(self._h, ptr(d), int(d.shape[0]), int(sample),
+                                        ctypes.byref(best), ptr(ms)), "tune_sssp")
+        return float(best.value), ms
+
     def reserve(self, max_rows: int = 0) -> None:
         check(lib().fap_graph_reserve(self._h, int(max_rows)), "fap_graph_reserve")
 

@@ -148,6 +148,17 @@ FAP_API int fap_graph_sssp_rows(fap_dgraph *g, const int32_t *sources, int32_t c
  * unchanged). */
 FAP_API int fap_graph_set_param(fap_dgraph *g, const char *key, double value);
 
+/* Tunes the SSSP bucket width: runs the SSSP stage on `sample` boundary
+ * sources spread over all parts (0 = one full wave of CTAs) for each of the
+ * `count` candidate deltas (>= 1e8 or <= 0 = plain Bellman-Ford), keeps the
+ * fastest for later solves and returns it in *best_delta; ms_out[count]
+ * (optional) receives each candidate's time.  Needs the partition. */
+FAP_API int fap_graph_tune_sssp(fap_dgraph *g, const double *deltas, int32_t count, int32_t sample,
+                                double *best_delta, float *ms_out);
+
+/* Mean edge weight of the graph (the scale SSSP bucket widths are tuned in). */
+FAP_API double fap_graph_mean_weight(const fap_dgraph *g);
+
 /* Device time (ms) of the stages of the last fap_solve, measured with events
  * on the context stream: [sssp, gather, floyd, minplus, total]. */
 FAP_API int fap_graph_last_timing(fap_dgraph *g, float *ms5);
