@@ -154,6 +154,7 @@ struct fap_dgraph {
   int64_t sssp_max_rounds = -1;  // <0: 8n + 1024
   bool floyd_per_cta = false;     // batched Floyd: one CTA per part instead of per-tile launches
   int sssp_chain = 0;             // SSSP chain-following budget (hops per thread per round)
+  int sssp_precheck = 1;          // SSSP: plain read of dist[v] before the atomicMin
   // CUDA graph of the batched launch sequence (replayed while nothing that
   // it captured changes: batch, buffers, parameters, stream)
   bool use_graph = true;
@@ -570,7 +571,7 @@ int run_solve(fap_dgraph *G, int mode) {
   if (mode == FAP_MODE_BATCHED) {
     FAP_CK(record_event(c->ev[0], st));
     FAP_CK(launch_sssp<T>(ro_s, col_s, w_s, G->n, src, srow, (int)G->src.size(), D, G->ldD, G->ldD,
-                          ed2st, scratch, delta, G->sssp_chain, max_rounds, status, st, &L));
+                          ed2st, scratch, delta, G->sssp_chain, G->sssp_precheck, max_rounds, status, st, &L));
     FAP_CK(record_event(c->ev[1], st));
     FAP_CK(launch_gather<T>(dp, np, G->max_ldf, ro, col, w, gid, st2ed, ed2st, D, G->ldD, F, st, &L));
     FAP_CK(record_event(c->ev[2], st));
@@ -594,7 +595,7 @@ int run_solve(fap_dgraph *G, int mode) {
       const int s0 = G->part_src_off[i], s1 = G->part_src_off[i + 1];
       const int w0 = G->part_work_begin[i], w1 = G->part_work_end[i];
       FAP_CK(launch_sssp<T>(ro_s, col_s, w_s, G->n, src + s0, srow + s0, s1 - s0, D, G->ldD,
-                            G->ldD, ed2st, scratch, delta, G->sssp_chain, max_rounds, status, st, &L));
+                            G->ldD, ed2st, scratch, delta, G->sssp_chain, G->sssp_precheck, max_rounds, status, st, &L));
       FAP_CK(launch_gather<T>(dp + i, 1, d.ldf, ro, col, w, gid, st2ed, ed2st, D, G->ldD, F, st, &L));
       FAP_CK(launch_floyd_matrix<T>(F + d.f_off, d.ldf, (int)ceil_div(d.s, kFloydTile), status, st, &L));
       FAP_CK(launch_bdy_scatter<T>(dp + i, 1, F, D, G->ldD, st2ed, d.b, d.s, st, &L));
@@ -804,12 +805,12 @@ extern "C" int fap_op_sssp(fap_ctx *c, int dtype, int32_t n, int64_t m, const in
   const int64_t rounds = 8 * (int64_t)n + 1024;
   if (dtype == FAP_DTYPE_I32) {
     FAP_CK(launch_sssp<int32_t>(row_offset, col_val, (const int32_t *)weight, n, sources, nullptr,
-                                num_sources, (int32_t *)out, ld_out, n, nullptr, nullptr, kInfI32, 32,
+                                num_sources, (int32_t *)out, ld_out, n, nullptr, nullptr, kInfI32, 0, 1,
                                 rounds,
                                 c->status.as<int>(), c->stream, &L));
   } else if (dtype == FAP_DTYPE_F32) {
     FAP_CK(launch_sssp<float>(row_offset, col_val, (const float *)weight, n, sources, nullptr,
-                              num_sources, (float *)out, ld_out, n, nullptr, nullptr, kInfF32, 32,
+                              num_sources, (float *)out, ld_out, n, nullptr, nullptr, kInfF32, 0, 1,
                               rounds,
                               c->status.as<int>(), c->stream, &L));
   } else {
@@ -919,11 +920,12 @@ cudaError_t sssp_rows_launch(fap_dgraph *G, const int32_t *h_sources, int32_t co
     return launch_sssp<T>(G->ro_s.as<int32_t>(), G->col_s.as<int32_t>(), G->w_s.as<T>(), G->n,
                           srcs.as<int32_t>(), nullptr, count, rows.as<T>(), n, n,
                           G->d_ed2st.as<int32_t>(), scratch.as<T>(), sssp_delta_for<T>(G),
-                          G->sssp_chain, rounds, G->d_status.as<int>(), st, L);
+                          G->sssp_chain, G->sssp_precheck, rounds, G->d_status.as<int>(), st, L);
   }
   return launch_sssp<T>(G->ro.as<int32_t>(), G->col.as<int32_t>(), G->w.as<T>(), G->n,
                         srcs.as<int32_t>(), nullptr, count, rows.as<T>(), n, n, nullptr, nullptr,
-                        sssp_delta_for<T>(G), G->sssp_chain, rounds, G->d_status.as<int>(), st, L);
+                        sssp_delta_for<T>(G), G->sssp_chain, G->sssp_precheck, rounds,
+                        G->d_status.as<int>(), st, L);
 }
 }  // namespace
 
@@ -975,6 +977,10 @@ extern "C" int fap_graph_set_param(fap_dgraph *G, const char *key, double value)
   }
   if (std::strcmp(key, "sssp_delta") == 0) {
     G->sssp_delta = (value > 0 && value < 1e8) ? value : -1.0;
+    return FAP_OK;
+  }
+  if (std::strcmp(key, "sssp_precheck") == 0) {
+    G->sssp_precheck = value != 0.0 ? 1 : 0;
     return FAP_OK;
   }
   if (std::strcmp(key, "sssp_chain") == 0) {
@@ -1032,7 +1038,8 @@ int tune_sssp_impl(fap_dgraph *G, const double *deltas, int32_t count, int32_t s
       FAP_CK(cudaEventRecord(c->ev[0], st));
       FAP_CK(launch_sssp<T>(G->ro_s.as<int32_t>(), G->col_s.as<int32_t>(), G->w_s.as<T>(), G->n,
                             d_src.as<int32_t>(), nullptr, ns, rows.as<T>(), n, n,
-                            G->d_ed2st.as<int32_t>(), scratch.as<T>(), (T)d, G->sssp_chain, rounds,
+                            G->d_ed2st.as<int32_t>(), scratch.as<T>(), (T)d, G->sssp_chain,
+                            G->sssp_precheck, rounds,
                             G->d_status.as<int>(), st, &L));
       FAP_CK(cudaEventRecord(c->ev[1], st));
       FAP_CK(cudaEventSynchronize(c->ev[1]));

@@ -180,8 +180,8 @@ template <typename T>
 cudaError_t launch_sssp(const int32_t *row_offset, const int32_t *col, const T *w, int n,
                         const int32_t *sources, const int64_t *out_rows, int num_sources, T *out,
                         int64_t ld, int64_t init_cols, const int32_t *perm_out, T *scratch,
-                        T delta, int chain, int64_t max_rounds, int *status, cudaStream_t stream,
-                        int64_t *launches) {
+                        T delta, int chain, int precheck, int64_t max_rounds, int *status,
+                        cudaStream_t stream, int64_t *launches) {
   if (num_sources <= 0) return cudaSuccess;
   const size_t smem = sssp_smem_bytes(n);
   auto kern = sssp_frontier_kernel<T>;
@@ -192,7 +192,7 @@ cudaError_t launch_sssp(const int32_t *row_offset, const int32_t *col, const T *
   const int grid = perm_out ? sssp_scratch_rows(n, num_sources) : num_sources;
   kern<<<grid, kSsspThreads, smem, stream>>>(row_offset, col, w, n, sources, out_rows, num_sources,
                                              out, ld, init_cols, perm_out, scratch, delta,
-                                             chain, max_rounds, status);
+                                             chain, precheck, max_rounds, status);
   *launches += 1;
   return cudaGetLastError();
 }
@@ -843,7 +843,7 @@ cudaError_t launch_relax_peak(T *sink, int blocks, int iters, cudaStream_t strea
 #define FAPB_INSTANTIATE(T)                                                                       \
   template cudaError_t launch_sssp<T>(const int32_t *, const int32_t *, const T *, int,           \
                                       const int32_t *, const int64_t *, int, T *, int64_t,        \
-                                      int64_t, const int32_t *, T *, T, int, int64_t, int *,      \
+                                      int64_t, const int32_t *, T *, T, int, int, int64_t, int *, \
                                       cudaStream_t, int64_t *);                                   \
   template cudaError_t launch_gather<T>(const PartDesc *, int, int, const int32_t *,              \
                                         const int32_t *, const T *, const int32_t *,              \

@@ -40,8 +40,8 @@ template <typename T>
 cudaError_t launch_sssp(const int32_t *row_offset, const int32_t *col, const T *w, int n,
                         const int32_t *sources, const int64_t *out_rows, int num_sources, T *out,
                         int64_t ld, int64_t init_cols, const int32_t *perm_out, T *scratch,
-                        T delta, int chain, int64_t max_rounds, int *status, cudaStream_t stream,
-                        int64_t *launches);
+                        T delta, int chain, int precheck, int64_t max_rounds, int *status,
+                        cudaStream_t stream, int64_t *launches);
 
 // Rows of scratch the relabelled SSSP needs (= CTAs it launches) for
 // num_sources sources on this device.

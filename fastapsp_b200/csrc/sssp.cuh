@@ -19,6 +19,9 @@
 //     atomics of a 4-edge group in flight at once; vertices with more than
 //     kHeavyDeg edges are expanded by a whole warp (lane-strided, coalesced
 //     column/weight reads).
+//   - Relaxation: a plain read of dist[v] first skips the atomic when it
+//     cannot improve (fewer atomics) at the price of one more dependent
+//     access; `precheck` selects it.
 //   - Chains: a thread that improves a near neighbour expands it at once
 //     (up to `chain` hops per round) instead of leaving it for the next
 //     round, so a hop along a path costs one load + atomic latency rather
@@ -99,7 +102,7 @@ template <typename T>
 __device__ __forceinline__ bool relax_edges_chain(const int32_t *__restrict__ col,
                                                   const T *__restrict__ w, int e0, int e1, T du,
                                                   T *dist, uint32_t *nb, T thresh, bool may_chain,
-                                                  int *next, T *dnext) {
+                                                  bool precheck, int *next, T *dnext) {
   bool any = false;
   *next = -1;
   for (int e = e0; e < e1; e += 4) {
@@ -112,7 +115,8 @@ __device__ __forceinline__ bool relax_edges_chain(const int32_t *__restrict__ co
       nd[k] = ek < e1 ? du + __ldg(w + ek) : du;
     }
 #pragma unroll
-    for (int k = 0; k < 4; k++) cur[k] = v[k] >= 0 ? ld_relaxed(dist + v[k]) : du;
+    for (int k = 0; k < 4; k++)
+      cur[k] = v[k] < 0 ? du : precheck ? ld_relaxed(dist + v[k]) : Dist<T>::inf() + Dist<T>::inf();
 #pragma unroll
     for (int k = 0; k < 4; k++)
       old[k] = (v[k] >= 0 && nd[k] < cur[k]) ? Dist<T>::atomic_min(dist + v[k], nd[k]) : nd[k];
@@ -136,7 +140,7 @@ __device__ __forceinline__ bool relax_edges_chain(const int32_t *__restrict__ co
 template <typename T>
 __device__ __forceinline__ bool relax_edges(const int32_t *__restrict__ col, const T *__restrict__ w,
                                             int e0, int e1, int stride, T du, T *dist,
-                                            uint32_t *nb) {
+                                            uint32_t *nb, bool precheck) {
   bool any = false;
   for (int e = e0; e < e1; e += 4 * stride) {
     int v[4];
@@ -148,7 +152,8 @@ __device__ __forceinline__ bool relax_edges(const int32_t *__restrict__ col, con
       nd[k] = ek < e1 ? du + __ldg(w + ek) : du;
     }
 #pragma unroll
-    for (int k = 0; k < 4; k++) cur[k] = v[k] >= 0 ? ld_relaxed(dist + v[k]) : du;
+    for (int k = 0; k < 4; k++)
+      cur[k] = v[k] < 0 ? du : precheck ? ld_relaxed(dist + v[k]) : Dist<T>::inf() + Dist<T>::inf();
 #pragma unroll
     for (int k = 0; k < 4; k++)
       old[k] = (v[k] >= 0 && nd[k] < cur[k]) ? Dist<T>::atomic_min(dist + v[k], nd[k]) : nd[k];
@@ -172,7 +177,7 @@ __global__ void __launch_bounds__(kSsspThreads)
                          const T *__restrict__ w, int n, const int32_t *__restrict__ sources,
                          const int64_t *__restrict__ out_rows, int num_sources, T *out, int64_t ld,
                          int64_t init_cols, const int32_t *__restrict__ perm_out, T *scratch,
-                         T delta, int chain, int64_t max_rounds, int *status) {
+                         T delta, int chain, int precheck, int64_t max_rounds, int *status) {
   extern __shared__ uint32_t sm_bits[];
   __shared__ int32_t s_minfar[3];
   __shared__ int s_warp[kSsspThreads / 32];
@@ -261,7 +266,8 @@ __global__ void __launch_bounds__(kSsspThreads)
             }
             int nx;
             T dn;
-            any |= relax_edges_chain<T>(col, w, e0, e1, dx, dist, nb, thresh, hop < chain, &nx, &dn);
+            any |= relax_edges_chain<T>(col, w, e0, e1, dx, dist, nb, thresh, hop < chain, precheck != 0,
+                                        &nx, &dn);
             if (nx < 0) break;
             x = nx;
             dx = dn;
@@ -274,7 +280,7 @@ __global__ void __launch_bounds__(kSsspThreads)
           const int u = heavy[h];
           const T du = ld_relaxed(dist + u);
           const int e0 = __ldg(row_offset + u), e1 = __ldg(row_offset + u + 1);
-          any |= relax_edges<T>(col, w, e0 + lane, e1, 32, du, dist, nb);
+          any |= relax_edges<T>(col, w, e0 + lane, e1, 32, du, dist, nb, precheck != 0);
         }
         __syncthreads();
         if (total <= kSsspList) break;
