@@ -53,6 +53,14 @@ def parse_args():
     ap.add_argument("--plain-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-procs", type=int, default=0, help="0 = min(cores, memory bound)")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving-stream measurement")
+    ap.add_argument("--serve-graphs", type=int, default=32)
+    ap.add_argument("--serve-burst", type=int, default=256,
+                    help="requests of the closed-loop burst that measures capacity")
+    ap.add_argument("--serve-seconds", type=float, default=4.0,
+                    help="arrival window of each offered-load run")
+    ap.add_argument("--serve-batch-rows", type=int, default=0,
+                    help="output rows per batch (0: memory budget only)")
     return ap.parse_args()
 
 
@@ -249,6 +257,103 @@ def main_reference(args):
 # ---------------------------------------------------------------------------
 # fap arm
 # ---------------------------------------------------------------------------
+def run_serving(args, device):
+    """Serving stream: Poisson arrivals of solveSubGraph / distance-row
+    requests over resident random-geometric graphs, answered by the native
+    serving loop (fap_server_*).  Capacity is measured with a closed-loop
+    burst; then requests arrive at 25/50/90% of it.  Each request returns
+    per-row checksums (its distances stay in HBM)."""
+    from fastapsp_b200 import workloads
+    from fastapsp_b200.serve import Server
+
+    t0 = time.perf_counter()
+    gs = workloads.load_serve_stream(args.serve_graphs)
+    log(f"serving stream: {len(gs)} graphs built in {time.perf_counter() - t0:.1f} s")
+    import torch
+    free_b = torch.cuda.mem_get_info()[0]
+    srv = Server(device, budget_bytes=0.6 * free_b, max_batch_rows=args.serve_batch_rows)
+    info = []
+    for g in gs:
+        idx = srv.add_graph(g.graph)
+        vn = g.graph.partInfo()[0]
+        info.append((idx, g.n, g.K, vn))
+    rng = np.random.default_rng(23)
+
+    def draw():
+        gi, n, K, vn = info[int(rng.integers(len(info)))]
+        if rng.random() < 0.8:
+            return ("sub", gi, int(rng.integers(1, K + 1)))
+        cnt = int(round(np.exp(rng.uniform(np.log(100), np.log(10000)))))
+        return ("rows", gi, rng.integers(0, n, min(cnt, n)).astype(np.int32))
+
+    def submit(req):
+        if req[0] == "sub":
+            return srv.submit_subgraph(req[1], req[2], distances=False, checksums=True)
+        return srv.submit_rows(req[1], req[2], distances=False, checksums=True)
+
+    def finish(handles):
+        srv.drain()
+        for h in handles:
+            if h.wait(0) != 2:
+                raise RuntimeError(f"serving request failed: {h.info()}")
+            h.forget()
+
+    # warm-up: one request per graph (first allocations)
+    finish([srv.submit_subgraph(i, 1, distances=False, checksums=True) for i, *_ in info])
+    srv.reset_stats()
+    # capacity: closed-loop burst
+    reqs = [draw() for _ in range(args.serve_burst)]
+    t0 = time.perf_counter()
+    hs = [submit(r) for r in reqs]
+    finish(hs)
+    burst_s = time.perf_counter() - t0
+    st = srv.stats()
+    cap_rps = len(reqs) / burst_s
+    out = {"graphs": len(gs),
+           "n": [min(g.n for g in gs), max(g.n for g in gs)],
+           "K": sorted({g.K for g in gs}),
+           "part_rows": [int(min(x[3][1:].min() for x in info)), int(max(x[3][1:].max() for x in info))],
+           "mix": "80% solveSubGraph (uniform graph, uniform part), 20% distance rows "
+                  "(100-10,000 sources, log-uniform); per-row checksums returned",
+           "budget_bytes": int(0.6 * free_b),
+           "capacity": {"requests_s": cap_rps, "entries_s": st.entries / burst_s,
+                        "requests": len(reqs), "batches": st.batches,
+                        "resident_hits": st.resident_hits, "p50_ms": st.p50_ms, "p99_ms": st.p99_ms},
+           "loads": []}
+    log(f"serving capacity {cap_rps:.1f} req/s, {st.entries / burst_s:.4g} entries/s")
+    for frac in (0.25, 0.5, 0.9):
+        rate = frac * cap_rps
+        count = int(min(max(32, rate * args.serve_seconds), 4 * args.serve_burst))
+        reqs = [draw() for _ in range(count)]
+        gaps = rng.exponential(1.0 / rate, count)
+        srv.reset_stats()
+        hs = []
+        t0 = time.perf_counter()
+        due = t0
+        for r, gap in zip(reqs, gaps):
+            due += gap
+            while True:
+                now = time.perf_counter()
+                if now >= due:
+                    break
+                time.sleep(min(due - now, 0.002))
+            hs.append(submit(r))
+        t_sub = time.perf_counter() - t0
+        finish(hs)
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+        out["loads"].append({"offered_frac": frac, "offered_requests_s": rate,
+                             "requests": count, "arrival_window_s": t_sub,
+                             "achieved_requests_s": count / wall, "entries_s": st.entries / wall,
+                             "p50_ms": st.p50_ms, "p99_ms": st.p99_ms, "mean_ms": st.mean_ms,
+                             "batches": st.batches, "resident_hits": st.resident_hits,
+                             "peak_device_bytes": st.peak_bytes})
+        log(f"serving at {frac:.0%}: p50 {st.p50_ms:.2f} ms, p99 {st.p99_ms:.2f} ms, "
+            f"{st.entries / wall:.4g} entries/s, {st.batches} batches")
+    srv.close()
+    return out
+
+
 def main_fap(args):
     import torch
     import torch.distributed as dist
@@ -449,6 +554,13 @@ def main_fap(args):
     e2e_value = total_entries * len(e2e_s) / e2e_max if e2e_s else None
     log(f"e2e: {e2e_s} s/step")
 
+    # ---- serving stream (rank 0, N=1 only) ----
+    serving = None
+    if rank == 0 and world == 1 and not args.no_serve:
+        del host_buf, hb
+        torch.cuda.empty_cache()
+        serving = run_serving(args, local)
+
     # ---- CPU baseline (rank 0, N=1 only) ----
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -487,6 +599,7 @@ def main_fap(args):
                     "s_per_step": e2e_max / max(len(e2e_s), 1)},
             "gpu_launches": int(launches),
             "clocks": clk,
+            "serving": serving,
         }
         emit(line)
     if world > 1:

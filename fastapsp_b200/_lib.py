@@ -87,6 +87,21 @@ _SIGS = {
     "fap_measure_relax_peak": (INT, [P, INT, ctypes.POINTER(DBL)]),
     "fap_graph_tune_sssp": (INT, [P, P, I32, I32, ctypes.POINTER(DBL), P]),
     "fap_graph_mean_weight": (DBL, [P]),
+    "fap_graph_release": (INT, [P]),
+    "fap_graph_device_bytes": (INT, [P, ctypes.POINTER(I64)]),
+    "fap_graph_resident": (INT, [P, I32]),
+    "fap_graph_rows_async": (INT, [P, P, I32, P]),
+    "fap_server_create": (INT, [INT, DBL, I64, PP]),
+    "fap_server_destroy": (INT, [P]),
+    "fap_server_add_graph": (INT, [P, I32, I64, P, P, P, INT, I32, P, P, P, P, P, ctypes.POINTER(I32)]),
+    "fap_server_submit": (INT, [P, I32, INT, P, I32, P, P, ctypes.POINTER(I64)]),
+    "fap_server_wait": (INT, [P, I64, DBL, ctypes.POINTER(INT)]),
+    "fap_server_request_info": (INT, [P, I64, P]),
+    "fap_server_forget": (INT, [P, I64]),
+    "fap_server_drain": (INT, [P]),
+    "fap_server_stats": (INT, [P, P]),
+    "fap_server_reset_stats": (INT, [P]),
+    "fap_server_last_error": (ctypes.c_char_p, []),
     "fap_floyd_noalloc": (INT, [INT, I32, P, I64, P]),
     "fap_floyd_noalloc_last_error": (ctypes.c_char_p, []),
     "fap_legacy_last_status": (INT, []),
@@ -147,9 +162,9 @@ def lib():
 
 def last_error() -> str:
     L = lib()
-    a = L.fap_last_error() or b""
-    b = L.fap_host_last_error() or b""
-    return (a.decode() + (" | " if a and b else "") + b.decode()) or "unknown error"
+    msgs = [m.decode() for m in (L.fap_last_error(), L.fap_host_last_error(),
+                                 L.fap_server_last_error()) if m]
+    return " | ".join(msgs) or "unknown error"
 
 
 def check(rc: int, what: str = "") -> None:

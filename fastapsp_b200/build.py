@@ -33,8 +33,10 @@ METIS_A = os.path.join(CUDA_LIB, "libmetis_static.a")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fvisibility=hidden",
           "-I" + INCLUDE, "-I" + CSRC]
-SOURCES = ["fap_device.cu", "fap_capi.cu", "fap_legacy.cu", "fap_noalloc.cu", "fap_host.cpp"]
-HEADERS = ["fap_common.cuh", "minplus_tile.cuh", "floyd.cuh", "sssp.cuh", "fap_internal.h"]
+SOURCES = ["fap_device.cu", "fap_capi.cu", "fap_legacy.cu", "fap_noalloc.cu", "fap_host.cpp",
+           "fap_serve.cpp"]
+HEADERS = ["fap_common.cuh", "minplus_tile.cuh", "floyd.cuh", "sssp.cuh", "tma.cuh", "tma_tile.cuh",
+           "fap_internal.h"]
 
 
 def _stale(target: str, deps: list[str]) -> bool:
@@ -55,7 +57,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(OBJDIR, exist_ok=True)
     hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [
         os.path.join(INCLUDE, "fap_b200.h"), os.path.join(INCLUDE, "fap_legacy_kernel.h"),
-        os.path.join(INCLUDE, "fap_host.h"),
+        os.path.join(INCLUDE, "fap_host.h"), os.path.join(INCLUDE, "fap_serve.h"),
         os.path.join(INCLUDE, "fap", "fap.h")]
     objs = []
     for src in SOURCES:
@@ -71,7 +73,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
             _run(cmd)
     if force or _stale(LIB, objs):
         cmd = [NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", LIB] + objs + [
-            METIS_A, "-Xlinker", "--exclude-libs,ALL", "-lm"]
+            METIS_A, "-Xlinker", "--exclude-libs,ALL", "-lm", "-lpthread"]
         if verbose:
             print(" ".join(cmd))
         _run(cmd)

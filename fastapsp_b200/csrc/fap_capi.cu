@@ -1074,3 +1074,88 @@ extern "C" int fap_graph_tune_sssp(fap_dgraph *G, const double *deltas, int32_t 
 }
 
 extern "C" double fap_graph_mean_weight(const fap_dgraph *G) { return G ? G->mean_w : 0.0; }
+
+// ---------------------------------------------------------------------------
+// Memory release and asynchronous distance rows (used by the serving loop)
+// ---------------------------------------------------------------------------
+extern "C" int fap_graph_release(fap_dgraph *G) {
+  if (!G) return fail(FAP_ERR_INVALID, "NULL graph");
+  DeviceGuard g(G->ctx->device);
+  FAP_CK(cudaStreamSynchronize(G->ctx->stream));
+  G->D.release();
+  G->F.release();
+  G->sssp_scratch.release();
+  G->staging.release();
+  G->d_checks.release();
+  G->max_rows = 0;
+  std::fill(G->row_base.begin(), G->row_base.end(), -1);
+  G->last_ids.clear();
+  G->epoch++;
+  return FAP_OK;
+}
+
+extern "C" int fap_graph_device_bytes(const fap_dgraph *G, int64_t *bytes) {
+  if (!G || !bytes) return fail(FAP_ERR_INVALID, "NULL argument");
+  int64_t t = 0;
+  for (const DevBuf *b : {&G->ro, &G->col, &G->w, &G->ro_s, &G->col_s, &G->w_s, &G->sssp_scratch,
+                          &G->d_thin, &G->d_gid, &G->d_st2ed, &G->d_ed2st, &G->D, &G->F, &G->d_parts,
+                          &G->d_work, &G->d_src, &G->d_srcrows, &G->d_status, &G->d_checks, &G->staging})
+    t += (int64_t)b->bytes;
+  *bytes = t;
+  return FAP_OK;
+}
+
+extern "C" int fap_graph_resident(fap_dgraph *G, int32_t part) {
+  if (!G || part < 1 || part > G->K) return 0;
+  return G->row_base[part] >= 0 ? 1 : 0;
+}
+
+namespace {
+template <typename T>
+int rows_async_impl(fap_dgraph *G, const int32_t *sources, int32_t count, float *d_out) {
+  cudaStream_t st = G->ctx->stream;
+  const int64_t n = G->n;
+  std::vector<int32_t> work(sources, sources + count);
+  const bool relabel = G->K > 0;
+  if (relabel)
+    for (auto &x : work) x = G->ed2st[x];
+  FAP_TRY(G->d_src.ensure(std::max<size_t>((size_t)count, G->d_src.bytes / 4) * 4));
+  // the batch descriptors on the device no longer match d_src
+  G->last_ids.clear();
+  FAP_CK(cudaMemcpyAsync(G->d_src.p, work.data(), (size_t)count * 4, cudaMemcpyHostToDevice, st));
+  FAP_CK(cudaStreamSynchronize(st));  // the host vector goes out of scope
+  FAP_CK(cudaMemsetAsync(G->d_status.p, 0, sizeof(int), st));
+  const int64_t rounds = G->sssp_max_rounds > 0 ? G->sssp_max_rounds : 8 * n + 1024;
+  int64_t L = 0;
+  T *out = reinterpret_cast<T *>(d_out);
+  if (relabel) {
+    FAP_TRY(G->sssp_scratch.ensure((size_t)std::max(sssp_scratch_rows(G->n, count), 1) * n * 4));
+    FAP_CK(launch_sssp<T>(G->ro_s.as<int32_t>(), G->col_s.as<int32_t>(), G->w_s.as<T>(), G->n,
+                          G->d_src.as<int32_t>(), nullptr, count, out, n, n, G->d_ed2st.as<int32_t>(),
+                          G->sssp_scratch.as<T>(), sssp_delta_for<T>(G), G->sssp_chain, G->sssp_precheck,
+                          rounds, G->d_status.as<int>(), st, &L));
+  } else {
+    FAP_CK(launch_sssp<T>(G->ro.as<int32_t>(), G->col.as<int32_t>(), G->w.as<T>(), G->n,
+                          G->d_src.as<int32_t>(), nullptr, count, out, n, n, nullptr, nullptr,
+                          sssp_delta_for<T>(G), G->sssp_chain, G->sssp_precheck, rounds,
+                          G->d_status.as<int>(), st, &L));
+  }
+  if (Dist<T>::kDtype == FAP_DTYPE_I32)
+    FAP_CK(launch_i32_to_f32(reinterpret_cast<int32_t *>(d_out), count, n, n, d_out, st, &L));
+  G->ctx->launches += L;
+  G->launches = L;
+  G->epoch++;
+  return FAP_OK;
+}
+}  // namespace
+
+extern "C" int fap_graph_rows_async(fap_dgraph *G, const int32_t *sources, int32_t count, float *d_out) {
+  if (!G || (count > 0 && (!sources || !d_out))) return fail(FAP_ERR_INVALID, "NULL argument");
+  if (count < 0) return fail(FAP_ERR_INVALID, "negative count");
+  if (count == 0) return FAP_OK;
+  for (int32_t i = 0; i < count; i++)
+    if (sources[i] < 0 || sources[i] >= G->n) return fail(FAP_ERR_INVALID, "source %d out of range", sources[i]);
+  DeviceGuard g(G->ctx->device);
+  return G->dtype == FAP_DTYPE_I32 ? rows_async_impl<int32_t>(G, sources, count, d_out)
+                                   : rows_async_impl<float>(G, sources, count, d_out);
+}

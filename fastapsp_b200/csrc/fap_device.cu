@@ -758,13 +758,19 @@ cudaError_t launch_fill(T *p, int64_t rows, int64_t cols, int64_t ld, T v, cudaS
   return cudaGetLastError();
 }
 
-__global__ void row_checksum_kernel(const int32_t *__restrict__ D, int64_t n, int64_t ld,
+// One CTA per row: sum over j of (uint32)D[r][j] * (2j + 1), mod 2^64.  Float
+// input holds exact integers (int32 distances converted for output).
+__device__ __forceinline__ uint32_t checksum_word(int32_t x) { return (uint32_t)x; }
+__device__ __forceinline__ uint32_t checksum_word(float x) { return (uint32_t)(int32_t)x; }
+
+template <typename T>
+__global__ void row_checksum_kernel(const T *__restrict__ D, int64_t n, int64_t ld,
                                     uint64_t *__restrict__ out) {
   const int64_t r = blockIdx.x;
-  const uint32_t *row = reinterpret_cast<const uint32_t *>(D + r * ld);
+  const T *row = D + r * ld;
   uint64_t acc = 0;
   for (int64_t j = threadIdx.x; j < n; j += blockDim.x)
-    acc += (uint64_t)__ldg(row + j) * (uint64_t)(2 * j + 1);
+    acc += (uint64_t)checksum_word(__ldg(row + j)) * (uint64_t)(2 * j + 1);
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
   __shared__ uint64_t part[32];
   if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
@@ -779,7 +785,15 @@ __global__ void row_checksum_kernel(const int32_t *__restrict__ D, int64_t n, in
 cudaError_t launch_row_checksums(const int32_t *D, int64_t rows, int64_t n, int64_t ld,
                                  uint64_t *out, cudaStream_t stream, int64_t *launches) {
   if (rows <= 0) return cudaSuccess;
-  row_checksum_kernel<<<(unsigned)rows, 256, 0, stream>>>(D, n, ld, out);
+  row_checksum_kernel<int32_t><<<(unsigned)rows, 256, 0, stream>>>(D, n, ld, out);
+  *launches += 1;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_row_checksums(const float *D, int64_t rows, int64_t n, int64_t ld,
+                                 uint64_t *out, cudaStream_t stream, int64_t *launches) {
+  if (rows <= 0) return cudaSuccess;
+  row_checksum_kernel<float><<<(unsigned)rows, 256, 0, stream>>>(D, n, ld, out);
   *launches += 1;
   return cudaGetLastError();
 }

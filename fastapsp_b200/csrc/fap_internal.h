@@ -110,8 +110,11 @@ template <typename T>
 cudaError_t launch_fill(T *p, int64_t rows, int64_t cols, int64_t ld, T v, cudaStream_t stream,
                         int64_t *launches);
 
-// Per-row checksums (int32 data).
+// Per-row checksums of int32 distances (the float overload reads int32
+// distances already converted to float, every value an exact integer).
 cudaError_t launch_row_checksums(const int32_t *D, int64_t rows, int64_t n, int64_t ld,
+                                 uint64_t *out, cudaStream_t stream, int64_t *launches);
+cudaError_t launch_row_checksums(const float *D, int64_t rows, int64_t n, int64_t ld,
                                  uint64_t *out, cudaStream_t stream, int64_t *launches);
 
 // int32 -> float copy of a rows x n block into a dense buffer.

@@ -1,0 +1,630 @@
+// Serving loop over resident graphs: continuous batching of sub-graph and
+// distance-row requests, HBM-footprint admission, one stream per graph so
+// batches of different graphs overlap on the GPU.  See include/fap_serve.h.
+#include "fap_serve.h"
+
+#include <cuda_runtime.h>
+
+#include "fap_internal.h"
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstdio>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+double now_s() {
+  return std::chrono::duration<double>(Clock::now().time_since_epoch()).count();
+}
+
+struct Req {
+  int64_t id = 0;
+  int32_t graph = 0;
+  int kind = FAP_REQ_SUBGRAPH;
+  std::vector<int32_t> ids;
+  float *host_out = nullptr;
+  uint64_t *cs_out = nullptr;
+  double t_submit = 0, t_start = 0, t_done = 0;
+  int state = FAP_REQ_PENDING;
+  int status = FAP_OK;
+  int64_t rows = 0;
+  int64_t entries = 0;
+  int64_t row_off = 0;  // FAP_REQ_ROWS: first row in the graph's rows buffer
+};
+
+struct GSlot {
+  fap_ctx *ctx = nullptr;
+  fap_dgraph *dg = nullptr;
+  int32_t n = 0, K = 0;
+  int dtype = FAP_DTYPE_I32;
+  int64_t ldD = 0;
+  int64_t base_bytes = 0;  // CSR + partition, always resident
+  std::vector<int32_t> vnum, voff, bnum;
+  int64_t reserved_rows = 0;   // output rows the graph's D holds (0: released)
+  float *rows_buf = nullptr;  // FAP_REQ_ROWS results, grown on demand
+  int64_t rows_cap = 0;
+  uint64_t *cs_buf = nullptr;  // FAP_REQ_ROWS checksums (one per row of rows_buf)
+  int64_t cs_cap = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+  bool busy = false;
+  int batch_kind = FAP_REQ_SUBGRAPH;
+  std::vector<Req *> inflight;
+  std::deque<Req *> pending;
+  double last_used = 0;
+};
+
+}  // namespace
+
+constexpr int kMaxGraphs = 256;
+
+struct fap_server {
+  int device = 0;
+  int64_t budget = 0;
+  int64_t max_batch_rows = 0;
+  // Slots [0, ngraphs) are complete; fap_server_add_graph fills the next slot
+  // before publishing it, so the worker never sees a slot being built.
+  std::unique_ptr<GSlot> graphs[kMaxGraphs];
+  std::atomic<int> ngraphs{0};
+  std::mutex mu;
+  std::mutex add_mu;  // serialises fap_server_add_graph
+  std::condition_variable cv_work, cv_done;
+  std::deque<Req *> incoming;
+  std::unordered_map<int64_t, Req *> reqs;
+  int64_t next_id = 1;
+  int64_t outstanding = 0;  // submitted, not yet done/failed
+  bool stop = false;
+  std::thread worker;
+  // stats (guarded by mu)
+  std::vector<double> lat_ms;
+  int64_t entries = 0, batches = 0, resident_hits = 0, peak_bytes = 0;
+
+  void loop();
+  bool complete(GSlot &g);
+  bool launch(int gi);
+  int64_t held_bytes();
+  bool make_room(int64_t need, int self, bool *hopeless);
+  void finish(Req *r, int state, int status);
+};
+
+namespace {
+thread_local std::string s_err;
+int serr(int code, const char *msg) {
+  s_err = msg;
+  return code;
+}
+}  // namespace
+
+int64_t fap_server::held_bytes() {
+  int64_t t = 0;
+  const int ng = ngraphs.load(std::memory_order_acquire);
+  for (int i = 0; i < ng; i++) {
+    int64_t b = 0;
+    if (fap_graph_device_bytes(graphs[i]->dg, &b) == FAP_OK) t += b;
+    t += graphs[i]->rows_cap * 4 + graphs[i]->cs_cap * 8;
+  }
+  return t;
+}
+
+namespace {
+void release_rows(GSlot &g) {
+  if (g.rows_buf) cudaFree(g.rows_buf);
+  if (g.cs_buf) cudaFree(g.cs_buf);
+  g.rows_buf = nullptr;
+  g.cs_buf = nullptr;
+  g.rows_cap = 0;
+  g.cs_cap = 0;
+}
+}  // namespace
+
+// Releases idle graphs' output/scratch buffers (least recently used first,
+// graph `self` last) until `need` more bytes fit in the budget.  Returns
+// whether they fit; *hopeless is set when they cannot fit even after every
+// busy graph finishes (nothing else holds memory that could be freed).
+bool fap_server::make_room(int64_t need, int self, bool *hopeless) {
+  *hopeless = false;
+  int64_t held = held_bytes();
+  if (held + need <= budget) return true;
+  std::vector<int> idle;
+  bool others_busy = false;
+  const int ng = ngraphs.load(std::memory_order_acquire);
+  for (int i = 0; i < ng; i++) {
+    if (i == self) continue;
+    if (graphs[i]->busy) others_busy = true;
+    else idle.push_back(i);
+  }
+  std::sort(idle.begin(), idle.end(),
+            [&](int a, int b) { return graphs[a]->last_used < graphs[b]->last_used; });
+  idle.push_back(self);
+  for (int i : idle) {
+    int64_t b = 0;
+    fap_graph_device_bytes(graphs[i]->dg, &b);
+    if (b > graphs[i]->base_bytes || graphs[i]->rows_cap > 0) {
+      fap_graph_release(graphs[i]->dg);
+      graphs[i]->reserved_rows = 0;
+      release_rows(*graphs[i]);
+      held = held_bytes();
+      if (held + need <= budget) return true;
+    }
+  }
+  *hopeless = !others_busy;
+  return false;
+}
+
+void fap_server::finish(Req *r, int state, int status) {
+  r->t_done = now_s();
+  std::lock_guard<std::mutex> lk(mu);
+  r->state = state;
+  r->status = status;
+  outstanding--;
+  if (state == FAP_REQ_DONE) {
+    lat_ms.push_back((r->t_done - r->t_submit) * 1e3);
+    entries += r->entries;
+  }
+  cv_done.notify_all();
+}
+
+// Copies the results of g's finished batch and retires its requests.
+bool fap_server::complete(GSlot &g) {
+  const int rc = fap_graph_check(g.dg);
+  for (Req *r : g.inflight) {
+    int st = rc;
+    if (st == FAP_OK) {
+      if (r->kind == FAP_REQ_SUBGRAPH) {
+        const int32_t p = r->ids[0];
+        if (r->host_out) st = fap_graph_copy_block(g.dg, p, r->host_out, FAP_DTYPE_F32);
+        if (st == FAP_OK && r->cs_out && g.dtype == FAP_DTYPE_I32)
+          st = fap_graph_block_checksums(g.dg, p, r->cs_out);
+      } else {
+        cudaError_t e = cudaSuccess;
+        if (r->host_out)
+          e = cudaMemcpyAsync(r->host_out, g.rows_buf + r->row_off * g.n, (size_t)r->rows * g.n * 4,
+                              cudaMemcpyDeviceToHost, g.stream);
+        if (e == cudaSuccess && r->cs_out && g.dtype == FAP_DTYPE_I32)
+          e = cudaMemcpyAsync(r->cs_out, g.cs_buf + r->row_off, (size_t)r->rows * 8,
+                              cudaMemcpyDeviceToHost, g.stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(g.stream);
+        if (e != cudaSuccess) {
+          cudaGetLastError();
+          st = FAP_ERR_CUDA;
+        }
+      }
+    }
+    finish(r, st == FAP_OK ? FAP_REQ_DONE : FAP_REQ_FAILED, st);
+  }
+  g.inflight.clear();
+  g.busy = false;
+  g.last_used = now_s();
+  return true;
+}
+
+// Starts the next batch of graph gi, if one fits.  Returns whether anything
+// was started or answered.
+bool fap_server::launch(int gi) {
+  GSlot &g = *graphs[gi];
+  bool progressed = false;
+  // Sub-graph requests whose block is still resident: answer at once.
+  while (!g.pending.empty()) {
+    Req *r = g.pending.front();
+    if (r->kind != FAP_REQ_SUBGRAPH || !fap_graph_resident(g.dg, r->ids[0])) break;
+    g.pending.pop_front();
+    r->t_start = now_s();
+    int st = FAP_OK;
+    if (r->host_out) st = fap_graph_copy_block(g.dg, r->ids[0], r->host_out, FAP_DTYPE_F32);
+    if (st == FAP_OK && r->cs_out && g.dtype == FAP_DTYPE_I32)
+      st = fap_graph_block_checksums(g.dg, r->ids[0], r->cs_out);
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      resident_hits++;
+    }
+    finish(r, st == FAP_OK ? FAP_REQ_DONE : FAP_REQ_FAILED, st);
+    progressed = true;
+  }
+  if (g.pending.empty()) return progressed;
+  const int kind = g.pending.front()->kind;
+  std::vector<Req *> batch;
+  std::vector<int32_t> parts;
+  std::vector<char> in_batch(g.K + 1, 0);
+  // Device bytes the batch will need (upper bounds of what fap_solve /
+  // fap_graph_copy_block / fap_graph_rows_async allocate):
+  //   sub-graph: output rows x ldD + one padded Floyd square per part (all of
+  //   the batch's largest side) + SSSP scratch rows (at most one per
+  //   boundary vertex) + the int32->float staging of the largest block;
+  //   rows: result rows + SSSP scratch rows + one checksum per row.
+  int64_t rows = 0, nparts = 0, ldf = 0, srcs = 0, stage_rows = 0;
+  auto footprint = [&](int64_t r, int64_t np, int64_t lf, int64_t sc, int64_t sg) -> int64_t {
+    if (kind == FAP_REQ_ROWS) return r * (int64_t)g.n * 4 * 2 + r * 8;
+    return r * g.ldD * 4 + np * lf * lf * 4 + sc * (int64_t)g.n * 4 + sg * (int64_t)g.n * 4;
+  };
+  for (auto it = g.pending.begin(); it != g.pending.end();) {
+    Req *r = *it;
+    if (r->kind != kind) break;  // one kind per batch, in arrival order
+    int64_t add_rows = 0, n_parts = nparts, n_ldf = ldf, n_srcs = srcs, n_stage = stage_rows;
+    if (kind == FAP_REQ_SUBGRAPH) {
+      const int32_t p = r->ids[0];
+      if (!in_batch[p]) {
+        add_rows = g.vnum[p];
+        n_parts++;
+        n_ldf = std::max<int64_t>(n_ldf, ((int64_t)std::max(g.vnum[p], 1) + 127) / 128 * 128);
+        n_srcs += g.bnum[p];
+      }
+      if (r->host_out && g.dtype == FAP_DTYPE_I32) n_stage = std::max<int64_t>(n_stage, g.vnum[p]);
+    } else {
+      add_rows = (int64_t)r->ids.size();
+    }
+    if (!batch.empty() && max_batch_rows > 0 && rows + add_rows > max_batch_rows) break;
+    bool hopeless = false;
+    if (!make_room(footprint(rows + add_rows, n_parts, n_ldf, n_srcs, n_stage), gi, &hopeless)) {
+      if (!batch.empty()) break;  // run what fits
+      if (!hopeless) return progressed;  // wait for another graph's batch to finish
+      it = g.pending.erase(it);  // larger than the whole budget
+      finish(r, FAP_REQ_FAILED, FAP_ERR_NOMEM);
+      progressed = true;
+      continue;
+    }
+    nparts = n_parts;
+    ldf = n_ldf;
+    srcs = n_srcs;
+    stage_rows = n_stage;
+    batch.push_back(r);
+    rows += add_rows;
+    if (kind == FAP_REQ_SUBGRAPH) {
+      if (!in_batch[r->ids[0]]) parts.push_back(r->ids[0]);
+      in_batch[r->ids[0]] = 1;
+    }
+    it = g.pending.erase(it);
+  }
+  if (batch.empty()) return progressed;
+  int rc = FAP_OK;
+  const double t0 = now_s();
+  if (kind == FAP_REQ_SUBGRAPH) {
+    if (rows > g.reserved_rows) {
+      rc = fap_graph_reserve(g.dg, rows);
+      if (rc == FAP_OK) g.reserved_rows = rows;
+    }
+    if (rc == FAP_OK) rc = fap_solve(g.dg, parts.data(), (int32_t)parts.size(), FAP_MODE_BATCHED);
+  } else {
+    // every rows request of the batch in one SSSP launch
+    std::vector<int32_t> sources;
+    for (Req *r : batch) {
+      r->row_off = (int64_t)sources.size();
+      sources.insert(sources.end(), r->ids.begin(), r->ids.end());
+    }
+    const int64_t need = (int64_t)sources.size() * g.n;
+    if (need > g.rows_cap) {
+      release_rows(g);
+      if (cudaMalloc(&g.rows_buf, (size_t)need * 4) != cudaSuccess) {
+        cudaGetLastError();
+        g.rows_buf = nullptr;
+        rc = FAP_ERR_NOMEM;
+      } else {
+        g.rows_cap = need;
+      }
+    }
+    bool want_cs = false;
+    for (Req *r : batch) want_cs |= (r->cs_out != nullptr);
+    want_cs &= (g.dtype == FAP_DTYPE_I32);
+    if (rc == FAP_OK && want_cs && (int64_t)sources.size() > g.cs_cap) {
+      if (g.cs_buf) cudaFree(g.cs_buf);
+      g.cs_buf = nullptr;
+      g.cs_cap = 0;
+      if (cudaMalloc(&g.cs_buf, sources.size() * 8) != cudaSuccess) {
+        cudaGetLastError();
+        g.cs_buf = nullptr;
+        rc = FAP_ERR_NOMEM;
+      } else {
+        g.cs_cap = (int64_t)sources.size();
+      }
+    }
+    if (rc == FAP_OK) rc = fap_graph_rows_async(g.dg, sources.data(), (int32_t)sources.size(), g.rows_buf);
+    if (rc == FAP_OK && want_cs) {
+      int64_t launches = 0;
+      if (fapb::launch_row_checksums(g.rows_buf, (int64_t)sources.size(), g.n, g.n, g.cs_buf, g.stream,
+                                     &launches) != cudaSuccess) {
+        cudaGetLastError();
+        rc = FAP_ERR_CUDA;
+      }
+    }
+  }
+  if (rc != FAP_OK) {
+    for (Req *r : batch) finish(r, FAP_REQ_FAILED, rc);
+    return true;
+  }
+  cudaEventRecord(g.done, g.stream);
+  for (Req *r : batch) {
+    r->t_start = t0;
+    std::lock_guard<std::mutex> lk(mu);
+    r->state = FAP_REQ_RUNNING;
+  }
+  g.inflight = std::move(batch);
+  g.batch_kind = kind;
+  g.busy = true;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    batches++;
+    peak_bytes = std::max(peak_bytes, held_bytes());
+  }
+  return true;
+}
+
+void fap_server::loop() {
+  cudaSetDevice(device);
+  size_t rr = 0;
+  for (;;) {
+    {
+      std::unique_lock<std::mutex> lk(mu);
+      const int ng = ngraphs.load(std::memory_order_acquire);
+      bool any_busy = false, any_pending = !incoming.empty();
+      for (int i = 0; i < ng; i++) {
+        any_busy |= graphs[i]->busy;
+        any_pending |= !graphs[i]->pending.empty();
+      }
+      if (!any_busy && !any_pending) {
+        if (stop) break;
+        cv_work.wait_for(lk, std::chrono::milliseconds(2));
+      }
+      while (!incoming.empty()) {
+        Req *r = incoming.front();
+        incoming.pop_front();
+        graphs[r->graph]->pending.push_back(r);
+      }
+      if (stop && !any_busy) {
+        // fail what is still queued
+        std::vector<Req *> dead;
+        for (int i = 0; i < ng; i++) {
+          for (Req *r : graphs[i]->pending) dead.push_back(r);
+          graphs[i]->pending.clear();
+        }
+        lk.unlock();
+        for (Req *r : dead) finish(r, FAP_REQ_FAILED, FAP_ERR_STATE);
+        break;
+      }
+    }
+    bool progressed = false;
+    const int ng = ngraphs.load(std::memory_order_acquire);
+    for (int i = 0; i < ng; i++)
+      if (graphs[i]->busy && cudaEventQuery(graphs[i]->done) != cudaErrorNotReady)
+        progressed |= complete(*graphs[i]);
+    if (!stop) {
+      for (int k = 0; k < ng; k++) {
+        const int gi = (int)((rr + (size_t)k) % (size_t)ng);
+        if (!graphs[gi]->busy && !graphs[gi]->pending.empty()) progressed |= launch(gi);
+      }
+      rr++;
+    }
+    if (!progressed) std::this_thread::sleep_for(std::chrono::microseconds(20));
+  }
+}
+
+extern "C" {
+
+int fap_server_create(int device, double budget_bytes, int64_t max_batch_rows, fap_server **out) {
+  if (!out) return serr(FAP_ERR_INVALID, "NULL out");
+  *out = nullptr;
+  if (cudaSetDevice(device) != cudaSuccess) {
+    cudaGetLastError();
+    return serr(FAP_ERR_CUDA, "cannot use the device");
+  }
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+    cudaGetLastError();
+    return serr(FAP_ERR_CUDA, "cudaMemGetInfo failed");
+  }
+  auto *s = new fap_server();
+  s->device = device;
+  s->budget = budget_bytes > 0 ? (int64_t)budget_bytes : (int64_t)(0.6 * (double)free_b);
+  s->max_batch_rows = max_batch_rows;
+  s->worker = std::thread([s] { s->loop(); });
+  *out = s;
+  return FAP_OK;
+}
+
+int fap_server_destroy(fap_server *s) {
+  if (!s) return FAP_OK;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+    s->cv_work.notify_all();
+  }
+  if (s->worker.joinable()) s->worker.join();
+  // requests submitted after the worker stopped
+  for (Req *r : s->incoming) {
+    r->state = FAP_REQ_FAILED;
+    r->status = FAP_ERR_STATE;
+  }
+  s->incoming.clear();
+  const int ng = s->ngraphs.load();
+  for (int i = 0; i < ng; i++) {
+    GSlot &g = *s->graphs[i];
+    if (g.done) cudaEventDestroy(g.done);
+    release_rows(g);
+    fap_graph_destroy(g.dg);
+    fap_ctx_destroy(g.ctx);
+  }
+  for (auto &kv : s->reqs) delete kv.second;
+  delete s;
+  return FAP_OK;
+}
+
+int fap_server_add_graph(fap_server *s, int32_t n, int64_t m, const int32_t *row_offset,
+                         const int32_t *col_val, const float *weight, int dtype, int32_t K,
+                         const int32_t *graph_id, const int32_t *st2ed, const int32_t *ver_num,
+                         const int32_t *ver_offset, const int32_t *bdy_num, int32_t *index) {
+  if (!s || !index) return serr(FAP_ERR_INVALID, "NULL argument");
+  std::lock_guard<std::mutex> add_lock(s->add_mu);
+  const int slot = s->ngraphs.load();
+  if (slot >= kMaxGraphs) return serr(FAP_ERR_NOMEM, "too many graphs");
+  auto g = std::make_unique<GSlot>();
+  int rc = fap_ctx_create(s->device, &g->ctx);
+  if (rc != FAP_OK) return serr(rc, fap_last_error());
+  rc = fap_graph_create(g->ctx, n, m, row_offset, col_val, weight, dtype, &g->dg);
+  if (rc == FAP_OK)
+    rc = fap_graph_set_parts(g->dg, K, graph_id, st2ed, ver_num, ver_offset, bdy_num);
+  if (rc != FAP_OK) {
+    std::string msg = fap_last_error();
+    if (g->dg) fap_graph_destroy(g->dg);
+    fap_ctx_destroy(g->ctx);
+    return serr(rc, msg.c_str());
+  }
+  g->n = n;
+  g->K = K;
+  g->dtype = fap_graph_dtype(g->dg);
+  g->ldD = ((int64_t)n + 127) / 128 * 128;
+  g->vnum.assign(ver_num, ver_num + K + 1);
+  g->voff.assign(ver_offset, ver_offset + K + 1);
+  g->bnum.assign(bdy_num, bdy_num + K + 1);
+  // Batches change from one launch to the next: launch the stages directly
+  // instead of capturing a CUDA graph per batch.
+  fap_graph_set_param(g->dg, "cuda_graph", 0);
+  fap_graph_device_bytes(g->dg, &g->base_bytes);
+  void *stream = nullptr;
+  fap_ctx_get_stream(g->ctx, &stream);
+  g->stream = reinterpret_cast<cudaStream_t>(stream);
+  if (cudaEventCreateWithFlags(&g->done, cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError();
+    fap_graph_destroy(g->dg);
+    fap_ctx_destroy(g->ctx);
+    return serr(FAP_ERR_CUDA, "cudaEventCreate failed");
+  }
+  s->graphs[slot] = std::move(g);
+  s->ngraphs.store(slot + 1, std::memory_order_release);
+  *index = slot;
+  return FAP_OK;
+}
+
+int fap_server_submit(fap_server *s, int32_t graph, int kind, const int32_t *ids, int32_t count,
+                      float *host_out, uint64_t *checksums_out, int64_t *req_id) {
+  if (!s || !ids || !req_id || count <= 0) return serr(FAP_ERR_INVALID, "bad request arguments");
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (s->stop) return serr(FAP_ERR_STATE, "server is stopping");
+  if (graph < 0 || graph >= s->ngraphs.load()) return serr(FAP_ERR_INVALID, "no such graph");
+  GSlot &g = *s->graphs[graph];
+  auto *r = new Req();
+  r->graph = graph;
+  r->kind = kind;
+  r->ids.assign(ids, ids + count);
+  r->host_out = host_out;
+  r->cs_out = checksums_out;
+  if (kind == FAP_REQ_SUBGRAPH) {
+    if (count != 1 || ids[0] < 1 || ids[0] > g.K) {
+      delete r;
+      return serr(FAP_ERR_INVALID, "a sub-graph request names one part id in 1..K");
+    }
+    r->rows = g.vnum[ids[0]];
+  } else if (kind == FAP_REQ_ROWS) {
+    for (int32_t i = 0; i < count; i++)
+      if (ids[i] < 0 || ids[i] >= g.n) {
+        delete r;
+        return serr(FAP_ERR_INVALID, "source vertex out of range");
+      }
+    r->rows = count;
+  } else {
+    delete r;
+    return serr(FAP_ERR_INVALID, "unknown request kind");
+  }
+  r->entries = r->rows * (int64_t)g.n;
+  r->id = s->next_id++;
+  r->t_submit = now_s();
+  s->reqs[r->id] = r;
+  s->outstanding++;
+  s->incoming.push_back(r);
+  s->cv_work.notify_all();
+  *req_id = r->id;
+  return FAP_OK;
+}
+
+int fap_server_wait(fap_server *s, int64_t req_id, double timeout_s, int *state) {
+  if (!s) return serr(FAP_ERR_INVALID, "NULL server");
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->reqs.find(req_id);
+  if (it == s->reqs.end()) return serr(FAP_ERR_INVALID, "unknown request");
+  Req *r = it->second;
+  auto done = [&] { return r->state == FAP_REQ_DONE || r->state == FAP_REQ_FAILED; };
+  if (timeout_s < 0) s->cv_done.wait(lk, done);
+  else s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), done);
+  if (state) *state = r->state;
+  return FAP_OK;
+}
+
+int fap_server_request_info(fap_server *s, int64_t req_id, double *out4) {
+  if (!s || !out4) return serr(FAP_ERR_INVALID, "NULL argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->reqs.find(req_id);
+  if (it == s->reqs.end()) return serr(FAP_ERR_INVALID, "unknown request");
+  Req *r = it->second;
+  const bool fin = r->state == FAP_REQ_DONE || r->state == FAP_REQ_FAILED;
+  out4[0] = fin ? (r->t_done - r->t_submit) * 1e3 : -1.0;
+  out4[1] = r->t_start > 0 ? (r->t_start - r->t_submit) * 1e3 : -1.0;
+  out4[2] = (double)r->entries;
+  out4[3] = (double)r->status;
+  return FAP_OK;
+}
+
+int fap_server_forget(fap_server *s, int64_t req_id) {
+  if (!s) return serr(FAP_ERR_INVALID, "NULL server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->reqs.find(req_id);
+  if (it == s->reqs.end()) return FAP_OK;
+  if (it->second->state != FAP_REQ_DONE && it->second->state != FAP_REQ_FAILED)
+    return serr(FAP_ERR_STATE, "request still in flight");
+  delete it->second;
+  s->reqs.erase(it);
+  return FAP_OK;
+}
+
+int fap_server_drain(fap_server *s) {
+  if (!s) return serr(FAP_ERR_INVALID, "NULL server");
+  std::unique_lock<std::mutex> lk(s->mu);
+  s->cv_done.wait(lk, [&] { return s->outstanding == 0; });
+  return FAP_OK;
+}
+
+int fap_server_stats(fap_server *s, double *out8) {
+  if (!s || !out8) return serr(FAP_ERR_INVALID, "NULL argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  std::vector<double> v = s->lat_ms;
+  std::sort(v.begin(), v.end());
+  auto pct = [&](double q) {
+    if (v.empty()) return 0.0;
+    const size_t i = std::min(v.size() - 1, (size_t)(q * (double)(v.size() - 1) + 0.5));
+    return v[i];
+  };
+  double mean = 0;
+  for (double x : v) mean += x;
+  out8[0] = (double)v.size();
+  out8[1] = (double)s->entries;
+  out8[2] = pct(0.50);
+  out8[3] = pct(0.99);
+  out8[4] = v.empty() ? 0.0 : mean / (double)v.size();
+  out8[5] = (double)s->peak_bytes;
+  out8[6] = (double)s->batches;
+  out8[7] = (double)s->resident_hits;
+  return FAP_OK;
+}
+
+int fap_server_reset_stats(fap_server *s) {
+  if (!s) return serr(FAP_ERR_INVALID, "NULL server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->lat_ms.clear();
+  s->entries = 0;
+  s->batches = 0;
+  s->resident_hits = 0;
+  s->peak_bytes = 0;
+  return FAP_OK;
+}
+
+const char *fap_server_last_error(void) { return s_err.c_str(); }
+
+}  // extern "C"

@@ -196,6 +196,51 @@ def random_geometric_graph(n: int, avg_degree: float, *, seed: int = 0,
     return road_graph(n, seed=seed, wmin=wmin, wmax=wmax, target_avg_degree=avg_degree)
 
 
+def edges_to_csr(g: EdgeList):
+    """CSR (row_offset, col_val, weight) of g with both directions of every
+    undirected edge; within a row, edges keep their input order."""
+    e = g.edges
+    if g.directed:
+        src, dst, w = e[:, 0], e[:, 1], g.weights
+    else:
+        src = np.concatenate([e[:, 0], e[:, 1]])
+        dst = np.concatenate([e[:, 1], e[:, 0]])
+        w = np.concatenate([g.weights, g.weights])
+    order = np.argsort(src, kind="stable")
+    ro = np.zeros(g.n + 1, np.int64)
+    np.add.at(ro, src + 1, 1)
+    return (np.cumsum(ro).astype(np.int32), dst[order].astype(np.int32),
+            w[order].astype(np.float32))
+
+
+# --------------------------------------------------------------------------
+# The serving stream: many resident graphs of different sizes
+# --------------------------------------------------------------------------
+
+def serve_specs(count: int = 32, seed: int = 17, n_range=(16000, 200000),
+                rows_range=(100, 10000), degree_range=(2.0, 4.0)) -> list:
+    """Seeded specs of the serving stream's random-geometric graphs: n
+    log-uniform in n_range, average degree uniform in degree_range, int
+    weights U[1,1000], and K a power of two in [16, 256] chosen so that the
+    parts' row counts (n / K) spread log-uniformly over rows_range."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(count):
+        n = int(round(np.exp(rng.uniform(np.log(n_range[0]), np.log(n_range[1])))))
+        rows = np.exp(rng.uniform(np.log(rows_range[0]), np.log(rows_range[1])))
+        K = int(2 ** np.clip(np.round(np.log2(n / rows)), 4, 8))
+        specs.append(dict(name=f"rgg{i:02d}", n=n, K=K,
+                          avg_degree=float(rng.uniform(*degree_range)), seed=1000 + i))
+    return specs
+
+
+def serve_graph_csr(spec: dict):
+    """(spec, row_offset, col_val, weight) of one serving-stream graph
+    (module-level so that a process pool can build the graphs in parallel)."""
+    el = random_geometric_graph(spec["n"], spec["avg_degree"], seed=spec["seed"])
+    return (spec,) + edges_to_csr(el)
+
+
 # --------------------------------------------------------------------------
 # The benchmark workloads, by name
 # --------------------------------------------------------------------------

@@ -67,3 +67,32 @@ def load(name: str, root: str | None = None) -> Workload:
     g.preCondition()
     vn, vo, bn = g.partInfo()
     return Workload(name, spec["K"], el, root, g, g.num_vertexs, vn, vo, bn)
+
+
+@dataclass
+class ServeGraph:
+    name: str
+    n: int
+    K: int
+    avg_degree: float
+    graph: fapGraph     # after preCondition (partition + renumbering)
+
+
+def load_serve_stream(count: int = 32, procs: int = 0, seed: int = 17) -> list:
+    """The serving stream's resident graphs (generators.serve_specs), built in
+    a spawn-started process pool and partitioned on the host (METIS)."""
+    import multiprocessing as mp
+    specs = G.serve_specs(count, seed)
+    procs = procs or max(1, min(8, os.cpu_count() or 1, count))
+    if procs > 1:
+        with mp.get_context("spawn").Pool(procs) as pool:
+            built = pool.map(G.serve_graph_csr, specs)
+    else:
+        built = [G.serve_graph_csr(s) for s in specs]
+    out = []
+    for spec, ro, col, w in built:
+        g = fapGraph.from_csr(spec["n"], int(ro[-1]), ro, col, w, spec["K"])
+        g.preCondition()
+        out.append(ServeGraph(spec["name"], spec["n"], spec["K"],
+                              round(float(ro[-1]) / spec["n"], 3), g))
+    return out

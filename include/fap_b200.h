@@ -159,6 +159,18 @@ FAP_API int fap_graph_tune_sssp(fap_dgraph *g, const double *deltas, int32_t cou
 /* Mean edge weight of the graph (the scale SSSP bucket widths are tuned in). */
 FAP_API double fap_graph_mean_weight(const fap_dgraph *g);
 
+/* Frees the output matrix, Floyd arena and scratch of g (the CSR and the
+ * partition stay resident); no block stays resident afterwards. */
+FAP_API int fap_graph_release(fap_dgraph *g);
+/* Device bytes g holds now. */
+FAP_API int fap_graph_device_bytes(const fap_dgraph *g, int64_t *bytes);
+/* 1 if part's block is resident in g's output matrix, else 0. */
+FAP_API int fap_graph_resident(fap_dgraph *g, int32_t part);
+/* Queues, on the context stream, shortest-distance rows from count sources
+ * (host ids) into d_out (device, count x n floats, dense); returns without
+ * waiting.  Device errors surface in fap_graph_check. */
+FAP_API int fap_graph_rows_async(fap_dgraph *g, const int32_t *sources, int32_t count, float *d_out);
+
 /* Device time (ms) of the stages of the last fap_solve, measured with events
  * on the context stream: [sssp, gather, floyd, minplus, total]. */
 FAP_API int fap_graph_last_timing(fap_dgraph *g, float *ms5);

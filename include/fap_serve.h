@@ -1,0 +1,95 @@
+/*
+ * fap_serve.h -- serving loop over resident graphs (no counterpart in the
+ * reference, whose fapGraph solves one part per call on the caller's thread).
+ *
+ * A server owns one CUDA device.  Graphs are added once (CSR + partition
+ * stay resident in HBM).  Clients submit requests from any thread:
+ *   FAP_REQ_SUBGRAPH  the block of one part (ver_num[part] x n distances,
+ *                     what solveSubGraph computes, fap/fap.cpp:197-207);
+ *   FAP_REQ_ROWS      shortest-distance rows from a list of source vertices.
+ * A worker thread batches pending requests per graph (all sub-graph requests
+ * of a graph that fit one batch run as one batched solve; a request for a
+ * part that is still resident from an earlier batch is answered without
+ * recomputing), admits a batch only when its estimated device footprint
+ * fits the memory budget (idle graphs' buffers are released first), and
+ * runs each graph on its own stream, so batches of different graphs overlap
+ * on the GPU while new requests keep arriving (continuous batching).
+ * Results are copied to the caller's host buffers (float distances) and/or
+ * reduced to per-row checksums (int32 graphs).
+ */
+#ifndef FAP_SERVE_H_
+#define FAP_SERVE_H_
+
+#include <stdint.h>
+
+#include "fap_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct fap_server fap_server;
+
+#define FAP_REQ_SUBGRAPH 0
+#define FAP_REQ_ROWS 1
+
+#define FAP_REQ_PENDING 0
+#define FAP_REQ_RUNNING 1
+#define FAP_REQ_DONE 2
+#define FAP_REQ_FAILED 3
+
+/* budget_bytes: device memory the server may hold for outputs and scratch
+ * (<= 0: 60% of the free memory at creation).  max_batch_rows: output rows of
+ * one batch (<= 0: no limit beyond the budget). */
+FAP_API int fap_server_create(int device, double budget_bytes, int64_t max_batch_rows,
+                              fap_server **out);
+/* Waits for the requests in flight, fails the queued ones, frees everything. */
+FAP_API int fap_server_destroy(fap_server *s);
+
+/* Adds a resident graph: CSR (weights as float, see fap_graph_create) and
+ * its partition / renumbering (see fap_graph_set_parts).  Host pointers,
+ * copied.  *index receives the graph's index for fap_server_submit. */
+FAP_API int fap_server_add_graph(fap_server *s, int32_t n, int64_t m, const int32_t *row_offset,
+                                 const int32_t *col_val, const float *weight, int dtype, int32_t K,
+                                 const int32_t *graph_id, const int32_t *st2ed,
+                                 const int32_t *ver_num, const int32_t *ver_offset,
+                                 const int32_t *bdy_num, int32_t *index);
+
+/* Submits a request.  FAP_REQ_SUBGRAPH: ids = {part} (count 1, 1-based);
+ * FAP_REQ_ROWS: ids = source vertices (count >= 1).  host_out (optional)
+ * receives rows x n float distances; checksums_out (optional, int32 graphs,
+ * either kind) receives one checksum per row (fap_graph_block_checksums'
+ * definition).
+ * Both must stay valid until the request is done.  *req_id identifies it. */
+FAP_API int fap_server_submit(fap_server *s, int32_t graph, int kind, const int32_t *ids,
+                              int32_t count, float *host_out, uint64_t *checksums_out,
+                              int64_t *req_id);
+
+/* Waits up to timeout_s (< 0: forever) for a request; *state receives
+ * FAP_REQ_*.  A done or failed request stays queryable until forgotten. */
+FAP_API int fap_server_wait(fap_server *s, int64_t req_id, double timeout_s, int *state);
+
+/* Per-request figures: out4 = [latency ms (submit -> done), queue ms
+ * (submit -> start on the GPU), entries (rows x n), status (FAP_* code)]. */
+FAP_API int fap_server_request_info(fap_server *s, int64_t req_id, double *out4);
+
+/* Drops a finished request's record. */
+FAP_API int fap_server_forget(fap_server *s, int64_t req_id);
+
+/* Waits until every submitted request is done or failed. */
+FAP_API int fap_server_drain(fap_server *s);
+
+/* out8 = [requests completed, entries produced, p50 latency ms, p99 latency
+ * ms, mean latency ms, peak device bytes held, batches launched, requests
+ * answered from resident blocks] over the requests completed since the last
+ * reset. */
+FAP_API int fap_server_stats(fap_server *s, double *out8);
+FAP_API int fap_server_reset_stats(fap_server *s);
+
+/* Message of the last fap_server_* failure on the calling thread. */
+FAP_API const char *fap_server_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FAP_SERVE_H_ */

@@ -68,3 +68,20 @@ def test_context_without_gpu_fails_loudly():
     rc = L.lib().fap_ctx_create(0, ctypes.byref(h))
     assert rc == L.FAP_ERR_CUDA
     assert "device" in L.last_error().lower()
+
+
+def test_server_without_gpu_fails_loudly():
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a GPU is present")
+    except Exception:
+        pass
+    h = ctypes.c_void_p()
+    rc = L.lib().fap_server_create(0, 0.0, 0, ctypes.byref(h))
+    assert rc == L.FAP_ERR_CUDA and not h.value
+    assert "device" in L.last_error().lower()
+    # NULL handles are rejected, not dereferenced
+    assert L.lib().fap_server_submit(None, 0, 0, None, 1, None, None, None) == L.FAP_ERR_INVALID
+    assert L.lib().fap_server_drain(None) == L.FAP_ERR_INVALID
+    assert L.lib().fap_server_destroy(None) == L.FAP_OK
