@@ -298,8 +298,12 @@ def run_serving(args, device):
                 raise RuntimeError(f"serving request failed: {h.info()}")
             h.forget()
 
-    # warm-up: one request per graph (first allocations)
-    finish([srv.submit_subgraph(i, 1, distances=False, checksums=True) for i, *_ in info])
+    # warm-up: one request of each kind per graph (resident caches, batch buffers)
+    finish([srv.submit_subgraph(i, 1, distances=False, checksums=True) for i, *_ in info] +
+           [srv.submit_rows(i, np.arange(100, dtype=np.int32) % n, distances=False, checksums=True)
+            for i, n, *_ in info])
+    warm = srv.stats()
+    log(f"serving warm-up: {warm.cache_builds} caches built, {warm.busy_ms:.1f} ms device time")
     srv.reset_stats()
     # capacity: closed-loop burst
     reqs = [draw() for _ in range(args.serve_burst)]
@@ -318,7 +322,9 @@ def run_serving(args, device):
            "budget_bytes": int(0.6 * free_b),
            "capacity": {"requests_s": cap_rps, "entries_s": st.entries / burst_s,
                         "requests": len(reqs), "batches": st.batches,
-                        "resident_hits": st.resident_hits, "p50_ms": st.p50_ms, "p99_ms": st.p99_ms},
+                        "resident_hits": st.resident_hits, "p50_ms": st.p50_ms, "p99_ms": st.p99_ms,
+                        "device_busy_frac": st.busy_ms * 1e-3 / burst_s},
+           "warmup_cache_builds": warm.cache_builds,
            "loads": []}
     log(f"serving capacity {cap_rps:.1f} req/s, {st.entries / burst_s:.4g} entries/s")
     for frac in (0.25, 0.5, 0.9):
@@ -347,7 +353,8 @@ def run_serving(args, device):
                              "achieved_requests_s": count / wall, "entries_s": st.entries / wall,
                              "p50_ms": st.p50_ms, "p99_ms": st.p99_ms, "mean_ms": st.mean_ms,
                              "batches": st.batches, "resident_hits": st.resident_hits,
-                             "peak_device_bytes": st.peak_bytes})
+                             "peak_device_bytes": st.peak_bytes, "cache_builds": st.cache_builds,
+                             "device_busy_frac": st.busy_ms * 1e-3 / wall})
         log(f"serving at {frac:.0%}: p50 {st.p50_ms:.2f} ms, p99 {st.p99_ms:.2f} ms, "
             f"{st.entries / wall:.4g} entries/s, {st.batches} batches")
     srv.close()

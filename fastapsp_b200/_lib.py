@@ -91,6 +91,9 @@ _SIGS = {
     "fap_graph_device_bytes": (INT, [P, ctypes.POINTER(I64)]),
     "fap_graph_resident": (INT, [P, I32]),
     "fap_graph_rows_async": (INT, [P, P, I32, P]),
+    "fap_graph_cache_build": (INT, [P]),
+    "fap_graph_cache_release": (INT, [P]),
+    "fap_graph_cache_bytes": (INT, [P, ctypes.POINTER(I64), ctypes.POINTER(INT)]),
     "fap_server_create": (INT, [INT, DBL, I64, PP]),
     "fap_server_destroy": (INT, [P]),
     "fap_server_add_graph": (INT, [P, I32, I64, P, P, P, INT, I32, P, P, P, P, P, ctypes.POINTER(I32)]),
@@ -99,8 +102,12 @@ _SIGS = {
     "fap_server_request_info": (INT, [P, I64, P]),
     "fap_server_forget": (INT, [P, I64]),
     "fap_server_drain": (INT, [P]),
-    "fap_server_stats": (INT, [P, P]),
+    "fap_server_stats": (INT, [P, P, I32]),
     "fap_server_reset_stats": (INT, [P]),
+    "fap_server_set_option": (INT, [P, ctypes.c_char_p, DBL]),
+    "fap_graph_checksums_async": (INT, [P, I32, P]),
+    "fap_graph_status_async": (INT, [P, P]),
+    "fap_status_code": (INT, [I32]),
     "fap_server_last_error": (ctypes.c_char_p, []),
     "fap_floyd_noalloc": (INT, [INT, I32, P, I64, P]),
     "fap_floyd_noalloc_last_error": (ctypes.c_char_p, []),

@@ -59,11 +59,22 @@ cudaError_t record_event(cudaEvent_t ev, cudaStream_t st) {
                                              : cudaEventRecord(ev, st);
 }
 
+// Bytes a DevBuf allocates for `want`: small buffers (descriptors, source
+// lists) grow to the next power of two, so that batches of changing
+// composition rarely reallocate (each cudaFree synchronises the device).
+size_t alloc_size(size_t want) {
+  if (want == 0 || want > (size_t(64) << 20)) return want;
+  size_t r = 4096;
+  while (r < want) r <<= 1;
+  return r;
+}
+
 struct DevBuf {
   void *p = nullptr;
   size_t bytes = 0;
   int ensure(size_t want) {
     if (want <= bytes) return FAP_OK;
+    want = alloc_size(want);
     if (p) cudaFree(p);
     p = nullptr;
     bytes = 0;
@@ -147,6 +158,7 @@ struct fap_dgraph {
   std::vector<int32_t> thin_pos;  // per batch index: position in thin, or -1
   DevBuf d_thin;
   std::vector<int32_t> last_ids;
+  bool last_cached = false;  // last_ids' descriptors point into the resident cache
   int64_t f_elems = 0;
   int max_ldf = 0, max_b = 0, max_s = 0;
   // tuning
@@ -163,6 +175,15 @@ struct fap_dgraph {
   uint64_t gexec_epoch = 0;
   cudaStream_t gexec_stream = nullptr;
   int64_t gexec_launches = 0;
+  // Resident cache: the boundary rows of every part (cBd, rows in part order,
+  // cb_off[p] = first row of part p) and every part's closed Floyd matrix
+  // (cF, equal padded squares of side cache_ldf, part p at (p - 1)).
+  bool cache_ready = false;
+  bool use_cache = true;
+  DevBuf cBd, cF, d_cparts, d_rowgroups, d_rowloc, d_rowout, d_rowidx;
+  std::vector<int64_t> cb_off;
+  std::vector<PartDesc> cparts;
+  int cache_ldf = 0, cache_max_b = 0, cache_max_s = 0;
   // last solve
   int last_mode = -1;
   float timing[5] = {-1, -1, -1, -1, -1};
@@ -336,6 +357,19 @@ extern "C" int fap_graph_create(fap_ctx *ctx, int32_t n, int64_t m, const int32_
   return FAP_OK;
 }
 
+namespace {
+void cache_drop(fap_dgraph *G) {
+  for (DevBuf *b : {&G->cBd, &G->cF, &G->d_cparts, &G->d_rowgroups, &G->d_rowloc, &G->d_rowout,
+                    &G->d_rowidx})
+    b->release();
+  G->cache_ready = false;
+  G->cb_off.clear();
+  G->cparts.clear();
+  G->last_ids.clear();
+  G->epoch++;
+}
+}  // namespace
+
 extern "C" int fap_graph_destroy(fap_dgraph *G) {
   if (!G) return FAP_OK;
   fap_ctx *c = G->ctx;
@@ -347,6 +381,7 @@ extern "C" int fap_graph_destroy(fap_dgraph *G) {
                       &G->d_gid, &G->d_st2ed, &G->d_ed2st, &G->D, &G->F, &G->d_parts, &G->d_work,
                       &G->d_src, &G->d_srcrows, &G->d_status, &G->d_checks, &G->staging})
       b->release();
+    cache_drop(G);
   }
   delete G;
   c->graphs--;
@@ -391,6 +426,7 @@ extern "C" int fap_graph_set_parts(fap_dgraph *G, int32_t K, const int32_t *grap
   G->bnum.assign(bdy_num, bdy_num + K + 1);
   G->row_base.assign(K + 1, -1);
   G->last_ids.clear();
+  cache_drop(G);
   FAP_TRY(G->d_gid.ensure((size_t)n * 4));
   FAP_TRY(G->d_st2ed.ensure((size_t)n * 4));
   FAP_TRY(G->d_ed2st.ensure((size_t)n * 4));
@@ -440,8 +476,8 @@ extern "C" int fap_graph_reserve(fap_dgraph *G, int64_t max_rows) {
 namespace {
 
 // Builds (or reuses) the batch descriptors for the requested parts.
-int prepare_batch(fap_dgraph *G, const std::vector<int32_t> &ids) {
-  const bool same = (ids == G->last_ids);
+int prepare_batch(fap_dgraph *G, const std::vector<int32_t> &ids, bool cached) {
+  const bool same = (ids == G->last_ids) && (cached == G->last_cached);
   if (same) return FAP_OK;
   const int64_t n = G->n;
   const bool full = (G->max_rows == n);
@@ -469,9 +505,11 @@ int prepare_batch(fap_dgraph *G, const std::vector<int32_t> &ids) {
   G->part_work_end.clear();
   G->thin.clear();
   G->thin_pos.clear();
-  // Floyd arena: equal padded squares (one tensor map describes all parts)
+  // Floyd arena: equal padded squares (one tensor map describes all parts);
+  // with the resident cache, the parts' closed matrices in the cache.
   int32_t ldf = kFloydTile;
   for (int32_t p : ids) ldf = std::max<int32_t>(ldf, (int32_t)round_up(std::max(G->vnum[p], 1), kFloydTile));
+  if (cached) ldf = G->cache_ldf;
   int64_t foff = 0;
   G->max_ldf = ldf;
   G->max_b = 0;
@@ -485,7 +523,8 @@ int prepare_batch(fap_dgraph *G, const std::vector<int32_t> &ids) {
     d.b = G->bnum[p];
     d.row_base = base[i];
     d.ldf = ldf;
-    d.f_off = foff;
+    d.f_off = cached ? (int64_t)(p - 1) * ldf * ldf : foff;
+    d.bd_row = cached ? (int32_t)G->cb_off[p] : 0;
     foff += (int64_t)d.ldf * d.ldf;
     G->max_b = std::max(G->max_b, d.b);
     G->max_s = std::max(G->max_s, d.s);
@@ -506,14 +545,15 @@ int prepare_batch(fap_dgraph *G, const std::vector<int32_t> &ids) {
     G->part_work_end.push_back((int32_t)G->work.size());
   }
   G->f_elems = foff;
-  FAP_TRY(G->F.ensure((size_t)std::max<int64_t>(foff, 1) * 4));
+  if (!cached) FAP_TRY(G->F.ensure((size_t)std::max<int64_t>(foff, 1) * 4));
   FAP_TRY(G->d_parts.ensure(std::max<size_t>(G->parts.size(), 1) * sizeof(PartDesc)));
   FAP_TRY(G->d_work.ensure(std::max<size_t>(G->work.size(), 1) * sizeof(MPWork)));
   FAP_TRY(G->d_thin.ensure(std::max<size_t>(G->thin.size(), 1) * 4));
   FAP_TRY(G->d_src.ensure(std::max<size_t>(G->src.size(), 1) * 4));
   FAP_TRY(G->d_srcrows.ensure(std::max<size_t>(G->srcrows.size(), 1) * 8));
-  FAP_TRY(G->sssp_scratch.ensure(
-      (size_t)std::max(sssp_scratch_rows(G->n, (int)G->src.size()), 1) * (size_t)G->n * 4));
+  if (!cached)
+    FAP_TRY(G->sssp_scratch.ensure(
+        (size_t)std::max(sssp_scratch_rows(G->n, (int)G->src.size()), 1) * (size_t)G->n * 4));
   cudaStream_t st = G->ctx->stream;
   FAP_CK(cudaStreamSynchronize(st));
   FAP_CK(cudaMemcpy(G->d_parts.p, G->parts.data(), G->parts.size() * sizeof(PartDesc), cudaMemcpyHostToDevice));
@@ -528,6 +568,7 @@ int prepare_batch(fap_dgraph *G, const std::vector<int32_t> &ids) {
   // Rows of other parts may have been overwritten by this batch.
   std::fill(G->row_base.begin(), G->row_base.end(), -1);
   G->last_ids = ids;
+  G->last_cached = cached;
   G->epoch++;
   return FAP_OK;
 }
@@ -568,7 +609,21 @@ int run_solve(fap_dgraph *G, int mode) {
   int64_t L = 0;
   FAP_CK(cudaMemsetAsync(status, 0, sizeof(int), st));
   for (int i = 0; i < 5; i++) G->timing[i] = -1.0f;
-  if (mode == FAP_MODE_BATCHED) {
+  if (mode == FAP_MODE_BATCHED && G->last_cached) {
+    // Resident cache: boundary rows and closed Floyd matrices are ready;
+    // copy the boundary rows into the block and run the min-plus merge.
+    const T *cF = G->cF.as<const T>();
+    FAP_CK(record_event(c->ev[0], st));
+    FAP_CK(record_event(c->ev[1], st));
+    FAP_CK(launch_bdy_copy<T>(dp, np, G->max_b, G->cBd.as<const T>(), D, G->ldD, st, &L));
+    FAP_CK(record_event(c->ev[2], st));
+    FAP_CK(record_event(c->ev[3], st));
+    FAP_CK(launch_minplus_thin<T>(dp, G->d_thin.as<int32_t>(), (int)G->thin.size(), G->max_s, G->n, cF, D,
+                                  G->ldD, gid, ed2st, st, &L));
+    FAP_CK(launch_minplus_parts<T>(dp, (int)G->K, dw, (int)G->work.size(), G->n, cF, G->cache_ldf, D,
+                                   G->ldD, G->max_rows, gid, ed2st, status, st, &L));
+    FAP_CK(record_event(c->ev[4], st));
+  } else if (mode == FAP_MODE_BATCHED) {
     FAP_CK(record_event(c->ev[0], st));
     FAP_CK(launch_sssp<T>(ro_s, col_s, w_s, G->n, src, srow, (int)G->src.size(), D, G->ldD, G->ldD,
                           ed2st, scratch, delta, G->sssp_chain, G->sssp_precheck, max_rounds, status, st, &L));
@@ -583,7 +638,7 @@ int run_solve(fap_dgraph *G, int mode) {
       FAP_CK(launch_bdy_scatter<T>(dp, np, F, D, G->ldD, st2ed, G->max_b, G->max_s, st, &L));
     }
     FAP_CK(record_event(c->ev[3], st));
-    FAP_CK(launch_minplus_thin<T>(dp, G->d_thin.as<int32_t>(), (int)G->thin.size(), G->n, F, D,
+    FAP_CK(launch_minplus_thin<T>(dp, G->d_thin.as<int32_t>(), (int)G->thin.size(), G->max_s, G->n, F, D,
                                   G->ldD, gid, ed2st, st, &L));
     FAP_CK(launch_minplus_parts<T>(dp, np, dw, (int)G->work.size(), G->n, F, G->max_ldf, D, G->ldD,
                                    G->max_rows, gid, ed2st, status, st, &L));
@@ -600,7 +655,7 @@ int run_solve(fap_dgraph *G, int mode) {
       FAP_CK(launch_floyd_matrix<T>(F + d.f_off, d.ldf, (int)ceil_div(d.s, kFloydTile), status, st, &L));
       FAP_CK(launch_bdy_scatter<T>(dp + i, 1, F, D, G->ldD, st2ed, d.b, d.s, st, &L));
       if (G->thin_pos[i] >= 0)
-        FAP_CK(launch_minplus_thin<T>(dp, G->d_thin.as<int32_t>() + G->thin_pos[i], 1, G->n, F, D,
+        FAP_CK(launch_minplus_thin<T>(dp, G->d_thin.as<int32_t>() + G->thin_pos[i], 1, d.s - d.b, G->n, F, D,
                                       G->ldD, gid, ed2st, st, &L));
       else
         FAP_CK(launch_minplus_parts<T>(dp, np, dw + w0, w1 - w0, G->n, F, G->max_ldf, D, G->ldD,
@@ -613,14 +668,18 @@ int run_solve(fap_dgraph *G, int mode) {
   return FAP_OK;
 }
 
-int read_status(fap_dgraph *G) {
-  int h = 0;
-  FAP_CK(cudaMemcpy(&h, G->d_status.p, sizeof(int), cudaMemcpyDeviceToHost));
+int status_code(int h) {
   if (h == kDevSsspRoundLimit)
     return fail(FAP_ERR_NOT_CONVERGED, "SSSP hit its round bound");
   if (h == kDevTmaTimeout) return fail(FAP_ERR_DEVICE, "a TMA tile load did not complete in time");
   if (h != kDevOk) return fail(FAP_ERR_DEVICE, "device-side error %d", h);
   return FAP_OK;
+}
+
+int read_status(fap_dgraph *G) {
+  int h = 0;
+  FAP_CK(cudaMemcpy(&h, G->d_status.p, sizeof(int), cudaMemcpyDeviceToHost));
+  return status_code(h);
 }
 
 }  // namespace
@@ -646,7 +705,7 @@ extern "C" int fap_solve(fap_dgraph *G, const int32_t *parts, int32_t count, int
   if (ids.empty()) return FAP_OK;
   DeviceGuard g(G->ctx->device);
   if (G->max_rows == 0) FAP_TRY(fap_graph_reserve(G, 0));
-  FAP_TRY(prepare_batch(G, ids));
+  FAP_TRY(prepare_batch(G, ids, mode == FAP_MODE_BATCHED && G->cache_ready && G->use_cache));
   int rc = FAP_OK;
   cudaStream_t st = G->ctx->stream;
   if (mode == FAP_MODE_BATCHED && G->use_graph && st != nullptr) {
@@ -776,6 +835,29 @@ extern "C" int fap_graph_block_checksums(fap_dgraph *G, int32_t part, uint64_t *
   FAP_TRY(read_status(G));
   return FAP_OK;
 }
+
+extern "C" int fap_graph_checksums_async(fap_dgraph *G, int32_t part, uint64_t *d_out) {
+  if (!G || !d_out) return fail(FAP_ERR_INVALID, "NULL argument");
+  if (G->dtype != FAP_DTYPE_I32) return fail(FAP_ERR_INVALID, "checksums need the int32 path");
+  void *dp;
+  int64_t rows, ld;
+  FAP_TRY(fap_graph_block(G, part, &dp, &rows, &ld));
+  DeviceGuard g(G->ctx->device);
+  int64_t L = 0;
+  FAP_CK(launch_row_checksums(reinterpret_cast<const int32_t *>(dp), rows, G->n, ld, d_out,
+                              G->ctx->stream, &L));
+  return FAP_OK;
+}
+
+extern "C" int fap_graph_status_async(fap_dgraph *G, int32_t *host_status) {
+  if (!G || !host_status) return fail(FAP_ERR_INVALID, "NULL argument");
+  DeviceGuard g(G->ctx->device);
+  FAP_CK(cudaMemcpyAsync(host_status, G->d_status.p, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                         G->ctx->stream));
+  return FAP_OK;
+}
+
+extern "C" int fap_status_code(int32_t device_status) { return status_code(device_status); }
 
 // ---------------------------------------------------------------------------
 // device-pointer operators
@@ -987,6 +1069,11 @@ extern "C" int fap_graph_set_param(fap_dgraph *G, const char *key, double value)
     G->sssp_chain = value >= 0 ? (int)value : 0;
     return FAP_OK;
   }
+  if (std::strcmp(key, "use_cache") == 0) {
+    G->use_cache = value != 0.0;
+    G->last_ids.clear();
+    return FAP_OK;
+  }
   if (std::strcmp(key, "floyd_per_cta") == 0) {
     G->floyd_per_cta = value != 0.0;
     return FAP_OK;
@@ -1099,7 +1186,9 @@ extern "C" int fap_graph_device_bytes(const fap_dgraph *G, int64_t *bytes) {
   int64_t t = 0;
   for (const DevBuf *b : {&G->ro, &G->col, &G->w, &G->ro_s, &G->col_s, &G->w_s, &G->sssp_scratch,
                           &G->d_thin, &G->d_gid, &G->d_st2ed, &G->d_ed2st, &G->D, &G->F, &G->d_parts,
-                          &G->d_work, &G->d_src, &G->d_srcrows, &G->d_status, &G->d_checks, &G->staging})
+                          &G->d_work, &G->d_src, &G->d_srcrows, &G->d_status, &G->d_checks, &G->staging,
+                          &G->cBd, &G->cF, &G->d_cparts, &G->d_rowgroups, &G->d_rowloc, &G->d_rowout,
+                          &G->d_rowidx})
     t += (int64_t)b->bytes;
   *bytes = t;
   return FAP_OK;
@@ -1108,6 +1197,217 @@ extern "C" int fap_graph_device_bytes(const fap_dgraph *G, int64_t *bytes) {
 extern "C" int fap_graph_resident(fap_dgraph *G, int32_t part) {
   if (!G || part < 1 || part > G->K) return 0;
   return G->row_base[part] >= 0 ? 1 : 0;
+}
+
+// ---------------------------------------------------------------------------
+// Resident cache (stages 1-2 of every part, kept in HBM for serving)
+// ---------------------------------------------------------------------------
+namespace {
+
+struct CacheShape {
+  int32_t ldf = kFloydTile, max_b = 0, max_s = 0;
+  int64_t total_b = 0;
+  int64_t bytes(const fap_dgraph *G) const {
+    // boundary rows + Floyd squares + descriptors + the sources' lists
+    auto a = [](int64_t b) { return (int64_t)alloc_size((size_t)b); };
+    return a(std::max<int64_t>(total_b, 1) * G->ldD * 4) + a((int64_t)G->K * ldf * ldf * 4) +
+           a((int64_t)G->K * (int64_t)sizeof(PartDesc)) + a(std::max<int64_t>(total_b, 1) * 4) +
+           a(std::max<int64_t>(total_b, 1) * 8);
+  }
+};
+
+CacheShape cache_shape(const fap_dgraph *G) {
+  CacheShape c;
+  for (int32_t p = 1; p <= G->K; p++) {
+    c.ldf = std::max<int32_t>(c.ldf, (int32_t)round_up(std::max(G->vnum[p], 1), kFloydTile));
+    c.max_b = std::max(c.max_b, G->bnum[p]);
+    c.max_s = std::max(c.max_s, G->vnum[p]);
+    c.total_b += G->bnum[p];
+  }
+  return c;
+}
+
+template <typename T>
+int cache_build_impl(fap_dgraph *G) {
+  fap_ctx *c = G->ctx;
+  cudaStream_t st = c->stream;
+  const int32_t K = G->K;
+  const CacheShape cs = cache_shape(G);
+  if (cs.total_b > INT32_MAX) return fail(FAP_ERR_RANGE, "too many boundary vertices for the cache");
+  FAP_CK(cudaStreamSynchronize(st));
+  FAP_TRY(G->cBd.ensure((size_t)std::max<int64_t>(cs.total_b, 1) * G->ldD * 4));
+  FAP_TRY(G->cF.ensure((size_t)K * cs.ldf * cs.ldf * 4));
+  G->cb_off.assign(K + 2, 0);
+  for (int32_t p = 1; p <= K; p++) G->cb_off[p + 1] = G->cb_off[p] + G->bnum[p];
+  G->cparts.clear();
+  std::vector<int32_t> src;
+  std::vector<int64_t> srows;
+  for (int32_t p = 1; p <= K; p++) {
+    PartDesc d{};
+    d.part = p;
+    d.start = G->voff[p];
+    d.s = G->vnum[p];
+    d.b = G->bnum[p];
+    d.row_base = G->cb_off[p];
+    d.ldf = cs.ldf;
+    d.f_off = (int64_t)(p - 1) * cs.ldf * cs.ldf;
+    d.bd_row = (int32_t)G->cb_off[p];
+    G->cparts.push_back(d);
+    for (int32_t k = 0; k < d.b; k++) {
+      src.push_back(d.start + k);
+      srows.push_back(d.row_base + k);
+    }
+  }
+  FAP_TRY(G->d_cparts.ensure(G->cparts.size() * sizeof(PartDesc)));
+  FAP_TRY(G->d_src.ensure(std::max<size_t>(src.size(), 1) * 4));
+  FAP_TRY(G->d_srcrows.ensure(std::max<size_t>(srows.size(), 1) * 8));
+  FAP_TRY(G->sssp_scratch.ensure(
+      (size_t)std::max(sssp_scratch_rows(G->n, (int)src.size()), 1) * (size_t)G->n * 4));
+  FAP_CK(cudaMemcpy(G->d_cparts.p, G->cparts.data(), G->cparts.size() * sizeof(PartDesc),
+                    cudaMemcpyHostToDevice));
+  if (!src.empty()) {
+    FAP_CK(cudaMemcpy(G->d_src.p, src.data(), src.size() * 4, cudaMemcpyHostToDevice));
+    FAP_CK(cudaMemcpy(G->d_srcrows.p, srows.data(), srows.size() * 8, cudaMemcpyHostToDevice));
+  }
+  G->last_ids.clear();  // d_src / d_srcrows now hold the cache's sources
+  G->epoch++;
+  const PartDesc *dp = G->d_cparts.as<const PartDesc>();
+  T *Bd = G->cBd.as<T>();
+  T *F = G->cF.as<T>();
+  int *status = G->d_status.as<int>();
+  const int32_t *gid = G->d_gid.as<const int32_t>(), *st2ed = G->d_st2ed.as<const int32_t>(),
+                *ed2st = G->d_ed2st.as<const int32_t>();
+  const int64_t rounds = G->sssp_max_rounds > 0 ? G->sssp_max_rounds : 8 * (int64_t)G->n + 1024;
+  int64_t L = 0;
+  FAP_CK(cudaMemsetAsync(status, 0, sizeof(int), st));
+  FAP_CK(launch_sssp<T>(G->ro_s.as<const int32_t>(), G->col_s.as<const int32_t>(), G->w_s.as<const T>(),
+                        G->n, G->d_src.as<const int32_t>(), G->d_srcrows.as<const int64_t>(),
+                        (int)src.size(), Bd, G->ldD, G->ldD, ed2st, G->sssp_scratch.as<T>(),
+                        sssp_delta_for<T>(G), G->sssp_chain, G->sssp_precheck, rounds, status, st, &L));
+  FAP_CK(launch_gather<T>(dp, K, cs.ldf, G->ro.as<const int32_t>(), G->col.as<const int32_t>(),
+                          G->w.as<const T>(), gid, st2ed, ed2st, Bd, G->ldD, F, st, &L));
+  if (G->floyd_per_cta) {
+    FAP_CK(launch_floyd_parts<T>(dp, K, F, cs.ldf, Bd, G->ldD, st2ed, status, st, &L));
+  } else {
+    FAP_CK(launch_floyd_parts_multi<T>(dp, K, (int)ceil_div(cs.max_s, kFloydTile), F, cs.ldf, status,
+                                       st, &L));
+    FAP_CK(launch_bdy_scatter<T>(dp, K, F, Bd, G->ldD, st2ed, cs.max_b, cs.max_s, st, &L));
+  }
+  G->cache_ldf = cs.ldf;
+  G->cache_max_b = cs.max_b;
+  G->cache_max_s = cs.max_s;
+  G->cache_ready = true;
+  G->launches = L;
+  c->launches += L;
+  // The SSSP scratch (up to one row of n per resident CTA) is not needed by
+  // the cached path: wait for the build and give it back.
+  FAP_CK(cudaStreamSynchronize(st));
+  G->sssp_scratch.release();
+  return FAP_OK;
+}
+
+// Distance rows from the cache: boundary sources copy their cached row;
+// inner sources take the min-plus of their closed Floyd row with the part's
+// boundary rows (the block min-plus restricted to the requested rows).
+template <typename T>
+int rows_cached_impl(fap_dgraph *G, const int32_t *sources, int32_t count, float *d_out) {
+  cudaStream_t st = G->ctx->stream;
+  const int32_t K = G->K;
+  std::vector<int64_t> gather;  // pairs: cache row, output row
+  std::vector<std::vector<std::pair<int32_t, int64_t>>> inner(K + 1);
+  for (int32_t r = 0; r < count; r++) {
+    const int32_t v = sources[r];
+    const int32_t p = G->gid[v];
+    const int32_t i = G->ed2st[v] - G->voff[p];
+    if (i < G->bnum[p]) {
+      gather.push_back(G->cb_off[p] + i);
+      gather.push_back(r);
+    } else {
+      inner[p].push_back({i, (int64_t)r});
+    }
+  }
+  std::vector<RowGroup> groups;
+  std::vector<int32_t> loc;
+  std::vector<int64_t> orow;
+  for (int32_t p = 1; p <= K; p++)
+    for (size_t a = 0; a < inner[p].size(); a += kRowsGroup) {
+      const int32_t cnt = (int32_t)std::min<size_t>(kRowsGroup, inner[p].size() - a);
+      groups.push_back(RowGroup{p - 1, (int32_t)loc.size(), cnt, 0});
+      for (int32_t j = 0; j < cnt; j++) {
+        loc.push_back(inner[p][a + j].first);
+        orow.push_back(inner[p][a + j].second);
+      }
+    }
+  const int64_t ng = (int64_t)gather.size() / 2;
+  std::vector<int64_t> gidx(ng), gout(ng);
+  for (int64_t k = 0; k < ng; k++) {
+    gidx[k] = gather[2 * k];
+    gout[k] = gather[2 * k + 1];
+  }
+  FAP_TRY(G->d_rowgroups.ensure(std::max<size_t>(groups.size(), 1) * sizeof(RowGroup)));
+  FAP_TRY(G->d_rowloc.ensure(std::max<size_t>(loc.size(), 1) * 4));
+  FAP_TRY(G->d_rowout.ensure(std::max<size_t>(orow.size(), 1) * 8));
+  FAP_TRY(G->d_rowidx.ensure(std::max<size_t>(2 * ng, 1) * 8));
+  FAP_CK(cudaStreamSynchronize(st));  // earlier launches may still read these buffers
+  if (!groups.empty()) {
+    FAP_CK(cudaMemcpy(G->d_rowgroups.p, groups.data(), groups.size() * sizeof(RowGroup), cudaMemcpyHostToDevice));
+    FAP_CK(cudaMemcpy(G->d_rowloc.p, loc.data(), loc.size() * 4, cudaMemcpyHostToDevice));
+    FAP_CK(cudaMemcpy(G->d_rowout.p, orow.data(), orow.size() * 8, cudaMemcpyHostToDevice));
+  }
+  if (ng > 0) {
+    FAP_CK(cudaMemcpy(G->d_rowidx.p, gidx.data(), ng * 8, cudaMemcpyHostToDevice));
+    FAP_CK(cudaMemcpy(G->d_rowidx.as<int64_t>() + ng, gout.data(), ng * 8, cudaMemcpyHostToDevice));
+  }
+  const int64_t n = G->n;
+  T *out = reinterpret_cast<T *>(d_out);
+  int64_t L = 0;
+  FAP_CK(launch_row_gather<T>(G->cBd.as<const T>(), G->ldD, G->d_rowidx.as<const int64_t>(), ng, (int)n,
+                              out, n, G->d_rowidx.as<const int64_t>() + ng, st, &L));
+  FAP_CK(launch_minplus_rows<T>(G->d_cparts.as<const PartDesc>(), G->d_rowgroups.as<const RowGroup>(),
+                                (int)groups.size(), G->d_rowloc.as<const int32_t>(),
+                                G->d_rowout.as<const int64_t>(), G->cache_max_b, (int)n,
+                                G->cF.as<const T>(), G->cBd.as<const T>(), G->ldD,
+                                G->d_gid.as<const int32_t>(), G->d_ed2st.as<const int32_t>(), out, n, st, &L));
+  if (Dist<T>::kDtype == FAP_DTYPE_I32)
+    FAP_CK(launch_i32_to_f32(reinterpret_cast<int32_t *>(d_out), count, n, n, d_out, st, &L));
+  G->ctx->launches += L;
+  G->launches = L;
+  return FAP_OK;
+}
+}  // namespace
+
+extern "C" int fap_graph_cache_build(fap_dgraph *G) {
+  if (!G) return fail(FAP_ERR_INVALID, "NULL graph");
+  if (G->K == 0) return fail(FAP_ERR_STATE, "fap_graph_cache_build before fap_graph_set_parts");
+  if (G->cache_ready) return FAP_OK;
+  DeviceGuard g(G->ctx->device);
+  const int rc = G->dtype == FAP_DTYPE_I32 ? cache_build_impl<int32_t>(G) : cache_build_impl<float>(G);
+  if (rc != FAP_OK) cache_drop(G);
+  return rc;
+}
+
+extern "C" int fap_graph_cache_release(fap_dgraph *G) {
+  if (!G) return fail(FAP_ERR_INVALID, "NULL graph");
+  DeviceGuard g(G->ctx->device);
+  FAP_CK(cudaStreamSynchronize(G->ctx->stream));
+  cache_drop(G);
+  return FAP_OK;
+}
+
+extern "C" int fap_graph_cache_bytes(const fap_dgraph *G, int64_t *bytes, int *built) {
+  if (!G || !bytes) return fail(FAP_ERR_INVALID, "NULL argument");
+  if (G->K == 0) return fail(FAP_ERR_STATE, "no partition");
+  if (built) *built = G->cache_ready ? 1 : 0;
+  if (G->cache_ready) {
+    *bytes = (int64_t)(G->cBd.bytes + G->cF.bytes + G->d_cparts.bytes);
+  } else {
+    // plus the SSSP scratch the build needs while it runs
+    const CacheShape cs = cache_shape(G);
+    *bytes = cs.bytes(G) + (int64_t)alloc_size(
+                               (size_t)std::max(sssp_scratch_rows(G->n, (int)std::min<int64_t>(cs.total_b, INT32_MAX)), 1) *
+                               (size_t)G->n * 4);
+  }
+  return FAP_OK;
 }
 
 namespace {
@@ -1156,6 +1456,9 @@ extern "C" int fap_graph_rows_async(fap_dgraph *G, const int32_t *sources, int32
   for (int32_t i = 0; i < count; i++)
     if (sources[i] < 0 || sources[i] >= G->n) return fail(FAP_ERR_INVALID, "source %d out of range", sources[i]);
   DeviceGuard g(G->ctx->device);
+  if (G->cache_ready && G->use_cache)
+    return G->dtype == FAP_DTYPE_I32 ? rows_cached_impl<int32_t>(G, sources, count, d_out)
+                                     : rows_cached_impl<float>(G, sources, count, d_out);
   return G->dtype == FAP_DTYPE_I32 ? rows_async_impl<int32_t>(G, sources, count, d_out)
                                    : rows_async_impl<float>(G, sources, count, d_out);
 }

@@ -459,7 +459,10 @@ __global__ void __launch_bounds__(MPCfg<T>::THREADS, 2)
   // A = F rows b+m0.. of part wk.pidx (columns 0..b-1); B = D rows
   // row_base..row_base+b-1 (the part's boundary rows).  Rows and columns past
   // the part's extent are never stored; k past b is never read.
-  if (!tma_minplus_tile<T, TC>(&mapF, 0, pd.b + wk.m0, wk.pidx, &mapD, n0, (int)pd.row_base, 0, K, acc,
+  // The part's square in the arena (its index there: a batch index, or the
+  // part's slot in the resident cache).
+  const int fz = (int)(pd.f_off / ((int64_t)pd.ldf * pd.ldf));
+  if (!tma_minplus_tile<T, TC>(&mapF, 0, pd.b + wk.m0, fz, &mapD, n0, (int)pd.row_base, 0, K, acc,
                                sm)) {
     if (threadIdx.x == 0) set_status(status, kDevTmaTimeout);
     return;
@@ -534,7 +537,7 @@ struct ThinShared {
 // c0 + {0..3} (g = 0) and c0 + kThinHalf + {0..3} (g = 1); B relaxations per
 // output.  G = 1 handles only group g0.
 template <typename T, int B, int G>
-__device__ __forceinline__ void thin_rows(ThinShared<T> &sh, const PartDesc &pd, int M, int64_t c0,
+__device__ __forceinline__ void thin_rows(ThinShared<T> &sh, const PartDesc &pd, int mb, int me, int64_t c0,
                                           const T *__restrict__ F, T *D, int64_t ldD, const int (&own)[8], bool any_own,
                                           int g0, const bool (&live)[2]) {
   using V = typename Vec4<T>::type;
@@ -551,8 +554,8 @@ __device__ __forceinline__ void thin_rows(ThinShared<T> &sh, const PartDesc &pd,
       sv[k][4 * g + 0] = v.x; sv[k][4 * g + 1] = v.y; sv[k][4 * g + 2] = v.z; sv[k][4 * g + 3] = v.w;
     }
   const T *Fp = F + pd.f_off;
-  for (int m0 = 0; m0 < M; m0 += kMinplusBM) {
-    const int rows = min(kMinplusBM, M - m0);
+  for (int m0 = mb; m0 < me; m0 += kMinplusBM) {
+    const int rows = min(kMinplusBM, me - m0);
     const T *Fr = Fp + (int64_t)(pd.b + m0) * pd.ldf;
     // stage this block's A values and own-part values
     __syncthreads();
@@ -608,30 +611,35 @@ __device__ __forceinline__ void thin_rows(ThinShared<T> &sh, const PartDesc &pd,
 }
 
 template <typename T, int B>
-__device__ __forceinline__ void thin_dispatch(ThinShared<T> &sh, const PartDesc &pd, int M,
+__device__ __forceinline__ void thin_dispatch(ThinShared<T> &sh, const PartDesc &pd, int mb, int me,
                                               int64_t c0, const T *F, T *D, int64_t ldD,
                                               const int (&own)[8], bool any_own,
                                               const bool (&live)[2]) {
   if (B <= 6) {
-    thin_rows<T, B, 2>(sh, pd, M, c0, F, D, ldD, own, any_own, 0, live);
+    thin_rows<T, B, 2>(sh, pd, mb, me, c0, F, D, ldD, own, any_own, 0, live);
   } else {
     // the two column groups in two passes keep the boundary strip in registers
-    thin_rows<T, B, 1>(sh, pd, M, c0, F, D, ldD, own, any_own, 0, live);
-    thin_rows<T, B, 1>(sh, pd, M, c0, F, D, ldD, own, any_own, 1, live);
+    thin_rows<T, B, 1>(sh, pd, mb, me, c0, F, D, ldD, own, any_own, 0, live);
+    thin_rows<T, B, 1>(sh, pd, mb, me, c0, F, D, ldD, own, any_own, 1, live);
   }
 }
 
-// grid (ceil(ldD / kThinCols), number of thin parts); blockIdx.y indexes
-// thin_parts (batch indices).
+// grid (ceil(ldD / kThinCols), number of thin parts, row chunks);
+// blockIdx.y indexes thin_parts (batch indices), blockIdx.z the chunk of
+// row_chunk inner rows (a multiple of kMinplusBM) the CTA walks, so that a
+// batch of few parts still spreads over every SM.
 template <typename T>
 __global__ void __launch_bounds__(kThinThreads, 2)
     minplus_thin_kernel(const PartDesc *__restrict__ parts, const int32_t *__restrict__ thin_parts,
                         int n, const T *__restrict__ F, T *D, int64_t ldD,
-                        const int32_t *__restrict__ graph_id, const int32_t *__restrict__ ed2st) {
+                        const int32_t *__restrict__ graph_id, const int32_t *__restrict__ ed2st,
+                        int row_chunk) {
   __shared__ ThinShared<T> sh;
   const PartDesc pd = parts[thin_parts[blockIdx.y]];
   const int M = pd.s - pd.b;
-  if (M <= 0) return;
+  const int mb = blockIdx.z * row_chunk;
+  const int me = min(M, mb + row_chunk);
+  if (mb >= me) return;
   if (threadIdx.x == 0) sh.nown = 0;
   const int64_t c0 = (int64_t)blockIdx.x * kThinCols + 4 * threadIdx.x;
   const bool live[2] = {c0 < ldD, c0 + kThinHalf < ldD};  // ldD is a multiple of 4
@@ -656,7 +664,7 @@ __global__ void __launch_bounds__(kThinThreads, 2)
   }
   switch (pd.b) {
 #define FAPB_THIN_CASE(NB) \
-  case NB: thin_dispatch<T, NB>(sh, pd, M, c0, F, D, ldD, own, any_own, live); break;
+  case NB: thin_dispatch<T, NB>(sh, pd, mb, me, c0, F, D, ldD, own, any_own, live); break;
     FAPB_THIN_CASE(0) FAPB_THIN_CASE(1) FAPB_THIN_CASE(2) FAPB_THIN_CASE(3) FAPB_THIN_CASE(4)
     FAPB_THIN_CASE(5) FAPB_THIN_CASE(6) FAPB_THIN_CASE(7) FAPB_THIN_CASE(8) FAPB_THIN_CASE(9)
     FAPB_THIN_CASE(10) FAPB_THIN_CASE(11) FAPB_THIN_CASE(12) FAPB_THIN_CASE(13)
@@ -690,13 +698,173 @@ cudaError_t launch_minplus_parts(const PartDesc *parts, int nparts, const MPWork
 }
 
 template <typename T>
-cudaError_t launch_minplus_thin(const PartDesc *parts, const int32_t *thin_parts, int nthin, int n,
-                                const T *F, T *D, int64_t ldD, const int32_t *graph_id,
+cudaError_t launch_minplus_thin(const PartDesc *parts, const int32_t *thin_parts, int nthin, int max_m,
+                                int n, const T *F, T *D, int64_t ldD, const int32_t *graph_id,
                                 const int32_t *ed2st, cudaStream_t stream, int64_t *launches) {
-  if (nthin <= 0) return cudaSuccess;
-  dim3 grid((unsigned)ceil_div(ldD, kThinCols), (unsigned)nthin);
+  if (nthin <= 0 || max_m <= 0) return cudaSuccess;
+  // Enough CTAs for about four per SM: split the parts' inner rows into
+  // chunks of whole kMinplusBM blocks when the column strips alone are few.
+  const int64_t col_ctas = ceil_div(ldD, kThinCols) * (int64_t)nthin;
+  const int64_t blocks = ceil_div(max_m, kMinplusBM);
+  const int64_t want = 4 * 148;
+  const int64_t zc = std::min<int64_t>(blocks, std::max<int64_t>(1, ceil_div(want, col_ctas)));
+  const int row_chunk = (int)(ceil_div(blocks, zc) * kMinplusBM);
+  const unsigned gz = (unsigned)ceil_div(max_m, row_chunk);
+  dim3 grid((unsigned)ceil_div(ldD, kThinCols), (unsigned)nthin, gz);
   minplus_thin_kernel<T><<<grid, kThinThreads, 0, stream>>>(parts, thin_parts, n, F, D, ldD,
-                                                            graph_id, ed2st);
+                                                            graph_id, ed2st, row_chunk);
+  *launches += 1;
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Resident cache kernels
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void bdy_copy_kernel(const PartDesc *__restrict__ parts, const T *__restrict__ Bd, T *D,
+                                int64_t ldD) {
+  const PartDesc pd = parts[blockIdx.y];
+  const int i = blockIdx.x;
+  if (i >= pd.b) return;
+  using V = typename Vec4<T>::type;  // ldD is a multiple of 128: rows are 16-byte aligned
+  const V *src = reinterpret_cast<const V *>(Bd + ((int64_t)pd.bd_row + i) * ldD);
+  V *dst = reinterpret_cast<V *>(D + (pd.row_base + i) * ldD);
+  for (int64_t j = threadIdx.x; j < ldD / 4; j += blockDim.x) dst[j] = __ldg(src + j);
+}
+
+template <typename T>
+cudaError_t launch_bdy_copy(const PartDesc *parts, int nparts, int max_b, const T *Bd, T *D,
+                            int64_t ldD, cudaStream_t stream, int64_t *launches) {
+  if (nparts <= 0 || max_b <= 0) return cudaSuccess;
+  bdy_copy_kernel<T><<<dim3(max_b, nparts), 256, 0, stream>>>(parts, Bd, D, ldD);
+  *launches += 1;
+  return cudaGetLastError();
+}
+
+template <typename T>
+__global__ void row_gather_kernel(const T *__restrict__ src, int64_t ld_src,
+                                  const int64_t *__restrict__ idx, int n, T *__restrict__ out,
+                                  int64_t ld_out, const int64_t *__restrict__ out_rows) {
+  const int64_t r = blockIdx.y;
+  const T *s = src + idx[r] * ld_src;
+  T *o = out + out_rows[r] * ld_out;
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n;
+       j += (int64_t)gridDim.x * blockDim.x)
+    o[j] = __ldg(s + j);
+}
+
+template <typename T>
+cudaError_t launch_row_gather(const T *src, int64_t ld_src, const int64_t *idx, int64_t rows, int n,
+                              T *out, int64_t ld_out, const int64_t *out_rows, cudaStream_t stream,
+                              int64_t *launches) {
+  if (rows <= 0 || n <= 0) return cudaSuccess;
+  const int bx = (int)std::min<int64_t>(ceil_div(n, 256), 16);
+  row_gather_kernel<T><<<dim3(bx, (unsigned)rows), 256, 0, stream>>>(src, ld_src, idx, n, out, ld_out,
+                                                                     out_rows);
+  *launches += 1;
+  return cudaGetLastError();
+}
+
+// grid (ngroups, column chunks of kRowsCols): consecutive CTAs take the
+// groups of one column chunk, so a part's boundary-row chunk is read from
+// DRAM once and from L2 by its other groups.  Each thread owns 4 columns
+// (stride 256: coalesced loads of the boundary rows), each group up to
+// kRowsGroup rows; the A values are staged in shared memory in chunks of
+// kRowsKC boundary columns.
+constexpr int kRowsThreads = 256;
+constexpr int kRowsCols = 4 * kRowsThreads;
+constexpr int kRowsKC = 256;
+
+// Body for groups of at most RG rows (RG a compile-time bound, so that the
+// accumulators of absent rows cost nothing).
+template <typename T, int RG>
+__device__ __forceinline__ void minplus_rows_body(const RowGroup &g, const PartDesc &pd,
+                                                  const int64_t *__restrict__ out_row, int n,
+                                                  const T *__restrict__ F, const T *__restrict__ Bd,
+                                                  int64_t ldD, const int32_t *__restrict__ graph_id,
+                                                  const int32_t *__restrict__ ed2st, T *__restrict__ out,
+                                                  int64_t ld_out, T (&As)[kRowsGroup][kRowsKC],
+                                                  const int32_t *rloc) {
+  const int c0 = blockIdx.y * kRowsCols + threadIdx.x;
+  const T inf = Dist<T>::inf();
+  T acc[RG][4];
+#pragma unroll
+  for (int r = 0; r < RG; r++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) acc[r][q] = inf;
+  const T *Fp = F + pd.f_off;
+  const T *Bp = Bd + (int64_t)pd.bd_row * ldD;
+  for (int k0 = 0; k0 < pd.b; k0 += kRowsKC) {
+    const int kc = min(kRowsKC, pd.b - k0);
+    __syncthreads();
+    for (int t = threadIdx.x; t < RG * kRowsKC; t += blockDim.x) {
+      const int r = t / kRowsKC, k = t % kRowsKC;
+      As[r][k] = (r < g.count && k < kc) ? __ldg(Fp + (int64_t)rloc[r] * pd.ldf + k0 + k) : inf;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int k = 0; k < kc; k++) {
+      const T *Bk = Bp + (int64_t)(k0 + k) * ldD;
+      T v[4];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int c = c0 + q * kRowsThreads;
+        v[q] = c < n ? __ldg(Bk + c) : inf;
+      }
+#pragma unroll
+      for (int r = 0; r < RG; r++) {
+        const T a = As[r][k];
+#pragma unroll
+        for (int q = 0; q < 4; q++) acc[r][q] = Dist<T>::relax(a, v[q], acc[r][q]);
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int c = c0 + q * kRowsThreads;
+    if (c >= n) continue;
+    const int o = (__ldg(graph_id + c) == pd.part) ? __ldg(ed2st + c) - pd.start : -1;
+#pragma unroll
+    for (int r = 0; r < RG; r++) {
+      if (r >= g.count) break;
+      const T val = o >= 0 ? __ldg(Fp + (int64_t)rloc[r] * pd.ldf + o) : acc[r][q];
+      out[out_row[g.first + r] * ld_out + c] = val;
+    }
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kRowsThreads, 2)
+    minplus_rows_kernel(const PartDesc *__restrict__ parts, const RowGroup *__restrict__ groups,
+                        const int32_t *__restrict__ loc, const int64_t *__restrict__ out_row, int n,
+                        const T *__restrict__ F, const T *__restrict__ Bd, int64_t ldD,
+                        const int32_t *__restrict__ graph_id, const int32_t *__restrict__ ed2st,
+                        T *__restrict__ out, int64_t ld_out) {
+  __shared__ T As[kRowsGroup][kRowsKC];
+  __shared__ int32_t rloc[kRowsGroup];
+  const RowGroup g = groups[blockIdx.x];
+  const PartDesc pd = parts[g.pidx];
+  if (threadIdx.x < kRowsGroup) rloc[threadIdx.x] = threadIdx.x < g.count ? loc[g.first + threadIdx.x] : 0;
+  __syncthreads();
+  if (g.count <= 1)
+    minplus_rows_body<T, 1>(g, pd, out_row, n, F, Bd, ldD, graph_id, ed2st, out, ld_out, As, rloc);
+  else if (g.count <= 4)
+    minplus_rows_body<T, 4>(g, pd, out_row, n, F, Bd, ldD, graph_id, ed2st, out, ld_out, As, rloc);
+  else
+    minplus_rows_body<T, kRowsGroup>(g, pd, out_row, n, F, Bd, ldD, graph_id, ed2st, out, ld_out, As, rloc);
+}
+
+template <typename T>
+cudaError_t launch_minplus_rows(const PartDesc *parts, const RowGroup *groups, int ngroups,
+                                const int32_t *loc, const int64_t *out_row, int max_b, int n,
+                                const T *F, const T *Bd, int64_t ldD, const int32_t *graph_id,
+                                const int32_t *ed2st, T *out, int64_t ld_out, cudaStream_t stream,
+                                int64_t *launches) {
+  (void)max_b;
+  if (ngroups <= 0 || n <= 0) return cudaSuccess;
+  dim3 grid((unsigned)ngroups, (unsigned)ceil_div(n, kRowsCols));
+  minplus_rows_kernel<T><<<grid, kRowsThreads, 0, stream>>>(parts, groups, loc, out_row, n, F, Bd,
+                                                            ldD, graph_id, ed2st, out, ld_out);
   *launches += 1;
   return cudaGetLastError();
 }
@@ -874,12 +1042,21 @@ cudaError_t launch_relax_peak(T *sink, int blocks, int iters, cudaStream_t strea
                                                const T *, int64_t, T *, int64_t, int64_t,         \
                                                const int32_t *, const int32_t *, int *,           \
                                                cudaStream_t, int64_t *);                          \
-  template cudaError_t launch_minplus_thin<T>(const PartDesc *, const int32_t *, int, int,        \
+  template cudaError_t launch_minplus_thin<T>(const PartDesc *, const int32_t *, int, int, int,   \
                                               const T *, T *, int64_t, const int32_t *,           \
                                               const int32_t *, cudaStream_t, int64_t *);          \
   template cudaError_t launch_minplus_generic<T>(int, int, int, const T *, int64_t, const T *,    \
                                                  int64_t, T *, int64_t, cudaStream_t, int64_t *); \
   template cudaError_t launch_fill<T>(T *, int64_t, int64_t, int64_t, T, cudaStream_t, int64_t *); \
+  template cudaError_t launch_bdy_copy<T>(const PartDesc *, int, int, const T *, T *, int64_t,    \
+                                          cudaStream_t, int64_t *);                               \
+  template cudaError_t launch_row_gather<T>(const T *, int64_t, const int64_t *, int64_t, int, T *, \
+                                            int64_t, const int64_t *, cudaStream_t, int64_t *);   \
+  template cudaError_t launch_minplus_rows<T>(const PartDesc *, const RowGroup *, int,            \
+                                              const int32_t *, const int64_t *, int, int,         \
+                                              const T *, const T *, int64_t, const int32_t *,     \
+                                              const int32_t *, T *, int64_t, cudaStream_t,        \
+                                              int64_t *);                                         \
   template cudaError_t launch_relax_peak<T>(T *, int, int, cudaStream_t, double *);
 
 FAPB_INSTANTIATE(int32_t)

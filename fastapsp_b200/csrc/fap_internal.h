@@ -16,6 +16,15 @@ struct PartDesc {
   int64_t row_base;  // first output row of the part's block
   int64_t f_off;     // offset of the part's padded Floyd matrix in the F arena
   int32_t ldf;       // padded Floyd leading dimension (multiple of kFloydTile)
+  int32_t bd_row;    // first row of the part's boundary rows in the resident cache
+};
+
+// Rows-from-cache work: up to kRowsGroup output rows of one part.
+constexpr int kRowsGroup = 16;
+struct RowGroup {
+  int32_t pidx;   // index into the cache's part descriptors
+  int32_t first;  // first entry of the group in the row lists
+  int32_t count;  // rows in the group (<= kRowsGroup)
   int32_t pad_;
 };
 
@@ -92,12 +101,37 @@ cudaError_t launch_minplus_parts(const PartDesc *parts, int nparts, const MPWork
                                  cudaStream_t stream, int64_t *launches);
 
 // Same for parts with at most kThinBoundary boundary vertices (store-bound
-// shape): thin_parts[0..nthin) are batch indices of such parts.
+// shape): thin_parts[0..nthin) are batch indices of such parts, max_m bounds
+// their inner row counts.
 constexpr int kThinBoundary = 16;
 template <typename T>
-cudaError_t launch_minplus_thin(const PartDesc *parts, const int32_t *thin_parts, int nthin, int n,
-                                const T *F, T *D, int64_t ldD, const int32_t *graph_id,
+cudaError_t launch_minplus_thin(const PartDesc *parts, const int32_t *thin_parts, int nthin, int max_m,
+                                int n, const T *F, T *D, int64_t ldD, const int32_t *graph_id,
                                 const int32_t *ed2st, cudaStream_t stream, int64_t *launches);
+
+// Resident cache: copy each listed part's boundary rows Bd[bd_row + i] into
+// D[row_base + i] (all ldD columns).
+template <typename T>
+cudaError_t launch_bdy_copy(const PartDesc *parts, int nparts, int max_b, const T *Bd, T *D,
+                            int64_t ldD, cudaStream_t stream, int64_t *launches);
+
+// out[r][0..n) = src[idx[r]][0..n) for r < rows.
+template <typename T>
+cudaError_t launch_row_gather(const T *src, int64_t ld_src, const int64_t *idx, int64_t rows, int n,
+                              T *out, int64_t ld_out, const int64_t *out_rows, cudaStream_t stream,
+                              int64_t *launches);
+
+// Distance rows of inner vertices from the resident cache: for entry e of
+// group g (part parts[g.pidx], local row loc[e] >= b),
+//   out[out_row[e]][j] = F[loc][local(j)]                     j in the part,
+//                      = min(INF, min_k F[loc][k] + Bd[bd_row + k][j])   else,
+// the same terms as the block min-plus and its decode.
+template <typename T>
+cudaError_t launch_minplus_rows(const PartDesc *parts, const RowGroup *groups, int ngroups,
+                                const int32_t *loc, const int64_t *out_row, int max_b, int n,
+                                const T *F, const T *Bd, int64_t ldD, const int32_t *graph_id,
+                                const int32_t *ed2st, T *out, int64_t ld_out, cudaStream_t stream,
+                                int64_t *launches);
 
 // Generic C = min(INF, A (x) B).
 template <typename T>

@@ -41,8 +41,25 @@ struct Req {
   int status = FAP_OK;
   int64_t rows = 0;
   int64_t entries = 0;
-  int64_t row_off = 0;  // FAP_REQ_ROWS: first row in the graph's rows buffer
+  int64_t row_off = 0;  // first row of the request in the batch's checksums / rows buffer
 };
+
+// Grows a pinned host buffer (rare: only when a batch is larger than every
+// earlier one).
+template <typename T>
+bool grow_host(T **p, int64_t *cap, int64_t want) {
+  if (want <= *cap) return true;
+  if (*p) cudaFreeHost(*p);
+  *p = nullptr;
+  *cap = 0;
+  if (cudaHostAlloc(reinterpret_cast<void **>(p), (size_t)want * sizeof(T), cudaHostAllocDefault) != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return false;
+  }
+  *cap = want;
+  return true;
+}
 
 struct GSlot {
   fap_ctx *ctx = nullptr;
@@ -52,13 +69,25 @@ struct GSlot {
   int64_t ldD = 0;
   int64_t base_bytes = 0;  // CSR + partition, always resident
   std::vector<int32_t> vnum, voff, bnum;
+  int64_t max_part = 0;        // largest part (rows)
   int64_t reserved_rows = 0;   // output rows the graph's D holds (0: released)
-  float *rows_buf = nullptr;  // FAP_REQ_ROWS results, grown on demand
-  int64_t rows_cap = 0;
-  uint64_t *cs_buf = nullptr;  // FAP_REQ_ROWS checksums (one per row of rows_buf)
+  // the batch in flight: distance rows, checksums on the device and their
+  // pinned host copy, status word (buffers grow with the largest batch)
+  // distance rows of the batch in flight: a small batch uses the graph's own
+  // buffer (rows_small, at most kSmallRowsBytes), a larger one a block of the
+  // server's pool freed after it (rows_pooled)
+  float *rows_out = nullptr;
+  bool rows_pooled = false;
+  float *rows_small = nullptr;
+  int64_t rows_small_cap = 0;
+  uint64_t *cs_dev = nullptr;
   int64_t cs_cap = 0;
+  uint64_t *cs_host = nullptr;
+  int64_t cs_host_cap = 0;
+  int32_t *status_host = nullptr;
+  int64_t status_host_cap = 0;
   cudaStream_t stream = nullptr;
-  cudaEvent_t done = nullptr;
+  cudaEvent_t start = nullptr, done = nullptr;  // around the batch in flight
   bool busy = false;
   int batch_kind = FAP_REQ_SUBGRAPH;
   std::vector<Req *> inflight;
@@ -69,11 +98,18 @@ struct GSlot {
 }  // namespace
 
 constexpr int kMaxGraphs = 256;
+constexpr int64_t kSmallRowsBytes = int64_t(32) << 20;
 
 struct fap_server {
   int device = 0;
-  int64_t budget = 0;
-  int64_t max_batch_rows = 0;
+  // limits (fap_server_set_option may change them while the worker runs)
+  std::atomic<int64_t> budget{0};
+  std::atomic<int64_t> max_batch_rows{0};
+  std::atomic<int64_t> max_batch_bytes{int64_t(512) << 20};
+  // Stream-ordered pool shared by all graphs for the distance-row buffers of
+  // the batches in flight: freed after each batch without synchronising the
+  // device; up to a quarter of the budget stays mapped for reuse.
+  cudaMemPool_t pool = nullptr;
   // Slots [0, ngraphs) are complete; fap_server_add_graph fills the next slot
   // before publishing it, so the worker never sees a slot being built.
   std::unique_ptr<GSlot> graphs[kMaxGraphs];
@@ -89,7 +125,8 @@ struct fap_server {
   std::thread worker;
   // stats (guarded by mu)
   std::vector<double> lat_ms;
-  int64_t entries = 0, batches = 0, resident_hits = 0, peak_bytes = 0;
+  int64_t entries = 0, batches = 0, resident_hits = 0, peak_bytes = 0, cache_builds = 0, failed = 0;
+  double busy_ms = 0;  // device time of finished batches
 
   void loop();
   bool complete(GSlot &g);
@@ -107,36 +144,75 @@ int serr(int code, const char *msg) {
 }
 }  // namespace
 
+// Device bytes held: every graph's buffers and the server's per-graph
+// batch buffers.
 int64_t fap_server::held_bytes() {
   int64_t t = 0;
   const int ng = ngraphs.load(std::memory_order_acquire);
   for (int i = 0; i < ng; i++) {
     int64_t b = 0;
     if (fap_graph_device_bytes(graphs[i]->dg, &b) == FAP_OK) t += b;
-    t += graphs[i]->rows_cap * 4 + graphs[i]->cs_cap * 8;
+    t += graphs[i]->cs_cap * 8 + graphs[i]->rows_small_cap * 4;
   }
+  uint64_t pooled = 0;
+  if (pool && cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &pooled) == cudaSuccess)
+    t += (int64_t)pooled;
   return t;
 }
 
 namespace {
-void release_rows(GSlot &g) {
-  if (g.rows_buf) cudaFree(g.rows_buf);
-  if (g.cs_buf) cudaFree(g.cs_buf);
-  g.rows_buf = nullptr;
-  g.cs_buf = nullptr;
-  g.rows_cap = 0;
+bool cache_built(const GSlot &g) {
+  int64_t b = 0;
+  int built = 0;
+  return fap_graph_cache_bytes(g.dg, &b, &built) == FAP_OK && built;
+}
+
+// Bytes of g beyond its CSR, partition and resident cache.
+int64_t output_bytes(const GSlot &g) {
+  int64_t all = 0, cache = 0;
+  int built = 0;
+  fap_graph_device_bytes(g.dg, &all);
+  if (fap_graph_cache_bytes(g.dg, &cache, &built) != FAP_OK || !built) cache = 0;
+  return all - g.base_bytes - cache + g.cs_cap * 8 + g.rows_small_cap * 4;
+}
+
+void release_outputs(GSlot &g) {
+  fap_graph_release(g.dg);
+  g.reserved_rows = 0;
+  if (g.cs_dev) cudaFree(g.cs_dev);
+  g.cs_dev = nullptr;
   g.cs_cap = 0;
+  if (g.rows_small) cudaFree(g.rows_small);
+  g.rows_small = nullptr;
+  g.rows_small_cap = 0;
+}
+
+// Grows a device buffer of the graph (frees the old one first: the graph
+// is idle when its next batch is assembled).
+template <typename T>
+bool grow_dev(T **p, int64_t *cap, int64_t want) {
+  if (want <= *cap) return true;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  *cap = 0;
+  if (cudaMalloc(reinterpret_cast<void **>(p), (size_t)want * sizeof(T)) != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return false;
+  }
+  *cap = want;
+  return true;
 }
 }  // namespace
 
-// Releases idle graphs' output/scratch buffers (least recently used first,
-// graph `self` last) until `need` more bytes fit in the budget.  Returns
-// whether they fit; *hopeless is set when they cannot fit even after every
-// busy graph finishes (nothing else holds memory that could be freed).
+// Frees memory until `need` more bytes fit in the budget: first the output
+// buffers of idle graphs (least recently used first), then their resident
+// caches, then graph `self`'s own output buffers.  Returns whether they fit;
+// *hopeless is set when they cannot fit even after every busy graph
+// finishes (nothing else holds memory that could be freed).
 bool fap_server::make_room(int64_t need, int self, bool *hopeless) {
   *hopeless = false;
-  int64_t held = held_bytes();
-  if (held + need <= budget) return true;
+  if (held_bytes() + need <= budget) return true;
   std::vector<int> idle;
   bool others_busy = false;
   const int ng = ngraphs.load(std::memory_order_acquire);
@@ -147,17 +223,23 @@ bool fap_server::make_room(int64_t need, int self, bool *hopeless) {
   }
   std::sort(idle.begin(), idle.end(),
             [&](int a, int b) { return graphs[a]->last_used < graphs[b]->last_used; });
-  idle.push_back(self);
-  for (int i : idle) {
-    int64_t b = 0;
-    fap_graph_device_bytes(graphs[i]->dg, &b);
-    if (b > graphs[i]->base_bytes || graphs[i]->rows_cap > 0) {
-      fap_graph_release(graphs[i]->dg);
-      graphs[i]->reserved_rows = 0;
-      release_rows(*graphs[i]);
-      held = held_bytes();
-      if (held + need <= budget) return true;
+  if (pool) {  // pooled memory of finished batches first
+    cudaMemPoolTrimTo(pool, 0);
+    if (held_bytes() + need <= budget) return true;
+  }
+  for (int i : idle)
+    if (output_bytes(*graphs[i]) > 0) {
+      release_outputs(*graphs[i]);
+      if (held_bytes() + need <= budget) return true;
     }
+  for (int i : idle)
+    if (cache_built(*graphs[i])) {
+      fap_graph_cache_release(graphs[i]->dg);
+      if (held_bytes() + need <= budget) return true;
+    }
+  if (output_bytes(*graphs[self]) > 0) {
+    release_outputs(*graphs[self]);
+    if (held_bytes() + need <= budget) return true;
   }
   *hopeless = !others_busy;
   return false;
@@ -172,38 +254,46 @@ void fap_server::finish(Req *r, int state, int status) {
   if (state == FAP_REQ_DONE) {
     lat_ms.push_back((r->t_done - r->t_submit) * 1e3);
     entries += r->entries;
+  } else {
+    failed++;
   }
   cv_done.notify_all();
 }
 
-// Copies the results of g's finished batch and retires its requests.
+// Retires g's finished batch: its status word and checksums are already in
+// pinned host memory; distances asked for on the host are copied now.
 bool fap_server::complete(GSlot &g) {
-  const int rc = fap_graph_check(g.dg);
+  int rc = fap_status_code(*g.status_host);
+  if (cudaEventQuery(g.done) != cudaSuccess) {
+    cudaGetLastError();
+    rc = FAP_ERR_CUDA;
+  }
+  float ms = 0.0f;
+  if (cudaEventElapsedTime(&ms, g.start, g.done) == cudaSuccess) {
+    std::lock_guard<std::mutex> lk(mu);
+    busy_ms += ms;
+  } else {
+    cudaGetLastError();
+  }
+  const bool cs_ok = g.dtype == FAP_DTYPE_I32;
   for (Req *r : g.inflight) {
     int st = rc;
-    if (st == FAP_OK) {
+    if (st == FAP_OK && r->cs_out && cs_ok)
+      std::memcpy(r->cs_out, g.cs_host + r->row_off, (size_t)r->rows * 8);
+    if (st == FAP_OK && r->host_out) {
       if (r->kind == FAP_REQ_SUBGRAPH) {
-        const int32_t p = r->ids[0];
-        if (r->host_out) st = fap_graph_copy_block(g.dg, p, r->host_out, FAP_DTYPE_F32);
-        if (st == FAP_OK && r->cs_out && g.dtype == FAP_DTYPE_I32)
-          st = fap_graph_block_checksums(g.dg, p, r->cs_out);
-      } else {
-        cudaError_t e = cudaSuccess;
-        if (r->host_out)
-          e = cudaMemcpyAsync(r->host_out, g.rows_buf + r->row_off * g.n, (size_t)r->rows * g.n * 4,
-                              cudaMemcpyDeviceToHost, g.stream);
-        if (e == cudaSuccess && r->cs_out && g.dtype == FAP_DTYPE_I32)
-          e = cudaMemcpyAsync(r->cs_out, g.cs_buf + r->row_off, (size_t)r->rows * 8,
-                              cudaMemcpyDeviceToHost, g.stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(g.stream);
-        if (e != cudaSuccess) {
-          cudaGetLastError();
-          st = FAP_ERR_CUDA;
-        }
+        st = fap_graph_copy_block(g.dg, r->ids[0], r->host_out, FAP_DTYPE_F32);
+      } else if (cudaMemcpyAsync(r->host_out, g.rows_out + r->row_off * g.n, (size_t)r->rows * g.n * 4,
+                                 cudaMemcpyDeviceToHost, g.stream) != cudaSuccess ||
+                 cudaStreamSynchronize(g.stream) != cudaSuccess) {
+        cudaGetLastError();
+        st = FAP_ERR_CUDA;
       }
     }
     finish(r, st == FAP_OK ? FAP_REQ_DONE : FAP_REQ_FAILED, st);
   }
+  if (g.rows_out && g.rows_pooled) cudaFreeAsync(g.rows_out, g.stream);
+  g.rows_out = nullptr;
   g.inflight.clear();
   g.busy = false;
   g.last_used = now_s();
@@ -215,7 +305,8 @@ bool fap_server::complete(GSlot &g) {
 bool fap_server::launch(int gi) {
   GSlot &g = *graphs[gi];
   bool progressed = false;
-  // Sub-graph requests whose block is still resident: answer at once.
+  // Sub-graph requests whose block is still resident: answer at once (the
+  // graph's stream is idle, so the copies do not wait on other work).
   while (!g.pending.empty()) {
     Req *r = g.pending.front();
     if (r->kind != FAP_REQ_SUBGRAPH || !fap_graph_resident(g.dg, r->ids[0])) break;
@@ -233,20 +324,57 @@ bool fap_server::launch(int gi) {
     progressed = true;
   }
   if (g.pending.empty()) return progressed;
+  cudaEventRecord(g.start, g.stream);
+  // Resident cache (every part's boundary rows and closed Floyd matrix):
+  // built on the graph's first batch when it fits, queued on the graph's
+  // stream ahead of the batch.
+  bool cached = cache_built(g);
+  if (!cached) {
+    int64_t cb = 0;
+    int built = 0;
+    bool hopeless = false;
+    if (fap_graph_cache_bytes(g.dg, &cb, &built) == FAP_OK && make_room(cb, gi, &hopeless) &&
+        fap_graph_cache_build(g.dg) == FAP_OK) {
+      cached = true;
+      std::lock_guard<std::mutex> lk(mu);
+      cache_builds++;
+    }
+  }
   const int kind = g.pending.front()->kind;
   std::vector<Req *> batch;
   std::vector<int32_t> parts;
-  std::vector<char> in_batch(g.K + 1, 0);
-  // Device bytes the batch will need (upper bounds of what fap_solve /
-  // fap_graph_copy_block / fap_graph_rows_async allocate):
-  //   sub-graph: output rows x ldD + one padded Floyd square per part (all of
-  //   the batch's largest side) + SSSP scratch rows (at most one per
-  //   boundary vertex) + the int32->float staging of the largest block;
-  //   rows: result rows + SSSP scratch rows + one checksum per row.
+  std::vector<int64_t> part_row(g.K + 1, -1);  // first row of a batch part in the checksums
+  // Batch buffers are sized once from the batch cap (output matrix, distance
+  // rows, checksums), so that steady-state batches allocate nothing: only a
+  // single request larger than the cap grows them.
+  const int64_t cap = max_batch_bytes > 0 ? (int64_t)max_batch_bytes : INT64_MAX / 4;
+  const int64_t row_bytes = kind == FAP_REQ_ROWS ? (int64_t)g.n * 4 : g.ldD * 4;
+  int64_t limit_rows = std::max<int64_t>(1, cap / row_bytes);
+  if (max_batch_rows > 0) limit_rows = std::min<int64_t>(limit_rows, max_batch_rows);
+  if (kind == FAP_REQ_SUBGRAPH) limit_rows = std::min<int64_t>(std::max<int64_t>(limit_rows, g.max_part), g.n);
+  // Device bytes the batch still needs beyond what the graph holds (upper
+  // bounds of what fap_solve / fap_graph_copy_block / fap_graph_rows_async
+  // allocate): the output matrix or rows buffer and the checksums up to
+  // their target sizes; without the resident cache also one padded Floyd
+  // square per part (all of the batch's largest side) and SSSP scratch rows
+  // (at most one per source); the int32->float staging of the largest block
+  // copied to the host.
+  // When the buffers at their target size do not fit the budget, the batch
+  // is sized exactly (its own rows only).
   int64_t rows = 0, nparts = 0, ldf = 0, srcs = 0, stage_rows = 0;
+  bool exact = false;
   auto footprint = [&](int64_t r, int64_t np, int64_t lf, int64_t sc, int64_t sg) -> int64_t {
-    if (kind == FAP_REQ_ROWS) return r * (int64_t)g.n * 4 * 2 + r * 8;
-    return r * g.ldD * 4 + np * lf * lf * 4 + sc * (int64_t)g.n * 4 + sg * (int64_t)g.n * 4;
+    const int64_t target = exact ? r : std::max(r, limit_rows);
+    int64_t need = std::max<int64_t>(0, target - g.cs_cap) * 8 + sg * (int64_t)g.n * 4;
+    if (kind == FAP_REQ_ROWS) {
+      const int64_t b = r * (int64_t)g.n * 4;
+      need += b > kSmallRowsBytes ? b : std::max<int64_t>(0, b - g.rows_small_cap * 4);
+      if (!cached) need += r * (int64_t)g.n * 4;
+    } else {
+      need += std::max<int64_t>(0, target - g.reserved_rows) * g.ldD * 4;
+      if (!cached) need += np * lf * lf * 4 + sc * (int64_t)g.n * 4;
+    }
+    return need;
   };
   for (auto it = g.pending.begin(); it != g.pending.end();) {
     Req *r = *it;
@@ -254,7 +382,7 @@ bool fap_server::launch(int gi) {
     int64_t add_rows = 0, n_parts = nparts, n_ldf = ldf, n_srcs = srcs, n_stage = stage_rows;
     if (kind == FAP_REQ_SUBGRAPH) {
       const int32_t p = r->ids[0];
-      if (!in_batch[p]) {
+      if (part_row[p] < 0) {
         add_rows = g.vnum[p];
         n_parts++;
         n_ldf = std::max<int64_t>(n_ldf, ((int64_t)std::max(g.vnum[p], 1) + 127) / 128 * 128);
@@ -264,11 +392,16 @@ bool fap_server::launch(int gi) {
     } else {
       add_rows = (int64_t)r->ids.size();
     }
-    if (!batch.empty() && max_batch_rows > 0 && rows + add_rows > max_batch_rows) break;
+    if (!batch.empty() && rows + add_rows > limit_rows) break;
     bool hopeless = false;
-    if (!make_room(footprint(rows + add_rows, n_parts, n_ldf, n_srcs, n_stage), gi, &hopeless)) {
+    bool fits = make_room(footprint(rows + add_rows, n_parts, n_ldf, n_srcs, n_stage), gi, &hopeless);
+    if (!fits && batch.empty() && !exact) {
+      exact = true;
+      fits = make_room(footprint(rows + add_rows, n_parts, n_ldf, n_srcs, n_stage), gi, &hopeless);
+    }
+    if (!fits) {
       if (!batch.empty()) break;  // run what fits
-      if (!hopeless) return progressed;  // wait for another graph's batch to finish
+      if (!hopeless) return true;  // wait for another graph's batch to finish
       it = g.pending.erase(it);  // larger than the whole budget
       finish(r, FAP_REQ_FAILED, FAP_ERR_NOMEM);
       progressed = true;
@@ -279,70 +412,83 @@ bool fap_server::launch(int gi) {
     srcs = n_srcs;
     stage_rows = n_stage;
     batch.push_back(r);
-    rows += add_rows;
     if (kind == FAP_REQ_SUBGRAPH) {
-      if (!in_batch[r->ids[0]]) parts.push_back(r->ids[0]);
-      in_batch[r->ids[0]] = 1;
+      const int32_t p = r->ids[0];
+      if (part_row[p] < 0) {
+        part_row[p] = rows;
+        parts.push_back(p);
+      }
+      r->row_off = part_row[p];
+    } else {
+      r->row_off = rows;
     }
+    rows += add_rows;
     it = g.pending.erase(it);
   }
   if (batch.empty()) return progressed;
+  bool want_cs = false;
+  for (Req *r : batch) want_cs |= (r->cs_out != nullptr);
+  want_cs &= (g.dtype == FAP_DTYPE_I32);
   int rc = FAP_OK;
+  const int64_t target = exact ? rows : std::max(rows, limit_rows);
+  if (want_cs && (!grow_dev(&g.cs_dev, &g.cs_cap, target) || !grow_host(&g.cs_host, &g.cs_host_cap, target)))
+    rc = FAP_ERR_NOMEM;
   const double t0 = now_s();
-  if (kind == FAP_REQ_SUBGRAPH) {
+  if (rc == FAP_OK && kind == FAP_REQ_SUBGRAPH) {
     if (rows > g.reserved_rows) {
-      rc = fap_graph_reserve(g.dg, rows);
-      if (rc == FAP_OK) g.reserved_rows = rows;
+      rc = fap_graph_reserve(g.dg, target);
+      if (rc == FAP_OK) g.reserved_rows = target;
     }
     if (rc == FAP_OK) rc = fap_solve(g.dg, parts.data(), (int32_t)parts.size(), FAP_MODE_BATCHED);
-  } else {
-    // every rows request of the batch in one SSSP launch
+    if (want_cs)
+      for (size_t i = 0; rc == FAP_OK && i < parts.size(); i++)
+        rc = fap_graph_checksums_async(g.dg, parts[i], g.cs_dev + part_row[parts[i]]);
+  } else if (rc == FAP_OK) {
+    // every rows request of the batch in one launch sequence
     std::vector<int32_t> sources;
-    for (Req *r : batch) {
-      r->row_off = (int64_t)sources.size();
-      sources.insert(sources.end(), r->ids.begin(), r->ids.end());
-    }
-    const int64_t need = (int64_t)sources.size() * g.n;
-    if (need > g.rows_cap) {
-      release_rows(g);
-      if (cudaMalloc(&g.rows_buf, (size_t)need * 4) != cudaSuccess) {
+    for (Req *r : batch) sources.insert(sources.end(), r->ids.begin(), r->ids.end());
+    const int64_t bytes = rows * (int64_t)g.n * 4;
+    g.rows_pooled = bytes > kSmallRowsBytes;
+    if (g.rows_pooled) {
+      if (cudaMallocFromPoolAsync(reinterpret_cast<void **>(&g.rows_out), (size_t)bytes, pool, g.stream) !=
+          cudaSuccess) {
         cudaGetLastError();
-        g.rows_buf = nullptr;
+        g.rows_out = nullptr;
         rc = FAP_ERR_NOMEM;
-      } else {
-        g.rows_cap = need;
       }
+    } else if (grow_dev(&g.rows_small, &g.rows_small_cap, rows * (int64_t)g.n)) {
+      g.rows_out = g.rows_small;
+    } else {
+      rc = FAP_ERR_NOMEM;
     }
-    bool want_cs = false;
-    for (Req *r : batch) want_cs |= (r->cs_out != nullptr);
-    want_cs &= (g.dtype == FAP_DTYPE_I32);
-    if (rc == FAP_OK && want_cs && (int64_t)sources.size() > g.cs_cap) {
-      if (g.cs_buf) cudaFree(g.cs_buf);
-      g.cs_buf = nullptr;
-      g.cs_cap = 0;
-      if (cudaMalloc(&g.cs_buf, sources.size() * 8) != cudaSuccess) {
-        cudaGetLastError();
-        g.cs_buf = nullptr;
-        rc = FAP_ERR_NOMEM;
-      } else {
-        g.cs_cap = (int64_t)sources.size();
-      }
-    }
-    if (rc == FAP_OK) rc = fap_graph_rows_async(g.dg, sources.data(), (int32_t)sources.size(), g.rows_buf);
+    float *out = g.rows_out;
+    if (rc == FAP_OK) rc = fap_graph_rows_async(g.dg, sources.data(), (int32_t)sources.size(), out);
     if (rc == FAP_OK && want_cs) {
       int64_t launches = 0;
-      if (fapb::launch_row_checksums(g.rows_buf, (int64_t)sources.size(), g.n, g.n, g.cs_buf, g.stream,
-                                     &launches) != cudaSuccess) {
+      if (fapb::launch_row_checksums(out, rows, g.n, g.n, g.cs_dev, g.stream, &launches) !=
+          cudaSuccess) {
         cudaGetLastError();
         rc = FAP_ERR_CUDA;
       }
     }
   }
+  if (rc == FAP_OK && want_cs &&
+      cudaMemcpyAsync(g.cs_host, g.cs_dev, (size_t)rows * 8, cudaMemcpyDeviceToHost, g.stream) != cudaSuccess) {
+    cudaGetLastError();
+    rc = FAP_ERR_CUDA;
+  }
+  if (rc == FAP_OK) rc = fap_graph_status_async(g.dg, g.status_host);
+  if (rc == FAP_OK && cudaEventRecord(g.done, g.stream) != cudaSuccess) {
+    cudaGetLastError();
+    rc = FAP_ERR_CUDA;
+  }
   if (rc != FAP_OK) {
+    cudaStreamSynchronize(g.stream);
+    if (g.rows_out && g.rows_pooled) cudaFreeAsync(g.rows_out, g.stream);
+    g.rows_out = nullptr;
     for (Req *r : batch) finish(r, FAP_REQ_FAILED, rc);
     return true;
   }
-  cudaEventRecord(g.done, g.stream);
   for (Req *r : batch) {
     r->t_start = t0;
     std::lock_guard<std::mutex> lk(mu);
@@ -426,6 +572,17 @@ int fap_server_create(int device, double budget_bytes, int64_t max_batch_rows, f
   s->device = device;
   s->budget = budget_bytes > 0 ? (int64_t)budget_bytes : (int64_t)(0.6 * (double)free_b);
   s->max_batch_rows = max_batch_rows;
+  cudaMemPoolProps props{};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = device;
+  if (cudaMemPoolCreate(&s->pool, &props) != cudaSuccess) {
+    cudaGetLastError();
+    delete s;
+    return serr(FAP_ERR_CUDA, "cudaMemPoolCreate failed");
+  }
+  uint64_t keep = (uint64_t)(s->budget / 4);
+  cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
   s->worker = std::thread([s] { s->loop(); });
   *out = s;
   return FAP_OK;
@@ -448,11 +605,17 @@ int fap_server_destroy(fap_server *s) {
   const int ng = s->ngraphs.load();
   for (int i = 0; i < ng; i++) {
     GSlot &g = *s->graphs[i];
+    cudaStreamSynchronize(g.stream);
+    if (g.start) cudaEventDestroy(g.start);
     if (g.done) cudaEventDestroy(g.done);
-    release_rows(g);
+    if (g.cs_dev) cudaFree(g.cs_dev);
+    if (g.rows_small) cudaFree(g.rows_small);
+    if (g.cs_host) cudaFreeHost(g.cs_host);
+    if (g.status_host) cudaFreeHost(g.status_host);
     fap_graph_destroy(g.dg);
     fap_ctx_destroy(g.ctx);
   }
+  if (s->pool) cudaMemPoolDestroy(s->pool);
   for (auto &kv : s->reqs) delete kv.second;
   delete s;
   return FAP_OK;
@@ -485,6 +648,7 @@ int fap_server_add_graph(fap_server *s, int32_t n, int64_t m, const int32_t *row
   g->vnum.assign(ver_num, ver_num + K + 1);
   g->voff.assign(ver_offset, ver_offset + K + 1);
   g->bnum.assign(bdy_num, bdy_num + K + 1);
+  for (int32_t p = 1; p <= K; p++) g->max_part = std::max<int64_t>(g->max_part, ver_num[p]);
   // Batches change from one launch to the next: launch the stages directly
   // instead of capturing a CUDA graph per batch.
   fap_graph_set_param(g->dg, "cuda_graph", 0);
@@ -492,8 +656,11 @@ int fap_server_add_graph(fap_server *s, int32_t n, int64_t m, const int32_t *row
   void *stream = nullptr;
   fap_ctx_get_stream(g->ctx, &stream);
   g->stream = reinterpret_cast<cudaStream_t>(stream);
-  if (cudaEventCreateWithFlags(&g->done, cudaEventDisableTiming) != cudaSuccess) {
+  if (cudaEventCreate(&g->start) != cudaSuccess || cudaEventCreate(&g->done) != cudaSuccess ||
+      !grow_host(&g->status_host, &g->status_host_cap, 1)) {
     cudaGetLastError();
+    if (g->start) cudaEventDestroy(g->start);
+    if (g->done) cudaEventDestroy(g->done);
     fap_graph_destroy(g->dg);
     fap_ctx_destroy(g->ctx);
     return serr(FAP_ERR_CUDA, "cudaEventCreate failed");
@@ -591,8 +758,8 @@ int fap_server_drain(fap_server *s) {
   return FAP_OK;
 }
 
-int fap_server_stats(fap_server *s, double *out8) {
-  if (!s || !out8) return serr(FAP_ERR_INVALID, "NULL argument");
+int fap_server_stats(fap_server *s, double *out, int32_t count) {
+  if (!s || (!out && count > 0)) return serr(FAP_ERR_INVALID, "NULL argument");
   std::lock_guard<std::mutex> lk(s->mu);
   std::vector<double> v = s->lat_ms;
   std::sort(v.begin(), v.end());
@@ -603,14 +770,18 @@ int fap_server_stats(fap_server *s, double *out8) {
   };
   double mean = 0;
   for (double x : v) mean += x;
-  out8[0] = (double)v.size();
-  out8[1] = (double)s->entries;
-  out8[2] = pct(0.50);
-  out8[3] = pct(0.99);
-  out8[4] = v.empty() ? 0.0 : mean / (double)v.size();
-  out8[5] = (double)s->peak_bytes;
-  out8[6] = (double)s->batches;
-  out8[7] = (double)s->resident_hits;
+  const double all[FAP_SERVER_NSTATS] = {(double)v.size(),
+                                         (double)s->entries,
+                                         pct(0.50),
+                                         pct(0.99),
+                                         v.empty() ? 0.0 : mean / (double)v.size(),
+                                         (double)s->peak_bytes,
+                                         (double)s->batches,
+                                         (double)s->resident_hits,
+                                         (double)s->failed,
+                                         (double)s->cache_builds,
+                                         s->busy_ms};
+  for (int32_t i = 0; i < count; i++) out[i] = i < FAP_SERVER_NSTATS ? all[i] : 0.0;
   return FAP_OK;
 }
 
@@ -622,7 +793,27 @@ int fap_server_reset_stats(fap_server *s) {
   s->batches = 0;
   s->resident_hits = 0;
   s->peak_bytes = 0;
+  s->failed = 0;
+  s->cache_builds = 0;
+  s->busy_ms = 0;
   return FAP_OK;
+}
+
+int fap_server_set_option(fap_server *s, const char *key, double value) {
+  if (!s || !key) return serr(FAP_ERR_INVALID, "NULL argument");
+  if (std::strcmp(key, "max_batch_bytes") == 0) {
+    s->max_batch_bytes = value > 0 ? (int64_t)value : 0;
+    return FAP_OK;
+  }
+  if (std::strcmp(key, "max_batch_rows") == 0) {
+    s->max_batch_rows = value > 0 ? (int64_t)value : 0;
+    return FAP_OK;
+  }
+  if (std::strcmp(key, "budget_bytes") == 0 && value > 0) {
+    s->budget = (int64_t)value;
+    return FAP_OK;
+  }
+  return serr(FAP_ERR_INVALID, "unknown option");
 }
 
 const char *fap_server_last_error(void) { return s_err.c_str(); }

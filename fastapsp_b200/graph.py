@@ -406,6 +406,41 @@ class DeviceGraph:
         check(lib().fap_graph_block_checksums(self._h, int(part), ptr(out)), "checksums")
         return out
 
+    def cache_build(self) -> None:
+        """Builds the resident cache (every part's boundary rows and closed
+        Floyd matrix); later batched solves and rows() use it."""
+        check(lib().fap_graph_cache_build(self._h), "fap_graph_cache_build")
+
+    def cache_release(self) -> None:
+        check(lib().fap_graph_cache_release(self._h), "fap_graph_cache_release")
+
+    def cache_bytes(self):
+        """(bytes, built): what the cache holds, or would need if not built."""
+        b = ctypes.c_int64()
+        built = ctypes.c_int()
+        check(lib().fap_graph_cache_bytes(self._h, ctypes.byref(b), ctypes.byref(built)),
+              "fap_graph_cache_bytes")
+        return int(b.value), bool(built.value)
+
+    def device_bytes(self) -> int:
+        b = ctypes.c_int64()
+        check(lib().fap_graph_device_bytes(self._h, ctypes.byref(b)), "fap_graph_device_bytes")
+        return int(b.value)
+
+    def release(self) -> None:
+        check(lib().fap_graph_release(self._h), "fap_graph_release")
+
+    def rows(self, sources: Sequence[int]) -> np.ndarray:
+        """Distance rows (float32) through fap_graph_rows_async: from the
+        resident cache when it is built, else by SSSP."""
+        import torch
+        s = _i32(list(sources))
+        out = torch.empty((s.shape[0], self.n), dtype=torch.float32, device="cuda")
+        check(lib().fap_graph_rows_async(self._h, ptr(s), int(s.shape[0]), ptr(out)),
+              "fap_graph_rows_async")
+        self.check()
+        return out.cpu().numpy()
+
     def sssp_rows(self, sources: Sequence[int]) -> np.ndarray:
         s = _i32(list(sources))
         out = np.empty((s.shape[0], self.n), np.float32)

@@ -41,6 +41,9 @@ class ServerStats:
     peak_bytes: int
     batches: int
     resident_hits: int
+    failed: int
+    cache_builds: int
+    busy_ms: float
 
 
 class Request:
@@ -108,7 +111,7 @@ class Server:
         ro, cv, w = g.csr()
         vn, vo, bn = g.partInfo()
         return self.add_csr(ro, cv, w, int(vn.shape[0] - 1), g.getGraphId(), g.getMapping(),
-                            vn, vo, bn, g.dtype if dtype is None else dtype)
+                            vn, vo, bn, g.dtype() if dtype is None else dtype)
 
     def add_csr(self, row_offset, col_val, weight, K: int, graph_id, st2ed, ver_num, ver_offset,
                 bdy_num, dtype: int = L.FAP_DTYPE_AUTO) -> int:
@@ -127,9 +130,14 @@ class Server:
         self._graphs.append((n, vn))
         return int(idx.value)
 
+    def _meta(self, graph: int):
+        if 0 <= graph < len(self._graphs):
+            return self._graphs[graph]
+        return 0, np.zeros(1, np.int32)   # unknown index: the library rejects the request
+
     def _submit(self, graph: int, kind: int, ids: np.ndarray, rows: int, distances: bool,
                 checksums: bool) -> Request:
-        n = self._graphs[graph][0]
+        n = self._meta(graph)[0]
         out = np.empty((rows, n), np.float32) if distances else None
         cs = np.empty(rows, np.uint64) if checksums else None
         rid = ctypes.c_int64()
@@ -140,7 +148,7 @@ class Server:
     def submit_subgraph(self, graph: int, part: int, distances: bool = True,
                         checksums: bool = False) -> Request:
         """The ver_num[part] x n block of one part (rows in st2ed order)."""
-        vn = self._graphs[graph][1]
+        vn = self._meta(graph)[1]
         rows = int(vn[part]) if 1 <= part < vn.shape[0] else 0
         return self._submit(graph, REQ_SUBGRAPH, L_i32([part]), rows, distances, checksums)
 
@@ -150,14 +158,18 @@ class Server:
         s = L_i32(np.asarray(sources).ravel())
         return self._submit(graph, REQ_ROWS, s, int(s.shape[0]), distances, checksums)
 
+    def set_option(self, key: str, value: float) -> None:
+        """"max_batch_bytes", "max_batch_rows" or "budget_bytes"."""
+        check(lib().fap_server_set_option(self._h, key.encode(), float(value)), "set_option")
+
     def drain(self) -> None:
         check(lib().fap_server_drain(self._h), "fap_server_drain")
 
     def stats(self) -> ServerStats:
-        v = np.zeros(8, np.float64)
-        check(lib().fap_server_stats(self._h, ptr(v)), "fap_server_stats")
+        v = np.zeros(11, np.float64)
+        check(lib().fap_server_stats(self._h, ptr(v), 11), "fap_server_stats")
         return ServerStats(int(v[0]), int(v[1]), float(v[2]), float(v[3]), float(v[4]), int(v[5]),
-                           int(v[6]), int(v[7]))
+                           int(v[6]), int(v[7]), int(v[8]), int(v[9]), float(v[10]))
 
     def reset_stats(self) -> None:
         check(lib().fap_server_reset_stats(self._h), "fap_server_reset_stats")

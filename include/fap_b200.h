@@ -145,7 +145,8 @@ FAP_API int fap_graph_sssp_rows(fap_dgraph *g, const int32_t *sources, int32_t c
  * chain-following off, the default); "cuda_graph" (non-zero, the default:
  * a batched solve captures its launch sequence in a CUDA graph on first use
  * and replays it while the batch, buffers, parameters and stream are
- * unchanged). */
+ * unchanged); "use_cache" (non-zero, the default: batched solves and
+ * fap_graph_rows_async use the resident cache once it is built). */
 FAP_API int fap_graph_set_param(fap_dgraph *g, const char *key, double value);
 
 /* Tunes the SSSP bucket width: runs the SSSP stage on `sample` boundary
@@ -159,8 +160,9 @@ FAP_API int fap_graph_tune_sssp(fap_dgraph *g, const double *deltas, int32_t cou
 /* Mean edge weight of the graph (the scale SSSP bucket widths are tuned in). */
 FAP_API double fap_graph_mean_weight(const fap_dgraph *g);
 
-/* Frees the output matrix, Floyd arena and scratch of g (the CSR and the
- * partition stay resident); no block stays resident afterwards. */
+/* Frees the output matrix, Floyd arena and scratch of g (the CSR, the
+ * partition and the resident cache stay); no block stays resident
+ * afterwards. */
 FAP_API int fap_graph_release(fap_dgraph *g);
 /* Device bytes g holds now. */
 FAP_API int fap_graph_device_bytes(const fap_dgraph *g, int64_t *bytes);
@@ -170,6 +172,33 @@ FAP_API int fap_graph_resident(fap_dgraph *g, int32_t part);
  * (host ids) into d_out (device, count x n floats, dense); returns without
  * waiting.  Device errors surface in fap_graph_check. */
 FAP_API int fap_graph_rows_async(fap_dgraph *g, const int32_t *sources, int32_t count, float *d_out);
+
+/* Asynchronous forms for pipelines that must not block: queue, on the
+ * context stream, the per-row checksums of a resident part's block into
+ * device memory (rows x uint64, int32 path), and a copy of the graph's
+ * device status word into host memory (pinned for the copy to be
+ * asynchronous).  Once the stream has passed the copy, fap_status_code turns
+ * the word into FAP_OK or the error code fap_graph_check would return. */
+FAP_API int fap_graph_checksums_async(fap_dgraph *g, int32_t part, uint64_t *d_out);
+FAP_API int fap_graph_status_async(fap_dgraph *g, int32_t *host_status);
+FAP_API int fap_status_code(int32_t device_status);
+
+/* Resident cache for serving (no counterpart in the reference, which
+ * recomputes every part's stages 1-2 on each solveSubGraph): computes, on
+ * the context stream, the boundary rows of every part (stage 1 for all
+ * boundary vertices) and every part's closed Floyd matrix (stage 2), and
+ * keeps both in HBM.  Later batched solves then copy the parts' boundary
+ * rows and run only the min-plus merge; fap_graph_rows_async computes a
+ * row as the min-plus of the source's closed Floyd row with its part's
+ * boundary rows.  Both give exactly the values of the uncached path (the
+ * same min over the same sums).  Returns once the cache is built (its SSSP
+ * scratch is freed again); device errors surface in fap_graph_check; a new
+ * partition drops the cache. */
+FAP_API int fap_graph_cache_build(fap_dgraph *g);
+FAP_API int fap_graph_cache_release(fap_dgraph *g);
+/* Device bytes the cache holds (*built = 1) or would need to be built,
+ * including its SSSP scratch (*built = 0). */
+FAP_API int fap_graph_cache_bytes(const fap_dgraph *g, int64_t *bytes, int *built);
 
 /* Device time (ms) of the stages of the last fap_solve, measured with events
  * on the context stream: [sssp, gather, floyd, minplus, total]. */

@@ -11,9 +11,13 @@
  * of a graph that fit one batch run as one batched solve; a request for a
  * part that is still resident from an earlier batch is answered without
  * recomputing), admits a batch only when its estimated device footprint
- * fits the memory budget (idle graphs' buffers are released first), and
- * runs each graph on its own stream, so batches of different graphs overlap
- * on the GPU while new requests keep arriving (continuous batching).
+ * fits the memory budget (idle graphs' output buffers, then their caches,
+ * are released first), and runs each graph on its own stream, so batches of
+ * different graphs overlap on the GPU while new requests keep arriving
+ * (continuous batching).  On a graph's first batch the server builds its
+ * resident cache (fap_graph_cache_build: every part's boundary rows and
+ * closed Floyd matrix) when it fits, after which sub-graph batches run only
+ * the min-plus merge and distance rows come from the cache.
  * Results are copied to the caller's host buffers (float distances) and/or
  * reduced to per-row checksums (int32 graphs).
  */
@@ -43,6 +47,12 @@ typedef struct fap_server fap_server;
  * one batch (<= 0: no limit beyond the budget). */
 FAP_API int fap_server_create(int device, double budget_bytes, int64_t max_batch_rows,
                               fap_server **out);
+/* Limits, changeable while the server runs: "max_batch_bytes" (output bytes
+ * of one batch beyond its first request, and the size each graph's batch
+ * buffers are allocated at once; default 512 MiB, <= 0: no limit),
+ * "max_batch_rows" (<= 0: no limit), "budget_bytes" (> 0). */
+FAP_API int fap_server_set_option(fap_server *s, const char *key, double value);
+
 /* Waits for the requests in flight, fails the queued ones, frees everything. */
 FAP_API int fap_server_destroy(fap_server *s);
 
@@ -79,11 +89,15 @@ FAP_API int fap_server_forget(fap_server *s, int64_t req_id);
 /* Waits until every submitted request is done or failed. */
 FAP_API int fap_server_drain(fap_server *s);
 
-/* out8 = [requests completed, entries produced, p50 latency ms, p99 latency
- * ms, mean latency ms, peak device bytes held, batches launched, requests
- * answered from resident blocks] over the requests completed since the last
- * reset. */
-FAP_API int fap_server_stats(fap_server *s, double *out8);
+/* Figures over the requests finished since the last reset; out[i] for
+ * i < count (entries past FAP_SERVER_NSTATS read 0):
+ *   0 requests completed   1 entries produced      2 p50 latency ms
+ *   3 p99 latency ms       4 mean latency ms       5 peak device bytes held
+ *   6 batches launched     7 answered from resident blocks
+ *   8 requests failed      9 resident caches built 10 device busy ms (sum of
+ *   the finished batches' durations, over all graphs' streams). */
+#define FAP_SERVER_NSTATS 11
+FAP_API int fap_server_stats(fap_server *s, double *out, int32_t count);
 FAP_API int fap_server_reset_stats(fap_server *s);
 
 /* Message of the last fap_server_* failure on the calling thread. */

@@ -1,8 +1,9 @@
 """Serving loop (fap_server_*): every request's result is the same whether it
 runs alone on a fresh server or mixed with other graphs' and other kinds of
 requests, submitted from several threads, under a roomy or a tiny memory
-budget; results also match the reference's outputs (golden fixtures) and the
-oracle's Dijkstra rows.  Tolerances as in the parity tests: int32 bit-exact,
+budget (the tiny one leaves the largest graph without its resident cache, so
+its requests take the uncached path); results also match the reference's
+outputs (golden fixtures: rows of its solved blocks).  Tolerances as in the parity tests: int32 bit-exact,
 float32 |d - ref| <= 1e-5 |ref| with reachability exact.
 """
 import threading
@@ -62,22 +63,24 @@ def _same(a, b):
 
 
 def _check_against_reference(case, req, got):
+    """Sub-graph blocks and distance rows against the reference's own output
+    (rows of its solved blocks: full distances, or per-row checksums)."""
     kind, ids = req
-    ro, col, w = case["row_offset"], case["col_val"], case["weight"]
+    n = int(case["n"])
     integral = bool(case["integral"])
     if kind == REQ_SUBGRAPH:
         p = ids[0]
         off, rows = int(case["ver_offset"][p]), int(case["ver_num"][p])
-        assert got.shape == (rows, int(case["n"]))
-        if "dist" in case:
-            ref = case["dist"][off:off + rows]
-        else:
-            np.testing.assert_array_equal(O.row_checksums(O.to_i32(got)),
-                                          case["row_checksums"][off:off + rows])
-            return
+        pos = np.arange(off, off + rows)
     else:
-        ref = np.stack([O.port_dijkstra(ro, col, w, s) for s in ids])
-    ref = np.asarray(ref, np.float32)
+        ed2st = np.empty(n, np.int64)
+        ed2st[case["st2ed"]] = np.arange(n)
+        pos = ed2st[np.asarray(ids)]
+    assert got.shape == (len(pos), n)
+    if "dist" not in case:
+        np.testing.assert_array_equal(O.row_checksums(O.to_i32(got)), case["row_checksums"][pos])
+        return
+    ref = np.asarray(case["dist"][pos], np.float32)
     if integral:
         _same(got, ref)
     else:
@@ -100,13 +103,16 @@ def test_alone_results_match_reference(cuda_ok, served):
         _check_against_reference(cases[ci], req, got)
 
 
-@pytest.mark.parametrize("budget_mb", [0, 24])
-def test_same_alone_and_in_mix(cuda_ok, served, budget_mb):
+@pytest.mark.parametrize("budget_mb,batch_bytes", [(0, 0), (24, 0), (0, 1)])
+def test_same_alone_and_in_mix(cuda_ok, served, budget_mb, batch_bytes):
     """Requests of four graphs, both kinds, submitted in a shuffled order from
     three threads; budget 0 = default (roomy), 24 MB = room for about one
-    part of the largest graph at a time (forces eviction and re-solves)."""
+    part of the largest graph at a time (forces eviction and re-solves);
+    batch_bytes 1 = one request per batch, 0 = the default cap."""
     cases, reqs, alone = served
     with Server(0, budget_bytes=budget_mb * 2**20) as srv:
+        if batch_bytes:
+            srv.set_option("max_batch_bytes", batch_bytes)
         gis = [_add(srv, c) for c in cases]
         handles = [None] * len(reqs)
 
@@ -126,8 +132,9 @@ def test_same_alone_and_in_mix(cuda_ok, served, budget_mb):
             assert info["status"] == L.FAP_OK and info["latency_ms"] >= 0
         srv.drain()
         st = srv.stats()
-        assert st.completed == len(reqs)
+        assert st.completed == len(reqs) and st.failed == 0
         assert st.batches + st.resident_hits <= len(reqs)
+        assert st.busy_ms > 0
         assert st.p99_ms >= st.p50_ms > 0
         if budget_mb:
             assert st.peak_bytes <= budget_mb * 2**20
@@ -142,7 +149,7 @@ def test_repeat_of_resident_block_is_not_recomputed(cuda_ok, served):
         _same(a, b)
         _same(a, alone[(0, (REQ_SUBGRAPH, (3,)))])
         st = srv.stats()
-        assert st.batches == 1 and st.resident_hits == 1
+        assert st.batches == 1 and st.resident_hits == 1 and st.cache_builds == 1
 
 
 def test_invalid_requests_fail_cleanly(cuda_ok, served):
@@ -159,7 +166,7 @@ def test_invalid_requests_fail_cleanly(cuda_ok, served):
         with pytest.raises(FapError):
             srv.submit_subgraph(gi + 5, 1)                  # no such graph
         # a request larger than the whole budget fails, the server carries on
-        big = srv.submit_rows(gi, list(range(int(c["n"]))) * 2)
+        big = srv.submit_rows(gi, list(range(int(c["n"]))) * 8)   # 5.8 MB > 2 MB
         assert big.wait(120) == FAILED
         assert big.info()["status"] == L.FAP_ERR_NOMEM
         ok = srv.submit_subgraph(gi, 2)
