@@ -211,8 +211,8 @@ def ref_available() -> bool:
 
 def run_ref(workdir: str, name: str, directed: bool, weighted: bool, K: int, *,
             parts="all", meta_out: str | None = None, dist_out: str | None = None,
-            threads: int | None = None, partition_file: str | None = None,
-            timeout: float | None = None) -> list:
+            path_out: str | None = None, threads: int | None = None,
+            partition_file: str | None = None, timeout: float | None = None) -> list:
     """Run the reference's CPU path (oracle/_ref/fap_ref) and return its JSON
     event lines."""
     if not ref_available():
@@ -224,6 +224,8 @@ def run_ref(workdir: str, name: str, directed: bool, weighted: bool, K: int, *,
         cmd += ["--meta", os.path.abspath(meta_out)]
     if dist_out:
         cmd += ["--dist", os.path.abspath(dist_out)]
+    if path_out:
+        cmd += ["--path", os.path.abspath(path_out)]
     env = dict(os.environ)
     if threads:
         env["OMP_NUM_THREADS"] = str(threads)
@@ -250,3 +252,143 @@ def row_checksums(block_i32: np.ndarray) -> np.ndarray:
     wts = (2 * np.arange(b.shape[1], dtype=np.uint64) + 1)
     with np.errstate(over="ignore"):
         return (b * wts[None, :]).sum(axis=1, dtype=np.uint64)
+
+
+# --------------------------------------------------------------------------
+# Predecessor (path) matrices
+# --------------------------------------------------------------------------
+#
+# The reference records, for every entry, the vertex before j on the
+# shortest path it found (path[u] = ver in dijkstra_path,
+# fap/kernel/batch_sssp.h:108-110; path[i][j] = path[k][j] in floyd_CPU_path,
+# fap/kernel/floyd.h:38-49; path = mat2_path[k][j] for the first minimal k in
+# min_plus_path_CPU_advanced, fap/kernel/minplus.h:51-65; edge entries
+# path = ver and the diagonal path = the vertex itself in MysubMatBuild_path,
+# fap/utils/util_Myalgorithm.h:30-73; -1 where nothing was set).  Which of
+# several equally short paths it keeps depends on its evaluation order.  The
+# B200 path picks, from the final distances, the in-neighbour u of j with the
+# least dist[u] + w(u, j) (the smallest u among equal sums): the same meaning,
+# a fixed rule on ties.  port_predecessors restates that rule;
+# tests/test_oracle.py pins it to the reference's own matrices on every entry
+# whose predecessor is unique.
+
+def in_edges(row_offset, col, weight):
+    """(tro, tcol, tw): the CSR of in-edges (j's sources in tcol[tro[j]:
+    tro[j+1]], ascending), with their weights."""
+    ro = np.asarray(row_offset, np.int64)
+    n = ro.shape[0] - 1
+    m = int(ro[-1])
+    src = np.repeat(np.arange(n, dtype=np.int64), np.diff(ro))
+    dst = np.asarray(col[:m], np.int64)
+    w = np.asarray(weight[:m])
+    order = np.lexsort((src, dst))
+    tro = np.zeros(n + 1, np.int64)
+    np.add.at(tro, dst + 1, 1)
+    return np.cumsum(tro), src[order], w[order]
+
+
+def port_predecessors(dist_rows, row_vertices, row_offset, col, weight, integral: bool):
+    """P[r][j] = argmin over in-edges (u -> j) of dist_rows[r][u] + w (sums in
+    int64 for integer distances, float32 otherwise; the smallest u among
+    equal sums), P[r][src] = src, -1 where dist_rows[r][j] >= 1e8."""
+    D = np.asarray(dist_rows)
+    R, n = D.shape
+    tro, tcol, tw = in_edges(row_offset, col, weight)
+    if integral:
+        Dv = D.astype(np.int64)
+        cand = Dv[:, tcol] + tw.astype(np.int64)[None, :]
+        big = np.int64(1) << 62
+        cand = np.where(Dv[:, tcol] >= 100000000, big, cand)
+    else:
+        Dv = D.astype(np.float32)
+        cand = Dv[:, tcol] + tw.astype(np.float32)[None, :]
+        big = np.float32(np.inf)
+        cand = np.where(Dv[:, tcol] >= np.float32(1e8), big, cand)
+    P = np.full((R, n), -1, np.int64)
+    deg = np.diff(tro)
+    has = np.nonzero(deg > 0)[0]
+    if has.size:
+        starts = tro[has]
+        mins = np.minimum.reduceat(cand, starts, axis=1)           # (R, |has|)
+        seg = np.repeat(np.arange(has.size), deg[has])               # edge -> segment
+        at_min = cand == mins[:, seg]
+        pos = np.where(at_min, np.arange(tcol.shape[0])[None, :], tcol.shape[0])
+        first = np.minimum.reduceat(pos, starts, axis=1)             # first edge with the min
+        preds = tcol[np.minimum(first, tcol.shape[0] - 1)]
+        ok = mins < big
+        P[:, has] = np.where(ok, preds, -1)
+    reach = (D < 100000000) if integral else (D.astype(np.float32) < np.float32(1e8))
+    P = np.where(reach, P, -1)
+    P[np.arange(R), np.asarray(row_vertices)] = np.asarray(row_vertices)
+    return P.astype(np.int32)
+
+
+def unique_predecessor_mask(dist_rows, row_vertices, row_offset, col, weight, integral: bool,
+                            rel_gap: float = 1e-5):
+    """Entries whose best in-edge is strictly better than the second best (by
+    rel_gap for float sums) and consistent with dist_rows[r][j]: there, every
+    shortest-path order must pick the same predecessor."""
+    D = np.asarray(dist_rows)
+    R, n = D.shape
+    tro, tcol, tw = in_edges(row_offset, col, weight)
+    Dv = D.astype(np.float64)
+    cand = Dv[:, tcol] + np.asarray(tw, np.float64)[None, :]
+    cand = np.where(Dv[:, tcol] >= 1e8, np.inf, cand)
+    out = np.zeros((R, n), bool)
+    for j in range(n):
+        a, b = tro[j], tro[j + 1]
+        if b - a == 0:
+            continue
+        c = np.sort(cand[:, a:b], axis=1)
+        best = c[:, 0]
+        second = c[:, 1] if b - a > 1 else np.full(R, np.inf)
+        # distinct in-neighbours only: duplicates of the best edge make ties
+        srcs = tcol[a:b]
+        if len(np.unique(srcs)) != len(srcs):
+            continue
+        with np.errstate(invalid="ignore"):
+            gap = (second - best) > (0.0 if integral else rel_gap * np.maximum(best, 1e-30))
+        consistent = np.abs(best - Dv[:, j]) <= (0.0 if integral else 1e-5 * np.maximum(Dv[:, j], 1e-30))
+        out[:, j] = gap & consistent & (Dv[:, j] < 1e8)
+    out[np.arange(R), np.asarray(row_vertices)] = False
+    return out
+
+
+def check_paths(dist_rows, pred_rows, row_vertices, row_offset, col, weight, integral: bool,
+                rel_tol: float = 1e-5):
+    """Validity of predecessor rows: the source maps to itself, unreachable
+    entries are -1, every other entry names an in-neighbour u of j with
+    dist[u] + w(u, j) == dist[j] (within rel_tol for float), and following
+    predecessors from any reachable vertex ends at the source.  Returns the
+    number of entries checked; raises AssertionError on the first failure."""
+    D = np.asarray(dist_rows, np.float64)
+    P = np.asarray(pred_rows, np.int64)
+    R, n = D.shape
+    ro = np.asarray(row_offset, np.int64)
+    m = int(ro[-1])
+    wmin = {}
+    for u in range(n):
+        for e in range(ro[u], ro[u + 1]):
+            key = (u, int(col[e]))
+            wmin[key] = min(wmin.get(key, np.inf), float(weight[e]))
+    checked = 0
+    for r in range(R):
+        s = int(row_vertices[r])
+        assert P[r, s] == s, f"row {r}: source {s} maps to {P[r, s]}"
+        reach = D[r] < 1e8
+        assert np.all(P[r, ~reach] == -1), f"row {r}: unreachable entries with predecessors"
+        for j in np.nonzero(reach)[0]:
+            if j == s:
+                continue
+            u = int(P[r, j])
+            assert (u, int(j)) in wmin, f"row {r}: {u} -> {j} is not an edge"
+            got = D[r, u] + wmin[(u, int(j))]
+            tol = 0.0 if integral else rel_tol * max(abs(D[r, j]), 1e-30)
+            assert abs(got - D[r, j]) <= tol, f"row {r}: d[{u}] + w = {got} != d[{j}] = {D[r, j]}"
+            checked += 1
+        # pointer doubling: every reachable vertex must lead to the source
+        Q = np.where(reach, P[r], s)
+        for _ in range(int(np.ceil(np.log2(max(n, 2)))) + 1):
+            Q = Q[Q]
+        assert np.all(Q[reach] == s), f"row {r}: predecessor chain does not reach the source"
+    return checked

@@ -15,11 +15,13 @@
 //
 // Usage:
 //   fap_ref --dir D -f NAME -k K -direct 0|1 -weight 0|1
-//           [--parts all|1,5,9] [--meta FILE] [--dist FILE] [--quiet]
+//           [--parts all|1,5,9] [--meta FILE] [--dist FILE] [--path FILE] [--quiet]
 //   The graph is read from D/graph/<kind>/NAME.mtx (the reference resolves the
 //   path relative to the working directory, fap/utils/readMatFile.h:43-51).
 //   --meta  writes the CSR, partition and renumbering (binary, see dump_meta).
 //   --dist  writes each solved part's s x n float block, in part order.
+//   --path  writes each solved part's s x n int32 predecessor block (the
+//           reference's run() always computes it), in part order.
 //   One JSON line per solved part goes to stdout with its wall time.
 //   FAP_PARTITION_FILE=<file of n int32 part ids, 0-based> replaces the METIS
 //   call by that partition (link-time wrap of METIS_PartGraphKway), so the
@@ -101,7 +103,7 @@ void dump_meta(fap::fapGraph &g, const char *path) {
 }  // namespace
 
 int main(int argc, char **argv) {
-  std::string dir = ".", name, parts = "all", meta, distf;
+  std::string dir = ".", name, parts = "all", meta, distf, pathf;
   int K = 0, directed = 0, weighted = 0;
   bool quiet = false;
   for (int i = 1; i < argc; i++) {
@@ -118,6 +120,7 @@ int main(int argc, char **argv) {
     else if (a == "--parts") parts = nxt();
     else if (a == "--meta") meta = nxt();
     else if (a == "--dist") distf = nxt();
+    else if (a == "--path") pathf = nxt();
     else if (a == "--quiet") quiet = true;
     else { fprintf(stderr, "unknown arg %s\n", a.c_str()); return 2; }
   }
@@ -127,6 +130,7 @@ int main(int argc, char **argv) {
   }
   if (!meta.empty() && meta[0] != '/') meta = std::string(getcwd(nullptr, 0)) + "/" + meta;
   if (!distf.empty() && distf[0] != '/') distf = std::string(getcwd(nullptr, 0)) + "/" + distf;
+  if (!pathf.empty() && pathf[0] != '/') pathf = std::string(getcwd(nullptr, 0)) + "/" + pathf;
   if (chdir(dir.c_str()) != 0) { perror(dir.c_str()); return 2; }
 
   // The reference prints a debug line on every min-plus call
@@ -151,10 +155,14 @@ int main(int argc, char **argv) {
     std::string tok;
     while (std::getline(ss, tok, ',')) todo.push_back(std::stoi(tok));
   }
-  FILE *df = nullptr;
+  FILE *df = nullptr, *pf = nullptr;
   if (!distf.empty()) {
     df = fopen(distf.c_str(), "wb");
     if (!df) { perror(distf.c_str()); return 2; }
+  }
+  if (!pathf.empty()) {
+    pf = fopen(pathf.c_str(), "wb");
+    if (!pf) { perror(pathf.c_str()); return 2; }
   }
   const int64_t n = g.num_vertexs;
   for (int p : todo) {
@@ -166,11 +174,13 @@ int main(int argc, char **argv) {
     g.run(dist.data(), path.data(), p);
     double b = now_s();
     if (df) put(df, dist.data(), dist.size());
+    if (pf) put(pf, path.data(), path.size());
     printf("{\"event\": \"part\", \"part\": %d, \"rows\": %lld, \"bdy\": %d, \"entries\": %lld, \"seconds\": %.6f}\n",
            p, (long long)s, g.C_BlockBdy_num[p], (long long)(s * n), b - a);
     fflush(stdout);
   }
   if (df) fclose(df);
+  if (pf) fclose(pf);
   std::cout.rdbuf(saved);
   return 0;
 }

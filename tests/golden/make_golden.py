@@ -9,7 +9,9 @@ Each case is a small seeded graph written as MatrixMarket; the reference's
 CPU path (fapGraph::run per part, driven by oracle/_ref/fap_ref) solves it
 and the fixture stores the graph text, the reference's partition and
 renumbering, and its distances (full matrix for small cases, per-row
-checksums plus sampled rows for the 64x64 grid).  Directed cases use a
+checksums plus sampled rows for the 64x64 grid) and, for the full cases,
+its predecessor matrix (row i, column j: the vertex before j on the
+reference's shortest path from row i's vertex; -1 unreachable).  Directed cases use a
 given contiguous partition (FAP_PARTITION_FILE), because the reference's
 METIS input for directed graphs is misaligned when a vertex has no edge.
 """
@@ -50,6 +52,16 @@ def disconnected():
                       integral=True, info={"kind": "disconnected"})
 
 
+def rgg_float(n, seed):
+    """Duplicate-free random geometric graph with float weights: shortest
+    paths are unique with probability one, so predecessors compare exactly."""
+    g = G.road_graph(n, seed=seed, target_avg_degree=2.6)
+    rng = np.random.default_rng(seed + 7)
+    g.weights = rng.uniform(0.5, 100.0, g.edges.shape[0]).astype(np.float32)
+    g.integral = False
+    return g
+
+
 def rmat_int(scale, m, seed):
     g = G.rmat_graph(scale, m, seed=seed)
     rng = np.random.default_rng(seed)
@@ -68,6 +80,7 @@ CASES = {
     "grid10_k1": (lambda: G.grid_graph(10, 10, seed=13, wmin=1, wmax=9), 1, "contig", True),
     "rmat8_int_k4": (lambda: rmat_int(8, 2048, 14), 4, "contig", True),
     "rmat8_f32_k4": (lambda: G.rmat_graph(8, 2048, seed=15), 4, "contig", True),
+    "rgg300_f32_k4": (lambda: rgg_float(300, 16), 4, None, True),
     "grid64_k8": (lambda: G.grid_graph(64, 64, drop_frac=0.02, seed=1), 8, None, False),
 }
 
@@ -85,8 +98,9 @@ def make_case(name, maker, K, partition, full, tmp):
         gid0.tofile(part_file)
     meta_f = os.path.join(tmp, name + ".meta")
     dist_f = os.path.join(tmp, name + ".dist")
+    path_f = os.path.join(tmp, name + ".path")
     ev = O.run_ref(root, name, g.directed, g.weighted, K, meta_out=meta_f, dist_out=dist_f,
-                   partition_file=part_file)
+                   path_out=path_f if full else None, partition_file=part_file)
     meta = O.read_meta(meta_f)
     dist = np.fromfile(dist_f, dtype=np.float32).reshape(meta.n, meta.n)
     out = dict(name=name, mtx=np.array(mtx_text), directed=g.directed, weighted=g.weighted,
@@ -97,6 +111,7 @@ def make_case(name, maker, K, partition, full, tmp):
                injected_partition=np.array(partition is not None))
     if full:
         out["dist"] = dist
+        out["path"] = np.fromfile(path_f, dtype=np.int32).reshape(meta.n, meta.n)
     else:
         out["row_checksums"] = O.row_checksums(O.to_i32(dist))
         rng = np.random.default_rng(0)

@@ -115,3 +115,58 @@ def test_port_matches_reference_binary(seed):
     out = O.port_solve_meta(meta)
     full = np.concatenate([out[p] for p in range(1, meta.K + 1)], 0)
     assert np.array_equal(full.view(np.int32), ref.view(np.int32))
+
+
+def _path_names():
+    return [n for n in golden_names() if "path" in load_golden(n)]
+
+
+def _duplicate_free(case):
+    ro, col = case["row_offset"], case["col_val"]
+    for u in range(int(case["n"])):
+        nb = col[ro[u]:ro[u + 1]].tolist()
+        if len(set(nb)) != len(nb) or u in nb:
+            return False
+    return True
+
+
+@pytest.mark.parametrize("name", _path_names())
+def test_predecessor_rule_matches_reference_paths(name):
+    """The predecessor rule of the B200 path (argmin over in-edges, smallest
+    vertex on ties), applied to the reference's distances, gives the
+    reference's own predecessor matrix on every entry whose predecessor is
+    unique (there every evaluation order must agree)."""
+    c = load_golden(name)
+    rows = c["st2ed"]
+    integral = bool(c["integral"])
+    P = O.port_predecessors(c["dist"], rows, c["row_offset"], c["col_val"], c["weight"], integral)
+    U = O.unique_predecessor_mask(c["dist"], rows, c["row_offset"], c["col_val"], c["weight"], integral)
+    assert U.sum() > 0
+    np.testing.assert_array_equal(P[U], c["path"][U])
+    # sources and unreachable entries agree everywhere
+    n = int(c["n"])
+    np.testing.assert_array_equal(P[np.arange(n), rows], c["path"][np.arange(n), rows])
+    unreach = c["dist"] >= 1e8
+    np.testing.assert_array_equal(P[unreach], c["path"][unreach])
+
+
+@pytest.mark.parametrize("name", [n for n in _path_names() if _duplicate_free(load_golden(n))])
+def test_reference_and_rule_paths_are_valid(name):
+    """On graphs without duplicate edges or self-loops (where the reference's
+    in-part distances are true shortest distances), both the reference's
+    predecessor matrix and the rule's pass the validity check."""
+    c = load_golden(name)
+    args = (c["st2ed"], c["row_offset"], c["col_val"], c["weight"], bool(c["integral"]))
+    assert O.check_paths(c["dist"], c["path"], *args) > 0
+    P = O.port_predecessors(c["dist"], *args)
+    assert O.check_paths(c["dist"], P, *args) > 0
+
+
+def test_check_paths_catches_a_planted_error():
+    c = load_golden("grid12_k4")
+    args = (c["st2ed"], c["row_offset"], c["col_val"], c["weight"], True)
+    P = c["path"].copy()
+    r, j = 5, int(np.nonzero(c["dist"][5] > 3)[0][0])
+    P[r, j] = c["st2ed"][r]          # the source is not adjacent to j
+    with pytest.raises(AssertionError):
+        O.check_paths(c["dist"], P, *args)
