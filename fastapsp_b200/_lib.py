@@ -77,6 +77,8 @@ _SIGS = {
     "fap_graph_block": (INT, [P, I32, PP, ctypes.POINTER(I64), ctypes.POINTER(I64)]),
     "fap_graph_copy_block": (INT, [P, I32, P, INT]),
     "fap_graph_block_checksums": (INT, [P, I32, P]),
+    "fap_graph_path_block": (INT, [P, I32, PP, ctypes.POINTER(I64), ctypes.POINTER(I64)]),
+    "fap_graph_copy_path_block": (INT, [P, I32, P]),
     "fap_graph_sssp_rows": (INT, [P, P, I32, P]),
     "fap_graph_set_param": (INT, [P, ctypes.c_char_p, DBL]),
     "fap_graph_last_timing": (INT, [P, P]),
@@ -133,6 +135,10 @@ _SIGS = {
     "fap_host_all_distance": (INT, [P, P]),
     "fap_host_distance_from_one_point": (INT, [P, INT, P]),
     "fap_host_distance_p2p": (INT, [P, INT, INT, ctypes.POINTER(ctypes.c_float)]),
+    "fap_host_subgraph_path": (INT, [P, INT, P]),
+    "fap_host_all_path": (INT, [P, P]),
+    "fap_host_path_from_one_point": (INT, [P, INT, P]),
+    "fap_host_path_p2p": (INT, [P, INT, INT, P, I32, ctypes.POINTER(I32)]),
     "fap_host_check_result": (INT, [P, INT, ctypes.POINTER(INT)]),
     "fap_host_device_graph": (P, [P]),
 }

@@ -180,6 +180,12 @@ struct fap_dgraph {
   // (cF, equal padded squares of side cache_ldf, part p at (p - 1)).
   bool cache_ready = false;
   bool use_cache = true;
+  // Predecessor matrices: P has D's shape; the in-edge CSR (tro/tcol/tw)
+  // is built when paths are switched on; path_ok[p]: p's resident block has
+  // its predecessor rows.
+  bool paths = false;
+  DevBuf P, d_tro, d_tcol, d_tw;
+  std::vector<char> path_ok;
   DevBuf cBd, cF, d_cparts, d_rowgroups, d_rowloc, d_rowout, d_rowidx;
   std::vector<int64_t> cb_off;
   std::vector<PartDesc> cparts;
@@ -379,7 +385,8 @@ extern "C" int fap_graph_destroy(fap_dgraph *G) {
     if (G->gexec) cudaGraphExecDestroy(G->gexec);
     for (DevBuf *b : {&G->ro, &G->col, &G->w, &G->ro_s, &G->col_s, &G->w_s, &G->sssp_scratch, &G->d_thin,
                       &G->d_gid, &G->d_st2ed, &G->d_ed2st, &G->D, &G->F, &G->d_parts, &G->d_work,
-                      &G->d_src, &G->d_srcrows, &G->d_status, &G->d_checks, &G->staging})
+                      &G->d_src, &G->d_srcrows, &G->d_status, &G->d_checks, &G->staging, &G->P,
+                      &G->d_tro, &G->d_tcol, &G->d_tw})
       b->release();
     cache_drop(G);
   }
@@ -465,6 +472,10 @@ extern "C" int fap_graph_reserve(fap_dgraph *G, int64_t max_rows) {
   if (G->D.bytes < bytes) {
     G->D.release();
     FAP_TRY(G->D.ensure(bytes));
+  }
+  if (G->paths && G->P.bytes < bytes) {
+    G->P.release();
+    FAP_TRY(G->P.ensure(bytes));
   }
   G->max_rows = max_rows;
   std::fill(G->row_base.begin(), G->row_base.end(), -1);
@@ -585,6 +596,15 @@ T sssp_delta_for(const fap_dgraph *G) {
   return (T)d;
 }
 
+// Predecessor rows of the batch's parts (after their distances).
+template <typename T>
+int launch_paths(fap_dgraph *G, const PartDesc *dp, int np, int max_s, int64_t *L) {
+  FAP_CK(launch_pred<T>(dp, np, max_s, G->D.as<const T>(), G->P.as<int32_t>(), G->ldD, G->n,
+                        G->d_tro.as<const int32_t>(), G->d_tcol.as<const int32_t>(), G->d_tw.as<const T>(),
+                        G->d_st2ed.as<const int32_t>(), G->ctx->stream, L));
+  return FAP_OK;
+}
+
 template <typename T>
 int run_solve(fap_dgraph *G, int mode) {
   fap_ctx *c = G->ctx;
@@ -622,6 +642,7 @@ int run_solve(fap_dgraph *G, int mode) {
                                   G->ldD, gid, ed2st, st, &L));
     FAP_CK(launch_minplus_parts<T>(dp, (int)G->K, dw, (int)G->work.size(), G->n, cF, G->cache_ldf, D,
                                    G->ldD, G->max_rows, gid, ed2st, status, st, &L));
+    if (G->paths) FAP_TRY(launch_paths<T>(G, dp, np, G->max_s, &L));
     FAP_CK(record_event(c->ev[4], st));
   } else if (mode == FAP_MODE_BATCHED) {
     FAP_CK(record_event(c->ev[0], st));
@@ -642,6 +663,7 @@ int run_solve(fap_dgraph *G, int mode) {
                                   G->ldD, gid, ed2st, st, &L));
     FAP_CK(launch_minplus_parts<T>(dp, np, dw, (int)G->work.size(), G->n, F, G->max_ldf, D, G->ldD,
                                    G->max_rows, gid, ed2st, status, st, &L));
+    if (G->paths) FAP_TRY(launch_paths<T>(G, dp, np, G->max_s, &L));
     FAP_CK(record_event(c->ev[4], st));
   } else {
     FAP_CK(record_event(c->ev[0], st));
@@ -660,6 +682,7 @@ int run_solve(fap_dgraph *G, int mode) {
       else
         FAP_CK(launch_minplus_parts<T>(dp, np, dw + w0, w1 - w0, G->n, F, G->max_ldf, D, G->ldD,
                                        G->max_rows, gid, ed2st, status, st, &L));
+      if (G->paths) FAP_TRY(launch_paths<T>(G, dp + i, 1, d.s, &L));
     }
     FAP_CK(record_event(c->ev[4], st));
   }
@@ -705,6 +728,12 @@ extern "C" int fap_solve(fap_dgraph *G, const int32_t *parts, int32_t count, int
   if (ids.empty()) return FAP_OK;
   DeviceGuard g(G->ctx->device);
   if (G->max_rows == 0) FAP_TRY(fap_graph_reserve(G, 0));
+  if (G->paths && G->P.bytes < (size_t)G->max_rows * G->ldD * 4) {
+    FAP_CK(cudaStreamSynchronize(G->ctx->stream));
+    G->P.release();
+    FAP_TRY(G->P.ensure((size_t)G->max_rows * G->ldD * 4));
+    G->epoch++;
+  }
   FAP_TRY(prepare_batch(G, ids, mode == FAP_MODE_BATCHED && G->cache_ready && G->use_cache));
   int rc = FAP_OK;
   cudaStream_t st = G->ctx->stream;
@@ -741,6 +770,9 @@ extern "C" int fap_solve(fap_dgraph *G, const int32_t *parts, int32_t count, int
     if (rc != FAP_OK) return rc;
   }
   for (const PartDesc &d : G->parts) G->row_base[d.part] = d.row_base;
+  G->path_ok.assign(G->K + 1, 0);
+  if (G->paths)
+    for (const PartDesc &d : G->parts) G->path_ok[d.part] = 1;
   G->last_mode = mode;
   return FAP_OK;
 }
@@ -812,6 +844,32 @@ extern "C" int fap_graph_copy_block(fap_dgraph *G, int32_t part, void *host, int
     return fail(FAP_ERR_INVALID, "cannot copy %s distances as int32",
                 G->dtype == FAP_DTYPE_F32 ? "float" : "?");
   }
+  FAP_CK(cudaStreamSynchronize(st));
+  FAP_TRY(read_status(G));
+  return FAP_OK;
+}
+
+extern "C" int fap_graph_path_block(fap_dgraph *G, int32_t part, void **dev_ptr, int64_t *rows,
+                                    int64_t *ld) {
+  if (!G || !dev_ptr || !rows || !ld) return fail(FAP_ERR_INVALID, "NULL argument");
+  void *dp;
+  FAP_TRY(fap_graph_block(G, part, &dp, rows, ld));
+  if ((int)G->path_ok.size() <= part || !G->path_ok[part])
+    return fail(FAP_ERR_STATE, "part %d was solved without paths", part);
+  *dev_ptr = G->P.as<char>() + (size_t)G->row_base[part] * G->ldD * 4;
+  return FAP_OK;
+}
+
+extern "C" int fap_graph_copy_path_block(fap_dgraph *G, int32_t part, int32_t *host) {
+  if (!G || !host) return fail(FAP_ERR_INVALID, "NULL argument");
+  void *dp;
+  int64_t rows, ld;
+  FAP_TRY(fap_graph_path_block(G, part, &dp, &rows, &ld));
+  if (rows == 0) return FAP_OK;
+  DeviceGuard g(G->ctx->device);
+  cudaStream_t st = G->ctx->stream;
+  FAP_CK(cudaMemcpy2DAsync(host, (size_t)G->n * 4, dp, (size_t)ld * 4, (size_t)G->n * 4, (size_t)rows,
+                           cudaMemcpyDeviceToHost, st));
   FAP_CK(cudaStreamSynchronize(st));
   FAP_TRY(read_status(G));
   return FAP_OK;
@@ -1050,6 +1108,53 @@ extern "C" int fap_graph_sssp_rows(fap_dgraph *G, const int32_t *sources, int32_
   return rc;
 }
 
+namespace {
+// Switches predecessor matrices on: checks that every weight is positive
+// (with zero-weight edges, equal distances would not order the
+// predecessors), then builds the in-edge CSR (sources ascending per vertex).
+int enable_paths(fap_dgraph *G) {
+  const int64_t m = (int64_t)G->h_col.size() < G->m ? (int64_t)G->h_col.size() : G->m;
+  for (int64_t e = 0; e < m; e++) {
+    uint32_t bits = G->h_w[e];
+    bool pos;
+    if (G->dtype == FAP_DTYPE_I32) {
+      int32_t v;
+      std::memcpy(&v, &bits, 4);
+      pos = v > 0;
+    } else {
+      float v;
+      std::memcpy(&v, &bits, 4);
+      pos = v > 0.0f;
+    }
+    if (!pos) return fail(FAP_ERR_RANGE, "paths need positive edge weights (edge %lld)", (long long)e);
+  }
+  if (G->d_tro.bytes == 0) {
+    const int32_t n = G->n;
+    std::vector<int32_t> tro((size_t)n + 1, 0), tcol((size_t)std::max<int64_t>(m, 1));
+    std::vector<uint32_t> tw((size_t)std::max<int64_t>(m, 1));
+    for (int64_t e = 0; e < m; e++) tro[(size_t)G->h_col[e] + 1]++;
+    for (int32_t j = 0; j < n; j++) tro[j + 1] += tro[j];
+    std::vector<int32_t> fill(tro.begin(), tro.end() - 1);
+    for (int32_t u = 0; u < n; u++)
+      for (int32_t e = G->h_ro[u]; e < G->h_ro[u + 1]; e++) {
+        const int32_t j = G->h_col[e];
+        tcol[fill[j]] = u;
+        tw[fill[j]] = G->h_w[e];
+        fill[j]++;
+      }
+    DeviceGuard g(G->ctx->device);
+    FAP_TRY(G->d_tro.ensure(tro.size() * 4));
+    FAP_TRY(G->d_tcol.ensure(tcol.size() * 4));
+    FAP_TRY(G->d_tw.ensure(tw.size() * 4));
+    FAP_CK(cudaMemcpy(G->d_tro.p, tro.data(), tro.size() * 4, cudaMemcpyHostToDevice));
+    FAP_CK(cudaMemcpy(G->d_tcol.p, tcol.data(), tcol.size() * 4, cudaMemcpyHostToDevice));
+    FAP_CK(cudaMemcpy(G->d_tw.p, tw.data(), tw.size() * 4, cudaMemcpyHostToDevice));
+  }
+  G->paths = true;
+  return FAP_OK;
+}
+}  // namespace
+
 extern "C" int fap_graph_set_param(fap_dgraph *G, const char *key, double value) {
   if (!G || !key) return fail(FAP_ERR_INVALID, "NULL argument");
   G->epoch++;  // a captured launch sequence no longer matches
@@ -1068,6 +1173,13 @@ extern "C" int fap_graph_set_param(fap_dgraph *G, const char *key, double value)
   if (std::strcmp(key, "sssp_chain") == 0) {
     G->sssp_chain = value >= 0 ? (int)value : 0;
     return FAP_OK;
+  }
+  if (std::strcmp(key, "paths") == 0) {
+    if (value == 0.0) {
+      G->paths = false;
+      return FAP_OK;
+    }
+    return enable_paths(G);
   }
   if (std::strcmp(key, "use_cache") == 0) {
     G->use_cache = value != 0.0;
@@ -1174,6 +1286,7 @@ extern "C" int fap_graph_release(fap_dgraph *G) {
   G->sssp_scratch.release();
   G->staging.release();
   G->d_checks.release();
+  G->P.release();
   G->max_rows = 0;
   std::fill(G->row_base.begin(), G->row_base.end(), -1);
   G->last_ids.clear();
@@ -1188,7 +1301,7 @@ extern "C" int fap_graph_device_bytes(const fap_dgraph *G, int64_t *bytes) {
                           &G->d_thin, &G->d_gid, &G->d_st2ed, &G->d_ed2st, &G->D, &G->F, &G->d_parts,
                           &G->d_work, &G->d_src, &G->d_srcrows, &G->d_status, &G->d_checks, &G->staging,
                           &G->cBd, &G->cF, &G->d_cparts, &G->d_rowgroups, &G->d_rowloc, &G->d_rowout,
-                          &G->d_rowidx})
+                          &G->d_rowidx, &G->P, &G->d_tro, &G->d_tcol, &G->d_tw})
     t += (int64_t)b->bytes;
   *bytes = t;
   return FAP_OK;

@@ -718,6 +718,74 @@ cudaError_t launch_minplus_thin(const PartDesc *parts, const int32_t *thin_parts
 }
 
 // ---------------------------------------------------------------------------
+// Predecessor (path) matrices
+// ---------------------------------------------------------------------------
+// P[row][j] for the batch's output rows: the in-neighbour u of j with the
+// least D[row][u] + w(u, j), the smallest u among equal sums; the row's own
+// vertex maps to itself and unreachable entries to -1.  That is the Bellman
+// condition on the final distances, so with positive weights following P
+// from any reachable j walks a shortest path back to the source.  The
+// reference keeps whichever predecessor its Dijkstra / Floyd / min-plus
+// evaluation order finds (fap/kernel/batch_sssp.h:108-110,
+// fap/kernel/floyd.h:38-49, fap/kernel/minplus.h:51-65); both agree wherever
+// the predecessor is unique.
+// grid (column chunks, batch parts, row chunks of kPredRows): consecutive
+// CTAs share their rows, which stay in L2 for the gathers D[row][u]; the
+// in-edge list of a column is read once per CTA for all of its rows.
+constexpr int kPredRows = 8;
+constexpr int kPredThreads = 256;
+
+template <typename T>
+__global__ void __launch_bounds__(kPredThreads)
+    pred_kernel(const PartDesc *__restrict__ parts, const T *__restrict__ D, int32_t *__restrict__ P,
+                int64_t ldD, int n, const int32_t *__restrict__ tro, const int32_t *__restrict__ tcol,
+                const T *__restrict__ tw, const int32_t *__restrict__ st2ed) {
+  const PartDesc pd = parts[blockIdx.y];
+  const int r0 = blockIdx.z * kPredRows;
+  if (r0 >= pd.s) return;
+  const int rows = min(kPredRows, pd.s - r0);
+  const T inf = Dist<T>::inf();
+  const int j = blockIdx.x * kPredThreads + threadIdx.x;
+  if (j >= n) return;
+  const int e0 = __ldg(tro + j), e1 = __ldg(tro + j + 1);
+  for (int rr = 0; rr < rows; rr++) {
+    const int64_t row = pd.row_base + r0 + rr;
+    const T *Dr = D + row * ldD;
+    const int src = __ldg(st2ed + pd.start + r0 + rr);
+    int pred = -1;
+    if (j == src) {
+      pred = src;
+    } else if (Dr[j] < inf) {
+      T best = Dist<T>::inf();
+      bool any = false;
+      for (int e = e0; e < e1; e++) {
+        const int u = __ldg(tcol + e);
+        const T du = Dr[u];
+        if (du >= inf) continue;
+        const T v = du + __ldg(tw + e);
+        if (!any || v < best || (v == best && u < pred)) {
+          best = v;
+          pred = u;
+          any = true;
+        }
+      }
+    }
+    P[row * ldD + j] = pred;
+  }
+}
+
+template <typename T>
+cudaError_t launch_pred(const PartDesc *parts, int nparts, int max_s, const T *D, int32_t *P,
+                        int64_t ldD, int n, const int32_t *tro, const int32_t *tcol, const T *tw,
+                        const int32_t *st2ed, cudaStream_t stream, int64_t *launches) {
+  if (nparts <= 0 || max_s <= 0 || n <= 0) return cudaSuccess;
+  dim3 grid((unsigned)ceil_div(n, kPredThreads), (unsigned)nparts, (unsigned)ceil_div(max_s, kPredRows));
+  pred_kernel<T><<<grid, kPredThreads, 0, stream>>>(parts, D, P, ldD, n, tro, tcol, tw, st2ed);
+  *launches += 1;
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 // Resident cache kernels
 // ---------------------------------------------------------------------------
 template <typename T>
@@ -1048,6 +1116,9 @@ cudaError_t launch_relax_peak(T *sink, int blocks, int iters, cudaStream_t strea
   template cudaError_t launch_minplus_generic<T>(int, int, int, const T *, int64_t, const T *,    \
                                                  int64_t, T *, int64_t, cudaStream_t, int64_t *); \
   template cudaError_t launch_fill<T>(T *, int64_t, int64_t, int64_t, T, cudaStream_t, int64_t *); \
+  template cudaError_t launch_pred<T>(const PartDesc *, int, int, const T *, int32_t *, int64_t,  \
+                                      int, const int32_t *, const int32_t *, const T *,            \
+                                      const int32_t *, cudaStream_t, int64_t *);                   \
   template cudaError_t launch_bdy_copy<T>(const PartDesc *, int, int, const T *, T *, int64_t,    \
                                           cudaStream_t, int64_t *);                               \
   template cudaError_t launch_row_gather<T>(const T *, int64_t, const int64_t *, int64_t, int, T *, \

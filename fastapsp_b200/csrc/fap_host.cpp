@@ -341,17 +341,31 @@ void fapGraph::copy_block(int32_t id, float *dst) {
   check(fap_graph_copy_block(dg_, id, dst, FAP_DTYPE_F32), "fap_graph_copy_block");
 }
 
+void fapGraph::copy_path_block(int32_t id, int32_t *dst) {
+  check(fap_graph_copy_path_block(dg_, id, dst), "fap_graph_copy_path_block");
+}
+
+void fapGraph::set_paths(bool on) {
+  check(fap_graph_set_param(dg_, "paths", on ? 1.0 : 0.0), "paths");
+}
+
 int32_t fapGraph::solve(bool path_needed) {
   if (!prepared_) raise(FAP_ERR_STATE, "solve before preCondition");
   is_path_needed = path_needed;
   ensure_device();
+  set_paths(path_needed);
   const int64_t n = num_vertexs;
   dist.assign((size_t)(n * n), 0.0f);
   path.assign((size_t)(n * n), -1);
+  path_ready_ = false;
   std::vector<int32_t> all;
   for (int32_t p = 1; p <= K; p++) all.push_back(p);
   run_parts(all);
-  for (int32_t p = 1; p <= K; p++) copy_block(p, dist.data() + (size_t)C_BlockVer_offset[p] * n);
+  for (int32_t p = 1; p <= K; p++) {
+    copy_block(p, dist.data() + (size_t)C_BlockVer_offset[p] * n);
+    if (path_needed) copy_path_block(p, path.data() + (size_t)C_BlockVer_offset[p] * n);
+  }
+  path_ready_ = path_needed;
   return 0;
 }
 
@@ -360,13 +374,15 @@ int32_t fapGraph::solveSubGraph(int32_t id, bool path_needed) {
   if (id < 1 || id > K) return -1;
   is_path_needed = path_needed;
   ensure_device();
+  if (path_needed) set_paths(true);
   const int64_t n = num_vertexs;
   void *dp;
   int64_t rows, ld;
   if (mode_ == SolveMode::Plain) {
     // Plain form: every call solves its part with its own launch sequence.
     run_parts({id});
-  } else if (fap_graph_block(dg_, id, &dp, &rows, &ld) != FAP_OK) {
+  } else if (fap_graph_block(dg_, id, &dp, &rows, &ld) != FAP_OK ||
+             (path_needed && fap_graph_path_block(dg_, id, &dp, &rows, &ld) != FAP_OK)) {
     // Batched form: solve every part once (blocks stay resident in HBM);
     // later calls only copy.  Without room for every block, solve this part.
     std::vector<int32_t> all;
@@ -381,6 +397,7 @@ int32_t fapGraph::solveSubGraph(int32_t id, bool path_needed) {
   subgraph_path.assign((size_t)C_BlockVer_num[id] * n, -1);
   current_subgraph_id = id;
   copy_block(id, subgraph_dist.data());
+  if (path_needed) copy_path_block(id, subgraph_path.data());
   return 0;
 }
 
@@ -443,10 +460,31 @@ float fapGraph::getDistanceP2P(int32_t from, int32_t to) {
   return subgraph_dist[(size_t)row * n + to];
 }
 
+// The vertices of a shortest path from `from` to `to` (both included), read
+// off the predecessor row of `from`; empty when `to` is unreachable.  The
+// reference leaves this a TODO (fap/fap.cpp:263-269).
 std::vector<int32_t> fapGraph::getPathP2P(int32_t from, int32_t to) {
-  raise(FAP_ERR_STATE, "paths are not computed by this build (distances only)");
-  (void)from;
-  (void)to;
+  if (from < 0 || from >= num_vertexs || to < 0 || to >= num_vertexs)
+    raise(FAP_ERR_INVALID, "vertex out of range");
+  const int64_t n = num_vertexs;
+  const int32_t *row = nullptr;
+  if (path_ready_) {
+    row = path.data() + (size_t)ed2st[from] * n;
+  } else {
+    if (graph_id[from] != current_subgraph_id || !is_path_needed) solveSubGraph(graph_id[from], true);
+    row = subgraph_path.data() + (size_t)(ed2st[from] - C_BlockVer_offset[current_subgraph_id]) * n;
+  }
+  std::vector<int32_t> out;
+  int32_t cur = to;
+  out.push_back(cur);
+  while (cur != from) {
+    cur = row[cur];
+    if (cur < 0) return {};
+    out.push_back(cur);
+    if ((int64_t)out.size() > n) raise(FAP_ERR_STATE, "predecessor chain does not end at the source");
+  }
+  std::reverse(out.begin(), out.end());
+  return out;
 }
 
 bool fapGraph::check_result(float *d, int *p, int *source, int source_num, int vertexs, int *,
@@ -625,6 +663,36 @@ int fap_host_distance_from_one_point(fap::fapGraph *g, int v, float *out) {
 
 int fap_host_distance_p2p(fap::fapGraph *g, int from, int to, float *out) {
   FAPH_BODY(*out = g->getDistanceP2P(from, to))
+}
+
+int fap_host_subgraph_path(fap::fapGraph *g, int id, int32_t *out) {
+  FAPH_BODY({
+    auto v = g->getSubGraphPath(id);
+    std::memcpy(out, v.data(), v.size() * sizeof(int32_t));
+  })
+}
+
+int fap_host_all_path(fap::fapGraph *g, int32_t *out) {
+  FAPH_BODY({
+    auto v = g->getAllPath();
+    std::memcpy(out, v.data(), v.size() * sizeof(int32_t));
+  })
+}
+
+int fap_host_path_from_one_point(fap::fapGraph *g, int v, int32_t *out) {
+  FAPH_BODY({
+    auto r = g->getPathFromOnePoint(v);
+    std::memcpy(out, r.data(), r.size() * sizeof(int32_t));
+  })
+}
+
+int fap_host_path_p2p(fap::fapGraph *g, int from, int to, int32_t *out, int32_t cap, int32_t *len) {
+  FAPH_BODY({
+    auto r = g->getPathP2P(from, to);
+    *len = (int32_t)r.size();
+    if ((int32_t)r.size() > cap) throw fap::fapError(FAP_ERR_INVALID, "output buffer too small");
+    std::memcpy(out, r.data(), r.size() * sizeof(int32_t));
+  })
 }
 
 int fap_host_check_result(fap::fapGraph *g, int id, int *ok) {

@@ -109,6 +109,15 @@ cudaError_t launch_minplus_thin(const PartDesc *parts, const int32_t *thin_parts
                                 int n, const T *F, T *D, int64_t ldD, const int32_t *graph_id,
                                 const int32_t *ed2st, cudaStream_t stream, int64_t *launches);
 
+// Predecessor rows of the listed parts' output rows: P[row][j] = the
+// in-neighbour u of j (in-edge CSR tro/tcol/tw) with the least D[row][u] +
+// w(u, j), the smallest u on ties; the row's vertex maps to itself, an
+// unreachable j to -1.  max_s bounds the parts' sizes.
+template <typename T>
+cudaError_t launch_pred(const PartDesc *parts, int nparts, int max_s, const T *D, int32_t *P,
+                        int64_t ldD, int n, const int32_t *tro, const int32_t *tcol, const T *tw,
+                        const int32_t *st2ed, cudaStream_t stream, int64_t *launches);
+
 // Resident cache: copy each listed part's boundary rows Bd[bd_row + i] into
 // D[row_base + i] (all ldD columns).
 template <typename T>

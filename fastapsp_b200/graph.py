@@ -233,6 +233,33 @@ class fapGraph:
               "getDistanceP2P")
         return float(x.value)
 
+    # ---- predecessor (path) matrices: solve(..., is_path_needed=True) ----
+    def getAllPath(self) -> np.ndarray:
+        n = self.num_vertexs
+        out = np.empty((n, n), np.int32)
+        check(lib().fap_host_all_path(self._h, ptr(out)), "getAllPath")
+        return out
+
+    def getSubGraphPath(self, sub_graph_id: int) -> np.ndarray:
+        vn, _, _ = self.partInfo()
+        out = np.empty((int(vn[sub_graph_id]), self.num_vertexs), np.int32)
+        check(lib().fap_host_subgraph_path(self._h, int(sub_graph_id), ptr(out)), "getSubGraphPath")
+        return out
+
+    def getPathFromOnePoint(self, vertex_id: int) -> np.ndarray:
+        out = np.empty(self.num_vertexs, np.int32)
+        check(lib().fap_host_path_from_one_point(self._h, int(vertex_id), ptr(out)),
+              "getPathFromOnePoint")
+        return out
+
+    def getPathP2P(self, u: int, v: int) -> list:
+        """Vertices of a shortest path u .. v (inclusive); [] if unreachable."""
+        out = np.empty(self.num_vertexs + 1, np.int32)
+        ln = ctypes.c_int32()
+        check(lib().fap_host_path_p2p(self._h, int(u), int(v), ptr(out), int(out.shape[0]),
+                                      ctypes.byref(ln)), "getPathP2P")
+        return out[:ln.value].tolist()
+
     def check_result(self, sub_graph_id: Optional[int] = None) -> bool:
         """Sampled self-check of the current part (fap/utils/checkResult.h:38-82)."""
         pid = self.getCurrentSubGraphId() if sub_graph_id is None else int(sub_graph_id)
@@ -398,6 +425,13 @@ class DeviceGraph:
             out = np.empty((rows, self.n), np.int32 if dt == L.FAP_DTYPE_I32 else np.float32)
         check(lib().fap_graph_copy_block(self._h, int(part), ptr(out), int(dt)),
               "fap_graph_copy_block")
+        return out
+
+    def copy_path_block(self, part: int) -> np.ndarray:
+        """rows x n int32 predecessors of a part solved with set_param("paths", 1)."""
+        _, rows, _ = self.block_info(part)
+        out = np.empty((rows, self.n), np.int32)
+        check(lib().fap_graph_copy_path_block(self._h, int(part), ptr(out)), "copy_path_block")
         return out
 
     def block_checksums(self, part: int) -> np.ndarray:

@@ -83,8 +83,12 @@ class __attribute__((visibility("default"))) fapGraph {
 
   void init_storage();
   void ensure_device();
+  bool path_ready_ = false;  // `path` holds every part's predecessors
+
   void run_parts(const std::vector<int32_t> &ids);
   void copy_block(int32_t id, float *dst);
+  void copy_path_block(int32_t id, int32_t *dst);
+  void set_paths(bool on);
 
  public:
   int32_t num_vertexs = 0;

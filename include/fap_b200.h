@@ -146,7 +146,9 @@ FAP_API int fap_graph_sssp_rows(fap_dgraph *g, const int32_t *sources, int32_t c
  * a batched solve captures its launch sequence in a CUDA graph on first use
  * and replays it while the batch, buffers, parameters and stream are
  * unchanged); "use_cache" (non-zero, the default: batched solves and
- * fap_graph_rows_async use the resident cache once it is built). */
+ * fap_graph_rows_async use the resident cache once it is built); "paths"
+ * (non-zero: later solves also produce the parts' predecessor rows, see
+ * fap_graph_path_block; needs every edge weight > 0, else FAP_ERR_RANGE). */
 FAP_API int fap_graph_set_param(fap_dgraph *g, const char *key, double value);
 
 /* Tunes the SSSP bucket width: runs the SSSP stage on `sample` boundary
@@ -172,6 +174,19 @@ FAP_API int fap_graph_resident(fap_dgraph *g, int32_t part);
  * (host ids) into d_out (device, count x n floats, dense); returns without
  * waiting.  Device errors surface in fap_graph_check. */
 FAP_API int fap_graph_rows_async(fap_dgraph *g, const int32_t *sources, int32_t count, float *d_out);
+
+/* Predecessor rows of a resident part solved with "paths" on (the
+ * reference's subgraph_path, fap/fap.cpp:92-181, is_path_needed): entry
+ * (r, j) is the vertex before j on a shortest path from the part's r-th
+ * vertex (sorted order), the vertex itself at j = source, -1 when j is
+ * unreachable.  Among several shortest paths the one kept is fixed: the
+ * in-neighbour u of j with the least dist(r, u) + w(u, j), the smallest u on
+ * equal sums (the reference keeps the first its evaluation order finds; the
+ * two agree wherever the predecessor is unique).  Same layout as
+ * fap_graph_block: int32, rows x ld, ld = ldD. */
+FAP_API int fap_graph_path_block(fap_dgraph *g, int32_t part, void **dev_ptr, int64_t *rows, int64_t *ld);
+/* rows x n int32 predecessors of the part into host memory. */
+FAP_API int fap_graph_copy_path_block(fap_dgraph *g, int32_t part, int32_t *host);
 
 /* Asynchronous forms for pipelines that must not block: queue, on the
  * context stream, the per-row checksums of a resident part's block into

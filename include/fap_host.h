@@ -65,6 +65,15 @@ FAP_API int fap_host_all_distance(fap_host_graph *g, float *out);
 /* out: n floats (vertex v must be in the current part) */
 FAP_API int fap_host_distance_from_one_point(fap_host_graph *g, int v, float *out);
 FAP_API int fap_host_distance_p2p(fap_host_graph *g, int from, int to, float *out);
+/* Predecessors (solved with path_needed): out ver_num[id] x n / n x n / n
+ * int32 (see fap_graph_path_block for their meaning). */
+FAP_API int fap_host_subgraph_path(fap_host_graph *g, int id, int32_t *out);
+FAP_API int fap_host_all_path(fap_host_graph *g, int32_t *out);
+FAP_API int fap_host_path_from_one_point(fap_host_graph *g, int v, int32_t *out);
+/* Vertices of a shortest path from..to (inclusive) into out[cap]; *len = its
+ * length, 0 when `to` is unreachable (no counterpart: a TODO in the
+ * reference, fap/fap.cpp:263-269). */
+FAP_API int fap_host_path_p2p(fap_host_graph *g, int from, int to, int32_t *out, int32_t cap, int32_t *len);
 /* Sampled self-check of part id's block against fresh GPU SSSP rows. */
 FAP_API int fap_host_check_result(fap_host_graph *g, int id, int *ok);
 /* The device-resident graph behind g (NULL before the first solve). */
