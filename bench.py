@@ -54,6 +54,8 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-procs", type=int, default=0, help="0 = min(cores, memory bound)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-stream measurement")
+    ap.add_argument("--paths", action="store_true",
+                    help="also time batched solves that produce predecessor matrices")
     ap.add_argument("--serve-graphs", type=int, default=32)
     ap.add_argument("--serve-burst", type=int, default=256,
                     help="requests of the closed-loop burst that measures capacity")
@@ -471,6 +473,33 @@ def main_fap(args):
     log(f"batched: {ms_per_step:.3f} ms/step, stages {np.round(st, 3).tolist()}, "
         f"{value:.4g} entries/s")
 
+    # ---- batched with predecessor matrices (optional) ----
+    paths = None
+    if args.paths:
+        try:
+            dg.set_param("paths", 1)
+            dg.solve(groups[0], FAP_MODE_BATCHED, check_errors=True)   # allocates P
+            p_ms = []
+            for _ in range(max(2, args.steps // 2)):
+                flush.zero_()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                solve_all(FAP_MODE_BATCHED)
+                e1.record(stream)
+                e1.synchronize()
+                p_ms.append(e0.elapsed_time(e1))
+            dg.check()
+            pm = allmax(float(np.sum(p_ms))) / len(p_ms)
+            paths = {"ms_per_step": pm, "pred_ms": pm - ms_per_step,
+                     "entries_s": total_entries / (pm * 1e-3),
+                     "note": "distances + predecessor rows (int32, same shape) per step"}
+            log(f"paths: {pm:.3f} ms/step (+{pm - ms_per_step:.3f} ms for predecessors)")
+        except Exception as e:  # noqa: BLE001 - reported, not fatal
+            paths = {"unavailable": str(e)[:200]}
+            log(f"paths: {e}")
+        dg.set_param("paths", 0)
+
     # ---- plain form ----
     plain_ms = []
     for i in range(1 + args.plain_steps if args.plain_steps > 0 else 0):
@@ -607,6 +636,7 @@ def main_fap(args):
             "gpu_launches": int(launches),
             "clocks": clk,
             "serving": serving,
+            "paths": paths,
         }
         emit(line)
     if world > 1:

@@ -732,45 +732,86 @@ cudaError_t launch_minplus_thin(const PartDesc *parts, const int32_t *thin_parts
 // grid (column chunks, batch parts, row chunks of kPredRows): consecutive
 // CTAs share their rows, which stay in L2 for the gathers D[row][u]; the
 // in-edge list of a column is read once per CTA for all of its rows.
-constexpr int kPredRows = 8;
+constexpr int kPredRows = 32;
 constexpr int kPredThreads = 256;
+constexpr int kPredDeg = 4;  // in-edges kept in registers (more are read in a loop)
+
+// A candidate predecessor as one 64-bit key: the sum dist(u) + w in the
+// high word (non-negative int32 and float32 values order like their bit
+// patterns), u in the low word, so that the least key is the least sum and,
+// among equal sums, the smallest u.  Unreachable u: the largest key.
+template <typename T>
+__device__ __forceinline__ uint64_t pred_key(T du, int u, T w, T inf) {
+  const T v = du + w;
+  uint32_t bits;
+  if constexpr (sizeof(T) == 4 && Dist<T>::kDtype == FAP_DTYPE_F32) bits = __float_as_uint((float)v);
+  else bits = (uint32_t)v;
+  return du < inf ? ((uint64_t)bits << 32) | (uint32_t)u : ~0ull;
+}
+
+// Rows are taken kPredUnroll at a time, and every load of a group (the
+// entry itself and the gathers of its in-neighbours' distances) is issued
+// before any is used, so a thread keeps up to kPredUnroll * (kPredDeg + 1)
+// loads in flight instead of waiting on each row in turn.
+constexpr int kPredUnroll = 4;
 
 template <typename T>
 __global__ void __launch_bounds__(kPredThreads)
     pred_kernel(const PartDesc *__restrict__ parts, const T *__restrict__ D, int32_t *__restrict__ P,
                 int64_t ldD, int n, const int32_t *__restrict__ tro, const int32_t *__restrict__ tcol,
                 const T *__restrict__ tw, const int32_t *__restrict__ st2ed) {
+  __shared__ int32_t src_s[kPredRows];
   const PartDesc pd = parts[blockIdx.y];
   const int r0 = blockIdx.z * kPredRows;
   if (r0 >= pd.s) return;
   const int rows = min(kPredRows, pd.s - r0);
+  if (threadIdx.x < rows) src_s[threadIdx.x] = __ldg(st2ed + pd.start + r0 + threadIdx.x);
+  __syncthreads();
   const T inf = Dist<T>::inf();
   const int j = blockIdx.x * kPredThreads + threadIdx.x;
   if (j >= n) return;
+  // the column's in-edges, read once for all of the CTA's rows
   const int e0 = __ldg(tro + j), e1 = __ldg(tro + j + 1);
-  for (int rr = 0; rr < rows; rr++) {
-    const int64_t row = pd.row_base + r0 + rr;
-    const T *Dr = D + row * ldD;
-    const int src = __ldg(st2ed + pd.start + r0 + rr);
-    int pred = -1;
-    if (j == src) {
-      pred = src;
-    } else if (Dr[j] < inf) {
-      T best = Dist<T>::inf();
-      bool any = false;
-      for (int e = e0; e < e1; e++) {
-        const int u = __ldg(tcol + e);
-        const T du = Dr[u];
-        if (du >= inf) continue;
-        const T v = du + __ldg(tw + e);
-        if (!any || v < best || (v == best && u < pred)) {
-          best = v;
-          pred = u;
-          any = true;
+  const int dk = min(e1 - e0, kPredDeg);
+  int us[kPredDeg];
+  T ws[kPredDeg];
+#pragma unroll
+  for (int k = 0; k < kPredDeg; k++) {
+    us[k] = k < dk ? __ldg(tcol + e0 + k) : j;
+    ws[k] = k < dk ? __ldg(tw + e0 + k) : T(0);
+  }
+  const T *Dr = D + (pd.row_base + r0) * ldD;
+  int32_t *Pr = P + (pd.row_base + r0) * ldD + j;
+  for (int rr = 0; rr < rows; rr += kPredUnroll, Dr += kPredUnroll * ldD, Pr += kPredUnroll * ldD) {
+    T dj[kPredUnroll], g[kPredUnroll][kPredDeg];
+#pragma unroll
+    for (int q = 0; q < kPredUnroll; q++) {
+      const bool live = rr + q < rows;
+      const T *Dq = Dr + (int64_t)q * ldD;
+      dj[q] = live ? __ldg(Dq + j) : inf;
+#pragma unroll
+      for (int k = 0; k < kPredDeg; k++) g[q][k] = (live && k < dk) ? __ldg(Dq + us[k]) : inf;
+    }
+#pragma unroll
+    for (int q = 0; q < kPredUnroll; q++) {
+      if (rr + q >= rows) break;
+      const int src = src_s[rr + q];
+      uint64_t best = ~0ull;
+#pragma unroll
+      for (int k = 0; k < kPredDeg; k++)
+        if (k < dk) best = min(best, pred_key<T>(g[q][k], us[k], ws[k], inf));
+      if (e1 - e0 > kPredDeg) {
+        const T *Dq = Dr + (int64_t)q * ldD;
+        for (int e = e0 + kPredDeg; e < e1; e++) {
+          const int u = __ldg(tcol + e);
+          best = min(best, pred_key<T>(__ldg(Dq + u), u, __ldg(tw + e), inf));
         }
       }
+      int pred = best == ~0ull ? -1 : (int)(uint32_t)best;
+      if (dj[q] >= inf) pred = -1;
+      if (j == src) pred = src;
+      Pr[(int64_t)q * ldD] = pred;
     }
-    P[row * ldD + j] = pred;
   }
 }
 
