@@ -83,6 +83,7 @@ _SIGS = {
     "fap_graph_set_param": (INT, [P, ctypes.c_char_p, DBL]),
     "fap_graph_last_timing": (INT, [P, P]),
     "fap_graph_last_launches": (INT, [P, ctypes.POINTER(I64)]),
+    "fap_graph_last_stage1": (INT, [P]),
     "fap_op_sssp": (INT, [P, INT, I32, I64, P, P, P, P, I32, P, I64]),
     "fap_op_floyd": (INT, [P, INT, I32, P, I64]),
     "fap_op_minplus": (INT, [P, INT, I32, I32, I32, P, I64, P, I64, P, I64]),

@@ -180,6 +180,18 @@ struct fap_dgraph {
   // (cF, equal padded squares of side cache_ldf, part p at (p - 1)).
   bool cache_ready = false;
   bool use_cache = true;
+  // Boundary-graph form of stage 1 (see launch_bgraph): applicable when no
+  // two arcs join the same ordered pair inside a part (the reference's
+  // matrix build keeps the last of such duplicates, which the local closure
+  // would not reproduce); boff = prefix sums of the boundary counts.
+  int stage1 = 0;  // 0 auto, 1 SSSP, 2 boundary graph whenever applicable
+  bool bnd_dupfree = false;
+  int64_t total_b = 0;
+  std::vector<int32_t> boff;
+  bool last_bmethod = false;   // the prepared batch uses it
+  bool cache_bmethod = false;  // the resident cache was built with it
+  int64_t ldB = 0;
+  DevBuf d_dB, d_bpart, d_brows, d_FB;
   // Predecessor matrices: P has D's shape; the in-edge CSR (tro/tcol/tw)
   // is built when paths are switched on; path_ok[p]: p's resident block has
   // its predecessor rows.
@@ -386,7 +398,7 @@ extern "C" int fap_graph_destroy(fap_dgraph *G) {
     for (DevBuf *b : {&G->ro, &G->col, &G->w, &G->ro_s, &G->col_s, &G->w_s, &G->sssp_scratch, &G->d_thin,
                       &G->d_gid, &G->d_st2ed, &G->d_ed2st, &G->D, &G->F, &G->d_parts, &G->d_work,
                       &G->d_src, &G->d_srcrows, &G->d_status, &G->d_checks, &G->staging, &G->P,
-                      &G->d_tro, &G->d_tcol, &G->d_tw})
+                      &G->d_tro, &G->d_tcol, &G->d_tw, &G->d_dB, &G->d_bpart, &G->d_brows, &G->d_FB})
       b->release();
     cache_drop(G);
   }
@@ -431,6 +443,24 @@ extern "C" int fap_graph_set_parts(fap_dgraph *G, int32_t K, const int32_t *grap
   G->vnum.assign(ver_num, ver_num + K + 1);
   G->voff.assign(ver_offset, ver_offset + K + 1);
   G->bnum.assign(bdy_num, bdy_num + K + 1);
+  G->boff.assign(K + 2, 0);
+  for (int32_t p = 1; p <= K; p++) G->boff[p + 1] = G->boff[p] + bdy_num[p];
+  G->total_b = G->boff[K + 1];
+  {
+    // duplicate arcs inside a part?
+    G->bnd_dupfree = true;
+    std::vector<int32_t> seen((size_t)n, -1);
+    for (int32_t u = 0; u < n && G->bnd_dupfree; u++)
+      for (int32_t e = G->h_ro[u]; e < G->h_ro[u + 1]; e++) {
+        const int32_t v = G->h_col[e];
+        if (graph_id[v] != graph_id[u]) continue;
+        if (seen[v] == u) {
+          G->bnd_dupfree = false;
+          break;
+        }
+        seen[v] = u;
+      }
+  }
   G->row_base.assign(K + 1, -1);
   G->last_ids.clear();
   cache_drop(G);
@@ -486,9 +516,49 @@ extern "C" int fap_graph_reserve(fap_dgraph *G, int64_t max_rows) {
 
 namespace {
 
+// Whether the boundary-graph form of stage 1 applies to g.
+// Automatic choice: int32 distances only (there both forms give the exact
+// shortest distances bit for bit; float32 sums would round in a different
+// order, a few ulps), at most 8192 boundary vertices.
+bool bmethod_ok(const fap_dgraph *G) {
+  if (G->stage1 == 1 || !G->bnd_dupfree || G->total_b <= 0) return false;
+  if (G->stage1 == 2) return true;
+  return G->dtype == FAP_DTYPE_I32 && G->total_b <= 8192;
+}
+
+// Per-part table, output-row list and dB for a batch of all parts in the
+// boundary-graph form (descriptors built, F offsets final).
+int prepare_bgraph(fap_dgraph *G, const std::vector<PartDesc> &parts) {
+  const int32_t K = G->K;
+  std::vector<BPart> bp((size_t)K + 1);
+  std::vector<int64_t> rows;
+  for (const PartDesc &d : parts) {
+    BPart &b = bp[d.part];
+    b.voff = d.start;
+    b.b = d.b;
+    b.boff = G->boff[d.part];
+    b.ldf = d.ldf;
+    b.f_off = d.f_off;
+    for (int32_t k = 0; k < d.b; k++) {
+      rows.push_back(G->boff[d.part] + k);
+      rows.push_back(d.row_base + k);
+    }
+  }
+  G->ldB = round_up(std::max<int64_t>(G->total_b, 1), kFloydTile);
+  FAP_TRY(G->d_dB.ensure((size_t)G->ldB * G->ldB * 4));
+  const int64_t ldFB = parts.empty() ? kFloydTile : parts[0].ldf;
+  FAP_TRY(G->d_FB.ensure((size_t)std::max<int64_t>(G->total_b, 1) * ldFB * 4));
+  FAP_TRY(G->d_bpart.ensure(bp.size() * sizeof(BPart)));
+  FAP_TRY(G->d_brows.ensure(std::max<size_t>(rows.size(), 2) * 8));
+  FAP_CK(cudaMemcpy(G->d_bpart.p, bp.data(), bp.size() * sizeof(BPart), cudaMemcpyHostToDevice));
+  if (!rows.empty())
+    FAP_CK(cudaMemcpy(G->d_brows.p, rows.data(), rows.size() * 8, cudaMemcpyHostToDevice));
+  return FAP_OK;
+}
+
 // Builds (or reuses) the batch descriptors for the requested parts.
-int prepare_batch(fap_dgraph *G, const std::vector<int32_t> &ids, bool cached) {
-  const bool same = (ids == G->last_ids) && (cached == G->last_cached);
+int prepare_batch(fap_dgraph *G, const std::vector<int32_t> &ids, bool cached, bool bmethod) {
+  const bool same = (ids == G->last_ids) && (cached == G->last_cached) && (bmethod == G->last_bmethod);
   if (same) return FAP_OK;
   const int64_t n = G->n;
   const bool full = (G->max_rows == n);
@@ -535,7 +605,8 @@ int prepare_batch(fap_dgraph *G, const std::vector<int32_t> &ids, bool cached) {
     d.row_base = base[i];
     d.ldf = ldf;
     d.f_off = cached ? (int64_t)(p - 1) * ldf * ldf : foff;
-    d.bd_row = cached ? (int32_t)G->cb_off[p] : 0;
+    d.bd_row = cached ? (int32_t)G->cb_off[p] : bmethod ? G->boff[p] : 0;
+    d.flags = bmethod ? kPartLocal : 0;
     foff += (int64_t)d.ldf * d.ldf;
     G->max_b = std::max(G->max_b, d.b);
     G->max_s = std::max(G->max_s, d.s);
@@ -562,11 +633,12 @@ int prepare_batch(fap_dgraph *G, const std::vector<int32_t> &ids, bool cached) {
   FAP_TRY(G->d_thin.ensure(std::max<size_t>(G->thin.size(), 1) * 4));
   FAP_TRY(G->d_src.ensure(std::max<size_t>(G->src.size(), 1) * 4));
   FAP_TRY(G->d_srcrows.ensure(std::max<size_t>(G->srcrows.size(), 1) * 8));
-  if (!cached)
+  if (!cached && !bmethod)
     FAP_TRY(G->sssp_scratch.ensure(
         (size_t)std::max(sssp_scratch_rows(G->n, (int)G->src.size()), 1) * (size_t)G->n * 4));
   cudaStream_t st = G->ctx->stream;
   FAP_CK(cudaStreamSynchronize(st));
+  if (bmethod) FAP_TRY(prepare_bgraph(G, G->parts));
   FAP_CK(cudaMemcpy(G->d_parts.p, G->parts.data(), G->parts.size() * sizeof(PartDesc), cudaMemcpyHostToDevice));
   if (!G->work.empty())
     FAP_CK(cudaMemcpy(G->d_work.p, G->work.data(), G->work.size() * sizeof(MPWork), cudaMemcpyHostToDevice));
@@ -580,6 +652,7 @@ int prepare_batch(fap_dgraph *G, const std::vector<int32_t> &ids, bool cached) {
   std::fill(G->row_base.begin(), G->row_base.end(), -1);
   G->last_ids = ids;
   G->last_cached = cached;
+  G->last_bmethod = bmethod;
   G->epoch++;
   return FAP_OK;
 }
@@ -629,7 +702,32 @@ int run_solve(fap_dgraph *G, int mode) {
   int64_t L = 0;
   FAP_CK(cudaMemsetAsync(status, 0, sizeof(int), st));
   for (int i = 0; i < 5; i++) G->timing[i] = -1.0f;
-  if (mode == FAP_MODE_BATCHED && G->last_cached) {
+  if (mode == FAP_MODE_BATCHED && G->last_bmethod) {
+    // Boundary-graph form: local closures of all parts, boundary-graph APSP,
+    // boundary rows by expansion, then the min-plus merge.  The events keep
+    // the stage slots in order of time: [gather, floyd, boundary graph +
+    // expansion, min-plus] (fap_graph_last_timing maps them back).
+    FAP_CK(record_event(c->ev[0], st));
+    FAP_CK(launch_gather<T>(dp, np, G->max_ldf, ro, col, w, gid, st2ed, ed2st, D, G->ldD, F, st, &L));
+    FAP_CK(record_event(c->ev[1], st));
+    FAP_CK(launch_floyd_parts_multi<T>(dp, np, (int)ceil_div(G->max_s, kFloydTile), F, G->max_ldf,
+                                       status, st, &L));
+    FAP_CK(record_event(c->ev[2], st));
+    T *dB = G->d_dB.as<T>();
+    const BPart *bp = G->d_bpart.as<const BPart>();
+    FAP_CK(launch_bgraph<T>(dp, np, G->max_b, F, dB, G->ldB, ro, col, w, G->n, gid, ed2st, bp, st, &L));
+    FAP_CK(launch_floyd_matrix<T>(dB, G->ldB, (int)(G->ldB / kFloydTile), status, st, &L));
+    FAP_CK(launch_bdy_expand<T>(G->d_brows.as<const int64_t>(), (int)G->total_b, bp, gid, ed2st, G->n, dB,
+                                G->ldB, (int)G->total_b, F, D, G->ldD, G->d_FB.as<T>(), G->max_ldf, st, &L));
+    FAP_CK(launch_local_fixup<T>(dp, np, G->max_s, F, G->d_FB.as<const T>(), G->max_ldf, st, &L));
+    FAP_CK(record_event(c->ev[3], st));
+    FAP_CK(launch_minplus_thin<T>(dp, G->d_thin.as<int32_t>(), (int)G->thin.size(), G->max_s, G->n, F, D,
+                                  G->ldD, gid, ed2st, st, &L));
+    FAP_CK(launch_minplus_parts<T>(dp, np, dw, (int)G->work.size(), G->n, F, G->max_ldf, D, G->ldD,
+                                   G->max_rows, gid, ed2st, status, st, &L));
+    if (G->paths) FAP_TRY(launch_paths<T>(G, dp, np, G->max_s, &L));
+    FAP_CK(record_event(c->ev[4], st));
+  } else if (mode == FAP_MODE_BATCHED && G->last_cached) {
     // Resident cache: boundary rows and closed Floyd matrices are ready;
     // copy the boundary rows into the block and run the min-plus merge.
     const T *cF = G->cF.as<const T>();
@@ -734,7 +832,9 @@ extern "C" int fap_solve(fap_dgraph *G, const int32_t *parts, int32_t count, int
     FAP_TRY(G->P.ensure((size_t)G->max_rows * G->ldD * 4));
     G->epoch++;
   }
-  FAP_TRY(prepare_batch(G, ids, mode == FAP_MODE_BATCHED && G->cache_ready && G->use_cache));
+  const bool cached = mode == FAP_MODE_BATCHED && G->cache_ready && G->use_cache;
+  const bool bmethod = !cached && mode == FAP_MODE_BATCHED && (int32_t)ids.size() == G->K && bmethod_ok(G);
+  FAP_TRY(prepare_batch(G, ids, cached, bmethod));
   int rc = FAP_OK;
   cudaStream_t st = G->ctx->stream;
   if (mode == FAP_MODE_BATCHED && G->use_graph && st != nullptr) {
@@ -796,13 +896,29 @@ extern "C" int fap_graph_last_timing(fap_dgraph *G, float *ms5) {
   FAP_CK(cudaEventElapsedTime(&t, c->ev[0], c->ev[4]));
   ms5[4] = t;
   if (G->last_mode == FAP_MODE_BATCHED) {
+    float seg[4];
     for (int i = 0; i < 4; i++) {
       FAP_CK(cudaEventElapsedTime(&t, c->ev[i], c->ev[i + 1]));
-      ms5[i] = t;
+      seg[i] = t;
+    }
+    if (G->last_bmethod) {  // recorded as [gather, floyd, boundary graph, min-plus]
+      ms5[0] = seg[2];
+      ms5[1] = seg[0];
+      ms5[2] = seg[1];
+      ms5[3] = seg[3];
+    } else {
+      for (int i = 0; i < 4; i++) ms5[i] = seg[i];
     }
   }
   for (int i = 0; i < 5; i++) G->timing[i] = ms5[i];
   return FAP_OK;
+}
+
+extern "C" int fap_graph_last_stage1(const fap_dgraph *G) {
+  if (!G) return fail(FAP_ERR_INVALID, "NULL graph");
+  if (G->last_mode < 0) return 0;
+  if (G->last_cached) return 3;
+  return G->last_bmethod ? 2 : 1;
 }
 
 extern "C" int fap_graph_last_launches(fap_dgraph *G, int64_t *count) {
@@ -1174,6 +1290,12 @@ extern "C" int fap_graph_set_param(fap_dgraph *G, const char *key, double value)
     G->sssp_chain = value >= 0 ? (int)value : 0;
     return FAP_OK;
   }
+  if (std::strcmp(key, "stage1") == 0) {
+    if (value != 0.0 && value != 1.0 && value != 2.0) return fail(FAP_ERR_INVALID, "stage1 is 0, 1 or 2");
+    G->stage1 = (int)value;
+    G->last_ids.clear();
+    return FAP_OK;
+  }
   if (std::strcmp(key, "paths") == 0) {
     if (value == 0.0) {
       G->paths = false;
@@ -1287,6 +1409,8 @@ extern "C" int fap_graph_release(fap_dgraph *G) {
   G->staging.release();
   G->d_checks.release();
   G->P.release();
+  G->d_dB.release();
+  G->d_FB.release();
   G->max_rows = 0;
   std::fill(G->row_base.begin(), G->row_base.end(), -1);
   G->last_ids.clear();
@@ -1301,7 +1425,8 @@ extern "C" int fap_graph_device_bytes(const fap_dgraph *G, int64_t *bytes) {
                           &G->d_thin, &G->d_gid, &G->d_st2ed, &G->d_ed2st, &G->D, &G->F, &G->d_parts,
                           &G->d_work, &G->d_src, &G->d_srcrows, &G->d_status, &G->d_checks, &G->staging,
                           &G->cBd, &G->cF, &G->d_cparts, &G->d_rowgroups, &G->d_rowloc, &G->d_rowout,
-                          &G->d_rowidx, &G->P, &G->d_tro, &G->d_tcol, &G->d_tw})
+                          &G->d_rowidx, &G->P, &G->d_tro, &G->d_tcol, &G->d_tw, &G->d_dB,
+                          &G->d_bpart, &G->d_brows, &G->d_FB})
     t += (int64_t)b->bytes;
   *bytes = t;
   return FAP_OK;
@@ -1355,6 +1480,7 @@ int cache_build_impl(fap_dgraph *G) {
   G->cparts.clear();
   std::vector<int32_t> src;
   std::vector<int64_t> srows;
+  const bool bm = bmethod_ok(G);
   for (int32_t p = 1; p <= K; p++) {
     PartDesc d{};
     d.part = p;
@@ -1365,6 +1491,7 @@ int cache_build_impl(fap_dgraph *G) {
     d.ldf = cs.ldf;
     d.f_off = (int64_t)(p - 1) * cs.ldf * cs.ldf;
     d.bd_row = (int32_t)G->cb_off[p];
+    d.flags = bm ? kPartLocal : 0;
     G->cparts.push_back(d);
     for (int32_t k = 0; k < d.b; k++) {
       src.push_back(d.start + k);
@@ -1374,8 +1501,9 @@ int cache_build_impl(fap_dgraph *G) {
   FAP_TRY(G->d_cparts.ensure(G->cparts.size() * sizeof(PartDesc)));
   FAP_TRY(G->d_src.ensure(std::max<size_t>(src.size(), 1) * 4));
   FAP_TRY(G->d_srcrows.ensure(std::max<size_t>(srows.size(), 1) * 8));
-  FAP_TRY(G->sssp_scratch.ensure(
-      (size_t)std::max(sssp_scratch_rows(G->n, (int)src.size()), 1) * (size_t)G->n * 4));
+  if (!bm)
+    FAP_TRY(G->sssp_scratch.ensure(
+        (size_t)std::max(sssp_scratch_rows(G->n, (int)src.size()), 1) * (size_t)G->n * 4));
   FAP_CK(cudaMemcpy(G->d_cparts.p, G->cparts.data(), G->cparts.size() * sizeof(PartDesc),
                     cudaMemcpyHostToDevice));
   if (!src.empty()) {
@@ -1393,18 +1521,36 @@ int cache_build_impl(fap_dgraph *G) {
   const int64_t rounds = G->sssp_max_rounds > 0 ? G->sssp_max_rounds : 8 * (int64_t)G->n + 1024;
   int64_t L = 0;
   FAP_CK(cudaMemsetAsync(status, 0, sizeof(int), st));
+  if (bm) {
+    // Boundary-graph form: local closures, boundary-graph APSP, expansion.
+    FAP_TRY(prepare_bgraph(G, G->cparts));
+    FAP_CK(launch_gather<T>(dp, K, cs.ldf, G->ro.as<const int32_t>(), G->col.as<const int32_t>(),
+                            G->w.as<const T>(), gid, st2ed, ed2st, Bd, G->ldD, F, st, &L));
+    FAP_CK(launch_floyd_parts_multi<T>(dp, K, (int)ceil_div(cs.max_s, kFloydTile), F, cs.ldf, status, st, &L));
+    T *dB = G->d_dB.as<T>();
+    const BPart *bp = G->d_bpart.as<const BPart>();
+    FAP_CK(launch_bgraph<T>(dp, K, cs.max_b, F, dB, G->ldB, G->ro.as<const int32_t>(),
+                            G->col.as<const int32_t>(), G->w.as<const T>(), G->n, gid, ed2st, bp, st, &L));
+    FAP_CK(launch_floyd_matrix<T>(dB, G->ldB, (int)(G->ldB / kFloydTile), status, st, &L));
+    FAP_CK(launch_bdy_expand<T>(G->d_brows.as<const int64_t>(), (int)G->total_b, bp, gid, ed2st, G->n, dB,
+                                G->ldB, (int)G->total_b, F, Bd, G->ldD, G->d_FB.as<T>(), cs.ldf, st, &L));
+    FAP_CK(launch_local_fixup<T>(dp, K, cs.max_s, F, G->d_FB.as<const T>(), cs.ldf, st, &L));
+    G->cache_bmethod = true;
+  } else {
   FAP_CK(launch_sssp<T>(G->ro_s.as<const int32_t>(), G->col_s.as<const int32_t>(), G->w_s.as<const T>(),
                         G->n, G->d_src.as<const int32_t>(), G->d_srcrows.as<const int64_t>(),
                         (int)src.size(), Bd, G->ldD, G->ldD, ed2st, G->sssp_scratch.as<T>(),
                         sssp_delta_for<T>(G), G->sssp_chain, G->sssp_precheck, rounds, status, st, &L));
   FAP_CK(launch_gather<T>(dp, K, cs.ldf, G->ro.as<const int32_t>(), G->col.as<const int32_t>(),
                           G->w.as<const T>(), gid, st2ed, ed2st, Bd, G->ldD, F, st, &L));
+  G->cache_bmethod = false;
   if (G->floyd_per_cta) {
     FAP_CK(launch_floyd_parts<T>(dp, K, F, cs.ldf, Bd, G->ldD, st2ed, status, st, &L));
   } else {
     FAP_CK(launch_floyd_parts_multi<T>(dp, K, (int)ceil_div(cs.max_s, kFloydTile), F, cs.ldf, status,
                                        st, &L));
     FAP_CK(launch_bdy_scatter<T>(dp, K, F, Bd, G->ldD, st2ed, cs.max_b, cs.max_s, st, &L));
+  }
   }
   G->cache_ldf = cs.ldf;
   G->cache_max_b = cs.max_b;
@@ -1514,11 +1660,20 @@ extern "C" int fap_graph_cache_bytes(const fap_dgraph *G, int64_t *bytes, int *b
   if (G->cache_ready) {
     *bytes = (int64_t)(G->cBd.bytes + G->cF.bytes + G->d_cparts.bytes);
   } else {
-    // plus the SSSP scratch the build needs while it runs
+    // plus what the build needs while it runs: the SSSP scratch, or the
+    // boundary-graph matrix and tables
     const CacheShape cs = cache_shape(G);
-    *bytes = cs.bytes(G) + (int64_t)alloc_size(
-                               (size_t)std::max(sssp_scratch_rows(G->n, (int)std::min<int64_t>(cs.total_b, INT32_MAX)), 1) *
-                               (size_t)G->n * 4);
+    if (bmethod_ok(G)) {
+      const int64_t ldB = round_up(std::max<int64_t>(G->total_b, 1), kFloydTile);
+      *bytes = cs.bytes(G) + (int64_t)alloc_size((size_t)(ldB * ldB * 4)) +
+               (int64_t)alloc_size((size_t)std::max<int64_t>(G->total_b, 1) * cs.ldf * 4) +
+               (int64_t)alloc_size((size_t)(G->K + 1) * sizeof(BPart)) +
+               (int64_t)alloc_size((size_t)std::max<int64_t>(2 * G->total_b, 2) * 8);
+    } else {
+      *bytes = cs.bytes(G) + (int64_t)alloc_size(
+                                 (size_t)std::max(sssp_scratch_rows(G->n, (int)std::min<int64_t>(cs.total_b, INT32_MAX)), 1) *
+                                 (size_t)G->n * 4);
+    }
   }
   return FAP_OK;
 }

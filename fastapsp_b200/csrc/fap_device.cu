@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(256)
     for (int j = threadIdx.x; j < pd.ldf; j += blockDim.x) Fi[j] = inf;
     return;
   }
-  if (i < pd.b) {
+  if (i < pd.b && !(pd.flags & kPartLocal)) {
     const T *Si = D + (pd.row_base + i) * ldD;
     for (int j = threadIdx.x; j < pd.ldf; j += blockDim.x) {
       T v = inf;
@@ -827,6 +827,194 @@ cudaError_t launch_pred(const PartDesc *parts, int nparts, int max_s, const T *D
 }
 
 // ---------------------------------------------------------------------------
+// Boundary-graph form of stage 1
+// ---------------------------------------------------------------------------
+// Every shortest path between boundary vertices is a chain of segments
+// inside one part (between two of its boundary vertices: the local closure)
+// and cross-part arcs (both ends are boundary vertices by construction,
+// fap/utils/util_preprocess.h:32-58).  dB closed by Floyd is therefore exact;
+// a path from a boundary vertex into part q last enters q at one of q's
+// boundary vertices b' and stays in q, so D[g][v] = min_b' dB[g][b'] +
+// F_q[b'][v] is the exact shortest distance.
+template <typename T>
+__global__ void bgraph_local_kernel(const PartDesc *__restrict__ parts, const T *__restrict__ F, T *dB,
+                                    int64_t ldB) {
+  const PartDesc pd = parts[blockIdx.y];
+  const int i = blockIdx.x;
+  if (i >= pd.b) return;
+  const T *Fi = F + pd.f_off + (int64_t)i * pd.ldf;
+  T *Bi = dB + ((int64_t)pd.bd_row + i) * ldB + pd.bd_row;
+  for (int k = threadIdx.x; k < pd.b; k += blockDim.x) Bi[k] = Fi[k];
+}
+
+template <typename T>
+__global__ void bgraph_cross_kernel(const int32_t *__restrict__ row_offset, const int32_t *__restrict__ col,
+                                    const T *__restrict__ w, int n, const int32_t *__restrict__ graph_id,
+                                    const int32_t *__restrict__ ed2st, const BPart *__restrict__ bpart,
+                                    T *dB, int64_t ldB) {
+  for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x) {
+    const int pu = __ldg(graph_id + u);
+    const int e0 = __ldg(row_offset + u), e1 = __ldg(row_offset + u + 1);
+    int gu = -1;
+    for (int e = e0; e < e1; e++) {
+      const int v = __ldg(col + e);
+      const int pv = __ldg(graph_id + v);
+      if (pv == pu) continue;
+      if (gu < 0) {
+        const BPart P = bpart[pu];
+        const int lu = __ldg(ed2st + u) - P.voff;
+        if (lu < 0 || lu >= P.b) break;  // not a boundary vertex: cannot happen
+        gu = P.boff + lu;
+      }
+      const BPart Q = bpart[pv];
+      const int lv = __ldg(ed2st + v) - Q.voff;
+      if (lv < 0 || lv >= Q.b) continue;
+      Dist<T>::atomic_min(dB + (int64_t)gu * ldB + Q.boff + lv, __ldg(w + e));
+    }
+  }
+}
+
+template <typename T>
+cudaError_t launch_bgraph(const PartDesc *parts, int nparts, int max_b, const T *F, T *dB, int64_t ldB,
+                          const int32_t *row_offset, const int32_t *col, const T *w, int n,
+                          const int32_t *graph_id, const int32_t *ed2st, const BPart *bpart,
+                          cudaStream_t stream, int64_t *launches) {
+  cudaError_t e = launch_fill<T>(dB, ldB, ldB, ldB, Dist<T>::inf(), stream, launches);
+  if (e != cudaSuccess) return e;
+  if (nparts > 0 && max_b > 0) {
+    bgraph_local_kernel<T><<<dim3(max_b, nparts), 128, 0, stream>>>(parts, F, dB, ldB);
+    *launches += 1;
+  }
+  const int blocks = (int)std::min<int64_t>(ceil_div(n, 256), 148 * 8);
+  bgraph_cross_kernel<T><<<blocks, 256, 0, stream>>>(row_offset, col, w, n, graph_id, ed2st, bpart, dB, ldB);
+  *launches += 1;
+  return cudaGetLastError();
+}
+
+// grid (column chunks, groups of kExpandRows listed rows); the rows' dB
+// entries sit in shared memory; a thread computes whole output columns
+// (coalesced stores in original column order) from the boundary rows of the
+// column's part, read once for all of the CTA's rows.  Own-part entries are
+// also written to FB[g][j] (the exact distances from boundary vertex g to
+// its part's vertices, for the local-closure fix-up).
+constexpr int kExpandRows = 8;
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+    bdy_expand_kernel(const int64_t *__restrict__ rows, int nrows, const BPart *__restrict__ bpart,
+                      const int32_t *__restrict__ graph_id, const int32_t *__restrict__ ed2st, int n,
+                      const T *__restrict__ dB, int64_t ldB, int nbB, const T *__restrict__ F, T *D,
+                      int64_t ldD, T *FB, int64_t ldFB) {
+  extern __shared__ unsigned char bx_smem_raw[];
+  T *drow = reinterpret_cast<T *>(bx_smem_raw);  // kExpandRows x nbB
+  const int r0 = blockIdx.y * kExpandRows;
+  const int nr = min(kExpandRows, nrows - r0);
+  int64_t g[kExpandRows], dr[kExpandRows];
+#pragma unroll
+  for (int q = 0; q < kExpandRows; q++) {
+    g[q] = q < nr ? rows[2 * (r0 + q)] : 0;
+    dr[q] = q < nr ? rows[2 * (r0 + q) + 1] : 0;
+  }
+  for (int t = threadIdx.x; t < nr * nbB; t += blockDim.x) {
+    const int q = t / nbB, k = t % nbB;
+    drow[t] = dB[rows[2 * (r0 + q)] * ldB + k];
+  }
+  __syncthreads();
+  const T inf = Dist<T>::inf();
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < ldD; v += (int64_t)gridDim.x * blockDim.x) {
+    T acc[kExpandRows];
+#pragma unroll
+    for (int q = 0; q < kExpandRows; q++) acc[q] = inf;
+    int j = -1, qb = 0, qoff = 0;
+    if (v < n) {
+      const BPart Q = bpart[__ldg(graph_id + v)];
+      j = __ldg(ed2st + v) - Q.voff;
+      qb = Q.b;
+      qoff = Q.boff;
+      const T *Fq = F + Q.f_off + j;
+      for (int k = 0; k < Q.b; k++) {
+        const T f = __ldg(Fq + (int64_t)k * Q.ldf);
+#pragma unroll
+        for (int q = 0; q < kExpandRows; q++) acc[q] = Dist<T>::relax(drow[q * nbB + Q.boff + k], f, acc[q]);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < kExpandRows; q++) {
+      if (q >= nr) break;
+      D[dr[q] * ldD + v] = acc[q];
+      if (j >= 0 && g[q] >= qoff && g[q] < qoff + qb) FB[g[q] * ldFB + j] = acc[q];
+    }
+  }
+}
+
+template <typename T>
+cudaError_t launch_bdy_expand(const int64_t *rows, int nrows, const BPart *bpart, const int32_t *graph_id,
+                              const int32_t *ed2st, int n, const T *dB, int64_t ldB, int nbB, const T *F,
+                              T *D, int64_t ldD, T *FB, int64_t ldFB, cudaStream_t stream, int64_t *launches) {
+  if (nrows <= 0) return cudaSuccess;
+  const size_t smem = (size_t)kExpandRows * std::max(nbB, 1) * sizeof(T);
+  auto kern = bdy_expand_kernel<T>;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  const int bx = (int)ceil_div(ldD, 256);
+  kern<<<dim3(bx, (unsigned)ceil_div(nrows, kExpandRows)), 256, smem, stream>>>(
+      rows, nrows, bpart, graph_id, ed2st, n, dB, ldB, nbB, F, D, ldD, FB, ldFB);
+  *launches += 1;
+  return cudaGetLastError();
+}
+
+// Local closure -> exact closure of each part, in place: for inner rows i,
+//   F[i][j] = min(F[i][j], min_{k<b} F[i][k] + FB[k][j])
+// (a path from i to j either stays in the part or leaves it through a
+// boundary vertex k first, after which FB holds the exact rest).  The
+// boundary rows of F take FB's values.  grid (parts, row chunks of 32).
+constexpr int kFixRows = 32;
+
+constexpr int kFixStage = 1024;
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+    local_fixup_kernel(const PartDesc *__restrict__ parts, T *F, const T *__restrict__ FB, int64_t ldFB) {
+  __shared__ T a_s[kFixStage];  // the row's local distances to its boundary vertices, before the update
+  const PartDesc pd = parts[blockIdx.x];
+  const int i0 = blockIdx.y * kFixRows;
+  if (i0 >= pd.s) return;
+  const T *FBp = FB + (int64_t)pd.bd_row * ldFB;
+  const int i1 = min(i0 + kFixRows, pd.s);
+  const bool staged = pd.b <= kFixStage;
+  for (int i = i0; i < i1; i++) {
+    T *Fi = F + pd.f_off + (int64_t)i * pd.ldf;
+    if (i < pd.b) {
+      for (int j = threadIdx.x; j < pd.s; j += blockDim.x) Fi[j] = FBp[(int64_t)i * ldFB + j];
+      continue;
+    }
+    if (staged) {
+      __syncthreads();
+      for (int k = threadIdx.x; k < pd.b; k += blockDim.x) a_s[k] = Fi[k];
+      __syncthreads();
+    }
+    for (int j = threadIdx.x; j < pd.s; j += blockDim.x) {
+      T acc = Fi[j];
+      for (int k = 0; k < pd.b; k++)
+        acc = Dist<T>::relax(staged ? a_s[k] : Fi[k], FBp[(int64_t)k * ldFB + j], acc);
+      Fi[j] = acc;
+    }
+  }
+}
+
+template <typename T>
+cudaError_t launch_local_fixup(const PartDesc *parts, int nparts, int max_s, T *F, const T *FB, int64_t ldFB,
+                               cudaStream_t stream, int64_t *launches) {
+  if (nparts <= 0 || max_s <= 0) return cudaSuccess;
+  local_fixup_kernel<T><<<dim3(nparts, (unsigned)ceil_div(max_s, kFixRows)), 256, 0, stream>>>(parts, F, FB,
+                                                                                              ldFB);
+  *launches += 1;
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 // Resident cache kernels
 // ---------------------------------------------------------------------------
 template <typename T>
@@ -1157,6 +1345,16 @@ cudaError_t launch_relax_peak(T *sink, int blocks, int iters, cudaStream_t strea
   template cudaError_t launch_minplus_generic<T>(int, int, int, const T *, int64_t, const T *,    \
                                                  int64_t, T *, int64_t, cudaStream_t, int64_t *); \
   template cudaError_t launch_fill<T>(T *, int64_t, int64_t, int64_t, T, cudaStream_t, int64_t *); \
+  template cudaError_t launch_bgraph<T>(const PartDesc *, int, int, const T *, T *, int64_t,       \
+                                        const int32_t *, const int32_t *, const T *, int,          \
+                                        const int32_t *, const int32_t *, const BPart *,           \
+                                        cudaStream_t, int64_t *);                                  \
+  template cudaError_t launch_bdy_expand<T>(const int64_t *, int, const BPart *, const int32_t *,  \
+                                            const int32_t *, int, const T *, int64_t, int,         \
+                                            const T *, T *, int64_t, T *, int64_t, cudaStream_t,   \
+                                            int64_t *);                                            \
+  template cudaError_t launch_local_fixup<T>(const PartDesc *, int, int, T *, const T *, int64_t,  \
+                                             cudaStream_t, int64_t *);                             \
   template cudaError_t launch_pred<T>(const PartDesc *, int, int, const T *, int32_t *, int64_t,  \
                                       int, const int32_t *, const int32_t *, const T *,            \
                                       const int32_t *, cudaStream_t, int64_t *);                   \

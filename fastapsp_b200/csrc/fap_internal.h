@@ -16,7 +16,24 @@ struct PartDesc {
   int64_t row_base;  // first output row of the part's block
   int64_t f_off;     // offset of the part's padded Floyd matrix in the F arena
   int32_t ldf;       // padded Floyd leading dimension (multiple of kFloydTile)
-  int32_t bd_row;    // first row of the part's boundary rows in the resident cache
+  int32_t bd_row;    // first row of the part's boundary rows in the resident cache /
+                     // boundary index space (prefix sum of the boundary counts)
+  int32_t flags;     // kPartLocal
+  int32_t pad_;
+};
+
+// PartDesc::flags.  kPartLocal: the Floyd matrix is built from the part's
+// own edges only (boundary rows included), i.e. the local closure (the
+// boundary-graph form of stage 1).
+constexpr int32_t kPartLocal = 1;
+
+// Per part id (1..K) for the boundary-graph expansion.
+struct BPart {
+  int32_t voff;   // first sorted position
+  int32_t b;      // boundary count
+  int32_t boff;   // first index in the boundary index space
+  int32_t ldf;    // Floyd leading dimension
+  int64_t f_off;  // the part's local closure in the Floyd arena
 };
 
 // Rows-from-cache work: up to kRowsGroup output rows of one part.
@@ -117,6 +134,32 @@ template <typename T>
 cudaError_t launch_pred(const PartDesc *parts, int nparts, int max_s, const T *D, int32_t *P,
                         int64_t ldD, int n, const int32_t *tro, const int32_t *tcol, const T *tw,
                         const int32_t *st2ed, cudaStream_t stream, int64_t *launches);
+
+// Boundary-graph form of stage 1 (exact shortest distances from boundary
+// vertices without SSSP).  With every part's local closure in F:
+//   launch_bgraph: dB (nbB x nbB, ld ldB) = INF; dB[b1][b2] = F_p[b1][b2] for
+//     boundary vertices of one part; cross-part arcs u -> v: dB[u][v] =
+//     min(.., w).  Then close dB with launch_floyd_matrix.
+//   launch_bdy_expand: for each listed (boundary index g, output row r):
+//     D[r][v] = min over boundary b' of v's part q of dB[g][b'] + F_q[b'][v].
+template <typename T>
+cudaError_t launch_bgraph(const PartDesc *parts, int nparts, int max_b, const T *F, T *dB, int64_t ldB,
+                          const int32_t *row_offset, const int32_t *col, const T *w, int n,
+                          const int32_t *graph_id, const int32_t *ed2st, const BPart *bpart,
+                          cudaStream_t stream, int64_t *launches);
+//     Own-part entries also go to FB[g][j] (FB: boundary index x part-local
+//     column, ld ldFB).
+//   launch_local_fixup: turns every part's local closure in F into its
+//     exact closure (inner rows: min over leaving through a boundary vertex;
+//     boundary rows: FB), so that the min-plus merge and its decode run as in
+//     the SSSP form.
+template <typename T>
+cudaError_t launch_bdy_expand(const int64_t *rows, int nrows, const BPart *bpart, const int32_t *graph_id,
+                              const int32_t *ed2st, int n, const T *dB, int64_t ldB, int nbB, const T *F,
+                              T *D, int64_t ldD, T *FB, int64_t ldFB, cudaStream_t stream, int64_t *launches);
+template <typename T>
+cudaError_t launch_local_fixup(const PartDesc *parts, int nparts, int max_s, T *F, const T *FB, int64_t ldFB,
+                               cudaStream_t stream, int64_t *launches);
 
 // Resident cache: copy each listed part's boundary rows Bd[bd_row + i] into
 // D[row_base + i] (all ldD columns).

@@ -245,7 +245,10 @@ __global__ void __launch_bounds__(kSsspThreads)
         const int take = min(total, kSsspList);
         for (int i = threadIdx.x; i < take; i += blockDim.x) {
           const int u = act[i];
+          // The distance and the edge range are independent loads: issue
+          // them together (one latency instead of two).
           const T du = ld_relaxed(dist + u);
+          const int u0 = __ldg(row_offset + u), u1 = __ldg(row_offset + u + 1);
           if (!(du < thresh)) {  // far: expand in a later bucket
             atomicOr(nb + (u >> 5), 1u << (u & 31));
             minfar = min(minfar, order_bits<T>(du));
@@ -256,7 +259,8 @@ __global__ void __launch_bounds__(kSsspThreads)
           int x = u;
           T dx = du;
           for (int hop = 0;; hop++) {
-            const int e0 = __ldg(row_offset + x), e1 = __ldg(row_offset + x + 1);
+            const int e0 = hop == 0 ? u0 : __ldg(row_offset + x);
+            const int e1 = hop == 0 ? u1 : __ldg(row_offset + x + 1);
             if (e1 - e0 > kHeavyDeg) {
               const int h = atomicAdd(&s_nheavy, 1);
               if (h < kHeavyList) {

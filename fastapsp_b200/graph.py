@@ -486,6 +486,10 @@ class DeviceGraph:
         check(lib().fap_graph_last_timing(self._h, ptr(t)), "last_timing")
         return t
 
+    def last_stage1(self) -> int:
+        """1 SSSP, 2 boundary graph, 3 resident cache (see fap_graph_last_stage1)."""
+        return int(lib().fap_graph_last_stage1(self._h))
+
     def last_launches(self) -> int:
         x = ctypes.c_int64()
         check(lib().fap_graph_last_launches(self._h, ctypes.byref(x)))

@@ -148,7 +148,10 @@ FAP_API int fap_graph_sssp_rows(fap_dgraph *g, const int32_t *sources, int32_t c
  * unchanged); "use_cache" (non-zero, the default: batched solves and
  * fap_graph_rows_async use the resident cache once it is built); "paths"
  * (non-zero: later solves also produce the parts' predecessor rows, see
- * fap_graph_path_block; needs every edge weight > 0, else FAP_ERR_RANGE). */
+ * fap_graph_path_block; needs every edge weight > 0, else FAP_ERR_RANGE);
+ * "stage1" (0 automatic, the default; 1 always SSSP; 2 the boundary graph
+ * whenever the graph allows it, whatever its dtype and boundary count; see
+ * fap_graph_last_stage1). */
 FAP_API int fap_graph_set_param(fap_dgraph *g, const char *key, double value);
 
 /* Tunes the SSSP bucket width: runs the SSSP stage on `sample` boundary
@@ -218,6 +221,15 @@ FAP_API int fap_graph_cache_bytes(const fap_dgraph *g, int64_t *bytes, int *buil
 /* Device time (ms) of the stages of the last fap_solve, measured with events
  * on the context stream: [sssp, gather, floyd, minplus, total]. */
 FAP_API int fap_graph_last_timing(fap_dgraph *g, float *ms5);
+
+/* How the last fap_solve obtained the boundary rows (stage 1): 1 SSSP from
+ * every boundary vertex; 2 the boundary graph (every part's local closure,
+ * APSP over the boundary vertices, expansion; chosen for batches of all
+ * parts of int32 graphs with at most 8192 boundary vertices and no two arcs
+ * joining the same ordered pair inside a part; with "stage1" = 2 also for
+ * float32 graphs, whose results then differ from the SSSP form by rounding
+ * order, a few ulps); 3 the resident cache; 0 no solve yet. */
+FAP_API int fap_graph_last_stage1(const fap_dgraph *g);
 
 /* Number of kernels the last fap_solve launched. */
 FAP_API int fap_graph_last_launches(fap_dgraph *g, int64_t *count);

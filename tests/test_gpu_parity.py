@@ -167,6 +167,7 @@ def test_sssp_round_bound_reports_error_and_context_survives(cuda_ok):
     dg = DeviceGraph(ctx, ro, col[:ro[-1]], w[:ro[-1]])
     dg.set_parts(case["K"], case["graph_id"], case["st2ed"], case["ver_num"],
                  case["ver_offset"], case["bdy_num"])
+    dg.set_param("stage1", 1)          # the SSSP form (the boundary-graph form has no rounds)
     dg.set_param("sssp_max_rounds", 3)
     with pytest.raises(FapError) as e:
         dg.solve(mode=FAP_MODE_BATCHED)
