@@ -57,8 +57,8 @@ def parse_args():
     ap.add_argument("--paths", action="store_true",
                     help="also time batched solves that produce predecessor matrices")
     ap.add_argument("--serve-graphs", type=int, default=32)
-    ap.add_argument("--serve-burst", type=int, default=256,
-                    help="requests of the closed-loop burst that measures capacity")
+    ap.add_argument("--serve-burst", type=int, default=1024,
+                    help="requests of the closed-loop run that measures capacity")
     ap.add_argument("--serve-seconds", type=float, default=4.0,
                     help="arrival window of each offered-load run")
     ap.add_argument("--serve-batch-rows", type=int, default=0,
@@ -262,9 +262,9 @@ def main_reference(args):
 def run_serving(args, device):
     """Serving stream: Poisson arrivals of solveSubGraph / distance-row
     requests over resident random-geometric graphs, answered by the native
-    serving loop (fap_server_*).  Capacity is measured with a closed-loop
-    burst; then requests arrive at 25/50/90% of it.  Each request returns
-    per-row checksums (its distances stay in HBM)."""
+    serving loop (fap_server_*).  Capacity is measured in a closed loop (64
+    requests in flight); then requests arrive at 25/50/90% of it.  Each
+    request returns per-row checksums (its distances stay in HBM)."""
     from fastapsp_b200 import workloads
     from fastapsp_b200.serve import Server
 
@@ -293,12 +293,18 @@ def run_serving(args, device):
             return srv.submit_subgraph(req[1], req[2], distances=False, checksums=True)
         return srv.submit_rows(req[1], req[2], distances=False, checksums=True)
 
-    def finish(handles):
+    def finish(handles, kinds=None):
+        """Waits for the handles; returns per-kind latency percentiles."""
         srv.drain()
-        for h in handles:
+        lat = {"sub": [], "rows": []}
+        for i, h in enumerate(handles):
             if h.wait(0) != 2:
                 raise RuntimeError(f"serving request failed: {h.info()}")
+            if kinds is not None:
+                lat[kinds[i]].append(h.info()["latency_ms"])
             h.forget()
+        return {k: {"requests": len(v), "p50_ms": float(np.percentile(v, 50)) if v else None,
+                    "p99_ms": float(np.percentile(v, 99)) if v else None} for k, v in lat.items()}
 
     # warm-up: one request of each kind per graph (resident caches, batch buffers)
     finish([srv.submit_subgraph(i, 1, distances=False, checksums=True) for i, *_ in info] +
@@ -307,11 +313,18 @@ def run_serving(args, device):
     warm = srv.stats()
     log(f"serving warm-up: {warm.cache_builds} caches built, {warm.busy_ms:.1f} ms device time")
     srv.reset_stats()
-    # capacity: closed-loop burst
+    # capacity: closed loop, a window of 64 requests in flight
     reqs = [draw() for _ in range(args.serve_burst)]
+    window = 64
     t0 = time.perf_counter()
-    hs = [submit(r) for r in reqs]
-    finish(hs)
+    hs, pending = [], []
+    for r in reqs:
+        if len(pending) >= window:
+            pending.pop(0).wait()
+        h = submit(r)
+        hs.append(h)
+        pending.append(h)
+    by_kind = finish(hs, [r[0] for r in reqs])
     burst_s = time.perf_counter() - t0
     st = srv.stats()
     cap_rps = len(reqs) / burst_s
@@ -323,15 +336,16 @@ def run_serving(args, device):
                   "(100-10,000 sources, log-uniform); per-row checksums returned",
            "budget_bytes": int(0.6 * free_b),
            "capacity": {"requests_s": cap_rps, "entries_s": st.entries / burst_s,
-                        "requests": len(reqs), "batches": st.batches,
+                        "requests": len(reqs), "window": window, "batches": st.batches,
                         "resident_hits": st.resident_hits, "p50_ms": st.p50_ms, "p99_ms": st.p99_ms,
-                        "device_busy_frac": st.busy_ms * 1e-3 / burst_s},
+                        "by_kind": by_kind, "device_busy_frac": st.busy_ms * 1e-3 / burst_s},
            "warmup_cache_builds": warm.cache_builds,
            "loads": []}
-    log(f"serving capacity {cap_rps:.1f} req/s, {st.entries / burst_s:.4g} entries/s")
+    log(f"serving capacity {cap_rps:.1f} req/s, {st.entries / burst_s:.4g} entries/s "
+        f"(closed loop, {window} in flight)")
     for frac in (0.25, 0.5, 0.9):
         rate = frac * cap_rps
-        count = int(min(max(32, rate * args.serve_seconds), 4 * args.serve_burst))
+        count = int(min(max(32, rate * args.serve_seconds), 2 * args.serve_burst))
         reqs = [draw() for _ in range(count)]
         gaps = rng.exponential(1.0 / rate, count)
         srv.reset_stats()
@@ -347,18 +361,21 @@ def run_serving(args, device):
                 time.sleep(min(due - now, 0.002))
             hs.append(submit(r))
         t_sub = time.perf_counter() - t0
-        finish(hs)
+        by_kind = finish(hs, [r[0] for r in reqs])
         wall = time.perf_counter() - t0
         st = srv.stats()
         out["loads"].append({"offered_frac": frac, "offered_requests_s": rate,
                              "requests": count, "arrival_window_s": t_sub,
                              "achieved_requests_s": count / wall, "entries_s": st.entries / wall,
                              "p50_ms": st.p50_ms, "p99_ms": st.p99_ms, "mean_ms": st.mean_ms,
+                             "by_kind": by_kind,
                              "batches": st.batches, "resident_hits": st.resident_hits,
                              "peak_device_bytes": st.peak_bytes, "cache_builds": st.cache_builds,
                              "device_busy_frac": st.busy_ms * 1e-3 / wall})
         log(f"serving at {frac:.0%}: p50 {st.p50_ms:.2f} ms, p99 {st.p99_ms:.2f} ms, "
-            f"{st.entries / wall:.4g} entries/s, {st.batches} batches")
+            f"{st.entries / wall:.4g} entries/s, {st.batches} batches; "
+            f"sub p50/p99 {by_kind['sub']['p50_ms']}/{by_kind['sub']['p99_ms']}, "
+            f"rows p50/p99 {by_kind['rows']['p50_ms']}/{by_kind['rows']['p99_ms']}")
     srv.close()
     return out
 
