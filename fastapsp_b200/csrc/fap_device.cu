@@ -554,6 +554,13 @@ __device__ __forceinline__ void thin_rows(ThinShared<T> &sh, const PartDesc &pd,
       sv[k][4 * g + 0] = v.x; sv[k][4 * g + 1] = v.y; sv[k][4 * g + 2] = v.z; sv[k][4 * g + 3] = v.w;
     }
   const T *Fp = F + pd.f_off;
+  // Own-part columns (the decode): staged slot per column, or -1.  Own
+  // columns are scattered over the strip, so the replacement is done with
+  // selects (no divergent branch per row) whenever any lane of the warp has
+  // one; a column whose value was not staged (more own columns than
+  // kThinOwnMax in the strip) takes the rare global-load path.
+  const bool warp_own = __any_sync(0xffffffffu, any_own);
+  const bool cta_unstaged = sh.nown > kThinOwnMax;  // same in every thread
   for (int m0 = mb; m0 < me; m0 += kMinplusBM) {
     const int rows = min(kMinplusBM, me - m0);
     const T *Fr = Fp + (int64_t)(pd.b + m0) * pd.ldf;
@@ -587,13 +594,19 @@ __device__ __forceinline__ void thin_rows(ThinShared<T> &sh, const PartDesc &pd,
               acc[q] = Dist<T>::relax(av[kk], sv[4 * k4 + kk][q], acc[q]);
           }
       }
-      if (any_own) {
+      if (warp_own) {
 #pragma unroll
         for (int q = 0; q < 4 * G; q++) {
           const int o = own[4 * g0 + q];  // -1, or (part-local column << 7) | (slot + 1)
-          if (o >= 0) {
-            const int sl = (o & 127) - 1;
-            acc[q] = sl >= 0 ? sh.Own[r][sl] : Fr[(int64_t)r * pd.ldf + (o >> 7)];
+          const int sl = o >= 0 ? (o & 127) - 1 : -1;
+          const T st = sh.Own[r][sl >= 0 ? sl : 0];
+          acc[q] = sl >= 0 ? st : acc[q];
+        }
+        if (cta_unstaged) {
+#pragma unroll
+          for (int q = 0; q < 4 * G; q++) {
+            const int o = own[4 * g0 + q];
+            if (o >= 0 && (o & 127) == 0) acc[q] = Fr[(int64_t)r * pd.ldf + (o >> 7)];
           }
         }
       }
