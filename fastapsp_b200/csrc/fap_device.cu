@@ -971,8 +971,11 @@ cudaError_t launch_bdy_expand(const int64_t *rows, int nrows, const BPart *bpart
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
-  const int bx = (int)ceil_div(ldD, 256);
-  kern<<<dim3(bx, (unsigned)ceil_div(nrows, kExpandRows)), 256, smem, stream>>>(
+  // Enough CTAs for about 16 per SM, each looping over columns so that the
+  // rows' dB entries are staged only once per CTA.
+  const int64_t ny = ceil_div(nrows, kExpandRows);
+  const int bx = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(ldD, 256), ceil_div(148 * 16, ny)));
+  kern<<<dim3(bx, (unsigned)ny), 256, smem, stream>>>(
       rows, nrows, bpart, graph_id, ed2st, n, dB, ldB, nbB, F, D, ldD, FB, ldFB);
   *launches += 1;
   return cudaGetLastError();
@@ -985,33 +988,36 @@ cudaError_t launch_bdy_expand(const int64_t *rows, int nrows, const BPart *bpart
 // boundary rows of F take FB's values.  grid (parts, row chunks of 32).
 constexpr int kFixRows = 32;
 
-constexpr int kFixStage = 1024;
+constexpr int kFixStage = 4096;  // staged values per CTA: rows x boundary count
 
 template <typename T>
 __global__ void __launch_bounds__(256)
     local_fixup_kernel(const PartDesc *__restrict__ parts, T *F, const T *__restrict__ FB, int64_t ldFB) {
-  __shared__ T a_s[kFixStage];  // the row's local distances to its boundary vertices, before the update
+  // the rows' local distances to their part's boundary vertices, before the update
+  __shared__ T a_s[kFixStage];
   const PartDesc pd = parts[blockIdx.x];
-  const int i0 = blockIdx.y * kFixRows;
+  const int i0 = max(blockIdx.y * kFixRows, 0);
   if (i0 >= pd.s) return;
   const T *FBp = FB + (int64_t)pd.bd_row * ldFB;
   const int i1 = min(i0 + kFixRows, pd.s);
-  const bool staged = pd.b <= kFixStage;
-  for (int i = i0; i < i1; i++) {
-    T *Fi = F + pd.f_off + (int64_t)i * pd.ldf;
-    if (i < pd.b) {
-      for (int j = threadIdx.x; j < pd.s; j += blockDim.x) Fi[j] = FBp[(int64_t)i * ldFB + j];
-      continue;
+  const bool staged = (int64_t)kFixRows * pd.b <= kFixStage;
+  if (staged) {
+    for (int t = threadIdx.x; t < (i1 - i0) * pd.b; t += blockDim.x) {
+      const int r = t / pd.b, k = t % pd.b;
+      a_s[t] = F[pd.f_off + (int64_t)(i0 + r) * pd.ldf + k];
     }
-    if (staged) {
-      __syncthreads();
-      for (int k = threadIdx.x; k < pd.b; k += blockDim.x) a_s[k] = Fi[k];
-      __syncthreads();
-    }
-    for (int j = threadIdx.x; j < pd.s; j += blockDim.x) {
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < pd.s; j += blockDim.x) {
+    for (int i = i0; i < i1; i++) {
+      T *Fi = F + pd.f_off + (int64_t)i * pd.ldf;
+      if (i < pd.b) {
+        Fi[j] = FBp[(int64_t)i * ldFB + j];
+        continue;
+      }
+      const T *ai = staged ? a_s + (int64_t)(i - i0) * pd.b : Fi;
       T acc = Fi[j];
-      for (int k = 0; k < pd.b; k++)
-        acc = Dist<T>::relax(staged ? a_s[k] : Fi[k], FBp[(int64_t)k * ldFB + j], acc);
+      for (int k = 0; k < pd.b; k++) acc = Dist<T>::relax(ai[k], FBp[(int64_t)k * ldFB + j], acc);
       Fi[j] = acc;
     }
   }
