@@ -671,10 +671,10 @@ T sssp_delta_for(const fap_dgraph *G) {
 
 // Predecessor rows of the batch's parts (after their distances).
 template <typename T>
-int launch_paths(fap_dgraph *G, const PartDesc *dp, int np, int max_s, int64_t *L) {
+int launch_paths(fap_dgraph *G, const PartDesc *dp, int np, int max_s, const T *F, int64_t *L) {
   FAP_CK(launch_pred<T>(dp, np, max_s, G->D.as<const T>(), G->P.as<int32_t>(), G->ldD, G->n,
                         G->d_tro.as<const int32_t>(), G->d_tcol.as<const int32_t>(), G->d_tw.as<const T>(),
-                        G->d_st2ed.as<const int32_t>(), G->ctx->stream, L));
+                        G->d_st2ed.as<const int32_t>(), F, G->ctx->stream, L));
   return FAP_OK;
 }
 
@@ -725,7 +725,7 @@ int run_solve(fap_dgraph *G, int mode) {
                                   G->ldD, gid, ed2st, st, &L));
     FAP_CK(launch_minplus_parts<T>(dp, np, dw, (int)G->work.size(), G->n, F, G->max_ldf, D, G->ldD,
                                    G->max_rows, gid, ed2st, status, st, &L));
-    if (G->paths) FAP_TRY(launch_paths<T>(G, dp, np, G->max_s, &L));
+    if (G->paths) FAP_TRY(launch_paths<T>(G, dp, np, G->max_s, F, &L));
     FAP_CK(record_event(c->ev[4], st));
   } else if (mode == FAP_MODE_BATCHED && G->last_cached) {
     // Resident cache: boundary rows and closed Floyd matrices are ready;
@@ -740,7 +740,7 @@ int run_solve(fap_dgraph *G, int mode) {
                                   G->ldD, gid, ed2st, st, &L));
     FAP_CK(launch_minplus_parts<T>(dp, (int)G->K, dw, (int)G->work.size(), G->n, cF, G->cache_ldf, D,
                                    G->ldD, G->max_rows, gid, ed2st, status, st, &L));
-    if (G->paths) FAP_TRY(launch_paths<T>(G, dp, np, G->max_s, &L));
+    if (G->paths) FAP_TRY(launch_paths<T>(G, dp, np, G->max_s, cF, &L));
     FAP_CK(record_event(c->ev[4], st));
   } else if (mode == FAP_MODE_BATCHED) {
     FAP_CK(record_event(c->ev[0], st));
@@ -761,7 +761,7 @@ int run_solve(fap_dgraph *G, int mode) {
                                   G->ldD, gid, ed2st, st, &L));
     FAP_CK(launch_minplus_parts<T>(dp, np, dw, (int)G->work.size(), G->n, F, G->max_ldf, D, G->ldD,
                                    G->max_rows, gid, ed2st, status, st, &L));
-    if (G->paths) FAP_TRY(launch_paths<T>(G, dp, np, G->max_s, &L));
+    if (G->paths) FAP_TRY(launch_paths<T>(G, dp, np, G->max_s, F, &L));
     FAP_CK(record_event(c->ev[4], st));
   } else {
     FAP_CK(record_event(c->ev[0], st));
@@ -780,7 +780,7 @@ int run_solve(fap_dgraph *G, int mode) {
       else
         FAP_CK(launch_minplus_parts<T>(dp, np, dw + w0, w1 - w0, G->n, F, G->max_ldf, D, G->ldD,
                                        G->max_rows, gid, ed2st, status, st, &L));
-      if (G->paths) FAP_TRY(launch_paths<T>(G, dp + i, 1, d.s, &L));
+      if (G->paths) FAP_TRY(launch_paths<T>(G, dp + i, 1, d.s, F, &L));
     }
     FAP_CK(record_event(c->ev[4], st));
   }

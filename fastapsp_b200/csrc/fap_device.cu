@@ -772,16 +772,30 @@ template <typename T>
 __global__ void __launch_bounds__(kPredThreads)
     pred_kernel(const PartDesc *__restrict__ parts, const T *__restrict__ D, int32_t *__restrict__ P,
                 int64_t ldD, int n, const int32_t *__restrict__ tro, const int32_t *__restrict__ tcol,
-                const T *__restrict__ tw, const int32_t *__restrict__ st2ed) {
+                const T *__restrict__ tw, const int32_t *__restrict__ st2ed, int mode) {
   __shared__ int32_t src_s[kPredRows];
   const PartDesc pd = parts[blockIdx.y];
-  const int r0 = blockIdx.z * kPredRows;
-  if (r0 >= pd.s) return;
-  const int rows = min(kPredRows, pd.s - r0);
+  // rows and columns this launch covers (PredMode)
+  const bool thin = pd.b <= kPredThinB;
+  int rlo = 0, rhi = pd.s;
+  if (mode == kPredBoundaryRows) rhi = pd.b;
+  if (mode == kPredOwnColumns && !thin) return;
+  if (mode == kPredThickInner) {
+    if (thin) return;
+    rlo = pd.b;
+  }
+  const int r0 = rlo + blockIdx.z * kPredRows;
+  if (r0 >= rhi) return;
+  const int rows = min(kPredRows, rhi - r0);
   if (threadIdx.x < rows) src_s[threadIdx.x] = __ldg(st2ed + pd.start + r0 + threadIdx.x);
   __syncthreads();
   const T inf = Dist<T>::inf();
-  const int j = blockIdx.x * kPredThreads + threadIdx.x;
+  const int jj = blockIdx.x * kPredThreads + threadIdx.x;
+  int j = jj;
+  if (mode == kPredOwnColumns) {
+    if (jj >= pd.s) return;
+    j = __ldg(st2ed + pd.start + jj);
+  }
   if (j >= n) return;
   // the column's in-edges, read once for all of the CTA's rows
   const int e0 = __ldg(tro + j), e1 = __ldg(tro + j + 1);
@@ -828,14 +842,122 @@ __global__ void __launch_bounds__(kPredThreads)
   }
 }
 
+// Inner rows of parts with b <= kPredThinB, all columns: the predecessor of
+// j on the path through the boundary vertex k* that the min-plus merge
+// chose (the first k with the least F[i][k] + D[k][j]) is the predecessor
+// on k*'s row: P[i][j] = P[k*][j] (-1 where unreachable).  A CTA owns a
+// strip of kPredStrip columns of one part and a block of up to 128 inner
+// rows: the strip of the b boundary rows sits in registers (distances) and
+// shared memory (predecessors), the rows' F values in shared memory; every
+// warp stores 512 contiguous bytes per row.  Own-part columns are left for
+// the own-column pass (their decode is the closure, not a min-plus).
+constexpr int kPredStrip = 4 * kPredThreads;
+
+template <typename T, int B>
+__device__ __forceinline__ void pred_thin_rows(const PartDesc &pd, const T *D, int32_t *P, int64_t ldD,
+                                               int64_t c0, bool live, int m0, int rows,
+                                               const T (*As)[kPredThinB], const int32_t (*Ps)[kPredStrip]) {
+  using V = typename Vec4<T>::type;
+  const T inf = Dist<T>::inf();
+  T sv[B > 0 ? B : 1][4];
+#pragma unroll
+  for (int k = 0; k < B; k++) {
+    V v;
+    if (live) v = __ldg(reinterpret_cast<const V *>(D + (pd.row_base + k) * ldD + c0));
+    else v.x = v.y = v.z = v.w = inf;
+    sv[k][0] = v.x; sv[k][1] = v.y; sv[k][2] = v.z; sv[k][3] = v.w;
+  }
+  const int cl = 4 * threadIdx.x;
+  for (int r = 0; r < rows; r++) {
+    T best[4];
+    int arg[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      best[q] = inf;
+      arg[q] = -1;
+    }
+#pragma unroll
+    for (int k = 0; k < B; k++) {
+      const T a = As[r][k];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const T v = a + sv[k][q];
+        if (v < best[q]) {
+          best[q] = v;
+          arg[q] = k;
+        }
+      }
+    }
+    int4 out;
+    out.x = arg[0] >= 0 ? Ps[arg[0] > 0 ? arg[0] : 0][cl + 0] : -1;
+    out.y = arg[1] >= 0 ? Ps[arg[1] > 0 ? arg[1] : 0][cl + 1] : -1;
+    out.z = arg[2] >= 0 ? Ps[arg[2] > 0 ? arg[2] : 0][cl + 2] : -1;
+    out.w = arg[3] >= 0 ? Ps[arg[3] > 0 ? arg[3] : 0][cl + 3] : -1;
+    if (live) __stcs(reinterpret_cast<int4 *>(P + (pd.row_base + pd.b + m0 + r) * ldD + c0), out);
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kPredThreads)
+    pred_thin_kernel(const PartDesc *__restrict__ parts, const T *__restrict__ F, const T *D, int32_t *P,
+                     int64_t ldD) {
+  extern __shared__ __align__(16) unsigned char pt_smem_raw[];
+  int32_t (*Ps)[kPredStrip] = reinterpret_cast<int32_t (*)[kPredStrip]>(pt_smem_raw);
+  T (*As)[kPredThinB] =
+      reinterpret_cast<T (*)[kPredThinB]>(pt_smem_raw + sizeof(int32_t) * kPredThinB * kPredStrip);
+  const PartDesc pd = parts[blockIdx.y];
+  if (pd.b > kPredThinB) return;
+  const int m0 = blockIdx.z * 128;
+  const int M = pd.s - pd.b;
+  if (m0 >= M) return;
+  const int rows = min(128, M - m0);
+  const int64_t c0 = (int64_t)blockIdx.x * kPredStrip + 4 * threadIdx.x;
+  const bool live = c0 < ldD;  // ldD is a multiple of 4
+  for (int t = threadIdx.x; t < 128 * kPredThinB; t += blockDim.x) {
+    const int r = t / kPredThinB, k = t % kPredThinB;
+    As[r][k] = (r < rows && k < pd.b) ? __ldg(F + pd.f_off + (int64_t)(pd.b + m0 + r) * pd.ldf + k)
+                                      : Dist<T>::inf();
+  }
+  for (int k = 0; k < pd.b; k++) {
+    int4 v = make_int4(-1, -1, -1, -1);
+    if (live) v = *reinterpret_cast<const int4 *>(P + (pd.row_base + k) * ldD + c0);
+    *reinterpret_cast<int4 *>(&Ps[k][4 * threadIdx.x]) = v;
+  }
+  __syncthreads();
+  switch (pd.b) {
+#define FAPB_PRED_CASE(NB) \
+  case NB: pred_thin_rows<T, NB>(pd, D, P, ldD, c0, live, m0, rows, As, Ps); break;
+    FAPB_PRED_CASE(0) FAPB_PRED_CASE(1) FAPB_PRED_CASE(2) FAPB_PRED_CASE(3) FAPB_PRED_CASE(4)
+    FAPB_PRED_CASE(5) FAPB_PRED_CASE(6) FAPB_PRED_CASE(7) FAPB_PRED_CASE(8) FAPB_PRED_CASE(9)
+    FAPB_PRED_CASE(10) FAPB_PRED_CASE(11) FAPB_PRED_CASE(12)
+#undef FAPB_PRED_CASE
+    default: break;
+  }
+}
+
 template <typename T>
 cudaError_t launch_pred(const PartDesc *parts, int nparts, int max_s, const T *D, int32_t *P,
                         int64_t ldD, int n, const int32_t *tro, const int32_t *tcol, const T *tw,
-                        const int32_t *st2ed, cudaStream_t stream, int64_t *launches) {
+                        const int32_t *st2ed, const T *F, cudaStream_t stream, int64_t *launches) {
   if (nparts <= 0 || max_s <= 0 || n <= 0) return cudaSuccess;
-  dim3 grid((unsigned)ceil_div(n, kPredThreads), (unsigned)nparts, (unsigned)ceil_div(max_s, kPredRows));
-  pred_kernel<T><<<grid, kPredThreads, 0, stream>>>(parts, D, P, ldD, n, tro, tcol, tw, st2ed);
-  *launches += 1;
+  const unsigned gz = (unsigned)ceil_div(max_s, kPredRows);
+  // 1. boundary rows, all columns (the gather rule)
+  pred_kernel<T><<<dim3((unsigned)ceil_div(n, kPredThreads), nparts, gz), kPredThreads, 0, stream>>>(
+      parts, D, P, ldD, n, tro, tcol, tw, st2ed, kPredBoundaryRows);
+  // 2. inner rows of thin parts from the min-plus argmin (own columns redone by 3)
+  const size_t smem = sizeof(int32_t) * kPredThinB * kPredStrip + sizeof(T) * 128 * kPredThinB;
+  cudaError_t e =
+      cudaFuncSetAttribute(pred_thin_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  pred_thin_kernel<T><<<dim3((unsigned)ceil_div(ldD, kPredStrip), nparts, (unsigned)ceil_div(max_s, 128)),
+                        kPredThreads, smem, stream>>>(parts, F, D, P, ldD);
+  // 3. own-part columns of thin parts (the gather rule)
+  pred_kernel<T><<<dim3((unsigned)ceil_div(max_s, kPredThreads), nparts, gz), kPredThreads, 0, stream>>>(
+      parts, D, P, ldD, n, tro, tcol, tw, st2ed, kPredOwnColumns);
+  // 4. inner rows of the other parts (the gather rule)
+  pred_kernel<T><<<dim3((unsigned)ceil_div(n, kPredThreads), nparts, gz), kPredThreads, 0, stream>>>(
+      parts, D, P, ldD, n, tro, tcol, tw, st2ed, kPredThickInner);
+  *launches += 4;
   return cudaGetLastError();
 }
 
@@ -1376,7 +1498,7 @@ cudaError_t launch_relax_peak(T *sink, int blocks, int iters, cudaStream_t strea
                                              cudaStream_t, int64_t *);                             \
   template cudaError_t launch_pred<T>(const PartDesc *, int, int, const T *, int32_t *, int64_t,  \
                                       int, const int32_t *, const int32_t *, const T *,            \
-                                      const int32_t *, cudaStream_t, int64_t *);                   \
+                                      const int32_t *, const T *, cudaStream_t, int64_t *);        \
   template cudaError_t launch_bdy_copy<T>(const PartDesc *, int, int, const T *, T *, int64_t,    \
                                           cudaStream_t, int64_t *);                               \
   template cudaError_t launch_row_gather<T>(const T *, int64_t, const int64_t *, int64_t, int, T *, \

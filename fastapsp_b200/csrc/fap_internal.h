@@ -126,14 +126,27 @@ cudaError_t launch_minplus_thin(const PartDesc *parts, const int32_t *thin_parts
                                 int n, const T *F, T *D, int64_t ldD, const int32_t *graph_id,
                                 const int32_t *ed2st, cudaStream_t stream, int64_t *launches);
 
-// Predecessor rows of the listed parts' output rows: P[row][j] = the
-// in-neighbour u of j (in-edge CSR tro/tcol/tw) with the least D[row][u] +
-// w(u, j), the smallest u on ties; the row's vertex maps to itself, an
-// unreachable j to -1.  max_s bounds the parts' sizes.
+// Predecessor rows of the listed parts' output rows (max_s bounds the
+// parts' sizes).  The gather rule: P[row][j] = the in-neighbour u of j
+// (in-edge CSR tro/tcol/tw) with the least D[row][u] + w(u, j), the
+// smallest u on ties; the row's vertex maps to itself, an unreachable j to
+// -1.  It gives the boundary rows, the own-part columns, and every row of
+// parts with more than kPredThinB boundary vertices.  Inner rows of the
+// other parts take, for columns outside their part, the predecessor on the
+// row of the boundary vertex k* that the min-plus merge chose (the first k
+// with the least F[i][k] + D[k][j]): P[i][j] = P[k*][j].  F is the batch's
+// closed Floyd arena.
+constexpr int kPredThinB = 12;
+enum PredMode : int {
+  kPredAll = 0,           // every row, every column
+  kPredBoundaryRows = 1,  // rows < b, every column
+  kPredOwnColumns = 2,    // every row, own-part columns, parts with b <= kPredThinB
+  kPredThickInner = 3,    // rows >= b, every column, parts with b > kPredThinB
+};
 template <typename T>
 cudaError_t launch_pred(const PartDesc *parts, int nparts, int max_s, const T *D, int32_t *P,
                         int64_t ldD, int n, const int32_t *tro, const int32_t *tcol, const T *tw,
-                        const int32_t *st2ed, cudaStream_t stream, int64_t *launches);
+                        const int32_t *st2ed, const T *F, cudaStream_t stream, int64_t *launches);
 
 // Boundary-graph form of stage 1 (exact shortest distances from boundary
 // vertices without SSSP).  With every part's local closure in F:

@@ -270,7 +270,10 @@ def row_checksums(block_i32: np.ndarray) -> np.ndarray:
 # least dist[u] + w(u, j) (the smallest u among equal sums): the same meaning,
 # a fixed rule on ties.  port_predecessors restates that rule;
 # tests/test_oracle.py pins it to the reference's own matrices on every entry
-# whose predecessor is unique.
+# whose predecessor is unique.  For the inner rows of parts with few
+# boundary vertices the B200 path takes the predecessor off the min-plus
+# choice instead (port_predecessors_block), again a valid shortest path that
+# agrees wherever the predecessor is unique.
 
 def in_edges(row_offset, col, weight):
     """(tro, tcol, tw): the CSR of in-edges (j's sources in tcol[tro[j]:
@@ -321,6 +324,65 @@ def port_predecessors(dist_rows, row_vertices, row_offset, col, weight, integral
     P = np.where(reach, P, -1)
     P[np.arange(R), np.asarray(row_vertices)] = np.asarray(row_vertices)
     return P.astype(np.int32)
+
+
+PRED_THIN_B = 12   # parts with at most this many boundary vertices use the argmin rule
+
+
+def port_predecessors_block(block, part_vertices, b: int, row_offset, col, weight, integral: bool,
+                            thin_b: int = PRED_THIN_B):
+    """Predecessor rows of one part's solved block (rows in sorted order:
+    the part's b boundary vertices first), as the B200 path produces them:
+    boundary rows, own-part columns and parts with more than thin_b boundary
+    vertices follow port_predecessors (the in-edge argmin); the inner rows of
+    the other parts take, for columns outside the part, the predecessor on
+    the row of the boundary vertex k* that the min-plus merge chose -- the
+    first k with the least F[i][k] + D[k][j] (F[i][k] = block[i][vertex of
+    boundary k], the closed distance the decode wrote) -- or -1 when that
+    least sum is the sentinel."""
+    D = np.asarray(block)
+    verts = np.asarray(part_vertices, np.int64)
+    P = port_predecessors(D, verts, row_offset, col, weight, integral).astype(np.int64)
+    s, n = D.shape
+    if b > thin_b or s <= b:
+        return P.astype(np.int32)
+    own = np.zeros(n, bool)
+    own[verts] = True
+    inner = np.arange(b, s)
+    if b == 0:
+        P[np.ix_(inner, np.nonzero(~own)[0])] = -1
+        return P.astype(np.int32)
+    if integral:
+        A = D[inner][:, verts[:b]].astype(np.int64)
+        S = D[:b].astype(np.int64)
+        inf = 100000000
+    else:
+        A = D[inner][:, verts[:b]].astype(np.float32)
+        S = D[:b].astype(np.float32)
+        inf = np.float32(1e8)
+    sums = A[:, :, None] + S[None, :, :]          # inner x b x n
+    k_star = np.argmin(sums, axis=1)               # first least k
+    best = np.take_along_axis(sums, k_star[:, None, :], axis=1)[:, 0, :]
+    Pi = P[:b][k_star, np.arange(n)[None, :]]
+    Pi = np.where(best < inf, Pi, -1)
+    cols = np.nonzero(~own)[0]
+    P[np.ix_(inner, cols)] = Pi[:, cols]
+    return P.astype(np.int32)
+
+
+def port_predecessors_parts(dist_sorted, st2ed, ver_num, ver_offset, bdy_num, row_offset, col, weight,
+                            integral: bool, thin_b: int = PRED_THIN_B):
+    """port_predecessors_block over every part of a full n x n matrix in
+    sorted row order."""
+    D = np.asarray(dist_sorted)
+    out = np.empty(D.shape, np.int32)
+    for p in range(1, len(ver_num)):
+        off, s = int(ver_offset[p]), int(ver_num[p])
+        if s == 0:
+            continue
+        out[off:off + s] = port_predecessors_block(D[off:off + s], st2ed[off:off + s], int(bdy_num[p]),
+                                                   row_offset, col, weight, integral, thin_b)
+    return out
 
 
 def unique_predecessor_mask(dist_rows, row_vertices, row_offset, col, weight, integral: bool,

@@ -92,5 +92,7 @@ def test_boundary_graph_with_paths(cuda_ok, name):
     D = _blocks(dg, K)
     P = np.concatenate([dg.copy_path_block(p) for p in range(1, K + 1)], 0)
     args = (case["st2ed"], case["row_offset"], case["col_val"], case["weight"], bool(case["integral"]))
-    np.testing.assert_array_equal(P, O.port_predecessors(D, *args))
+    want = O.port_predecessors_parts(D, case["st2ed"], case["ver_num"], case["ver_offset"],
+                                     case["bdy_num"], *args[1:])
+    np.testing.assert_array_equal(P, want)
     assert O.check_paths(D, P, *args) > 0

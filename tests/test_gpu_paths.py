@@ -1,7 +1,7 @@
 """Predecessor (path) matrices on the GPU, through the C ABI.
 
-For every golden fixture: the predecessor rows equal the rule's restatement
-(oracle.port_predecessors on the same distances) bit for bit, equal the
+For every golden fixture: the predecessor rows equal the rules' restatement
+(oracle.port_predecessors_parts on the same distances) bit for bit, equal the
 reference's own predecessor matrix wherever the predecessor is unique, and
 pass the validity check (edge, distance equation, chain back to the source)
 on graphs without duplicate edges; the same in the plain form, the batched
@@ -53,8 +53,11 @@ def _duplicate_free(case):
 def _check_case(case, D, P):
     integral = bool(case["integral"])
     args = (case["st2ed"], case["row_offset"], case["col_val"], case["weight"], integral)
-    # the rule, restated on the CPU over the same distances: bit-exact
-    np.testing.assert_array_equal(P, O.port_predecessors(D, *args))
+    # the rules, restated on the CPU over the same distances: bit-exact
+    want = O.port_predecessors_parts(D, case["st2ed"], case["ver_num"], case["ver_offset"],
+                                     case["bdy_num"], case["row_offset"], case["col_val"],
+                                     case["weight"], integral)
+    np.testing.assert_array_equal(P, want)
     # the reference's own predecessors wherever the predecessor is unique
     U = O.unique_predecessor_mask(case["dist"], *args)
     np.testing.assert_array_equal(P[U], case["path"][U])
@@ -85,6 +88,9 @@ def test_paths_on_grid64_sample_rows(cuda_ok):
     dg.set_param("paths", 1)
     dg.solve(mode=FAP_MODE_BATCHED)
     D, P = _all_rows(dg, K)
+    # every part has more boundary vertices than the min-plus rule's limit, so
+    # every row follows the in-edge rule
+    assert int(case["bdy_num"][1:].min()) > O.PRED_THIN_B
     rows = np.sort(np.random.default_rng(4).choice(int(case["n"]), 48, replace=False))
     args = (case["st2ed"][rows], case["row_offset"], case["col_val"], case["weight"], True)
     np.testing.assert_array_equal(P[rows], O.port_predecessors(D[rows], *args))

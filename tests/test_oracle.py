@@ -170,3 +170,20 @@ def test_check_paths_catches_a_planted_error():
     P[r, j] = c["st2ed"][r]          # the source is not adjacent to j
     with pytest.raises(AssertionError):
         O.check_paths(c["dist"], P, *args)
+
+
+@pytest.mark.parametrize("name", _path_names())
+def test_min_plus_predecessor_rule_matches_reference_paths(name):
+    """The rule the GPU uses for inner rows of parts with few boundary
+    vertices (the predecessor on the row of the boundary vertex the min-plus
+    merge chose), applied to the reference's distances: equal to the
+    reference's predecessors wherever unique, valid everywhere (graphs
+    without duplicate arcs)."""
+    c = load_golden(name)
+    integral = bool(c["integral"])
+    args = (c["row_offset"], c["col_val"], c["weight"], integral)
+    P = O.port_predecessors_parts(c["dist"], c["st2ed"], c["ver_num"], c["ver_offset"], c["bdy_num"], *args)
+    U = O.unique_predecessor_mask(c["dist"], c["st2ed"], *args)
+    np.testing.assert_array_equal(P[U], c["path"][U])
+    if _duplicate_free(c):
+        assert O.check_paths(c["dist"], P, c["st2ed"], *args) > 0
