@@ -54,6 +54,10 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-procs", type=int, default=0, help="0 = min(cores, memory bound)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-stream measurement")
+    ap.add_argument("--stage1", type=int, default=0, choices=[0, 1, 2],
+                    help="stage 1 form: 0 automatic, 1 SSSP, 2 boundary graph")
+    ap.add_argument("--sssp-form", type=int, default=0, choices=[0, 1, 2],
+                    help="SSSP form of stage 1: 0 automatic, 1 frontier, 2 tiled Bellman-Ford")
     ap.add_argument("--paths", action="store_true",
                     help="also time batched solves that produce predecessor matrices")
     ap.add_argument("--serve-graphs", type=int, default=32)
@@ -440,6 +444,8 @@ def main_fap(args):
         for grp in groups:
             dg.solve(grp, mode, check_errors=False)
     from fastapsp_b200 import autotune
+    dg.set_param("stage1", args.stage1)
+    dg.set_param("sssp_form", args.sssp_form)
     tuned = autotune.tune_sssp(dg, vn, bn)
     log(f"SSSP delta {tuned['delta']:.6g} ({'cached' if tuned['cached'] else 'tuned'}: "
         f"{tuned['key']}, factor {tuned['factor']})")
@@ -487,6 +493,10 @@ def main_fap(args):
     ms_per_step = max_ms / args.steps
     value = total_entries * args.steps / (max_ms * 1e-3)
     st = np.mean(np.stack(stages), 0)  # [sssp, gather, floyd, minplus, total]
+    stage1_used = {1: "SSSP", 2: "boundary graph", 3: "resident cache"}.get(dg.last_stage1(), "?")
+    if stage1_used == "SSSP":
+        stage1_used += " (tiled Bellman-Ford)" if (args.sssp_form == 2 or (
+            args.sssp_form == 0 and int(ro[-1]) >= 6 * n)) else " (frontier)"
     log(f"batched: {ms_per_step:.3f} ms/step, stages {np.round(st, 3).tolist()}, "
         f"{value:.4g} entries/s")
 
@@ -633,7 +643,8 @@ def main_fap(args):
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
             "dtype": "int32" if dtype == 0 else "f32",
             "data": wl.data_description(),
-            "config": {**wl.describe(), "mode": "batched", "parallelism": f"parts sharded x{world}",
+            "config": {**wl.describe(), "mode": "batched", "stage1": stage1_used,
+                       "parallelism": f"parts sharded x{world}",
                        "groups": len(groups),
                        "sssp_delta": {"value": tuned["delta"], "factor_of_mean_weight": tuned["factor"],
                                       "bucket": tuned["key"], "from_cache": tuned["cached"]},

@@ -192,6 +192,13 @@ struct fap_dgraph {
   bool cache_bmethod = false;  // the resident cache was built with it
   int64_t ldB = 0;
   DevBuf d_dB, d_bpart, d_brows, d_FB;
+  // Tiled form of stage 1's SSSP (launch_msbf): 0 automatic (graphs with at
+  // least 6 arcs per vertex, where few Bellman-Ford iterations suffice), 1
+  // frontier kernel, 2 tiled.  Work items over the in-edge CSR.
+  int sssp_form = 0;
+  DevBuf d_msbf_items, d_msbf_act, d_msbf_changed;
+  int msbf_nitems = 0;
+  int *h_changed = nullptr;  // pinned, 4 ints
   // Predecessor matrices: P has D's shape; the in-edge CSR (tro/tcol/tw)
   // is built when paths are switched on; path_ok[p]: p's resident block has
   // its predecessor rows.
@@ -398,8 +405,10 @@ extern "C" int fap_graph_destroy(fap_dgraph *G) {
     for (DevBuf *b : {&G->ro, &G->col, &G->w, &G->ro_s, &G->col_s, &G->w_s, &G->sssp_scratch, &G->d_thin,
                       &G->d_gid, &G->d_st2ed, &G->d_ed2st, &G->D, &G->F, &G->d_parts, &G->d_work,
                       &G->d_src, &G->d_srcrows, &G->d_status, &G->d_checks, &G->staging, &G->P,
-                      &G->d_tro, &G->d_tcol, &G->d_tw, &G->d_dB, &G->d_bpart, &G->d_brows, &G->d_FB})
+                      &G->d_tro, &G->d_tcol, &G->d_tw, &G->d_dB, &G->d_bpart, &G->d_brows, &G->d_FB,
+                      &G->d_msbf_items, &G->d_msbf_act, &G->d_msbf_changed})
       b->release();
+    if (G->h_changed) cudaFreeHost(G->h_changed);
     cache_drop(G);
   }
   delete G;
@@ -678,6 +687,58 @@ int launch_paths(fap_dgraph *G, const PartDesc *dp, int np, int max_s, const T *
   return FAP_OK;
 }
 
+int ensure_in_edges(fap_dgraph *G);
+
+// Whether stage 1's SSSP runs in the tiled form.
+bool use_msbf(const fap_dgraph *G) {
+  if (G->sssp_form == 1) return false;
+  if (G->sssp_form == 2) return true;
+  return G->n > 0 && G->m >= 6 * (int64_t)G->n;
+}
+
+// Work items, bitmaps and the pinned convergence flags of the tiled form.
+int prepare_msbf(fap_dgraph *G) {
+  FAP_TRY(ensure_in_edges(G));
+  if (G->msbf_nitems == 0) {
+    std::vector<int32_t> tro((size_t)G->n + 1);
+    FAP_CK(cudaMemcpy(tro.data(), G->d_tro.p, tro.size() * 4, cudaMemcpyDeviceToHost));
+    std::vector<MsbfItem> items;
+    for (int32_t v = 0; v < G->n; v++)
+      for (int32_t e = tro[v]; e < tro[v + 1]; e += 32) items.push_back(MsbfItem{v, e});
+    FAP_TRY(G->d_msbf_items.ensure(std::max<size_t>(items.size(), 1) * sizeof(MsbfItem)));
+    if (!items.empty())
+      FAP_CK(cudaMemcpy(G->d_msbf_items.p, items.data(), items.size() * sizeof(MsbfItem), cudaMemcpyHostToDevice));
+    G->msbf_nitems = (int)items.size();
+  }
+  FAP_TRY(G->d_msbf_act.ensure((size_t)2 * ceil_div(G->n, 32) * 4));
+  FAP_TRY(G->d_msbf_changed.ensure(4 * sizeof(int)));
+  if (!G->h_changed) FAP_CK(cudaHostAlloc(reinterpret_cast<void **>(&G->h_changed), 4 * sizeof(int), 0));
+  FAP_TRY(G->sssp_scratch.ensure((size_t)G->n * kMsbfS * 4));
+  return FAP_OK;
+}
+
+// Stage 1's SSSP from `count` sources (sorted positions) into rows srow of
+// D (ld ldD, all ldD columns): the tiled form or the frontier kernel.
+template <typename T>
+int run_stage1_sssp(fap_dgraph *G, const int32_t *src, const int64_t *srow, int count, T *D, int *status,
+                    int64_t max_rounds, int64_t *L) {
+  cudaStream_t st = G->ctx->stream;
+  if (use_msbf(G)) {
+    FAP_TRY(prepare_msbf(G));
+    FAP_CK(launch_msbf<T>(G->d_msbf_items.as<const MsbfItem>(), G->msbf_nitems, G->d_tro.as<const int32_t>(),
+                          G->d_tcol.as<const int32_t>(), G->d_tw.as<const T>(), G->n,
+                          G->d_st2ed.as<const int32_t>(), src, srow, count, D, G->ldD, G->ldD,
+                          G->sssp_scratch.as<T>(), G->d_msbf_act.as<uint32_t>(), G->d_msbf_changed.as<int>(),
+                          G->h_changed, max_rounds, status, st, L));
+    return FAP_OK;
+  }
+  FAP_CK(launch_sssp<T>(G->ro_s.as<const int32_t>(), G->col_s.as<const int32_t>(), G->w_s.as<const T>(), G->n,
+                        src, srow, count, D, G->ldD, G->ldD, G->d_ed2st.as<const int32_t>(),
+                        G->sssp_scratch.as<T>(), sssp_delta_for<T>(G), G->sssp_chain, G->sssp_precheck,
+                        max_rounds, status, st, L));
+  return FAP_OK;
+}
+
 template <typename T>
 int run_solve(fap_dgraph *G, int mode) {
   fap_ctx *c = G->ctx;
@@ -744,8 +805,7 @@ int run_solve(fap_dgraph *G, int mode) {
     FAP_CK(record_event(c->ev[4], st));
   } else if (mode == FAP_MODE_BATCHED) {
     FAP_CK(record_event(c->ev[0], st));
-    FAP_CK(launch_sssp<T>(ro_s, col_s, w_s, G->n, src, srow, (int)G->src.size(), D, G->ldD, G->ldD,
-                          ed2st, scratch, delta, G->sssp_chain, G->sssp_precheck, max_rounds, status, st, &L));
+    FAP_TRY(run_stage1_sssp<T>(G, src, srow, (int)G->src.size(), D, status, max_rounds, &L));
     FAP_CK(record_event(c->ev[1], st));
     FAP_CK(launch_gather<T>(dp, np, G->max_ldf, ro, col, w, gid, st2ed, ed2st, D, G->ldD, F, st, &L));
     FAP_CK(record_event(c->ev[2], st));
@@ -837,7 +897,9 @@ extern "C" int fap_solve(fap_dgraph *G, const int32_t *parts, int32_t count, int
   FAP_TRY(prepare_batch(G, ids, cached, bmethod));
   int rc = FAP_OK;
   cudaStream_t st = G->ctx->stream;
-  if (mode == FAP_MODE_BATCHED && G->use_graph && st != nullptr) {
+  // (the tiled SSSP form tests convergence on the host: not capturable)
+  const bool host_loop = !cached && !bmethod && use_msbf(G);
+  if (mode == FAP_MODE_BATCHED && G->use_graph && st != nullptr && !host_loop) {
     if (!G->gexec || G->gexec_epoch != G->epoch || G->gexec_stream != st) {
       if (G->gexec) cudaGraphExecDestroy(G->gexec);
       G->gexec = nullptr;
@@ -1225,6 +1287,8 @@ extern "C" int fap_graph_sssp_rows(fap_dgraph *G, const int32_t *sources, int32_
 }
 
 namespace {
+int ensure_in_edges(fap_dgraph *G);
+
 // Switches predecessor matrices on: checks that every weight is positive
 // (with zero-weight edges, equal distances would not order the
 // predecessors), then builds the in-edge CSR (sources ascending per vertex).
@@ -1244,6 +1308,14 @@ int enable_paths(fap_dgraph *G) {
     }
     if (!pos) return fail(FAP_ERR_RANGE, "paths need positive edge weights (edge %lld)", (long long)e);
   }
+  FAP_TRY(ensure_in_edges(G));
+  G->paths = true;
+  return FAP_OK;
+}
+
+// The in-edge CSR (sources ascending per vertex, original ids), built once.
+int ensure_in_edges(fap_dgraph *G) {
+  const int64_t m = (int64_t)G->h_col.size() < G->m ? (int64_t)G->h_col.size() : G->m;
   if (G->d_tro.bytes == 0) {
     const int32_t n = G->n;
     std::vector<int32_t> tro((size_t)n + 1, 0), tcol((size_t)std::max<int64_t>(m, 1));
@@ -1266,7 +1338,6 @@ int enable_paths(fap_dgraph *G) {
     FAP_CK(cudaMemcpy(G->d_tcol.p, tcol.data(), tcol.size() * 4, cudaMemcpyHostToDevice));
     FAP_CK(cudaMemcpy(G->d_tw.p, tw.data(), tw.size() * 4, cudaMemcpyHostToDevice));
   }
-  G->paths = true;
   return FAP_OK;
 }
 }  // namespace
@@ -1288,6 +1359,11 @@ extern "C" int fap_graph_set_param(fap_dgraph *G, const char *key, double value)
   }
   if (std::strcmp(key, "sssp_chain") == 0) {
     G->sssp_chain = value >= 0 ? (int)value : 0;
+    return FAP_OK;
+  }
+  if (std::strcmp(key, "sssp_form") == 0) {
+    if (value != 0.0 && value != 1.0 && value != 2.0) return fail(FAP_ERR_INVALID, "sssp_form is 0, 1 or 2");
+    G->sssp_form = (int)value;
     return FAP_OK;
   }
   if (std::strcmp(key, "stage1") == 0) {
@@ -1426,7 +1502,8 @@ extern "C" int fap_graph_device_bytes(const fap_dgraph *G, int64_t *bytes) {
                           &G->d_work, &G->d_src, &G->d_srcrows, &G->d_status, &G->d_checks, &G->staging,
                           &G->cBd, &G->cF, &G->d_cparts, &G->d_rowgroups, &G->d_rowloc, &G->d_rowout,
                           &G->d_rowidx, &G->P, &G->d_tro, &G->d_tcol, &G->d_tw, &G->d_dB,
-                          &G->d_bpart, &G->d_brows, &G->d_FB})
+                          &G->d_bpart, &G->d_brows, &G->d_FB, &G->d_msbf_items, &G->d_msbf_act,
+                          &G->d_msbf_changed})
     t += (int64_t)b->bytes;
   *bytes = t;
   return FAP_OK;
@@ -1537,10 +1614,8 @@ int cache_build_impl(fap_dgraph *G) {
     FAP_CK(launch_local_fixup<T>(dp, K, cs.max_s, F, G->d_FB.as<const T>(), cs.ldf, st, &L));
     G->cache_bmethod = true;
   } else {
-  FAP_CK(launch_sssp<T>(G->ro_s.as<const int32_t>(), G->col_s.as<const int32_t>(), G->w_s.as<const T>(),
-                        G->n, G->d_src.as<const int32_t>(), G->d_srcrows.as<const int64_t>(),
-                        (int)src.size(), Bd, G->ldD, G->ldD, ed2st, G->sssp_scratch.as<T>(),
-                        sssp_delta_for<T>(G), G->sssp_chain, G->sssp_precheck, rounds, status, st, &L));
+  FAP_TRY(run_stage1_sssp<T>(G, G->d_src.as<const int32_t>(), G->d_srcrows.as<const int64_t>(),
+                             (int)src.size(), Bd, status, rounds, &L));
   FAP_CK(launch_gather<T>(dp, K, cs.ldf, G->ro.as<const int32_t>(), G->col.as<const int32_t>(),
                           G->w.as<const T>(), gid, st2ed, ed2st, Bd, G->ldD, F, st, &L));
   G->cache_bmethod = false;

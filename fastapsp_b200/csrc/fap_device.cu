@@ -198,6 +198,166 @@ cudaError_t launch_sssp(const int32_t *row_offset, const int32_t *col, const T *
 }
 
 // ---------------------------------------------------------------------------
+// Stage 1, tiled form: multi-source Bellman-Ford over in-edges
+// ---------------------------------------------------------------------------
+// kMsbfS sources at a time share one pass over the graph per iteration.  The
+// tile Dt[v][s] (vertex-major, the sources of a vertex contiguous: one
+// 16-byte load per lane for a whole row) stays in L2 on mid-size graphs.  An
+// iteration pulls, for every work item (a vertex and up to 32 of its
+// in-edges), only from in-neighbours that changed in the previous iteration,
+// and lowers the vertex's row with atomic minima where it improves; the tile
+// is updated in place, so values are monotone and the fixed point is the
+// exact shortest distances, each the sum along its path edge by edge (the
+// same additions in the same order as Dijkstra's).  The host repeats
+// iterations until one changes nothing (or the round bound is reached).
+template <typename T>
+__global__ void msbf_seed_kernel(T *Dt, const int32_t *__restrict__ sources, const int32_t *__restrict__ st2ed,
+                                 int ns, uint32_t *act) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= ns) return;
+  const int v = __ldg(st2ed + __ldg(sources + s));
+  Dt[(int64_t)v * kMsbfS + s] = T(0);
+  atomicOr(act + (v >> 5), 1u << (v & 31));
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+    msbf_iter_kernel(T *Dt, const MsbfItem *__restrict__ items, int nitems, const int32_t *__restrict__ tro,
+                     const int32_t *__restrict__ tcol, const T *__restrict__ tw, const uint32_t *__restrict__ act_cur,
+                     uint32_t *act_next, int *changed) {
+  using V = typename Vec4<T>::type;
+  const T inf = Dist<T>::inf();
+  const int lane = threadIdx.x & 31;
+  const int nwarps = gridDim.x * (blockDim.x >> 5);
+  for (int it = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < nitems; it += nwarps) {
+    const MsbfItem m = items[it];
+    const int e1 = min(m.e0 + 32, __ldg(tro + m.v + 1));
+    const int e = m.e0 + lane;
+    int u = -1;
+    T w = T(0);
+    if (e < e1) {
+      u = __ldg(tcol + e);
+      if ((__ldcg(act_cur + (u >> 5)) >> (u & 31)) & 1u) w = __ldg(tw + e);
+      else u = -1;
+    }
+    unsigned mask = __ballot_sync(0xffffffffu, u >= 0);
+    if (!mask) continue;
+    T acc[4] = {inf, inf, inf, inf};
+    while (mask) {  // warp-uniform: four active in-edges per step, loads in flight together
+      int uu[4];
+      T ww[4];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        uu[q] = -1;
+        ww[q] = T(0);
+        if (mask) {
+          const int k = __ffs(mask) - 1;
+          mask &= mask - 1;
+          uu[q] = __shfl_sync(0xffffffffu, u, k);
+          ww[q] = __shfl_sync(0xffffffffu, w, k);
+        }
+      }
+      V d[4];
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+        if (uu[q] >= 0) d[q] = __ldcg(reinterpret_cast<const V *>(Dt + (int64_t)uu[q] * kMsbfS) + lane);
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+        if (uu[q] >= 0) {
+          acc[0] = Dist<T>::relax(d[q].x, ww[q], acc[0]);
+          acc[1] = Dist<T>::relax(d[q].y, ww[q], acc[1]);
+          acc[2] = Dist<T>::relax(d[q].z, ww[q], acc[2]);
+          acc[3] = Dist<T>::relax(d[q].w, ww[q], acc[3]);
+        }
+    }
+    T *row = Dt + (int64_t)m.v * kMsbfS + 4 * lane;
+    const V cur = __ldcg(reinterpret_cast<const V *>(row));
+    const T cv[4] = {cur.x, cur.y, cur.z, cur.w};
+    bool imp = false;
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+      if (acc[q] < cv[q]) imp |= acc[q] < Dist<T>::atomic_min(row + q, acc[q]);
+    if (__any_sync(0xffffffffu, imp) && lane == 0) {
+      atomicOr(act_next + (m.v >> 5), 1u << (m.v & 31));
+      *changed = 1;
+    }
+  }
+}
+
+// out[out_rows[s]][v] = Dt[v][s] for s < ns, all init_cols columns (INF past
+// n): 32 vertices per CTA, transposed through shared memory, 128-byte row
+// segments stored.
+template <typename T>
+__global__ void __launch_bounds__(256)
+    msbf_store_kernel(const T *__restrict__ Dt, int n, int ns, T *out, int64_t ld, const int64_t *__restrict__ out_rows,
+                      int64_t init_cols) {
+  __shared__ T tile[32][kMsbfS + 1];
+  const int64_t v0 = (int64_t)blockIdx.x * 32;
+  const T inf = Dist<T>::inf();
+  for (int t = threadIdx.x; t < 32 * kMsbfS; t += blockDim.x) {
+    const int vv = t / kMsbfS, s = t % kMsbfS;
+    const int64_t v = v0 + vv;
+    tile[vv][s] = v < n ? __ldcg(Dt + v * kMsbfS + s) : inf;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  for (int s = threadIdx.x >> 5; s < ns; s += blockDim.x >> 5) {
+    const int64_t v = v0 + lane;
+    if (v < init_cols) out[out_rows[s] * ld + v] = tile[lane][s];
+  }
+}
+
+template <typename T>
+cudaError_t launch_msbf(const MsbfItem *items, int nitems, const int32_t *tro, const int32_t *tcol, const T *tw,
+                        int n, const int32_t *st2ed, const int32_t *sources, const int64_t *out_rows,
+                        int num_sources, T *out, int64_t ld, int64_t init_cols, T *Dt, uint32_t *act,
+                        int *changed, int *host_changed, int64_t max_rounds, int *status, cudaStream_t stream,
+                        int64_t *launches) {
+  if (num_sources <= 0) return cudaSuccess;
+  const int64_t words = ceil_div(n, 32);
+  uint32_t *act_a = act, *act_b = act + words;
+  const int iter_blocks = 148 * 8;
+  constexpr int kChunk = 4;  // iterations between convergence checks
+  for (int s0 = 0; s0 < num_sources; s0 += kMsbfS) {
+    const int ns = std::min(kMsbfS, num_sources - s0);
+    cudaError_t e = launch_fill<T>(Dt, n, kMsbfS, kMsbfS, Dist<T>::inf(), stream, launches);
+    if (e == cudaSuccess) e = cudaMemsetAsync(act_a, 0, words * 4, stream);
+    if (e != cudaSuccess) return e;
+    msbf_seed_kernel<T><<<1, kMsbfS, 0, stream>>>(Dt, sources + s0, st2ed, ns, act_a);
+    *launches += 1;
+    bool done = false;
+    for (int64_t round = 0; !done; round += kChunk) {
+      if (round >= max_rounds) {
+        // the bound: report it (the host status path reads it)
+        e = cudaMemcpyAsync(status, &kMsbfRoundLimit, sizeof(int), cudaMemcpyHostToDevice, stream);
+        if (e != cudaSuccess) return e;
+        break;
+      }
+      e = cudaMemsetAsync(changed, 0, kChunk * sizeof(int), stream);
+      if (e != cudaSuccess) return e;
+      for (int c = 0; c < kChunk; c++) {
+        e = cudaMemsetAsync(act_b, 0, words * 4, stream);
+        if (e != cudaSuccess) return e;
+        msbf_iter_kernel<T><<<iter_blocks, 256, 0, stream>>>(Dt, items, nitems, tro, tcol, tw, act_a, act_b,
+                                                            changed + c);
+        *launches += 1;
+        std::swap(act_a, act_b);
+      }
+      e = cudaMemcpyAsync(host_changed, changed, kChunk * sizeof(int), cudaMemcpyDeviceToHost, stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+      if (e != cudaSuccess) return e;
+      for (int c = 0; c < kChunk; c++) done |= host_changed[c] == 0;
+    }
+    msbf_store_kernel<T><<<(unsigned)ceil_div(init_cols, 32), 256, 0, stream>>>(Dt, n, ns, out, ld, out_rows + s0,
+                                                                               init_cols);
+    *launches += 1;
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+// ---------------------------------------------------------------------------
 // Stage 2.2: Floyd-Warshall
 // ---------------------------------------------------------------------------
 template <typename T>
@@ -1465,6 +1625,10 @@ cudaError_t launch_relax_peak(T *sink, int blocks, int iters, cudaStream_t strea
                                       const int32_t *, const int64_t *, int, T *, int64_t,        \
                                       int64_t, const int32_t *, T *, T, int, int, int64_t, int *, \
                                       cudaStream_t, int64_t *);                                   \
+  template cudaError_t launch_msbf<T>(const MsbfItem *, int, const int32_t *, const int32_t *,     \
+                                      const T *, int, const int32_t *, const int32_t *,            \
+                                      const int64_t *, int, T *, int64_t, int64_t, T *, uint32_t *, \
+                                      int *, int *, int64_t, int *, cudaStream_t, int64_t *);      \
   template cudaError_t launch_gather<T>(const PartDesc *, int, int, const int32_t *,              \
                                         const int32_t *, const T *, const int32_t *,              \
                                         const int32_t *, const int32_t *, const T *, int64_t, T *, \

@@ -69,6 +69,27 @@ cudaError_t launch_sssp(const int32_t *row_offset, const int32_t *col, const T *
                         T delta, int chain, int precheck, int64_t max_rounds, int *status,
                         cudaStream_t stream, int64_t *launches);
 
+// Tiled form of stage 1 (multi-source Bellman-Ford over in-edges, kMsbfS
+// sources per tile; see fap_device.cu).  items: the work list, one entry
+// per vertex and chunk of up to 32 in-edges (tro/tcol/tw, original ids);
+// sources are sorted positions (st2ed maps them to vertices); row s of the
+// output is out_rows[s] (original column order, init_cols columns).  Dt
+// holds n x kMsbfS values, act 2 x ceil(n/32) words, changed 4 ints on the
+// device and host_changed 4 ints on the host (the launcher synchronises the
+// stream every 4 iterations to test convergence).
+constexpr int kMsbfS = 128;
+constexpr int kMsbfRoundLimit = 1;  // = kDevSsspRoundLimit
+struct MsbfItem {
+  int32_t v;
+  int32_t e0;
+};
+template <typename T>
+cudaError_t launch_msbf(const MsbfItem *items, int nitems, const int32_t *tro, const int32_t *tcol, const T *tw,
+                        int n, const int32_t *st2ed, const int32_t *sources, const int64_t *out_rows,
+                        int num_sources, T *out, int64_t ld, int64_t init_cols, T *Dt, uint32_t *act,
+                        int *changed, int *host_changed, int64_t max_rounds, int *status, cudaStream_t stream,
+                        int64_t *launches);
+
 // Rows of scratch the relabelled SSSP needs (= CTAs it launches) for
 // num_sources sources on this device.
 int sssp_scratch_rows(int n, int num_sources);
