@@ -151,7 +151,12 @@ FAP_API int fap_graph_sssp_rows(fap_dgraph *g, const int32_t *sources, int32_t c
  * fap_graph_path_block; needs every edge weight > 0, else FAP_ERR_RANGE);
  * "stage1" (0 automatic, the default; 1 always SSSP; 2 the boundary graph
  * whenever the graph allows it, whatever its dtype and boundary count; see
- * fap_graph_last_stage1). */
+ * fap_graph_last_stage1); "sssp_form" (how the SSSP form of stage 1 runs:
+ * 0 automatic, the default, tiled when the graph has at least 6 arcs per
+ * vertex; 1 one CTA per source, near/far frontier; 2 tiled multi-source
+ * Bellman-Ford, 128 sources per pass over the in-edges; the tiled form
+ * checks convergence on the host, so a solve that uses it is not captured
+ * in a CUDA graph). */
 FAP_API int fap_graph_set_param(fap_dgraph *g, const char *key, double value);
 
 /* Tunes the SSSP bucket width: runs the SSSP stage on `sample` boundary
