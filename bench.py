@@ -58,6 +58,10 @@ def parse_args():
                     help="stage 1 form: 0 automatic, 1 SSSP, 2 boundary graph")
     ap.add_argument("--sssp-form", type=int, default=0, choices=[0, 1, 2],
                     help="SSSP form of stage 1: 0 automatic, 1 frontier, 2 tiled Bellman-Ford")
+    ap.add_argument("--bgraph-form", type=int, default=0, choices=[0, 1, 2],
+                    help="boundary-graph closure: 0 by size, 1 Floyd, 2 Bellman-Ford + tiled expansion")
+    ap.add_argument("--no-stage-cache", action="store_true",
+                    help="grouped jobs: run stages 1-2 per group instead of once for all parts")
     ap.add_argument("--paths", action="store_true",
                     help="also time batched solves that produce predecessor matrices")
     ap.add_argument("--serve-graphs", type=int, default=32)
@@ -430,8 +434,24 @@ def main_fap(args):
     # Output rows that fit on the device (leaving room for the Floyd arena,
     # scratch and the e2e copy); larger jobs are produced in groups of parts.
     ldD = (n + 127) // 128 * 128
+    dg.set_param("stage1", args.stage1)
+    dg.set_param("sssp_form", args.sssp_form)
+    dg.set_param("bgraph_form", args.bgraph_form)
     free_b = torch.cuda.mem_get_info()[0]
     budget_rows = int(0.60 * free_b / (4 * ldD))
+    # A job larger than the device is produced in groups of parts.  On one
+    # GPU, stages 1-2 of every part then run once per step (the resident
+    # cache: boundary rows and closed Floyd matrices of all parts) and each
+    # group only runs its min-plus merge from it; the cache is allocated
+    # before the groups are sized.
+    staged = my_rows > budget_rows and world == 1 and not args.no_stage_cache
+    if staged:
+        dg.cache_build()
+        dg.check()
+        free_b = torch.cuda.mem_get_info()[0]
+        budget_rows = int(0.60 * free_b / (4 * ldD))
+        log(f"stage 1-2 cache for all parts: {dg.cache_bytes()[0] / 2**30:.1f} GiB "
+            f"({dg.stage1_name() or 'built'})")
     if my_rows <= budget_rows:
         groups = [mine]
         dg.reserve(0 if world == 1 else my_rows)
@@ -441,11 +461,11 @@ def main_fap(args):
     log(f"{len(groups)} group(s) of parts; rows budget {budget_rows}")
 
     def solve_all(mode):
+        if staged and mode == FAP_MODE_BATCHED:
+            dg.cache_build(rebuild=True)
         for grp in groups:
             dg.solve(grp, mode, check_errors=False)
     from fastapsp_b200 import autotune
-    dg.set_param("stage1", args.stage1)
-    dg.set_param("sssp_form", args.sssp_form)
     tuned = autotune.tune_sssp(dg, vn, bn)
     log(f"SSSP delta {tuned['delta']:.6g} ({'cached' if tuned['cached'] else 'tuned'}: "
         f"{tuned['key']}, factor {tuned['factor']})")
@@ -471,6 +491,11 @@ def main_fap(args):
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         st_step = np.zeros(5)
+        if staged:
+            ec = torch.cuda.Event(enable_timing=True)
+            dg.cache_build(rebuild=True)
+            launches += dg.last_launches()
+            ec.record(stream)
         for grp in groups:
             dg.solve(grp, FAP_MODE_BATCHED, check_errors=False)
             if len(groups) > 1:
@@ -482,6 +507,10 @@ def main_fap(args):
         if len(groups) == 1:
             st_step = dg.last_timing()
             launches += dg.last_launches()
+        if staged:   # the cache build holds stages 1-2 of every part
+            cb = e0.elapsed_time(ec)
+            st_step[0] += cb
+            st_step[4] += cb
         stages.append(st_step)
     torch.cuda.synchronize()
     barrier()
@@ -493,10 +522,7 @@ def main_fap(args):
     ms_per_step = max_ms / args.steps
     value = total_entries * args.steps / (max_ms * 1e-3)
     st = np.mean(np.stack(stages), 0)  # [sssp, gather, floyd, minplus, total]
-    stage1_used = {1: "SSSP", 2: "boundary graph", 3: "resident cache"}.get(dg.last_stage1(), "?")
-    if stage1_used == "SSSP":
-        stage1_used += " (tiled Bellman-Ford)" if (args.sssp_form == 2 or (
-            args.sssp_form == 0 and int(ro[-1]) >= 6 * n)) else " (frontier)"
+    stage1_used = dg.stage1_name()
     log(f"batched: {ms_per_step:.3f} ms/step, stages {np.round(st, 3).tolist()}, "
         f"{value:.4g} entries/s")
 
@@ -572,7 +598,8 @@ def main_fap(args):
                 "traffic": read_traffic(wl.name, "floyd_part_kernel")}
     else:
         thin_only = all(int(bn[p]) <= 16 for p in mine)
-        kern = ("sssp_frontier_kernel" if dom == "sssp" else
+        kern = (("msbf_iter_kernel" if "Bellman-Ford" in stage1_used else "sssp_frontier_kernel")
+                if dom == "sssp" else
                 "minplus_thin_kernel" if thin_only else "minplus_part_kernel")
         a = stage_roof[dom]["achieved_gbs"]
         roof = {"kernel": kern, "bound": "hbm", "achieved": a, "peak": hbm_peak, "unit": "GB/s",
@@ -605,6 +632,8 @@ def main_fap(args):
         g2 = DeviceGraph(ctx, pin["ro"], pin["col"], pin["w"])
         g2.set_parts(wl.K, pin["gid"], pin["st2ed"], pin["vn"], pin["vo"], pin["bn"])
         g2.reserve(max(rows_of(g, vn) for g in groups))
+        if staged:
+            g2.cache_build()
         for grp in groups:
             g2.solve(grp, FAP_MODE_BATCHED)
             for p in grp:

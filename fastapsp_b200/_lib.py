@@ -84,6 +84,7 @@ _SIGS = {
     "fap_graph_last_timing": (INT, [P, P]),
     "fap_graph_last_launches": (INT, [P, ctypes.POINTER(I64)]),
     "fap_graph_last_stage1": (INT, [P]),
+    "fap_graph_stage1_name": (ctypes.c_char_p, [P]),
     "fap_op_sssp": (INT, [P, INT, I32, I64, P, P, P, P, I32, P, I64]),
     "fap_op_floyd": (INT, [P, INT, I32, P, I64]),
     "fap_op_minplus": (INT, [P, INT, I32, I32, I32, P, I64, P, I64, P, I64]),
@@ -95,6 +96,7 @@ _SIGS = {
     "fap_graph_resident": (INT, [P, I32]),
     "fap_graph_rows_async": (INT, [P, P, I32, P]),
     "fap_graph_cache_build": (INT, [P]),
+    "fap_graph_cache_rebuild": (INT, [P]),
     "fap_graph_cache_release": (INT, [P]),
     "fap_graph_cache_bytes": (INT, [P, ctypes.POINTER(I64), ctypes.POINTER(INT)]),
     "fap_server_create": (INT, [INT, DBL, I64, PP]),

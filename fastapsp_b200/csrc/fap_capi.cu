@@ -192,6 +192,18 @@ struct fap_dgraph {
   bool cache_bmethod = false;  // the resident cache was built with it
   int64_t ldB = 0;
   DevBuf d_dB, d_bpart, d_brows, d_FB;
+  // Large boundary sets: dB closed by Bellman-Ford in alternating local
+  // (min-plus with the parts' local closures) and cross steps (the in-arc
+  // CSR of the cross-part arcs over boundary indices, built once per
+  // partition; gpart: part of every boundary index) and the boundary rows
+  // written by the tiled expansion (grow: boundary index -> D row).
+  std::string stage1_name, cache_stage1_name;  // fap_graph_stage1_name
+  int bgraph_form = 0;        // 0 by size, 1 Floyd + staged expansion, 2 Bellman-Ford + tiled expansion
+  int64_t bgraph_edges = 0;  // sum_p b_p (b_p - 1) + cross-part arcs
+  int64_t bgraph_cross = 0;  // cross-part arcs
+  bool bg_csr_ready = false;
+  int bg_nitems = 0;
+  DevBuf d_btro, d_btcol, d_btw, d_bitems, d_bDt, d_bact, d_bpact, d_bgpart, d_grow;
   // Tiled form of stage 1's SSSP (launch_msbf): 0 automatic (graphs with at
   // least 6 arcs per vertex, where few Bellman-Ford iterations suffice), 1
   // frontier kernel, 2 tiled.  Work items over the in-edge CSR.
@@ -406,7 +418,9 @@ extern "C" int fap_graph_destroy(fap_dgraph *G) {
                       &G->d_gid, &G->d_st2ed, &G->d_ed2st, &G->D, &G->F, &G->d_parts, &G->d_work,
                       &G->d_src, &G->d_srcrows, &G->d_status, &G->d_checks, &G->staging, &G->P,
                       &G->d_tro, &G->d_tcol, &G->d_tw, &G->d_dB, &G->d_bpart, &G->d_brows, &G->d_FB,
-                      &G->d_msbf_items, &G->d_msbf_act, &G->d_msbf_changed})
+                      &G->d_msbf_items, &G->d_msbf_act, &G->d_msbf_changed, &G->d_btro, &G->d_btcol,
+                      &G->d_btw, &G->d_bitems, &G->d_bDt, &G->d_bact, &G->d_bpact, &G->d_bgpart,
+                      &G->d_grow})
       b->release();
     if (G->h_changed) cudaFreeHost(G->h_changed);
     cache_drop(G);
@@ -470,6 +484,16 @@ extern "C" int fap_graph_set_parts(fap_dgraph *G, int32_t K, const int32_t *grap
         seen[v] = u;
       }
   }
+  {
+    // edges of the boundary graph
+    int64_t cross = 0;
+    for (int32_t u = 0; u < n; u++)
+      for (int32_t e = G->h_ro[u]; e < G->h_ro[u + 1]; e++) cross += graph_id[G->h_col[e]] != graph_id[u];
+    G->bgraph_cross = cross;
+    G->bgraph_edges = cross;
+    for (int32_t p = 1; p <= K; p++) G->bgraph_edges += (int64_t)bdy_num[p] * std::max(bdy_num[p] - 1, 0);
+    G->bg_csr_ready = false;
+  }
   G->row_base.assign(K + 1, -1);
   G->last_ids.clear();
   cache_drop(G);
@@ -525,14 +549,95 @@ extern "C" int fap_graph_reserve(fap_dgraph *G, int64_t max_rows) {
 
 namespace {
 
+// Boundary sets up to this size close dB by Floyd; larger ones by the tiled
+// Bellman-Ford over the boundary graph (Floyd's cube grows too fast).
+constexpr int64_t kBgraphFloydMax = 8192;
+// The staged expansion keeps kExpandRows rows of dB in shared memory.
+constexpr int64_t kBgraphStagedMax = 4096;
+// Automatic Bellman-Ford closure only while the boundary graph has at most
+// this many edges per edge of the graph (its cliques grow as b_p^2) and dB
+// stays within 64 Ki boundary vertices (17 GB).
+constexpr int64_t kBgraphEdgeRatio = 8;
+constexpr int64_t kBgraphAutoMaxB = 65536;
+
+bool bgraph_bf(const fap_dgraph *G) {
+  return G->bgraph_form == 2 || (G->bgraph_form == 0 && G->total_b > kBgraphFloydMax);
+}
+const char *stage1_form_name(const fap_dgraph *G, bool bmethod);
+
+bool bgraph_tiled_expand(const fap_dgraph *G) { return G->bgraph_form == 2 || G->total_b > kBgraphStagedMax; }
+
 // Whether the boundary-graph form of stage 1 applies to g.
 // Automatic choice: int32 distances only (there both forms give the exact
 // shortest distances bit for bit; float32 sums would round in a different
-// order, a few ulps), at most 8192 boundary vertices.
+// order, a few ulps); up to 8192 boundary vertices with Floyd on the boundary
+// graph, beyond that with the tiled Bellman-Ford while the boundary graph
+// stays sparse (grid-like graphs with many parts).
 bool bmethod_ok(const fap_dgraph *G) {
   if (G->stage1 == 1 || !G->bnd_dupfree || G->total_b <= 0) return false;
+  if (bgraph_bf(G) && (G->bgraph_cross >= INT32_MAX || G->total_b >= INT32_MAX / kMsbfS)) return false;
   if (G->stage1 == 2) return true;
-  return G->dtype == FAP_DTYPE_I32 && G->total_b <= 8192;
+  if (G->dtype != FAP_DTYPE_I32) return false;
+  return !bgraph_bf(G) ||
+         (G->bgraph_edges <= kBgraphEdgeRatio * G->m && G->total_b <= kBgraphAutoMaxB);
+}
+
+// Cross-part in-arcs of every boundary vertex (g = boff[p] + c for the c-th
+// boundary vertex of part p) as a CSR over boundary indices, its work items
+// (up to 32 in-arcs each), and the part of every boundary index.
+int build_bgraph_csr(fap_dgraph *G) {
+  if (G->bg_csr_ready) return FAP_OK;
+  const int64_t nb = G->total_b;
+  auto bidx = [&](int32_t v) -> int64_t {
+    const int32_t p = G->gid[v];
+    const int32_t l = G->ed2st[v] - G->voff[p];
+    return l < G->bnum[p] ? G->boff[p] + l : -1;
+  };
+  std::vector<int32_t> tro((size_t)nb + 1, 0), gpart((size_t)nb);
+  for (int32_t p = 1; p <= G->K; p++)
+    for (int32_t c = 0; c < G->bnum[p]; c++) gpart[G->boff[p] + c] = p;
+  for (int32_t u = 0; u < G->n; u++)
+    for (int32_t e = G->h_ro[u]; e < G->h_ro[u + 1]; e++) {
+      const int32_t v = G->h_col[e];
+      if (G->gid[v] == G->gid[u]) continue;
+      const int64_t gv = bidx(v);
+      if (gv >= 0 && bidx(u) >= 0) tro[gv + 1]++;
+    }
+  for (int64_t g = 0; g < nb; g++) tro[g + 1] += tro[g];
+  const int64_t ne = tro[nb];
+  std::vector<int32_t> tcol((size_t)std::max<int64_t>(ne, 1)), fill(tro.begin(), tro.end() - 1);
+  std::vector<uint32_t> tw((size_t)std::max<int64_t>(ne, 1), 0);
+  for (int32_t u = 0; u < G->n; u++)
+    for (int32_t e = G->h_ro[u]; e < G->h_ro[u + 1]; e++) {
+      const int32_t v = G->h_col[e];
+      if (G->gid[v] == G->gid[u]) continue;
+      const int64_t gu = bidx(u), gv = bidx(v);
+      if (gu < 0 || gv < 0) continue;
+      tcol[fill[gv]] = (int32_t)gu;
+      tw[fill[gv]++] = G->h_w[e];
+    }
+  std::vector<MsbfItem> items;
+  for (int64_t g = 0; g < nb; g++)
+    for (int32_t e = tro[g]; e < tro[g + 1]; e += 32) items.push_back(MsbfItem{(int32_t)g, e});
+  FAP_TRY(G->d_btro.ensure(tro.size() * 4));
+  FAP_TRY(G->d_btcol.ensure(tcol.size() * 4));
+  FAP_TRY(G->d_btw.ensure(tw.size() * 4));
+  FAP_TRY(G->d_bitems.ensure(std::max<size_t>(items.size(), 1) * sizeof(MsbfItem)));
+  FAP_TRY(G->d_bgpart.ensure((size_t)nb * 4));
+  FAP_TRY(G->d_bDt.ensure((size_t)nb * kMsbfS * 4));
+  FAP_TRY(G->d_bact.ensure((size_t)2 * nb * 4));
+  FAP_TRY(G->d_bpact.ensure((size_t)(G->K + 1) * 4));
+  FAP_TRY(G->d_msbf_changed.ensure(4 * sizeof(int)));
+  if (!G->h_changed) FAP_CK(cudaHostAlloc(reinterpret_cast<void **>(&G->h_changed), 4 * sizeof(int), 0));
+  FAP_CK(cudaMemcpy(G->d_btro.p, tro.data(), tro.size() * 4, cudaMemcpyHostToDevice));
+  FAP_CK(cudaMemcpy(G->d_btcol.p, tcol.data(), tcol.size() * 4, cudaMemcpyHostToDevice));
+  FAP_CK(cudaMemcpy(G->d_btw.p, tw.data(), tw.size() * 4, cudaMemcpyHostToDevice));
+  FAP_CK(cudaMemcpy(G->d_bgpart.p, gpart.data(), gpart.size() * 4, cudaMemcpyHostToDevice));
+  if (!items.empty())
+    FAP_CK(cudaMemcpy(G->d_bitems.p, items.data(), items.size() * sizeof(MsbfItem), cudaMemcpyHostToDevice));
+  G->bg_nitems = (int)items.size();
+  G->bg_csr_ready = true;
+  return FAP_OK;
 }
 
 // Per-part table, output-row list and dB for a batch of all parts in the
@@ -562,6 +667,55 @@ int prepare_bgraph(fap_dgraph *G, const std::vector<PartDesc> &parts) {
   FAP_CK(cudaMemcpy(G->d_bpart.p, bp.data(), bp.size() * sizeof(BPart), cudaMemcpyHostToDevice));
   if (!rows.empty())
     FAP_CK(cudaMemcpy(G->d_brows.p, rows.data(), rows.size() * 8, cudaMemcpyHostToDevice));
+  if (bgraph_tiled_expand(G)) {
+    std::vector<int64_t> grow((size_t)G->total_b, 0);
+    for (size_t i = 0; i + 1 < rows.size(); i += 2) grow[rows[i]] = rows[i + 1];
+    FAP_TRY(G->d_grow.ensure(grow.size() * 8));
+    FAP_CK(cudaMemcpy(G->d_grow.p, grow.data(), grow.size() * 8, cudaMemcpyHostToDevice));
+  }
+  if (bgraph_bf(G)) FAP_TRY(build_bgraph_csr(G));
+  return FAP_OK;
+}
+
+// dB (total_b x total_b, ld ldB) = the closed boundary graph of the local
+// closures F of all parts: Floyd for small boundary sets, the tiled
+// Bellman-Ford (host-polled convergence) for large ones.
+template <typename T>
+int close_bgraph(fap_dgraph *G, const PartDesc *dp, int np, int max_b, const T *F, int *status,
+                 int64_t max_rounds, int64_t *L) {
+  cudaStream_t st = G->ctx->stream;
+  T *dB = G->d_dB.as<T>();
+  if (!bgraph_bf(G)) {
+    FAP_CK(launch_bgraph<T>(dp, np, max_b, F, dB, G->ldB, G->ro.as<const int32_t>(), G->col.as<const int32_t>(),
+                            G->w.as<const T>(), G->n, G->d_gid.as<const int32_t>(),
+                            G->d_ed2st.as<const int32_t>(), G->d_bpart.as<const BPart>(), st, L));
+    FAP_CK(launch_floyd_matrix<T>(dB, G->ldB, (int)(G->ldB / kFloydTile), status, st, L));
+    return FAP_OK;
+  }
+  FAP_CK(launch_bgraph_bf<T>(dp, np, max_b, F, G->d_bitems.as<const MsbfItem>(), G->bg_nitems,
+                             G->d_btro.as<const int32_t>(), G->d_btcol.as<const int32_t>(), G->d_btw.as<const T>(),
+                             G->d_bgpart.as<const int32_t>(), (int)G->total_b, G->K, dB, G->ldB, G->d_bDt.as<T>(),
+                             G->d_bact.as<int>(), G->d_bpact.as<int>(), G->d_msbf_changed.as<int>(), G->h_changed,
+                             max_rounds, status, st, L));
+  return FAP_OK;
+}
+
+// Boundary rows of D (or of the cache) from the closed dB: the staged
+// expansion for small boundary sets, the tiled one otherwise.  Also FB.
+template <typename T>
+int expand_bgraph(fap_dgraph *G, const PartDesc *dp, int np, int max_s, const T *F, T *Dout, int64_t ldFB,
+                  int64_t *L) {
+  cudaStream_t st = G->ctx->stream;
+  if (!bgraph_tiled_expand(G)) {
+    FAP_CK(launch_bdy_expand<T>(G->d_brows.as<const int64_t>(), (int)G->total_b, G->d_bpart.as<const BPart>(),
+                                G->d_gid.as<const int32_t>(), G->d_ed2st.as<const int32_t>(), G->n,
+                                G->d_dB.as<const T>(), G->ldB, (int)G->total_b, F, Dout, G->ldD, G->d_FB.as<T>(),
+                                ldFB, st, L));
+  } else {
+    FAP_CK(launch_bdy_expand_tiled<T>(dp, np, max_s, (int)G->total_b, G->d_grow.as<const int64_t>(),
+                                      G->d_st2ed.as<const int32_t>(), G->d_dB.as<const T>(), G->ldB, F, Dout,
+                                      G->ldD, G->d_FB.as<T>(), ldFB, st, L));
+  }
   return FAP_OK;
 }
 
@@ -696,6 +850,11 @@ bool use_msbf(const fap_dgraph *G) {
   return G->n > 0 && G->m >= 6 * (int64_t)G->n;
 }
 
+const char *stage1_form_name(const fap_dgraph *G, bool bmethod) {
+  if (bmethod) return bgraph_bf(G) ? "boundary graph, Bellman-Ford closure" : "boundary graph, Floyd closure";
+  return use_msbf(G) ? "SSSP, tiled Bellman-Ford" : "SSSP, frontier";
+}
+
 // Work items, bitmaps and the pinned convergence flags of the tiled form.
 int prepare_msbf(fap_dgraph *G) {
   FAP_TRY(ensure_in_edges(G));
@@ -774,12 +933,8 @@ int run_solve(fap_dgraph *G, int mode) {
     FAP_CK(launch_floyd_parts_multi<T>(dp, np, (int)ceil_div(G->max_s, kFloydTile), F, G->max_ldf,
                                        status, st, &L));
     FAP_CK(record_event(c->ev[2], st));
-    T *dB = G->d_dB.as<T>();
-    const BPart *bp = G->d_bpart.as<const BPart>();
-    FAP_CK(launch_bgraph<T>(dp, np, G->max_b, F, dB, G->ldB, ro, col, w, G->n, gid, ed2st, bp, st, &L));
-    FAP_CK(launch_floyd_matrix<T>(dB, G->ldB, (int)(G->ldB / kFloydTile), status, st, &L));
-    FAP_CK(launch_bdy_expand<T>(G->d_brows.as<const int64_t>(), (int)G->total_b, bp, gid, ed2st, G->n, dB,
-                                G->ldB, (int)G->total_b, F, D, G->ldD, G->d_FB.as<T>(), G->max_ldf, st, &L));
+    FAP_TRY(close_bgraph<T>(G, dp, np, G->max_b, F, status, max_rounds, &L));
+    FAP_TRY(expand_bgraph<T>(G, dp, np, G->max_s, F, D, G->max_ldf, &L));
     FAP_CK(launch_local_fixup<T>(dp, np, G->max_s, F, G->d_FB.as<const T>(), G->max_ldf, st, &L));
     FAP_CK(record_event(c->ev[3], st));
     FAP_CK(launch_minplus_thin<T>(dp, G->d_thin.as<int32_t>(), (int)G->thin.size(), G->max_s, G->n, F, D,
@@ -898,7 +1053,8 @@ extern "C" int fap_solve(fap_dgraph *G, const int32_t *parts, int32_t count, int
   int rc = FAP_OK;
   cudaStream_t st = G->ctx->stream;
   // (the tiled SSSP form tests convergence on the host: not capturable)
-  const bool host_loop = !cached && !bmethod && use_msbf(G);
+  const bool host_loop = !cached && (bmethod ? bgraph_bf(G) : use_msbf(G));
+  G->stage1_name = cached ? "resident cache (" + G->cache_stage1_name + ")" : stage1_form_name(G, bmethod);
   if (mode == FAP_MODE_BATCHED && G->use_graph && st != nullptr && !host_loop) {
     if (!G->gexec || G->gexec_epoch != G->epoch || G->gexec_stream != st) {
       if (G->gexec) cudaGraphExecDestroy(G->gexec);
@@ -981,6 +1137,14 @@ extern "C" int fap_graph_last_stage1(const fap_dgraph *G) {
   if (G->last_mode < 0) return 0;
   if (G->last_cached) return 3;
   return G->last_bmethod ? 2 : 1;
+}
+
+extern "C" const char *fap_graph_stage1_name(const fap_dgraph *G) {
+  if (!G) {
+    fail(FAP_ERR_INVALID, "NULL graph");
+    return "";
+  }
+  return G->stage1_name.c_str();
 }
 
 extern "C" int fap_graph_last_launches(fap_dgraph *G, int64_t *count) {
@@ -1372,6 +1536,13 @@ extern "C" int fap_graph_set_param(fap_dgraph *G, const char *key, double value)
     G->last_ids.clear();
     return FAP_OK;
   }
+  if (std::strcmp(key, "bgraph_form") == 0) {
+    if (value != 0.0 && value != 1.0 && value != 2.0) return fail(FAP_ERR_INVALID, "bgraph_form is 0, 1 or 2");
+    G->bgraph_form = (int)value;
+    G->last_ids.clear();
+    G->epoch++;
+    return FAP_OK;
+  }
   if (std::strcmp(key, "paths") == 0) {
     if (value == 0.0) {
       G->paths = false;
@@ -1503,7 +1674,8 @@ extern "C" int fap_graph_device_bytes(const fap_dgraph *G, int64_t *bytes) {
                           &G->cBd, &G->cF, &G->d_cparts, &G->d_rowgroups, &G->d_rowloc, &G->d_rowout,
                           &G->d_rowidx, &G->P, &G->d_tro, &G->d_tcol, &G->d_tw, &G->d_dB,
                           &G->d_bpart, &G->d_brows, &G->d_FB, &G->d_msbf_items, &G->d_msbf_act,
-                          &G->d_msbf_changed})
+                          &G->d_msbf_changed, &G->d_btro, &G->d_btcol, &G->d_btw, &G->d_bitems,
+                          &G->d_bDt, &G->d_bact, &G->d_bpact, &G->d_bgpart, &G->d_grow})
     t += (int64_t)b->bytes;
   *bytes = t;
   return FAP_OK;
@@ -1604,16 +1776,13 @@ int cache_build_impl(fap_dgraph *G) {
     FAP_CK(launch_gather<T>(dp, K, cs.ldf, G->ro.as<const int32_t>(), G->col.as<const int32_t>(),
                             G->w.as<const T>(), gid, st2ed, ed2st, Bd, G->ldD, F, st, &L));
     FAP_CK(launch_floyd_parts_multi<T>(dp, K, (int)ceil_div(cs.max_s, kFloydTile), F, cs.ldf, status, st, &L));
-    T *dB = G->d_dB.as<T>();
-    const BPart *bp = G->d_bpart.as<const BPart>();
-    FAP_CK(launch_bgraph<T>(dp, K, cs.max_b, F, dB, G->ldB, G->ro.as<const int32_t>(),
-                            G->col.as<const int32_t>(), G->w.as<const T>(), G->n, gid, ed2st, bp, st, &L));
-    FAP_CK(launch_floyd_matrix<T>(dB, G->ldB, (int)(G->ldB / kFloydTile), status, st, &L));
-    FAP_CK(launch_bdy_expand<T>(G->d_brows.as<const int64_t>(), (int)G->total_b, bp, gid, ed2st, G->n, dB,
-                                G->ldB, (int)G->total_b, F, Bd, G->ldD, G->d_FB.as<T>(), cs.ldf, st, &L));
+    FAP_TRY(close_bgraph<T>(G, dp, K, cs.max_b, F, status, rounds, &L));
+    FAP_TRY(expand_bgraph<T>(G, dp, K, cs.max_s, F, Bd, cs.ldf, &L));
     FAP_CK(launch_local_fixup<T>(dp, K, cs.max_s, F, G->d_FB.as<const T>(), cs.ldf, st, &L));
     G->cache_bmethod = true;
+    G->cache_stage1_name = stage1_form_name(G, true);
   } else {
+  G->cache_stage1_name = stage1_form_name(G, false);
   FAP_TRY(run_stage1_sssp<T>(G, G->d_src.as<const int32_t>(), G->d_srcrows.as<const int64_t>(),
                              (int)src.size(), Bd, status, rounds, &L));
   FAP_CK(launch_gather<T>(dp, K, cs.ldf, G->ro.as<const int32_t>(), G->col.as<const int32_t>(),
@@ -1720,6 +1889,15 @@ extern "C" int fap_graph_cache_build(fap_dgraph *G) {
   return rc;
 }
 
+extern "C" int fap_graph_cache_rebuild(fap_dgraph *G) {
+  if (!G) return fail(FAP_ERR_INVALID, "NULL graph");
+  if (G->K == 0) return fail(FAP_ERR_STATE, "fap_graph_cache_rebuild before fap_graph_set_parts");
+  DeviceGuard g(G->ctx->device);
+  const int rc = G->dtype == FAP_DTYPE_I32 ? cache_build_impl<int32_t>(G) : cache_build_impl<float>(G);
+  if (rc != FAP_OK) cache_drop(G);
+  return rc;
+}
+
 extern "C" int fap_graph_cache_release(fap_dgraph *G) {
   if (!G) return fail(FAP_ERR_INVALID, "NULL graph");
   DeviceGuard g(G->ctx->device);
@@ -1734,6 +1912,10 @@ extern "C" int fap_graph_cache_bytes(const fap_dgraph *G, int64_t *bytes, int *b
   if (built) *built = G->cache_ready ? 1 : 0;
   if (G->cache_ready) {
     *bytes = (int64_t)(G->cBd.bytes + G->cF.bytes + G->d_cparts.bytes);
+    if (G->cache_bmethod)  // the boundary graph's buffers stay for rebuilds
+      for (const DevBuf *b : {&G->d_dB, &G->d_FB, &G->d_btro, &G->d_btcol, &G->d_btw, &G->d_bitems, &G->d_bDt,
+                              &G->d_bact, &G->d_bpact, &G->d_bgpart, &G->d_grow})
+        *bytes += (int64_t)b->bytes;
   } else {
     // plus what the build needs while it runs: the SSSP scratch, or the
     // boundary-graph matrix and tables
@@ -1744,6 +1926,14 @@ extern "C" int fap_graph_cache_bytes(const fap_dgraph *G, int64_t *bytes, int *b
                (int64_t)alloc_size((size_t)std::max<int64_t>(G->total_b, 1) * cs.ldf * 4) +
                (int64_t)alloc_size((size_t)(G->K + 1) * sizeof(BPart)) +
                (int64_t)alloc_size((size_t)std::max<int64_t>(2 * G->total_b, 2) * 8);
+      if (bgraph_tiled_expand(G)) *bytes += (int64_t)alloc_size((size_t)G->total_b * 8);
+      if (bgraph_bf(G)) {  // cross-arc CSR, work items, tile, stamps, part table
+        const int64_t xe = std::max<int64_t>(G->bgraph_cross, 1);
+        *bytes += 2 * (int64_t)alloc_size((size_t)(G->total_b + 1) * 4) + 2 * (int64_t)alloc_size((size_t)xe * 4) +
+                  (int64_t)alloc_size((size_t)(xe / 32 + G->total_b + 1) * sizeof(MsbfItem)) +
+                  (int64_t)alloc_size((size_t)G->total_b * kMsbfS * 4) +
+                  (int64_t)alloc_size((size_t)2 * G->total_b * 4) + (int64_t)alloc_size((size_t)(G->K + 1) * 4);
+      }
     } else {
       *bytes = cs.bytes(G) + (int64_t)alloc_size(
                                  (size_t)std::max(sssp_scratch_rows(G->n, (int)std::min<int64_t>(cs.total_b, INT32_MAX)), 1) *

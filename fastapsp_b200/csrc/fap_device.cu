@@ -210,14 +210,74 @@ cudaError_t launch_sssp(const int32_t *row_offset, const int32_t *col, const T *
 // exact shortest distances, each the sum along its path edge by edge (the
 // same additions in the same order as Dijkstra's).  The host repeats
 // iterations until one changes nothing (or the round bound is reached).
+// Source s of the tile (global index s0 + s): vertex st2ed[sources[s0 + s]];
+// without a source list the work graph's own vertex s0 + s.
 template <typename T>
 __global__ void msbf_seed_kernel(T *Dt, const int32_t *__restrict__ sources, const int32_t *__restrict__ st2ed,
-                                 int ns, uint32_t *act) {
+                                 int s0, int ns, uint32_t *act) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= ns) return;
-  const int v = __ldg(st2ed + __ldg(sources + s));
+  const int v = sources ? __ldg(st2ed + __ldg(sources + s0 + s)) : s0 + s;
   Dt[(int64_t)v * kMsbfS + s] = T(0);
   atomicOr(act + (v >> 5), 1u << (v & 31));
+}
+
+// One warp lowers row v of the tile from up to 32 in-edges e0..e1 whose
+// tails pass `active` (warp-uniform loop, four tail rows in flight); the
+// row's lanes each hold 4 sources.  Returns (warp-uniform) whether any entry
+// improved.  Atomic minima: other warps may lower the same row meanwhile.
+template <typename T, class Active>
+__device__ __forceinline__ bool msbf_pull_row(T *Dt, int v, int e0, int e1, const int32_t *__restrict__ tcol,
+                                              const T *__restrict__ tw, Active active) {
+  using V = typename Vec4<T>::type;
+  const T inf = Dist<T>::inf();
+  const int lane = threadIdx.x & 31;
+  const int e = e0 + lane;
+  int u = -1;
+  T w = T(0);
+  if (e < e1) {
+    u = __ldg(tcol + e);
+    if (active(u)) w = __ldg(tw + e);
+    else u = -1;
+  }
+  unsigned mask = __ballot_sync(0xffffffffu, u >= 0);
+  if (!mask) return false;
+  T acc[4] = {inf, inf, inf, inf};
+  while (mask) {  // warp-uniform: four active in-edges per step, loads in flight together
+    int uu[4];
+    T ww[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      uu[q] = -1;
+      ww[q] = T(0);
+      if (mask) {
+        const int k = __ffs(mask) - 1;
+        mask &= mask - 1;
+        uu[q] = __shfl_sync(0xffffffffu, u, k);
+        ww[q] = __shfl_sync(0xffffffffu, w, k);
+      }
+    }
+    V d[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+      if (uu[q] >= 0) d[q] = __ldcg(reinterpret_cast<const V *>(Dt + (int64_t)uu[q] * kMsbfS) + lane);
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+      if (uu[q] >= 0) {
+        acc[0] = Dist<T>::relax(d[q].x, ww[q], acc[0]);
+        acc[1] = Dist<T>::relax(d[q].y, ww[q], acc[1]);
+        acc[2] = Dist<T>::relax(d[q].z, ww[q], acc[2]);
+        acc[3] = Dist<T>::relax(d[q].w, ww[q], acc[3]);
+      }
+  }
+  T *row = Dt + (int64_t)v * kMsbfS + 4 * lane;
+  const V cur = __ldcg(reinterpret_cast<const V *>(row));
+  const T cv[4] = {cur.x, cur.y, cur.z, cur.w};
+  bool imp = false;
+#pragma unroll
+  for (int q = 0; q < 4; q++)
+    if (acc[q] < cv[q]) imp |= acc[q] < Dist<T>::atomic_min(row + q, acc[q]);
+  return __any_sync(0xffffffffu, imp);
 }
 
 template <typename T>
@@ -225,72 +285,26 @@ __global__ void __launch_bounds__(256)
     msbf_iter_kernel(T *Dt, const MsbfItem *__restrict__ items, int nitems, const int32_t *__restrict__ tro,
                      const int32_t *__restrict__ tcol, const T *__restrict__ tw, const uint32_t *__restrict__ act_cur,
                      uint32_t *act_next, int *changed) {
-  using V = typename Vec4<T>::type;
-  const T inf = Dist<T>::inf();
   const int lane = threadIdx.x & 31;
   const int nwarps = gridDim.x * (blockDim.x >> 5);
+  auto active = [act_cur](int u) { return ((__ldcg(act_cur + (u >> 5)) >> (u & 31)) & 1u) != 0; };
   for (int it = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < nitems; it += nwarps) {
     const MsbfItem m = items[it];
     const int e1 = min(m.e0 + 32, __ldg(tro + m.v + 1));
-    const int e = m.e0 + lane;
-    int u = -1;
-    T w = T(0);
-    if (e < e1) {
-      u = __ldg(tcol + e);
-      if ((__ldcg(act_cur + (u >> 5)) >> (u & 31)) & 1u) w = __ldg(tw + e);
-      else u = -1;
-    }
-    unsigned mask = __ballot_sync(0xffffffffu, u >= 0);
-    if (!mask) continue;
-    T acc[4] = {inf, inf, inf, inf};
-    while (mask) {  // warp-uniform: four active in-edges per step, loads in flight together
-      int uu[4];
-      T ww[4];
-#pragma unroll
-      for (int q = 0; q < 4; q++) {
-        uu[q] = -1;
-        ww[q] = T(0);
-        if (mask) {
-          const int k = __ffs(mask) - 1;
-          mask &= mask - 1;
-          uu[q] = __shfl_sync(0xffffffffu, u, k);
-          ww[q] = __shfl_sync(0xffffffffu, w, k);
-        }
-      }
-      V d[4];
-#pragma unroll
-      for (int q = 0; q < 4; q++)
-        if (uu[q] >= 0) d[q] = __ldcg(reinterpret_cast<const V *>(Dt + (int64_t)uu[q] * kMsbfS) + lane);
-#pragma unroll
-      for (int q = 0; q < 4; q++)
-        if (uu[q] >= 0) {
-          acc[0] = Dist<T>::relax(d[q].x, ww[q], acc[0]);
-          acc[1] = Dist<T>::relax(d[q].y, ww[q], acc[1]);
-          acc[2] = Dist<T>::relax(d[q].z, ww[q], acc[2]);
-          acc[3] = Dist<T>::relax(d[q].w, ww[q], acc[3]);
-        }
-    }
-    T *row = Dt + (int64_t)m.v * kMsbfS + 4 * lane;
-    const V cur = __ldcg(reinterpret_cast<const V *>(row));
-    const T cv[4] = {cur.x, cur.y, cur.z, cur.w};
-    bool imp = false;
-#pragma unroll
-    for (int q = 0; q < 4; q++)
-      if (acc[q] < cv[q]) imp |= acc[q] < Dist<T>::atomic_min(row + q, acc[q]);
-    if (__any_sync(0xffffffffu, imp) && lane == 0) {
+    if (msbf_pull_row<T>(Dt, m.v, m.e0, e1, tcol, tw, active) && lane == 0) {
       atomicOr(act_next + (m.v >> 5), 1u << (m.v & 31));
       *changed = 1;
     }
   }
 }
 
-// out[out_rows[s]][v] = Dt[v][s] for s < ns, all init_cols columns (INF past
-// n): 32 vertices per CTA, transposed through shared memory, 128-byte row
-// segments stored.
+// out[out_rows[s0 + s]][v] = Dt[v][s] for s < ns (row s0 + s without a row
+// list), all init_cols columns (INF past n): 32 vertices per CTA, transposed
+// through shared memory, 128-byte row segments stored.
 template <typename T>
 __global__ void __launch_bounds__(256)
-    msbf_store_kernel(const T *__restrict__ Dt, int n, int ns, T *out, int64_t ld, const int64_t *__restrict__ out_rows,
-                      int64_t init_cols) {
+    msbf_store_kernel(const T *__restrict__ Dt, int n, int s0, int ns, T *out, int64_t ld,
+                      const int64_t *__restrict__ out_rows, int64_t init_cols) {
   __shared__ T tile[32][kMsbfS + 1];
   const int64_t v0 = (int64_t)blockIdx.x * 32;
   const T inf = Dist<T>::inf();
@@ -303,7 +317,8 @@ __global__ void __launch_bounds__(256)
   const int lane = threadIdx.x & 31;
   for (int s = threadIdx.x >> 5; s < ns; s += blockDim.x >> 5) {
     const int64_t v = v0 + lane;
-    if (v < init_cols) out[out_rows[s] * ld + v] = tile[lane][s];
+    const int64_t row = out_rows ? out_rows[s0 + s] : (int64_t)(s0 + s);
+    if (v < init_cols) out[row * ld + v] = tile[lane][s];
   }
 }
 
@@ -323,7 +338,7 @@ cudaError_t launch_msbf(const MsbfItem *items, int nitems, const int32_t *tro, c
     cudaError_t e = launch_fill<T>(Dt, n, kMsbfS, kMsbfS, Dist<T>::inf(), stream, launches);
     if (e == cudaSuccess) e = cudaMemsetAsync(act_a, 0, words * 4, stream);
     if (e != cudaSuccess) return e;
-    msbf_seed_kernel<T><<<1, kMsbfS, 0, stream>>>(Dt, sources + s0, st2ed, ns, act_a);
+    msbf_seed_kernel<T><<<1, kMsbfS, 0, stream>>>(Dt, sources, st2ed, s0, ns, act_a);
     *launches += 1;
     bool done = false;
     for (int64_t round = 0; !done; round += kChunk) {
@@ -348,7 +363,7 @@ cudaError_t launch_msbf(const MsbfItem *items, int nitems, const int32_t *tro, c
       if (e != cudaSuccess) return e;
       for (int c = 0; c < kChunk; c++) done |= host_changed[c] == 0;
     }
-    msbf_store_kernel<T><<<(unsigned)ceil_div(init_cols, 32), 256, 0, stream>>>(Dt, n, ns, out, ld, out_rows + s0,
+    msbf_store_kernel<T><<<(unsigned)ceil_div(init_cols, 32), 256, 0, stream>>>(Dt, n, s0, ns, out, ld, out_rows,
                                                                                init_cols);
     *launches += 1;
     e = cudaGetLastError();
@@ -1263,6 +1278,279 @@ cudaError_t launch_bdy_expand(const int64_t *rows, int nrows, const BPart *bpart
   return cudaGetLastError();
 }
 
+// Boundary graph closed by Bellman-Ford in alternating steps (large
+// boundary sets).  A shortest path between boundary vertices alternates
+// segments inside one part (their lengths are the local closure F_p, already
+// transitive) and cross-part arcs, so for kMsbfS sources at a time (tile
+// Dt[g][s], boundary index g):
+//   local step, per part p whose rows changed in the last cross step:
+//     Dt[c][s] = min(Dt[c][s], min_a Dt[a][s] + F_p[a][c])
+//   over the rows a that the cross step changed (the others were closed
+//   before, and F_p is transitive): a min-plus product run from shared
+//   memory, 128 sources x 64 columns per CTA, K = the changed rows; rows
+//   that improve are stamped for the cross step;
+//   cross step: rows with cross-part in-arcs pull from stamped tails
+//   (msbf_pull_row) and stamp their parts for the next local step.
+// Stamps are iteration numbers (xact: per boundary vertex, the iteration in
+// which its row changed, by either step, so that the next cross step pulls
+// from it; lact: the iteration whose local step takes it as a changed row;
+// pact: per part, the local step to run), so nothing is cleared between
+// iterations or tiles.  Values only decrease
+// and each is a path length, so the fixed point (no cross-step improvement)
+// is the exact closure whatever the order of the updates.
+template <typename T>
+using LStepCfg = TileCfg<T, kMsbfS, 64, 16, 8, 4>;
+
+constexpr int kLStepList = 2048;  // changed rows listed per part (larger parts take all rows)
+
+template <typename T>
+__global__ void bgraph_seed_kernel(T *Dt, int s0, int ns, const int32_t *__restrict__ gpart, int *xact, int *lact,
+                                   int *pact, int stamp) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= ns) return;
+  Dt[(int64_t)(s0 + s) * kMsbfS + s] = T(0);
+  xact[s0 + s] = stamp;  // the source's own cross arcs
+  lact[s0 + s] = stamp;  // and its part's rows
+  pact[__ldg(gpart + s0 + s)] = stamp;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(LStepCfg<T>::THREADS)
+    bgraph_lstep_kernel(const PartDesc *__restrict__ parts, const T *__restrict__ F, T *Dt,
+                        const int *__restrict__ pact, const int *__restrict__ lact, int stamp, int *xact) {
+  using C = LStepCfg<T>;
+  using V = typename Vec4<T>::type;
+  const PartDesc pd = parts[blockIdx.y];
+  const int c0 = blockIdx.x * C::BN;
+  if (c0 >= pd.b || __ldcg(pact + pd.part) != stamp) return;
+  __shared__ __align__(16) T smem[C::SMEM_ELEMS];
+  __shared__ int klist[kLStepList];
+  __shared__ int kcount;
+  const T inf = Dist<T>::inf();
+  const int tid = threadIdx.x, ty = tid / C::TX, tx = tid % C::TX;
+  const T *Dp = Dt + (int64_t)pd.bd_row * kMsbfS;  // rows a of the part: A^T (k = a, i = s)
+  const T *Fp = F + pd.f_off + c0;                  // rows a, columns c0..: B (k = a, j = c)
+  // the rows the last cross step (or the seed) changed
+  const bool listed = pd.b <= kLStepList;
+  if (tid == 0) kcount = 0;
+  __syncthreads();
+  if (listed)
+    for (int a = tid; a < pd.b; a += C::THREADS)
+      if (__ldcg(lact + pd.bd_row + a) == stamp) klist[atomicAdd(&kcount, 1)] = a;
+  __syncthreads();
+  const int K = listed ? kcount : pd.b;
+  if (K == 0) return;
+  auto krow = [&](int k) { return listed ? klist[k] : k; };
+  constexpr int A4 = C::BK * C::BM / 4 / C::THREADS;  // 16-byte loads per thread and chunk
+  constexpr int B4 = C::BK * C::BN / 4 / C::THREADS;
+  static_assert(A4 * 4 * C::THREADS == C::BK * C::BM && B4 * 4 * C::THREADS == C::BK * C::BN, "even");
+  V ra[A4], rb[B4];
+  auto load = [&](int k0) {
+#pragma unroll
+    for (int r = 0; r < A4; r++) {
+      const int idx = tid + r * C::THREADS, k = idx / (C::BM / 4), i4 = (idx % (C::BM / 4)) * 4;
+      if (k0 + k < K) ra[r] = __ldcg(reinterpret_cast<const V *>(Dp + (int64_t)krow(k0 + k) * kMsbfS + i4));
+      else ra[r] = V{inf, inf, inf, inf};
+    }
+#pragma unroll
+    for (int r = 0; r < B4; r++) {
+      const int idx = tid + r * C::THREADS, k = idx / (C::BN / 4), j4 = (idx % (C::BN / 4)) * 4;
+      if (k0 + k < K) rb[r] = __ldg(reinterpret_cast<const V *>(Fp + (int64_t)krow(k0 + k) * pd.ldf + j4));
+      else rb[r] = V{inf, inf, inf, inf};
+    }
+  };
+  auto store = [&](T *As, T *Bs) {
+#pragma unroll
+    for (int r = 0; r < A4; r++) {
+      const int idx = tid + r * C::THREADS, k = idx / (C::BM / 4), i4 = (idx % (C::BM / 4)) * 4;
+      *reinterpret_cast<V *>(As + k * C::AP + i4) = ra[r];
+    }
+#pragma unroll
+    for (int r = 0; r < B4; r++) {
+      const int idx = tid + r * C::THREADS, k = idx / (C::BN / 4), j4 = (idx % (C::BN / 4)) * 4;
+      *reinterpret_cast<V *>(Bs + k * C::BN + j4) = rb[r];
+    }
+  };
+  T acc[C::TM][C::TN];
+  acc_fill<T, C>(acc, inf);
+  T *const As0 = smem;
+  T *const Bs0 = smem + 2 * C::A_ELEMS;
+  const int nchunks = (int)ceil_div(K, C::BK);
+  load(0);
+  store(As0, Bs0);
+  __syncthreads();
+  for (int c = 0; c < nchunks; c++) {
+    const int cur = c & 1;
+    if (c + 1 < nchunks) load((c + 1) * C::BK);
+    mma_chunk<T, C>(As0 + cur * C::A_ELEMS, Bs0 + cur * C::B_ELEMS, acc, ty, tx, min(C::BK, K - c * C::BK));
+    if (c + 1 < nchunks) store(As0 + (cur ^ 1) * C::A_ELEMS, Bs0 + (cur ^ 1) * C::B_ELEMS);
+    __syncthreads();
+  }
+  // Rows c of the part: lower the thread's 4 consecutive sources per group.
+#pragma unroll
+  for (int gj = 0; gj < C::GN; gj++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int c = c0 + tile_col<C>(tx, gj, q);
+      if (c >= pd.b) continue;
+      T *row = Dt + ((int64_t)pd.bd_row + c) * kMsbfS;
+      bool imp = false;
+#pragma unroll
+      for (int gi = 0; gi < C::GM; gi++) {
+        const int s = tile_row<C>(ty, gi, 0);
+        V cur = __ldcg(reinterpret_cast<const V *>(row + s));
+        const T n0 = acc[4 * gi + 0][4 * gj + q], n1 = acc[4 * gi + 1][4 * gj + q];
+        const T n2 = acc[4 * gi + 2][4 * gj + q], n3 = acc[4 * gi + 3][4 * gj + q];
+        if (n0 < cur.x || n1 < cur.y || n2 < cur.z || n3 < cur.w) {
+          imp = true;
+          cur.x = min(cur.x, n0);
+          cur.y = min(cur.y, n1);
+          cur.z = min(cur.z, n2);
+          cur.w = min(cur.w, n3);
+          __stcg(reinterpret_cast<V *>(row + s), cur);
+        }
+      }
+      if (imp) xact[pd.bd_row + c] = stamp;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+    bgraph_xstep_kernel(T *Dt, const MsbfItem *__restrict__ items, int nitems, const int32_t *__restrict__ xtro,
+                        const int32_t *__restrict__ xtcol, const T *__restrict__ xtw, int *xact, int *lact,
+                        int stamp, const int32_t *__restrict__ gpart, int *pact, int *changed) {
+  const int lane = threadIdx.x & 31;
+  const int nwarps = gridDim.x * (blockDim.x >> 5);
+  auto active = [xact, stamp](int u) { return __ldcg(xact + u) == stamp; };
+  for (int it = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < nitems; it += nwarps) {
+    const MsbfItem m = items[it];
+    const int e1 = min(m.e0 + 32, __ldg(xtro + m.v + 1));
+    if (msbf_pull_row<T>(Dt, m.v, m.e0, e1, xtcol, xtw, active) && lane == 0) {
+      // (a warp that reads act[v] after this store skips v as a tail in this
+      // step; v then counts as changed in the next one)
+      xact[m.v] = stamp + 1;
+      lact[m.v] = stamp + 1;
+      pact[__ldg(gpart + m.v)] = stamp + 1;
+      *changed = 1;
+    }
+  }
+}
+
+template <typename T>
+cudaError_t launch_bgraph_bf(const PartDesc *parts, int nparts, int max_b, const T *F, const MsbfItem *xitems,
+                             int nxitems, const int32_t *xtro, const int32_t *xtcol, const T *xtw,
+                             const int32_t *gpart, int nb, int K, T *dB, int64_t ldB, T *Dt, int *act, int *pact,
+                             int *changed, int *host_changed, int64_t max_rounds, int *status, cudaStream_t stream,
+                             int64_t *launches) {
+  using C = LStepCfg<T>;
+  if (nb <= 0 || nparts <= 0) return cudaSuccess;
+  if (nparts > 65535) return cudaErrorInvalidConfiguration;
+  int *xact = act, *lact = act + nb;
+  cudaError_t e = cudaMemsetAsync(act, 0xff, (size_t)2 * nb * sizeof(int), stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(pact, 0xff, (size_t)(K + 1) * sizeof(int), stream);
+  if (e != cudaSuccess) return e;
+  const dim3 lgrid((unsigned)ceil_div(std::max(max_b, 1), C::BN), (unsigned)nparts);
+  const int xblocks = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(nxitems, 8), 148 * 8));
+  constexpr int kChunk = 4;  // iterations between convergence checks
+  int stamp = 0;
+  for (int s0 = 0; s0 < nb; s0 += kMsbfS) {
+    const int ns = std::min(kMsbfS, nb - s0);
+    e = launch_fill<T>(Dt, nb, kMsbfS, kMsbfS, Dist<T>::inf(), stream, launches);
+    if (e != cudaSuccess) return e;
+    bgraph_seed_kernel<T><<<1, kMsbfS, 0, stream>>>(Dt, s0, ns, gpart, xact, lact, pact, stamp);
+    *launches += 1;
+    bool done = false;
+    for (int64_t round = 0; !done; round += kChunk) {
+      if (round >= max_rounds) {
+        e = cudaMemcpyAsync(status, &kMsbfRoundLimit, sizeof(int), cudaMemcpyHostToDevice, stream);
+        if (e != cudaSuccess) return e;
+        break;
+      }
+      e = cudaMemsetAsync(changed, 0, kChunk * sizeof(int), stream);
+      if (e != cudaSuccess) return e;
+      for (int c = 0; c < kChunk; c++, stamp++) {
+        bgraph_lstep_kernel<T><<<lgrid, C::THREADS, 0, stream>>>(parts, F, Dt, pact, lact, stamp, xact);
+        if (nxitems > 0)
+          bgraph_xstep_kernel<T><<<xblocks, 256, 0, stream>>>(Dt, xitems, nxitems, xtro, xtcol, xtw, xact, lact,
+                                                              stamp, gpart, pact, changed + c);
+        *launches += nxitems > 0 ? 2 : 1;
+      }
+      e = cudaMemcpyAsync(host_changed, changed, kChunk * sizeof(int), cudaMemcpyDeviceToHost, stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+      if (e != cudaSuccess) return e;
+      for (int c = 0; c < kChunk; c++) done |= host_changed[c] == 0;
+    }
+    msbf_store_kernel<T><<<(unsigned)ceil_div(nb, 32), 256, 0, stream>>>(Dt, nb, s0, ns, dB, ldB, nullptr, nb);
+    *launches += 1;
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+// Expansion as one min-plus tile per CTA: rows m0.. of dB (boundary indices)
+// restricted to part q's boundary columns, times q's local rows F_q[0..b_q)
+// over its columns n0..; the register-tiled engine streams K = b_q through
+// shared memory.  Stores go to the columns' original ids (st2ed).
+template <typename T>
+__global__ void __launch_bounds__(MPCfg<T>::THREADS)
+    bdy_expand_tiled_kernel(const PartDesc *__restrict__ parts, int nbB, const int64_t *__restrict__ grow,
+                            const int32_t *__restrict__ st2ed, const T *__restrict__ dB, int64_t ldB,
+                            const T *__restrict__ F, T *D, int64_t ldD, T *FB, int64_t ldFB) {
+  using C = MPCfg<T>;
+  __shared__ __align__(16) T smem[C::SMEM_ELEMS];
+  const PartDesc pd = parts[blockIdx.z];
+  const int n0 = blockIdx.y * C::BN;
+  if (n0 >= pd.s) return;
+  const int m0 = blockIdx.x * C::BM;
+  T acc[C::TM][C::TN];
+  acc_fill<T, C>(acc, Dist<T>::inf());
+  minplus_tile<T, C, true, true>(dB + pd.bd_row, ldB, F + pd.f_off, pd.ldf, m0, n0, nbB, pd.s, pd.b, acc,
+                                 smem);
+  const int tid = threadIdx.x, ty = tid / C::TX, tx = tid % C::TX;
+  int col[C::TN];
+#pragma unroll
+  for (int gj = 0; gj < C::GN; gj++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int j = n0 + tile_col<C>(tx, gj, q);
+      col[4 * gj + q] = j < pd.s ? __ldg(st2ed + pd.start + j) : -1;
+    }
+#pragma unroll
+  for (int gi = 0; gi < C::GM; gi++)
+#pragma unroll
+    for (int l = 0; l < 4; l++) {
+      const int r = m0 + tile_row<C>(ty, gi, l);
+      if (r >= nbB) continue;
+      T *dst = D + __ldg(grow + r) * ldD;
+      const bool own = r >= pd.bd_row && r < pd.bd_row + pd.b;
+      T *fb = FB + (int64_t)r * ldFB + n0;
+#pragma unroll
+      for (int gj = 0; gj < C::GN; gj++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          const int c = col[4 * gj + q];
+          if (c < 0) continue;
+          const T v = acc[4 * gi + l][4 * gj + q];
+          __stcs(dst + c, v);
+          if (own) fb[tile_col<C>(tx, gj, q)] = v;
+        }
+    }
+}
+
+template <typename T>
+cudaError_t launch_bdy_expand_tiled(const PartDesc *parts, int nparts, int max_s, int nbB, const int64_t *grow,
+                                    const int32_t *st2ed, const T *dB, int64_t ldB, const T *F, T *D,
+                                    int64_t ldD, T *FB, int64_t ldFB, cudaStream_t stream, int64_t *launches) {
+  using C = MPCfg<T>;
+  if (nparts <= 0 || max_s <= 0 || nbB <= 0) return cudaSuccess;
+  if (nparts > 65535 || ceil_div(max_s, C::BN) > 65535) return cudaErrorInvalidConfiguration;
+  bdy_expand_tiled_kernel<T><<<dim3((unsigned)ceil_div(nbB, C::BM), (unsigned)ceil_div(max_s, C::BN), nparts),
+                               C::THREADS, 0, stream>>>(parts, nbB, grow, st2ed, dB, ldB, F, D, ldD, FB, ldFB);
+  *launches += 1;
+  return cudaGetLastError();
+}
+
 // Local closure -> exact closure of each part, in place: for inner rows i,
 //   F[i][j] = min(F[i][j], min_{k<b} F[i][k] + FB[k][j])
 // (a path from i to j either stays in the part or leaves it through a
@@ -1660,6 +1948,15 @@ cudaError_t launch_relax_peak(T *sink, int blocks, int iters, cudaStream_t strea
                                             int64_t *);                                            \
   template cudaError_t launch_local_fixup<T>(const PartDesc *, int, int, T *, const T *, int64_t,  \
                                              cudaStream_t, int64_t *);                             \
+  template cudaError_t launch_bgraph_bf<T>(const PartDesc *, int, int, const T *, const MsbfItem *, \
+                                           int, const int32_t *, const int32_t *, const T *,       \
+                                           const int32_t *, int, int, T *, int64_t, T *, int *,     \
+                                           int *, int *, int *, int64_t, int *, cudaStream_t,       \
+                                           int64_t *);                                              \
+  template cudaError_t launch_bdy_expand_tiled<T>(const PartDesc *, int, int, int, const int64_t *, \
+                                                  const int32_t *, const T *, int64_t, const T *,  \
+                                                  T *, int64_t, T *, int64_t, cudaStream_t,        \
+                                                  int64_t *);                                      \
   template cudaError_t launch_pred<T>(const PartDesc *, int, int, const T *, int32_t *, int64_t,  \
                                       int, const int32_t *, const int32_t *, const T *,            \
                                       const int32_t *, const T *, cudaStream_t, int64_t *);        \

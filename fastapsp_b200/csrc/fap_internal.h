@@ -73,7 +73,9 @@ cudaError_t launch_sssp(const int32_t *row_offset, const int32_t *col, const T *
 // sources per tile; see fap_device.cu).  items: the work list, one entry
 // per vertex and chunk of up to 32 in-edges (tro/tcol/tw, original ids);
 // sources are sorted positions (st2ed maps them to vertices); row s of the
-// output is out_rows[s] (original column order, init_cols columns).  Dt
+// output is out_rows[s] (original column order, init_cols columns).  With
+// sources == nullptr the sources are the work graph's vertices 0..num-1, and
+// with out_rows == nullptr source s goes to row s.  Dt
 // holds n x kMsbfS values, act 2 x ceil(n/32) words, changed 4 ints on the
 // device and host_changed 4 ints on the host (the launcher synchronises the
 // stream every 4 iterations to test convergence).
@@ -191,6 +193,27 @@ template <typename T>
 cudaError_t launch_bdy_expand(const int64_t *rows, int nrows, const BPart *bpart, const int32_t *graph_id,
                               const int32_t *ed2st, int n, const T *dB, int64_t ldB, int nbB, const T *F,
                               T *D, int64_t ldD, T *FB, int64_t ldFB, cudaStream_t stream, int64_t *launches);
+// Boundary graph closed by Bellman-Ford (large boundary sets), kMsbfS
+// sources at a time, alternating a local step (per part whose rows changed:
+// min-plus of the tile's rows with the part's local closure F_p) and a cross
+// step (rows with cross-part in-arcs pull from the rows the local step
+// changed; xitems over the cross in-arc CSR xtro/xtcol/xtw); gpart: part id
+// of every boundary index; Dt nb x kMsbfS; act 2 nb ints; pact K+1 ints;
+// changed 4 ints; host_changed 4 pinned ints (convergence is tested on the
+// host every 4 iterations).  Writes rows 0..nb-1 of dB (columns < nb).
+template <typename T>
+cudaError_t launch_bgraph_bf(const PartDesc *parts, int nparts, int max_b, const T *F, const MsbfItem *xitems,
+                             int nxitems, const int32_t *xtro, const int32_t *xtcol, const T *xtw,
+                             const int32_t *gpart, int nb, int K, T *dB, int64_t ldB, T *Dt, int *act, int *pact,
+                             int *changed, int *host_changed, int64_t max_rounds, int *status, cudaStream_t stream,
+                             int64_t *launches);
+// Tiled expansion (any boundary count): grid (boundary-index tiles, column
+// tiles, parts); a CTA is a min-plus tile dB[g][b'_q] (x) F_q[b'][j] written
+// to D[grow[g]][st2ed[start_q + j]] (and FB[g][j] for g of part q).
+template <typename T>
+cudaError_t launch_bdy_expand_tiled(const PartDesc *parts, int nparts, int max_s, int nbB, const int64_t *grow,
+                                    const int32_t *st2ed, const T *dB, int64_t ldB, const T *F, T *D,
+                                    int64_t ldD, T *FB, int64_t ldFB, cudaStream_t stream, int64_t *launches);
 template <typename T>
 cudaError_t launch_local_fixup(const PartDesc *parts, int nparts, int max_s, T *F, const T *FB, int64_t ldFB,
                                cudaStream_t stream, int64_t *launches);

@@ -255,6 +255,10 @@ WORKLOADS = {
     # 512x512 grid + 1% long-range edges, int weights in [1,100], K=256
     "grid512": dict(make=lambda: grid_graph(512, 512, extra_frac=0.01, wmin=1, wmax=100,
                                             seed=3), K=256),
+    # profiling-size stand-in for grid512: same part size (~1024 vertices),
+    # over 8192 boundary vertices (the Bellman-Ford closure of the boundary graph)
+    "grid256": dict(make=lambda: grid_graph(256, 256, extra_frac=0.01, wmin=1, wmax=100,
+                                            seed=5), K=64),
     # R-MAT scale 16, 2^20 directed edges, float weights, K=64
     "rmat16": dict(make=lambda: rmat_graph(16, 1 << 20, seed=4), K=64),
 }

@@ -440,10 +440,14 @@ class DeviceGraph:
         check(lib().fap_graph_block_checksums(self._h, int(part), ptr(out)), "checksums")
         return out
 
-    def cache_build(self) -> None:
+    def cache_build(self, rebuild: bool = False) -> None:
         """Builds the resident cache (every part's boundary rows and closed
-        Floyd matrix); later batched solves and rows() use it."""
-        check(lib().fap_graph_cache_build(self._h), "fap_graph_cache_build")
+        Floyd matrix); later batched solves and rows() use it.  rebuild:
+        compute it again in the same buffers even when it exists."""
+        if rebuild:
+            check(lib().fap_graph_cache_rebuild(self._h), "fap_graph_cache_rebuild")
+        else:
+            check(lib().fap_graph_cache_build(self._h), "fap_graph_cache_build")
 
     def cache_release(self) -> None:
         check(lib().fap_graph_cache_release(self._h), "fap_graph_cache_release")
@@ -489,6 +493,10 @@ class DeviceGraph:
     def last_stage1(self) -> int:
         """1 SSSP, 2 boundary graph, 3 resident cache (see fap_graph_last_stage1)."""
         return int(lib().fap_graph_last_stage1(self._h))
+
+    def stage1_name(self) -> str:
+        """How stage 1 of the last solve ran, in words (fap_graph_stage1_name)."""
+        return (lib().fap_graph_stage1_name(self._h) or b"").decode()
 
     def last_launches(self) -> int:
         x = ctypes.c_int64()

@@ -151,7 +151,12 @@ FAP_API int fap_graph_sssp_rows(fap_dgraph *g, const int32_t *sources, int32_t c
  * fap_graph_path_block; needs every edge weight > 0, else FAP_ERR_RANGE);
  * "stage1" (0 automatic, the default; 1 always SSSP; 2 the boundary graph
  * whenever the graph allows it, whatever its dtype and boundary count; see
- * fap_graph_last_stage1); "sssp_form" (how the SSSP form of stage 1 runs:
+ * fap_graph_last_stage1); "bgraph_form" (how the boundary graph is closed
+ * and expanded: 0 by size, the default, Floyd up to 8192 boundary vertices
+ * and the tiled Bellman-Ford beyond, the staged expansion up to 4096 and the
+ * tiled one beyond; 1 Floyd; 2 Bellman-Ford and the tiled expansion; the
+ * Bellman-Ford closure checks convergence on the host, so such solves are
+ * not captured in a CUDA graph); "sssp_form" (how the SSSP form of stage 1 runs:
  * 0 automatic, the default, tiled when the graph has at least 6 arcs per
  * vertex; 1 one CTA per source, near/far frontier; 2 tiled multi-source
  * Bellman-Ford, 128 sources per pass over the in-edges; the tiled form
@@ -218,6 +223,11 @@ FAP_API int fap_status_code(int32_t device_status);
  * scratch is freed again); device errors surface in fap_graph_check; a new
  * partition drops the cache. */
 FAP_API int fap_graph_cache_build(fap_dgraph *g);
+/* Computes the resident cache again even when it is built, in the same
+ * buffers (fap_graph_cache_build returns at once when the cache exists):
+ * stages 1-2 of every part, e.g. once per pass of a job whose output is
+ * produced in groups of parts. */
+FAP_API int fap_graph_cache_rebuild(fap_dgraph *g);
 FAP_API int fap_graph_cache_release(fap_dgraph *g);
 /* Device bytes the cache holds (*built = 1) or would need to be built,
  * including its SSSP scratch (*built = 0). */
@@ -230,11 +240,19 @@ FAP_API int fap_graph_last_timing(fap_dgraph *g, float *ms5);
 /* How the last fap_solve obtained the boundary rows (stage 1): 1 SSSP from
  * every boundary vertex; 2 the boundary graph (every part's local closure,
  * APSP over the boundary vertices, expansion; chosen for batches of all
- * parts of int32 graphs with at most 8192 boundary vertices and no two arcs
- * joining the same ordered pair inside a part; with "stage1" = 2 also for
- * float32 graphs, whose results then differ from the SSSP form by rounding
- * order, a few ulps); 3 the resident cache; 0 no solve yet. */
+ * parts of int32 graphs without two arcs joining the same ordered pair
+ * inside a part, when they have at most 8192 boundary vertices (closed by
+ * Floyd) or when the boundary graph has at most 8 edges per graph edge and
+ * at most 65536 vertices (closed by the tiled Bellman-Ford); with "stage1" =
+ * 2 also for float32 graphs, whose results then differ from the SSSP form by
+ * rounding order, a few ulps); 3 the resident cache; 0 no solve yet. */
 FAP_API int fap_graph_last_stage1(const fap_dgraph *g);
+
+/* How stage 1 of the last solve ran, in words: "SSSP, frontier", "SSSP,
+ * tiled Bellman-Ford", "boundary graph, Floyd closure", "boundary graph,
+ * Bellman-Ford closure", or "resident cache (<how it was built>)"; "" before
+ * the first solve.  The string lives until the next solve or cache build. */
+FAP_API const char *fap_graph_stage1_name(const fap_dgraph *g);
 
 /* Number of kernels the last fap_solve launched. */
 FAP_API int fap_graph_last_launches(fap_dgraph *g, int64_t *count);

@@ -96,3 +96,44 @@ def test_boundary_graph_with_paths(cuda_ok, name):
                                      case["bdy_num"], *args[1:])
     np.testing.assert_array_equal(P, want)
     assert O.check_paths(D, P, *args) > 0
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_bellman_ford_closure_and_tiled_expansion(cuda_ok, name):
+    """bgraph_form 2: the boundary graph closed by the tiled Bellman-Ford over
+    its in-edge CSR and the boundary rows written by the tiled expansion (the
+    automatic choice above 8192 boundary vertices), forced on every fixture:
+    the same blocks as the SSSP form and the reference, in one batch and
+    from the resident cache."""
+    case = load_golden(name)
+    K, integral = int(case["K"]), bool(case["integral"])
+    if _dup_inside_parts(case) or int(case["bdy_num"][1:].sum()) == 0:
+        pytest.skip("boundary-graph form not applicable")
+    ctx, dg = _dg(case)
+    dg.set_param("stage1", 1)
+    dg.solve(mode=FAP_MODE_BATCHED)
+    ref = _blocks(dg, K)
+    dg.set_param("stage1", 2)
+    dg.set_param("bgraph_form", 2)
+    dg.solve(mode=FAP_MODE_BATCHED)
+    dg.check()
+    assert dg.last_stage1() == 2
+    got = _blocks(dg, K)
+    _close(got, ref, integral)
+    if "dist" in case:
+        _close(got, case["dist"], integral)
+    else:
+        np.testing.assert_array_equal(O.row_checksums(O.to_i32(got)), case["row_checksums"])
+    dg.solve(mode=FAP_MODE_BATCHED)    # again: local weights refreshed, CSR reused
+    _close(_blocks(dg, K), got, True)
+    dg.cache_build()
+    dg.check()
+    held, built = dg.cache_bytes()
+    assert built and held > 0
+    dg.solve(mode=FAP_MODE_BATCHED)
+    assert dg.last_stage1() == 3
+    assert dg.stage1_name() == "resident cache (boundary graph, Bellman-Ford closure)"
+    _close(_blocks(dg, K), got, True)
+    dg.cache_build(rebuild=True)     # stages 1-2 again in the same buffers
+    dg.solve(mode=FAP_MODE_BATCHED)
+    _close(_blocks(dg, K), got, True)
