@@ -202,8 +202,8 @@ struct fap_dgraph {
   int64_t bgraph_edges = 0;  // sum_p b_p (b_p - 1) + cross-part arcs
   int64_t bgraph_cross = 0;  // cross-part arcs
   bool bg_csr_ready = false;
-  int bg_nitems = 0;
-  DevBuf d_btro, d_btcol, d_btw, d_bitems, d_bDt, d_bact, d_bpact, d_bgpart, d_grow;
+  DevBuf d_bitro, d_bitcol, d_botro, d_botcol, d_bitw;     // cross-arc CSRs (in with weights, out)
+  DevBuf d_bitems, d_bDt, d_bact, d_bpact, d_bgpart, d_grow;  // d_bitems: the two work lists
   // Tiled form of stage 1's SSSP (launch_msbf): 0 automatic (graphs with at
   // least 6 arcs per vertex, where few Bellman-Ford iterations suffice), 1
   // frontier kernel, 2 tiled.  Work items over the in-edge CSR.
@@ -418,9 +418,9 @@ extern "C" int fap_graph_destroy(fap_dgraph *G) {
                       &G->d_gid, &G->d_st2ed, &G->d_ed2st, &G->D, &G->F, &G->d_parts, &G->d_work,
                       &G->d_src, &G->d_srcrows, &G->d_status, &G->d_checks, &G->staging, &G->P,
                       &G->d_tro, &G->d_tcol, &G->d_tw, &G->d_dB, &G->d_bpart, &G->d_brows, &G->d_FB,
-                      &G->d_msbf_items, &G->d_msbf_act, &G->d_msbf_changed, &G->d_btro, &G->d_btcol,
-                      &G->d_btw, &G->d_bitems, &G->d_bDt, &G->d_bact, &G->d_bpact, &G->d_bgpart,
-                      &G->d_grow})
+                      &G->d_msbf_items, &G->d_msbf_act, &G->d_msbf_changed, &G->d_bitro, &G->d_bitcol,
+                      &G->d_botro, &G->d_botcol, &G->d_bitw, &G->d_bitems, &G->d_bDt, &G->d_bact, &G->d_bpact,
+                      &G->d_bgpart, &G->d_grow})
       b->release();
     if (G->h_changed) cudaFreeHost(G->h_changed);
     cache_drop(G);
@@ -582,9 +582,17 @@ bool bmethod_ok(const fap_dgraph *G) {
          (G->bgraph_edges <= kBgraphEdgeRatio * G->m && G->total_b <= kBgraphAutoMaxB);
 }
 
-// Cross-part in-arcs of every boundary vertex (g = boff[p] + c for the c-th
-// boundary vertex of part p) as a CSR over boundary indices, its work items
-// (up to 32 in-arcs each), and the part of every boundary index.
+// Tiles of the Bellman-Ford closure run side by side: as many as keep the
+// tiles within 96 MB (L2 holds them), at most 16.
+int bgraph_ztiles(const fap_dgraph *G) {
+  const int64_t per = std::max<int64_t>(G->total_b, 1) * kMsbfS * 4;
+  const int64_t tiles = ceil_div(std::max<int64_t>(G->total_b, 1), kMsbfS);
+  return (int)std::max<int64_t>(1, std::min<int64_t>({((int64_t)96 << 20) / per, 16, tiles}));
+}
+
+// Cross-part arcs between boundary vertices (g = boff[p] + c for the c-th
+// boundary vertex of part p) as two CSRs over boundary indices, in-arcs with
+// their weights and out-arcs, and the part of every boundary index.
 int build_bgraph_csr(fap_dgraph *G) {
   if (G->bg_csr_ready) return FAP_OK;
   const int64_t nb = G->total_b;
@@ -593,49 +601,58 @@ int build_bgraph_csr(fap_dgraph *G) {
     const int32_t l = G->ed2st[v] - G->voff[p];
     return l < G->bnum[p] ? G->boff[p] + l : -1;
   };
-  std::vector<int32_t> tro((size_t)nb + 1, 0), gpart((size_t)nb);
+  std::vector<int32_t> gpart((size_t)nb);
   for (int32_t p = 1; p <= G->K; p++)
     for (int32_t c = 0; c < G->bnum[p]; c++) gpart[G->boff[p] + c] = p;
-  for (int32_t u = 0; u < G->n; u++)
-    for (int32_t e = G->h_ro[u]; e < G->h_ro[u + 1]; e++) {
-      const int32_t v = G->h_col[e];
-      if (G->gid[v] == G->gid[u]) continue;
-      const int64_t gv = bidx(v);
-      if (gv >= 0 && bidx(u) >= 0) tro[gv + 1]++;
-    }
-  for (int64_t g = 0; g < nb; g++) tro[g + 1] += tro[g];
-  const int64_t ne = tro[nb];
-  std::vector<int32_t> tcol((size_t)std::max<int64_t>(ne, 1)), fill(tro.begin(), tro.end() - 1);
-  std::vector<uint32_t> tw((size_t)std::max<int64_t>(ne, 1), 0);
+  std::vector<int64_t> au, av;  // arcs (boundary indices) in CSR order
+  std::vector<uint32_t> aw;
   for (int32_t u = 0; u < G->n; u++)
     for (int32_t e = G->h_ro[u]; e < G->h_ro[u + 1]; e++) {
       const int32_t v = G->h_col[e];
       if (G->gid[v] == G->gid[u]) continue;
       const int64_t gu = bidx(u), gv = bidx(v);
       if (gu < 0 || gv < 0) continue;
-      tcol[fill[gv]] = (int32_t)gu;
-      tw[fill[gv]++] = G->h_w[e];
+      au.push_back(gu);
+      av.push_back(gv);
+      aw.push_back(G->h_w[e]);
     }
-  std::vector<MsbfItem> items;
-  for (int64_t g = 0; g < nb; g++)
-    for (int32_t e = tro[g]; e < tro[g + 1]; e += 32) items.push_back(MsbfItem{(int32_t)g, e});
-  FAP_TRY(G->d_btro.ensure(tro.size() * 4));
-  FAP_TRY(G->d_btcol.ensure(tcol.size() * 4));
-  FAP_TRY(G->d_btw.ensure(tw.size() * 4));
-  FAP_TRY(G->d_bitems.ensure(std::max<size_t>(items.size(), 1) * sizeof(MsbfItem)));
+  const size_t ne = au.size();
+  std::vector<int32_t> itro((size_t)nb + 1, 0), otro((size_t)nb + 1, 0);
+  for (size_t a = 0; a < ne; a++) {
+    itro[av[a] + 1]++;
+    otro[au[a] + 1]++;
+  }
+  for (int64_t g = 0; g < nb; g++) {
+    itro[g + 1] += itro[g];
+    otro[g + 1] += otro[g];
+  }
+  std::vector<int32_t> itcol(std::max<size_t>(ne, 1)), otcol(std::max<size_t>(ne, 1));
+  std::vector<uint32_t> itw(std::max<size_t>(ne, 1), 0);
+  std::vector<int32_t> ifill(itro.begin(), itro.end() - 1), ofill(otro.begin(), otro.end() - 1);
+  for (size_t a = 0; a < ne; a++) {
+    itcol[ifill[av[a]]] = (int32_t)au[a];
+    itw[ifill[av[a]]++] = aw[a];
+    otcol[ofill[au[a]]++] = (int32_t)av[a];
+  }
+  const int z = bgraph_ztiles(G);
+  FAP_TRY(G->d_bitro.ensure(itro.size() * 4));
+  FAP_TRY(G->d_bitcol.ensure(itcol.size() * 4));
+  FAP_TRY(G->d_bitw.ensure(itw.size() * 4));
+  FAP_TRY(G->d_botro.ensure(otro.size() * 4));
+  FAP_TRY(G->d_botcol.ensure(otcol.size() * 4));
   FAP_TRY(G->d_bgpart.ensure((size_t)nb * 4));
-  FAP_TRY(G->d_bDt.ensure((size_t)nb * kMsbfS * 4));
-  FAP_TRY(G->d_bact.ensure((size_t)2 * nb * 4));
-  FAP_TRY(G->d_bpact.ensure((size_t)(G->K + 1) * 4));
+  FAP_TRY(G->d_bDt.ensure((size_t)z * nb * kMsbfS * 4));
+  FAP_TRY(G->d_bact.ensure((size_t)3 * z * nb * 4));
+  FAP_TRY(G->d_bpact.ensure((size_t)z * (G->K + 1) * 4));
+  FAP_TRY(G->d_bitems.ensure((size_t)2 * z * nb * 4 + 4 * sizeof(int)));  // two work lists + counts
   FAP_TRY(G->d_msbf_changed.ensure(4 * sizeof(int)));
   if (!G->h_changed) FAP_CK(cudaHostAlloc(reinterpret_cast<void **>(&G->h_changed), 4 * sizeof(int), 0));
-  FAP_CK(cudaMemcpy(G->d_btro.p, tro.data(), tro.size() * 4, cudaMemcpyHostToDevice));
-  FAP_CK(cudaMemcpy(G->d_btcol.p, tcol.data(), tcol.size() * 4, cudaMemcpyHostToDevice));
-  FAP_CK(cudaMemcpy(G->d_btw.p, tw.data(), tw.size() * 4, cudaMemcpyHostToDevice));
+  FAP_CK(cudaMemcpy(G->d_bitro.p, itro.data(), itro.size() * 4, cudaMemcpyHostToDevice));
+  FAP_CK(cudaMemcpy(G->d_bitcol.p, itcol.data(), itcol.size() * 4, cudaMemcpyHostToDevice));
+  FAP_CK(cudaMemcpy(G->d_bitw.p, itw.data(), itw.size() * 4, cudaMemcpyHostToDevice));
+  FAP_CK(cudaMemcpy(G->d_botro.p, otro.data(), otro.size() * 4, cudaMemcpyHostToDevice));
+  FAP_CK(cudaMemcpy(G->d_botcol.p, otcol.data(), otcol.size() * 4, cudaMemcpyHostToDevice));
   FAP_CK(cudaMemcpy(G->d_bgpart.p, gpart.data(), gpart.size() * 4, cudaMemcpyHostToDevice));
-  if (!items.empty())
-    FAP_CK(cudaMemcpy(G->d_bitems.p, items.data(), items.size() * sizeof(MsbfItem), cudaMemcpyHostToDevice));
-  G->bg_nitems = (int)items.size();
   G->bg_csr_ready = true;
   return FAP_OK;
 }
@@ -692,10 +709,13 @@ int close_bgraph(fap_dgraph *G, const PartDesc *dp, int np, int max_b, const T *
     FAP_CK(launch_floyd_matrix<T>(dB, G->ldB, (int)(G->ldB / kFloydTile), status, st, L));
     return FAP_OK;
   }
-  FAP_CK(launch_bgraph_bf<T>(dp, np, max_b, F, G->d_bitems.as<const MsbfItem>(), G->bg_nitems,
-                             G->d_btro.as<const int32_t>(), G->d_btcol.as<const int32_t>(), G->d_btw.as<const T>(),
-                             G->d_bgpart.as<const int32_t>(), (int)G->total_b, G->K, dB, G->ldB, G->d_bDt.as<T>(),
-                             G->d_bact.as<int>(), G->d_bpact.as<int>(), G->d_msbf_changed.as<int>(), G->h_changed,
+  const int z = bgraph_ztiles(G);
+  int *wl = G->d_bitems.as<int>();
+  FAP_CK(launch_bgraph_bf<T>(dp, np, max_b, F, G->d_bitro.as<const int32_t>(), G->d_bitcol.as<const int32_t>(),
+                             G->d_bitw.as<const T>(), G->d_botro.as<const int32_t>(), G->d_botcol.as<const int32_t>(),
+                             G->d_bgpart.as<const int32_t>(), (int)G->total_b, G->K, z, dB,
+                             G->ldB, G->d_bDt.as<T>(), G->d_bact.as<int>(), G->d_bpact.as<int>(), wl,
+                             wl + (int64_t)2 * z * G->total_b, G->d_msbf_changed.as<int>(), G->h_changed,
                              max_rounds, status, st, L));
   return FAP_OK;
 }
@@ -1674,7 +1694,7 @@ extern "C" int fap_graph_device_bytes(const fap_dgraph *G, int64_t *bytes) {
                           &G->cBd, &G->cF, &G->d_cparts, &G->d_rowgroups, &G->d_rowloc, &G->d_rowout,
                           &G->d_rowidx, &G->P, &G->d_tro, &G->d_tcol, &G->d_tw, &G->d_dB,
                           &G->d_bpart, &G->d_brows, &G->d_FB, &G->d_msbf_items, &G->d_msbf_act,
-                          &G->d_msbf_changed, &G->d_btro, &G->d_btcol, &G->d_btw, &G->d_bitems,
+                          &G->d_msbf_changed, &G->d_bitro, &G->d_bitcol, &G->d_botro, &G->d_botcol, &G->d_bitw, &G->d_bitems,
                           &G->d_bDt, &G->d_bact, &G->d_bpact, &G->d_bgpart, &G->d_grow})
     t += (int64_t)b->bytes;
   *bytes = t;
@@ -1913,7 +1933,7 @@ extern "C" int fap_graph_cache_bytes(const fap_dgraph *G, int64_t *bytes, int *b
   if (G->cache_ready) {
     *bytes = (int64_t)(G->cBd.bytes + G->cF.bytes + G->d_cparts.bytes);
     if (G->cache_bmethod)  // the boundary graph's buffers stay for rebuilds
-      for (const DevBuf *b : {&G->d_dB, &G->d_FB, &G->d_btro, &G->d_btcol, &G->d_btw, &G->d_bitems, &G->d_bDt,
+      for (const DevBuf *b : {&G->d_dB, &G->d_FB, &G->d_bitro, &G->d_bitcol, &G->d_botro, &G->d_botcol, &G->d_bitw, &G->d_bitems, &G->d_bDt,
                               &G->d_bact, &G->d_bpact, &G->d_bgpart, &G->d_grow})
         *bytes += (int64_t)b->bytes;
   } else {
@@ -1927,12 +1947,13 @@ extern "C" int fap_graph_cache_bytes(const fap_dgraph *G, int64_t *bytes, int *b
                (int64_t)alloc_size((size_t)(G->K + 1) * sizeof(BPart)) +
                (int64_t)alloc_size((size_t)std::max<int64_t>(2 * G->total_b, 2) * 8);
       if (bgraph_tiled_expand(G)) *bytes += (int64_t)alloc_size((size_t)G->total_b * 8);
-      if (bgraph_bf(G)) {  // cross-arc CSR, work items, tile, stamps, part table
+      if (bgraph_bf(G)) {  // cross-arc CSR, work lists, tiles, stamps, part table
         const int64_t xe = std::max<int64_t>(G->bgraph_cross, 1);
-        *bytes += 2 * (int64_t)alloc_size((size_t)(G->total_b + 1) * 4) + 2 * (int64_t)alloc_size((size_t)xe * 4) +
-                  (int64_t)alloc_size((size_t)(xe / 32 + G->total_b + 1) * sizeof(MsbfItem)) +
-                  (int64_t)alloc_size((size_t)G->total_b * kMsbfS * 4) +
-                  (int64_t)alloc_size((size_t)2 * G->total_b * 4) + (int64_t)alloc_size((size_t)(G->K + 1) * 4);
+        *bytes += 3 * (int64_t)alloc_size((size_t)(G->total_b + 1) * 4) + 3 * (int64_t)alloc_size((size_t)xe * 4) +
+                  (int64_t)alloc_size((size_t)2 * bgraph_ztiles(G) * G->total_b * 4 + 4 * sizeof(int)) +
+                  (int64_t)alloc_size((size_t)bgraph_ztiles(G) * G->total_b * kMsbfS * 4) +
+                  (int64_t)alloc_size((size_t)3 * bgraph_ztiles(G) * G->total_b * 4) +
+                  (int64_t)alloc_size((size_t)bgraph_ztiles(G) * (G->K + 1) * 4);
       }
     } else {
       *bytes = cs.bytes(G) + (int64_t)alloc_size(

@@ -1289,13 +1289,19 @@ cudaError_t launch_bdy_expand(const int64_t *rows, int nrows, const BPart *bpart
 //   before, and F_p is transitive): a min-plus product run from shared
 //   memory, 128 sources x 64 columns per CTA, K = the changed rows; rows
 //   that improve are stamped for the cross step;
-//   cross step: rows with cross-part in-arcs pull from stamped tails
-//   (msbf_pull_row) and stamp their parts for the next local step.
-// Stamps are iteration numbers (xact: per boundary vertex, the iteration in
-// which its row changed, by either step, so that the next cross step pulls
-// from it; lact: the iteration whose local step takes it as a changed row;
-// pact: per part, the local step to run), so nothing is cleared between
-// iterations or tiles.  Values only decrease
+//   cross step: every head of a cross-part arc whose tail row changed since
+//   the last cross step (a work list) pulls over its cross-part in-arcs (one
+//   warp per head row, plain stores); heads that improve put their own
+//   arcs' heads on the next list and stamp their parts for the next local
+//   step.
+// Stamps are iteration numbers (per boundary vertex: cact, the list its
+// out-arcs' heads last went to; hact, the list it last joined as a head;
+// lact, the iteration whose local step takes it as a changed row; per part:
+// pact, the local step to run), so nothing is cleared between iterations or
+// tiles.  The work list of iteration t (entries z * nb + g) is filled by the
+// cross step t - 1 and the local step t and read by the cross step t; lists
+// alternate between two buffers by parity, and the local step t empties the
+// list t + 1 before the cross step t fills it.  Values only decrease
 // and each is a path length, so the fixed point (no cross-step improvement)
 // is the exact closure whatever the order of the updates.
 template <typename T>
@@ -1303,26 +1309,55 @@ using LStepCfg = TileCfg<T, kMsbfS, 64, 16, 8, 4>;
 
 constexpr int kLStepList = 2048;  // changed rows listed per part (larger parts take all rows)
 
+// Several tiles run side by side (blockIdx.z / the item range): tile z has
+// its own Dt, xact, lact (nb each) and pact (K + 1) at offset z; its sources
+// are s0 + z * kMsbfS + s for s < kMsbfS and below nb.
+// Row g of tile z changed: the heads of g's cross-part out-arcs join the
+// work list of iteration `stamp` (each row's heads once per list, each head
+// once per list).  cact/hact point at tile z's stamps.
+__device__ __forceinline__ void bgraph_mark_heads(int g, int64_t znb, int *cact, int *hact, int stamp,
+                                                  const int32_t *__restrict__ otro,
+                                                  const int32_t *__restrict__ otcol, int *wl, int *wl_count) {
+  if (atomicExch(cact + g, stamp) == stamp) return;
+  const int e1 = __ldg(otro + g + 1);
+  for (int e = __ldg(otro + g); e < e1; e++) {
+    const int h = __ldg(otcol + e);
+    if (atomicExch(hact + h, stamp) != stamp)
+      wl[(stamp & 1) * (int64_t)wl_count[2] + atomicAdd(wl_count + (stamp & 1), 1)] = (int)(znb + h);
+  }
+}
+
 template <typename T>
-__global__ void bgraph_seed_kernel(T *Dt, int s0, int ns, const int32_t *__restrict__ gpart, int *xact, int *lact,
-                                   int *pact, int stamp) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= ns) return;
-  Dt[(int64_t)(s0 + s) * kMsbfS + s] = T(0);
-  xact[s0 + s] = stamp;  // the source's own cross arcs
-  lact[s0 + s] = stamp;  // and its part's rows
-  pact[__ldg(gpart + s0 + s)] = stamp;
+__global__ void bgraph_seed_kernel(T *Dt, int s0, int nb, int K1, const int32_t *__restrict__ gpart, int *cact,
+                                   int *hact, int *lact, int *pact, int stamp, const int32_t *__restrict__ otro,
+                                   const int32_t *__restrict__ otcol, int *wl, int *wl_count) {
+  const int z = blockIdx.y, s = threadIdx.x;
+  const int g = s0 + z * kMsbfS + s;
+  if (g >= nb) return;
+  const int64_t znb = (int64_t)z * nb;
+  Dt[(znb + g) * kMsbfS + s] = T(0);
+  bgraph_mark_heads(g, znb, cact + znb, hact + znb, stamp, otro, otcol, wl, wl_count);  // its cross arcs
+  lact[znb + g] = stamp;  // and its part's rows
+  pact[(int64_t)z * K1 + __ldg(gpart + g)] = stamp;
 }
 
 template <typename T>
 __global__ void __launch_bounds__(LStepCfg<T>::THREADS)
-    bgraph_lstep_kernel(const PartDesc *__restrict__ parts, const T *__restrict__ F, T *Dt,
-                        const int *__restrict__ pact, const int *__restrict__ lact, int stamp, int *xact) {
+    bgraph_lstep_kernel(const PartDesc *__restrict__ parts, const T *__restrict__ F, T *Dt, int nb, int K1,
+                        const int *__restrict__ pact, const int *__restrict__ lact, int stamp, int *cact, int *hact,
+                        const int32_t *__restrict__ otro, const int32_t *__restrict__ otcol, int *wl,
+                        int *wl_count) {
   using C = LStepCfg<T>;
   using V = typename Vec4<T>::type;
+  if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0) wl_count[(stamp + 1) & 1] = 0;
   const PartDesc pd = parts[blockIdx.y];
   const int c0 = blockIdx.x * C::BN;
-  if (c0 >= pd.b || __ldcg(pact + pd.part) != stamp) return;
+  const int64_t z = blockIdx.z;
+  if (c0 >= pd.b || __ldcg(pact + z * K1 + pd.part) != stamp) return;
+  Dt += z * nb * kMsbfS;
+  lact += z * nb;
+  cact += z * nb;
+  hact += z * nb;
   __shared__ __align__(16) T smem[C::SMEM_ELEMS];
   __shared__ int klist[kLStepList];
   __shared__ int kcount;
@@ -1410,54 +1445,95 @@ __global__ void __launch_bounds__(LStepCfg<T>::THREADS)
           __stcg(reinterpret_cast<V *>(row + s), cur);
         }
       }
-      if (imp) xact[pd.bd_row + c] = stamp;
+      if (imp) bgraph_mark_heads(pd.bd_row + c, z * nb, cact, hact, stamp, otro, otcol, wl, wl_count);
     }
 }
 
 template <typename T>
 __global__ void __launch_bounds__(256)
-    bgraph_xstep_kernel(T *Dt, const MsbfItem *__restrict__ items, int nitems, const int32_t *__restrict__ xtro,
-                        const int32_t *__restrict__ xtcol, const T *__restrict__ xtw, int *xact, int *lact,
-                        int stamp, const int32_t *__restrict__ gpart, int *pact, int *changed) {
+    bgraph_xstep_kernel(T *Dt, int nb, int K1, const int32_t *__restrict__ itro, const int32_t *__restrict__ itcol,
+                        const T *__restrict__ itw, const int32_t *__restrict__ otro,
+                        const int32_t *__restrict__ otcol, int *cact, int *hact, int *lact, int stamp,
+                        const int32_t *__restrict__ gpart, int *pact, int *wl, int *wl_count, int *changed) {
+  using V = typename Vec4<T>::type;
+  const T inf = Dist<T>::inf();
   const int lane = threadIdx.x & 31;
   const int nwarps = gridDim.x * (blockDim.x >> 5);
-  auto active = [xact, stamp](int u) { return __ldcg(xact + u) == stamp; };
-  for (int it = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < nitems; it += nwarps) {
-    const MsbfItem m = items[it];
-    const int e1 = min(m.e0 + 32, __ldg(xtro + m.v + 1));
-    if (msbf_pull_row<T>(Dt, m.v, m.e0, e1, xtcol, xtw, active) && lane == 0) {
-      // (a warp that reads act[v] after this store skips v as a tail in this
-      // step; v then counts as changed in the next one)
-      xact[m.v] = stamp + 1;
-      lact[m.v] = stamp + 1;
-      pact[__ldg(gpart + m.v)] = stamp + 1;
+  const int count = __ldcg(wl_count + (stamp & 1));
+  const int *list = wl + (stamp & 1) * (int64_t)wl_count[2];
+  for (int it = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < count; it += nwarps) {
+    const int entry = __ldcg(list + it);
+    const int64_t z = entry / nb;
+    const int v = entry - (int)(z * nb);
+    T *Dz = Dt + z * nb * kMsbfS;
+    T acc[4] = {inf, inf, inf, inf};
+    const int e0 = __ldg(itro + v), e1 = __ldg(itro + v + 1);
+    for (int e = e0; e < e1; e += 4) {  // four tail rows in flight
+      V d[4];
+      T w[4];
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+        if (e + q < e1) {
+          d[q] = __ldcg(reinterpret_cast<const V *>(Dz + (int64_t)__ldg(itcol + e + q) * kMsbfS) + lane);
+          w[q] = __ldg(itw + e + q);
+        }
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+        if (e + q < e1) {
+          acc[0] = Dist<T>::relax(d[q].x, w[q], acc[0]);
+          acc[1] = Dist<T>::relax(d[q].y, w[q], acc[1]);
+          acc[2] = Dist<T>::relax(d[q].z, w[q], acc[2]);
+          acc[3] = Dist<T>::relax(d[q].w, w[q], acc[3]);
+        }
+    }
+    V *row = reinterpret_cast<V *>(Dz + (int64_t)v * kMsbfS) + lane;
+    V cur = __ldcg(row);
+    const bool imp = acc[0] < cur.x || acc[1] < cur.y || acc[2] < cur.z || acc[3] < cur.w;
+    if (imp) {  // this warp is the row's only writer in this step
+      cur.x = min(cur.x, acc[0]);
+      cur.y = min(cur.y, acc[1]);
+      cur.z = min(cur.z, acc[2]);
+      cur.w = min(cur.w, acc[3]);
+      __stcg(row, cur);
+    }
+    if (__any_sync(0xffffffffu, imp) && lane == 0) {
+      bgraph_mark_heads(v, z * nb, cact + z * nb, hact + z * nb, stamp + 1, otro, otcol, wl, wl_count);
+      lact[z * nb + v] = stamp + 1;
+      pact[z * K1 + __ldg(gpart + v)] = stamp + 1;
       *changed = 1;
     }
   }
 }
 
 template <typename T>
-cudaError_t launch_bgraph_bf(const PartDesc *parts, int nparts, int max_b, const T *F, const MsbfItem *xitems,
-                             int nxitems, const int32_t *xtro, const int32_t *xtcol, const T *xtw,
-                             const int32_t *gpart, int nb, int K, T *dB, int64_t ldB, T *Dt, int *act, int *pact,
-                             int *changed, int *host_changed, int64_t max_rounds, int *status, cudaStream_t stream,
-                             int64_t *launches) {
+cudaError_t launch_bgraph_bf(const PartDesc *parts, int nparts, int max_b, const T *F, const int32_t *itro,
+                             const int32_t *itcol, const T *itw, const int32_t *otro, const int32_t *otcol,
+                             const int32_t *gpart, int nb, int K, int ztiles, T *dB, int64_t ldB, T *Dt, int *act,
+                             int *pact, int *wl, int *wl_count, int *changed, int *host_changed, int64_t max_rounds,
+                             int *status, cudaStream_t stream, int64_t *launches) {
   using C = LStepCfg<T>;
   if (nb <= 0 || nparts <= 0) return cudaSuccess;
-  if (nparts > 65535) return cudaErrorInvalidConfiguration;
-  int *xact = act, *lact = act + nb;
-  cudaError_t e = cudaMemsetAsync(act, 0xff, (size_t)2 * nb * sizeof(int), stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(pact, 0xff, (size_t)(K + 1) * sizeof(int), stream);
+  if (nparts > 65535 || ztiles < 1 || ztiles > 64) return cudaErrorInvalidConfiguration;
+  const int K1 = K + 1;
+  int *cact = act, *hact = act + (int64_t)ztiles * nb, *lact = act + (int64_t)2 * ztiles * nb;
+  if ((int64_t)ztiles * nb >= INT32_MAX) return cudaErrorInvalidValue;
+  cudaError_t e = cudaMemsetAsync(act, 0xff, (size_t)3 * ztiles * nb * sizeof(int), stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(pact, 0xff, (size_t)ztiles * K1 * sizeof(int), stream);
+  // wl_count: the two lists' lengths and the capacity of each list
+  const int counts[3] = {0, 0, ztiles * nb};
+  if (e == cudaSuccess) e = cudaMemcpyAsync(wl_count, counts, sizeof(counts), cudaMemcpyHostToDevice, stream);
   if (e != cudaSuccess) return e;
-  const dim3 lgrid((unsigned)ceil_div(std::max(max_b, 1), C::BN), (unsigned)nparts);
-  const int xblocks = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(nxitems, 8), 148 * 8));
   constexpr int kChunk = 4;  // iterations between convergence checks
   int stamp = 0;
-  for (int s0 = 0; s0 < nb; s0 += kMsbfS) {
-    const int ns = std::min(kMsbfS, nb - s0);
-    e = launch_fill<T>(Dt, nb, kMsbfS, kMsbfS, Dist<T>::inf(), stream, launches);
+  for (int s0 = 0; s0 < nb; s0 += ztiles * kMsbfS) {
+    const int z = (int)std::min<int64_t>(ztiles, ceil_div(nb - s0, kMsbfS));  // tiles side by side
+    const dim3 lgrid((unsigned)ceil_div(std::max(max_b, 1), C::BN), (unsigned)nparts, (unsigned)z);
+    const int xblocks = 148 * 5;  // about the resident limit at 256 threads
+    e = launch_fill<T>(Dt, (int64_t)z * nb, kMsbfS, kMsbfS, Dist<T>::inf(), stream, launches);
+    if (e == cudaSuccess) e = cudaMemsetAsync(wl_count, 0, 2 * sizeof(int), stream);
     if (e != cudaSuccess) return e;
-    bgraph_seed_kernel<T><<<1, kMsbfS, 0, stream>>>(Dt, s0, ns, gpart, xact, lact, pact, stamp);
+    bgraph_seed_kernel<T><<<dim3(1, z), kMsbfS, 0, stream>>>(Dt, s0, nb, K1, gpart, cact, hact, lact, pact, stamp,
+                                                            otro, otcol, wl, wl_count);
     *launches += 1;
     bool done = false;
     for (int64_t round = 0; !done; round += kChunk) {
@@ -1469,19 +1545,24 @@ cudaError_t launch_bgraph_bf(const PartDesc *parts, int nparts, int max_b, const
       e = cudaMemsetAsync(changed, 0, kChunk * sizeof(int), stream);
       if (e != cudaSuccess) return e;
       for (int c = 0; c < kChunk; c++, stamp++) {
-        bgraph_lstep_kernel<T><<<lgrid, C::THREADS, 0, stream>>>(parts, F, Dt, pact, lact, stamp, xact);
-        if (nxitems > 0)
-          bgraph_xstep_kernel<T><<<xblocks, 256, 0, stream>>>(Dt, xitems, nxitems, xtro, xtcol, xtw, xact, lact,
-                                                              stamp, gpart, pact, changed + c);
-        *launches += nxitems > 0 ? 2 : 1;
+        bgraph_lstep_kernel<T><<<lgrid, C::THREADS, 0, stream>>>(parts, F, Dt, nb, K1, pact, lact, stamp, cact, hact,
+                                                                 otro, otcol, wl, wl_count);
+        bgraph_xstep_kernel<T><<<xblocks, 256, 0, stream>>>(Dt, nb, K1, itro, itcol, itw, otro, otcol, cact, hact,
+                                                            lact, stamp, gpart, pact, wl, wl_count, changed + c);
+        *launches += 2;
       }
       e = cudaMemcpyAsync(host_changed, changed, kChunk * sizeof(int), cudaMemcpyDeviceToHost, stream);
       if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
       if (e != cudaSuccess) return e;
       for (int c = 0; c < kChunk; c++) done |= host_changed[c] == 0;
     }
-    msbf_store_kernel<T><<<(unsigned)ceil_div(nb, 32), 256, 0, stream>>>(Dt, nb, s0, ns, dB, ldB, nullptr, nb);
-    *launches += 1;
+    for (int q = 0; q < z; q++) {
+      const int sq = s0 + q * kMsbfS;
+      msbf_store_kernel<T><<<(unsigned)ceil_div(nb, 32), 256, 0, stream>>>(Dt + (int64_t)q * nb * kMsbfS, nb, sq,
+                                                                          std::min(kMsbfS, nb - sq), dB, ldB,
+                                                                          nullptr, nb);
+    }
+    *launches += z;
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
@@ -1493,7 +1574,7 @@ cudaError_t launch_bgraph_bf(const PartDesc *parts, int nparts, int max_b, const
 // over its columns n0..; the register-tiled engine streams K = b_q through
 // shared memory.  Stores go to the columns' original ids (st2ed).
 template <typename T>
-__global__ void __launch_bounds__(MPCfg<T>::THREADS)
+__global__ void __launch_bounds__(MPCfg<T>::THREADS, 2)
     bdy_expand_tiled_kernel(const PartDesc *__restrict__ parts, int nbB, const int64_t *__restrict__ grow,
                             const int32_t *__restrict__ st2ed, const T *__restrict__ dB, int64_t ldB,
                             const T *__restrict__ F, T *D, int64_t ldD, T *FB, int64_t ldFB) {
@@ -1555,10 +1636,46 @@ cudaError_t launch_bdy_expand_tiled(const PartDesc *parts, int nparts, int max_s
 //   F[i][j] = min(F[i][j], min_{k<b} F[i][k] + FB[k][j])
 // (a path from i to j either stays in the part or leaves it through a
 // boundary vertex k first, after which FB holds the exact rest).  The
-// boundary rows of F take FB's values.  grid (parts, row chunks of 32).
+// boundary rows of F take FB's values.  Two launches, so that every row
+// reads its local values F[i][0..b) before they change:
+//   1. columns j >= b of the inner rows, one min-plus tile (A = F[i][k],
+//      B = FB[k][j]) per CTA, grid (column tiles, row tiles, parts);
+//   2. columns j < b of the inner rows (each CTA stages its rows' local
+//      values first) and the boundary rows, grid (parts, row chunks of 32).
 constexpr int kFixRows = 32;
 
 constexpr int kFixStage = 4096;  // staged values per CTA: rows x boundary count
+
+template <typename T>
+__global__ void __launch_bounds__(MPCfg<T>::THREADS, 2)
+    local_fixup_tile_kernel(const PartDesc *__restrict__ parts, T *F, const T *__restrict__ FB, int64_t ldFB) {
+  using C = MPCfg<T>;
+  __shared__ __align__(16) T smem[C::SMEM_ELEMS];
+  const PartDesc pd = parts[blockIdx.z];
+  const int n0 = blockIdx.x * C::BN, m0 = blockIdx.y * C::BM;
+  const int M = pd.s - pd.b;
+  if (n0 + C::BN <= pd.b || n0 >= pd.s || m0 >= M || pd.b == 0) return;
+  T *Fi = F + pd.f_off + (int64_t)pd.b * pd.ldf;  // inner rows
+  T acc[C::TM][C::TN];
+  acc_load<T, C, false>(acc, Fi, pd.ldf, m0, n0, M, pd.s);
+  minplus_tile<T, C, true, true>(Fi, pd.ldf, FB + (int64_t)pd.bd_row * ldFB, ldFB, m0, n0, M, pd.s, pd.b, acc,
+                                 smem);
+  const int tid = threadIdx.x, ty = tid / C::TX, tx = tid % C::TX;
+#pragma unroll
+  for (int gi = 0; gi < C::GM; gi++)
+#pragma unroll
+    for (int l = 0; l < 4; l++) {
+      const int r = m0 + tile_row<C>(ty, gi, l);
+      if (r >= M) continue;
+#pragma unroll
+      for (int gj = 0; gj < C::GN; gj++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          const int c = n0 + tile_col<C>(tx, gj, q);
+          if (c >= pd.b && c < pd.s) Fi[(int64_t)r * pd.ldf + c] = acc[4 * gi + l][4 * gj + q];
+        }
+    }
+}
 
 template <typename T>
 __global__ void __launch_bounds__(256)
@@ -1578,14 +1695,24 @@ __global__ void __launch_bounds__(256)
     }
   }
   __syncthreads();
-  for (int j = threadIdx.x; j < pd.s; j += blockDim.x) {
-    for (int i = i0; i < i1; i++) {
-      T *Fi = F + pd.f_off + (int64_t)i * pd.ldf;
-      if (i < pd.b) {
-        Fi[j] = FBp[(int64_t)i * ldFB + j];
-        continue;
-      }
-      const T *ai = staged ? a_s + (int64_t)(i - i0) * pd.b : Fi;
+  const bool row_staged = !staged && pd.b <= kFixStage;  // one row at a time
+  for (int i = i0; i < i1; i++) {
+    T *Fi = F + pd.f_off + (int64_t)i * pd.ldf;
+    if (i < pd.b) {
+      for (int j = threadIdx.x; j < pd.s; j += blockDim.x) Fi[j] = FBp[(int64_t)i * ldFB + j];
+      continue;
+    }
+    // columns j < b only (the tile launch did the rest)
+    if (row_staged) {
+      __syncthreads();
+      for (int k = threadIdx.x; k < pd.b; k += blockDim.x) a_s[k] = Fi[k];
+      __syncthreads();
+    }
+    // (more than kFixStage boundary vertices: the row reads values that other
+    // threads may already have lowered to the exact ones, which gives the
+    // same minimum in int32)
+    const T *ai = staged ? a_s + (int64_t)(i - i0) * pd.b : row_staged ? a_s : Fi;
+    for (int j = threadIdx.x; j < pd.b; j += blockDim.x) {
       T acc = Fi[j];
       for (int k = 0; k < pd.b; k++) acc = Dist<T>::relax(ai[k], FBp[(int64_t)k * ldFB + j], acc);
       Fi[j] = acc;
@@ -1596,10 +1723,14 @@ __global__ void __launch_bounds__(256)
 template <typename T>
 cudaError_t launch_local_fixup(const PartDesc *parts, int nparts, int max_s, T *F, const T *FB, int64_t ldFB,
                                cudaStream_t stream, int64_t *launches) {
+  using C = MPCfg<T>;
   if (nparts <= 0 || max_s <= 0) return cudaSuccess;
+  if (nparts > 65535) return cudaErrorInvalidConfiguration;
+  local_fixup_tile_kernel<T><<<dim3((unsigned)ceil_div(max_s, C::BN), (unsigned)ceil_div(max_s, C::BM), nparts),
+                               C::THREADS, 0, stream>>>(parts, F, FB, ldFB);
   local_fixup_kernel<T><<<dim3(nparts, (unsigned)ceil_div(max_s, kFixRows)), 256, 0, stream>>>(parts, F, FB,
                                                                                               ldFB);
-  *launches += 1;
+  *launches += 2;
   return cudaGetLastError();
 }
 
@@ -1948,11 +2079,11 @@ cudaError_t launch_relax_peak(T *sink, int blocks, int iters, cudaStream_t strea
                                             int64_t *);                                            \
   template cudaError_t launch_local_fixup<T>(const PartDesc *, int, int, T *, const T *, int64_t,  \
                                              cudaStream_t, int64_t *);                             \
-  template cudaError_t launch_bgraph_bf<T>(const PartDesc *, int, int, const T *, const MsbfItem *, \
-                                           int, const int32_t *, const int32_t *, const T *,       \
-                                           const int32_t *, int, int, T *, int64_t, T *, int *,     \
-                                           int *, int *, int *, int64_t, int *, cudaStream_t,       \
-                                           int64_t *);                                              \
+  template cudaError_t launch_bgraph_bf<T>(const PartDesc *, int, int, const T *, const int32_t *,  \
+                                           const int32_t *, const T *, const int32_t *,              \
+                                           const int32_t *, const int32_t *, int, int, int, T *,     \
+                                           int64_t, T *, int *, int *, int *, int *, int *, int *,   \
+                                           int64_t, int *, cudaStream_t, int64_t *);                 \
   template cudaError_t launch_bdy_expand_tiled<T>(const PartDesc *, int, int, int, const int64_t *, \
                                                   const int32_t *, const T *, int64_t, const T *,  \
                                                   T *, int64_t, T *, int64_t, cudaStream_t,        \

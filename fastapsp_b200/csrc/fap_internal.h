@@ -193,20 +193,23 @@ template <typename T>
 cudaError_t launch_bdy_expand(const int64_t *rows, int nrows, const BPart *bpart, const int32_t *graph_id,
                               const int32_t *ed2st, int n, const T *dB, int64_t ldB, int nbB, const T *F,
                               T *D, int64_t ldD, T *FB, int64_t ldFB, cudaStream_t stream, int64_t *launches);
-// Boundary graph closed by Bellman-Ford (large boundary sets), kMsbfS
-// sources at a time, alternating a local step (per part whose rows changed:
-// min-plus of the tile's rows with the part's local closure F_p) and a cross
-// step (rows with cross-part in-arcs pull from the rows the local step
-// changed; xitems over the cross in-arc CSR xtro/xtcol/xtw); gpart: part id
-// of every boundary index; Dt nb x kMsbfS; act 2 nb ints; pact K+1 ints;
-// changed 4 ints; host_changed 4 pinned ints (convergence is tested on the
-// host every 4 iterations).  Writes rows 0..nb-1 of dB (columns < nb).
+// Boundary graph closed by Bellman-Ford (large boundary sets), ztiles tiles
+// of kMsbfS sources side by side, alternating a local step (per part whose
+// rows changed: min-plus of the tile's rows with the part's local closure
+// F_p) and a cross step (the heads of cross-part arcs whose tails changed
+// pull over their cross-part in-arcs; CSRs over boundary indices: in-arcs
+// itro/itcol/itw, out-arcs otro/otcol); gpart: part id of every boundary
+// index; Dt ztiles x nb x kMsbfS; act 3 x ztiles x nb ints; pact ztiles x
+// (K + 1) ints; wl 2 x ztiles x nb ints
+// (two work lists); wl_count 3 ints; changed 4 ints; host_changed 4 pinned
+// ints (convergence is tested on the host every 4 iterations).  Writes rows
+// 0..nb-1 of dB (columns < nb).
 template <typename T>
-cudaError_t launch_bgraph_bf(const PartDesc *parts, int nparts, int max_b, const T *F, const MsbfItem *xitems,
-                             int nxitems, const int32_t *xtro, const int32_t *xtcol, const T *xtw,
-                             const int32_t *gpart, int nb, int K, T *dB, int64_t ldB, T *Dt, int *act, int *pact,
-                             int *changed, int *host_changed, int64_t max_rounds, int *status, cudaStream_t stream,
-                             int64_t *launches);
+cudaError_t launch_bgraph_bf(const PartDesc *parts, int nparts, int max_b, const T *F, const int32_t *itro,
+                             const int32_t *itcol, const T *itw, const int32_t *otro, const int32_t *otcol,
+                             const int32_t *gpart, int nb, int K, int ztiles, T *dB, int64_t ldB, T *Dt, int *act,
+                             int *pact, int *wl, int *wl_count, int *changed, int *host_changed, int64_t max_rounds,
+                             int *status, cudaStream_t stream, int64_t *launches);
 // Tiled expansion (any boundary count): grid (boundary-index tiles, column
 // tiles, parts); a CTA is a min-plus tile dB[g][b'_q] (x) F_q[b'][j] written
 // to D[grow[g]][st2ed[start_q + j]] (and FB[g][j] for g of part q).
