@@ -484,6 +484,7 @@ def main_fap(args):
     clocks = ClockSampler(local)
     clocks.start()
     step_ms, stages = [], []
+    cache_phases = []
     launches = 0
     for _ in range(args.steps):
         flush.zero_()
@@ -509,7 +510,15 @@ def main_fap(args):
             launches += dg.last_launches()
         if staged:   # the cache build holds stages 1-2 of every part
             cb = e0.elapsed_time(ec)
-            st_step[0] += cb
+            ct = dg.cache_timing()
+            cache_phases.append(ct)
+            if "boundary graph" in dg.stage1_name():   # local closures, closure, expansion, fix-up
+                st_step[0] += ct[1] + ct[2] + ct[3]
+                st_step[2] += ct[0]
+            else:                                       # SSSP, gather, Floyd
+                st_step[0] += ct[0]
+                st_step[1] += ct[1]
+                st_step[2] += ct[2]
             st_step[4] += cb
         stages.append(st_step)
     torch.cuda.synchronize()
@@ -675,6 +684,13 @@ def main_fap(args):
             "config": {**wl.describe(), "mode": "batched", "stage1": stage1_used,
                        "parallelism": f"parts sharded x{world}",
                        "groups": len(groups),
+                       "stage_cache": ({"note": "stages 1-2 of every part once per step (resident cache), "
+                                                "then each group's min-plus merge",
+                                        "phases_ms": np.round(np.mean(cache_phases, 0), 3).tolist(),
+                                        "phases": ("local closures, boundary-graph closure, expansion, fix-up"
+                                                   if "boundary graph" in stage1_used else
+                                                   "SSSP, gather, Floyd, -")}
+                                       if staged and cache_phases else None),
                        "sssp_delta": {"value": tuned["delta"], "factor_of_mean_weight": tuned["factor"],
                                       "bucket": tuned["key"], "from_cache": tuned["cached"]},
                        "l2": "256 MB buffer written between timed steps (outside the events); "

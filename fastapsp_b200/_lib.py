@@ -97,6 +97,7 @@ _SIGS = {
     "fap_graph_rows_async": (INT, [P, P, I32, P]),
     "fap_graph_cache_build": (INT, [P]),
     "fap_graph_cache_rebuild": (INT, [P]),
+    "fap_graph_cache_timing": (INT, [P, P]),
     "fap_graph_cache_release": (INT, [P]),
     "fap_graph_cache_bytes": (INT, [P, ctypes.POINTER(I64), ctypes.POINTER(INT)]),
     "fap_server_create": (INT, [INT, DBL, I64, PP]),

@@ -188,6 +188,7 @@ struct fap_dgraph {
   bool bnd_dupfree = false;
   int64_t total_b = 0;
   std::vector<int32_t> boff;
+  std::vector<int32_t> bpcol;  // boundary columns of dB padded per part to multiples of 4 (prefix sums)
   bool last_bmethod = false;   // the prepared batch uses it
   bool cache_bmethod = false;  // the resident cache was built with it
   int64_t ldB = 0;
@@ -203,7 +204,7 @@ struct fap_dgraph {
   int64_t bgraph_cross = 0;  // cross-part arcs
   bool bg_csr_ready = false;
   DevBuf d_bitro, d_bitcol, d_botro, d_botcol, d_bitw;     // cross-arc CSRs (in with weights, out)
-  DevBuf d_bitems, d_bDt, d_bact, d_bpact, d_bgpart, d_grow;  // d_bitems: the two work lists
+  DevBuf d_bitems, d_bDt, d_bact, d_bpact, d_bgpart, d_bpcolmap, d_grow;  // d_bitems: the two work lists
   // Tiled form of stage 1's SSSP (launch_msbf): 0 automatic (graphs with at
   // least 6 arcs per vertex, where few Bellman-Ford iterations suffice), 1
   // frontier kernel, 2 tiled.  Work items over the in-edge CSR.
@@ -220,6 +221,8 @@ struct fap_dgraph {
   DevBuf cBd, cF, d_cparts, d_rowgroups, d_rowloc, d_rowout, d_rowidx;
   std::vector<int64_t> cb_off;
   std::vector<PartDesc> cparts;
+  cudaEvent_t cev[5] = {};                  // phases of the last cache build
+  float cache_ms[4] = {-1, -1, -1, -1};     // fap_graph_cache_timing
   int cache_ldf = 0, cache_max_b = 0, cache_max_s = 0;
   // last solve
   int last_mode = -1;
@@ -420,9 +423,11 @@ extern "C" int fap_graph_destroy(fap_dgraph *G) {
                       &G->d_tro, &G->d_tcol, &G->d_tw, &G->d_dB, &G->d_bpart, &G->d_brows, &G->d_FB,
                       &G->d_msbf_items, &G->d_msbf_act, &G->d_msbf_changed, &G->d_bitro, &G->d_bitcol,
                       &G->d_botro, &G->d_botcol, &G->d_bitw, &G->d_bitems, &G->d_bDt, &G->d_bact, &G->d_bpact,
-                      &G->d_bgpart, &G->d_grow})
+                      &G->d_bgpart, &G->d_bpcolmap, &G->d_grow})
       b->release();
     if (G->h_changed) cudaFreeHost(G->h_changed);
+    for (cudaEvent_t &ev : G->cev)
+      if (ev) cudaEventDestroy(ev);
     cache_drop(G);
   }
   delete G;
@@ -469,6 +474,8 @@ extern "C" int fap_graph_set_parts(fap_dgraph *G, int32_t K, const int32_t *grap
   G->boff.assign(K + 2, 0);
   for (int32_t p = 1; p <= K; p++) G->boff[p + 1] = G->boff[p] + bdy_num[p];
   G->total_b = G->boff[K + 1];
+  G->bpcol.assign(K + 2, 0);
+  for (int32_t p = 1; p <= K; p++) G->bpcol[p + 1] = G->bpcol[p] + (int32_t)round_up(bdy_num[p], 4);
   {
     // duplicate arcs inside a part?
     G->bnd_dupfree = true;
@@ -641,6 +648,7 @@ int build_bgraph_csr(fap_dgraph *G) {
   FAP_TRY(G->d_botro.ensure(otro.size() * 4));
   FAP_TRY(G->d_botcol.ensure(otcol.size() * 4));
   FAP_TRY(G->d_bgpart.ensure((size_t)nb * 4));
+  FAP_TRY(G->d_bpcolmap.ensure((size_t)nb * 4));
   FAP_TRY(G->d_bDt.ensure((size_t)z * nb * kMsbfS * 4));
   FAP_TRY(G->d_bact.ensure((size_t)3 * z * nb * 4));
   FAP_TRY(G->d_bpact.ensure((size_t)z * (G->K + 1) * 4));
@@ -653,6 +661,9 @@ int build_bgraph_csr(fap_dgraph *G) {
   FAP_CK(cudaMemcpy(G->d_botro.p, otro.data(), otro.size() * 4, cudaMemcpyHostToDevice));
   FAP_CK(cudaMemcpy(G->d_botcol.p, otcol.data(), otcol.size() * 4, cudaMemcpyHostToDevice));
   FAP_CK(cudaMemcpy(G->d_bgpart.p, gpart.data(), gpart.size() * 4, cudaMemcpyHostToDevice));
+  std::vector<int32_t> pcol((size_t)nb);
+  for (int64_t g = 0; g < nb; g++) pcol[g] = G->bpcol[gpart[g]] + (int32_t)(g - G->boff[gpart[g]]);
+  FAP_CK(cudaMemcpy(G->d_bpcolmap.p, pcol.data(), pcol.size() * 4, cudaMemcpyHostToDevice));
   G->bg_csr_ready = true;
   return FAP_OK;
 }
@@ -675,7 +686,9 @@ int prepare_bgraph(fap_dgraph *G, const std::vector<PartDesc> &parts) {
       rows.push_back(d.row_base + k);
     }
   }
-  G->ldB = round_up(std::max<int64_t>(G->total_b, 1), kFloydTile);
+  // (the Bellman-Ford closure writes dB's columns padded per part, so that
+  // the expansion's TMA boxes start on 16-byte boundaries)
+  G->ldB = round_up(std::max<int64_t>(bgraph_bf(G) ? G->bpcol[G->K + 1] : G->total_b, 1), kFloydTile);
   FAP_TRY(G->d_dB.ensure((size_t)G->ldB * G->ldB * 4));
   const int64_t ldFB = parts.empty() ? kFloydTile : parts[0].ldf;
   FAP_TRY(G->d_FB.ensure((size_t)std::max<int64_t>(G->total_b, 1) * ldFB * 4));
@@ -713,7 +726,8 @@ int close_bgraph(fap_dgraph *G, const PartDesc *dp, int np, int max_b, const T *
   int *wl = G->d_bitems.as<int>();
   FAP_CK(launch_bgraph_bf<T>(dp, np, max_b, F, G->d_bitro.as<const int32_t>(), G->d_bitcol.as<const int32_t>(),
                              G->d_bitw.as<const T>(), G->d_botro.as<const int32_t>(), G->d_botcol.as<const int32_t>(),
-                             G->d_bgpart.as<const int32_t>(), (int)G->total_b, G->K, z, dB,
+                             G->d_bgpart.as<const int32_t>(), G->d_bpcolmap.as<const int32_t>(), (int)G->total_b,
+                             G->K, z, dB,
                              G->ldB, G->d_bDt.as<T>(), G->d_bact.as<int>(), G->d_bpact.as<int>(), wl,
                              wl + (int64_t)2 * z * G->total_b, G->d_msbf_changed.as<int>(), G->h_changed,
                              max_rounds, status, st, L));
@@ -724,8 +738,14 @@ int close_bgraph(fap_dgraph *G, const PartDesc *dp, int np, int max_b, const T *
 // expansion for small boundary sets, the tiled one otherwise.  Also FB.
 template <typename T>
 int expand_bgraph(fap_dgraph *G, const PartDesc *dp, int np, int max_s, const T *F, T *Dout, int64_t ldFB,
-                  int64_t *L) {
+                  int *status, int64_t *L) {
   cudaStream_t st = G->ctx->stream;
+  if (bgraph_bf(G)) {  // padded dB columns: TMA-fed tiles (F: np squares of side ldFB)
+    FAP_CK(launch_bdy_expand_tma<T>(dp, np, max_s, (int)G->total_b, G->d_grow.as<const int64_t>(),
+                                    G->d_st2ed.as<const int32_t>(), G->d_dB.as<const T>(), G->ldB, F, ldFB, np,
+                                    Dout, G->ldD, G->d_FB.as<T>(), ldFB, status, st, L));
+    return FAP_OK;
+  }
   if (!bgraph_tiled_expand(G)) {
     FAP_CK(launch_bdy_expand<T>(G->d_brows.as<const int64_t>(), (int)G->total_b, G->d_bpart.as<const BPart>(),
                                 G->d_gid.as<const int32_t>(), G->d_ed2st.as<const int32_t>(), G->n,
@@ -790,6 +810,7 @@ int prepare_batch(fap_dgraph *G, const std::vector<int32_t> &ids, bool cached, b
     d.f_off = cached ? (int64_t)(p - 1) * ldf * ldf : foff;
     d.bd_row = cached ? (int32_t)G->cb_off[p] : bmethod ? G->boff[p] : 0;
     d.flags = bmethod ? kPartLocal : 0;
+    d.bd_col = G->bpcol[p];
     foff += (int64_t)d.ldf * d.ldf;
     G->max_b = std::max(G->max_b, d.b);
     G->max_s = std::max(G->max_s, d.s);
@@ -954,7 +975,7 @@ int run_solve(fap_dgraph *G, int mode) {
                                        status, st, &L));
     FAP_CK(record_event(c->ev[2], st));
     FAP_TRY(close_bgraph<T>(G, dp, np, G->max_b, F, status, max_rounds, &L));
-    FAP_TRY(expand_bgraph<T>(G, dp, np, G->max_s, F, D, G->max_ldf, &L));
+    FAP_TRY(expand_bgraph<T>(G, dp, np, G->max_s, F, D, G->max_ldf, status, &L));
     FAP_CK(launch_local_fixup<T>(dp, np, G->max_s, F, G->d_FB.as<const T>(), G->max_ldf, st, &L));
     FAP_CK(record_event(c->ev[3], st));
     FAP_CK(launch_minplus_thin<T>(dp, G->d_thin.as<int32_t>(), (int)G->thin.size(), G->max_s, G->n, F, D,
@@ -1695,7 +1716,7 @@ extern "C" int fap_graph_device_bytes(const fap_dgraph *G, int64_t *bytes) {
                           &G->d_rowidx, &G->P, &G->d_tro, &G->d_tcol, &G->d_tw, &G->d_dB,
                           &G->d_bpart, &G->d_brows, &G->d_FB, &G->d_msbf_items, &G->d_msbf_act,
                           &G->d_msbf_changed, &G->d_bitro, &G->d_bitcol, &G->d_botro, &G->d_botcol, &G->d_bitw, &G->d_bitems,
-                          &G->d_bDt, &G->d_bact, &G->d_bpact, &G->d_bgpart, &G->d_grow})
+                          &G->d_bDt, &G->d_bact, &G->d_bpact, &G->d_bgpart, &G->d_bpcolmap, &G->d_grow})
     t += (int64_t)b->bytes;
   *bytes = t;
   return FAP_OK;
@@ -1761,6 +1782,7 @@ int cache_build_impl(fap_dgraph *G) {
     d.f_off = (int64_t)(p - 1) * cs.ldf * cs.ldf;
     d.bd_row = (int32_t)G->cb_off[p];
     d.flags = bm ? kPartLocal : 0;
+    d.bd_col = G->bpcol[p];
     G->cparts.push_back(d);
     for (int32_t k = 0; k < d.b; k++) {
       src.push_back(d.start + k);
@@ -1789,24 +1811,34 @@ int cache_build_impl(fap_dgraph *G) {
                 *ed2st = G->d_ed2st.as<const int32_t>();
   const int64_t rounds = G->sssp_max_rounds > 0 ? G->sssp_max_rounds : 8 * (int64_t)G->n + 1024;
   int64_t L = 0;
+  for (cudaEvent_t &ev : G->cev)
+    if (!ev) FAP_CK(cudaEventCreate(&ev));
   FAP_CK(cudaMemsetAsync(status, 0, sizeof(int), st));
   if (bm) {
     // Boundary-graph form: local closures, boundary-graph APSP, expansion.
     FAP_TRY(prepare_bgraph(G, G->cparts));
+    FAP_CK(cudaEventRecord(G->cev[0], st));
     FAP_CK(launch_gather<T>(dp, K, cs.ldf, G->ro.as<const int32_t>(), G->col.as<const int32_t>(),
                             G->w.as<const T>(), gid, st2ed, ed2st, Bd, G->ldD, F, st, &L));
     FAP_CK(launch_floyd_parts_multi<T>(dp, K, (int)ceil_div(cs.max_s, kFloydTile), F, cs.ldf, status, st, &L));
+    FAP_CK(cudaEventRecord(G->cev[1], st));
     FAP_TRY(close_bgraph<T>(G, dp, K, cs.max_b, F, status, rounds, &L));
-    FAP_TRY(expand_bgraph<T>(G, dp, K, cs.max_s, F, Bd, cs.ldf, &L));
+    FAP_CK(cudaEventRecord(G->cev[2], st));
+    FAP_TRY(expand_bgraph<T>(G, dp, K, cs.max_s, F, Bd, cs.ldf, status, &L));
+    FAP_CK(cudaEventRecord(G->cev[3], st));
     FAP_CK(launch_local_fixup<T>(dp, K, cs.max_s, F, G->d_FB.as<const T>(), cs.ldf, st, &L));
+    FAP_CK(cudaEventRecord(G->cev[4], st));
     G->cache_bmethod = true;
     G->cache_stage1_name = stage1_form_name(G, true);
   } else {
   G->cache_stage1_name = stage1_form_name(G, false);
+  FAP_CK(cudaEventRecord(G->cev[0], st));
   FAP_TRY(run_stage1_sssp<T>(G, G->d_src.as<const int32_t>(), G->d_srcrows.as<const int64_t>(),
                              (int)src.size(), Bd, status, rounds, &L));
+  FAP_CK(cudaEventRecord(G->cev[1], st));
   FAP_CK(launch_gather<T>(dp, K, cs.ldf, G->ro.as<const int32_t>(), G->col.as<const int32_t>(),
                           G->w.as<const T>(), gid, st2ed, ed2st, Bd, G->ldD, F, st, &L));
+  FAP_CK(cudaEventRecord(G->cev[2], st));
   G->cache_bmethod = false;
   if (G->floyd_per_cta) {
     FAP_CK(launch_floyd_parts<T>(dp, K, F, cs.ldf, Bd, G->ldD, st2ed, status, st, &L));
@@ -1815,6 +1847,8 @@ int cache_build_impl(fap_dgraph *G) {
                                        st, &L));
     FAP_CK(launch_bdy_scatter<T>(dp, K, F, Bd, G->ldD, st2ed, cs.max_b, cs.max_s, st, &L));
   }
+  FAP_CK(cudaEventRecord(G->cev[3], st));
+  FAP_CK(cudaEventRecord(G->cev[4], st));
   }
   G->cache_ldf = cs.ldf;
   G->cache_max_b = cs.max_b;
@@ -1825,6 +1859,7 @@ int cache_build_impl(fap_dgraph *G) {
   // The SSSP scratch (up to one row of n per resident CTA) is not needed by
   // the cached path: wait for the build and give it back.
   FAP_CK(cudaStreamSynchronize(st));
+  for (int i = 0; i < 4; i++) FAP_CK(cudaEventElapsedTime(&G->cache_ms[i], G->cev[i], G->cev[i + 1]));
   G->sssp_scratch.release();
   return FAP_OK;
 }
@@ -1918,6 +1953,13 @@ extern "C" int fap_graph_cache_rebuild(fap_dgraph *G) {
   return rc;
 }
 
+extern "C" int fap_graph_cache_timing(const fap_dgraph *G, float *ms4) {
+  if (!G || !ms4) return fail(FAP_ERR_INVALID, "NULL argument");
+  if (!G->cache_ready) return fail(FAP_ERR_STATE, "no resident cache");
+  for (int i = 0; i < 4; i++) ms4[i] = G->cache_ms[i];
+  return FAP_OK;
+}
+
 extern "C" int fap_graph_cache_release(fap_dgraph *G) {
   if (!G) return fail(FAP_ERR_INVALID, "NULL graph");
   DeviceGuard g(G->ctx->device);
@@ -1934,14 +1976,15 @@ extern "C" int fap_graph_cache_bytes(const fap_dgraph *G, int64_t *bytes, int *b
     *bytes = (int64_t)(G->cBd.bytes + G->cF.bytes + G->d_cparts.bytes);
     if (G->cache_bmethod)  // the boundary graph's buffers stay for rebuilds
       for (const DevBuf *b : {&G->d_dB, &G->d_FB, &G->d_bitro, &G->d_bitcol, &G->d_botro, &G->d_botcol, &G->d_bitw, &G->d_bitems, &G->d_bDt,
-                              &G->d_bact, &G->d_bpact, &G->d_bgpart, &G->d_grow})
+                              &G->d_bact, &G->d_bpact, &G->d_bgpart, &G->d_bpcolmap, &G->d_grow})
         *bytes += (int64_t)b->bytes;
   } else {
     // plus what the build needs while it runs: the SSSP scratch, or the
     // boundary-graph matrix and tables
     const CacheShape cs = cache_shape(G);
     if (bmethod_ok(G)) {
-      const int64_t ldB = round_up(std::max<int64_t>(G->total_b, 1), kFloydTile);
+      const int64_t ldB =
+          round_up(std::max<int64_t>(bgraph_bf(G) ? G->bpcol[G->K + 1] : G->total_b, 1), kFloydTile);
       *bytes = cs.bytes(G) + (int64_t)alloc_size((size_t)(ldB * ldB * 4)) +
                (int64_t)alloc_size((size_t)std::max<int64_t>(G->total_b, 1) * cs.ldf * 4) +
                (int64_t)alloc_size((size_t)(G->K + 1) * sizeof(BPart)) +

@@ -299,12 +299,13 @@ __global__ void __launch_bounds__(256)
 }
 
 // out[out_rows[s0 + s]][v] = Dt[v][s] for s < ns (row s0 + s without a row
-// list), all init_cols columns (INF past n): 32 vertices per CTA, transposed
-// through shared memory, 128-byte row segments stored.
+// list), all init_cols columns (INF past n; column col_map[v] with a column
+// map, then init_cols <= n): 32 vertices per CTA, transposed through shared
+// memory, 128-byte row segments stored.
 template <typename T>
 __global__ void __launch_bounds__(256)
     msbf_store_kernel(const T *__restrict__ Dt, int n, int s0, int ns, T *out, int64_t ld,
-                      const int64_t *__restrict__ out_rows, int64_t init_cols) {
+                      const int64_t *__restrict__ out_rows, int64_t init_cols, const int32_t *__restrict__ col_map) {
   __shared__ T tile[32][kMsbfS + 1];
   const int64_t v0 = (int64_t)blockIdx.x * 32;
   const T inf = Dist<T>::inf();
@@ -318,7 +319,7 @@ __global__ void __launch_bounds__(256)
   for (int s = threadIdx.x >> 5; s < ns; s += blockDim.x >> 5) {
     const int64_t v = v0 + lane;
     const int64_t row = out_rows ? out_rows[s0 + s] : (int64_t)(s0 + s);
-    if (v < init_cols) out[row * ld + v] = tile[lane][s];
+    if (v < init_cols) out[row * ld + (col_map ? (int64_t)__ldg(col_map + v) : v)] = tile[lane][s];
   }
 }
 
@@ -364,7 +365,7 @@ cudaError_t launch_msbf(const MsbfItem *items, int nitems, const int32_t *tro, c
       for (int c = 0; c < kChunk; c++) done |= host_changed[c] == 0;
     }
     msbf_store_kernel<T><<<(unsigned)ceil_div(init_cols, 32), 256, 0, stream>>>(Dt, n, s0, ns, out, ld, out_rows,
-                                                                               init_cols);
+                                                                               init_cols, nullptr);
     *launches += 1;
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -1508,9 +1509,10 @@ __global__ void __launch_bounds__(256)
 template <typename T>
 cudaError_t launch_bgraph_bf(const PartDesc *parts, int nparts, int max_b, const T *F, const int32_t *itro,
                              const int32_t *itcol, const T *itw, const int32_t *otro, const int32_t *otcol,
-                             const int32_t *gpart, int nb, int K, int ztiles, T *dB, int64_t ldB, T *Dt, int *act,
-                             int *pact, int *wl, int *wl_count, int *changed, int *host_changed, int64_t max_rounds,
-                             int *status, cudaStream_t stream, int64_t *launches) {
+                             const int32_t *gpart, const int32_t *pcol, int nb, int K, int ztiles, T *dB,
+                             int64_t ldB, T *Dt, int *act, int *pact, int *wl, int *wl_count, int *changed,
+                             int *host_changed, int64_t max_rounds, int *status, cudaStream_t stream,
+                             int64_t *launches) {
   using C = LStepCfg<T>;
   if (nb <= 0 || nparts <= 0) return cudaSuccess;
   if (nparts > 65535 || ztiles < 1 || ztiles > 64) return cudaErrorInvalidConfiguration;
@@ -1560,13 +1562,92 @@ cudaError_t launch_bgraph_bf(const PartDesc *parts, int nparts, int max_b, const
       const int sq = s0 + q * kMsbfS;
       msbf_store_kernel<T><<<(unsigned)ceil_div(nb, 32), 256, 0, stream>>>(Dt + (int64_t)q * nb * kMsbfS, nb, sq,
                                                                           std::min(kMsbfS, nb - sq), dB, ldB,
-                                                                          nullptr, nb);
+                                                                          nullptr, nb, pcol);
     }
     *launches += z;
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
+}
+
+// Expansion with TMA-fed tiles: A = dB rows m0.. at part q's padded
+// boundary columns (bd_col.., a 16-byte start), B = q's local rows
+// F_q[0..b_q) over columns n0.. (the arena map), K = b_q; the stores go to
+// the columns' original ids (st2ed), own-part values also to FB.
+template <typename T>
+__global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS, 2)
+    bdy_expand_tma_kernel(const PartDesc *__restrict__ parts, int nbB, const int64_t *__restrict__ grow,
+                          const int32_t *__restrict__ st2ed, T *D, int64_t ldD, T *FB, int64_t ldFB,
+                          const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+                          int *status) {
+  using TC = typename FloydCfg<T, kFloydTile>::TC;
+  extern __shared__ __align__(128) unsigned char bxt_smem_raw[];
+  const PartDesc pd = parts[blockIdx.z];
+  const int n0 = blockIdx.y * TC::BN, m0 = blockIdx.x * TC::BM;
+  if (n0 >= pd.s) return;
+  auto sm = tma_smem_init<T, TC>(bxt_smem_raw);
+  T acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; i++)
+#pragma unroll
+    for (int j = 0; j < 8; j++) acc[i][j] = Dist<T>::inf();
+  const int fz = (int)(pd.f_off / ((int64_t)pd.ldf * pd.ldf));
+  if (!tma_minplus_tile<T, TC>(&mapA, pd.bd_col, m0, 0, &mapB, n0, 0, fz, pd.b, acc, sm)) {
+    if (threadIdx.x == 0) set_status(status, kDevTmaTimeout);
+    return;
+  }
+  const int tid = threadIdx.x, ty = tid / TC::TX, tx = tid % TC::TX;
+  int col[8];
+#pragma unroll
+  for (int g = 0; g < 2; g++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int j = n0 + g * (TC::BN / 2) + tx * 4 + q;
+      col[4 * g + q] = j < pd.s ? __ldg(st2ed + pd.start + j) : -1;
+    }
+#pragma unroll
+  for (int gi = 0; gi < 2; gi++)
+#pragma unroll
+    for (int l = 0; l < 4; l++) {
+      const int r = m0 + gi * (TC::BM / 2) + ty * 4 + l;
+      if (r >= nbB) continue;
+      T *dst = D + __ldg(grow + r) * ldD;
+      const bool own = r >= pd.bd_row && r < pd.bd_row + pd.b;
+      T *fb = FB + (int64_t)r * ldFB + n0;
+#pragma unroll
+      for (int g = 0; g < 2; g++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          const int c = col[4 * g + q];
+          if (c < 0) continue;
+          const T v = acc[4 * gi + l][4 * g + q];
+          __stcs(dst + c, v);
+          if (own) fb[g * (TC::BN / 2) + tx * 4 + q] = v;
+        }
+    }
+}
+
+template <typename T>
+cudaError_t launch_bdy_expand_tma(const PartDesc *parts, int nparts, int max_s, int nbB, const int64_t *grow,
+                                  const int32_t *st2ed, const T *dB, int64_t ldB, const T *F, int64_t ldf,
+                                  int nparts_f, T *D, int64_t ldD, T *FB, int64_t ldFB, int *status,
+                                  cudaStream_t stream, int64_t *launches) {
+  using TC = typename FloydCfg<T, kFloydTile>::TC;
+  if (nparts <= 0 || max_s <= 0 || nbB <= 0) return cudaSuccess;
+  if (nparts > 65535 || ceil_div(max_s, TC::BN) > 65535) return cudaErrorInvalidConfiguration;
+  CUtensorMap mapA, mapB, unused;
+  cudaError_t e = make_tmap_3d(&mapA, dB, Dist<T>::kDtype == FAP_DTYPE_F32, ldB, nbB, 1, TC::BK, TC::BM);
+  if (e == cudaSuccess) e = make_arena_tmaps<T>(F, ldf, nparts_f, &unused, &mapB);
+  if (e != cudaSuccess) return e;
+  const size_t smem = TC::SMEM_BYTES;
+  auto kern = bdy_expand_tma_kernel<T>;
+  e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  kern<<<dim3((unsigned)ceil_div(nbB, TC::BM), (unsigned)ceil_div(max_s, TC::BN), nparts), TC::THREADS, smem,
+         stream>>>(parts, nbB, grow, st2ed, D, ldD, FB, ldFB, mapA, mapB, status);
+  *launches += 1;
+  return cudaGetLastError();
 }
 
 // Expansion as one min-plus tile per CTA: rows m0.. of dB (boundary indices)
@@ -2081,9 +2162,13 @@ cudaError_t launch_relax_peak(T *sink, int blocks, int iters, cudaStream_t strea
                                              cudaStream_t, int64_t *);                             \
   template cudaError_t launch_bgraph_bf<T>(const PartDesc *, int, int, const T *, const int32_t *,  \
                                            const int32_t *, const T *, const int32_t *,              \
-                                           const int32_t *, const int32_t *, int, int, int, T *,     \
-                                           int64_t, T *, int *, int *, int *, int *, int *, int *,   \
-                                           int64_t, int *, cudaStream_t, int64_t *);                 \
+                                           const int32_t *, const int32_t *, const int32_t *, int,   \
+                                           int, int, T *, int64_t, T *, int *, int *, int *, int *,  \
+                                           int *, int *, int64_t, int *, cudaStream_t, int64_t *);   \
+  template cudaError_t launch_bdy_expand_tma<T>(const PartDesc *, int, int, int, const int64_t *,  \
+                                                const int32_t *, const T *, int64_t, const T *,    \
+                                                int64_t, int, T *, int64_t, T *, int64_t, int *,   \
+                                                cudaStream_t, int64_t *);                          \
   template cudaError_t launch_bdy_expand_tiled<T>(const PartDesc *, int, int, int, const int64_t *, \
                                                   const int32_t *, const T *, int64_t, const T *,  \
                                                   T *, int64_t, T *, int64_t, cudaStream_t,        \

@@ -19,7 +19,8 @@ struct PartDesc {
   int32_t bd_row;    // first row of the part's boundary rows in the resident cache /
                      // boundary index space (prefix sum of the boundary counts)
   int32_t flags;     // kPartLocal
-  int32_t pad_;
+  int32_t bd_col;    // first column of the part's boundary vertices in dB when its
+                     // columns are padded per part to 16-byte starts (Bellman-Ford closure)
 };
 
 // PartDesc::flags.  kPartLocal: the Floyd matrix is built from the part's
@@ -199,17 +200,28 @@ cudaError_t launch_bdy_expand(const int64_t *rows, int nrows, const BPart *bpart
 // F_p) and a cross step (the heads of cross-part arcs whose tails changed
 // pull over their cross-part in-arcs; CSRs over boundary indices: in-arcs
 // itro/itcol/itw, out-arcs otro/otcol); gpart: part id of every boundary
-// index; Dt ztiles x nb x kMsbfS; act 3 x ztiles x nb ints; pact ztiles x
-// (K + 1) ints; wl 2 x ztiles x nb ints
-// (two work lists); wl_count 3 ints; changed 4 ints; host_changed 4 pinned
-// ints (convergence is tested on the host every 4 iterations).  Writes rows
-// 0..nb-1 of dB (columns < nb).
+// index; pcol: its dB column; Dt ztiles x nb x kMsbfS; act 3 x ztiles x nb
+// ints; pact ztiles x (K + 1) ints; wl 2 x ztiles x nb ints (two work
+// lists); wl_count 3 ints; changed 4 ints; host_changed 4 pinned ints
+// (convergence is tested on the host every 4 iterations).  Writes rows
+// 0..nb-1 of dB at columns pcol[0..nb).
 template <typename T>
 cudaError_t launch_bgraph_bf(const PartDesc *parts, int nparts, int max_b, const T *F, const int32_t *itro,
                              const int32_t *itcol, const T *itw, const int32_t *otro, const int32_t *otcol,
-                             const int32_t *gpart, int nb, int K, int ztiles, T *dB, int64_t ldB, T *Dt, int *act,
-                             int *pact, int *wl, int *wl_count, int *changed, int *host_changed, int64_t max_rounds,
-                             int *status, cudaStream_t stream, int64_t *launches);
+                             const int32_t *gpart, const int32_t *pcol, int nb, int K, int ztiles, T *dB,
+                             int64_t ldB, T *Dt, int *act, int *pact, int *wl, int *wl_count, int *changed,
+                             int *host_changed, int64_t max_rounds, int *status, cudaStream_t stream,
+                             int64_t *launches);
+// Expansion with TMA-fed tiles (dB closed by Bellman-Ford, its columns
+// padded per part: part q's boundary columns start at bd_col, a multiple of
+// 4): grid (boundary-index tiles, column tiles, parts); A boxes from dB,
+// B boxes from the F arena (nparts_f squares of side ldf).  A stage that
+// never completes sets kDevTmaTimeout in status.
+template <typename T>
+cudaError_t launch_bdy_expand_tma(const PartDesc *parts, int nparts, int max_s, int nbB, const int64_t *grow,
+                                  const int32_t *st2ed, const T *dB, int64_t ldB, const T *F, int64_t ldf,
+                                  int nparts_f, T *D, int64_t ldD, T *FB, int64_t ldFB, int *status,
+                                  cudaStream_t stream, int64_t *launches);
 // Tiled expansion (any boundary count): grid (boundary-index tiles, column
 // tiles, parts); a CTA is a min-plus tile dB[g][b'_q] (x) F_q[b'][j] written
 // to D[grow[g]][st2ed[start_q + j]] (and FB[g][j] for g of part q).

@@ -449,6 +449,12 @@ class DeviceGraph:
         else:
             check(lib().fap_graph_cache_build(self._h), "fap_graph_cache_build")
 
+    def cache_timing(self) -> list:
+        """Device ms of the last cache build's four phases (fap_graph_cache_timing)."""
+        out = np.zeros(4, np.float32)
+        check(lib().fap_graph_cache_timing(self._h, ptr(out)), "fap_graph_cache_timing")
+        return [float(x) for x in out]
+
     def cache_release(self) -> None:
         check(lib().fap_graph_cache_release(self._h), "fap_graph_cache_release")
 

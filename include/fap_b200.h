@@ -228,6 +228,11 @@ FAP_API int fap_graph_cache_build(fap_dgraph *g);
  * stages 1-2 of every part, e.g. once per pass of a job whose output is
  * produced in groups of parts. */
 FAP_API int fap_graph_cache_rebuild(fap_dgraph *g);
+/* Device time of the last cache build's phases, ms4[4]: built with the
+ * boundary graph, [local closures (gather + Floyd), boundary-graph closure,
+ * expansion into the boundary rows, fix-up of the closures]; built with
+ * SSSP, [SSSP, gather, Floyd, 0].  FAP_ERR_STATE without a cache. */
+FAP_API int fap_graph_cache_timing(const fap_dgraph *g, float *ms4);
 FAP_API int fap_graph_cache_release(fap_dgraph *g);
 /* Device bytes the cache holds (*built = 1) or would need to be built,
  * including its SSSP scratch (*built = 0). */
