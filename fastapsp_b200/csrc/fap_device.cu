@@ -387,7 +387,7 @@ __global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS, 2)
   const PartDesc pd = parts[blockIdx.x];
   T *mat = F + pd.f_off;
   const int nb = (int)ceil_div(pd.s, kFloydTile);
-  if (!floyd_close_cta<T, kFloydTile>(&mapA, &mapB, blockIdx.x, mat, pd.ldf, nb, sm)) {
+  if (!floyd_close_cta<T, kFloydTile>(&mapA, &mapB, blockIdx.x, mat, pd.ldf, nb, pd.s, sm)) {
     if (threadIdx.x == 0) set_status(status, kDevTmaTimeout);
     return;
   }
@@ -508,7 +508,8 @@ __global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS, 2)
   const PartDesc pd = parts[blockIdx.x];
   if (kb >= (int)ceil_div(pd.s, kFloydTile)) return;
   auto sm = tma_smem_init<T, TC>(fm_smem_raw);
-  floyd_diag_close<T, kFloydTile>(F + pd.f_off, pd.ldf, kb * kFloydTile, sm.ring);
+  floyd_diag_close<T, kFloydTile>(F + pd.f_off, pd.ldf, kb * kFloydTile, sm.ring,
+                                  min(kFloydTile, pd.s - kb * kFloydTile));
 }
 
 template <typename T>
@@ -527,11 +528,13 @@ __global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS, 2)
   bool ok;
   if (t < nb - 1) {
     const int j = t < kb ? t : t + 1;
-    ok = floyd_tile_update<T, kFloydTile>(&mapA, &mapB, blockIdx.y, mat, pd.ldf, kb, j, kb, sm);
+    ok = floyd_tile_update<T, kFloydTile>(&mapA, &mapB, blockIdx.y, mat, pd.ldf, kb, j, kb, sm,
+                                          min(kFloydTile, pd.s - kb * kFloydTile));
   } else {
     t -= nb - 1;
     const int i = t < kb ? t : t + 1;
-    ok = floyd_tile_update<T, kFloydTile>(&mapA, &mapB, blockIdx.y, mat, pd.ldf, i, kb, kb, sm);
+    ok = floyd_tile_update<T, kFloydTile>(&mapA, &mapB, blockIdx.y, mat, pd.ldf, i, kb, kb, sm,
+                                          min(kFloydTile, pd.s - kb * kFloydTile));
   }
   if (!ok && threadIdx.x == 0) set_status(status, kDevTmaTimeout);
 }
@@ -551,7 +554,8 @@ __global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS, 2)
   int i = t / (nb - 1), j = t % (nb - 1);
   i = i < kb ? i : i + 1;
   j = j < kb ? j : j + 1;
-  if (!floyd_tile_update<T, kFloydTile>(&mapA, &mapB, blockIdx.y, F + pd.f_off, pd.ldf, i, j, kb, sm) &&
+  if (!floyd_tile_update<T, kFloydTile>(&mapA, &mapB, blockIdx.y, F + pd.f_off, pd.ldf, i, j, kb, sm,
+                                        min(kFloydTile, pd.s - kb * kFloydTile)) &&
       threadIdx.x == 0)
     set_status(status, kDevTmaTimeout);
 }

@@ -43,14 +43,15 @@ struct FloydCfg {
 };
 
 // Phase 1 on the tile at (r0, r0) of a padded matrix.  Block-wide; `buf`
-// holds 4*TILE elements of shared memory.
+// holds 4*TILE elements of shared memory.  Pivots past kvalid (padding, the
+// sentinel) change nothing and are skipped.
 template <typename T, int TILE>
-__device__ __forceinline__ void floyd_diag_close(T *mat, int64_t ld, int r0, T *buf) {
+__device__ __forceinline__ void floyd_diag_close(T *mat, int64_t ld, int r0, T *buf, int kvalid = TILE) {
   using C = typename FloydCfg<T, TILE>::C;
   const int tid = threadIdx.x, ty = tid / C::TX, tx = tid % C::TX;
   T acc[C::TM][C::TN];
   acc_load<T, C, true>(acc, mat, ld, r0, r0, 0, 0);
-  for (int k = 0; k < TILE; k++) {
+  for (int k = 0; k < kvalid; k++) {
     T *rowbuf0 = buf + (k & 1) * TILE;
     T *colbuf0 = buf + 2 * TILE + (k & 1) * TILE;
     // publish the current pivot row k and pivot column k (all register
@@ -104,39 +105,43 @@ __device__ __forceinline__ void floyd_diag_close(T *mat, int64_t ld, int r0, T *
 
 // Phase 2/3 on one tile of part z: D[ti][tj] = min(D[ti][tj], D[ti][tk] (x)
 // D[tk][tj]).  mat is the part's matrix (ld = arena leading dimension);
-// mapA/mapB describe the arena with TILE x 16 and 16 x TILE boxes.
+// mapA/mapB describe the arena with TILE x 16 and 16 x TILE boxes; only the
+// first kvalid pivots of block tk are real (the rest is padding).
 // Block-wide; false if a TMA stage never completed.
 template <typename T, int TILE>
 __device__ __forceinline__ bool floyd_tile_update(const CUtensorMap *mapA, const CUtensorMap *mapB,
                                                   int z, T *mat, int64_t ld, int ti, int tj, int tk,
-                                                  TmaSmem<T, typename FloydCfg<T, TILE>::TC> &sm) {
+                                                  TmaSmem<T, typename FloydCfg<T, TILE>::TC> &sm,
+                                                  int kvalid = TILE) {
   using C = typename FloydCfg<T, TILE>::C;
   using TC = typename FloydCfg<T, TILE>::TC;
   T acc[C::TM][C::TN];
   const int64_t r0 = (int64_t)ti * TILE, c0 = (int64_t)tj * TILE;
   acc_load<T, C, true>(acc, mat + r0 * ld + c0, ld, 0, 0, 0, 0);
   const bool ok = tma_minplus_tile<T, TC>(mapA, tk * TILE, ti * TILE, z, mapB, tj * TILE, tk * TILE,
-                                          z, TILE, acc, sm);
+                                          z, kvalid, acc, sm);
   if (ok) acc_store<T, C, true>(acc, mat + r0 * ld + c0, ld, 0, 0, 0, 0);
   return ok;
 }
 
-// Closes one padded matrix (nb x nb tiles) of part z with the calling CTA.
+// Closes one padded matrix (nb x nb tiles, s real rows) of part z with the
+// calling CTA.
 template <typename T, int TILE>
 __device__ bool floyd_close_cta(const CUtensorMap *mapA, const CUtensorMap *mapB, int z, T *mat,
-                                int64_t ld, int nb, TmaSmem<T, typename FloydCfg<T, TILE>::TC> &sm) {
+                                int64_t ld, int nb, int s, TmaSmem<T, typename FloydCfg<T, TILE>::TC> &sm) {
   bool ok = true;
   for (int kb = 0; kb < nb && ok; kb++) {
-    floyd_diag_close<T, TILE>(mat, ld, kb * TILE, sm.ring);
+    const int kv = min(TILE, s - kb * TILE);
+    floyd_diag_close<T, TILE>(mat, ld, kb * TILE, sm.ring, kv);
     for (int j = 0; j < nb && ok; j++)
-      if (j != kb) ok = floyd_tile_update<T, TILE>(mapA, mapB, z, mat, ld, kb, j, kb, sm);
+      if (j != kb) ok = floyd_tile_update<T, TILE>(mapA, mapB, z, mat, ld, kb, j, kb, sm, kv);
     for (int i = 0; i < nb && ok; i++)
-      if (i != kb) ok = floyd_tile_update<T, TILE>(mapA, mapB, z, mat, ld, i, kb, kb, sm);
+      if (i != kb) ok = floyd_tile_update<T, TILE>(mapA, mapB, z, mat, ld, i, kb, kb, sm, kv);
     __syncthreads();
     for (int i = 0; i < nb && ok; i++) {
       if (i == kb) continue;
       for (int j = 0; j < nb && ok; j++)
-        if (j != kb) ok = floyd_tile_update<T, TILE>(mapA, mapB, z, mat, ld, i, j, kb, sm);
+        if (j != kb) ok = floyd_tile_update<T, TILE>(mapA, mapB, z, mat, ld, i, j, kb, sm, kv);
     }
     __syncthreads();
   }
