@@ -1300,7 +1300,9 @@ cudaError_t launch_bdy_expand(const int64_t *rows, int nrows, const BPart *bpart
 //   arcs' heads on the next list and stamp their parts for the next local
 //   step.
 // Stamps are iteration numbers (per boundary vertex: cact, the list its
-// out-arcs' heads last went to; hact, the list it last joined as a head;
+// out-arcs' heads last went to from a local step or the seed (several
+// threads of a local step may change one row); hact, the list it last
+// joined as a head;
 // lact, the iteration whose local step takes it as a changed row; per part:
 // pact, the local step to run), so nothing is cleared between iterations or
 // tiles.  The work list of iteration t (entries z * nb + g) is filled by the
@@ -1462,50 +1464,75 @@ __global__ void __launch_bounds__(256)
                         const int32_t *__restrict__ gpart, int *pact, int *wl, int *wl_count, int *changed) {
   using V = typename Vec4<T>::type;
   const T inf = Dist<T>::inf();
-  const int lane = threadIdx.x & 31;
+  // one head per half-warp (two heads in flight per warp), 8 sources a lane
+  const int lane = threadIdx.x & 31, half = lane >> 4, hl = lane & 15;
   const int nwarps = gridDim.x * (blockDim.x >> 5);
   const int count = __ldcg(wl_count + (stamp & 1));
   const int *list = wl + (stamp & 1) * (int64_t)wl_count[2];
-  for (int it = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < count; it += nwarps) {
-    const int entry = __ldcg(list + it);
+  const int t1 = stamp + 1;
+  for (int base = 2 * (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)); base < count; base += 2 * nwarps) {
+    const int it = base + half;
+    const bool live = it < count;
+    const int entry = live ? __ldcg(list + it) : 0;
     const int64_t z = entry / nb;
     const int v = entry - (int)(z * nb);
     T *Dz = Dt + z * nb * kMsbfS;
-    T acc[4] = {inf, inf, inf, inf};
-    const int e0 = __ldg(itro + v), e1 = __ldg(itro + v + 1);
+    T acc[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) acc[q] = inf;
+    const int e0 = live ? __ldg(itro + v) : 0, e1 = live ? __ldg(itro + v + 1) : 0;
     for (int e = e0; e < e1; e += 4) {  // four tail rows in flight
-      V d[4];
+      V d[4][2];
       T w[4];
 #pragma unroll
       for (int q = 0; q < 4; q++)
         if (e + q < e1) {
-          d[q] = __ldcg(reinterpret_cast<const V *>(Dz + (int64_t)__ldg(itcol + e + q) * kMsbfS) + lane);
+          const V *r = reinterpret_cast<const V *>(Dz + (int64_t)__ldg(itcol + e + q) * kMsbfS) + 2 * hl;
+          d[q][0] = __ldcg(r);
+          d[q][1] = __ldcg(r + 1);
           w[q] = __ldg(itw + e + q);
         }
 #pragma unroll
       for (int q = 0; q < 4; q++)
-        if (e + q < e1) {
-          acc[0] = Dist<T>::relax(d[q].x, w[q], acc[0]);
-          acc[1] = Dist<T>::relax(d[q].y, w[q], acc[1]);
-          acc[2] = Dist<T>::relax(d[q].z, w[q], acc[2]);
-          acc[3] = Dist<T>::relax(d[q].w, w[q], acc[3]);
+        if (e + q < e1)
+#pragma unroll
+          for (int h = 0; h < 2; h++) {
+            acc[4 * h + 0] = Dist<T>::relax(d[q][h].x, w[q], acc[4 * h + 0]);
+            acc[4 * h + 1] = Dist<T>::relax(d[q][h].y, w[q], acc[4 * h + 1]);
+            acc[4 * h + 2] = Dist<T>::relax(d[q][h].z, w[q], acc[4 * h + 2]);
+            acc[4 * h + 3] = Dist<T>::relax(d[q][h].w, w[q], acc[4 * h + 3]);
+          }
+    }
+    bool imp = false;
+    if (live) {  // this half-warp is the row's only writer in this step
+      V *row = reinterpret_cast<V *>(Dz + (int64_t)v * kMsbfS) + 2 * hl;
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        V cur = __ldcg(row + h);
+        if (acc[4 * h] < cur.x || acc[4 * h + 1] < cur.y || acc[4 * h + 2] < cur.z || acc[4 * h + 3] < cur.w) {
+          imp = true;
+          cur.x = min(cur.x, acc[4 * h]);
+          cur.y = min(cur.y, acc[4 * h + 1]);
+          cur.z = min(cur.z, acc[4 * h + 2]);
+          cur.w = min(cur.w, acc[4 * h + 3]);
+          __stcg(row + h, cur);
         }
+      }
     }
-    V *row = reinterpret_cast<V *>(Dz + (int64_t)v * kMsbfS) + lane;
-    V cur = __ldcg(row);
-    const bool imp = acc[0] < cur.x || acc[1] < cur.y || acc[2] < cur.z || acc[3] < cur.w;
-    if (imp) {  // this warp is the row's only writer in this step
-      cur.x = min(cur.x, acc[0]);
-      cur.y = min(cur.y, acc[1]);
-      cur.z = min(cur.z, acc[2]);
-      cur.w = min(cur.w, acc[3]);
-      __stcg(row, cur);
-    }
-    if (__any_sync(0xffffffffu, imp) && lane == 0) {
-      bgraph_mark_heads(v, z * nb, cact + z * nb, hact + z * nb, stamp + 1, otro, otcol, wl, wl_count);
-      lact[z * nb + v] = stamp + 1;
-      pact[z * K1 + __ldg(gpart + v)] = stamp + 1;
-      *changed = 1;
+    const unsigned bal = __ballot_sync(0xffffffffu, imp);
+    if ((bal >> (16 * half)) & 0xffffu) {
+      // the heads of v's out-arcs join the next list, one lane per arc
+      const int f1 = __ldg(otro + v + 1);
+      for (int e = __ldg(otro + v) + hl; e < f1; e += 16) {
+        const int h = __ldg(otcol + e);
+        if (atomicExch(hact + z * nb + h, t1) != t1)
+          wl[(t1 & 1) * (int64_t)wl_count[2] + atomicAdd(wl_count + (t1 & 1), 1)] = (int)(z * nb + h);
+      }
+      if (hl == 0) {
+        lact[z * nb + v] = t1;
+        pact[z * K1 + __ldg(gpart + v)] = t1;
+        *changed = 1;
+      }
     }
   }
 }
