@@ -62,6 +62,8 @@ def parse_args():
                     help="boundary-graph closure: 0 by size, 1 Floyd, 2 Bellman-Ford + tiled expansion")
     ap.add_argument("--no-stage-cache", action="store_true",
                     help="grouped jobs: run stages 1-2 per group instead of once for all parts")
+    ap.add_argument("--cache-only", action="store_true",
+                    help="time only stages 1-2 of every part (the resident cache build), no output matrix")
     ap.add_argument("--paths", action="store_true",
                     help="also time batched solves that produce predecessor matrices")
     ap.add_argument("--serve-graphs", type=int, default=32)
@@ -388,6 +390,34 @@ def run_serving(args, device):
     return out
 
 
+def run_cache_only(args, dg, stream, world):
+    """Stages 1-2 of every part into the resident cache (boundary rows and
+    closed Floyd matrices), without the output matrix: the profiling mode of
+    stage 1 (a few GB on the device for the grid256 stand-in)."""
+    import torch
+    dg.cache_build()
+    dg.check()
+    for _ in range(args.warmup):
+        dg.cache_build(rebuild=True)
+    torch.cuda.synchronize()
+    ms, phases = [], []
+    for _ in range(args.steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        dg.cache_build(rebuild=True)
+        e1.record(stream)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+        phases.append(dg.cache_timing())
+    dg.check()
+    ph = np.round(np.mean(phases, 0), 3).tolist()
+    log(f"cache build: {np.mean(ms):.3f} ms ({dg.stage1_name() or 'cache'}), phases {ph}")
+    if int(os.environ.get("RANK", "0")) == 0:
+        print(json.dumps({"mode": "cache_only", "ms_per_step": float(np.mean(ms)), "steps": args.steps,
+                          "phases_ms": ph, "world": world}))
+
+
 def main_fap(args):
     import torch
     import torch.distributed as dist
@@ -437,6 +467,11 @@ def main_fap(args):
     dg.set_param("stage1", args.stage1)
     dg.set_param("sssp_form", args.sssp_form)
     dg.set_param("bgraph_form", args.bgraph_form)
+    if args.cache_only:
+        run_cache_only(args, dg, stream, world)
+        if world > 1:
+            dist.destroy_process_group()
+        return
     free_b = torch.cuda.mem_get_info()[0]
     budget_rows = int(0.60 * free_b / (4 * ldD))
     # A job larger than the device is produced in groups of parts.  On one
