@@ -33,6 +33,10 @@ import sys
 import tempfile
 import time
 
+# Load every kernel when the context is created, so that no timed region
+# pays a kernel's first-launch module load.
+os.environ.setdefault("CUDA_MODULE_LOADING", "EAGER")
+
 import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -322,22 +326,32 @@ def run_serving(args, device):
             for i, n, *_ in info])
     warm = srv.stats()
     log(f"serving warm-up: {warm.cache_builds} caches built, {warm.busy_ms:.1f} ms device time")
-    srv.reset_stats()
-    # capacity: closed loop, a window of 64 requests in flight
-    reqs = [draw() for _ in range(args.serve_burst)]
     window = 64
-    t0 = time.perf_counter()
-    hs, pending = [], []
-    for r in reqs:
-        if len(pending) >= window:
-            pending.pop(0).wait()
-        h = submit(r)
-        hs.append(h)
-        pending.append(h)
-    by_kind = finish(hs, [r[0] for r in reqs])
-    burst_s = time.perf_counter() - t0
-    st = srv.stats()
-    cap_rps = len(reqs) / burst_s
+
+    def closed_loop(reqs):
+        t0 = time.perf_counter()
+        hs, pending = [], []
+        for r in reqs:
+            if len(pending) >= window:
+                pending.pop(0).wait()
+            h = submit(r)
+            hs.append(h)
+            pending.append(h)
+        by_kind = finish(hs, [r[0] for r in reqs])
+        return by_kind, time.perf_counter() - t0
+
+    # warm-up of the mixed stream itself (every kernel shape it uses, batch
+    # buffers at their working sizes), untimed
+    closed_loop([draw() for _ in range(max(64, args.serve_burst // 4))])
+    # capacity: closed loop, a window of 64 requests in flight, measured twice;
+    # the lower figure sets the offered loads, so that "90%" is not an overload
+    caps = []
+    for _ in range(2):
+        srv.reset_stats()
+        reqs = [draw() for _ in range(args.serve_burst)]
+        by_kind, burst_s = closed_loop(reqs)
+        caps.append((len(reqs) / burst_s, burst_s, by_kind, srv.stats()))
+    cap_rps, burst_s, by_kind, st = min(caps, key=lambda c: c[0])
     out = {"graphs": len(gs),
            "n": [min(g.n for g in gs), max(g.n for g in gs)],
            "K": sorted({g.K for g in gs}),
@@ -345,14 +359,15 @@ def run_serving(args, device):
            "mix": "80% solveSubGraph (uniform graph, uniform part), 20% distance rows "
                   "(100-10,000 sources, log-uniform); per-row checksums returned",
            "budget_bytes": int(0.6 * free_b),
-           "capacity": {"requests_s": cap_rps, "entries_s": st.entries / burst_s,
+           "capacity": {"requests_s": cap_rps, "runs_requests_s": [c[0] for c in caps],
+                        "entries_s": st.entries / burst_s,
                         "requests": len(reqs), "window": window, "batches": st.batches,
                         "resident_hits": st.resident_hits, "p50_ms": st.p50_ms, "p99_ms": st.p99_ms,
                         "by_kind": by_kind, "device_busy_frac": st.busy_ms * 1e-3 / burst_s},
            "warmup_cache_builds": warm.cache_builds,
            "loads": []}
-    log(f"serving capacity {cap_rps:.1f} req/s, {st.entries / burst_s:.4g} entries/s "
-        f"(closed loop, {window} in flight)")
+    log(f"serving capacity {cap_rps:.1f} req/s (runs {[round(c[0], 1) for c in caps]}), "
+        f"{st.entries / burst_s:.4g} entries/s (closed loop, {window} in flight)")
     for frac in (0.25, 0.5, 0.9):
         rate = frac * cap_rps
         count = int(min(max(32, rate * args.serve_seconds), 2 * args.serve_burst))

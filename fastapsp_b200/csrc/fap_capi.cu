@@ -88,6 +88,25 @@ struct DevBuf {
     bytes = want;
     return FAP_OK;
   }
+  // Stream-ordered growth for buffers used on one stream only: the old
+  // buffer is freed after the stream's earlier work, and nothing waits for
+  // the rest of the device (cudaFree would).  release() works on either kind.
+  int ensure_async(size_t want, cudaStream_t st) {
+    if (want <= bytes) return FAP_OK;
+    want = alloc_size(want);
+    if (p) cudaFreeAsync(p, st);
+    p = nullptr;
+    bytes = 0;
+    if (want == 0) return FAP_OK;
+    cudaError_t e = cudaMallocAsync(&p, want, st);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      p = nullptr;
+      return fail(FAP_ERR_NOMEM, "cudaMallocAsync(%zu bytes): %s", want, cudaGetErrorString(e));
+    }
+    bytes = want;
+    return FAP_OK;
+  }
   void release() {
     if (p) cudaFree(p);
     p = nullptr;
@@ -1902,10 +1921,12 @@ int rows_cached_impl(fap_dgraph *G, const int32_t *sources, int32_t count, float
     gidx[k] = gather[2 * k];
     gout[k] = gather[2 * k + 1];
   }
-  FAP_TRY(G->d_rowgroups.ensure(std::max<size_t>(groups.size(), 1) * sizeof(RowGroup)));
-  FAP_TRY(G->d_rowloc.ensure(std::max<size_t>(loc.size(), 1) * 4));
-  FAP_TRY(G->d_rowout.ensure(std::max<size_t>(orow.size(), 1) * 8));
-  FAP_TRY(G->d_rowidx.ensure(std::max<size_t>(2 * ng, 1) * 8));
+  // (grown in stream order: cudaFree would wait for the whole device, other
+  // graphs' streams of a server included)
+  FAP_TRY(G->d_rowgroups.ensure_async(std::max<size_t>(groups.size(), 1) * sizeof(RowGroup), st));
+  FAP_TRY(G->d_rowloc.ensure_async(std::max<size_t>(loc.size(), 1) * 4, st));
+  FAP_TRY(G->d_rowout.ensure_async(std::max<size_t>(orow.size(), 1) * 8, st));
+  FAP_TRY(G->d_rowidx.ensure_async(std::max<size_t>(2 * ng, 1) * 8, st));
   FAP_CK(cudaStreamSynchronize(st));  // earlier launches may still read these buffers
   if (!groups.empty()) {
     FAP_CK(cudaMemcpy(G->d_rowgroups.p, groups.data(), groups.size() * sizeof(RowGroup), cudaMemcpyHostToDevice));

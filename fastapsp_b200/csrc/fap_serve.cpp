@@ -368,7 +368,8 @@ bool fap_server::launch(int gi) {
     int64_t need = std::max<int64_t>(0, target - g.cs_cap) * 8 + sg * (int64_t)g.n * 4;
     if (kind == FAP_REQ_ROWS) {
       const int64_t b = r * (int64_t)g.n * 4;
-      need += b > kSmallRowsBytes ? b : std::max<int64_t>(0, b - g.rows_small_cap * 4);
+      // (the small buffer grows to kSmallRowsBytes at once unless the batch is sized exactly)
+      need += b > kSmallRowsBytes ? b : std::max<int64_t>(0, (exact ? b : kSmallRowsBytes) - g.rows_small_cap * 4);
       if (!cached) need += r * (int64_t)g.n * 4;
     } else {
       need += std::max<int64_t>(0, target - g.reserved_rows) * g.ldD * 4;
@@ -456,7 +457,8 @@ bool fap_server::launch(int gi) {
         g.rows_out = nullptr;
         rc = FAP_ERR_NOMEM;
       }
-    } else if (grow_dev(&g.rows_small, &g.rows_small_cap, rows * (int64_t)g.n)) {
+    } else if (grow_dev(&g.rows_small, &g.rows_small_cap,
+                        exact ? rows * (int64_t)g.n : kSmallRowsBytes / 4)) {  // once per graph
       g.rows_out = g.rows_small;
     } else {
       rc = FAP_ERR_NOMEM;
