@@ -259,6 +259,8 @@ WORKLOADS = {
     # over 8192 boundary vertices (the Bellman-Ford closure of the boundary graph)
     "grid256": dict(make=lambda: grid_graph(256, 256, extra_frac=0.01, wmin=1, wmax=100,
                                             seed=5), K=64),
+    # profiling-size stand-in for rmat16: same average degree and part size
+    "rmat14": dict(make=lambda: rmat_graph(14, 1 << 18, seed=6), K=16),
     # R-MAT scale 16, 2^20 directed edges, float weights, K=64
     "rmat16": dict(make=lambda: rmat_graph(16, 1 << 20, seed=4), K=64),
 }
