@@ -223,7 +223,10 @@ __global__ void msbf_seed_kernel(T *Dt, const int32_t *__restrict__ sources, con
 }
 
 // One warp lowers row v of the tile from up to 32 in-edges e0..e1 whose
-// tails pass `active` (warp-uniform loop, four tail rows in flight); the
+// tails pass `active` (warp-uniform loop, four tail rows in flight, read
+// through L1: a tail row that another SM lowers during this iteration may be
+// seen stale here, which is harmless, because that lowering marks the tail
+// as changed and its out-neighbours pull from it again next iteration); the
 // row's lanes each hold 4 sources.  Returns (warp-uniform) whether any entry
 // improved.  Atomic minima: other warps may lower the same row meanwhile.
 template <typename T, class Active>
@@ -260,7 +263,7 @@ __device__ __forceinline__ bool msbf_pull_row(T *Dt, int v, int e0, int e1, cons
     V d[4];
 #pragma unroll
     for (int q = 0; q < 4; q++)
-      if (uu[q] >= 0) d[q] = __ldcg(reinterpret_cast<const V *>(Dt + (int64_t)uu[q] * kMsbfS) + lane);
+      if (uu[q] >= 0) d[q] = __ldca(reinterpret_cast<const V *>(Dt + (int64_t)uu[q] * kMsbfS) + lane);
 #pragma unroll
     for (int q = 0; q < 4; q++)
       if (uu[q] >= 0) {
@@ -287,7 +290,7 @@ __global__ void __launch_bounds__(256)
                      uint32_t *act_next, int *changed) {
   const int lane = threadIdx.x & 31;
   const int nwarps = gridDim.x * (blockDim.x >> 5);
-  auto active = [act_cur](int u) { return ((__ldcg(act_cur + (u >> 5)) >> (u & 31)) & 1u) != 0; };
+  auto active = [act_cur](int u) { return ((__ldg(act_cur + (u >> 5)) >> (u & 31)) & 1u) != 0; };
   for (int it = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < nitems; it += nwarps) {
     const MsbfItem m = items[it];
     const int e1 = min(m.e0 + 32, __ldg(tro + m.v + 1));
