@@ -856,7 +856,7 @@ int prepare_batch(fap_dgraph *G, const std::vector<int32_t> &ids, bool cached, b
   FAP_TRY(G->d_thin.ensure(std::max<size_t>(G->thin.size(), 1) * 4));
   FAP_TRY(G->d_src.ensure(std::max<size_t>(G->src.size(), 1) * 4));
   FAP_TRY(G->d_srcrows.ensure(std::max<size_t>(G->srcrows.size(), 1) * 8));
-  if (!cached && !bmethod)
+  if (!cached && !bmethod)  // (the plain form runs the frontier SSSP per part whatever the form)
     FAP_TRY(G->sssp_scratch.ensure(
         (size_t)std::max(sssp_scratch_rows(G->n, (int)G->src.size()), 1) * (size_t)G->n * 4));
   cudaStream_t st = G->ctx->stream;
@@ -915,8 +915,16 @@ const char *stage1_form_name(const fap_dgraph *G, bool bmethod) {
   return use_msbf(G) ? "SSSP, tiled Bellman-Ford" : "SSSP, frontier";
 }
 
-// Work items, bitmaps and the pinned convergence flags of the tiled form.
-int prepare_msbf(fap_dgraph *G) {
+// Tiles of the tiled SSSP form run side by side: as many as keep them within
+// 96 MB (L2 holds them), at most 16.
+int msbf_ztiles(const fap_dgraph *G, int count) {
+  const int64_t per = std::max<int64_t>(G->n, 1) * kMsbfS * 4;
+  return (int)std::max<int64_t>(1, std::min<int64_t>({((int64_t)96 << 20) / per, 16, ceil_div(count, kMsbfS)}));
+}
+
+// Work items, bitmaps and the pinned convergence flags of the tiled form,
+// for `count` sources.
+int prepare_msbf(fap_dgraph *G, int count) {
   FAP_TRY(ensure_in_edges(G));
   if (G->msbf_nitems == 0) {
     std::vector<int32_t> tro((size_t)G->n + 1);
@@ -929,10 +937,11 @@ int prepare_msbf(fap_dgraph *G) {
       FAP_CK(cudaMemcpy(G->d_msbf_items.p, items.data(), items.size() * sizeof(MsbfItem), cudaMemcpyHostToDevice));
     G->msbf_nitems = (int)items.size();
   }
-  FAP_TRY(G->d_msbf_act.ensure((size_t)2 * ceil_div(G->n, 32) * 4));
+  const int z = msbf_ztiles(G, count);
+  FAP_TRY(G->d_msbf_act.ensure((size_t)2 * z * ceil_div(G->n, 32) * 4));
   FAP_TRY(G->d_msbf_changed.ensure(4 * sizeof(int)));
   if (!G->h_changed) FAP_CK(cudaHostAlloc(reinterpret_cast<void **>(&G->h_changed), 4 * sizeof(int), 0));
-  FAP_TRY(G->sssp_scratch.ensure((size_t)G->n * kMsbfS * 4));
+  FAP_TRY(G->sssp_scratch.ensure((size_t)z * G->n * kMsbfS * 4));
   return FAP_OK;
 }
 
@@ -943,11 +952,11 @@ int run_stage1_sssp(fap_dgraph *G, const int32_t *src, const int64_t *srow, int 
                     int64_t max_rounds, int64_t *L) {
   cudaStream_t st = G->ctx->stream;
   if (use_msbf(G)) {
-    FAP_TRY(prepare_msbf(G));
+    FAP_TRY(prepare_msbf(G, count));
     FAP_CK(launch_msbf<T>(G->d_msbf_items.as<const MsbfItem>(), G->msbf_nitems, G->d_tro.as<const int32_t>(),
                           G->d_tcol.as<const int32_t>(), G->d_tw.as<const T>(), G->n,
                           G->d_st2ed.as<const int32_t>(), src, srow, count, D, G->ldD, G->ldD,
-                          G->sssp_scratch.as<T>(), G->d_msbf_act.as<uint32_t>(), G->d_msbf_changed.as<int>(),
+                          msbf_ztiles(G, count), G->sssp_scratch.as<T>(), G->d_msbf_act.as<uint32_t>(), G->d_msbf_changed.as<int>(),
                           G->h_changed, max_rounds, status, st, L));
     return FAP_OK;
   }
@@ -1811,7 +1820,7 @@ int cache_build_impl(fap_dgraph *G) {
   FAP_TRY(G->d_cparts.ensure(G->cparts.size() * sizeof(PartDesc)));
   FAP_TRY(G->d_src.ensure(std::max<size_t>(src.size(), 1) * 4));
   FAP_TRY(G->d_srcrows.ensure(std::max<size_t>(srows.size(), 1) * 8));
-  if (!bm)
+  if (!bm && !use_msbf(G))  // (the tiled form sizes its own tiles)
     FAP_TRY(G->sssp_scratch.ensure(
         (size_t)std::max(sssp_scratch_rows(G->n, (int)src.size()), 1) * (size_t)G->n * 4));
   FAP_CK(cudaMemcpy(G->d_cparts.p, G->cparts.data(), G->cparts.size() * sizeof(PartDesc),
@@ -2020,9 +2029,14 @@ extern "C" int fap_graph_cache_bytes(const fap_dgraph *G, int64_t *bytes, int *b
                   (int64_t)alloc_size((size_t)bgraph_ztiles(G) * (G->K + 1) * 4);
       }
     } else {
-      *bytes = cs.bytes(G) + (int64_t)alloc_size(
-                                 (size_t)std::max(sssp_scratch_rows(G->n, (int)std::min<int64_t>(cs.total_b, INT32_MAX)), 1) *
-                                 (size_t)G->n * 4);
+      const int cnt = (int)std::min<int64_t>(cs.total_b, INT32_MAX);
+      if (use_msbf(G))  // tiles, bitmaps, work items
+        *bytes = cs.bytes(G) + (int64_t)alloc_size((size_t)msbf_ztiles(G, cnt) * G->n * kMsbfS * 4) +
+                 (int64_t)alloc_size((size_t)2 * msbf_ztiles(G, cnt) * ceil_div(G->n, 32) * 4) +
+                 (int64_t)alloc_size((size_t)(G->m / 32 + G->n + 1) * sizeof(MsbfItem));
+      else
+        *bytes = cs.bytes(G) + (int64_t)alloc_size((size_t)std::max(sssp_scratch_rows(G->n, cnt), 1) *
+                                                   (size_t)G->n * 4);
     }
   }
   return FAP_OK;

@@ -212,14 +212,18 @@ cudaError_t launch_sssp(const int32_t *row_offset, const int32_t *col, const T *
 // iterations until one changes nothing (or the round bound is reached).
 // Source s of the tile (global index s0 + s): vertex st2ed[sources[s0 + s]];
 // without a source list the work graph's own vertex s0 + s.
+// Several tiles run side by side: tile z (blockIdx.y here) at
+// Dt + z * n * kMsbfS with its bitmaps at act + z * words, sources
+// s0 + z * kMsbfS + s.
 template <typename T>
-__global__ void msbf_seed_kernel(T *Dt, const int32_t *__restrict__ sources, const int32_t *__restrict__ st2ed,
-                                 int s0, int ns, uint32_t *act) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= ns) return;
-  const int v = sources ? __ldg(st2ed + __ldg(sources + s0 + s)) : s0 + s;
-  Dt[(int64_t)v * kMsbfS + s] = T(0);
-  atomicOr(act + (v >> 5), 1u << (v & 31));
+__global__ void msbf_seed_kernel(T *Dt, int n, const int32_t *__restrict__ sources, const int32_t *__restrict__ st2ed,
+                                 int s0, int num_sources, int64_t words, uint32_t *act) {
+  const int64_t z = blockIdx.y;
+  const int s = threadIdx.x, g = s0 + (int)z * kMsbfS + s;
+  if (g >= num_sources) return;
+  const int v = sources ? __ldg(st2ed + __ldg(sources + g)) : g;
+  Dt[(z * n + v) * kMsbfS + s] = T(0);
+  atomicOr(act + z * words + (v >> 5), 1u << (v & 31));
 }
 
 // One warp lowers row v of the tile from up to 32 in-edges e0..e1 whose
@@ -285,17 +289,20 @@ __device__ __forceinline__ bool msbf_pull_row(T *Dt, int v, int e0, int e1, cons
 
 template <typename T>
 __global__ void __launch_bounds__(256)
-    msbf_iter_kernel(T *Dt, const MsbfItem *__restrict__ items, int nitems, const int32_t *__restrict__ tro,
-                     const int32_t *__restrict__ tcol, const T *__restrict__ tw, const uint32_t *__restrict__ act_cur,
-                     uint32_t *act_next, int *changed) {
+    msbf_iter_kernel(T *Dt, int n, int ntiles, const MsbfItem *__restrict__ items, int nitems,
+                     const int32_t *__restrict__ tro, const int32_t *__restrict__ tcol, const T *__restrict__ tw,
+                     const uint32_t *__restrict__ act_cur, uint32_t *act_next, int64_t words, int *changed) {
   const int lane = threadIdx.x & 31;
-  const int nwarps = gridDim.x * (blockDim.x >> 5);
-  auto active = [act_cur](int u) { return ((__ldg(act_cur + (u >> 5)) >> (u & 31)) & 1u) != 0; };
-  for (int it = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < nitems; it += nwarps) {
-    const MsbfItem m = items[it];
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  const int64_t total = (int64_t)ntiles * nitems;
+  for (int64_t it = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < total; it += nwarps) {
+    const int64_t z = it / nitems;
+    const MsbfItem m = items[it - z * nitems];
+    const uint32_t *ac = act_cur + z * words;
+    auto active = [ac](int u) { return ((__ldg(ac + (u >> 5)) >> (u & 31)) & 1u) != 0; };
     const int e1 = min(m.e0 + 32, __ldg(tro + m.v + 1));
-    if (msbf_pull_row<T>(Dt, m.v, m.e0, e1, tcol, tw, active) && lane == 0) {
-      atomicOr(act_next + (m.v >> 5), 1u << (m.v & 31));
+    if (msbf_pull_row<T>(Dt + z * n * kMsbfS, m.v, m.e0, e1, tcol, tw, active) && lane == 0) {
+      atomicOr(act_next + z * words + (m.v >> 5), 1u << (m.v & 31));
       *changed = 1;
     }
   }
@@ -329,20 +336,21 @@ __global__ void __launch_bounds__(256)
 template <typename T>
 cudaError_t launch_msbf(const MsbfItem *items, int nitems, const int32_t *tro, const int32_t *tcol, const T *tw,
                         int n, const int32_t *st2ed, const int32_t *sources, const int64_t *out_rows,
-                        int num_sources, T *out, int64_t ld, int64_t init_cols, T *Dt, uint32_t *act,
+                        int num_sources, T *out, int64_t ld, int64_t init_cols, int ztiles, T *Dt, uint32_t *act,
                         int *changed, int *host_changed, int64_t max_rounds, int *status, cudaStream_t stream,
                         int64_t *launches) {
   if (num_sources <= 0) return cudaSuccess;
+  if (ztiles < 1 || ztiles > 64) return cudaErrorInvalidValue;
   const int64_t words = ceil_div(n, 32);
-  uint32_t *act_a = act, *act_b = act + words;
+  uint32_t *act_a = act, *act_b = act + ztiles * words;
   const int iter_blocks = 148 * 8;
   constexpr int kChunk = 4;  // iterations between convergence checks
-  for (int s0 = 0; s0 < num_sources; s0 += kMsbfS) {
-    const int ns = std::min(kMsbfS, num_sources - s0);
-    cudaError_t e = launch_fill<T>(Dt, n, kMsbfS, kMsbfS, Dist<T>::inf(), stream, launches);
-    if (e == cudaSuccess) e = cudaMemsetAsync(act_a, 0, words * 4, stream);
+  for (int s0 = 0; s0 < num_sources; s0 += ztiles * kMsbfS) {
+    const int z = (int)std::min<int64_t>(ztiles, ceil_div(num_sources - s0, kMsbfS));  // tiles side by side
+    cudaError_t e = launch_fill<T>(Dt, (int64_t)z * n, kMsbfS, kMsbfS, Dist<T>::inf(), stream, launches);
+    if (e == cudaSuccess) e = cudaMemsetAsync(act_a, 0, z * words * 4, stream);
     if (e != cudaSuccess) return e;
-    msbf_seed_kernel<T><<<1, kMsbfS, 0, stream>>>(Dt, sources, st2ed, s0, ns, act_a);
+    msbf_seed_kernel<T><<<dim3(1, z), kMsbfS, 0, stream>>>(Dt, n, sources, st2ed, s0, num_sources, words, act_a);
     *launches += 1;
     bool done = false;
     for (int64_t round = 0; !done; round += kChunk) {
@@ -355,10 +363,10 @@ cudaError_t launch_msbf(const MsbfItem *items, int nitems, const int32_t *tro, c
       e = cudaMemsetAsync(changed, 0, kChunk * sizeof(int), stream);
       if (e != cudaSuccess) return e;
       for (int c = 0; c < kChunk; c++) {
-        e = cudaMemsetAsync(act_b, 0, words * 4, stream);
+        e = cudaMemsetAsync(act_b, 0, z * words * 4, stream);
         if (e != cudaSuccess) return e;
-        msbf_iter_kernel<T><<<iter_blocks, 256, 0, stream>>>(Dt, items, nitems, tro, tcol, tw, act_a, act_b,
-                                                            changed + c);
+        msbf_iter_kernel<T><<<iter_blocks, 256, 0, stream>>>(Dt, n, z, items, nitems, tro, tcol, tw, act_a, act_b,
+                                                            words, changed + c);
         *launches += 1;
         std::swap(act_a, act_b);
       }
@@ -367,9 +375,13 @@ cudaError_t launch_msbf(const MsbfItem *items, int nitems, const int32_t *tro, c
       if (e != cudaSuccess) return e;
       for (int c = 0; c < kChunk; c++) done |= host_changed[c] == 0;
     }
-    msbf_store_kernel<T><<<(unsigned)ceil_div(init_cols, 32), 256, 0, stream>>>(Dt, n, s0, ns, out, ld, out_rows,
-                                                                               init_cols, nullptr);
-    *launches += 1;
+    for (int q = 0; q < z; q++) {
+      const int sq = s0 + q * kMsbfS;
+      msbf_store_kernel<T><<<(unsigned)ceil_div(init_cols, 32), 256, 0, stream>>>(
+          Dt + (int64_t)q * n * kMsbfS, n, sq, std::min(kMsbfS, num_sources - sq), out, ld, out_rows, init_cols,
+          nullptr);
+    }
+    *launches += z;
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
@@ -2161,8 +2173,9 @@ cudaError_t launch_relax_peak(T *sink, int blocks, int iters, cudaStream_t strea
                                       cudaStream_t, int64_t *);                                   \
   template cudaError_t launch_msbf<T>(const MsbfItem *, int, const int32_t *, const int32_t *,     \
                                       const T *, int, const int32_t *, const int32_t *,            \
-                                      const int64_t *, int, T *, int64_t, int64_t, T *, uint32_t *, \
-                                      int *, int *, int64_t, int *, cudaStream_t, int64_t *);      \
+                                      const int64_t *, int, T *, int64_t, int64_t, int, T *,       \
+                                      uint32_t *, int *, int *, int64_t, int *, cudaStream_t,      \
+                                      int64_t *); \
   template cudaError_t launch_gather<T>(const PartDesc *, int, int, const int32_t *,              \
                                         const int32_t *, const T *, const int32_t *,              \
                                         const int32_t *, const int32_t *, const T *, int64_t, T *, \

@@ -76,8 +76,9 @@ cudaError_t launch_sssp(const int32_t *row_offset, const int32_t *col, const T *
 // sources are sorted positions (st2ed maps them to vertices); row s of the
 // output is out_rows[s] (original column order, init_cols columns).  With
 // sources == nullptr the sources are the work graph's vertices 0..num-1, and
-// with out_rows == nullptr source s goes to row s.  Dt
-// holds n x kMsbfS values, act 2 x ceil(n/32) words, changed 4 ints on the
+// with out_rows == nullptr source s goes to row s.  ztiles tiles run side
+// by side: Dt holds ztiles x n x kMsbfS values, act 2 x ztiles x ceil(n/32)
+// words, changed 4 ints on the
 // device and host_changed 4 ints on the host (the launcher synchronises the
 // stream every 4 iterations to test convergence).
 constexpr int kMsbfS = 128;
@@ -89,7 +90,7 @@ struct MsbfItem {
 template <typename T>
 cudaError_t launch_msbf(const MsbfItem *items, int nitems, const int32_t *tro, const int32_t *tcol, const T *tw,
                         int n, const int32_t *st2ed, const int32_t *sources, const int64_t *out_rows,
-                        int num_sources, T *out, int64_t ld, int64_t init_cols, T *Dt, uint32_t *act,
+                        int num_sources, T *out, int64_t ld, int64_t init_cols, int ztiles, T *Dt, uint32_t *act,
                         int *changed, int *host_changed, int64_t max_rounds, int *status, cudaStream_t stream,
                         int64_t *launches);
 
