@@ -228,7 +228,7 @@ struct fap_dgraph {
   // least 6 arcs per vertex, where few Bellman-Ford iterations suffice), 1
   // frontier kernel, 2 tiled.  Work items over the in-edge CSR.
   int sssp_form = 0;
-  int64_t tile_mb = 96;  // memory for tiles side by side (tiled SSSP, Bellman-Ford closure)
+  int64_t tile_bytes = int64_t(96) << 20;  // memory for tiles side by side (tiled SSSP, Bellman-Ford closure)
   DevBuf d_msbf_items, d_msbf_act, d_msbf_changed;
   int msbf_nitems = 0;
   int *h_changed = nullptr;  // pinned, 4 ints
@@ -614,7 +614,7 @@ bool bmethod_ok(const fap_dgraph *G) {
 int bgraph_ztiles(const fap_dgraph *G) {
   const int64_t per = std::max<int64_t>(G->total_b, 1) * kMsbfS * 4;
   const int64_t tiles = ceil_div(std::max<int64_t>(G->total_b, 1), kMsbfS);
-  return (int)std::max<int64_t>(1, std::min<int64_t>({(G->tile_mb << 20) / per, 16, tiles}));
+  return (int)std::max<int64_t>(1, std::min<int64_t>({G->tile_bytes / per, 16, tiles}));
 }
 
 // Cross-part arcs between boundary vertices (g = boff[p] + c for the c-th
@@ -920,7 +920,7 @@ const char *stage1_form_name(const fap_dgraph *G, bool bmethod) {
 // 96 MB (L2 holds them), at most 16.
 int msbf_ztiles(const fap_dgraph *G, int count) {
   const int64_t per = std::max<int64_t>(G->n, 1) * kMsbfS * 4;
-  return (int)std::max<int64_t>(1, std::min<int64_t>({(G->tile_mb << 20) / per, 16, ceil_div(count, kMsbfS)}));
+  return (int)std::max<int64_t>(1, std::min<int64_t>({G->tile_bytes / per, 16, ceil_div(count, kMsbfS)}));
 }
 
 // Work items, bitmaps and the pinned convergence flags of the tiled form,
@@ -1596,8 +1596,8 @@ extern "C" int fap_graph_set_param(fap_dgraph *G, const char *key, double value)
     return FAP_OK;
   }
   if (std::strcmp(key, "tile_mb") == 0) {
-    if (value < 1.0 || value > 65536.0) return fail(FAP_ERR_INVALID, "tile_mb is 1..65536");
-    G->tile_mb = (int64_t)value;
+    if (!(value > 0.0) || value > 65536.0) return fail(FAP_ERR_INVALID, "tile_mb is in (0, 65536]");
+    G->tile_bytes = std::max<int64_t>(1, (int64_t)(value * 1048576.0));
     G->bg_csr_ready = false;  // the closure's tile buffers are sized with it
     G->last_ids.clear();
     G->epoch++;

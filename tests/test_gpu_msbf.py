@@ -71,3 +71,32 @@ def test_tiled_sssp_round_bound(cuda_ok):
     dg.solve(mode=FAP_MODE_BATCHED)
     cs = np.concatenate([dg.block_checksums(p) for p in range(1, int(case["K"]) + 1)])
     np.testing.assert_array_equal(cs, case["row_checksums"])
+
+
+@pytest.mark.parametrize("name", ["grid64_k8", "rmat8_f32_k4", "rmat8_int_k4"])
+@pytest.mark.parametrize("form", ["sssp", "bgraph"])
+def test_tiles_side_by_side_or_one_at_a_time(cuda_ok, name, form):
+    """The same blocks whether the 128-source tiles run side by side (the
+    default memory budget) or one at a time (tile_mb = 0.1, smaller than
+    one tile: every tile its own group, the stamps carried from group to
+    group), in the tiled SSSP form and in the Bellman-Ford closure of the
+    boundary graph."""
+    case = load_golden(name)
+    K, integral = int(case["K"]), bool(case["integral"])
+    if form == "bgraph" and not integral:
+        pytest.skip("the boundary-graph form is compared bit for bit on int32 graphs")
+    ctx, dg = _dg(case)
+    if form == "sssp":
+        dg.set_param("sssp_form", 2)
+    else:
+        dg.set_param("stage1", 2)
+        dg.set_param("bgraph_form", 2)
+    outs = []
+    for mb in (96, 0.1):
+        dg.set_param("tile_mb", mb)
+        dg.solve(mode=FAP_MODE_BATCHED)
+        dg.check()
+        outs.append(_blocks(dg, K))
+    _close(outs[1], outs[0], True)
+    if "dist" in case:
+        _close(outs[0], case["dist"], integral)
