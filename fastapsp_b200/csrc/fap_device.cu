@@ -544,11 +544,15 @@ __global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS, 2)
   if (t < nb - 1) {
     const int j = t < kb ? t : t + 1;
     ok = floyd_tile_update<T, kFloydTile>(&mapA, &mapB, blockIdx.y, mat, pd.ldf, kb, j, kb, sm,
-                                          min(kFloydTile, pd.s - kb * kFloydTile));
+                                          min(kFloydTile, pd.s - kb * kFloydTile),
+                                          min(kFloydTile, pd.s - kb * kFloydTile),
+                                          min(kFloydTile, pd.s - j * kFloydTile));
   } else {
     t -= nb - 1;
     const int i = t < kb ? t : t + 1;
     ok = floyd_tile_update<T, kFloydTile>(&mapA, &mapB, blockIdx.y, mat, pd.ldf, i, kb, kb, sm,
+                                          min(kFloydTile, pd.s - kb * kFloydTile),
+                                          min(kFloydTile, pd.s - i * kFloydTile),
                                           min(kFloydTile, pd.s - kb * kFloydTile));
   }
   if (!ok && threadIdx.x == 0) set_status(status, kDevTmaTimeout);
@@ -570,7 +574,9 @@ __global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS, 2)
   i = i < kb ? i : i + 1;
   j = j < kb ? j : j + 1;
   if (!floyd_tile_update<T, kFloydTile>(&mapA, &mapB, blockIdx.y, F + pd.f_off, pd.ldf, i, j, kb, sm,
-                                        min(kFloydTile, pd.s - kb * kFloydTile)) &&
+                                        min(kFloydTile, pd.s - kb * kFloydTile),
+                                        min(kFloydTile, pd.s - i * kFloydTile),
+                                        min(kFloydTile, pd.s - j * kFloydTile)) &&
       threadIdx.x == 0)
     set_status(status, kDevTmaTimeout);
 }

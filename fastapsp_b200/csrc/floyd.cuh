@@ -106,20 +106,21 @@ __device__ __forceinline__ void floyd_diag_close(T *mat, int64_t ld, int r0, T *
 // Phase 2/3 on one tile of part z: D[ti][tj] = min(D[ti][tj], D[ti][tk] (x)
 // D[tk][tj]).  mat is the part's matrix (ld = arena leading dimension);
 // mapA/mapB describe the arena with TILE x 16 and 16 x TILE boxes; only the
-// first kvalid pivots of block tk are real (the rest is padding).
+// first kvalid pivots of block tk, mvalid rows of block ti and nvalid columns
+// of block tj are real (the rest is padding, the sentinel, left as it is).
 // Block-wide; false if a TMA stage never completed.
 template <typename T, int TILE>
 __device__ __forceinline__ bool floyd_tile_update(const CUtensorMap *mapA, const CUtensorMap *mapB,
                                                   int z, T *mat, int64_t ld, int ti, int tj, int tk,
                                                   TmaSmem<T, typename FloydCfg<T, TILE>::TC> &sm,
-                                                  int kvalid = TILE) {
+                                                  int kvalid = TILE, int mvalid = TILE, int nvalid = TILE) {
   using C = typename FloydCfg<T, TILE>::C;
   using TC = typename FloydCfg<T, TILE>::TC;
   T acc[C::TM][C::TN];
   const int64_t r0 = (int64_t)ti * TILE, c0 = (int64_t)tj * TILE;
   acc_load<T, C, true>(acc, mat + r0 * ld + c0, ld, 0, 0, 0, 0);
-  const bool ok = tma_minplus_tile<T, TC>(mapA, tk * TILE, ti * TILE, z, mapB, tj * TILE, tk * TILE,
-                                          z, kvalid, acc, sm);
+  const bool ok = tma_minplus_tile<T, TC, true>(mapA, tk * TILE, ti * TILE, z, mapB, tj * TILE, tk * TILE,
+                                                z, kvalid, acc, sm, mvalid, nvalid);
   if (ok) acc_store<T, C, true>(acc, mat + r0 * ld + c0, ld, 0, 0, 0, 0);
   return ok;
 }
@@ -133,15 +134,17 @@ __device__ bool floyd_close_cta(const CUtensorMap *mapA, const CUtensorMap *mapB
   for (int kb = 0; kb < nb && ok; kb++) {
     const int kv = min(TILE, s - kb * TILE);
     floyd_diag_close<T, TILE>(mat, ld, kb * TILE, sm.ring, kv);
+    auto valid = [&](int t) { return min(TILE, s - t * TILE); };
     for (int j = 0; j < nb && ok; j++)
-      if (j != kb) ok = floyd_tile_update<T, TILE>(mapA, mapB, z, mat, ld, kb, j, kb, sm, kv);
+      if (j != kb) ok = floyd_tile_update<T, TILE>(mapA, mapB, z, mat, ld, kb, j, kb, sm, kv, kv, valid(j));
     for (int i = 0; i < nb && ok; i++)
-      if (i != kb) ok = floyd_tile_update<T, TILE>(mapA, mapB, z, mat, ld, i, kb, kb, sm, kv);
+      if (i != kb) ok = floyd_tile_update<T, TILE>(mapA, mapB, z, mat, ld, i, kb, kb, sm, kv, valid(i), kv);
     __syncthreads();
     for (int i = 0; i < nb && ok; i++) {
       if (i == kb) continue;
       for (int j = 0; j < nb && ok; j++)
-        if (j != kb) ok = floyd_tile_update<T, TILE>(mapA, mapB, z, mat, ld, i, j, kb, sm, kv);
+        if (j != kb)
+          ok = floyd_tile_update<T, TILE>(mapA, mapB, z, mat, ld, i, j, kb, sm, kv, valid(i), valid(j));
     }
     __syncthreads();
   }

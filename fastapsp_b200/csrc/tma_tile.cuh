@@ -63,8 +63,10 @@ __device__ __forceinline__ TmaSmem<T, C> tma_smem_init(unsigned char *raw) {
 // One chunk of K from shared memory: As is BM x BK, Bs is BK x BN.  Per k:
 // the thread's 8 A values are 8 broadcast loads (each address is shared by
 // the 16 threads of a half-warp), its 8 B values two conflict-free 16-byte
-// loads, then 64 relaxations.
-template <typename T, class C>
+// loads, then 64 relaxations.  GI / GJ: the thread's row / column groups
+// computed (1 skips the second group, rows or columns BM/2.. or BN/2..,
+// when they are all padding).
+template <typename T, class C, int GI = 2, int GJ = 2>
 __device__ __forceinline__ void tma_chunk_compute(const T *As, const T *Bs, T (&acc)[8][8], int ty,
                                                   int tx, int kc) {
   using V = typename Vec4<T>::type;
@@ -73,28 +75,35 @@ __device__ __forceinline__ void tma_chunk_compute(const T *As, const T *Bs, T (&
   for (int k = 0; k < kc; k++) {
     T a[8], b[8];
 #pragma unroll
-    for (int g = 0; g < 2; g++)
+    for (int g = 0; g < GI; g++)
 #pragma unroll
       for (int l = 0; l < 4; l++) a[4 * g + l] = Arow[(g * (C::BM / 2) + l) * C::BK + k];
 #pragma unroll
-    for (int g = 0; g < 2; g++) {
+    for (int g = 0; g < GJ; g++) {
       const V v = *reinterpret_cast<const V *>(Bs + k * C::BN + g * (C::BN / 2) + tx * 4);
       b[4 * g + 0] = v.x; b[4 * g + 1] = v.y; b[4 * g + 2] = v.z; b[4 * g + 3] = v.w;
     }
 #pragma unroll
-    for (int i = 0; i < 8; i++)
+    for (int i = 0; i < 4 * GI; i++)
 #pragma unroll
-      for (int j = 0; j < 8; j++) acc[i][j] = Dist<T>::relax(a[i], b[j], acc[i][j]);
+      for (int j = 0; j < 4 * GJ; j++) acc[i][j] = Dist<T>::relax(a[i], b[j], acc[i][j]);
   }
 }
 
 // acc <- min(acc, A (x) B) for K elements of the inner dimension, A boxes at
 // (ax + c*BK, ay, az) of mapA and B boxes at (bx, by + c*BK, bz) of mapB.
 // Block-wide.  Returns false (in every thread) if a stage never completed.
-template <typename T, class C>
+// mvalid / nvalid: rows / columns of the tile that are not padding (the
+// second half of the thread's rows or columns is skipped when they are all
+// padding; the caller's padding then keeps its values).
+// (PAD: the caller may pass tiles with padding; otherwise the full-tile
+// compute is the only one compiled.)
+template <typename T, class C, bool PAD = false>
 __device__ __forceinline__ bool tma_minplus_tile(const CUtensorMap *mapA, int ax, int ay, int az,
                                                  const CUtensorMap *mapB, int bx, int by, int bz,
-                                                 int K, T (&acc)[8][8], TmaSmem<T, C> &sm) {
+                                                 int K, T (&acc)[8][8], TmaSmem<T, C> &sm,
+                                                 int mvalid = C::BM, int nvalid = C::BN) {
+  const bool rhi = !PAD || mvalid > C::BM / 2, chi = !PAD || nvalid > C::BN / 2;
   const int tid = threadIdx.x, ty = tid / C::TX, tx = tid % C::TX;
   const int n = (int)ceil_div(K, C::BK);
   if (n == 0) return true;
@@ -117,7 +126,11 @@ __device__ __forceinline__ bool tma_minplus_tile(const CUtensorMap *mapA, int ax
     sm.phase ^= 1u << s;
     if (got) {
       const T *As = sm.ring + s * C::STAGE_ELEMS;
-      tma_chunk_compute<T, C>(As, As + C::A_ELEMS, acc, ty, tx, min(C::BK, K - c * C::BK));
+      const int kc = min(C::BK, K - c * C::BK);
+      if (!PAD || (rhi && chi)) tma_chunk_compute<T, C, 2, 2>(As, As + C::A_ELEMS, acc, ty, tx, kc);
+      else if (rhi) tma_chunk_compute<T, C, 2, 1>(As, As + C::A_ELEMS, acc, ty, tx, kc);
+      else if (chi) tma_chunk_compute<T, C, 1, 2>(As, As + C::A_ELEMS, acc, ty, tx, kc);
+      else tma_chunk_compute<T, C, 1, 1>(As, As + C::A_ELEMS, acc, ty, tx, kc);
     }
     fence_proxy_async_smem();  // this thread's reads of stage s precede its refill
     if (__syncthreads_or(!got)) {

@@ -255,6 +255,10 @@ WORKLOADS = {
     # 512x512 grid + 1% long-range edges, int weights in [1,100], K=256
     "grid512": dict(make=lambda: grid_graph(512, 512, extra_frac=0.01, wmin=1, wmax=100,
                                             seed=3), K=256),
+    # min-plus profiling case of the grid shape: ~1024-vertex parts with
+    # ~120 boundary vertices, 1 GB of output
+    "grid128": dict(make=lambda: grid_graph(128, 128, extra_frac=0.01, wmin=1, wmax=100,
+                                            seed=7), K=16),
     # profiling-size stand-in for grid512: same part size (~1024 vertices),
     # over 8192 boundary vertices (the Bellman-Ford closure of the boundary graph)
     "grid256": dict(make=lambda: grid_graph(256, 256, extra_frac=0.01, wmin=1, wmax=100,
