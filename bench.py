@@ -105,12 +105,13 @@ class ClockSampler:
     """nvidia-smi clocks/throttle reasons sampled during the timed region."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,timestamp")
 
     def __init__(self, index):
         self.index = index
         self.proc = None
         self.path = None
+        self.window = None  # (start, stop) wall times of the timed region
 
     def start(self):
         fd, self.path = tempfile.mkstemp(suffix=".csv")
@@ -118,10 +119,21 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+            return
+        # nvidia-smi takes a moment to start: wait (bounded) for its first sample
+        t0 = time.time()
+        while time.time() - t0 < 5.0 and self.proc.poll() is None:
+            if os.path.getsize(self.path) > 0:
+                break
+            time.sleep(0.02)
+
+    def mark(self, start, stop):
+        """Wall times of the timed region: only samples inside it count."""
+        self.window = (start, stop)
 
     def stop(self):
         if self.proc is None:
@@ -131,26 +143,39 @@ class ClockSampler:
             self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
-        sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        rows = []
         with open(self.path) as f:
             for line in f:
                 parts = [x.strip() for x in line.split(",")]
-                if len(parts) < 9:
+                if len(parts) < 10:
                     continue
                 try:
-                    sm.append(float(parts[1]))
-                    smax.append(float(parts[2]))
+                    row = (None, float(parts[1]), float(parts[2]), parts[5:9])
                 except ValueError:
                     continue
-                for nm, v in zip(names, parts[5:9]):
-                    if v.lower().startswith("active"):
-                        reasons.add(nm)
+                try:
+                    t = datetime.datetime.strptime(parts[9], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                    row = (t,) + row[1:]
+                except ValueError:
+                    pass
+                rows.append(row)
         os.unlink(self.path)
+        inside = [r for r in rows if self.window and r[0] is not None
+                  and self.window[0] - 0.05 <= r[0] <= self.window[1] + 0.05]
+        use = inside or rows
+        sm = [r[1] for r in use]
+        smax = [r[2] for r in use]
+        reasons = set()
+        for r in use:
+            for nm, v in zip(names, r[3]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax),
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm),
+                "window": "timed region" if inside else "around the timed region (none inside)"}
 
 
 def _jsonable(o):
@@ -342,7 +367,7 @@ def run_serving(args, device):
 
     # warm-up of the mixed stream itself (every kernel shape it uses, batch
     # buffers at their working sizes), untimed
-    closed_loop([draw() for _ in range(max(64, args.serve_burst // 4))])
+    closed_loop([draw() for _ in range(max(64, args.serve_burst))])
     # capacity: closed loop, a window of 64 requests in flight, measured twice;
     # the lower figure sets the offered loads, so that "90%" is not an overload
     caps = []
@@ -533,6 +558,7 @@ def main_fap(args):
     torch.cuda.synchronize()
     clocks = ClockSampler(local)
     clocks.start()
+    t_timed = time.time()
     step_ms, stages = [], []
     cache_phases = []
     launches = 0
@@ -574,6 +600,7 @@ def main_fap(args):
     torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
+    clocks.mark(t_timed, time.time())
     clk = clocks.stop()
     dg.check()
     my_ms = float(np.sum(step_ms))
