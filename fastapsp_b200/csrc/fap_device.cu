@@ -1232,22 +1232,25 @@ cudaError_t launch_bgraph(const PartDesc *parts, int nparts, int max_b, const T 
 // (coalesced stores in original column order) from the boundary rows of the
 // column's part, read once for all of the CTA's rows.  Own-part entries are
 // also written to FB[g][j] (the exact distances from boundary vertex g to
-// its part's vertices, for the local-closure fix-up).
+// its part's vertices, for the local-closure fix-up).  RG rows per CTA:
+// 32 where their dB entries fit in shared memory (each scattered F load
+// then serves 32 rows), else 8.
 constexpr int kExpandRows = 8;
+constexpr int kExpandRowsWide = 32;
 
-template <typename T>
+template <typename T, int RG>
 __global__ void __launch_bounds__(256)
     bdy_expand_kernel(const int64_t *__restrict__ rows, int nrows, const BPart *__restrict__ bpart,
                       const int32_t *__restrict__ graph_id, const int32_t *__restrict__ ed2st, int n,
                       const T *__restrict__ dB, int64_t ldB, int nbB, const T *__restrict__ F, T *D,
                       int64_t ldD, T *FB, int64_t ldFB) {
   extern __shared__ unsigned char bx_smem_raw[];
-  T *drow = reinterpret_cast<T *>(bx_smem_raw);  // kExpandRows x nbB
-  const int r0 = blockIdx.y * kExpandRows;
-  const int nr = min(kExpandRows, nrows - r0);
-  int64_t g[kExpandRows], dr[kExpandRows];
+  T *drow = reinterpret_cast<T *>(bx_smem_raw);  // RG x nbB
+  const int r0 = blockIdx.y * RG;
+  const int nr = min(RG, nrows - r0);
+  int64_t g[RG], dr[RG];
 #pragma unroll
-  for (int q = 0; q < kExpandRows; q++) {
+  for (int q = 0; q < RG; q++) {
     g[q] = q < nr ? rows[2 * (r0 + q)] : 0;
     dr[q] = q < nr ? rows[2 * (r0 + q) + 1] : 0;
   }
@@ -1258,9 +1261,9 @@ __global__ void __launch_bounds__(256)
   __syncthreads();
   const T inf = Dist<T>::inf();
   for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < ldD; v += (int64_t)gridDim.x * blockDim.x) {
-    T acc[kExpandRows];
+    T acc[RG];
 #pragma unroll
-    for (int q = 0; q < kExpandRows; q++) acc[q] = inf;
+    for (int q = 0; q < RG; q++) acc[q] = inf;
     int j = -1, qb = 0, qoff = 0;
     if (v < n) {
       const BPart Q = bpart[__ldg(graph_id + v)];
@@ -1271,11 +1274,11 @@ __global__ void __launch_bounds__(256)
       for (int k = 0; k < Q.b; k++) {
         const T f = __ldg(Fq + (int64_t)k * Q.ldf);
 #pragma unroll
-        for (int q = 0; q < kExpandRows; q++) acc[q] = Dist<T>::relax(drow[q * nbB + Q.boff + k], f, acc[q]);
+        for (int q = 0; q < RG; q++) acc[q] = Dist<T>::relax(drow[q * nbB + Q.boff + k], f, acc[q]);
       }
     }
 #pragma unroll
-    for (int q = 0; q < kExpandRows; q++) {
+    for (int q = 0; q < RG; q++) {
       if (q >= nr) break;
       D[dr[q] * ldD + v] = acc[q];
       if (j >= 0 && g[q] >= qoff && g[q] < qoff + qb) FB[g[q] * ldFB + j] = acc[q];
@@ -1283,25 +1286,36 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-template <typename T>
-cudaError_t launch_bdy_expand(const int64_t *rows, int nrows, const BPart *bpart, const int32_t *graph_id,
-                              const int32_t *ed2st, int n, const T *dB, int64_t ldB, int nbB, const T *F,
-                              T *D, int64_t ldD, T *FB, int64_t ldFB, cudaStream_t stream, int64_t *launches) {
-  if (nrows <= 0) return cudaSuccess;
-  const size_t smem = (size_t)kExpandRows * std::max(nbB, 1) * sizeof(T);
-  auto kern = bdy_expand_kernel<T>;
+template <typename T, int RG>
+cudaError_t launch_bdy_expand_rg(const int64_t *rows, int nrows, const BPart *bpart, const int32_t *graph_id,
+                                 const int32_t *ed2st, int n, const T *dB, int64_t ldB, int nbB, const T *F,
+                                 T *D, int64_t ldD, T *FB, int64_t ldFB, cudaStream_t stream, int64_t *launches) {
+  const size_t smem = (size_t)RG * std::max(nbB, 1) * sizeof(T);
+  auto kern = bdy_expand_kernel<T, RG>;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
   // Enough CTAs for about 16 per SM, each looping over columns so that the
   // rows' dB entries are staged only once per CTA.
-  const int64_t ny = ceil_div(nrows, kExpandRows);
+  const int64_t ny = ceil_div(nrows, RG);
   const int bx = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(ldD, 256), ceil_div(148 * 16, ny)));
   kern<<<dim3(bx, (unsigned)ny), 256, smem, stream>>>(
       rows, nrows, bpart, graph_id, ed2st, n, dB, ldB, nbB, F, D, ldD, FB, ldFB);
   *launches += 1;
   return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_bdy_expand(const int64_t *rows, int nrows, const BPart *bpart, const int32_t *graph_id,
+                              const int32_t *ed2st, int n, const T *dB, int64_t ldB, int nbB, const T *F,
+                              T *D, int64_t ldD, T *FB, int64_t ldFB, cudaStream_t stream, int64_t *launches) {
+  if (nrows <= 0) return cudaSuccess;
+  if ((size_t)kExpandRowsWide * std::max(nbB, 1) * sizeof(T) <= 160 * 1024)
+    return launch_bdy_expand_rg<T, kExpandRowsWide>(rows, nrows, bpart, graph_id, ed2st, n, dB, ldB, nbB, F, D,
+                                                     ldD, FB, ldFB, stream, launches);
+  return launch_bdy_expand_rg<T, kExpandRows>(rows, nrows, bpart, graph_id, ed2st, n, dB, ldB, nbB, F, D, ldD,
+                                              FB, ldFB, stream, launches);
 }
 
 // Boundary graph closed by Bellman-Ford in alternating steps (large
