@@ -739,7 +739,8 @@ int close_bgraph(fap_dgraph *G, const PartDesc *dp, int np, int max_b, const T *
     FAP_CK(launch_bgraph<T>(dp, np, max_b, F, dB, G->ldB, G->ro.as<const int32_t>(), G->col.as<const int32_t>(),
                             G->w.as<const T>(), G->n, G->d_gid.as<const int32_t>(),
                             G->d_ed2st.as<const int32_t>(), G->d_bpart.as<const BPart>(), st, L));
-    FAP_CK(launch_floyd_matrix<T>(dB, G->ldB, (int)(G->ldB / kFloydTile), status, st, L));
+    FAP_CK(launch_floyd_matrix<T>(dB, G->ldB, (int)ceil_div(G->total_b, kFloydTile), status, st, L,
+                                  (int)G->total_b));
     return FAP_OK;
   }
   const int z = bgraph_ztiles(G);
@@ -1057,7 +1058,7 @@ int run_solve(fap_dgraph *G, int mode) {
       FAP_CK(launch_sssp<T>(ro_s, col_s, w_s, G->n, src + s0, srow + s0, s1 - s0, D, G->ldD,
                             G->ldD, ed2st, scratch, delta, G->sssp_chain, G->sssp_precheck, max_rounds, status, st, &L));
       FAP_CK(launch_gather<T>(dp + i, 1, d.ldf, ro, col, w, gid, st2ed, ed2st, D, G->ldD, F, st, &L));
-      FAP_CK(launch_floyd_matrix<T>(F + d.f_off, d.ldf, (int)ceil_div(d.s, kFloydTile), status, st, &L));
+      FAP_CK(launch_floyd_matrix<T>(F + d.f_off, d.ldf, (int)ceil_div(d.s, kFloydTile), status, st, &L, d.s));
       FAP_CK(launch_bdy_scatter<T>(dp + i, 1, F, D, G->ldD, st2ed, d.b, d.s, st, &L));
       if (G->thin_pos[i] >= 0)
         FAP_CK(launch_minplus_thin<T>(dp, G->d_thin.as<int32_t>() + G->thin_pos[i], 1, d.s - d.b, G->n, F, D,

@@ -436,57 +436,61 @@ cudaError_t launch_floyd_parts(const PartDesc *parts, int nparts, T *F, int64_t 
 // sentinel to nb tiles per side), one launch per phase per pivot block.
 template <typename T>
 __global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS, 2)
-    floyd_mat_phase1_kernel(T *mat, int64_t ld, int kb) {
+    floyd_mat_phase1_kernel(T *mat, int64_t ld, int kb, int s) {
   using TC = typename FloydCfg<T, kFloydTile>::TC;
   extern __shared__ __align__(128) unsigned char fq_smem_raw[];
   auto sm = tma_smem_init<T, TC>(fq_smem_raw);
-  floyd_diag_close<T, kFloydTile>(mat, ld, kb * kFloydTile, sm.ring);
+  floyd_diag_close<T, kFloydTile>(mat, ld, kb * kFloydTile, sm.ring, min(kFloydTile, s - kb * kFloydTile));
 }
 
 // blockIdx.x in [0, 2*(nb-1)): first nb-1 are row-panel tiles, rest column.
 template <typename T>
 __global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS, 2)
-    floyd_mat_phase2_kernel(T *mat, int64_t ld, int kb, int nb,
+    floyd_mat_phase2_kernel(T *mat, int64_t ld, int kb, int nb, int s,
                             const __grid_constant__ CUtensorMap mapA,
                             const __grid_constant__ CUtensorMap mapB, int *status) {
   using TC = typename FloydCfg<T, kFloydTile>::TC;
   extern __shared__ __align__(128) unsigned char fq_smem_raw[];
   auto sm = tma_smem_init<T, TC>(fq_smem_raw);
+  auto valid = [s](int t) { return min(kFloydTile, s - t * kFloydTile); };
   int t = blockIdx.x;
   bool ok;
   if (t < nb - 1) {
     const int j = t < kb ? t : t + 1;
-    ok = floyd_tile_update<T, kFloydTile>(&mapA, &mapB, 0, mat, ld, kb, j, kb, sm);
+    ok = floyd_tile_update<T, kFloydTile>(&mapA, &mapB, 0, mat, ld, kb, j, kb, sm, valid(kb), valid(kb), valid(j));
   } else {
     t -= nb - 1;
     const int i = t < kb ? t : t + 1;
-    ok = floyd_tile_update<T, kFloydTile>(&mapA, &mapB, 0, mat, ld, i, kb, kb, sm);
+    ok = floyd_tile_update<T, kFloydTile>(&mapA, &mapB, 0, mat, ld, i, kb, kb, sm, valid(kb), valid(i), valid(kb));
   }
   if (!ok && threadIdx.x == 0 && status) set_status(status, kDevTmaTimeout);
 }
 
 template <typename T>
 __global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS, 2)
-    floyd_mat_phase3_kernel(T *mat, int64_t ld, int kb, int nb,
+    floyd_mat_phase3_kernel(T *mat, int64_t ld, int kb, int nb, int s,
                             const __grid_constant__ CUtensorMap mapA,
                             const __grid_constant__ CUtensorMap mapB, int *status) {
   using TC = typename FloydCfg<T, kFloydTile>::TC;
   extern __shared__ __align__(128) unsigned char fq_smem_raw[];
   auto sm = tma_smem_init<T, TC>(fq_smem_raw);
+  auto valid = [s](int t) { return min(kFloydTile, s - t * kFloydTile); };
   const int t = blockIdx.x;
   int i = t / (nb - 1), j = t % (nb - 1);
   i = i < kb ? i : i + 1;
   j = j < kb ? j : j + 1;
-  if (!floyd_tile_update<T, kFloydTile>(&mapA, &mapB, 0, mat, ld, i, j, kb, sm) && threadIdx.x == 0 &&
-      status)
+  if (!floyd_tile_update<T, kFloydTile>(&mapA, &mapB, 0, mat, ld, i, j, kb, sm, valid(kb), valid(i), valid(j)) &&
+      threadIdx.x == 0 && status)
     set_status(status, kDevTmaTimeout);
 }
 
 template <typename T>
 cudaError_t launch_floyd_matrix(T *mat, int64_t ld, int nb, int *status, cudaStream_t stream,
-                                int64_t *launches) {
+                                int64_t *launches, int s) {
   using FC = FloydCfg<T, kFloydTile>;
   if (nb <= 0) return cudaSuccess;
+  if (s < 0 || s > nb * kFloydTile) s = nb * kFloydTile;
+  if (s <= (nb - 1) * kFloydTile) return cudaErrorInvalidValue;  // the last block holds real rows
   CUtensorMap mapA, mapB;
   cudaError_t e = make_arena_tmaps<T>(mat, ld, 1, &mapA, &mapB);
   if (e != cudaSuccess) return e;
@@ -497,12 +501,12 @@ cudaError_t launch_floyd_matrix(T *mat, int64_t ld, int nb, int *status, cudaStr
     if (e != cudaSuccess) return e;
   }
   for (int kb = 0; kb < nb; kb++) {
-    floyd_mat_phase1_kernel<T><<<1, FC::THREADS, smem, stream>>>(mat, ld, kb);
+    floyd_mat_phase1_kernel<T><<<1, FC::THREADS, smem, stream>>>(mat, ld, kb, s);
     *launches += 1;
     if (nb > 1) {
-      floyd_mat_phase2_kernel<T><<<2 * (nb - 1), FC::THREADS, smem, stream>>>(mat, ld, kb, nb, mapA, mapB,
+      floyd_mat_phase2_kernel<T><<<2 * (nb - 1), FC::THREADS, smem, stream>>>(mat, ld, kb, nb, s, mapA, mapB,
                                                                              status);
-      floyd_mat_phase3_kernel<T><<<(nb - 1) * (nb - 1), FC::THREADS, smem, stream>>>(mat, ld, kb, nb, mapA,
+      floyd_mat_phase3_kernel<T><<<(nb - 1) * (nb - 1), FC::THREADS, smem, stream>>>(mat, ld, kb, nb, s, mapA,
                                                                                     mapB, status);
       *launches += 2;
     }
@@ -2202,7 +2206,7 @@ cudaError_t launch_relax_peak(T *sink, int blocks, int iters, cudaStream_t strea
                                         cudaStream_t, int64_t *);                                 \
   template cudaError_t launch_floyd_parts<T>(const PartDesc *, int, T *, int64_t, T *, int64_t,   \
                                              const int32_t *, int *, cudaStream_t, int64_t *);    \
-  template cudaError_t launch_floyd_matrix<T>(T *, int64_t, int, int *, cudaStream_t, int64_t *); \
+  template cudaError_t launch_floyd_matrix<T>(T *, int64_t, int, int *, cudaStream_t, int64_t *, int); \
   template cudaError_t launch_floyd_parts_multi<T>(const PartDesc *, int, int, T *, int64_t, int *, \
                                                    cudaStream_t, int64_t *);                      \
   template cudaError_t launch_bdy_scatter<T>(const PartDesc *, int, const T *, T *, int64_t,      \

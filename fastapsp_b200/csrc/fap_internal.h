@@ -121,10 +121,12 @@ cudaError_t launch_floyd_parts_multi(const PartDesc *parts, int nparts, int max_
                                      int *status, cudaStream_t stream, int64_t *launches);
 
 // Plain: one padded matrix (ld a multiple of kFloydTile, nb tiles per side
-// in use), one launch per phase per pivot block.  status may be null.
+// in use), one launch per phase per pivot block.  status may be null.  s:
+// the real rows and columns (the rest is padding holding the sentinel,
+// whose pivots and tile halves are skipped); -1 = all of the nb tiles.
 template <typename T>
 cudaError_t launch_floyd_matrix(T *mat, int64_t ld, int nb, int *status, cudaStream_t stream,
-                                int64_t *launches);
+                                int64_t *launches, int s = -1);
 
 // Boundary rows of the listed parts: F[i][j] -> D[row_base+i][st2ed[start+j]].
 template <typename T>
