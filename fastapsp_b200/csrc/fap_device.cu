@@ -1654,7 +1654,9 @@ __global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS, 2)
   using TC = typename FloydCfg<T, kFloydTile>::TC;
   extern __shared__ __align__(128) unsigned char bxt_smem_raw[];
   const PartDesc pd = parts[blockIdx.z];
-  const int n0 = blockIdx.y * TC::BN, m0 = blockIdx.x * TC::BM;
+  // column tiles vary fastest: consecutive CTAs share their A tile (dB rows
+  // of part q's boundary columns) in L2; q's B tiles are small enough to stay
+  const int n0 = blockIdx.x * TC::BN, m0 = blockIdx.y * TC::BM;
   if (n0 >= pd.s) return;
   auto sm = tma_smem_init<T, TC>(bxt_smem_raw);
   T acc[8][8];
@@ -1705,7 +1707,7 @@ cudaError_t launch_bdy_expand_tma(const PartDesc *parts, int nparts, int max_s, 
                                   cudaStream_t stream, int64_t *launches) {
   using TC = typename FloydCfg<T, kFloydTile>::TC;
   if (nparts <= 0 || max_s <= 0 || nbB <= 0) return cudaSuccess;
-  if (nparts > 65535 || ceil_div(max_s, TC::BN) > 65535) return cudaErrorInvalidConfiguration;
+  if (nparts > 65535 || ceil_div(nbB, TC::BM) > 65535) return cudaErrorInvalidConfiguration;
   CUtensorMap mapA, mapB, unused;
   cudaError_t e = make_tmap_3d(&mapA, dB, Dist<T>::kDtype == FAP_DTYPE_F32, ldB, nbB, 1, TC::BK, TC::BM);
   if (e == cudaSuccess) e = make_arena_tmaps<T>(F, ldf, nparts_f, &unused, &mapB);
@@ -1714,7 +1716,7 @@ cudaError_t launch_bdy_expand_tma(const PartDesc *parts, int nparts, int max_s, 
   auto kern = bdy_expand_tma_kernel<T>;
   e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  kern<<<dim3((unsigned)ceil_div(nbB, TC::BM), (unsigned)ceil_div(max_s, TC::BN), nparts), TC::THREADS, smem,
+  kern<<<dim3((unsigned)ceil_div(max_s, TC::BN), (unsigned)ceil_div(nbB, TC::BM), nparts), TC::THREADS, smem,
          stream>>>(parts, nbB, grow, st2ed, D, ldD, FB, ldFB, mapA, mapB, status);
   *launches += 1;
   return cudaGetLastError();

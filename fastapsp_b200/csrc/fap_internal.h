@@ -217,7 +217,7 @@ cudaError_t launch_bgraph_bf(const PartDesc *parts, int nparts, int max_b, const
                              int64_t *launches);
 // Expansion with TMA-fed tiles (dB closed by Bellman-Ford, its columns
 // padded per part: part q's boundary columns start at bd_col, a multiple of
-// 4): grid (boundary-index tiles, column tiles, parts); A boxes from dB,
+// 4): grid (column tiles, boundary-index tiles, parts); A boxes from dB,
 // B boxes from the F arena (nparts_f squares of side ldf).  A stage that
 // never completes sets kDevTmaTimeout in status.
 template <typename T>
