@@ -228,7 +228,10 @@ struct fap_dgraph {
   // least 6 arcs per vertex, where few Bellman-Ford iterations suffice), 1
   // frontier kernel, 2 tiled.  Work items over the in-edge CSR.
   int sssp_form = 0;
-  int64_t tile_bytes = int64_t(96) << 20;  // memory for tiles side by side (tiled SSSP, Bellman-Ford closure)
+  // memory for tiles side by side (tiled SSSP, Bellman-Ford closure): more
+  // than L2 holds, since an iteration touches only its changed rows, and
+  // fewer groups of tiles mean fewer launches and convergence read-backs
+  int64_t tile_bytes = int64_t(384) << 20;
   DevBuf d_msbf_items, d_msbf_act, d_msbf_changed;
   int msbf_nitems = 0;
   int *h_changed = nullptr;  // pinned, 4 ints
@@ -609,8 +612,8 @@ bool bmethod_ok(const fap_dgraph *G) {
          (G->bgraph_edges <= kBgraphEdgeRatio * G->m && G->total_b <= kBgraphAutoMaxB);
 }
 
-// Tiles of the Bellman-Ford closure run side by side: as many as keep the
-// tiles within 96 MB (L2 holds them), at most 16.
+// Tiles of the Bellman-Ford closure run side by side: as many as fit in
+// tile_bytes, at most 16.
 int bgraph_ztiles(const fap_dgraph *G) {
   const int64_t per = std::max<int64_t>(G->total_b, 1) * kMsbfS * 4;
   const int64_t tiles = ceil_div(std::max<int64_t>(G->total_b, 1), kMsbfS);
@@ -917,8 +920,8 @@ const char *stage1_form_name(const fap_dgraph *G, bool bmethod) {
   return use_msbf(G) ? "SSSP, tiled Bellman-Ford" : "SSSP, frontier";
 }
 
-// Tiles of the tiled SSSP form run side by side: as many as keep them within
-// 96 MB (L2 holds them), at most 16.
+// Tiles of the tiled SSSP form run side by side: as many as fit in
+// tile_bytes, at most 16.
 int msbf_ztiles(const fap_dgraph *G, int count) {
   const int64_t per = std::max<int64_t>(G->n, 1) * kMsbfS * 4;
   return (int)std::max<int64_t>(1, std::min<int64_t>({G->tile_bytes / per, 16, ceil_div(count, kMsbfS)}));

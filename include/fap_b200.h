@@ -163,7 +163,7 @@ FAP_API int fap_graph_sssp_rows(fap_dgraph *g, const int32_t *sources, int32_t c
  * checks convergence on the host, so a solve that uses it is not captured
  * in a CUDA graph); "tile_mb" (device memory for the 128-source tiles that
  * the tiled SSSP and the Bellman-Ford closure of the boundary graph run side
- * by side, at most 16 of them, at least one; default 96, which L2 holds). */
+ * by side, at most 16 of them, at least one; default 384). */
 FAP_API int fap_graph_set_param(fap_dgraph *g, const char *key, double value);
 
 /* Tunes the SSSP bucket width: runs the SSSP stage on `sample` boundary
