@@ -1,0 +1,74 @@
+"""Host-side pieces of bench.py that need no GPU: the clock sampler keeps
+only the samples taken inside the timed region (and reports throttle
+reasons seen there), and the default run keeps at least 3 warm-up steps."""
+import datetime
+import importlib.util
+import os
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _bench():
+    spec = importlib.util.spec_from_file_location("bench_under_test", os.path.join(ROOT, "bench.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+class _Done:
+    def terminate(self):
+        pass
+
+    def wait(self, timeout=None):
+        pass
+
+    def kill(self):
+        pass
+
+
+def _sample_line(t, sm, power_cap):
+    ts = datetime.datetime.fromtimestamp(t).strftime("%Y/%m/%d %H:%M:%S.%f")[:-3]
+    cap = "Active" if power_cap else "Not Active"
+    return (f"0, {sm}, 1965, 600.0, 0x0, Not Active, Not Active, Not Active, {cap}, {ts}\n")
+
+
+def test_clock_samples_are_kept_to_the_timed_region():
+    b = _bench()
+    c = b.ClockSampler(0)
+    fd, c.path = tempfile.mkstemp(suffix=".csv")
+    os.close(fd)
+    now = time.time()
+    with open(c.path, "w") as f:
+        f.write(_sample_line(now - 2.0, 900, True))     # before: throttled, not counted
+        f.write(_sample_line(now + 0.10, 1965, False))
+        f.write(_sample_line(now + 0.20, 1950, False))
+        f.write(_sample_line(now + 9.0, 600, True))      # after: not counted
+    c.proc = _Done()
+    c.mark(now, now + 0.5)
+    out = c.stop()
+    assert out["samples"] == 2 and out["window"] == "timed region"
+    assert out["sm_mhz"] == 1957.5 and out["sm_max_mhz"] == 1965.0
+    assert out["reasons"] == []
+
+
+def test_clock_samples_without_a_window_use_every_line():
+    b = _bench()
+    c = b.ClockSampler(0)
+    fd, c.path = tempfile.mkstemp(suffix=".csv")
+    os.close(fd)
+    now = time.time()
+    with open(c.path, "w") as f:
+        f.write(_sample_line(now, 1800, True))
+    c.proc = _Done()
+    out = c.stop()
+    assert out["samples"] == 1 and out["reasons"] == ["sw_power_cap"]
+
+
+def test_default_run_has_three_warmup_steps(monkeypatch):
+    b = _bench()
+    monkeypatch.setattr(sys, "argv", ["bench.py"])
+    args = b.parse_args()
+    assert args.warmup >= 3 and args.steps >= 1 and args.gpus == 1
