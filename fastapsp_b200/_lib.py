@@ -121,6 +121,9 @@ _SIGS = {
     "fap_host_last_error": (ctypes.c_char_p, []),
     "fap_host_from_mtx": (INT, [ctypes.c_char_p, INT, INT, INT, PP]),
     "fap_host_from_csr": (INT, [I32, I64, P, P, P, INT, INT, PP]),
+    "fap_host_save": (INT, [P, ctypes.c_char_p]),
+    "fap_host_load": (INT, [ctypes.c_char_p, PP]),
+    "fap_host_flags": (INT, [P, P, P]),
     "fap_host_destroy": (INT, [P]),
     "fap_host_set_partition": (INT, [P, P]),
     "fap_host_set_options": (INT, [P, INT, INT, INT]),

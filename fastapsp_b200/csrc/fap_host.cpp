@@ -12,6 +12,7 @@
 #include "fap/fap.h"
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -255,6 +256,116 @@ void fapGraph::setPartition(const std::vector<int32_t> &gid) {
   for (int i = 0; i < num_vertexs; i++) BlockVer[graph_id[i]].push_back(i);
   partition_injected_ = true;
   prepared_ = false;
+}
+
+// ---------------------------------------------------------------------------
+// Binary graph file: magic, sizes, CSR, partition, FNV-1a 64 checksum of
+// everything before it.  Little-endian, as written by this library.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr char kBinMagic[8] = {'F', 'A', 'P', 'C', 'S', 'R', '0', '1'};
+
+struct BinHeader {
+  char magic[8];
+  int32_t n;
+  int32_t K;
+  int64_t m_decl;  // the declared edge count (num_edges)
+  int64_t nnz;     // row_offset[n]
+  int32_t directed;
+  int32_t weighted;
+};
+
+uint64_t fnv1a(uint64_t h, const void *p, size_t len) {
+  const unsigned char *b = static_cast<const unsigned char *>(p);
+  for (size_t i = 0; i < len; i++) {
+    h ^= b[i];
+    h *= 1099511628211ull;
+  }
+  return h;
+}
+}  // namespace
+
+void fapGraph::saveBinary(const std::string &path) const {
+  BinHeader h{};
+  std::memcpy(h.magic, kBinMagic, 8);
+  h.n = num_vertexs;
+  h.K = K;
+  h.m_decl = num_edges;
+  h.nnz = row_offset.empty() ? 0 : row_offset[num_vertexs];
+  h.directed = directed ? 1 : 0;
+  h.weighted = weighted ? 1 : 0;
+  std::ofstream f(path, std::ios::binary | std::ios::trunc);
+  if (!f) raise(FAP_ERR_IO, "cannot write " + path);
+  uint64_t sum = 14695981039346656037ull;
+  auto put = [&](const void *p, size_t len) {
+    f.write(static_cast<const char *>(p), (std::streamsize)len);
+    sum = fnv1a(sum, p, len);
+  };
+  put(&h, sizeof(h));
+  put(row_offset.data(), ((size_t)num_vertexs + 1) * 4);
+  put(col_val.data(), (size_t)h.nnz * 4);
+  put(weight.data(), (size_t)h.nnz * 4);
+  put(graph_id.data(), (size_t)num_vertexs * 4);
+  f.write(reinterpret_cast<const char *>(&sum), sizeof(sum));
+  if (!f) raise(FAP_ERR_IO, "write failed: " + path);
+}
+
+std::unique_ptr<fapGraph> fapGraph::loadBinary(const std::string &path) {
+  std::ifstream f(path, std::ios::binary | std::ios::ate);
+  if (!f) raise(FAP_ERR_IO, "cannot read " + path);
+  const int64_t size = (int64_t)f.tellg();
+  f.seekg(0);
+  BinHeader h{};
+  if (size < (int64_t)sizeof(h) || !f.read(reinterpret_cast<char *>(&h), sizeof(h)) ||
+      std::memcmp(h.magic, kBinMagic, 8) != 0)
+    raise(FAP_ERR_IO, path + ": not a binary graph file");
+  if (h.n <= 0 || h.K < 1 || h.K > h.n || h.nnz < 0 || h.nnz > INT32_MAX || h.m_decl < h.nnz)
+    raise(FAP_ERR_IO, path + ": bad sizes");
+  const int64_t want = (int64_t)sizeof(h) + ((int64_t)h.n + 1) * 4 + 2 * h.nnz * 4 + (int64_t)h.n * 4 + 8;
+  if (size != want) raise(FAP_ERR_IO, path + ": truncated or oversized");
+  uint64_t sum = fnv1a(14695981039346656037ull, &h, sizeof(h));
+  auto get = [&](void *p, size_t len) {
+    if (!f.read(static_cast<char *>(p), (std::streamsize)len)) raise(FAP_ERR_IO, path + ": short read");
+    sum = fnv1a(sum, p, len);
+  };
+  std::vector<int32_t> ro((size_t)h.n + 1), cv((size_t)h.nnz), gid((size_t)h.n);
+  std::vector<float> w((size_t)h.nnz);
+  get(ro.data(), ro.size() * 4);
+  get(cv.data(), cv.size() * 4);
+  get(w.data(), w.size() * 4);
+  get(gid.data(), gid.size() * 4);
+  uint64_t stored = 0;
+  if (!f.read(reinterpret_cast<char *>(&stored), sizeof(stored)) || stored != sum)
+    raise(FAP_ERR_IO, path + ": checksum mismatch");
+  if (ro[0] != 0 || ro[h.n] != h.nnz) raise(FAP_ERR_IO, path + ": inconsistent CSR");
+  for (int32_t v = 0; v < h.n; v++)
+    if (ro[v + 1] < ro[v]) raise(FAP_ERR_IO, path + ": row_offset not monotone");
+  for (int32_t c : cv)
+    if (c < 0 || c >= h.n) raise(FAP_ERR_IO, path + ": col_val out of range");
+  for (int32_t p : gid)
+    if (p < 1 || p > h.K) raise(FAP_ERR_IO, path + ": part id outside 1..K");
+  return std::unique_ptr<fapGraph>(new fapGraph(LoadedTag{}, h.n, h.m_decl, std::move(ro), std::move(cv),
+                                                std::move(w), h.K, h.directed != 0, h.weighted != 0,
+                                                std::move(gid)));
+}
+
+fapGraph::fapGraph(LoadedTag, int32_t n, int64_t m, std::vector<int32_t> ro, std::vector<int32_t> cv,
+                   std::vector<float> w, int32_t K, bool directed, bool weighted, std::vector<int32_t> gid) {
+  num_vertexs = n;
+  num_edges = (int32_t)m;
+  this->K = K;
+  this->directed = directed;
+  this->weighted = weighted;
+  row_offset = std::move(ro);
+  col_val = std::move(cv);
+  weight = std::move(w);
+  col_val.resize(std::max<int64_t>(m, row_offset[n]), 0);
+  weight.resize(std::max<int64_t>(m, row_offset[n]), 0.0f);
+  adj_size.assign(n, 0);
+  for (int32_t v = 0; v < n; v++) adj_size[v] = row_offset[v + 1] - row_offset[v];
+  init_storage();
+  graph_id.assign(gid.begin(), gid.end());
+  for (int i = 0; i < num_vertexs; i++) BlockVer[graph_id[i]].push_back(i);
 }
 
 void fapGraph::setDevice(int device) { device_ = device; }
@@ -563,6 +674,16 @@ int fap_host_from_csr(int32_t n, int64_t m, const int32_t *ro, const int32_t *co
   })
 }
 
+int fap_host_save(fap::fapGraph *g, const char *path) {
+  if (!g || !path) return FAP_ERR_INVALID;
+  FAPH_BODY(g->saveBinary(path))
+}
+
+int fap_host_load(const char *path, fap::fapGraph **out) {
+  if (!path || !out) return FAP_ERR_INVALID;
+  FAPH_BODY(*out = fap::fapGraph::loadBinary(path).release())
+}
+
 int fap_host_destroy(fap::fapGraph *g) {
   delete g;
   return FAP_OK;
@@ -593,6 +714,13 @@ int fap_host_dtype(fap::fapGraph *g) {
 }
 
 // sizes: [n, m_decl, K, stored arcs]
+int fap_host_flags(fap::fapGraph *g, int *directed, int *weighted) {
+  if (!g || !directed || !weighted) return FAP_ERR_INVALID;
+  *directed = g->directed ? 1 : 0;
+  *weighted = g->weighted ? 1 : 0;
+  return FAP_OK;
+}
+
 int fap_host_sizes(fap::fapGraph *g, int64_t *out4) {
   out4[0] = g->num_vertexs;
   out4[1] = g->num_edges;

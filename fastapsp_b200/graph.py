@@ -77,6 +77,20 @@ class fapGraph:
         self._dtype = L.FAP_DTYPE_AUTO
         self._device = 0
 
+    def save(self, path: str) -> None:
+        """Writes the graph and its partition to a binary file (fap_host_save)."""
+        check(lib().fap_host_save(self._h, str(path).encode()), "fapGraph.save")
+
+    @classmethod
+    def load(cls, path: str) -> "fapGraph":
+        """Rebuilds a graph saved by save() without text parsing or METIS;
+        call preCondition() next (fap_host_load)."""
+        h = ctypes.c_void_p()
+        check(lib().fap_host_load(str(path).encode(), ctypes.byref(h)), "fapGraph.load")
+        d, w = ctypes.c_int(), ctypes.c_int()
+        check(lib().fap_host_flags(h, ctypes.byref(d), ctypes.byref(w)), "fapGraph.load")
+        return cls(_handle=h, directed=bool(d.value), weighted=bool(w.value))
+
     @classmethod
     def from_csr(cls, num_vertexs: int, num_edges: int, row_offset, col_val, weight, K: int,
                  directed: bool = False) -> "fapGraph":

@@ -22,6 +22,7 @@
 
 #include <sstream>
 #include <stdexcept>
+#include <memory>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -72,6 +73,9 @@ class __attribute__((visibility("default"))) fapGraph {
   int32_t max_subgraph_vertexs = 0;
 
  private:
+  struct LoadedTag {};
+  fapGraph(LoadedTag, int32_t n, int64_t m, std::vector<int32_t> ro, std::vector<int32_t> cv,
+           std::vector<float> w, int32_t K, bool directed, bool weighted, std::vector<int32_t> gid);
   // GPU state
   fap_ctx *ctx_ = nullptr;
   fap_dgraph *dg_ = nullptr;
@@ -111,6 +115,13 @@ class __attribute__((visibility("default"))) fapGraph {
   fapGraph(int32_t num_vertexs, int64_t num_edges, std::vector<int32_t> row_offset,
            std::vector<int32_t> col_val, std::vector<float> weight, int32_t K, bool directed);
   ~fapGraph();
+  // Binary graph file (CSR + partition): saveBinary writes what the
+  // constructor built (the graph and its METIS or injected partition);
+  // loadBinary rebuilds the graph without parsing text or running METIS,
+  // ready for preCondition.  A checksum guards the file; a bad file raises
+  // fapError (FAP_ERR_IO).
+  void saveBinary(const std::string &path) const;
+  static std::unique_ptr<fapGraph> loadBinary(const std::string &path);
   fapGraph(const fapGraph &) = delete;
   fapGraph &operator=(const fapGraph &) = delete;
 

@@ -39,6 +39,13 @@ FAP_API const char *fap_host_last_error(void);
 FAP_API int fap_host_from_mtx(const char *name, int directed, int weighted, int K, fap_host_graph **out);
 FAP_API int fap_host_from_csr(int32_t n, int64_t m, const int32_t *row_offset, const int32_t *col_val,
                               const float *weight, int K, int directed, fap_host_graph **out);
+/* Binary graph file (CSR + partition; no counterpart in the reference, which
+ * re-reads the text file and re-runs METIS every time): fap_host_save
+ * writes the graph as constructed (before or after preCondition);
+ * fap_host_load rebuilds it without text parsing or METIS, ready for
+ * fap_host_precondition.  A checksum guards the file (FAP_ERR_IO). */
+FAP_API int fap_host_save(fap_host_graph *g, const char *path);
+FAP_API int fap_host_load(const char *path, fap_host_graph **out);
 FAP_API int fap_host_destroy(fap_host_graph *g);
 /* 1-based part id per vertex; replaces the METIS result (before precondition). */
 FAP_API int fap_host_set_partition(fap_host_graph *g, const int32_t *graph_id);
@@ -47,6 +54,8 @@ FAP_API int fap_host_set_options(fap_host_graph *g, int device, int dtype, int m
 FAP_API int fap_host_precondition(fap_host_graph *g);
 FAP_API int fap_host_is_split(fap_host_graph *g);
 FAP_API int fap_host_dtype(fap_host_graph *g);
+/* The graph's directed / weighted flags (as given or as loaded). */
+FAP_API int fap_host_flags(fap_host_graph *g, int *directed, int *weighted);
 /* out4 = [n, num_edges (declared arcs), K, stored arcs] */
 FAP_API int fap_host_sizes(fap_host_graph *g, int64_t *out4);
 /* row_offset[n+1], col_val[stored], weight[stored] */

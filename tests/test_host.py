@@ -98,3 +98,43 @@ def test_solve_before_precondition_is_an_error():
         with pytest.raises(FapError) as e:
             g.solveSubGraph(1)
         assert e.value.code == L.FAP_ERR_STATE
+
+
+@pytest.mark.parametrize("name", ["grid12_k4", "road300_k6", "rmat8_f32_k4", "disconnected_k3"])
+def test_binary_file_round_trip(name):
+    """save() then load(): the same CSR, partition and, after preCondition,
+    the same renumbering and part counts as the reference's, without text
+    parsing or METIS; flags and sizes kept."""
+    case = load_golden(name)
+    with tempfile.TemporaryDirectory() as tmp:
+        g = _host_graph(case, tmp)
+        path = os.path.join(tmp, "g.fapb")
+        g.save(path)
+        h = fapGraph.load(path)
+        assert (h.directed, h.weighted) == (bool(case["directed"]), bool(case["weighted"]))
+        assert (h.num_vertexs, h.num_edges) == (g.num_vertexs, g.num_edges)
+        h.preCondition()
+        for a, b in zip(h.csr(), g.csr()):
+            np.testing.assert_array_equal(a, b)
+        np.testing.assert_array_equal(h.getGraphId(), case["graph_id"])
+        np.testing.assert_array_equal(h.getMapping(), case["st2ed"])
+        for a, b in zip(h.partInfo(), g.partInfo()):
+            np.testing.assert_array_equal(a, b)
+
+
+def test_binary_file_damage_is_an_io_error():
+    case = load_golden("grid12_k4")
+    with tempfile.TemporaryDirectory() as tmp:
+        g = _host_graph(case, tmp)
+        path = os.path.join(tmp, "g.fapb")
+        g.save(path)
+        raw = bytearray(open(path, "rb").read())
+        for damaged in (raw[:-9], raw[:40] + bytes([raw[40] ^ 1]) + raw[41:], b"NOTAFAPB" + raw[8:]):
+            with open(path, "wb") as f:
+                f.write(bytes(damaged))
+            with pytest.raises(FapError) as e:
+                fapGraph.load(path)
+            assert e.value.code == L.FAP_ERR_IO
+        with pytest.raises(FapError) as e:
+            fapGraph.load(os.path.join(tmp, "missing.fapb"))
+        assert e.value.code == L.FAP_ERR_IO
