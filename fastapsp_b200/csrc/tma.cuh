@@ -1,5 +1,5 @@
 // Tensor Memory Accelerator (TMA) helpers for sm_100a: mbarrier wrappers,
-// tiled bulk tensor loads into shared memory (no multicast), and a bounded
+// tiled bulk tensor loads into each CTA's own shared memory, and a bounded
 // wait that reports a timeout instead of spinning forever.
 #pragma once
 
@@ -64,8 +64,8 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
 }
 
 // 3-D tiled load of one box into shared memory; completion is counted on
-// `bar` in bytes.  The destination is this CTA's own shared memory; no
-// multicast.  The innermost coordinate x must be a multiple of 4 (16 bytes of
+// `bar` in bytes.  The destination is this CTA's own shared memory only.
+// The innermost coordinate x must be a multiple of 4 (16 bytes of
 // 32-bit elements): callers only pass multiples of their 16-element chunks.
 __device__ __forceinline__ void tma_load_3d(void *smem_dst, const CUtensorMap *map, int x, int y, int z,
                                             uint64_t *bar) {
