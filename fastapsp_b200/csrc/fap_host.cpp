@@ -319,7 +319,8 @@ std::unique_ptr<fapGraph> fapGraph::loadBinary(const std::string &path) {
   if (size < (int64_t)sizeof(h) || !f.read(reinterpret_cast<char *>(&h), sizeof(h)) ||
       std::memcmp(h.magic, kBinMagic, 8) != 0)
     raise(FAP_ERR_IO, path + ": not a binary graph file");
-  if (h.n <= 0 || h.K < 1 || h.K > h.n || h.nnz < 0 || h.nnz > INT32_MAX || h.m_decl < h.nnz)
+  if (h.n <= 0 || h.K < 1 || h.K > h.n || h.nnz < 0 || h.nnz > INT32_MAX || h.m_decl < h.nnz ||
+      h.m_decl > INT32_MAX)
     raise(FAP_ERR_IO, path + ": bad sizes");
   const int64_t want = (int64_t)sizeof(h) + ((int64_t)h.n + 1) * 4 + 2 * h.nnz * 4 + (int64_t)h.n * 4 + 8;
   if (size != want) raise(FAP_ERR_IO, path + ": truncated or oversized");

@@ -138,3 +138,42 @@ def test_binary_file_damage_is_an_io_error():
         with pytest.raises(FapError) as e:
             fapGraph.load(os.path.join(tmp, "missing.fapb"))
         assert e.value.code == L.FAP_ERR_IO
+
+
+def _fnv1a64(data):
+    h = 14695981039346656037
+    for b in data:
+        h = ((h ^ b) * 1099511628211) & 0xFFFFFFFFFFFFFFFF
+    return h
+
+
+def test_binary_file_with_valid_checksum_but_bad_contents_is_an_io_error():
+    """Files that pass the checksum are still checked: a declared edge
+    count beyond int32 (no huge allocation), a column id past n, a part id
+    past K."""
+    case = load_golden("grid12_k4")
+    with tempfile.TemporaryDirectory() as tmp:
+        g = _host_graph(case, tmp)
+        path = os.path.join(tmp, "g.fapb")
+        g.save(path)
+        raw = bytearray(open(path, "rb").read())
+        n = int.from_bytes(raw[8:12], "little")
+        nnz = int.from_bytes(raw[24:32], "little")
+        cv_at = 40 + (n + 1) * 4
+        gid_at = cv_at + 2 * nnz * 4
+        edits = [(16, (1 << 40).to_bytes(8, "little")),        # m_decl
+                 (cv_at, n.to_bytes(4, "little")),             # col_val[0] = n
+                 (gid_at, (1000).to_bytes(4, "little"))]       # graph_id[0] > K
+        for at, val in edits:
+            body = bytearray(raw[:-8])
+            body[at:at + len(val)] = val
+            with open(path, "wb") as f:
+                f.write(bytes(body) + _fnv1a64(body).to_bytes(8, "little"))
+            with pytest.raises(FapError) as e:
+                fapGraph.load(path)
+            assert e.value.code == L.FAP_ERR_IO
+        # the unedited body with its recomputed checksum still loads
+        body = bytes(raw[:-8])
+        with open(path, "wb") as f:
+            f.write(body + _fnv1a64(body).to_bytes(8, "little"))
+        assert fapGraph.load(path).num_vertexs == n
