@@ -486,6 +486,18 @@ extern "C" int fap_graph_set_parts(fap_dgraph *G, int32_t K, const int32_t *grap
     off += ver_num[p];
   }
   if (off != n) return fail(FAP_ERR_PARTITION, "part sizes sum to %lld, not n", (long long)off);
+  // Both ends of every cross-part arc are boundary vertices
+  // (fap/utils/util_preprocess.h:32-59), i.e. sit in the first bdy_num[p]
+  // places of their part's block; every stage relies on it.
+  for (int32_t u = 0; u < n; u++)
+    for (int32_t e = G->h_ro[u]; e < G->h_ro[u + 1]; e++) {
+      const int32_t v = G->h_col[e];
+      const int32_t pu = graph_id[u], pv = graph_id[v];
+      if (pu == pv) continue;
+      if (ed2st[u] - ver_offset[pu] >= bdy_num[pu] || ed2st[v] - ver_offset[pv] >= bdy_num[pv])
+        return fail(FAP_ERR_PARTITION, "arc %d->%d crosses parts but an end is not in its part's boundary block",
+                    u, v);
+    }
   DeviceGuard g(G->ctx->device);
   G->K = K;
   G->gid.assign(graph_id, graph_id + n);

@@ -98,7 +98,10 @@ FAP_API int fap_graph_dtype(const fap_dgraph *g);
  *   graph_id[n]  1-based part of every vertex,
  *   st2ed[n]     vertex at each sorted position,
  *   ver_num[K+1], ver_offset[K+1], bdy_num[K+1]  per part, index 1..K.
- * Checks that they are consistent.  Host pointers. */
+ * Checks that they are consistent: st2ed a permutation, each part's block
+ * holding only its own vertices, and both ends of every cross-part arc in
+ * the first bdy_num[p] places of their part's block (FAP_ERR_PARTITION
+ * otherwise).  Host pointers. */
 FAP_API int fap_graph_set_parts(fap_dgraph *g, int32_t K, const int32_t *graph_id,
                         const int32_t *st2ed, const int32_t *ver_num,
                         const int32_t *ver_offset, const int32_t *bdy_num);

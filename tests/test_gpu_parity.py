@@ -178,6 +178,27 @@ def test_sssp_round_bound_reports_error_and_context_survives(cuda_ok):
     np.testing.assert_array_equal(cs, case["row_checksums"])
 
 
+def test_partition_with_a_cross_arc_end_outside_the_boundary_block_is_refused(cuda_ok):
+    """A part's last boundary vertex counted as inner (bdy_num one short):
+    set_parts refuses it before any device work, and the true partition is
+    accepted on the same graph afterwards."""
+    case = load_golden("grid12_k4")
+    ctx = Context(0)
+    ro, col, w = case["row_offset"], case["col_val"], case["weight"]
+    dg = DeviceGraph(ctx, ro, col[:ro[-1]], w[:ro[-1]])
+    bn = np.array(case["bdy_num"], copy=True)
+    p = int(np.argmax(bn[1:])) + 1
+    bn[p] -= 1
+    with pytest.raises(FapError) as e:
+        dg.set_parts(case["K"], case["graph_id"], case["st2ed"], case["ver_num"], case["ver_offset"], bn)
+    assert e.value.code == L.FAP_ERR_PARTITION
+    dg.set_parts(case["K"], case["graph_id"], case["st2ed"], case["ver_num"], case["ver_offset"],
+                 case["bdy_num"])
+    dg.solve(mode=FAP_MODE_BATCHED)
+    cs = np.concatenate([dg.block_checksums(p) for p in range(1, case["K"] + 1)])
+    np.testing.assert_array_equal(cs, case["row_checksums"])
+
+
 def test_sssp_delta_stepping_same_result(cuda_ok):
     case = load_golden("road300_k6")
     ctx = Context(0)
