@@ -9,6 +9,8 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <exception>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -30,6 +32,20 @@ int fail(int code, const char *fmt, ...) {
   va_end(ap);
   g_err = buf;
   return code;
+}
+
+// No C++ exception leaves an entry point of the C ABI: the host-side
+// std::vector / std::string allocations turn into FAP_ERR_NOMEM.
+int fail_exception() {
+  try {
+    throw;
+  } catch (const std::bad_alloc &) {
+    return fail(FAP_ERR_NOMEM, "host allocation failed");
+  } catch (const std::exception &e) {
+    return fail(FAP_ERR_INVALID, "%s", e.what());
+  } catch (...) {
+    return fail(FAP_ERR_INVALID, "unknown C++ exception");
+  }
 }
 
 #define FAP_CK(call)                                                                     \
@@ -262,7 +278,7 @@ extern "C" int fap_version(void) { return 0x000100; }
 // ---------------------------------------------------------------------------
 // context
 // ---------------------------------------------------------------------------
-extern "C" int fap_ctx_create(int device, fap_ctx **out) {
+extern "C" int fap_ctx_create(int device, fap_ctx **out) try {
   if (!out) return fail(FAP_ERR_INVALID, "fap_ctx_create: out is NULL");
   *out = nullptr;
   int count = 0;
@@ -298,6 +314,8 @@ extern "C" int fap_ctx_create(int device, fap_ctx **out) {
   }
   *out = c;
   return FAP_OK;
+} catch (...) {
+  return fail_exception();
 }
 
 namespace {
@@ -317,7 +335,7 @@ void ctx_release(fap_ctx *c) {
 // A context outlives its graphs: with graphs still alive the release is
 // deferred until the last of them is destroyed, so callers (and garbage
 // collectors) may destroy the two in either order.
-extern "C" int fap_ctx_destroy(fap_ctx *c) {
+extern "C" int fap_ctx_destroy(fap_ctx *c) try {
   if (!c) return FAP_OK;
   if (c->graphs > 0) {
     c->destroy_pending = true;
@@ -325,25 +343,33 @@ extern "C" int fap_ctx_destroy(fap_ctx *c) {
   }
   ctx_release(c);
   return FAP_OK;
+} catch (...) {
+  return fail_exception();
 }
 
-extern "C" int fap_ctx_set_stream(fap_ctx *c, void *stream) {
+extern "C" int fap_ctx_set_stream(fap_ctx *c, void *stream) try {
   if (!c) return fail(FAP_ERR_INVALID, "ctx is NULL");
   c->stream = stream ? reinterpret_cast<cudaStream_t>(stream) : c->own;
   return FAP_OK;
+} catch (...) {
+  return fail_exception();
 }
 
-extern "C" int fap_ctx_get_stream(fap_ctx *c, void **stream) {
+extern "C" int fap_ctx_get_stream(fap_ctx *c, void **stream) try {
   if (!c || !stream) return fail(FAP_ERR_INVALID, "NULL argument");
   *stream = reinterpret_cast<void *>(c->stream);
   return FAP_OK;
+} catch (...) {
+  return fail_exception();
 }
 
-extern "C" int fap_ctx_sync(fap_ctx *c) {
+extern "C" int fap_ctx_sync(fap_ctx *c) try {
   if (!c) return fail(FAP_ERR_INVALID, "ctx is NULL");
   DeviceGuard g(c->device);
   FAP_CK(cudaStreamSynchronize(c->stream));
   return FAP_OK;
+} catch (...) {
+  return fail_exception();
 }
 
 // ---------------------------------------------------------------------------
@@ -351,7 +377,7 @@ extern "C" int fap_ctx_sync(fap_ctx *c) {
 // ---------------------------------------------------------------------------
 extern "C" int fap_graph_create(fap_ctx *ctx, int32_t n, int64_t m, const int32_t *row_offset,
                                 const int32_t *col_val, const float *weight, int dtype,
-                                fap_dgraph **out) {
+                                fap_dgraph **out) try {
   if (!ctx || !out) return fail(FAP_ERR_INVALID, "NULL argument");
   *out = nullptr;
   if (n <= 0) return fail(FAP_ERR_INVALID, "n must be positive (got %d)", n);
@@ -418,6 +444,8 @@ extern "C" int fap_graph_create(fap_ctx *ctx, int32_t n, int64_t m, const int32_
   cudaMemset(G->d_status.p, 0, sizeof(int));
   *out = G;
   return FAP_OK;
+} catch (...) {
+  return fail_exception();
 }
 
 namespace {
@@ -433,7 +461,7 @@ void cache_drop(fap_dgraph *G) {
 }
 }  // namespace
 
-extern "C" int fap_graph_destroy(fap_dgraph *G) {
+extern "C" int fap_graph_destroy(fap_dgraph *G) try {
   if (!G) return FAP_OK;
   fap_ctx *c = G->ctx;
   {
@@ -457,13 +485,15 @@ extern "C" int fap_graph_destroy(fap_dgraph *G) {
   c->graphs--;
   if (c->destroy_pending && c->graphs == 0) ctx_release(c);
   return FAP_OK;
+} catch (...) {
+  return fail_exception();
 }
 
 extern "C" int fap_graph_dtype(const fap_dgraph *G) { return G ? G->dtype : FAP_ERR_INVALID; }
 
 extern "C" int fap_graph_set_parts(fap_dgraph *G, int32_t K, const int32_t *graph_id,
                                    const int32_t *st2ed, const int32_t *ver_num,
-                                   const int32_t *ver_offset, const int32_t *bdy_num) {
+                                   const int32_t *ver_offset, const int32_t *bdy_num) try {
   if (!G || !graph_id || !st2ed || !ver_num || !ver_offset || !bdy_num)
     return fail(FAP_ERR_INVALID, "NULL argument");
   const int32_t n = G->n;
@@ -566,9 +596,11 @@ extern "C" int fap_graph_set_parts(fap_dgraph *G, int32_t K, const int32_t *grap
   FAP_CK(cudaMemcpy(G->col_s.p, col_s.data(), col_s.size() * 4, cudaMemcpyHostToDevice));
   FAP_CK(cudaMemcpy(G->w_s.p, w_s.data(), w_s.size() * 4, cudaMemcpyHostToDevice));
   return FAP_OK;
+} catch (...) {
+  return fail_exception();
 }
 
-extern "C" int fap_graph_reserve(fap_dgraph *G, int64_t max_rows) {
+extern "C" int fap_graph_reserve(fap_dgraph *G, int64_t max_rows) try {
   if (!G) return fail(FAP_ERR_INVALID, "NULL graph");
   if (max_rows <= 0 || max_rows > G->n) max_rows = G->n;
   DeviceGuard g(G->ctx->device);
@@ -587,6 +619,8 @@ extern "C" int fap_graph_reserve(fap_dgraph *G, int64_t max_rows) {
   G->last_ids.clear();
   G->epoch++;
   return FAP_OK;
+} catch (...) {
+  return fail_exception();
 }
 
 namespace {
@@ -1106,7 +1140,7 @@ int read_status(fap_dgraph *G) {
 
 }  // namespace
 
-extern "C" int fap_solve(fap_dgraph *G, const int32_t *parts, int32_t count, int mode) {
+extern "C" int fap_solve(fap_dgraph *G, const int32_t *parts, int32_t count, int mode) try {
   if (!G) return fail(FAP_ERR_INVALID, "NULL graph");
   if (G->K == 0) return fail(FAP_ERR_STATE, "fap_solve before fap_graph_set_parts");
   if (mode != FAP_MODE_PLAIN && mode != FAP_MODE_BATCHED) return fail(FAP_ERR_INVALID, "bad mode %d", mode);
@@ -1179,17 +1213,21 @@ extern "C" int fap_solve(fap_dgraph *G, const int32_t *parts, int32_t count, int
     for (const PartDesc &d : G->parts) G->path_ok[d.part] = 1;
   G->last_mode = mode;
   return FAP_OK;
+} catch (...) {
+  return fail_exception();
 }
 
-extern "C" int fap_graph_check(fap_dgraph *G) {
+extern "C" int fap_graph_check(fap_dgraph *G) try {
   if (!G) return fail(FAP_ERR_INVALID, "NULL graph");
   DeviceGuard g(G->ctx->device);
   FAP_CK(cudaStreamSynchronize(G->ctx->stream));
   FAP_TRY(read_status(G));
   return FAP_OK;
+} catch (...) {
+  return fail_exception();
 }
 
-extern "C" int fap_graph_last_timing(fap_dgraph *G, float *ms5) {
+extern "C" int fap_graph_last_timing(fap_dgraph *G, float *ms5) try {
   if (!G || !ms5) return fail(FAP_ERR_INVALID, "NULL argument");
   for (int i = 0; i < 5; i++) ms5[i] = -1.0f;
   if (G->last_mode < 0) return fail(FAP_ERR_STATE, "no solve yet");
@@ -1216,13 +1254,17 @@ extern "C" int fap_graph_last_timing(fap_dgraph *G, float *ms5) {
   }
   for (int i = 0; i < 5; i++) G->timing[i] = ms5[i];
   return FAP_OK;
+} catch (...) {
+  return fail_exception();
 }
 
-extern "C" int fap_graph_last_stage1(const fap_dgraph *G) {
+extern "C" int fap_graph_last_stage1(const fap_dgraph *G) try {
   if (!G) return fail(FAP_ERR_INVALID, "NULL graph");
   if (G->last_mode < 0) return 0;
   if (G->last_cached) return 3;
   return G->last_bmethod ? 2 : 1;
+} catch (...) {
+  return fail_exception();
 }
 
 extern "C" const char *fap_graph_stage1_name(const fap_dgraph *G) {
@@ -1233,14 +1275,16 @@ extern "C" const char *fap_graph_stage1_name(const fap_dgraph *G) {
   return G->stage1_name.c_str();
 }
 
-extern "C" int fap_graph_last_launches(fap_dgraph *G, int64_t *count) {
+extern "C" int fap_graph_last_launches(fap_dgraph *G, int64_t *count) try {
   if (!G || !count) return fail(FAP_ERR_INVALID, "NULL argument");
   *count = G->launches;
   return FAP_OK;
+} catch (...) {
+  return fail_exception();
 }
 
 extern "C" int fap_graph_block(fap_dgraph *G, int32_t part, void **dev_ptr, int64_t *rows,
-                               int64_t *ld) {
+                               int64_t *ld) try {
   if (!G || !dev_ptr || !rows || !ld) return fail(FAP_ERR_INVALID, "NULL argument");
   if (part < 1 || part > G->K) return fail(FAP_ERR_INVALID, "part %d outside 1..%d", part, G->K);
   if (G->row_base[part] < 0) return fail(FAP_ERR_STATE, "part %d is not resident", part);
@@ -1248,9 +1292,11 @@ extern "C" int fap_graph_block(fap_dgraph *G, int32_t part, void **dev_ptr, int6
   *rows = G->vnum[part];
   *ld = G->ldD;
   return FAP_OK;
+} catch (...) {
+  return fail_exception();
 }
 
-extern "C" int fap_graph_copy_block(fap_dgraph *G, int32_t part, void *host, int out_dtype) {
+extern "C" int fap_graph_copy_block(fap_dgraph *G, int32_t part, void *host, int out_dtype) try {
   if (!G || !host) return fail(FAP_ERR_INVALID, "NULL argument");
   void *dp;
   int64_t rows, ld;
@@ -1275,10 +1321,12 @@ extern "C" int fap_graph_copy_block(fap_dgraph *G, int32_t part, void *host, int
   FAP_CK(cudaStreamSynchronize(st));
   FAP_TRY(read_status(G));
   return FAP_OK;
+} catch (...) {
+  return fail_exception();
 }
 
 extern "C" int fap_graph_path_block(fap_dgraph *G, int32_t part, void **dev_ptr, int64_t *rows,
-                                    int64_t *ld) {
+                                    int64_t *ld) try {
   if (!G || !dev_ptr || !rows || !ld) return fail(FAP_ERR_INVALID, "NULL argument");
   void *dp;
   FAP_TRY(fap_graph_block(G, part, &dp, rows, ld));
@@ -1286,9 +1334,11 @@ extern "C" int fap_graph_path_block(fap_dgraph *G, int32_t part, void **dev_ptr,
     return fail(FAP_ERR_STATE, "part %d was solved without paths", part);
   *dev_ptr = G->P.as<char>() + (size_t)G->row_base[part] * G->ldD * 4;
   return FAP_OK;
+} catch (...) {
+  return fail_exception();
 }
 
-extern "C" int fap_graph_copy_path_block(fap_dgraph *G, int32_t part, int32_t *host) {
+extern "C" int fap_graph_copy_path_block(fap_dgraph *G, int32_t part, int32_t *host) try {
   if (!G || !host) return fail(FAP_ERR_INVALID, "NULL argument");
   void *dp;
   int64_t rows, ld;
@@ -1301,9 +1351,11 @@ extern "C" int fap_graph_copy_path_block(fap_dgraph *G, int32_t part, int32_t *h
   FAP_CK(cudaStreamSynchronize(st));
   FAP_TRY(read_status(G));
   return FAP_OK;
+} catch (...) {
+  return fail_exception();
 }
 
-extern "C" int fap_graph_block_checksums(fap_dgraph *G, int32_t part, uint64_t *host_out) {
+extern "C" int fap_graph_block_checksums(fap_dgraph *G, int32_t part, uint64_t *host_out) try {
   if (!G || !host_out) return fail(FAP_ERR_INVALID, "NULL argument");
   if (G->dtype != FAP_DTYPE_I32) return fail(FAP_ERR_INVALID, "checksums need the int32 path");
   void *dp;
@@ -1320,9 +1372,11 @@ extern "C" int fap_graph_block_checksums(fap_dgraph *G, int32_t part, uint64_t *
   FAP_CK(cudaStreamSynchronize(st));
   FAP_TRY(read_status(G));
   return FAP_OK;
+} catch (...) {
+  return fail_exception();
 }
 
-extern "C" int fap_graph_checksums_async(fap_dgraph *G, int32_t part, uint64_t *d_out) {
+extern "C" int fap_graph_checksums_async(fap_dgraph *G, int32_t part, uint64_t *d_out) try {
   if (!G || !d_out) return fail(FAP_ERR_INVALID, "NULL argument");
   if (G->dtype != FAP_DTYPE_I32) return fail(FAP_ERR_INVALID, "checksums need the int32 path");
   void *dp;
@@ -1333,14 +1387,18 @@ extern "C" int fap_graph_checksums_async(fap_dgraph *G, int32_t part, uint64_t *
   FAP_CK(launch_row_checksums(reinterpret_cast<const int32_t *>(dp), rows, G->n, ld, d_out,
                               G->ctx->stream, &L));
   return FAP_OK;
+} catch (...) {
+  return fail_exception();
 }
 
-extern "C" int fap_graph_status_async(fap_dgraph *G, int32_t *host_status) {
+extern "C" int fap_graph_status_async(fap_dgraph *G, int32_t *host_status) try {
   if (!G || !host_status) return fail(FAP_ERR_INVALID, "NULL argument");
   DeviceGuard g(G->ctx->device);
   FAP_CK(cudaMemcpyAsync(host_status, G->d_status.p, sizeof(int32_t), cudaMemcpyDeviceToHost,
                          G->ctx->stream));
   return FAP_OK;
+} catch (...) {
+  return fail_exception();
 }
 
 extern "C" int fap_status_code(int32_t device_status) { return status_code(device_status); }
@@ -1361,7 +1419,7 @@ int read_ctx_status(fap_ctx *c) {
 
 extern "C" int fap_op_sssp(fap_ctx *c, int dtype, int32_t n, int64_t m, const int32_t *row_offset,
                            const int32_t *col_val, const void *weight, const int32_t *sources,
-                           int32_t num_sources, void *out, int64_t ld_out) {
+                           int32_t num_sources, void *out, int64_t ld_out) try {
   if (!c || !row_offset || (m > 0 && (!col_val || !weight)) || (num_sources > 0 && (!sources || !out)))
     return fail(FAP_ERR_INVALID, "NULL argument");
   if (n <= 0 || m < 0 || num_sources < 0 || ld_out < n) return fail(FAP_ERR_INVALID, "bad sizes");
@@ -1386,9 +1444,11 @@ extern "C" int fap_op_sssp(fap_ctx *c, int dtype, int32_t n, int64_t m, const in
   }
   c->launches += L;
   return read_ctx_status(c);
+} catch (...) {
+  return fail_exception();
 }
 
-extern "C" int fap_op_floyd(fap_ctx *c, int dtype, int32_t s, void *mat, int64_t ld) {
+extern "C" int fap_op_floyd(fap_ctx *c, int dtype, int32_t s, void *mat, int64_t ld) try {
   if (!c || (s > 0 && !mat)) return fail(FAP_ERR_INVALID, "NULL argument");
   if (s < 0 || ld < s) return fail(FAP_ERR_INVALID, "bad sizes");
   if (s == 0) return FAP_OK;
@@ -1416,10 +1476,12 @@ extern "C" int fap_op_floyd(fap_ctx *c, int dtype, int32_t s, void *mat, int64_t
                            cudaMemcpyDeviceToDevice, st));
   c->launches += L;
   return read_ctx_status(c);
+} catch (...) {
+  return fail_exception();
 }
 
 extern "C" int fap_op_minplus(fap_ctx *c, int dtype, int32_t M, int32_t N, int32_t K, const void *A,
-                              int64_t lda, const void *B, int64_t ldb, void *C, int64_t ldc) {
+                              int64_t lda, const void *B, int64_t ldb, void *C, int64_t ldc) try {
   if (!c) return fail(FAP_ERR_INVALID, "NULL ctx");
   if (M < 0 || N < 0 || K < 0) return fail(FAP_ERR_INVALID, "negative size");
   if (M == 0 || N == 0) return FAP_OK;
@@ -1438,9 +1500,11 @@ extern "C" int fap_op_minplus(fap_ctx *c, int dtype, int32_t M, int32_t N, int32
   FAP_CK(cudaStreamSynchronize(c->stream));
   c->launches += L;
   return FAP_OK;
+} catch (...) {
+  return fail_exception();
 }
 
-extern "C" int fap_measure_relax_peak(fap_ctx *c, int dtype, double *relax_per_s) {
+extern "C" int fap_measure_relax_peak(fap_ctx *c, int dtype, double *relax_per_s) try {
   if (!c || !relax_per_s) return fail(FAP_ERR_INVALID, "NULL argument");
   DeviceGuard g(c->device);
   cudaStream_t st = c->stream;
@@ -1463,6 +1527,8 @@ extern "C" int fap_measure_relax_peak(fap_ctx *c, int dtype, double *relax_per_s
   }
   *relax_per_s = count / (best * 1e-3);
   return FAP_OK;
+} catch (...) {
+  return fail_exception();
 }
 
 namespace {
@@ -1498,7 +1564,7 @@ cudaError_t sssp_rows_launch(fap_dgraph *G, const int32_t *h_sources, int32_t co
 }  // namespace
 
 extern "C" int fap_graph_sssp_rows(fap_dgraph *G, const int32_t *sources, int32_t count,
-                                   float *host_out) {
+                                   float *host_out) try {
   if (!G || (count > 0 && (!sources || !host_out))) return fail(FAP_ERR_INVALID, "NULL argument");
   if (count < 0) return fail(FAP_ERR_INVALID, "negative count");
   if (count == 0) return FAP_OK;
@@ -1534,6 +1600,8 @@ extern "C" int fap_graph_sssp_rows(fap_dgraph *G, const int32_t *sources, int32_
   scratch.release();
   G->ctx->launches += L;
   return rc;
+} catch (...) {
+  return fail_exception();
 }
 
 namespace {
@@ -1592,7 +1660,7 @@ int ensure_in_edges(fap_dgraph *G) {
 }
 }  // namespace
 
-extern "C" int fap_graph_set_param(fap_dgraph *G, const char *key, double value) {
+extern "C" int fap_graph_set_param(fap_dgraph *G, const char *key, double value) try {
   if (!G || !key) return fail(FAP_ERR_INVALID, "NULL argument");
   G->epoch++;  // a captured launch sequence no longer matches
   if (std::strcmp(key, "cuda_graph") == 0) {
@@ -1658,6 +1726,8 @@ extern "C" int fap_graph_set_param(fap_dgraph *G, const char *key, double value)
     return FAP_OK;
   }
   return fail(FAP_ERR_INVALID, "unknown parameter '%s'", key);
+} catch (...) {
+  return fail_exception();
 }
 
 // ---------------------------------------------------------------------------
@@ -1727,12 +1797,14 @@ int tune_sssp_impl(fap_dgraph *G, const double *deltas, int32_t count, int32_t s
 }  // namespace
 
 extern "C" int fap_graph_tune_sssp(fap_dgraph *G, const double *deltas, int32_t count, int32_t sample,
-                                   double *best_delta, float *ms_out) {
+                                   double *best_delta, float *ms_out) try {
   if (!G || !deltas || count <= 0) return fail(FAP_ERR_INVALID, "need a graph and candidate deltas");
   if (G->K == 0) return fail(FAP_ERR_STATE, "tune before fap_graph_set_parts");
   DeviceGuard g(G->ctx->device);
   return G->dtype == FAP_DTYPE_I32 ? tune_sssp_impl<int32_t>(G, deltas, count, sample, best_delta, ms_out)
                                    : tune_sssp_impl<float>(G, deltas, count, sample, best_delta, ms_out);
+} catch (...) {
+  return fail_exception();
 }
 
 extern "C" double fap_graph_mean_weight(const fap_dgraph *G) { return G ? G->mean_w : 0.0; }
@@ -1740,7 +1812,7 @@ extern "C" double fap_graph_mean_weight(const fap_dgraph *G) { return G ? G->mea
 // ---------------------------------------------------------------------------
 // Memory release and asynchronous distance rows (used by the serving loop)
 // ---------------------------------------------------------------------------
-extern "C" int fap_graph_release(fap_dgraph *G) {
+extern "C" int fap_graph_release(fap_dgraph *G) try {
   if (!G) return fail(FAP_ERR_INVALID, "NULL graph");
   DeviceGuard g(G->ctx->device);
   FAP_CK(cudaStreamSynchronize(G->ctx->stream));
@@ -1757,9 +1829,11 @@ extern "C" int fap_graph_release(fap_dgraph *G) {
   G->last_ids.clear();
   G->epoch++;
   return FAP_OK;
+} catch (...) {
+  return fail_exception();
 }
 
-extern "C" int fap_graph_device_bytes(const fap_dgraph *G, int64_t *bytes) {
+extern "C" int fap_graph_device_bytes(const fap_dgraph *G, int64_t *bytes) try {
   if (!G || !bytes) return fail(FAP_ERR_INVALID, "NULL argument");
   int64_t t = 0;
   for (const DevBuf *b : {&G->ro, &G->col, &G->w, &G->ro_s, &G->col_s, &G->w_s, &G->sssp_scratch,
@@ -1773,11 +1847,15 @@ extern "C" int fap_graph_device_bytes(const fap_dgraph *G, int64_t *bytes) {
     t += (int64_t)b->bytes;
   *bytes = t;
   return FAP_OK;
+} catch (...) {
+  return fail_exception();
 }
 
-extern "C" int fap_graph_resident(fap_dgraph *G, int32_t part) {
+extern "C" int fap_graph_resident(fap_dgraph *G, int32_t part) try {
   if (!G || part < 1 || part > G->K) return 0;
   return G->row_base[part] >= 0 ? 1 : 0;
+} catch (...) {
+  return fail_exception();
 }
 
 // ---------------------------------------------------------------------------
@@ -1989,7 +2067,7 @@ int rows_cached_impl(fap_dgraph *G, const int32_t *sources, int32_t count, float
 }
 }  // namespace
 
-extern "C" int fap_graph_cache_build(fap_dgraph *G) {
+extern "C" int fap_graph_cache_build(fap_dgraph *G) try {
   if (!G) return fail(FAP_ERR_INVALID, "NULL graph");
   if (G->K == 0) return fail(FAP_ERR_STATE, "fap_graph_cache_build before fap_graph_set_parts");
   if (G->cache_ready) return FAP_OK;
@@ -1997,33 +2075,41 @@ extern "C" int fap_graph_cache_build(fap_dgraph *G) {
   const int rc = G->dtype == FAP_DTYPE_I32 ? cache_build_impl<int32_t>(G) : cache_build_impl<float>(G);
   if (rc != FAP_OK) cache_drop(G);
   return rc;
+} catch (...) {
+  return fail_exception();
 }
 
-extern "C" int fap_graph_cache_rebuild(fap_dgraph *G) {
+extern "C" int fap_graph_cache_rebuild(fap_dgraph *G) try {
   if (!G) return fail(FAP_ERR_INVALID, "NULL graph");
   if (G->K == 0) return fail(FAP_ERR_STATE, "fap_graph_cache_rebuild before fap_graph_set_parts");
   DeviceGuard g(G->ctx->device);
   const int rc = G->dtype == FAP_DTYPE_I32 ? cache_build_impl<int32_t>(G) : cache_build_impl<float>(G);
   if (rc != FAP_OK) cache_drop(G);
   return rc;
+} catch (...) {
+  return fail_exception();
 }
 
-extern "C" int fap_graph_cache_timing(const fap_dgraph *G, float *ms4) {
+extern "C" int fap_graph_cache_timing(const fap_dgraph *G, float *ms4) try {
   if (!G || !ms4) return fail(FAP_ERR_INVALID, "NULL argument");
   if (!G->cache_ready) return fail(FAP_ERR_STATE, "no resident cache");
   for (int i = 0; i < 4; i++) ms4[i] = G->cache_ms[i];
   return FAP_OK;
+} catch (...) {
+  return fail_exception();
 }
 
-extern "C" int fap_graph_cache_release(fap_dgraph *G) {
+extern "C" int fap_graph_cache_release(fap_dgraph *G) try {
   if (!G) return fail(FAP_ERR_INVALID, "NULL graph");
   DeviceGuard g(G->ctx->device);
   FAP_CK(cudaStreamSynchronize(G->ctx->stream));
   cache_drop(G);
   return FAP_OK;
+} catch (...) {
+  return fail_exception();
 }
 
-extern "C" int fap_graph_cache_bytes(const fap_dgraph *G, int64_t *bytes, int *built) {
+extern "C" int fap_graph_cache_bytes(const fap_dgraph *G, int64_t *bytes, int *built) try {
   if (!G || !bytes) return fail(FAP_ERR_INVALID, "NULL argument");
   if (G->K == 0) return fail(FAP_ERR_STATE, "no partition");
   if (built) *built = G->cache_ready ? 1 : 0;
@@ -2065,6 +2151,8 @@ extern "C" int fap_graph_cache_bytes(const fap_dgraph *G, int64_t *bytes, int *b
     }
   }
   return FAP_OK;
+} catch (...) {
+  return fail_exception();
 }
 
 namespace {
@@ -2106,7 +2194,7 @@ int rows_async_impl(fap_dgraph *G, const int32_t *sources, int32_t count, float 
 }
 }  // namespace
 
-extern "C" int fap_graph_rows_async(fap_dgraph *G, const int32_t *sources, int32_t count, float *d_out) {
+extern "C" int fap_graph_rows_async(fap_dgraph *G, const int32_t *sources, int32_t count, float *d_out) try {
   if (!G || (count > 0 && (!sources || !d_out))) return fail(FAP_ERR_INVALID, "NULL argument");
   if (count < 0) return fail(FAP_ERR_INVALID, "negative count");
   if (count == 0) return FAP_OK;
@@ -2118,4 +2206,6 @@ extern "C" int fap_graph_rows_async(fap_dgraph *G, const int32_t *sources, int32
                                      : rows_cached_impl<float>(G, sources, count, d_out);
   return G->dtype == FAP_DTYPE_I32 ? rows_async_impl<int32_t>(G, sources, count, d_out)
                                    : rows_async_impl<float>(G, sources, count, d_out);
+} catch (...) {
+  return fail_exception();
 }

@@ -14,8 +14,10 @@
 #include <cstdio>
 #include <cstring>
 #include <deque>
+#include <exception>
 #include <memory>
 #include <mutex>
+#include <new>
 #include <string>
 #include <thread>
 #include <unordered_map>
@@ -141,6 +143,19 @@ thread_local std::string s_err;
 int serr(int code, const char *msg) {
   s_err = msg;
   return code;
+}
+
+// No C++ exception leaves an entry point of the server's C ABI.
+int serr_exception() {
+  try {
+    throw;
+  } catch (const std::bad_alloc &) {
+    return serr(FAP_ERR_NOMEM, "host allocation failed");
+  } catch (const std::exception &e) {
+    return serr(FAP_ERR_INVALID, e.what());
+  } catch (...) {
+    return serr(FAP_ERR_INVALID, "unknown C++ exception");
+  }
 }
 }  // namespace
 
@@ -558,7 +573,7 @@ void fap_server::loop() {
 
 extern "C" {
 
-int fap_server_create(int device, double budget_bytes, int64_t max_batch_rows, fap_server **out) {
+int fap_server_create(int device, double budget_bytes, int64_t max_batch_rows, fap_server **out) try {
   if (!out) return serr(FAP_ERR_INVALID, "NULL out");
   *out = nullptr;
   if (cudaSetDevice(device) != cudaSuccess) {
@@ -588,9 +603,11 @@ int fap_server_create(int device, double budget_bytes, int64_t max_batch_rows, f
   s->worker = std::thread([s] { s->loop(); });
   *out = s;
   return FAP_OK;
+} catch (...) {
+  return serr_exception();
 }
 
-int fap_server_destroy(fap_server *s) {
+int fap_server_destroy(fap_server *s) try {
   if (!s) return FAP_OK;
   {
     std::lock_guard<std::mutex> lk(s->mu);
@@ -621,12 +638,14 @@ int fap_server_destroy(fap_server *s) {
   for (auto &kv : s->reqs) delete kv.second;
   delete s;
   return FAP_OK;
+} catch (...) {
+  return serr_exception();
 }
 
 int fap_server_add_graph(fap_server *s, int32_t n, int64_t m, const int32_t *row_offset,
                          const int32_t *col_val, const float *weight, int dtype, int32_t K,
                          const int32_t *graph_id, const int32_t *st2ed, const int32_t *ver_num,
-                         const int32_t *ver_offset, const int32_t *bdy_num, int32_t *index) {
+                         const int32_t *ver_offset, const int32_t *bdy_num, int32_t *index) try {
   if (!s || !index) return serr(FAP_ERR_INVALID, "NULL argument");
   std::lock_guard<std::mutex> add_lock(s->add_mu);
   const int slot = s->ngraphs.load();
@@ -671,10 +690,12 @@ int fap_server_add_graph(fap_server *s, int32_t n, int64_t m, const int32_t *row
   s->ngraphs.store(slot + 1, std::memory_order_release);
   *index = slot;
   return FAP_OK;
+} catch (...) {
+  return serr_exception();
 }
 
 int fap_server_submit(fap_server *s, int32_t graph, int kind, const int32_t *ids, int32_t count,
-                      float *host_out, uint64_t *checksums_out, int64_t *req_id) {
+                      float *host_out, uint64_t *checksums_out, int64_t *req_id) try {
   if (!s || !ids || !req_id || count <= 0) return serr(FAP_ERR_INVALID, "bad request arguments");
   std::lock_guard<std::mutex> lk(s->mu);
   if (s->stop) return serr(FAP_ERR_STATE, "server is stopping");
@@ -712,9 +733,11 @@ int fap_server_submit(fap_server *s, int32_t graph, int kind, const int32_t *ids
   s->cv_work.notify_all();
   *req_id = r->id;
   return FAP_OK;
+} catch (...) {
+  return serr_exception();
 }
 
-int fap_server_wait(fap_server *s, int64_t req_id, double timeout_s, int *state) {
+int fap_server_wait(fap_server *s, int64_t req_id, double timeout_s, int *state) try {
   if (!s) return serr(FAP_ERR_INVALID, "NULL server");
   std::unique_lock<std::mutex> lk(s->mu);
   auto it = s->reqs.find(req_id);
@@ -725,9 +748,11 @@ int fap_server_wait(fap_server *s, int64_t req_id, double timeout_s, int *state)
   else s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), done);
   if (state) *state = r->state;
   return FAP_OK;
+} catch (...) {
+  return serr_exception();
 }
 
-int fap_server_request_info(fap_server *s, int64_t req_id, double *out4) {
+int fap_server_request_info(fap_server *s, int64_t req_id, double *out4) try {
   if (!s || !out4) return serr(FAP_ERR_INVALID, "NULL argument");
   std::lock_guard<std::mutex> lk(s->mu);
   auto it = s->reqs.find(req_id);
@@ -739,9 +764,11 @@ int fap_server_request_info(fap_server *s, int64_t req_id, double *out4) {
   out4[2] = (double)r->entries;
   out4[3] = (double)r->status;
   return FAP_OK;
+} catch (...) {
+  return serr_exception();
 }
 
-int fap_server_forget(fap_server *s, int64_t req_id) {
+int fap_server_forget(fap_server *s, int64_t req_id) try {
   if (!s) return serr(FAP_ERR_INVALID, "NULL server");
   std::lock_guard<std::mutex> lk(s->mu);
   auto it = s->reqs.find(req_id);
@@ -751,16 +778,20 @@ int fap_server_forget(fap_server *s, int64_t req_id) {
   delete it->second;
   s->reqs.erase(it);
   return FAP_OK;
+} catch (...) {
+  return serr_exception();
 }
 
-int fap_server_drain(fap_server *s) {
+int fap_server_drain(fap_server *s) try {
   if (!s) return serr(FAP_ERR_INVALID, "NULL server");
   std::unique_lock<std::mutex> lk(s->mu);
   s->cv_done.wait(lk, [&] { return s->outstanding == 0; });
   return FAP_OK;
+} catch (...) {
+  return serr_exception();
 }
 
-int fap_server_stats(fap_server *s, double *out, int32_t count) {
+int fap_server_stats(fap_server *s, double *out, int32_t count) try {
   if (!s || (!out && count > 0)) return serr(FAP_ERR_INVALID, "NULL argument");
   std::lock_guard<std::mutex> lk(s->mu);
   std::vector<double> v = s->lat_ms;
@@ -785,9 +816,11 @@ int fap_server_stats(fap_server *s, double *out, int32_t count) {
                                          s->busy_ms};
   for (int32_t i = 0; i < count; i++) out[i] = i < FAP_SERVER_NSTATS ? all[i] : 0.0;
   return FAP_OK;
+} catch (...) {
+  return serr_exception();
 }
 
-int fap_server_reset_stats(fap_server *s) {
+int fap_server_reset_stats(fap_server *s) try {
   if (!s) return serr(FAP_ERR_INVALID, "NULL server");
   std::lock_guard<std::mutex> lk(s->mu);
   s->lat_ms.clear();
@@ -799,9 +832,11 @@ int fap_server_reset_stats(fap_server *s) {
   s->cache_builds = 0;
   s->busy_ms = 0;
   return FAP_OK;
+} catch (...) {
+  return serr_exception();
 }
 
-int fap_server_set_option(fap_server *s, const char *key, double value) {
+int fap_server_set_option(fap_server *s, const char *key, double value) try {
   if (!s || !key) return serr(FAP_ERR_INVALID, "NULL argument");
   if (std::strcmp(key, "max_batch_bytes") == 0) {
     s->max_batch_bytes = value > 0 ? (int64_t)value : 0;
@@ -816,6 +851,8 @@ int fap_server_set_option(fap_server *s, const char *key, double value) {
     return FAP_OK;
   }
   return serr(FAP_ERR_INVALID, "unknown option");
+} catch (...) {
+  return serr_exception();
 }
 
 const char *fap_server_last_error(void) { return s_err.c_str(); }
