@@ -1,6 +1,7 @@
 """Host-side pieces of bench.py that need no GPU: the clock sampler keeps
 only the samples taken inside the timed region (and reports throttle
-reasons seen there), and the default run keeps at least 3 warm-up steps."""
+reasons seen there), the default run keeps at least 3 warm-up steps, and
+the reference arm prints its contract line from rank 0 only."""
 import datetime
 import importlib.util
 import os
@@ -72,3 +73,36 @@ def test_default_run_has_three_warmup_steps(monkeypatch):
     monkeypatch.setattr(sys, "argv", ["bench.py"])
     args = b.parse_args()
     assert args.warmup >= 3 and args.steps >= 1 and args.gpus == 1
+
+
+def _run_bench(args, env_extra=None):
+    import json
+    import subprocess
+    env = dict(os.environ)
+    env.update(env_extra or {})
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py")] + args, cwd=ROOT, env=env,
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    return [json.loads(ln) for ln in lines]
+
+
+def test_reference_arm_prints_one_contract_line():
+    """`bench.py --impl reference` times the reference's CPU path on the
+    host (no GPU) and prints one JSON line with the contract's keys."""
+    out = _run_bench(["--impl", "reference", "--workload", "grid64", "--steps", "1", "--warmup", "0"])
+    assert len(out) == 1
+    line = out[0]
+    assert line["impl"] == "reference" and line["value"] > 0 and line["unit"] == "entries/s"
+    assert line["higher_is_better"] is True and line["steps"] == 1 and line["n_gpus"] == 1
+    assert line["config"]["workload"] == "grid64"
+    cb = line["cpu_baseline"]
+    assert cb["kind"] in ("reference", "port") and cb["cores"] >= 1 and cb["value"] == line["value"]
+    assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}
+
+
+def test_reference_arm_runs_on_rank_zero_only():
+    out = _run_bench(["--impl", "reference", "--workload", "grid64", "--steps", "1", "--warmup", "0"],
+                     {"RANK": "1", "LOCAL_RANK": "1", "WORLD_SIZE": "2"})
+    assert out == []
