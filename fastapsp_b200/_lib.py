@@ -156,6 +156,11 @@ LEGACY_SYMBOLS = {
     "handle_boundry_Nvidia_GPU": "_Z25handle_boundry_Nvidia_GPUPfiiiPiS0_S0_S_S0_i",
     "floyd_GPU_Nvidia_path": "_Z21floyd_GPU_Nvidia_pathiPfPi",
     "minplus_NVIDIA_path": "_Z19minplus_NVIDIA_pathPfS_PiS_S0_iii",
+    "floyd_NVIDIA_GPU": "_Z16floyd_NVIDIA_GPUiPf",
+    "floyd_path_A_Nvidia": "_Z19floyd_path_A_NvidiaPfPiiiS_S0_",
+    "floyd_path_B_Nvidia": "_Z19floyd_path_B_NvidiaPfPiiiS_S0_",
+    "floyd_min_plus_Nvidia": "_Z21floyd_min_plus_NvidiaPfS_PiS_S0_iii",
+    "minplus_NVIDIA_GPU": "_Z18minplus_NVIDIA_GPUPfS_S_iii",
 }
 
 

@@ -2,7 +2,9 @@
 // implemented on top of the C ABI in fap_b200.h.  See fap_legacy_kernel.h.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <vector>
 
@@ -108,13 +110,16 @@ void floyd_GPU_Nvidia_path(int num_node, float *arc, int *path) {
   }
 }
 
-void minplus_NVIDIA_path(float *mat1, float *mat2, int *mat2_path, float *res, int *res_path, int m,
-                         int n, int k) {
-  (void)mat2_path;
-  (void)res_path;
+namespace {
+
+// res[m x n] = min(1e8, mat1[m x k] (x) mat2[k x n]) on the GPU for host
+// row-major matrices, in int32 when every input is an integral distance,
+// else in float32.  res may be one of the inputs: both are uploaded before
+// it is written.
+void host_minplus(const float *mat1, const float *mat2, float *res, int m, int n, int k, const char *where) {
   fap_ctx *c = legacy_ctx();
   if (!c) {
-    report(FAP_ERR_CUDA, "minplus_NVIDIA_path");
+    report(FAP_ERR_CUDA, where);
     return;
   }
   if (m <= 0 || n <= 0) {
@@ -125,7 +130,7 @@ void minplus_NVIDIA_path(float *mat1, float *mat2, int *mat2_path, float *res, i
   const bool ints = all_integral(mat1, ca) && all_integral(mat2, cb);
   Dev A, B, C;
   if (!A.alloc(ca * 4) || !B.alloc(cb * 4) || !C.alloc(cc * 4)) {
-    report(FAP_ERR_NOMEM, "minplus_NVIDIA_path");
+    report(FAP_ERR_NOMEM, where);
     return;
   }
   if (ints) {
@@ -138,9 +143,9 @@ void minplus_NVIDIA_path(float *mat1, float *mat2, int *mat2_path, float *res, i
     cudaMemcpy(A.p, mat1, ca * 4, cudaMemcpyHostToDevice);
     cudaMemcpy(B.p, mat2, cb * 4, cudaMemcpyHostToDevice);
   }
-  if (!report(fap_op_minplus(c, ints ? FAP_DTYPE_I32 : FAP_DTYPE_F32, m, n, k, A.p, k > 0 ? k : 1, B.p,
-                             n, C.p, n),
-              "minplus_NVIDIA_path"))
+  if (!report(fap_op_minplus(c, ints ? FAP_DTYPE_I32 : FAP_DTYPE_F32, m, n, k, A.p, k > 0 ? k : 1, B.p, n,
+                             C.p, n),
+              where))
     return;
   if (ints) {
     std::vector<int32_t> t(cc);
@@ -149,4 +154,63 @@ void minplus_NVIDIA_path(float *mat1, float *mat2, int *mat2_path, float *res, i
   } else {
     cudaMemcpy(res, C.p, cc * 4, cudaMemcpyDeviceToHost);
   }
+}
+
+}  // namespace
+
+void minplus_NVIDIA_path(float *mat1, float *mat2, int *mat2_path, float *res, int *res_path, int m,
+                         int n, int k) {
+  (void)mat2_path;
+  (void)res_path;
+  host_minplus(mat1, mat2, res, m, n, k, "minplus_NVIDIA_path");
+}
+
+void minplus_NVIDIA_GPU(float *mat1, float *mat2, float *res, int M, int N, int K) {
+  host_minplus(mat1, mat2, res, M, N, K, "minplus_NVIDIA_GPU");
+}
+
+void floyd_NVIDIA_GPU(int num_node, float *arc) { floyd_GPU_Nvidia_path(num_node, arc, nullptr); }
+
+// Column panel of a blocked Floyd (fap/kernel/floyd.h:106-115): the new
+// panel from the old one and the closed diagonal block, computed out of
+// place as the reference's CUDA kernel intends.
+void floyd_path_A_Nvidia(float *A, int *A_path, const int row, const int col, float *diag, int *diag_path) {
+  (void)A_path;
+  (void)diag_path;
+  host_minplus(A, diag, A, row, col, col, "floyd_path_A_Nvidia");
+}
+
+// Row panel of a blocked Floyd (fap/kernel/floyd.h:118-127).
+void floyd_path_B_Nvidia(float *B, int *B_path, const int row, const int col, float *diag, int *diag_path) {
+  (void)B_path;
+  (void)diag_path;
+  host_minplus(diag, B, B, row, col, row, "floyd_path_B_Nvidia");
+}
+
+// res = min(res, mat1 (x) mat2) (fap/kernel/floyd.h:130-139) as one product
+// from the sentinel: [mat1 | E] (x) [mat2 ; res], E the min-plus identity
+// (0 on the diagonal, 1e8 elsewhere), so that E (x) res = res.
+void floyd_min_plus_Nvidia(float *mat1, float *mat2, int *mat2_path, float *res, int *res_path, int m, int n,
+                           int k) {
+  (void)mat2_path;
+  (void)res_path;
+  if (m <= 0 || n <= 0) {
+    t_status = FAP_OK;
+    return;
+  }
+  const int64_t kk = k > 0 ? k : 0;
+  const int64_t k2 = kk + m;
+  if (k2 > INT32_MAX) {
+    report(FAP_ERR_RANGE, "floyd_min_plus_Nvidia");
+    return;
+  }
+  std::vector<float> a2((size_t)m * (size_t)k2, 1e8f), b2((size_t)k2 * (size_t)n);
+  for (int64_t i = 0; i < m; i++) {
+    float *row = a2.data() + i * k2;
+    for (int64_t j = 0; j < kk; j++) row[j] = mat1[i * kk + j];
+    row[kk + i] = 0.0f;
+  }
+  std::copy(mat2, mat2 + kk * n, b2.begin());
+  std::copy(res, res + (int64_t)m * n, b2.begin() + kk * n);
+  host_minplus(a2.data(), b2.data(), res, m, n, (int)k2, "floyd_min_plus_Nvidia");
 }

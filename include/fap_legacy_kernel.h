@@ -4,8 +4,10 @@
  * -DWITH_CUDA) links against this library unchanged.
  *
  * Signatures and C++ linkage are exactly those of
- * fap/kernel/cuda/cuda_kernel.h:21-24, :29 and :41-42 (Liu-xiandong/FastAPSP).
- * All pointers are host pointers; calls are synchronous, like the reference.
+ * fap/kernel/cuda/cuda_kernel.h:21-42 (Liu-xiandong/FastAPSP), every entry
+ * point but batched_sssp_cuGraph (:16-19, the nvGraph build, whose library
+ * CUDA no longer ships).  All pointers are host pointers; calls are
+ * synchronous, like the reference.
  *
  * Behaviour:
  *   - distances are computed on the GPU in int32 when every input value is an
@@ -41,6 +43,34 @@ FAP_LEGACY_API void floyd_GPU_Nvidia_path(int num_node, float *arc, int *path);
  * Replaces cuda_kernel.h:41-42. */
 FAP_LEGACY_API void minplus_NVIDIA_path(float *mat1, float *mat2, int *mat2_path, float *res, int *res_path,
                          int m, int n, int k);
+
+/* The rest of the reference's kernel header, which fap/fap.cpp also calls
+ * (fap/kernel/minplus.h:69-76, fap/kernel/floyd.h:106-139) and so needs at
+ * link time.  Same meanings as the reference's CUDA versions; paths are left
+ * unchanged as above. */
+
+/* Floyd-Warshall of arc[num_node x num_node] in place, no paths.
+ * Replaces cuda_kernel.h:27. */
+FAP_LEGACY_API void floyd_NVIDIA_GPU(int num_node, float *arc);
+
+/* Blocked Floyd, column panel: A[row x col] = min(1e8, A (x) diag[col x col]).
+ * Replaces cuda_kernel.h:31-32. */
+FAP_LEGACY_API void floyd_path_A_Nvidia(float *A, int *A_path, const int row, const int col, float *diag,
+                                        int *diag_path);
+
+/* Blocked Floyd, row panel: B[row x col] = min(1e8, diag[row x row] (x) B).
+ * Replaces cuda_kernel.h:33-34. */
+FAP_LEGACY_API void floyd_path_B_Nvidia(float *B, int *B_path, const int row, const int col, float *diag,
+                                        int *diag_path);
+
+/* Blocked Floyd, remaining blocks: res[m x n] = min(res, mat1[m x k] (x)
+ * mat2[k x n]) (res entries at most 1e8).  Replaces cuda_kernel.h:35-36. */
+FAP_LEGACY_API void floyd_min_plus_Nvidia(float *mat1, float *mat2, int *mat2_path, float *res, int *res_path,
+                                          int m, int n, int k);
+
+/* res[M x N] = min(1e8, mat1[M x K] (x) mat2[K x N]), no paths.
+ * Replaces cuda_kernel.h:39-40. */
+FAP_LEGACY_API void minplus_NVIDIA_GPU(float *mat1, float *mat2, float *res, int M, int N, int K);
 
 #ifdef __cplusplus
 extern "C" {

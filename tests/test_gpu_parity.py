@@ -357,6 +357,74 @@ def test_legacy_abi_matches_oracle(cuda_ok):
     np.testing.assert_array_equal(sub, case["dist"][off:off + b])
 
 
+def test_legacy_abi_blocked_floyd_entry_points(cuda_ok):
+    """The rest of the reference's kernel header, which its fap/fap.cpp also
+    calls: the blocked-Floyd column and row panels (fap/kernel/floyd.h:
+    51-84, their CUDA versions from the sentinel), the remaining-block update
+    res = min(res, mat1 (x) mat2) (:86-102), the path-free min-plus
+    (minplus.h:69-76) and Floyd.  Integral inputs run in int32 and must match
+    exactly; real-valued ones in float32 within the tolerance.  Path arrays
+    are left unchanged."""
+    lib = L.lib()
+    f = {k: getattr(lib, L.LEGACY_SYMBOLS[k]) for k in
+         ("floyd_NVIDIA_GPU", "floyd_path_A_Nvidia", "floyd_path_B_Nvidia", "floyd_min_plus_Nvidia",
+          "minplus_NVIDIA_GPU")}
+    inf = np.float32(1e8)
+    rng = np.random.default_rng(21)
+    for integral in (True, False):
+        def mat(r, c, p_inf=0.4):
+            if integral:
+                x = rng.integers(0, 60, (r, c)).astype(np.float32)
+            else:
+                x = (rng.random((r, c)) * 60).astype(np.float32)
+            x[rng.random((r, c)) < p_inf] = inf
+            return x
+
+        def closed(s):
+            d = mat(s, s, 0.7)
+            np.fill_diagonal(d, 0)
+            return O.port_floyd(d)
+
+        row, col = 37, 23
+        # Floyd without paths
+        arc = mat(50, 50, 0.85)
+        np.fill_diagonal(arc, 0)
+        want = O.port_floyd(arc)
+        f["floyd_NVIDIA_GPU"](50, L.ptr(arc))
+        assert lib.fap_legacy_last_status() == 0
+        assert_dist_equal(arc, want, integral)
+        # column panel A[row x col] against diag[col x col]
+        diag = closed(col)
+        A = mat(row, col)
+        want = _np_minplus(A, diag, inf)
+        A_path, diag_path = np.zeros((row, col), np.int32), np.zeros((col, col), np.int32)
+        f["floyd_path_A_Nvidia"](L.ptr(A), L.ptr(A_path), row, col, L.ptr(diag), L.ptr(diag_path))
+        assert lib.fap_legacy_last_status() == 0
+        assert_dist_equal(A, want, integral)
+        assert not A_path.any()
+        # row panel B[row x col] against diag[row x row]
+        diag = closed(row)
+        B = mat(row, col)
+        want = _np_minplus(diag, B, inf)
+        B_path, diag_path = np.zeros((row, col), np.int32), np.zeros((row, row), np.int32)
+        f["floyd_path_B_Nvidia"](L.ptr(B), L.ptr(B_path), row, col, L.ptr(diag), L.ptr(diag_path))
+        assert lib.fap_legacy_last_status() == 0
+        assert_dist_equal(B, want, integral)
+        # remaining blocks: res = min(res, mat1 (x) mat2), also with k = 0
+        for m_, n_, k_ in ((29, 41, 13), (5, 9, 0)):
+            m1, m2, res = mat(m_, k_), mat(k_, n_), mat(m_, n_, 0.3)
+            want = np.minimum(res, _np_minplus(m1, m2, inf))
+            f["floyd_min_plus_Nvidia"](L.ptr(m1), L.ptr(m2), L.ptr(np.zeros((k_, n_), np.int32)), L.ptr(res),
+                                       L.ptr(np.zeros((m_, n_), np.int32)), m_, n_, k_)
+            assert lib.fap_legacy_last_status() == 0
+            assert_dist_equal(res, want, integral)
+        # path-free min-plus from the sentinel (res's old values are ignored)
+        m1, m2, res = mat(33, 19), mat(19, 47), np.zeros((33, 47), np.float32)
+        f["minplus_NVIDIA_GPU"](L.ptr(m1), L.ptr(m2), L.ptr(res), 33, 47, 19)
+        assert lib.fap_legacy_last_status() == 0
+        assert_dist_equal(res, _np_minplus(m1, m2, inf), integral)
+
+
 def test_relax_peak_is_positive(cuda_ok):
     ctx = Context(0)
     assert ctx.relax_peak(FAP_DTYPE_I32) > 1e12
