@@ -572,6 +572,14 @@ float fapGraph::getDistanceP2P(int32_t from, int32_t to) {
   return subgraph_dist[(size_t)row * n + to];
 }
 
+float fapGraph::getDistanceP2P() {
+  raise(FAP_ERR_INVALID, "getDistanceP2P needs its two endpoints: getDistanceP2P(from, to)");
+}
+
+std::vector<int32_t> fapGraph::getPathP2P() {
+  raise(FAP_ERR_INVALID, "getPathP2P needs its two endpoints: getPathP2P(from, to)");
+}
+
 // The vertices of a shortest path from `from` to `to` (both included), read
 // off the predecessor row of `from`; empty when `to` is unreachable.  The
 // reference leaves this a TODO (fap/fap.cpp:263-269).

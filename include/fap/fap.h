@@ -13,7 +13,7 @@
 //   - getDistanceFromOnePoint / getPathFromOnePoint index the requested row
 //     (fap/fap.cpp:245-258 forget the row length);
 //   - getDistanceP2P / getPathP2P take the two endpoints (TODO in the
-//     reference, fap/fap.cpp:263-269);
+//     reference, fap/fap.cpp:263-269; the argument-free forms throw);
 //   - errors throw fap::fapError instead of exit().
 #ifndef FAP_B200_FAP_H_
 #define FAP_B200_FAP_H_
@@ -155,6 +155,12 @@ class __attribute__((visibility("default"))) fapGraph {
   std::vector<int32_t> getPathFromOnePoint(int32_t vectex_id);
   float getDistanceP2P(int32_t from, int32_t to);
   std::vector<int32_t> getPathP2P(int32_t from, int32_t to);
+  // The reference's argument-free declarations (fap/fap.h:116-119), kept so
+  // that its callers compile; with no endpoints there is nothing to answer,
+  // so they throw fapError(FAP_ERR_INVALID) (the reference's bodies are
+  // empty TODOs that return nothing, fap/fap.cpp:263-269).
+  float getDistanceP2P();
+  std::vector<int32_t> getPathP2P();
 
   // Per-part counts after preCondition (index 1..K).
   const std::vector<int> &getBlockVerNum() const { return C_BlockVer_num; }
