@@ -469,7 +469,10 @@ def main_fap(args):
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
     if world > 1:
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+        # Ranks do the same work between collectives (loading the workload,
+        # tuning, one timed pass); a rank that died or hangs ends the others'
+        # next collective with an error after this long.
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
 
     def barrier():
