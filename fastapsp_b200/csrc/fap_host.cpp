@@ -649,7 +649,15 @@ int h_fail_std(const std::exception &e) {
   h_err = e.what();
   return FAP_ERR_INVALID;
 }
+int h_invalid(const char *msg) {
+  h_err = msg;
+  return FAP_ERR_INVALID;
+}
 }  // namespace
+
+// Every pointer argument of a wrapper is checked: NULL is FAP_ERR_INVALID.
+#define FAPH_NEED(cond) \
+  if (!(cond)) return h_invalid("NULL argument")
 
 #define FAPH_BODY(...)                         \
   try {                                        \
@@ -669,13 +677,14 @@ extern "C" {
 const char *fap_host_last_error(void) { return h_err.c_str(); }
 
 int fap_host_from_mtx(const char *name, int directed, int weighted, int K, fap::fapGraph **out) {
-  if (!name || !out) return FAP_ERR_INVALID;
+  FAPH_NEED(name && out);
   FAPH_BODY(*out = new fap::fapGraph(std::string(name), directed != 0, weighted != 0, K))
 }
 
 int fap_host_from_csr(int32_t n, int64_t m, const int32_t *ro, const int32_t *col, const float *w,
                       int K, int directed, fap::fapGraph **out) {
-  if (!ro || !out || (m > 0 && (!col || !w))) return FAP_ERR_INVALID;
+  FAPH_NEED(ro && out && (m <= 0 || (col && w)));
+  if (n <= 0 || m < 0) return h_invalid("n must be positive and m non-negative");
   FAPH_BODY({
     std::vector<int32_t> r(ro, ro + n + 1), c(col, col + m);
     std::vector<float> ww(w, w + m);
@@ -684,12 +693,12 @@ int fap_host_from_csr(int32_t n, int64_t m, const int32_t *ro, const int32_t *co
 }
 
 int fap_host_save(fap::fapGraph *g, const char *path) {
-  if (!g || !path) return FAP_ERR_INVALID;
+  FAPH_NEED(g && path);
   FAPH_BODY(g->saveBinary(path))
 }
 
 int fap_host_load(const char *path, fap::fapGraph **out) {
-  if (!path || !out) return FAP_ERR_INVALID;
+  FAPH_NEED(path && out);
   FAPH_BODY(*out = fap::fapGraph::loadBinary(path).release())
 }
 
@@ -699,10 +708,12 @@ int fap_host_destroy(fap::fapGraph *g) {
 }
 
 int fap_host_set_partition(fap::fapGraph *g, const int32_t *gid) {
+  FAPH_NEED(g && gid);
   FAPH_BODY(g->setPartition(std::vector<int32_t>(gid, gid + g->num_vertexs)))
 }
 
 int fap_host_set_options(fap::fapGraph *g, int device, int dtype, int mode) {
+  FAPH_NEED(g);
   FAPH_BODY({
     g->setDevice(device);
     g->setDtype(dtype);
@@ -710,27 +721,42 @@ int fap_host_set_options(fap::fapGraph *g, int device, int dtype, int mode) {
   })
 }
 
-int fap_host_precondition(fap::fapGraph *g) { FAPH_BODY(g->preCondition()) }
+int fap_host_precondition(fap::fapGraph *g) {
+  FAPH_NEED(g);
+  FAPH_BODY(g->preCondition())
+}
 
-int fap_host_is_split(fap::fapGraph *g) { return g->isSplit() ? 1 : 0; }
+int fap_host_is_split(fap::fapGraph *g) {
+  FAPH_NEED(g);
+  return g->isSplit() ? 1 : 0;
+}
 
 int fap_host_dtype(fap::fapGraph *g) {
+  FAPH_NEED(g);
+  int dt = FAP_ERR_INVALID;
   try {
-    return g->getDtype();
+    dt = g->getDtype();
   } catch (const fap::fapError &e) {
     return h_fail(e);
+  } catch (const std::bad_alloc &) {
+    h_err = "host allocation failed";
+    return FAP_ERR_NOMEM;
+  } catch (const std::exception &e) {
+    return h_fail_std(e);
   }
+  return dt;
 }
 
 // sizes: [n, m_decl, K, stored arcs]
 int fap_host_flags(fap::fapGraph *g, int *directed, int *weighted) {
-  if (!g || !directed || !weighted) return FAP_ERR_INVALID;
+  FAPH_NEED(g && directed && weighted);
   *directed = g->directed ? 1 : 0;
   *weighted = g->weighted ? 1 : 0;
   return FAP_OK;
 }
 
 int fap_host_sizes(fap::fapGraph *g, int64_t *out4) {
+  FAPH_NEED(g && out4);
   out4[0] = g->num_vertexs;
   out4[1] = g->num_edges;
   out4[2] = g->getK();
@@ -739,6 +765,7 @@ int fap_host_sizes(fap::fapGraph *g, int64_t *out4) {
 }
 
 int fap_host_csr(fap::fapGraph *g, int32_t *ro, int32_t *col, float *w) {
+  FAPH_NEED(g && ro && col && w);
   const int64_t used = g->row_offset.back();
   std::memcpy(ro, g->row_offset.data(), (g->num_vertexs + 1) * sizeof(int32_t));
   std::memcpy(col, g->col_val.data(), used * sizeof(int32_t));
@@ -747,12 +774,14 @@ int fap_host_csr(fap::fapGraph *g, int32_t *ro, int32_t *col, float *w) {
 }
 
 int fap_host_graph_id(fap::fapGraph *g, int32_t *out) {
+  FAPH_NEED(g && out);
   auto v = g->getGraphId();
   std::memcpy(out, v.data(), v.size() * sizeof(int32_t));
   return FAP_OK;
 }
 
 int fap_host_mapping(fap::fapGraph *g, int32_t *out) {
+  FAPH_NEED(g && out);
   auto v = g->getMapping();
   std::memcpy(out, v.data(), v.size() * sizeof(int32_t));
   return FAP_OK;
@@ -760,6 +789,7 @@ int fap_host_mapping(fap::fapGraph *g, int32_t *out) {
 
 // ver_num, ver_offset, bdy_num: K+1 entries each
 int fap_host_parts(fap::fapGraph *g, int32_t *vnum, int32_t *voff, int32_t *bnum) {
+  FAPH_NEED(g && vnum && voff && bnum);
   const int K = g->getK();
   std::memcpy(vnum, g->getBlockVerNum().data(), (K + 1) * sizeof(int32_t));
   std::memcpy(voff, g->getBlockVerOffset().data(), (K + 1) * sizeof(int32_t));
@@ -767,17 +797,25 @@ int fap_host_parts(fap::fapGraph *g, int32_t *vnum, int32_t *voff, int32_t *bnum
   return FAP_OK;
 }
 
-int fap_host_solve(fap::fapGraph *g, int path_needed) { FAPH_BODY(g->solve(path_needed != 0)) }
+int fap_host_solve(fap::fapGraph *g, int path_needed) {
+  FAPH_NEED(g);
+  FAPH_BODY(g->solve(path_needed != 0))
+}
 
 int fap_host_solve_subgraph(fap::fapGraph *g, int id, int path_needed) {
+  FAPH_NEED(g);
   FAPH_BODY({
     if (g->solveSubGraph(id, path_needed != 0) != 0) throw fap::fapError(FAP_ERR_INVALID, "bad part id");
   })
 }
 
-int fap_host_current_subgraph(fap::fapGraph *g) { return g->getCurrentSubGraphId(); }
+int fap_host_current_subgraph(fap::fapGraph *g) {
+  FAPH_NEED(g);
+  return g->getCurrentSubGraphId();
+}
 
 int fap_host_subgraph_distance(fap::fapGraph *g, int id, float *out) {
+  FAPH_NEED(g && out);
   FAPH_BODY({
     auto v = g->getSubGraphDistance(id);
     std::memcpy(out, v.data(), v.size() * sizeof(float));
@@ -785,6 +823,7 @@ int fap_host_subgraph_distance(fap::fapGraph *g, int id, float *out) {
 }
 
 int fap_host_all_distance(fap::fapGraph *g, float *out) {
+  FAPH_NEED(g && out);
   FAPH_BODY({
     auto v = g->getAllDistance();
     std::memcpy(out, v.data(), v.size() * sizeof(float));
@@ -792,6 +831,7 @@ int fap_host_all_distance(fap::fapGraph *g, float *out) {
 }
 
 int fap_host_distance_from_one_point(fap::fapGraph *g, int v, float *out) {
+  FAPH_NEED(g && out);
   FAPH_BODY({
     auto r = g->getDistanceFromOnePoint(v);
     std::memcpy(out, r.data(), r.size() * sizeof(float));
@@ -799,10 +839,12 @@ int fap_host_distance_from_one_point(fap::fapGraph *g, int v, float *out) {
 }
 
 int fap_host_distance_p2p(fap::fapGraph *g, int from, int to, float *out) {
+  FAPH_NEED(g && out);
   FAPH_BODY(*out = g->getDistanceP2P(from, to))
 }
 
 int fap_host_subgraph_path(fap::fapGraph *g, int id, int32_t *out) {
+  FAPH_NEED(g && out);
   FAPH_BODY({
     auto v = g->getSubGraphPath(id);
     std::memcpy(out, v.data(), v.size() * sizeof(int32_t));
@@ -810,6 +852,7 @@ int fap_host_subgraph_path(fap::fapGraph *g, int id, int32_t *out) {
 }
 
 int fap_host_all_path(fap::fapGraph *g, int32_t *out) {
+  FAPH_NEED(g && out);
   FAPH_BODY({
     auto v = g->getAllPath();
     std::memcpy(out, v.data(), v.size() * sizeof(int32_t));
@@ -817,6 +860,7 @@ int fap_host_all_path(fap::fapGraph *g, int32_t *out) {
 }
 
 int fap_host_path_from_one_point(fap::fapGraph *g, int v, int32_t *out) {
+  FAPH_NEED(g && out);
   FAPH_BODY({
     auto r = g->getPathFromOnePoint(v);
     std::memcpy(out, r.data(), r.size() * sizeof(int32_t));
@@ -824,6 +868,7 @@ int fap_host_path_from_one_point(fap::fapGraph *g, int v, int32_t *out) {
 }
 
 int fap_host_path_p2p(fap::fapGraph *g, int from, int to, int32_t *out, int32_t cap, int32_t *len) {
+  FAPH_NEED(g && len && (out || cap <= 0));
   FAPH_BODY({
     auto r = g->getPathP2P(from, to);
     *len = (int32_t)r.size();
@@ -833,6 +878,7 @@ int fap_host_path_p2p(fap::fapGraph *g, int from, int to, int32_t *out, int32_t 
 }
 
 int fap_host_check_result(fap::fapGraph *g, int id, int *ok) {
+  FAPH_NEED(g && ok);
   FAPH_BODY({
     auto d = g->getSubGraphDistance(id);
     auto src = g->getSubGraphIndex(id);
@@ -843,6 +889,6 @@ int fap_host_check_result(fap::fapGraph *g, int id, int *ok) {
   })
 }
 
-fap_dgraph *fap_host_device_graph(fap::fapGraph *g) { return g->deviceGraph(); }
+fap_dgraph *fap_host_device_graph(fap::fapGraph *g) { return g ? g->deviceGraph() : nullptr; }
 
 }  // extern "C"

@@ -2,6 +2,7 @@
 METIS partition, boundary detection and renumbering must reproduce the
 reference's CSR, graph_id and st2ed exactly (golden fixtures made by the
 reference itself)."""
+import ctypes
 import os
 import tempfile
 
@@ -177,3 +178,45 @@ def test_binary_file_with_valid_checksum_but_bad_contents_is_an_io_error():
         with open(path, "wb") as f:
             f.write(body + _fnv1a64(body).to_bytes(8, "little"))
         assert fapGraph.load(path).num_vertexs == n
+
+
+def test_host_wrappers_refuse_null_arguments():
+    """Every C wrapper of fapGraph checks its pointers: NULL is
+    FAP_ERR_INVALID with a message, never a crash (no GPU needed)."""
+    lib = L.lib()
+    calls = [
+        lambda: lib.fap_host_sizes(None, None),
+        lambda: lib.fap_host_csr(None, None, None, None),
+        lambda: lib.fap_host_graph_id(None, None),
+        lambda: lib.fap_host_mapping(None, None),
+        lambda: lib.fap_host_parts(None, None, None, None),
+        lambda: lib.fap_host_precondition(None),
+        lambda: lib.fap_host_is_split(None),
+        lambda: lib.fap_host_dtype(None),
+        lambda: lib.fap_host_set_partition(None, None),
+        lambda: lib.fap_host_set_options(None, 0, 0, 0),
+        lambda: lib.fap_host_solve(None, 0),
+        lambda: lib.fap_host_solve_subgraph(None, 1, 0),
+        lambda: lib.fap_host_current_subgraph(None),
+        lambda: lib.fap_host_subgraph_distance(None, 1, None),
+        lambda: lib.fap_host_all_distance(None, None),
+        lambda: lib.fap_host_distance_from_one_point(None, 0, None),
+        lambda: lib.fap_host_distance_p2p(None, 0, 0, None),
+        lambda: lib.fap_host_subgraph_path(None, 1, None),
+        lambda: lib.fap_host_all_path(None, None),
+        lambda: lib.fap_host_path_from_one_point(None, 0, None),
+        lambda: lib.fap_host_path_p2p(None, 0, 0, None, 0, None),
+        lambda: lib.fap_host_check_result(None, 1, None),
+        lambda: lib.fap_host_flags(None, None, None),
+        lambda: lib.fap_host_save(None, None),
+        lambda: lib.fap_host_load(None, None),
+        lambda: lib.fap_host_from_mtx(None, 0, 0, 2, None),
+        lambda: lib.fap_host_from_csr(4, 0, None, None, None, 2, 0, None),
+    ]
+    for i, call in enumerate(calls):
+        assert call() == L.FAP_ERR_INVALID, i
+        assert lib.fap_host_last_error()
+    assert lib.fap_host_device_graph(None) is None
+    out = ctypes.c_void_p()
+    ro = np.zeros(1, np.int32)
+    assert lib.fap_host_from_csr(0, 0, L.ptr(ro), None, None, 1, 0, ctypes.byref(out)) == L.FAP_ERR_INVALID
