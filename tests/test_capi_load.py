@@ -85,3 +85,47 @@ def test_server_without_gpu_fails_loudly():
     assert L.lib().fap_server_submit(None, 0, 0, None, 1, None, None, None) == L.FAP_ERR_INVALID
     assert L.lib().fap_server_drain(None) == L.FAP_ERR_INVALID
     assert L.lib().fap_server_destroy(None) == L.FAP_OK
+
+
+def test_entry_points_refuse_null_handles_without_a_gpu():
+    """NULL handles and output pointers come back as FAP_ERR_INVALID with a
+    message before any device work, so these run without a GPU."""
+    lib = L.lib()
+    calls = [
+        lambda: lib.fap_ctx_create(0, None),
+        lambda: lib.fap_ctx_set_stream(None, None),
+        lambda: lib.fap_ctx_get_stream(None, None),
+        lambda: lib.fap_ctx_sync(None),
+        lambda: lib.fap_graph_create(None, 4, 0, None, None, None, -1, None),
+        lambda: lib.fap_graph_set_parts(None, 1, None, None, None, None, None),
+        lambda: lib.fap_graph_reserve(None, 0),
+        lambda: lib.fap_solve(None, None, 0, 1),
+        lambda: lib.fap_graph_check(None),
+        lambda: lib.fap_graph_last_timing(None, None),
+        lambda: lib.fap_graph_last_launches(None, None),
+        lambda: lib.fap_graph_block(None, 1, None, None, None),
+        lambda: lib.fap_graph_copy_block(None, 1, None, 0),
+        lambda: lib.fap_graph_path_block(None, 1, None, None, None),
+        lambda: lib.fap_graph_copy_path_block(None, 1, None),
+        lambda: lib.fap_graph_block_checksums(None, 1, None),
+        lambda: lib.fap_graph_checksums_async(None, 1, None),
+        lambda: lib.fap_graph_status_async(None, None),
+        lambda: lib.fap_op_floyd(None, 0, 4, None, 4),
+        lambda: lib.fap_op_minplus(None, 0, 1, 1, 1, None, 1, None, 1, None, 1),
+        lambda: lib.fap_graph_sssp_rows(None, None, 1, None),
+        lambda: lib.fap_graph_set_param(None, None, 0.0),
+        lambda: lib.fap_graph_release(None),
+        lambda: lib.fap_graph_device_bytes(None, None),
+        lambda: lib.fap_graph_cache_build(None),
+        lambda: lib.fap_graph_cache_rebuild(None),
+        lambda: lib.fap_graph_cache_timing(None, None),
+        lambda: lib.fap_graph_cache_release(None),
+        lambda: lib.fap_graph_cache_bytes(None, None, None),
+        lambda: lib.fap_graph_rows_async(None, None, 1, None),
+    ]
+    for i, call in enumerate(calls):
+        assert call() == L.FAP_ERR_INVALID, i
+        assert L.last_error()
+    assert lib.fap_graph_dtype(None) == L.FAP_ERR_INVALID
+    assert lib.fap_graph_resident(None, 1) == 0
+    assert lib.fap_ctx_destroy(None) == 0 and lib.fap_graph_destroy(None) == 0
