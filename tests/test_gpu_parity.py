@@ -195,8 +195,10 @@ def test_partition_with_a_cross_arc_end_outside_the_boundary_block_is_refused(cu
     dg.set_parts(case["K"], case["graph_id"], case["st2ed"], case["ver_num"], case["ver_offset"],
                  case["bdy_num"])
     dg.solve(mode=FAP_MODE_BATCHED)
-    cs = np.concatenate([dg.block_checksums(p) for p in range(1, case["K"] + 1)])
-    np.testing.assert_array_equal(cs, case["row_checksums"])
+    for q in range(1, case["K"] + 1):
+        off = int(case["ver_offset"][q])
+        blk = dg.copy_block(q, out_dtype=FAP_DTYPE_F32)
+        assert_dist_equal(blk, case["dist"][off:off + blk.shape[0]], True)
 
 
 def test_sssp_delta_stepping_same_result(cuda_ok):
