@@ -529,7 +529,10 @@ extern "C" int fap_graph_set_parts(fap_dgraph *G, int32_t K, const int32_t *grap
                     u, v);
     }
   DeviceGuard g(G->ctx->device);
-  G->K = K;
+  // The graph has no parts until every step below has succeeded: a failure
+  // part-way (an allocation, a copy) leaves K = 0, so a later solve is
+  // refused instead of reading half-updated tables.
+  G->K = 0;
   G->gid.assign(graph_id, graph_id + n);
   G->st2ed.assign(st2ed, st2ed + n);
   G->ed2st = std::move(ed2st);
@@ -595,6 +598,7 @@ extern "C" int fap_graph_set_parts(fap_dgraph *G, int32_t K, const int32_t *grap
   FAP_CK(cudaMemcpy(G->ro_s.p, ro_s.data(), (size_t)(n + 1) * 4, cudaMemcpyHostToDevice));
   FAP_CK(cudaMemcpy(G->col_s.p, col_s.data(), col_s.size() * 4, cudaMemcpyHostToDevice));
   FAP_CK(cudaMemcpy(G->w_s.p, w_s.data(), w_s.size() * 4, cudaMemcpyHostToDevice));
+  G->K = K;
   return FAP_OK;
 } catch (...) {
   return fail_exception();
