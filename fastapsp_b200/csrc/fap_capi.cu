@@ -610,6 +610,13 @@ extern "C" int fap_graph_reserve(fap_dgraph *G, int64_t max_rows) try {
   DeviceGuard g(G->ctx->device);
   cudaStreamSynchronize(G->ctx->stream);
   const size_t bytes = (size_t)max_rows * (size_t)G->ldD * 4;
+  // No block is resident while the buffers change: a failed allocation
+  // below leaves max_rows = 0 and no part placed, so the next solve
+  // reserves again instead of writing through a released buffer.
+  G->max_rows = 0;
+  std::fill(G->row_base.begin(), G->row_base.end(), -1);
+  G->last_ids.clear();
+  G->epoch++;
   if (G->D.bytes < bytes) {
     G->D.release();
     FAP_TRY(G->D.ensure(bytes));
@@ -619,9 +626,6 @@ extern "C" int fap_graph_reserve(fap_dgraph *G, int64_t max_rows) try {
     FAP_TRY(G->P.ensure(bytes));
   }
   G->max_rows = max_rows;
-  std::fill(G->row_base.begin(), G->row_base.end(), -1);
-  G->last_ids.clear();
-  G->epoch++;
   return FAP_OK;
 } catch (...) {
   return fail_exception();
