@@ -2084,6 +2084,7 @@ extern "C" int fap_graph_cache_build(fap_dgraph *G) try {
   if (rc != FAP_OK) cache_drop(G);
   return rc;
 } catch (...) {
+  if (G) cache_drop(G);  // a half-built cache is not kept
   return fail_exception();
 }
 
@@ -2095,6 +2096,7 @@ extern "C" int fap_graph_cache_rebuild(fap_dgraph *G) try {
   if (rc != FAP_OK) cache_drop(G);
   return rc;
 } catch (...) {
+  if (G) cache_drop(G);  // a half-built cache is not kept
   return fail_exception();
 }
 
