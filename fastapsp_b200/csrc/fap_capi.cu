@@ -841,6 +841,9 @@ int expand_bgraph(fap_dgraph *G, const PartDesc *dp, int np, int max_s, const T 
 int prepare_batch(fap_dgraph *G, const std::vector<int32_t> &ids, bool cached, bool bmethod) {
   const bool same = (ids == G->last_ids) && (cached == G->last_cached) && (bmethod == G->last_bmethod);
   if (same) return FAP_OK;
+  // The descriptors change from here on: until they are complete no batch
+  // counts as prepared, so a failure below forces a full rebuild next time.
+  G->last_ids.clear();
   const int64_t n = G->n;
   const bool full = (G->max_rows == n);
   // rows
