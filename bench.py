@@ -223,17 +223,22 @@ def cpu_procs(requested):
     return max(1, p)
 
 
-def run_reference_sample(wl, parts_per_proc, procs, timeout=900):
+def run_reference_sample(wl, parts_per_proc, procs, timeout=900, extra=None, partition_file=None):
     """Runs the reference CPU path on `procs` concurrent processes, process i
-    solving parts_per_proc[i] in order.  Returns (kind, per-process list of
+    solving parts_per_proc[i] in order (extra[i]: more arguments of process
+    i, e.g. output files; partition_file: a shared partition in place of the
+    reference's METIS call).  Returns (kind, per-process list of
     (part, rows, entries, seconds))."""
     from oracle import oracle as O
     kind = "reference" if O.ref_available() else "port"
     env = dict(os.environ, OMP_NUM_THREADS="1")
+    if partition_file:
+        env["FAP_PARTITION_FILE"] = os.path.abspath(partition_file)
     if kind == "reference":
         cmds = [[O.REF_BIN, "--dir", wl.root, "-f", wl.name, "-k", str(wl.K),
                  "-direct", str(int(wl.edges.directed)), "-weight", str(int(wl.edges.weighted)),
-                 "--parts", ",".join(map(str, pp)), "--quiet"] for pp in parts_per_proc]
+                 "--parts", ",".join(map(str, pp)), "--quiet"] + list((extra or {}).get(i, []))
+                for i, pp in enumerate(parts_per_proc)]
     else:
         script = os.path.join(ROOT, "oracle", "port_cli.py")
         cmds = [[sys.executable, script, "--dir", wl.root, "-f", wl.name, "-k", str(wl.K),
@@ -252,6 +257,74 @@ def run_reference_sample(wl, parts_per_proc, procs, timeout=900):
     return kind, out
 
 
+PARITY_FLOAT_PARTS = 4   # float32 workloads: whole blocks compared for this many parts
+FLOAT_RTOL = 1e-5        # float32 bar: |d - ref| <= 1e-5 |ref|, reachability exact
+
+
+def gpu_parity_blocks(dg, groups, parts, dtype, staged, mode):
+    """What the GPU produced for the parity sample: per-row checksums of each
+    part's block (int32) or the blocks themselves (float32, the first
+    PARITY_FLOAT_PARTS parts).  Blocks of the timed run are still resident
+    when the job is one group; otherwise the groups holding sampled parts
+    are solved again (untimed) the way the timed loop solves them."""
+    from fastapsp_b200 import FAP_DTYPE_F32
+    want = set(parts if dtype == 0 else parts[:PARITY_FLOAT_PARTS])
+    out = {}
+    for grp in groups:
+        hit = [p for p in grp if p in want]
+        if not hit:
+            continue
+        if len(groups) > 1:
+            dg.solve(grp, mode)
+        for p in hit:
+            out[p] = (dg.block_checksums(p) if dtype == 0
+                      else dg.copy_block(p, out_dtype=FAP_DTYPE_F32))
+    dg.check()
+    return out
+
+
+def compare_parity(wl, gpu, ref_files, dtype, st2ed, ref_meta):
+    """Compares the GPU's blocks of the sampled parts with the reference
+    binary's output for the same parts under the same partition."""
+    rows = mism = 0
+    worst = 0.0
+    reach_mism = 0
+    n = wl.n
+    for p, f in ref_files.items():
+        if p not in gpu:
+            continue
+        if dtype == 0:
+            ref = np.fromfile(f, dtype=np.uint64)
+            got = gpu[p]
+            rows += int(got.size)
+            mism += int(got.size) if ref.size != got.size else int((ref != got).sum())
+        else:
+            ref = np.fromfile(f, dtype=np.float32).reshape(-1, n)
+            got = gpu[p]
+            rows += int(got.shape[0])
+            inf_r, inf_g = ref >= np.float32(1e8), got >= np.float32(1e8)
+            reach_mism += int((inf_r != inf_g).sum())
+            fin = ~inf_r & ~inf_g
+            err = np.abs(got[fin].astype(np.float64) - ref[fin]) / np.maximum(np.abs(ref[fin]), 1e-30)
+            e = float(err.max()) if err.size else 0.0
+            worst = max(worst, e)
+            mism += int((err > FLOAT_RTOL).sum()) + int((inf_r != inf_g).sum())
+    res = {"config": wl.name, "parts": len([p for p in ref_files if p in gpu]), "rows": rows,
+           "mismatches": mism,
+           "st2ed_equal": (bool(np.array_equal(ref_meta.st2ed, st2ed))
+                           if ref_meta is not None else None),
+           "partition": "the GPU run's partition given to the reference binary (FAP_PARTITION_FILE)"}
+    if dtype == 0:
+        res["rule"] = "bit-exact int32: per-row checksums sum_j uint32(d[r][j])*(2j+1) mod 2^64"
+        res["mismatches_unit"] = "rows"
+    else:
+        res["rule"] = f"float32: |d - ref| <= {FLOAT_RTOL} |ref|, reachability exact"
+        res["mismatches_unit"] = "entries"
+        res["max_rel_err"] = worst
+        res["reachability_mismatches"] = reach_mism
+    return res
+
+
 def sample_parts(K, count, seed):
     rng = np.random.default_rng(seed)
     return [int(x) + 1 for x in rng.permutation(K)[:count]]
@@ -260,19 +333,74 @@ def sample_parts(K, count, seed):
 # ---------------------------------------------------------------------------
 # reference arm
 # ---------------------------------------------------------------------------
+def reference_partition(wf, workdir):
+    """The reference binary's own host preprocessing of the workload file
+    (MatrixMarket reader, METIS, findBoundry, sort_and_encode): its CSR,
+    partition and renumbering, read back from `fap_ref --parts none --meta`.
+    Returns None when the reference binary is absent."""
+    from oracle import oracle as O
+    if not O.ref_available():
+        return None
+    meta = os.path.join(workdir, "ref_meta.bin")
+    O.run_ref(wf.root, wf.name, wf.edges.directed, wf.edges.weighted, wf.K, parts="none",
+              meta_out=meta, threads=1, timeout=900)
+    m = O.read_meta(meta)
+    os.unlink(meta)
+    return m
+
+
+def describe_meta(name, K, directed, m):
+    """The workload description of `Workload.describe`, from the reference's
+    own preprocessing."""
+    vn, bn = m.ver_num[1:], m.bdy_num[1:]
+    return {"workload": name, "n": int(m.n), "arcs": int(m.row_offset[-1]), "K": int(K),
+            "directed": bool(directed), "avg_degree": round(float(m.row_offset[-1]) / m.n, 3),
+            "part_size": [int(vn.min()), int(np.median(vn)), int(vn.max())],
+            "boundary": [int(bn.min()), int(np.median(bn)), int(bn.max()), int(bn.sum())]}
+
+
+def common_config(desc, n_gpus):
+    """The `config` both arms print: the workload's description, the
+    parallelism and what keeps L2 from serving the timed steps."""
+    n = int(desc["n"])
+    return {**desc, "parallelism": f"parts sharded x{n_gpus}",
+            "l2": (f"outputs larger than L2: each step writes {4 * n * n / 1e9:.1f} GB of "
+                   "distances; the GPU arm also writes a 256 MB buffer between timed steps, "
+                   "outside the events")}
+
+
+def product_library_loaded():
+    """Whether this process has mapped the product's shared library."""
+    try:
+        with open("/proc/self/maps") as f:
+            return any("libfap_b200.so" in ln for ln in f)
+    except OSError:
+        return None
+
+
 def main_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return
+    # Only the seeded generator and the MatrixMarket writer run here: the
+    # reference binary reads the file, partitions it with METIS and renumbers
+    # it itself, so this process never loads the product's library.
     from fastapsp_b200 import workloads
-    wl = workloads.load(args.workload)
+    wf = workloads.write(args.workload)
+    with tempfile.TemporaryDirectory() as tmp:
+        meta = reference_partition(wf, tmp)
+    if meta is not None:
+        config = common_config(describe_meta(wf.name, wf.K, wf.edges.directed, meta), args.gpus)
+    else:
+        config = common_config({"workload": wf.name, "n": wf.n, "K": wf.K,
+                                "directed": wf.edges.directed}, args.gpus)
     P = cpu_procs(args.cpu_procs)
     steps = args.warmup + args.steps
     need = P * steps
-    order = [int(x) + 1 for x in np.random.default_rng(7).permutation(wl.K)]
-    order = (order * (need // wl.K + 1))[:need]
+    order = [int(x) + 1 for x in np.random.default_rng(7).permutation(wf.K)]
+    order = (order * (need // wf.K + 1))[:need]
     per = [order[i::P] for i in range(P)]
-    kind, res = run_reference_sample(wl, per, P)
+    kind, res = run_reference_sample(wf, per, P)
     tot_entries, tot_time, step_ms = 0, 0.0, []
     for s in range(args.warmup, steps):
         ent = sum(r[s][2] for r in res)
@@ -282,15 +410,18 @@ def main_reference(args):
         step_ms.append(sec * 1e3)
     value = tot_entries / tot_time
     sample = (f"{args.steps} timed steps x {P} processes x 1 part "
-              f"({wl.name}, K={wl.K}); step time = slowest process")
+              f"({wf.name}, K={wf.K}); step time = slowest process")
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": float(np.mean(step_ms)), "higher_is_better": True,
         "impl": "reference", "scaling": "strong", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic", "config": {**wl.describe(), "mode": "reference CPU path"},
+        "data": "synthetic", "config": config,
+        "solve": {"mode": "reference CPU path (oracle/_ref/fap_ref: the reference's fap.cpp, "
+                          "fapGraph::run per part)"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": P, "kind": kind,
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "product_library_loaded": product_library_loaded(),
     }
     emit(line)
 
@@ -612,6 +743,13 @@ def main_fap(args):
     value = total_entries * args.steps / (max_ms * 1e-3)
     st = np.mean(np.stack(stages), 0)  # [sssp, gather, floyd, minplus, total]
     stage1_used = dg.stage1_name()
+
+    # ---- parity sample: the timed run's blocks of the parts that the CPU
+    # baseline leg below has the reference binary solve (rank 0, N=1) ----
+    cpu_leg = rank == 0 and world == 1 and not args.no_cpu_baseline
+    parity_parts = sample_parts(wl.K, cpu_procs(args.cpu_procs), seed=11) if cpu_leg else []
+    gpu_par = (gpu_parity_blocks(dg, groups, parity_parts, dtype, staged, FAP_MODE_BATCHED)
+               if parity_parts else {})
     log(f"batched: {ms_per_step:.3f} ms/step, stages {np.round(st, 3).tolist()}, "
         f"{value:.4g} entries/s")
 
@@ -742,17 +880,40 @@ def main_fap(args):
         torch.cuda.empty_cache()
         serving = run_serving(args, local)
 
-    # ---- CPU baseline (rank 0, N=1 only) ----
+    # ---- CPU baseline (rank 0, N=1 only) and parity of the same parts ----
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    parity = None
+    if cpu_leg:
+        from oracle import oracle as O
         P = cpu_procs(args.cpu_procs)
-        parts = sample_parts(wl.K, P, seed=11)
-        kind, res = run_reference_sample(wl, [[p] for p in parts], P)
+        parts = parity_parts
+        with tempfile.TemporaryDirectory() as tmp:
+            # the GPU run's partition (0-based part ids), so that both solve
+            # the same parts; process 0 also dumps the reference's renumbering
+            pfile = os.path.join(tmp, "partition.bin")
+            (np.asarray(gid, dtype=np.int64) - 1).astype(np.int32).tofile(pfile)
+            meta_f = os.path.join(tmp, "meta.bin")
+            extra, files = {0: ["--meta", meta_f]}, {}
+            for i, p in enumerate(parts):
+                if dtype == 0:
+                    files[p] = os.path.join(tmp, f"rowsum_{p}.bin")
+                    extra.setdefault(i, []).extend(["--rowsum", files[p]])
+                elif i < PARITY_FLOAT_PARTS:
+                    files[p] = os.path.join(tmp, f"dist_{p}.bin")
+                    extra.setdefault(i, []).extend(["--dist", files[p]])
+            kind, res = run_reference_sample(wl, [[p] for p in parts], P, extra=extra,
+                                             partition_file=pfile)
+            if kind == "reference":
+                parity = compare_parity(wl, gpu_par, files, dtype, st2ed, O.read_meta(meta_f))
+            else:
+                parity = {"unavailable": "reference binary absent (C restatement timed instead)"}
+        del gpu_par
         ent = sum(r[0][2] for r in res)
         sec = max(r[0][3] for r in res)
         cpu = {"value": ent / sec, "unit": UNIT, "cores": P, "kind": kind,
                "sample": f"{P} parts of {wl.name} (K={wl.K}), one process per core, "
                          f"1 thread each; time = slowest process ({sec:.2f} s)"}
+        log(f"parity vs reference on {len(files)} sampled parts: {parity}")
 
     if rank == 0:
         line = {
@@ -761,20 +922,18 @@ def main_fap(args):
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
             "dtype": "int32" if dtype == 0 else "f32",
             "data": wl.data_description(),
-            "config": {**wl.describe(), "mode": "batched", "stage1": stage1_used,
-                       "parallelism": f"parts sharded x{world}",
-                       "groups": len(groups),
-                       "stage_cache": ({"note": "stages 1-2 of every part once per step (resident cache), "
-                                                "then each group's min-plus merge",
-                                        "phases_ms": np.round(np.mean(cache_phases, 0), 3).tolist(),
-                                        "phases": ("local closures, boundary-graph closure, expansion, fix-up"
-                                                   if "boundary graph" in stage1_used else
-                                                   "SSSP, gather, Floyd, -")}
-                                       if staged and cache_phases else None),
-                       "sssp_delta": {"value": tuned["delta"], "factor_of_mean_weight": tuned["factor"],
-                                      "bucket": tuned["key"], "from_cache": tuned["cached"]},
-                       "l2": "256 MB buffer written between timed steps (outside the events); "
-                             f"each step also writes {4 * n * n / 1e9:.1f} GB of output"},
+            "config": common_config(wl.describe(), world),
+            "solve": {"mode": "batched", "stage1": stage1_used,
+                      "groups": len(groups),
+                      "stage_cache": ({"note": "stages 1-2 of every part once per step (resident cache), "
+                                               "then each group's min-plus merge",
+                                       "phases_ms": np.round(np.mean(cache_phases, 0), 3).tolist(),
+                                       "phases": ("local closures, boundary-graph closure, expansion, fix-up"
+                                                  if "boundary graph" in stage1_used else
+                                                  "SSSP, gather, Floyd, -")}
+                                      if staged and cache_phases else None),
+                      "sssp_delta": {"value": tuned["delta"], "factor_of_mean_weight": tuned["factor"],
+                                     "bucket": tuned["key"], "from_cache": tuned["cached"]}},
             "plain": {"value": plain_value, "ms_per_step": plain_max / max(len(plain_ms), 1),
                       "steps": len(plain_ms)},
             "batched_over_plain": (value / plain_value) if plain_value else None,
@@ -783,6 +942,7 @@ def main_fap(args):
             "roofline": roof, "stage_roofline": stage_roof,
             "relax_peak_grelax_s": peak_grelax,
             "cpu_baseline": cpu,
+            "parity": parity,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "steps": len(e2e_s),
                     "s_per_step": e2e_max / max(len(e2e_s), 1)},

@@ -24,7 +24,38 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <atomic>
+#include <map>
+#include <mutex>
+#include <utility>
+
 namespace fapb {
+
+// ---------------------------------------------------------------------------
+// Launch shapes: grid sizes are multiples of the current device's SM count,
+// queried once per device.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int kMaxSmDevices = 64;
+std::atomic<int> g_sm_count[kMaxSmDevices];
+
+int device_sm_count() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxSmDevices) {
+    cudaGetLastError();
+    return 148;
+  }
+  int v = g_sm_count[dev].load(std::memory_order_relaxed);
+  if (v <= 0) {
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) {
+      cudaGetLastError();
+      v = 148;
+    }
+    g_sm_count[dev].store(v, std::memory_order_relaxed);
+  }
+  return v;
+}
+}  // namespace
 
 // ---------------------------------------------------------------------------
 // Tensor maps (host).  cuTensorMapEncodeTiled comes from the driver through
@@ -156,19 +187,24 @@ cudaError_t launch_gather(const PartDesc *parts, int nparts, int max_ldf, const 
 // ---------------------------------------------------------------------------
 namespace {
 int sssp_resident_ctas(int n) {
-  static int cached_n = -1, cached = 0;
-  if (n == cached_n) return cached;
-  int dev = 0, sms = 0, per_sm = 0;
+  // resident frontier-SSSP CTAs per (device, n): shared memory grows with n
+  static std::mutex mu;
+  static std::map<std::pair<int, int>, int> cache;
+  int dev = 0;
   cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  std::lock_guard<std::mutex> lock(mu);
+  const auto key = std::make_pair(dev, n);
+  const auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  int per_sm = 0;
   const size_t smem = sssp_smem_bytes(n);
   cudaFuncSetAttribute(sssp_frontier_kernel<int32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   cudaFuncSetAttribute(sssp_frontier_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sssp_frontier_kernel<int32_t>, kSsspThreads, smem);
   cudaGetLastError();
-  cached_n = n;
-  cached = std::max(1, per_sm) * std::max(1, sms);
-  return cached;
+  const int v = std::max(1, per_sm) * device_sm_count();
+  cache[key] = v;
+  return v;
 }
 }  // namespace
 
@@ -343,7 +379,7 @@ cudaError_t launch_msbf(const MsbfItem *items, int nitems, const int32_t *tro, c
   if (ztiles < 1 || ztiles > 64) return cudaErrorInvalidValue;
   const int64_t words = ceil_div(n, 32);
   uint32_t *act_a = act, *act_b = act + ztiles * words;
-  const int iter_blocks = 148 * 8;
+  const int iter_blocks = device_sm_count() * 8;
   constexpr int kChunk = 4;  // iterations between convergence checks
   for (int s0 = 0; s0 < num_sources; s0 += ztiles * kMsbfS) {
     const int z = (int)std::min<int64_t>(ztiles, ceil_div(num_sources - s0, kMsbfS));  // tiles side by side
@@ -924,7 +960,7 @@ cudaError_t launch_minplus_thin(const PartDesc *parts, const int32_t *thin_parts
   // chunks of whole kMinplusBM blocks when the column strips alone are few.
   const int64_t col_ctas = ceil_div(ldD, kThinCols) * (int64_t)nthin;
   const int64_t blocks = ceil_div(max_m, kMinplusBM);
-  const int64_t want = 4 * 148;
+  const int64_t want = 4 * (int64_t)device_sm_count();
   const int64_t zc = std::min<int64_t>(blocks, std::max<int64_t>(1, ceil_div(want, col_ctas)));
   const int row_chunk = (int)(ceil_div(blocks, zc) * kMinplusBM);
   const unsigned gz = (unsigned)ceil_div(max_m, row_chunk);
@@ -1225,7 +1261,7 @@ cudaError_t launch_bgraph(const PartDesc *parts, int nparts, int max_b, const T 
     bgraph_local_kernel<T><<<dim3(max_b, nparts), 128, 0, stream>>>(parts, F, dB, ldB);
     *launches += 1;
   }
-  const int blocks = (int)std::min<int64_t>(ceil_div(n, 256), 148 * 8);
+  const int blocks = (int)std::min<int64_t>(ceil_div(n, 256), device_sm_count() * 8);
   bgraph_cross_kernel<T><<<blocks, 256, 0, stream>>>(row_offset, col, w, n, graph_id, ed2st, bpart, dB, ldB);
   *launches += 1;
   return cudaGetLastError();
@@ -1303,7 +1339,7 @@ cudaError_t launch_bdy_expand_rg(const int64_t *rows, int nrows, const BPart *bp
   // Enough CTAs for about 16 per SM, each looping over columns so that the
   // rows' dB entries are staged only once per CTA.
   const int64_t ny = ceil_div(nrows, RG);
-  const int bx = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(ldD, 256), ceil_div(148 * 16, ny)));
+  const int bx = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(ldD, 256), ceil_div((int64_t)device_sm_count() * 16, ny)));
   kern<<<dim3(bx, (unsigned)ny), 256, smem, stream>>>(
       rows, nrows, bpart, graph_id, ed2st, n, dB, ldB, nbB, F, D, ldD, FB, ldFB);
   *launches += 1;
@@ -1600,7 +1636,7 @@ cudaError_t launch_bgraph_bf(const PartDesc *parts, int nparts, int max_b, const
   for (int s0 = 0; s0 < nb; s0 += ztiles * kMsbfS) {
     const int z = (int)std::min<int64_t>(ztiles, ceil_div(nb - s0, kMsbfS));  // tiles side by side
     const dim3 lgrid((unsigned)ceil_div(std::max(max_b, 1), C::BN), (unsigned)nparts, (unsigned)z);
-    const int xblocks = 148 * 5;  // about the resident limit at 256 threads
+    const int xblocks = device_sm_count() * 5;  // about the resident limit at 256 threads
     e = launch_fill<T>(Dt, (int64_t)z * nb, kMsbfS, kMsbfS, Dist<T>::inf(), stream, launches);
     if (e == cudaSuccess) e = cudaMemsetAsync(wl_count, 0, 2 * sizeof(int), stream);
     if (e != cudaSuccess) return e;
@@ -2090,7 +2126,7 @@ cudaError_t launch_fill(T *p, int64_t rows, int64_t cols, int64_t ld, T v, cudaS
                         int64_t *launches) {
   if (rows <= 0 || cols <= 0) return cudaSuccess;
   const int64_t total = rows * cols;
-  const int blocks = (int)std::min<int64_t>(ceil_div(total, 256), 148 * 32);
+  const int blocks = (int)std::min<int64_t>(ceil_div(total, 256), device_sm_count() * 32);
   fill_kernel<T><<<blocks, 256, 0, stream>>>(p, rows, cols, ld, v);
   *launches += 1;
   return cudaGetLastError();
@@ -2149,7 +2185,7 @@ __global__ void i32_to_f32_kernel(const int32_t *__restrict__ src, int64_t rows,
 cudaError_t launch_i32_to_f32(const int32_t *src, int64_t rows, int64_t n, int64_t ld, float *dst,
                               cudaStream_t stream, int64_t *launches) {
   if (rows <= 0 || n <= 0) return cudaSuccess;
-  const int blocks = (int)std::min<int64_t>(ceil_div(rows * n, 256), 148 * 32);
+  const int blocks = (int)std::min<int64_t>(ceil_div(rows * n, 256), device_sm_count() * 32);
   i32_to_f32_kernel<<<blocks, 256, 0, stream>>>(src, rows, n, ld, dst);
   *launches += 1;
   return cudaGetLastError();

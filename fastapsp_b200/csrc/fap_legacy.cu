@@ -46,6 +46,154 @@ struct Dev {
   }
 };
 
+// ---------------------------------------------------------------------------
+// Predecessor-carrying forms.  They compute in float32 on the GPU with the
+// reference CPU path's own arithmetic: one IEEE single-precision add and a
+// strict comparison per candidate, candidates in the reference's order, so
+// distances and predecessors are bit-identical to it (also on ties).
+// ---------------------------------------------------------------------------
+constexpr int kPT = 32;   // output tile kPT x kPT; block kPT x 8 threads, 4 rows each
+
+// C[i][j], P[i][j]: the first strict minimum, in the order "start" then
+// k = 0, 1, ..., k-1, of the candidates A[i][k] + B[k][j], where a candidate
+// that wins brings the predecessor Bp[k][j].  start = (C0[i][j], P0[i][j])
+// when C0 is given (res = min(res, A (x) B), fap/kernel/floyd.h:86-102 and
+// the panels :51-84), else (1e8, -1) (fap/kernel/minplus.h:51-65).
+__global__ void __launch_bounds__(kPT * 8)
+legacy_minplus_path_kernel(const float *__restrict__ A, const float *__restrict__ B,
+                           const int *__restrict__ Bp, const float *__restrict__ C0,
+                           const int *__restrict__ P0, float *__restrict__ C, int *__restrict__ P,
+                           int m, int n, int k) {
+  __shared__ float As[kPT][kPT + 1];
+  __shared__ float Bs[kPT][kPT];
+  __shared__ int Ps[kPT][kPT];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int64_t i0 = (int64_t)blockIdx.y * kPT;
+  const int64_t j = (int64_t)blockIdx.x * kPT + tx;
+  float v[4];
+  int p[4];
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int64_t i = i0 + ty + 8 * q;
+    v[q] = 1e8f;
+    p[q] = -1;
+    if (C0 != nullptr && i < m && j < n) {
+      v[q] = C0[i * n + j];
+      p[q] = P0[i * n + j];
+    }
+  }
+  for (int k0 = 0; k0 < k; k0 += kPT) {
+    const int kc = min(kPT, k - k0);
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int r = ty + 8 * q;
+      const int64_t i = i0 + r;
+      As[r][tx] = (i < m && tx < kc) ? A[i * k + k0 + tx] : 0.0f;
+      const bool ok = r < kc && j < n;
+      Bs[r][tx] = ok ? B[(int64_t)(k0 + r) * n + j] : 0.0f;
+      Ps[r][tx] = ok ? Bp[(int64_t)(k0 + r) * n + j] : -1;
+    }
+    __syncthreads();
+    for (int t = 0; t < kc; t++) {
+      const float b = Bs[t][tx];
+      const int bp = Ps[t][tx];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const float c = As[ty + 8 * q][t] + b;
+        if (v[q] > c) {
+          v[q] = c;
+          p[q] = bp;
+        }
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int64_t i = i0 + ty + 8 * q;
+    if (i < m && j < n) {
+      C[i * n + j] = v[q];
+      P[i * n + j] = p[q];
+    }
+  }
+}
+
+// Pivot k of Floyd-Warshall with predecessors (fap/kernel/floyd.h:38-49):
+// d[i][j] = d[i][k] + d[k][j], path[i][j] = path[k][j] where that is
+// strictly shorter.  With every entry non-negative, row k and column k do
+// not change during pivot k (that needs d[k][k] < 0), so all (i, j) of one
+// pivot may run at once and the result equals the reference's sequential
+// k-i-j loop entry for entry, ties included.
+__global__ void legacy_floyd_step_kernel(float *__restrict__ d, int *__restrict__ path, int n, int k) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const float dkj = d[(int64_t)k * n + j];
+  const int pkj = path[(int64_t)k * n + j];
+  for (int64_t i = blockIdx.y; i < n; i += gridDim.y) {
+    const float c = d[i * n + k] + dkj;
+    if (d[i * n + j] > c) {
+      d[i * n + j] = c;
+      path[i * n + j] = pkj;
+    }
+  }
+}
+
+bool upload(Dev &d, const void *host, size_t bytes) {
+  return d.alloc(bytes) && (bytes == 0 || cudaMemcpy(d.p, host, bytes, cudaMemcpyHostToDevice) == cudaSuccess);
+}
+
+bool cuda_failed(const char *where) {
+  const cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) return false;
+  std::fprintf(stderr, "fap legacy %s: %s\n", where, cudaGetErrorString(e));
+  t_status = FAP_ERR_CUDA;
+  return true;
+}
+
+// res/res_path[m x n] by the rule of legacy_minplus_path_kernel, for host
+// row-major arrays; c0/p0 (start values and predecessors) may be NULL.
+// Every input is uploaded before an output is written, so res may alias
+// mat1, mat2 or c0 and res_path may alias mat2_path or p0.
+void host_minplus_path(const float *mat1, const float *mat2, const int *mat2_path, const float *c0,
+                       const int *p0, float *res, int *res_path, int m, int n, int k, const char *where) {
+  if (m <= 0 || n <= 0) {
+    t_status = FAP_OK;
+    return;
+  }
+  if (k < 0) k = 0;
+  const size_t ca = (size_t)m * k, cb = (size_t)k * n, cc = (size_t)m * n;
+  Dev A, B, Bp, C0, P0, C, P;
+  if (!upload(A, mat1, ca * 4) || !upload(B, mat2, cb * 4) || !upload(Bp, mat2_path, cb * 4) ||
+      (c0 && (!upload(C0, c0, cc * 4) || !upload(P0, p0, cc * 4))) || !C.alloc(cc * 4) ||
+      !P.alloc(cc * 4)) {
+    cudaGetLastError();
+    report(FAP_ERR_NOMEM, where);
+    return;
+  }
+  const dim3 grid((unsigned)((n + kPT - 1) / kPT), (unsigned)((m + kPT - 1) / kPT));
+  if (grid.y > 65535u) {
+    report(FAP_ERR_RANGE, where);
+    return;
+  }
+  legacy_minplus_path_kernel<<<grid, dim3(kPT, 8)>>>(
+      static_cast<const float *>(A.p), static_cast<const float *>(B.p), static_cast<const int *>(Bp.p),
+      c0 ? static_cast<const float *>(C0.p) : nullptr, c0 ? static_cast<const int *>(P0.p) : nullptr,
+      static_cast<float *>(C.p), static_cast<int *>(P.p), m, n, k);
+  if (cuda_failed(where)) return;
+  if (cudaMemcpy(res, C.p, cc * 4, cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(res_path, P.p, cc * 4, cudaMemcpyDeviceToHost) != cudaSuccess) {
+    cuda_failed(where);
+    return;
+  }
+  t_status = FAP_OK;
+}
+
+bool has_negative(const float *v, size_t count) {
+  for (size_t i = 0; i < count; i++)
+    if (!(v[i] >= 0.0f)) return true;
+  return false;
+}
+
 }  // namespace
 
 extern "C" int fap_legacy_last_status(void) { return t_status; }
@@ -74,7 +222,32 @@ void handle_boundry_Nvidia_GPU(float *subGraph, int vertexs, int edges, int bdy_
 }
 
 void floyd_GPU_Nvidia_path(int num_node, float *arc, int *path) {
-  (void)path;
+  if (path != nullptr && num_node > 0) {
+    // with predecessors: one launch per pivot, the reference's k-i-j order
+    const size_t cnt = (size_t)num_node * num_node;
+    if (has_negative(arc, cnt)) {
+      std::fprintf(stderr, "fap legacy floyd_GPU_Nvidia_path: negative or NaN entries\n");
+      t_status = FAP_ERR_INVALID;
+      return;
+    }
+    Dev d, p;
+    if (!upload(d, arc, cnt * 4) || !upload(p, path, cnt * 4)) {
+      cudaGetLastError();
+      report(FAP_ERR_NOMEM, "floyd_GPU_Nvidia_path");
+      return;
+    }
+    const dim3 grid((unsigned)((num_node + 255) / 256), (unsigned)std::min(num_node, 65535));
+    for (int k = 0; k < num_node; k++)
+      legacy_floyd_step_kernel<<<grid, 256>>>(static_cast<float *>(d.p), static_cast<int *>(p.p), num_node, k);
+    if (cuda_failed("floyd_GPU_Nvidia_path")) return;
+    if (cudaMemcpy(arc, d.p, cnt * 4, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(path, p.p, cnt * 4, cudaMemcpyDeviceToHost) != cudaSuccess) {
+      cuda_failed("floyd_GPU_Nvidia_path");
+      return;
+    }
+    t_status = FAP_OK;
+    return;
+  }
   fap_ctx *c = legacy_ctx();
   if (!c) {
     report(FAP_ERR_CUDA, "floyd_GPU_Nvidia_path");
@@ -160,8 +333,10 @@ void host_minplus(const float *mat1, const float *mat2, float *res, int m, int n
 
 void minplus_NVIDIA_path(float *mat1, float *mat2, int *mat2_path, float *res, int *res_path, int m,
                          int n, int k) {
-  (void)mat2_path;
-  (void)res_path;
+  if (mat2_path && res_path) {
+    host_minplus_path(mat1, mat2, mat2_path, nullptr, nullptr, res, res_path, m, n, k, "minplus_NVIDIA_path");
+    return;
+  }
   host_minplus(mat1, mat2, res, m, n, k, "minplus_NVIDIA_path");
 }
 
@@ -173,16 +348,26 @@ void floyd_NVIDIA_GPU(int num_node, float *arc) { floyd_GPU_Nvidia_path(num_node
 
 // Column panel of a blocked Floyd (fap/kernel/floyd.h:106-115): the new
 // panel from the old one and the closed diagonal block, computed out of
-// place as the reference's CUDA kernel intends.
+// place as the reference's CUDA kernel intends.  With paths, each entry
+// starts from its current value and predecessor, as the reference's CPU
+// panel does (floyd_path_A_CPU, fap/kernel/floyd.h:68-84), and takes
+// diag_path[k][j] from the first strictly shorter A[i][k] + diag[k][j].
 void floyd_path_A_Nvidia(float *A, int *A_path, const int row, const int col, float *diag, int *diag_path) {
-  (void)A_path;
-  (void)diag_path;
+  if (A_path && diag_path) {
+    host_minplus_path(A, diag, diag_path, A, A_path, A, A_path, row, col, col, "floyd_path_A_Nvidia");
+    return;
+  }
   host_minplus(A, diag, A, row, col, col, "floyd_path_A_Nvidia");
 }
 
-// Row panel of a blocked Floyd (fap/kernel/floyd.h:118-127).
+// Row panel of a blocked Floyd (fap/kernel/floyd.h:118-127); with paths,
+// as floyd_path_B_CPU (:51-66) starts: current value and predecessor, then
+// B_path[k][j] of the first strictly shorter diag[i][k] + B[k][j].
 void floyd_path_B_Nvidia(float *B, int *B_path, const int row, const int col, float *diag, int *diag_path) {
-  (void)B_path;
+  if (B_path) {
+    host_minplus_path(diag, B, B_path, B, B_path, B, B_path, row, col, row, "floyd_path_B_Nvidia");
+    return;
+  }
   (void)diag_path;
   host_minplus(diag, B, B, row, col, row, "floyd_path_B_Nvidia");
 }
@@ -192,8 +377,12 @@ void floyd_path_B_Nvidia(float *B, int *B_path, const int row, const int col, fl
 // (0 on the diagonal, 1e8 elsewhere), so that E (x) res = res.
 void floyd_min_plus_Nvidia(float *mat1, float *mat2, int *mat2_path, float *res, int *res_path, int m, int n,
                            int k) {
-  (void)mat2_path;
-  (void)res_path;
+  if (mat2_path && res_path) {
+    // floyd_min_plus_CPU (fap/kernel/floyd.h:86-102): start from res and
+    // res_path, take mat2_path[k][j] from the first strictly shorter sum
+    host_minplus_path(mat1, mat2, mat2_path, res, res_path, res, res_path, m, n, k, "floyd_min_plus_Nvidia");
+    return;
+  }
   if (m <= 0 || n <= 0) {
     t_status = FAP_OK;
     return;

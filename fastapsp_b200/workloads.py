@@ -1,6 +1,11 @@
 """Benchmark workloads: seeded synthetic graphs of the named shapes, written
 as MatrixMarket and loaded through the drop-in fapGraph (host IO, METIS,
-boundary detection and renumbering)."""
+boundary detection and renumbering).
+
+`write()` only generates the graph and writes its MatrixMarket file; it
+neither imports the fapGraph binding nor loads libfap_b200.so, so a process
+that drives the reference's own binary on that file (the reference arm of
+the benchmark) runs none of this library's code."""
 from __future__ import annotations
 
 import os
@@ -10,7 +15,6 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import generators as G
-from .graph import fapGraph
 
 
 @dataclass
@@ -19,7 +23,7 @@ class Workload:
     K: int
     edges: G.EdgeList
     root: str           # directory holding graph/<kind>/<name>.mtx
-    graph: fapGraph     # after preCondition
+    graph: "fapGraph"   # after preCondition
     n: int
     ver_num: np.ndarray
     ver_offset: np.ndarray
@@ -56,13 +60,36 @@ class Workload:
                 "boundary": [int(bn.min()), int(np.median(bn)), int(bn.max()), int(bn.sum())]}
 
 
-def load(name: str, root: str | None = None) -> Workload:
+@dataclass
+class WorkloadFile:
+    """A workload's MatrixMarket file on disk (no partition, no library)."""
+    name: str
+    K: int
+    edges: G.EdgeList
+    root: str           # directory holding graph/<kind>/<name>.mtx
+
+    @property
+    def n(self) -> int:
+        return self.edges.n
+
+
+def write(name: str, root: str | None = None) -> WorkloadFile:
+    """Generates workload `name` (seeded) and writes its MatrixMarket file
+    under root/graph/<kind>/ in the layout the reference's reader resolves."""
     spec = G.WORKLOADS[name]
     el = spec["make"]()
     root = root or tempfile.mkdtemp(prefix="fap_wl_")
     path = G.mtx_path(root, name, el.directed, el.weighted)
     if not os.path.exists(path):
         G.write_mtx(el, root, name)
+    return WorkloadFile(name, spec["K"], el, root)
+
+
+def load(name: str, root: str | None = None) -> Workload:
+    from .graph import fapGraph
+    wf = write(name, root)
+    el, root = wf.edges, wf.root
+    spec = G.WORKLOADS[name]
     g = fapGraph(name, el.directed, el.weighted, spec["K"], root=root)
     g.preCondition()
     vn, vo, bn = g.partInfo()
@@ -75,13 +102,15 @@ class ServeGraph:
     n: int
     K: int
     avg_degree: float
-    graph: fapGraph     # after preCondition (partition + renumbering)
+    graph: "fapGraph"   # after preCondition (partition + renumbering)
 
 
 def load_serve_stream(count: int = 32, procs: int = 0, seed: int = 17) -> list:
     """The serving stream's resident graphs (generators.serve_specs), built in
     a spawn-started process pool and partitioned on the host (METIS)."""
     import multiprocessing as mp
+
+    from .graph import fapGraph
     specs = G.serve_specs(count, seed)
     procs = procs or max(1, min(8, os.cpu_count() or 1, count))
     if procs > 1:

@@ -305,12 +305,24 @@ FAP_API int fap_op_minplus(fap_ctx *ctx, int dtype, int32_t M, int32_t N, int32_
  *   - Every call on a device uses the same array, so calls whose GPU work
  *     overlaps (different streams, or host threads, on one device) race and
  *     corrupt each other: serialise them.
- *   - The first call on a device looks up the array's device address; make
- *     that first call before any stream capture.
+ *   - Each call outside a stream capture looks up the array's device
+ *     address (so a cudaDeviceReset in between is harmless); inside a
+ *     capture the last lookup on that device is used, so make the first
+ *     call on a device before any stream capture.
+ *   - The call returns before the GPU work ends, so a device-side failure (a
+ *     bounded TMA wait in the closure that gave up) cannot be its return
+ *     value: after synchronising the stream, fap_floyd_noalloc_status()
+ *     returns FAP_OK, or FAP_ERR_DEVICE when the last call's closure did not
+ *     complete (mat then holds no valid closure).
  * Messages: fap_floyd_noalloc_last_error(). */
 #define FAP_NOALLOC_FLOYD_MAX 1024
 FAP_API int fap_floyd_noalloc(int dtype, int32_t s, void *mat, int64_t ld, void *stream);
 FAP_API const char *fap_floyd_noalloc_last_error(void);
+/* Device-side status of the last fap_floyd_noalloc call on the current
+ * device (a status word beside the built-in array, cleared by each call).
+ * Read it only after that call's stream has been synchronised; it copies
+ * 4 bytes to the host and allocates nothing. */
+FAP_API int fap_floyd_noalloc_status(void);
 
 /* Measured relaxation throughput of this device (relaxations/s) for the
  * given dtype, from a register-resident microbenchmark. */

@@ -10,12 +10,34 @@
  * synchronous, like the reference.
  *
  * Behaviour:
- *   - distances are computed on the GPU in int32 when every input value is an
- *     integer (bit-exact with the reference's float results while finite
- *     distances stay below 2^24), else in float32;
- *   - the predecessor outputs (path, res_path) are not computed by this build
- *     and are left unchanged; the reference's CUDA SSSP also leaves them
- *     unset (fap/kernel/cuda/batch_sssp.cu:222-281);
+ *   - without predecessor arrays, distances are computed on the GPU in int32
+ *     when every input value is an integer (bit-exact with the reference's
+ *     float results while finite distances stay below 2^24), else in float32;
+ *   - with predecessor arrays (path / mat2_path and res_path / A_path,
+ *     diag_path / B_path non-NULL) the GPU computes in float32 with the
+ *     reference CPU kernels' own arithmetic and candidate order, and writes
+ *     the predecessors the reference's CPU path writes:
+ *       floyd_GPU_Nvidia_path   path[i][j] = path[k][j] on every strict
+ *                               improvement, pivots in order (floyd_CPU_path,
+ *                               fap/kernel/floyd.h:38-49); all entries must
+ *                               be non-negative;
+ *       minplus_NVIDIA_path     res_path[i][j] = mat2_path[k][j] of the first
+ *                               k with the least sum, -1 when none is below
+ *                               1e8 (min_plus_path_CPU_advanced,
+ *                               fap/kernel/minplus.h:51-65);
+ *       floyd_min_plus_Nvidia   the same, starting from res and res_path
+ *                               (floyd_min_plus_CPU, fap/kernel/floyd.h:86-102);
+ *       floyd_path_A/B_Nvidia   the same, starting from the panel's own value
+ *                               and predecessor, candidates from the closed
+ *                               diagonal block, computed out of place: equal
+ *                               to the reference's in-place CPU panels
+ *                               (floyd.h:51-84) in every value, and in every
+ *                               predecessor wherever the shortest path is
+ *                               unique.  (The reference's CUDA panels start
+ *                               from 1e8 and so report diag_path[j][j] where
+ *                               the panel entry itself is shortest.)
+ *     The SSSP rows carry no predecessors (the reference's CUDA SSSP leaves
+ *     them unset too, fap/kernel/cuda/batch_sssp.cu:222-281);
  *   - on an error the outputs are left unchanged, a message goes to stderr
  *     and fap_legacy_last_status() returns the FAP_ERR_* code (the reference
  *     calls exit(EXIT_FAILURE) instead).
@@ -46,8 +68,8 @@ FAP_LEGACY_API void minplus_NVIDIA_path(float *mat1, float *mat2, int *mat2_path
 
 /* The rest of the reference's kernel header, which fap/fap.cpp also calls
  * (fap/kernel/minplus.h:69-76, fap/kernel/floyd.h:106-139) and so needs at
- * link time.  Same meanings as the reference's CUDA versions; paths are left
- * unchanged as above. */
+ * link time.  Same meanings as the reference's CUDA versions; predecessors
+ * as above. */
 
 /* Floyd-Warshall of arc[num_node x num_node] in place, no paths.
  * Replaces cuda_kernel.h:27. */

@@ -209,3 +209,84 @@ int fo_run_part(int n, const int *row_offset, const int *col, const float *w,
   free(mat);
   return 0;
 }
+
+/* ---- predecessor-carrying kernels of the reference's kernel header ---- */
+
+/* floyd_CPU_path, fap/kernel/floyd.h:38-49: k-i-j, strict >, path[i][j] =
+ * path[k][j] on every improvement. */
+void fo_floyd_path(int s, float *mat, int *path) {
+  for (int64_t k = 0; k < s; k++)
+    for (int64_t i = 0; i < s; i++)
+      for (int64_t j = 0; j < s; j++) {
+        const float c = mat[i * s + k] + mat[k * s + j];
+        if (mat[i * s + j] > c) {
+          mat[i * s + j] = c;
+          path[i * s + j] = path[k * s + j];
+        }
+      }
+}
+
+/* min_plus_path_CPU_advanced, fap/kernel/minplus.h:51-65 (c0 == NULL: start
+ * from the sentinel with path -1), and floyd_min_plus_CPU, fap/kernel/
+ * floyd.h:86-102 (c0/p0 given: start from them): for k ascending, a strictly
+ * smaller mat1[i][k] + mat2[k][j] replaces the value and takes
+ * mat2_path[k][j].  Out of place: res/path must not alias the inputs. */
+void fo_minplus_path(int M, int N, int K, const float *mat1, const float *mat2,
+                     const int *mat2_path, const float *c0, const int *p0,
+                     float *res, int *path) {
+  for (int64_t i = 0; i < M; i++)
+    for (int64_t j = 0; j < N; j++) {
+      float v = c0 ? c0[i * N + j] : FO_MAXVALUE;
+      int p = c0 ? p0[i * N + j] : -1;
+      for (int64_t k = 0; k < K; k++) {
+        const float c = mat1[i * K + k] + mat2[k * N + j];
+        if (v > c) {
+          v = c;
+          p = mat2_path[k * N + j];
+        }
+      }
+      res[i * N + j] = v;
+      path[i * N + j] = p;
+    }
+}
+
+/* floyd_path_A_CPU, fap/kernel/floyd.h:68-84, in place as the reference
+ * does it (entries of row i left of j are already updated when j runs). */
+void fo_floyd_path_A(float *A, int *A_path, int row, int col, const float *diag,
+                     const int *diag_path) {
+  for (int64_t i = 0; i < row; i++)
+    for (int64_t j = 0; j < col; j++) {
+      float v = A[i * col + j];
+      int p = A_path[i * col + j];
+      for (int64_t k = 0; k < col; k++) {
+        const float c = A[i * col + k] + diag[k * col + j];
+        if (v > c) {
+          v = c;
+          p = diag_path[k * col + j];
+        }
+      }
+      A[i * col + j] = v;
+      A_path[i * col + j] = p;
+    }
+}
+
+/* floyd_path_B_CPU, fap/kernel/floyd.h:51-66, in place as the reference
+ * does it (rows above i are already updated when row i runs). */
+void fo_floyd_path_B(float *B, int *B_path, int row, int col, const float *diag,
+                     const int *diag_path) {
+  (void)diag_path;
+  for (int64_t i = 0; i < row; i++)
+    for (int64_t j = 0; j < col; j++) {
+      float v = B[i * col + j];
+      int p = B_path[i * col + j];
+      for (int64_t k = 0; k < row; k++) {
+        const float c = diag[i * row + k] + B[k * col + j];
+        if (v > c) {
+          v = c;
+          p = B_path[k * col + j];
+        }
+      }
+      B[i * col + j] = v;
+      B_path[i * col + j] = p;
+    }
+}

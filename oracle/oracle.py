@@ -103,6 +103,14 @@ def port_lib():
         lib.fo_dijkstra_path.restype = None
         lib.fo_floyd.argtypes = [I, P]
         lib.fo_floyd.restype = None
+        lib.fo_floyd_path.argtypes = [I, P, P]
+        lib.fo_floyd_path.restype = None
+        lib.fo_minplus_path.argtypes = [I, I, I, P, P, P, P, P, P, P]
+        lib.fo_minplus_path.restype = None
+        lib.fo_floyd_path_A.argtypes = [P, P, I, I, P, P]
+        lib.fo_floyd_path_A.restype = None
+        lib.fo_floyd_path_B.argtypes = [P, P, I, I, P, P]
+        lib.fo_floyd_path_B.restype = None
         _port = lib
     return _port
 
@@ -144,6 +152,46 @@ def port_floyd(mat: np.ndarray) -> np.ndarray:
     m = np.ascontiguousarray(mat, np.float32).copy()
     port_lib().fo_floyd(int(m.shape[0]), _p(m))
     return m
+
+
+def port_floyd_path(mat: np.ndarray, path: np.ndarray):
+    """floyd_CPU_path (fap/kernel/floyd.h:38-49): (closed matrix, paths)."""
+    m = np.ascontiguousarray(mat, np.float32).copy()
+    p = np.ascontiguousarray(path, np.int32).copy()
+    port_lib().fo_floyd_path(int(m.shape[0]), _p(m), _p(p))
+    return m, p
+
+
+def port_minplus_path(mat1, mat2, mat2_path, c0=None, p0=None):
+    """min_plus_path_CPU_advanced (fap/kernel/minplus.h:51-65) when c0 is
+    None, floyd_min_plus_CPU (fap/kernel/floyd.h:86-102) from (c0, p0)
+    otherwise: (values, paths)."""
+    a = np.ascontiguousarray(mat1, np.float32)
+    b = np.ascontiguousarray(mat2, np.float32)
+    bp = np.ascontiguousarray(mat2_path, np.int32)
+    M, K = a.shape
+    N = b.shape[1]
+    res = np.empty((M, N), np.float32)
+    path = np.empty((M, N), np.int32)
+    c0a = None if c0 is None else np.ascontiguousarray(c0, np.float32)
+    p0a = None if c0 is None else np.ascontiguousarray(p0, np.int32)
+    port_lib().fo_minplus_path(int(M), int(N), int(K), _p(a), _p(b), _p(bp),
+                               None if c0a is None else _p(c0a), None if p0a is None else _p(p0a),
+                               _p(res), _p(path))
+    return res, path
+
+
+def port_floyd_path_panel(which: str, panel, panel_path, diag, diag_path):
+    """floyd_path_A_CPU / floyd_path_B_CPU (fap/kernel/floyd.h:51-84), in
+    place like the reference: (values, paths)."""
+    x = np.ascontiguousarray(panel, np.float32).copy()
+    xp = np.ascontiguousarray(panel_path, np.int32).copy()
+    d = np.ascontiguousarray(diag, np.float32)
+    dp = np.ascontiguousarray(diag_path, np.int32)
+    row, col = x.shape
+    fn = port_lib().fo_floyd_path_A if which == "A" else port_lib().fo_floyd_path_B
+    fn(_p(x), _p(xp), int(row), int(col), _p(d), _p(dp))
+    return x, xp
 
 
 def port_solve_meta(meta: Meta, parts=None) -> dict:
@@ -211,7 +259,8 @@ def ref_available() -> bool:
 
 def run_ref(workdir: str, name: str, directed: bool, weighted: bool, K: int, *,
             parts="all", meta_out: str | None = None, dist_out: str | None = None,
-            path_out: str | None = None, threads: int | None = None,
+            path_out: str | None = None, rowsum_out: str | None = None,
+            threads: int | None = None,
             partition_file: str | None = None, timeout: float | None = None) -> list:
     """Run the reference's CPU path (oracle/_ref/fap_ref) and return its JSON
     event lines."""
@@ -226,6 +275,8 @@ def run_ref(workdir: str, name: str, directed: bool, weighted: bool, K: int, *,
         cmd += ["--dist", os.path.abspath(dist_out)]
     if path_out:
         cmd += ["--path", os.path.abspath(path_out)]
+    if rowsum_out:
+        cmd += ["--rowsum", os.path.abspath(rowsum_out)]
     env = dict(os.environ)
     if threads:
         env["OMP_NUM_THREADS"] = str(threads)

@@ -15,13 +15,19 @@
 //
 // Usage:
 //   fap_ref --dir D -f NAME -k K -direct 0|1 -weight 0|1
-//           [--parts all|1,5,9] [--meta FILE] [--dist FILE] [--path FILE] [--quiet]
+//           [--parts all|1,5,9] [--meta FILE] [--dist FILE] [--path FILE]
+//           [--rowsum FILE] [--quiet]
 //   The graph is read from D/graph/<kind>/NAME.mtx (the reference resolves the
 //   path relative to the working directory, fap/utils/readMatFile.h:43-51).
 //   --meta  writes the CSR, partition and renumbering (binary, see dump_meta).
 //   --dist  writes each solved part's s x n float block, in part order.
 //   --path  writes each solved part's s x n int32 predecessor block (the
 //           reference's run() always computes it), in part order.
+//   --rowsum writes, per solved part and row, the uint64 checksum
+//           sum_j uint32(int32(d[r][j])) * (2j + 1) mod 2^64 of the row's
+//           distances cast to int32 (exact for integer weights while the
+//           finite distances stay below 2^24; the sentinel 1e8 becomes
+//           100000000): s values per part, in part order.
 //   One JSON line per solved part goes to stdout with its wall time.
 //   FAP_PARTITION_FILE=<file of n int32 part ids, 0-based> replaces the METIS
 //   call by that partition (link-time wrap of METIS_PartGraphKway), so the
@@ -100,10 +106,25 @@ void dump_meta(fap::fapGraph &g, const char *path) {
   fclose(f);
 }
 
+// Per-row checksums of an s x n block, int32 view of the float distances.
+void put_rowsums(FILE *f, const float *d, int64_t s, int64_t n) {
+  std::vector<uint64_t> sums((size_t)s);
+  for (int64_t r = 0; r < s; r++) {
+    uint64_t acc = 0;
+    const float *row = d + r * n;
+    for (int64_t j = 0; j < n; j++) {
+      const uint32_t v = (uint32_t)(int32_t)(int64_t)row[j];
+      acc += (uint64_t)v * (uint64_t)(2 * j + 1);
+    }
+    sums[(size_t)r] = acc;
+  }
+  put(f, sums.data(), sums.size());
+}
+
 }  // namespace
 
 int main(int argc, char **argv) {
-  std::string dir = ".", name, parts = "all", meta, distf, pathf;
+  std::string dir = ".", name, parts = "all", meta, distf, pathf, sumf;
   int K = 0, directed = 0, weighted = 0;
   bool quiet = false;
   for (int i = 1; i < argc; i++) {
@@ -121,6 +142,7 @@ int main(int argc, char **argv) {
     else if (a == "--meta") meta = nxt();
     else if (a == "--dist") distf = nxt();
     else if (a == "--path") pathf = nxt();
+    else if (a == "--rowsum") sumf = nxt();
     else if (a == "--quiet") quiet = true;
     else { fprintf(stderr, "unknown arg %s\n", a.c_str()); return 2; }
   }
@@ -131,6 +153,7 @@ int main(int argc, char **argv) {
   if (!meta.empty() && meta[0] != '/') meta = std::string(getcwd(nullptr, 0)) + "/" + meta;
   if (!distf.empty() && distf[0] != '/') distf = std::string(getcwd(nullptr, 0)) + "/" + distf;
   if (!pathf.empty() && pathf[0] != '/') pathf = std::string(getcwd(nullptr, 0)) + "/" + pathf;
+  if (!sumf.empty() && sumf[0] != '/') sumf = std::string(getcwd(nullptr, 0)) + "/" + sumf;
   if (chdir(dir.c_str()) != 0) { perror(dir.c_str()); return 2; }
 
   // The reference prints a debug line on every min-plus call
@@ -155,7 +178,7 @@ int main(int argc, char **argv) {
     std::string tok;
     while (std::getline(ss, tok, ',')) todo.push_back(std::stoi(tok));
   }
-  FILE *df = nullptr, *pf = nullptr;
+  FILE *df = nullptr, *pf = nullptr, *sf = nullptr;
   if (!distf.empty()) {
     df = fopen(distf.c_str(), "wb");
     if (!df) { perror(distf.c_str()); return 2; }
@@ -163,6 +186,10 @@ int main(int argc, char **argv) {
   if (!pathf.empty()) {
     pf = fopen(pathf.c_str(), "wb");
     if (!pf) { perror(pathf.c_str()); return 2; }
+  }
+  if (!sumf.empty()) {
+    sf = fopen(sumf.c_str(), "wb");
+    if (!sf) { perror(sumf.c_str()); return 2; }
   }
   const int64_t n = g.num_vertexs;
   for (int p : todo) {
@@ -175,12 +202,14 @@ int main(int argc, char **argv) {
     double b = now_s();
     if (df) put(df, dist.data(), dist.size());
     if (pf) put(pf, path.data(), path.size());
+    if (sf) put_rowsums(sf, dist.data(), s, n);
     printf("{\"event\": \"part\", \"part\": %d, \"rows\": %lld, \"bdy\": %d, \"entries\": %lld, \"seconds\": %.6f}\n",
            p, (long long)s, g.C_BlockBdy_num[p], (long long)(s * n), b - a);
     fflush(stdout);
   }
   if (df) fclose(df);
   if (pf) fclose(pf);
+  if (sf) fclose(sf);
   std::cout.rdbuf(saved);
   return 0;
 }

@@ -100,6 +100,27 @@ def test_reference_arm_prints_one_contract_line():
     assert cb["kind"] in ("reference", "port") and cb["cores"] >= 1 and cb["value"] == line["value"]
     assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
+    # the reference arm builds its workload with the generator alone and lets
+    # the reference binary partition it: the product library stays unloaded
+    assert line["product_library_loaded"] is False
+    assert {"parallelism", "l2", "part_size", "boundary"} <= set(line["config"])
+
+
+def test_reference_partition_matches_the_product():
+    """The reference arm describes the workload from the reference binary's
+    own preprocessing; on an undirected workload it equals the product's."""
+    b = _bench()
+    from fastapsp_b200 import workloads
+    from oracle import oracle as O
+    if not O.ref_available():
+        import pytest
+        pytest.skip("reference binary not built")
+    wl = workloads.load("grid64")
+    with tempfile.TemporaryDirectory() as tmp:
+        meta = b.reference_partition(wl, tmp)
+    assert b.describe_meta(wl.name, wl.K, wl.edges.directed, meta) == wl.describe()
+    import numpy as np
+    assert np.array_equal(meta.st2ed, wl.graph.getMapping())
 
 
 def test_reference_arm_runs_on_rank_zero_only():

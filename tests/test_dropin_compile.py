@@ -16,7 +16,8 @@ import pytest
 from conftest import ROOT
 from fastapsp_b200 import _lib as L
 
-REFERENCE = os.environ.get("FAP_REFERENCE_DIR", "/root/reference")
+# $FAP_REFERENCE_DIR, else a checkout named "reference" beside this repository
+REFERENCE = os.environ.get("FAP_REFERENCE_DIR") or os.path.join(os.path.dirname(ROOT), "reference")
 EXAMPLE = os.path.join(REFERENCE, "app", "singleNodeExample.cpp")
 
 

@@ -365,8 +365,9 @@ def test_legacy_abi_blocked_floyd_entry_points(cuda_ok):
     51-84, their CUDA versions from the sentinel), the remaining-block update
     res = min(res, mat1 (x) mat2) (:86-102), the path-free min-plus
     (minplus.h:69-76) and Floyd.  Integral inputs run in int32 and must match
-    exactly; real-valued ones in float32 within the tolerance.  Path arrays
-    are left unchanged."""
+    exactly; real-valued ones in float32 within the tolerance.  The path
+    arrays given here are all zero, so they stay zero (predecessor outputs
+    are tested in tests/test_legacy_paths.py)."""
     lib = L.lib()
     f = {k: getattr(lib, L.LEGACY_SYMBOLS[k]) for k in
          ("floyd_NVIDIA_GPU", "floyd_path_A_Nvidia", "floyd_path_B_Nvidia", "floyd_min_plus_Nvidia",

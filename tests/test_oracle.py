@@ -7,7 +7,7 @@ import tempfile
 import numpy as np
 import pytest
 
-from conftest import golden_names, load_golden
+from conftest import ROOT, golden_names, load_golden
 from oracle import oracle as O
 
 
@@ -115,6 +115,51 @@ def test_port_matches_reference_binary(seed):
     out = O.port_solve_meta(meta)
     full = np.concatenate([out[p] for p in range(1, meta.K + 1)], 0)
     assert np.array_equal(full.view(np.int32), ref.view(np.int32))
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference binary not built here")
+def test_reference_row_checksums_and_shared_partition():
+    """fap_ref --rowsum writes the per-row checksums of its int32-cast blocks
+    (the same formula as the library's fap_graph_block_checksums), and a
+    partition given through FAP_PARTITION_FILE replaces its METIS call; a
+    checksum changed on the oracle side is caught by the bench's comparison."""
+    import importlib.util
+    from fastapsp_b200 import generators as G
+    g = G.road_graph(500, seed=3, wmin=1, wmax=100)
+    K = 5
+    with tempfile.TemporaryDirectory() as tmp:
+        G.write_mtx(g, tmp, "r")
+        meta_f = os.path.join(tmp, "m.bin")
+        dist_f = os.path.join(tmp, "d.bin")
+        sum_f = os.path.join(tmp, "s.bin")
+        part_f = os.path.join(tmp, "p.bin")
+        gid0 = (np.arange(g.n) * K // g.n).astype(np.int32)
+        gid0.tofile(part_f)
+        O.run_ref(tmp, "r", False, True, K, parts=[2, 4], meta_out=meta_f, dist_out=dist_f,
+                  rowsum_out=sum_f, partition_file=part_f)
+        meta = O.read_meta(meta_f)
+        assert np.array_equal(meta.graph_id, gid0 + 1)
+        dist = np.fromfile(dist_f, np.float32).reshape(-1, meta.n)
+        sums = np.fromfile(sum_f, np.uint64)
+        assert np.array_equal(sums, O.row_checksums(O.to_i32(dist)))
+        # the bench's comparison: equal sums pass, one planted change is a mismatch
+        spec = importlib.util.spec_from_file_location(
+            "bench_parity", os.path.join(ROOT, "bench.py"))
+        b = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(b)
+        s2 = int(meta.ver_num[2])
+        gpu = {2: sums[:s2].copy(), 4: sums[s2:].copy()}
+        f2, f4 = os.path.join(tmp, "s2.bin"), os.path.join(tmp, "s4.bin")
+        sums[:s2].tofile(f2)
+        planted = sums[s2:].copy()
+        planted[3] += np.uint64(1)
+        planted.tofile(f4)
+
+        class W:
+            name, n = "r", meta.n
+        res = b.compare_parity(W, gpu, {2: f2, 4: f4}, 0, meta.st2ed, meta)
+        assert res["parts"] == 2 and res["rows"] == sums.size and res["mismatches"] == 1
+        assert res["st2ed_equal"] is True
 
 
 def _path_names():

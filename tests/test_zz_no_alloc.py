@@ -67,9 +67,35 @@ def test_noalloc_matches_allocating_floyd_twice(cuda_ok, dtype):
                                    ctypes.c_void_p(stream))
         assert rc == L.FAP_OK, lib.fap_floyd_noalloc_last_error()
         torch.cuda.synchronize()
+        assert lib.fap_floyd_noalloc_status() == L.FAP_OK, lib.fap_floyd_noalloc_last_error()
         _compare(b.cpu().numpy(), a.cpu().numpy(), dtype)
         # the padding columns of the caller's buffer are untouched
         assert torch.all(buf_b[:, s:] == -1).item(), f"call {call} wrote past column s"
+
+
+@pytest.mark.parametrize("dtype", [FAP_DTYPE_I32, FAP_DTYPE_F32])
+def test_noalloc_matches_the_oracle_at_edge_sizes(cuda_ok, dtype):
+    """One element, exactly one tile, a ragged size, and the largest size the
+    built-in array holds (its last tile row and column), each against the
+    oracle's Floyd-Warshall (the reference's k-i-j loop with strict >)."""
+    import torch
+
+    from oracle import oracle as O
+    lib = L.lib()
+    stream = torch.cuda.current_stream().cuda_stream
+    for s, seed in [(1, 5), (128, 6), (700, 7), (L.FAP_NOALLOC_FLOYD_MAX, 8)]:
+        M = _matrix(s, dtype, seed + 10 * dtype)
+        if dtype == FAP_DTYPE_I32:
+            M[M == L.FAP_INF_I32] = 100000000
+        ref = O.port_floyd(M.astype(np.float32))
+        if dtype == FAP_DTYPE_I32:
+            ref = O.to_i32(ref)
+        b = torch.from_numpy(M).to("cuda")
+        rc = lib.fap_floyd_noalloc(dtype, s, ctypes.c_void_p(b.data_ptr()), s, ctypes.c_void_p(stream))
+        assert rc == L.FAP_OK, lib.fap_floyd_noalloc_last_error()
+        torch.cuda.synchronize()
+        assert lib.fap_floyd_noalloc_status() == L.FAP_OK, lib.fap_floyd_noalloc_last_error()
+        _compare(b.cpu().numpy(), ref, dtype)
 
 
 def test_noalloc_rejects_oversize_before_gpu_work(cuda_ok):
