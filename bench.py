@@ -64,12 +64,20 @@ def parse_args():
                     help="SSSP form of stage 1: 0 automatic, 1 frontier, 2 tiled Bellman-Ford")
     ap.add_argument("--bgraph-form", type=int, default=0, choices=[0, 1, 2],
                     help="boundary-graph closure: 0 by size, 1 Floyd, 2 Bellman-Ford + tiled expansion")
+    ap.add_argument("--no-pack16", action="store_true",
+                    help="min-plus tiles in int32 only (no packed 16-bit tiles)")
     ap.add_argument("--no-stage-cache", action="store_true",
                     help="grouped jobs: run stages 1-2 per group instead of once for all parts")
     ap.add_argument("--cache-only", action="store_true",
                     help="time only stages 1-2 of every part (the resident cache build), no output matrix")
     ap.add_argument("--paths", action="store_true",
                     help="also time batched solves that produce predecessor matrices")
+    ap.add_argument("--extra", default=",".join(EXTRA_WORKLOADS),
+                    help="further workloads timed after the headline one (comma list, '' for none)")
+    ap.add_argument("--extra-steps", type=int, default=2)
+    ap.add_argument("--extra-warmup", type=int, default=3)
+    ap.add_argument("--extra-parity-parts", type=int, default=2,
+                    help="parts of each further workload checked against the reference binary")
     ap.add_argument("--serve-graphs", type=int, default=32)
     ap.add_argument("--serve-burst", type=int, default=1024,
                     help="requests of the closed-loop run that measures capacity")
@@ -223,7 +231,8 @@ def cpu_procs(requested):
     return max(1, p)
 
 
-def run_reference_sample(wl, parts_per_proc, procs, timeout=900, extra=None, partition_file=None):
+def run_reference_sample(wl, parts_per_proc, procs, timeout=900, extra=None, partition_file=None,
+                         threads=1):
     """Runs the reference CPU path on `procs` concurrent processes, process i
     solving parts_per_proc[i] in order (extra[i]: more arguments of process
     i, e.g. output files; partition_file: a shared partition in place of the
@@ -231,7 +240,7 @@ def run_reference_sample(wl, parts_per_proc, procs, timeout=900, extra=None, par
     (part, rows, entries, seconds))."""
     from oracle import oracle as O
     kind = "reference" if O.ref_available() else "port"
-    env = dict(os.environ, OMP_NUM_THREADS="1")
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
     if partition_file:
         env["FAP_PARTITION_FILE"] = os.path.abspath(partition_file)
     if kind == "reference":
@@ -519,7 +528,8 @@ def run_serving(args, device):
                         "entries_s": st.entries / burst_s,
                         "requests": len(reqs), "window": window, "batches": st.batches,
                         "resident_hits": st.resident_hits, "p50_ms": st.p50_ms, "p99_ms": st.p99_ms,
-                        "by_kind": by_kind, "device_busy_frac": st.busy_ms * 1e-3 / burst_s},
+                        "by_kind": by_kind, "device_busy_frac": st.busy_ms * 1e-3 / burst_s,
+                        "worker_host_max_ms": {k: round(v, 3) for k, v in st.host_max_ms.items()}},
            "warmup_cache_builds": warm.cache_builds,
            "loads": []}
     log(f"serving capacity {cap_rps:.1f} req/s (runs {[round(c[0], 1) for c in caps]}), "
@@ -552,7 +562,8 @@ def run_serving(args, device):
                              "by_kind": by_kind,
                              "batches": st.batches, "resident_hits": st.resident_hits,
                              "peak_device_bytes": st.peak_bytes, "cache_builds": st.cache_builds,
-                             "device_busy_frac": st.busy_ms * 1e-3 / wall})
+                             "device_busy_frac": st.busy_ms * 1e-3 / wall,
+                             "worker_host_max_ms": {k: round(v, 3) for k, v in st.host_max_ms.items()}})
         log(f"serving at {frac:.0%}: p50 {st.p50_ms:.2f} ms, p99 {st.p99_ms:.2f} ms, "
             f"{st.entries / wall:.4g} entries/s, {st.batches} batches; "
             f"sub p50/p99 {by_kind['sub']['p50_ms']}/{by_kind['sub']['p99_ms']}, "
@@ -587,6 +598,134 @@ def run_cache_only(args, dg, stream, world):
     if int(os.environ.get("RANK", "0")) == 0:
         print(json.dumps({"mode": "cache_only", "ms_per_step": float(np.mean(ms)), "steps": args.steps,
                           "phases_ms": ph, "world": world}))
+
+
+EXTRA_WORKLOADS = ("grid512", "rmat16")
+
+
+def run_extra(args, name, ctx, relax_peak, hbm_peak, peak_kind):
+    """A further workload of the same metric on one GPU: batched solves of
+    every part (timed with CUDA events on the library's stream, inputs
+    resident, L2 flushed between steps), its min-plus as a fraction of the
+    measured relaxation peak, and parity of sampled parts against the
+    reference binary under the same partition.  The sampled parts are the
+    ones with the fewest boundary vertices (the reference's serial min-plus
+    and Floyd then finish in seconds); the reference runs them side by side
+    with all host threads split between them."""
+    import torch
+
+    from fastapsp_b200 import FAP_MODE_BATCHED, DeviceGraph, autotune, workloads
+    from fastapsp_b200.sharding import group_parts_by_rows, rows_of
+    t0 = time.perf_counter()
+    wl = workloads.load(name)
+    n = wl.n
+    vn, vo, bn = wl.ver_num, wl.ver_offset, wl.bdy_num
+    ro, col, w = wl.csr()
+    gid = wl.graph.getGraphId()
+    st2ed = wl.graph.getMapping()
+    dg = DeviceGraph(ctx, ro, col, w)
+    dtype = dg.dtype
+    dg.set_parts(wl.K, gid, st2ed, vn, vo, bn)
+    dg.set_param("minplus_pack16", 0 if args.no_pack16 else 1)
+    ldD = (n + 127) // 128 * 128
+    stream = torch.cuda.current_stream()
+    mine = list(range(1, wl.K + 1))
+    all_rows = rows_of(mine, vn)
+    free_b = torch.cuda.mem_get_info()[0]
+    budget_rows = int(0.60 * free_b / (4 * ldD))
+    staged = all_rows > budget_rows
+    if staged:
+        dg.cache_build()
+        dg.check()
+        budget_rows = int(0.60 * torch.cuda.mem_get_info()[0] / (4 * ldD))
+    groups = [mine] if all_rows <= budget_rows else group_parts_by_rows(mine, vn, budget_rows)
+    dg.reserve(max(rows_of(g, vn) for g in groups) if len(groups) > 1 else 0)
+    tuned = autotune.tune_sssp(dg, vn, bn)
+    log(f"{name} loaded in {time.perf_counter() - t0:.1f} s: {wl.describe()}, {len(groups)} group(s)")
+
+    def step():
+        if staged:
+            dg.cache_build(rebuild=True)
+        for grp in groups:
+            dg.solve(grp, FAP_MODE_BATCHED, check_errors=False)
+
+    for _ in range(args.extra_warmup):
+        step()
+    dg.check()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    ms, mp_ms = [], []
+    for _ in range(args.extra_steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        mp = 0.0
+        if staged:
+            dg.cache_build(rebuild=True)
+        for grp in groups:
+            dg.solve(grp, FAP_MODE_BATCHED, check_errors=False)
+            mp += float(dg.last_timing()[3])
+        e1.record(stream)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+        mp_ms.append(mp)
+    dg.check()
+    del flush
+    ms_step = float(np.mean(ms))
+    mp_step = float(np.mean(mp_ms))
+    mp_relax = float(sum(float(vn[p] - bn[p]) * float(bn[p]) * n for p in mine))
+    mp_bytes = float(sum(4.0 * ((vn[p] - bn[p]) * n + (vn[p] - bn[p]) * bn[p] + bn[p] * n) for p in mine))
+    a = mp_relax / (mp_step * 1e-3) / 1e9
+    # parity: the parts with the fewest boundary vertices
+    order = sorted(mine, key=lambda p: (int(bn[p]), p))
+    ppart = order[:max(0, args.extra_parity_parts)]
+    parity = None
+    if ppart:
+        gpu = gpu_parity_blocks(dg, groups, ppart, dtype, staged, FAP_MODE_BATCHED)
+    stage1 = dg.stage1_name()
+    pk_tiles = dg.pack16_tiles()
+    del dg
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    if ppart:
+        from oracle import oracle as O
+        threads = max(1, (os.cpu_count() or 1) // len(ppart))
+        with tempfile.TemporaryDirectory() as tmp:
+            pfile = os.path.join(tmp, "partition.bin")
+            (np.asarray(gid, dtype=np.int64) - 1).astype(np.int32).tofile(pfile)
+            meta_f = os.path.join(tmp, "meta.bin")
+            files = {p: os.path.join(tmp, f"out_{p}.bin") for p in ppart}
+            extra = {i: ["--rowsum" if dtype == 0 else "--dist", files[p]] for i, p in enumerate(ppart)}
+            extra[0] = extra[0] + ["--meta", meta_f]
+            if O.ref_available():
+                tr = time.perf_counter()
+                kind, res = run_reference_sample(wl, [[p] for p in ppart], len(ppart), extra=extra,
+                                                 partition_file=pfile, threads=threads)
+                parity = compare_parity(wl, gpu, files, dtype, st2ed, O.read_meta(meta_f))
+                parity["parts_chosen"] = "fewest boundary vertices"
+                parity["reference_s"] = round(time.perf_counter() - tr, 2)
+            else:
+                parity = {"unavailable": "reference binary absent"}
+        del gpu
+    out = {
+        "value": all_rows * n / (ms_step * 1e-3), "unit": UNIT, "ms_per_step": ms_step,
+        "steps": args.extra_steps, "warmup": args.extra_warmup,
+        "dtype": "int32" if dtype == 0 else "f32", "data": wl.data_description(),
+        "config": {**wl.describe(), "groups": len(groups), "stage_cache": staged, "stage1": stage1,
+                   "minplus_packed_tiles": {"packed": pk_tiles[0], "total": pk_tiles[1]},
+                   "sssp_delta_factor": tuned["factor"],
+                   "l2": "256 MB buffer written between timed steps (outside the events); "
+                         f"each step writes {4 * n * all_rows / 1e9:.1f} GB of distances"},
+        "minplus": {"ms": mp_step, "relax": mp_relax, "bytes": mp_bytes, "achieved_grelax_s": a,
+                    "frac_of_relax_peak": a / (relax_peak / 1e9),
+                    "frac_of_hbm": mp_bytes / (mp_step * 1e-3) / 1e9 / hbm_peak,
+                    "peaks": f"relaxation peak measured live (fap_measure_relax_peak); HBM {peak_kind}"},
+        "parity": parity,
+    }
+    log(f"{name}: {ms_step:.1f} ms/step, {out['value']:.4g} entries/s, min-plus {mp_step:.1f} ms "
+        f"({out['minplus']['frac_of_relax_peak']:.2f} of the relaxation peak), parity {parity}")
+    return out
 
 
 def main_fap(args):
@@ -641,6 +780,7 @@ def main_fap(args):
     dg.set_param("stage1", args.stage1)
     dg.set_param("sssp_form", args.sssp_form)
     dg.set_param("bgraph_form", args.bgraph_form)
+    dg.set_param("minplus_pack16", 0 if args.no_pack16 else 1)
     if args.cache_only:
         run_cache_only(args, dg, stream, world)
         if world > 1:
@@ -880,6 +1020,19 @@ def main_fap(args):
         torch.cuda.empty_cache()
         serving = run_serving(args, local)
 
+    # ---- further workloads (rank 0, N=1 only) ----
+    extras = None
+    if rank == 0 and world == 1 and args.extra:
+        extras = {}
+        torch.cuda.empty_cache()
+        for name in [x for x in args.extra.split(",") if x]:
+            try:
+                extras[name] = run_extra(args, name, ctx, relax_peak, hbm_peak, peak_kind)
+            except Exception as e:  # noqa: BLE001 - reported in the line, not fatal
+                extras[name] = {"unavailable": str(e)[:300]}
+                log(f"{name}: {e}")
+            torch.cuda.empty_cache()
+
     # ---- CPU baseline (rank 0, N=1 only) and parity of the same parts ----
     cpu = None
     parity = None
@@ -950,6 +1103,7 @@ def main_fap(args):
             "clocks": clk,
             "serving": serving,
             "paths": paths,
+            "workloads": extras,
         }
         emit(line)
     if world > 1:

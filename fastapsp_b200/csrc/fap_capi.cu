@@ -202,6 +202,11 @@ struct fap_dgraph {
   bool floyd_per_cta = false;     // batched Floyd: one CTA per part instead of per-tile launches
   int sssp_chain = 0;             // SSSP chain-following budget (hops per thread per round)
   int sssp_precheck = 1;          // SSSP: plain read of dist[v] before the atomicMin
+  // Min-plus tiles in the packed 16-bit form where the distances provably
+  // fit (int32 graphs; Pack16): bounds buffers of the prepared batch.
+  bool pack16 = true;
+  DevBuf d_pk_off, d_pk_range, d_pk_maxa, d_pk_tiles;
+  Pack16 pk{};
   // CUDA graph of the batched launch sequence (replayed while nothing that
   // it captured changes: batch, buffers, parameters, stream)
   bool use_graph = true;
@@ -474,7 +479,8 @@ extern "C" int fap_graph_destroy(fap_dgraph *G) try {
                       &G->d_tro, &G->d_tcol, &G->d_tw, &G->d_dB, &G->d_bpart, &G->d_brows, &G->d_FB,
                       &G->d_msbf_items, &G->d_msbf_act, &G->d_msbf_changed, &G->d_bitro, &G->d_bitcol,
                       &G->d_botro, &G->d_botcol, &G->d_bitw, &G->d_bitems, &G->d_bDt, &G->d_bact, &G->d_bpact,
-                      &G->d_bgpart, &G->d_bpcolmap, &G->d_grow})
+                      &G->d_bgpart, &G->d_bpcolmap, &G->d_grow, &G->d_pk_off, &G->d_pk_range,
+                      &G->d_pk_maxa, &G->d_pk_tiles})
       b->release();
     if (G->h_changed) cudaFreeHost(G->h_changed);
     for (cudaEvent_t &ev : G->cev)
@@ -912,16 +918,34 @@ int prepare_batch(fap_dgraph *G, const std::vector<int32_t> &ids, bool cached, b
     G->part_work_end.push_back((int32_t)G->work.size());
   }
   G->f_elems = foff;
-  if (!cached) FAP_TRY(G->F.ensure((size_t)std::max<int64_t>(foff, 1) * 4));
-  FAP_TRY(G->d_parts.ensure(std::max<size_t>(G->parts.size(), 1) * sizeof(PartDesc)));
-  FAP_TRY(G->d_work.ensure(std::max<size_t>(G->work.size(), 1) * sizeof(MPWork)));
-  FAP_TRY(G->d_thin.ensure(std::max<size_t>(G->thin.size(), 1) * 4));
-  FAP_TRY(G->d_src.ensure(std::max<size_t>(G->src.size(), 1) * 4));
-  FAP_TRY(G->d_srcrows.ensure(std::max<size_t>(G->srcrows.size(), 1) * 8));
-  if (!cached && !bmethod)  // (the plain form runs the frontier SSSP per part whatever the form)
-    FAP_TRY(G->sssp_scratch.ensure(
-        (size_t)std::max(sssp_scratch_rows(G->n, (int)G->src.size()), 1) * (size_t)G->n * 4));
+  // These buffers are used on the context's stream only, so they grow in
+  // stream order: a cudaFree would wait for the whole device (every other
+  // graph's stream of a server included).  The synchronisation below makes
+  // the new buffers ready for the host copies that fill them.
   cudaStream_t st = G->ctx->stream;
+  if (!cached) FAP_TRY(G->F.ensure_async((size_t)std::max<int64_t>(foff, 1) * 4, st));
+  FAP_TRY(G->d_parts.ensure_async(std::max<size_t>(G->parts.size(), 1) * sizeof(PartDesc), st));
+  FAP_TRY(G->d_work.ensure_async(std::max<size_t>(G->work.size(), 1) * sizeof(MPWork), st));
+  FAP_TRY(G->d_thin.ensure_async(std::max<size_t>(G->thin.size(), 1) * 4, st));
+  FAP_TRY(G->d_src.ensure_async(std::max<size_t>(G->src.size(), 1) * 4, st));
+  FAP_TRY(G->d_srcrows.ensure_async(std::max<size_t>(G->srcrows.size(), 1) * 8, st));
+  if (!cached && !bmethod)  // (the plain form runs the frontier SSSP per part whatever the form)
+    FAP_TRY(G->sssp_scratch.ensure_async(
+        (size_t)std::max(sssp_scratch_rows(G->n, (int)G->src.size()), 1) * (size_t)G->n * 4, st));
+  G->pk = Pack16{};
+  if (G->pack16 && G->dtype == FAP_DTYPE_I32 && !G->work.empty()) {
+    const size_t np = G->parts.size();
+    const int64_t ntiles = G->ldD / kMinplusBN;
+    FAP_TRY(G->d_pk_off.ensure_async(np * (size_t)G->ldD * 4, st));
+    FAP_TRY(G->d_pk_range.ensure_async(np * (size_t)ntiles * 4, st));
+    FAP_TRY(G->d_pk_maxa.ensure_async(np * 4, st));
+    if (!G->d_pk_tiles.p) {
+      FAP_TRY(G->d_pk_tiles.ensure_async(2 * sizeof(unsigned long long), st));
+      FAP_CK(cudaMemsetAsync(G->d_pk_tiles.p, 0, 2 * sizeof(unsigned long long), st));
+    }
+    G->pk = Pack16{G->d_pk_off.as<int32_t>(), G->d_pk_range.as<int32_t>(), G->d_pk_maxa.as<int32_t>(),
+                   (int32_t)ntiles, G->d_pk_tiles.as<unsigned long long>()};
+  }
   FAP_CK(cudaStreamSynchronize(st));
   if (bmethod) FAP_TRY(prepare_bgraph(G, G->parts));
   FAP_CK(cudaMemcpy(G->d_parts.p, G->parts.data(), G->parts.size() * sizeof(PartDesc), cudaMemcpyHostToDevice));
@@ -964,6 +988,9 @@ int launch_paths(fap_dgraph *G, const PartDesc *dp, int np, int max_s, const T *
 }
 
 int ensure_in_edges(fap_dgraph *G);
+
+// Bounds buffers of the packed min-plus for the prepared batch, or null.
+const Pack16 *pack16_of(const fap_dgraph *G) { return G->pk.off != nullptr ? &G->pk : nullptr; }
 
 // Whether stage 1's SSSP runs in the tiled form.
 bool use_msbf(const fap_dgraph *G) {
@@ -1071,7 +1098,7 @@ int run_solve(fap_dgraph *G, int mode) {
     FAP_CK(launch_minplus_thin<T>(dp, G->d_thin.as<int32_t>(), (int)G->thin.size(), G->max_s, G->n, F, D,
                                   G->ldD, gid, ed2st, st, &L));
     FAP_CK(launch_minplus_parts<T>(dp, np, dw, (int)G->work.size(), G->n, F, G->max_ldf, D, G->ldD,
-                                   G->max_rows, gid, ed2st, status, st, &L));
+                                   G->max_rows, gid, ed2st, status, st, &L, pack16_of(G)));
     if (G->paths) FAP_TRY(launch_paths<T>(G, dp, np, G->max_s, F, &L));
     FAP_CK(record_event(c->ev[4], st));
   } else if (mode == FAP_MODE_BATCHED && G->last_cached) {
@@ -1086,7 +1113,7 @@ int run_solve(fap_dgraph *G, int mode) {
     FAP_CK(launch_minplus_thin<T>(dp, G->d_thin.as<int32_t>(), (int)G->thin.size(), G->max_s, G->n, cF, D,
                                   G->ldD, gid, ed2st, st, &L));
     FAP_CK(launch_minplus_parts<T>(dp, (int)G->K, dw, (int)G->work.size(), G->n, cF, G->cache_ldf, D,
-                                   G->ldD, G->max_rows, gid, ed2st, status, st, &L));
+                                   G->ldD, G->max_rows, gid, ed2st, status, st, &L, pack16_of(G)));
     if (G->paths) FAP_TRY(launch_paths<T>(G, dp, np, G->max_s, cF, &L));
     FAP_CK(record_event(c->ev[4], st));
   } else if (mode == FAP_MODE_BATCHED) {
@@ -1106,7 +1133,7 @@ int run_solve(fap_dgraph *G, int mode) {
     FAP_CK(launch_minplus_thin<T>(dp, G->d_thin.as<int32_t>(), (int)G->thin.size(), G->max_s, G->n, F, D,
                                   G->ldD, gid, ed2st, st, &L));
     FAP_CK(launch_minplus_parts<T>(dp, np, dw, (int)G->work.size(), G->n, F, G->max_ldf, D, G->ldD,
-                                   G->max_rows, gid, ed2st, status, st, &L));
+                                   G->max_rows, gid, ed2st, status, st, &L, pack16_of(G)));
     if (G->paths) FAP_TRY(launch_paths<T>(G, dp, np, G->max_s, F, &L));
     FAP_CK(record_event(c->ev[4], st));
   } else {
@@ -1125,7 +1152,7 @@ int run_solve(fap_dgraph *G, int mode) {
                                       G->ldD, gid, ed2st, st, &L));
       else
         FAP_CK(launch_minplus_parts<T>(dp, np, dw + w0, w1 - w0, G->n, F, G->max_ldf, D, G->ldD,
-                                       G->max_rows, gid, ed2st, status, st, &L));
+                                       G->max_rows, gid, ed2st, status, st, &L, pack16_of(G)));
       if (G->paths) FAP_TRY(launch_paths<T>(G, dp + i, 1, d.s, F, &L));
     }
     FAP_CK(record_event(c->ev[4], st));
@@ -1728,6 +1755,11 @@ extern "C" int fap_graph_set_param(fap_dgraph *G, const char *key, double value)
     G->last_ids.clear();
     return FAP_OK;
   }
+  if (std::strcmp(key, "minplus_pack16") == 0) {
+    G->pack16 = value != 0.0;
+    G->last_ids.clear();
+    return FAP_OK;
+  }
   if (std::strcmp(key, "floyd_per_cta") == 0) {
     G->floyd_per_cta = value != 0.0;
     return FAP_OK;
@@ -1823,6 +1855,21 @@ extern "C" double fap_graph_mean_weight(const fap_dgraph *G) { return G ? G->mea
 // ---------------------------------------------------------------------------
 // Memory release and asynchronous distance rows (used by the serving loop)
 // ---------------------------------------------------------------------------
+extern "C" int fap_graph_pack16_tiles(fap_dgraph *G, int64_t *packed, int64_t *total) try {
+  if (!G || !packed || !total) return fail(FAP_ERR_INVALID, "NULL argument");
+  *packed = *total = 0;
+  if (!G->d_pk_tiles.p) return FAP_OK;
+  DeviceGuard g(G->ctx->device);
+  unsigned long long h[2] = {0, 0};
+  FAP_CK(cudaMemcpyAsync(h, G->d_pk_tiles.p, sizeof(h), cudaMemcpyDeviceToHost, G->ctx->stream));
+  FAP_CK(cudaStreamSynchronize(G->ctx->stream));
+  *packed = (int64_t)h[0];
+  *total = (int64_t)h[1];
+  return FAP_OK;
+} catch (...) {
+  return fail_exception();
+}
+
 extern "C" int fap_graph_release(fap_dgraph *G) try {
   if (!G) return fail(FAP_ERR_INVALID, "NULL graph");
   DeviceGuard g(G->ctx->device);
@@ -1835,6 +1882,9 @@ extern "C" int fap_graph_release(fap_dgraph *G) try {
   G->P.release();
   G->d_dB.release();
   G->d_FB.release();
+  G->d_pk_off.release();
+  G->d_pk_range.release();
+  G->d_pk_maxa.release();
   G->max_rows = 0;
   std::fill(G->row_base.begin(), G->row_base.end(), -1);
   G->last_ids.clear();

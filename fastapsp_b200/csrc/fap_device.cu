@@ -27,6 +27,7 @@
 #include <atomic>
 #include <map>
 #include <mutex>
+#include <type_traits>
 #include <utility>
 
 namespace fapb {
@@ -679,36 +680,16 @@ cudaError_t launch_bdy_scatter(const PartDesc *parts, int nparts, const T *F, T 
 //   boundary rows of D), then for own-part columns j the closed Floyd value
 //   F[b+i][ed2st[j]-start] replaces it, as the reference's decode does.
 // ---------------------------------------------------------------------------
-template <typename T>
-__global__ void __launch_bounds__(MPCfg<T>::THREADS, 2)
-    minplus_part_kernel(const PartDesc *__restrict__ parts, const MPWork *__restrict__ work, int n,
-                        const T *__restrict__ F, T *D, int64_t ldD,
-                        const int32_t *__restrict__ graph_id, const int32_t *__restrict__ ed2st,
-                        const __grid_constant__ CUtensorMap mapF, const __grid_constant__ CUtensorMap mapD,
-                        int *status) {
-  using C = MPCfg<T>;
-  using TC = typename FloydCfg<T, kFloydTile>::TC;
-  extern __shared__ __align__(128) unsigned char mp_smem_raw[];
-  auto sm = tma_smem_init<T, TC>(mp_smem_raw);
-  const MPWork wk = work[blockIdx.y];
-  const PartDesc pd = parts[wk.pidx];
-  const int n0 = blockIdx.x * C::BN;
-  const int M = pd.s - pd.b, K = pd.b;
-  T *Cm = D + (pd.row_base + pd.b) * ldD;
-  T acc[C::TM][C::TN];
-  acc_fill<T, C>(acc, Dist<T>::inf());
-  // A = F rows b+m0.. of part wk.pidx (columns 0..b-1); B = D rows
-  // row_base..row_base+b-1 (the part's boundary rows).  Rows and columns past
-  // the part's extent are never stored; k past b is never read.
-  // The part's square in the arena (its index there: a batch index, or the
-  // part's slot in the resident cache).
-  const int fz = (int)(pd.f_off / ((int64_t)pd.ldf * pd.ldf));
-  if (!tma_minplus_tile<T, TC>(&mapF, 0, pd.b + wk.m0, fz, &mapD, n0, (int)pd.row_base, 0, K, acc,
-                               sm)) {
-    if (threadIdx.x == 0) set_status(status, kDevTmaTimeout);
-    return;
-  }
-
+// Epilogue of a min-plus tile: own-part columns take the closed Floyd value
+// (the reference's decode), then 16-byte streaming stores of the rows that
+// exist.
+template <typename T, class C>
+__device__ __forceinline__ void minplus_part_epilogue(const PartDesc &pd, const MPWork &wk, int n0, int n,
+                                                      const T *__restrict__ F, T *Cm, int64_t ldD,
+                                                      const int32_t *__restrict__ graph_id,
+                                                      const int32_t *__restrict__ ed2st,
+                                                      T (&acc)[C::TM][C::TN]) {
+  const int M = pd.s - pd.b;
   const int tid = threadIdx.x, ty = tid / C::TX, tx = tid % C::TX;
   // Own-part columns of this thread (fused decode).
   int own[C::TN];
@@ -747,6 +728,171 @@ __global__ void __launch_bounds__(MPCfg<T>::THREADS, 2)
         __stcs(reinterpret_cast<V *>(dst + tile_col<C>(tx, gj, 0)), v);
       }
     }
+}
+
+// ---------------------------------------------------------------------------
+// Stage 3: min-plus merge with the fused decode of own-part columns.
+// grid (ldD / BN, nwork): CTA (x, y) computes rows work[y].m0 .. +BM of the
+// part's inner block against columns x*BN .. +BN.
+//   R[i][j] = min(INF, min_{k<b} F[b+i][k] + S[k][j])   (S = the part's
+//   boundary rows of D), then for own-part columns j the closed Floyd value
+//   F[b+i][ed2st[j]-start] replaces it, as the reference's decode does.
+// PACK (int32): a tile whose entries provably fit (Pack16) runs the packed
+// 16-bit engine and shifts its results back by the column offsets; the
+// others run the int32 engine.  Both give the same int32 values.
+// ---------------------------------------------------------------------------
+template <typename T, bool PACK>
+__global__ void __launch_bounds__(MPCfg<T>::THREADS, 2)
+    minplus_part_kernel(const PartDesc *__restrict__ parts, const MPWork *__restrict__ work, int n,
+                        const T *__restrict__ F, T *D, int64_t ldD,
+                        const int32_t *__restrict__ graph_id, const int32_t *__restrict__ ed2st,
+                        const __grid_constant__ CUtensorMap mapF, const __grid_constant__ CUtensorMap mapD,
+                        int *status, Pack16 pk) {
+  using C = MPCfg<T>;
+  using TC = typename FloydCfg<T, kFloydTile>::TC;
+  extern __shared__ __align__(128) unsigned char mp_smem_raw[];
+  auto sm = tma_smem_init<T, TC>(mp_smem_raw);
+  const MPWork wk = work[blockIdx.y];
+  const PartDesc pd = parts[wk.pidx];
+  const int n0 = blockIdx.x * C::BN;
+  const int K = pd.b;
+  T *Cm = D + (pd.row_base + pd.b) * ldD;
+  T acc[C::TM][C::TN];
+  // A = F rows b+m0.. of part wk.pidx (columns 0..b-1); B = D rows
+  // row_base..row_base+b-1 (the part's boundary rows).  Rows and columns past
+  // the part's extent are never stored; k past b is never read.
+  // The part's square in the arena (its index there: a batch index, or the
+  // part's slot in the resident cache).
+  const int fz = (int)(pd.f_off / ((int64_t)pd.ldf * pd.ldf));
+  bool packed = false;
+  if constexpr (PACK) {
+    packed = __ldg(pk.maxA + wk.pidx) + __ldg(pk.range + (int64_t)wk.pidx * pk.ntiles + blockIdx.x) < kPackCap;
+    if (threadIdx.x == 0) {
+      atomicAdd(pk.tiles + 1, 1ull);
+      if (packed) atomicAdd(pk.tiles, 1ull);
+    }
+  }
+  if (packed) {
+    if constexpr (PACK) {
+      using P = Pack16Cfg<TC>;
+      const uintptr_t base = (reinterpret_cast<uintptr_t>(mp_smem_raw) + 127) & ~uintptr_t(127);
+      uint32_t *pbuf = reinterpret_cast<uint32_t *>(base + P::BUF_OFFSET);
+      int32_t *coff = reinterpret_cast<int32_t *>(pbuf + 2 * P::BUF_ELEMS);
+      for (int c = threadIdx.x; c < C::BN; c += blockDim.x)
+        coff[c] = __ldg(pk.off + (int64_t)wk.pidx * ldD + n0 + c);
+      uint32_t a16[4][8];
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 8; j++) a16[i][j] = kPackInit;
+      // (the engine's first barrier orders the column offsets before use)
+      if (!tma_minplus_tile16<TC>(&mapF, 0, pd.b + wk.m0, fz, &mapD, n0, (int)pd.row_base, 0, K, a16, sm,
+                                  pbuf, coff)) {
+        if (threadIdx.x == 0) set_status(status, kDevTmaTimeout);
+        return;
+      }
+      const int tx = threadIdx.x % C::TX;
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        const int32_t off = coff[tile_col<C>(tx, j / 4, j % 4)];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+          const int32_t lo = (int32_t)(int16_t)(a16[i][j] & 0xffffu);
+          const int32_t hi = (int32_t)(int16_t)(a16[i][j] >> 16);
+          // pair i = 2g + h holds rows 4g + 2h and 4g + 2h + 1 of the thread
+          const int r0 = 4 * (i / 2) + 2 * (i % 2);
+          acc[r0][j] = lo < kPackCap ? lo + off : Dist<T>::inf();
+          acc[r0 + 1][j] = hi < kPackCap ? hi + off : Dist<T>::inf();
+        }
+      }
+    }
+  } else {
+    acc_fill<T, C>(acc, Dist<T>::inf());
+    if (!tma_minplus_tile<T, TC>(&mapF, 0, pd.b + wk.m0, fz, &mapD, n0, (int)pd.row_base, 0, K, acc,
+                                 sm)) {
+      if (threadIdx.x == 0) set_status(status, kDevTmaTimeout);
+      return;
+    }
+  }
+  minplus_part_epilogue<T, C>(pd, wk, n0, n, F, Cm, ldD, graph_id, ed2st, acc);
+}
+
+// Packed-form bounds of a batch (see Pack16): one CTA per (column tile, work
+// item); only a part's first work item (m0 == 0) works, so each part is
+// scanned once.  Thread t owns column n0 + t and walks the part's b boundary
+// rows of D; columns past n read as having no finite entry.
+__global__ void __launch_bounds__(kMinplusBN)
+    pack16_cols_kernel(const PartDesc *__restrict__ parts, const MPWork *__restrict__ work, int n,
+                       const int32_t *__restrict__ D, int64_t ldD, Pack16 pk) {
+  const MPWork wk = work[blockIdx.y];
+  if (wk.m0 != 0) return;
+  const PartDesc pd = parts[wk.pidx];
+  const int j = blockIdx.x * kMinplusBN + threadIdx.x;
+  int32_t lo = INT32_MAX, hi = 0;
+  if (j < n) {
+    const int32_t *col = D + pd.row_base * ldD + j;
+    int k = 0;
+    for (; k + 4 <= pd.b; k += 4) {
+      int32_t v[4];
+#pragma unroll
+      for (int q = 0; q < 4; q++) v[q] = __ldg(col + (int64_t)(k + q) * ldD);
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+        if (v[q] < kInfI32) {
+          lo = min(lo, v[q]);
+          hi = max(hi, v[q]);
+        }
+    }
+    for (; k < pd.b; k++) {
+      const int32_t v = __ldg(col + (int64_t)k * ldD);
+      if (v < kInfI32) {
+        lo = min(lo, v);
+        hi = max(hi, v);
+      }
+    }
+  }
+  int32_t range = 0;
+  if (lo == INT32_MAX) lo = 0;
+  else range = hi - lo;
+  pk.off[(int64_t)wk.pidx * ldD + j] = lo;
+  // the tile's largest range
+  __shared__ int32_t red[kMinplusBN / 32];
+  for (int o = 16; o > 0; o >>= 1) range = max(range, __shfl_xor_sync(0xffffffffu, range, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x / 32] = range;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int32_t m = 0;
+    for (int w = 0; w < kMinplusBN / 32; w++) m = max(m, red[w]);
+    pk.range[(int64_t)wk.pidx * pk.ntiles + blockIdx.x] = m;
+  }
+}
+
+// Largest finite A = F[b+i][k] (i < s-b, k < b) of each part of the work
+// (one CTA per work item; a part's first item does it).  A negative entry
+// (never produced from non-negative weights) makes the part run in int32.
+__global__ void __launch_bounds__(256)
+    pack16_maxa_kernel(const PartDesc *__restrict__ parts, const MPWork *__restrict__ work,
+                       const int32_t *__restrict__ F, Pack16 pk) {
+  const MPWork wk = work[blockIdx.x];
+  if (wk.m0 != 0) return;
+  const PartDesc pd = parts[wk.pidx];
+  const int64_t cnt = (int64_t)(pd.s - pd.b) * pd.b;
+  int32_t m = 0;
+  for (int64_t e = threadIdx.x; e < cnt; e += blockDim.x) {
+    const int64_t i = e / pd.b, k = e % pd.b;
+    const int32_t v = __ldg(F + pd.f_off + (pd.b + i) * pd.ldf + k);
+    if (v < 0) m = kPackCap;
+    else if (v < kInfI32) m = max(m, v);
+  }
+  __shared__ int32_t red[8];
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x / 32] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int32_t x = 0;
+    for (int w = 0; w < 8; w++) x = max(x, red[w]);
+    pk.maxA[wk.pidx] = x;
+  }
 }
 
 // Thin-K variant (b <= kThinK): the product is store-bound, not
@@ -932,7 +1078,7 @@ template <typename T>
 cudaError_t launch_minplus_parts(const PartDesc *parts, int nparts, const MPWork *work, int nwork, int n,
                                  const T *F, int64_t ldf, T *D, int64_t ldD, int64_t drows,
                                  const int32_t *graph_id, const int32_t *ed2st, int *status,
-                                 cudaStream_t stream, int64_t *launches) {
+                                 cudaStream_t stream, int64_t *launches, const Pack16 *pk) {
   if (nwork <= 0) return cudaSuccess;
   using C = MPCfg<T>;
   using TC = typename FloydCfg<T, kFloydTile>::TC;
@@ -941,12 +1087,34 @@ cudaError_t launch_minplus_parts(const PartDesc *parts, int nparts, const MPWork
   cudaError_t e = make_tmap_3d(&mapF, F, f, ldf, ldf, nparts, TC::BK, TC::BM);
   if (e == cudaSuccess) e = make_tmap_3d(&mapD, D, f, ldD, drows, 1, TC::BN, TC::BK);
   if (e != cudaSuccess) return e;
-  const size_t smem = TC::SMEM_BYTES;
-  auto kern = minplus_part_kernel<T>;
-  e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
   dim3 grid((unsigned)(ldD / C::BN), (unsigned)nwork);
-  kern<<<grid, C::THREADS, smem, stream>>>(parts, work, n, F, D, ldD, graph_id, ed2st, mapF, mapD, status);
+  Pack16 none{};
+  bool done = false;
+  if constexpr (std::is_same<T, int32_t>::value) {
+    if (pk != nullptr) {
+      // bounds of the packed form for the work's parts, then the merge
+      if (pk->ntiles < (int)(ldD / C::BN)) return cudaErrorInvalidValue;
+      pack16_cols_kernel<<<grid, kMinplusBN, 0, stream>>>(parts, work, n, D, ldD, *pk);
+      pack16_maxa_kernel<<<(unsigned)nwork, 256, 0, stream>>>(parts, work, F, *pk);
+      *launches += 2;
+      using P = Pack16Cfg<TC>;
+      const size_t smem = P::SMEM_BYTES;
+      auto kern = minplus_part_kernel<T, true>;
+      e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+      kern<<<grid, C::THREADS, smem, stream>>>(parts, work, n, F, D, ldD, graph_id, ed2st, mapF, mapD, status,
+                                               *pk);
+      done = true;
+    }
+  }
+  if (!done) {
+    const size_t smem = TC::SMEM_BYTES;
+    auto kern = minplus_part_kernel<T, false>;
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    kern<<<grid, C::THREADS, smem, stream>>>(parts, work, n, F, D, ldD, graph_id, ed2st, mapF, mapD, status,
+                                             none);
+  }
   *launches += 1;
   return cudaGetLastError();
 }
@@ -2252,7 +2420,7 @@ cudaError_t launch_relax_peak(T *sink, int blocks, int iters, cudaStream_t strea
   template cudaError_t launch_minplus_parts<T>(const PartDesc *, int, const MPWork *, int, int,   \
                                                const T *, int64_t, T *, int64_t, int64_t,         \
                                                const int32_t *, const int32_t *, int *,           \
-                                               cudaStream_t, int64_t *);                          \
+                                               cudaStream_t, int64_t *, const Pack16 *);          \
   template cudaError_t launch_minplus_thin<T>(const PartDesc *, const int32_t *, int, int, int,   \
                                               const T *, T *, int64_t, const int32_t *,           \
                                               const int32_t *, cudaStream_t, int64_t *);          \

@@ -52,6 +52,20 @@ struct MPWork {
   int32_t m0;
 };
 
+// Packed 16-bit min-plus of one batch (int32 distances): per batch part
+// (index pidx) and column, the least finite entry of its boundary rows in D
+// (off); per column tile of kMinplusBN columns the largest finite entry minus
+// its column's off (range); per part the largest finite A = F[b+i][k]
+// (maxA).  A tile runs packed when maxA + range < kPackCap, otherwise in
+// int32.  Buffers: off [nparts][ldD], range [nparts][ntiles], maxA [nparts].
+struct Pack16 {
+  int32_t *off;
+  int32_t *range;
+  int32_t *maxA;
+  int32_t ntiles;
+  unsigned long long *tiles;  // [2]: tiles run packed, tiles run (cumulative)
+};
+
 constexpr int kFloydTile = 128;
 constexpr int kMinplusBM = 128;
 constexpr int kMinplusBN = 128;
@@ -138,11 +152,14 @@ cudaError_t launch_bdy_scatter(const PartDesc *parts, int nparts, const T *F, T 
 // columns taken from the closed Floyd matrices (fused decode).
 // (F is the batch's Floyd arena with leading dimension ldf and nparts parts;
 // D has drows rows.)
+// pk (int32 only, may be null): buffers of the packed 16-bit form; the
+// launcher first fills them for the work's parts, then every tile that
+// provably fits runs packed (two relaxations per DPX instruction).
 template <typename T>
 cudaError_t launch_minplus_parts(const PartDesc *parts, int nparts, const MPWork *work, int nwork, int n,
                                  const T *F, int64_t ldf, T *D, int64_t ldD, int64_t drows,
                                  const int32_t *graph_id, const int32_t *ed2st, int *status,
-                                 cudaStream_t stream, int64_t *launches);
+                                 cudaStream_t stream, int64_t *launches, const Pack16 *pk = nullptr);
 
 // Same for parts with at most kThinBoundary boundary vertices (store-bound
 // shape): thin_parts[0..nthin) are batch indices of such parts, max_m bounds

@@ -99,6 +99,19 @@ struct GSlot {
 
 }  // namespace
 
+// Kinds of host calls the worker times (fap_server_stats 11..18).
+enum HostStep : int {
+  kStepLaunch = 0,     // one launch(): assembling and queueing a batch
+  kStepComplete = 1,   // one complete(): retiring a finished batch
+  kStepCache = 2,      // fap_graph_cache_build
+  kStepRoom = 3,       // make_room (admission, evictions)
+  kStepReserve = 4,    // fap_graph_reserve (output buffer growth)
+  kStepSolve = 5,      // fap_solve of a sub-graph batch
+  kStepRows = 6,       // rows buffer + fap_graph_rows_async
+  kStepTail = 7,       // checksums, status and event queued after the batch
+  kHostSteps = 8
+};
+
 constexpr int kMaxGraphs = 256;
 constexpr int64_t kSmallRowsBytes = int64_t(32) << 20;
 
@@ -125,6 +138,15 @@ struct fap_server {
   int64_t outstanding = 0;  // submitted, not yet done/failed
   bool stop = false;
   std::thread worker;
+  // Host time of the worker's calls, the longest single call of each kind
+  // since the last reset (the worker is one thread, so a slow call delays
+  // every graph's next batch): indices are the HostStep values.
+  double host_max_ms[kHostSteps] = {};
+  void note_host(int step, double t0) {
+    const double ms = (now_s() - t0) * 1e3;
+    std::lock_guard<std::mutex> lk(mu);
+    host_max_ms[step] = std::max(host_max_ms[step], ms);
+  }
   // stats (guarded by mu)
   std::vector<double> lat_ms;
   int64_t entries = 0, batches = 0, resident_hits = 0, peak_bytes = 0, cache_builds = 0, failed = 0;
@@ -157,6 +179,17 @@ int serr_exception() {
     return serr(FAP_ERR_INVALID, "unknown C++ exception");
   }
 }
+}  // namespace
+
+namespace {
+// Times one host call of the worker into fap_server::host_max_ms.
+struct HostTimer {
+  fap_server *s;
+  int step;
+  double t0;
+  HostTimer(fap_server *srv, int st) : s(srv), step(st), t0(now_s()) {}
+  ~HostTimer() { s->note_host(step, t0); }
+};
 }  // namespace
 
 // Device bytes held: every graph's buffers and the server's per-graph
@@ -226,6 +259,7 @@ bool grow_dev(T **p, int64_t *cap, int64_t want) {
 // *hopeless is set when they cannot fit even after every busy graph
 // finishes (nothing else holds memory that could be freed).
 bool fap_server::make_room(int64_t need, int self, bool *hopeless) {
+  HostTimer timer(this, kStepRoom);
   *hopeless = false;
   if (held_bytes() + need <= budget) return true;
   std::vector<int> idle;
@@ -278,6 +312,7 @@ void fap_server::finish(Req *r, int state, int status) {
 // Retires g's finished batch: its status word and checksums are already in
 // pinned host memory; distances asked for on the host are copied now.
 bool fap_server::complete(GSlot &g) {
+  HostTimer timer(this, kStepComplete);
   int rc = fap_status_code(*g.status_host);
   if (cudaEventQuery(g.done) != cudaSuccess) {
     cudaGetLastError();
@@ -318,6 +353,7 @@ bool fap_server::complete(GSlot &g) {
 // Starts the next batch of graph gi, if one fits.  Returns whether anything
 // was started or answered.
 bool fap_server::launch(int gi) {
+  HostTimer timer(this, kStepLaunch);
   GSlot &g = *graphs[gi];
   bool progressed = false;
   // Sub-graph requests whose block is still resident: answer at once (the
@@ -349,7 +385,10 @@ bool fap_server::launch(int gi) {
     int built = 0;
     bool hopeless = false;
     if (fap_graph_cache_bytes(g.dg, &cb, &built) == FAP_OK && make_room(cb, gi, &hopeless) &&
-        fap_graph_cache_build(g.dg) == FAP_OK) {
+        [&] {
+          HostTimer t(this, kStepCache);
+          return fap_graph_cache_build(g.dg);
+        }() == FAP_OK) {
       cached = true;
       std::lock_guard<std::mutex> lk(mu);
       cache_builds++;
@@ -452,15 +491,20 @@ bool fap_server::launch(int gi) {
   const double t0 = now_s();
   if (rc == FAP_OK && kind == FAP_REQ_SUBGRAPH) {
     if (rows > g.reserved_rows) {
+      HostTimer t(this, kStepReserve);
       rc = fap_graph_reserve(g.dg, target);
       if (rc == FAP_OK) g.reserved_rows = target;
     }
-    if (rc == FAP_OK) rc = fap_solve(g.dg, parts.data(), (int32_t)parts.size(), FAP_MODE_BATCHED);
+    if (rc == FAP_OK) {
+      HostTimer t(this, kStepSolve);
+      rc = fap_solve(g.dg, parts.data(), (int32_t)parts.size(), FAP_MODE_BATCHED);
+    }
     if (want_cs)
       for (size_t i = 0; rc == FAP_OK && i < parts.size(); i++)
         rc = fap_graph_checksums_async(g.dg, parts[i], g.cs_dev + part_row[parts[i]]);
   } else if (rc == FAP_OK) {
     // every rows request of the batch in one launch sequence
+    HostTimer t(this, kStepRows);
     std::vector<int32_t> sources;
     for (Req *r : batch) sources.insert(sources.end(), r->ids.begin(), r->ids.end());
     const int64_t bytes = rows * (int64_t)g.n * 4;
@@ -489,6 +533,7 @@ bool fap_server::launch(int gi) {
       }
     }
   }
+  HostTimer tail_timer(this, kStepTail);
   if (rc == FAP_OK && want_cs &&
       cudaMemcpyAsync(g.cs_host, g.cs_dev, (size_t)rows * 8, cudaMemcpyDeviceToHost, g.stream) != cudaSuccess) {
     cudaGetLastError();
@@ -813,7 +858,15 @@ int fap_server_stats(fap_server *s, double *out, int32_t count) try {
                                          (double)s->resident_hits,
                                          (double)s->failed,
                                          (double)s->cache_builds,
-                                         s->busy_ms};
+                                         s->busy_ms,
+                                         s->host_max_ms[kStepLaunch],
+                                         s->host_max_ms[kStepComplete],
+                                         s->host_max_ms[kStepCache],
+                                         s->host_max_ms[kStepRoom],
+                                         s->host_max_ms[kStepReserve],
+                                         s->host_max_ms[kStepSolve],
+                                         s->host_max_ms[kStepRows],
+                                         s->host_max_ms[kStepTail]};
   for (int32_t i = 0; i < count; i++) out[i] = i < FAP_SERVER_NSTATS ? all[i] : 0.0;
   return FAP_OK;
 } catch (...) {
@@ -831,6 +884,7 @@ int fap_server_reset_stats(fap_server *s) try {
   s->failed = 0;
   s->cache_builds = 0;
   s->busy_ms = 0;
+  for (double &x : s->host_max_ms) x = 0;
   return FAP_OK;
 } catch (...) {
   return serr_exception();

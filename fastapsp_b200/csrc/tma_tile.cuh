@@ -148,4 +148,147 @@ __device__ __forceinline__ bool tma_minplus_tile(const CUtensorMap *mapA, int ax
   return true;
 }
 
+// ---------------------------------------------------------------------------
+// Packed 16-bit form (int32 distances that provably fit in 14 bits after a
+// per-column shift): one __viaddmin_s16x2 relaxes two outputs, the same
+// column of two rows.  Stages arrive as int32 tiles through the same TMA
+// ring; the CTA converts each stage into packed shared buffers:
+//   PA[k][p]  = (A[2p][k], A[2p+1][k])            row pairs, k-major
+//   PB[k][c]  = (B'[k][c], B'[k][c])              B' = B[k][c] - off[c]
+// with every entry clamped to kPackCap (the sentinel and anything at least
+// as large become kPackCap).  The caller guarantees, per tile, that every
+// finite A is >= 0, every finite B' is in [0, range] and
+// maxA + range < kPackCap: then every sum of finite entries is below
+// kPackCap, every sum with a clamped entry is at least kPackCap, no sum
+// exceeds 2 * kPackCap < 2^15, and a packed result r < kPackCap is exactly
+// min_k A[i][k] + B[k][c] - off[c] (r >= kPackCap: no finite path).
+// ---------------------------------------------------------------------------
+constexpr int32_t kPackCap = 16383;
+constexpr uint32_t kPackInit = 0x7FFE7FFEu;   // 32766 in both halves
+
+template <class C>
+struct Pack16Cfg {
+  static constexpr int PA_LD = C::BM / 2 + 2;      // padded k-row of PA (conflict-free stores)
+  static constexpr int PA_ELEMS = C::BK * PA_LD;
+  static constexpr int PB_ELEMS = C::BK * C::BN;
+  static constexpr int BUF_ELEMS = PA_ELEMS + PB_ELEMS;   // one buffer (two are used)
+  // after the ring (128-byte aligned) and its mbarriers (64 bytes): the two
+  // packed buffers, then the tile's column offsets
+  static constexpr int BUF_OFFSET = C::RING_BYTES + 64;
+  static constexpr int SMEM_BYTES = 128 + BUF_OFFSET + 2 * BUF_ELEMS * 4 + C::BN * 4;
+  static_assert(C::STAGES * 8 <= 64, "mbarriers fit before the packed buffers");
+  static_assert((PA_ELEMS * 4) % 16 == 0 && (BUF_ELEMS * 4) % 16 == 0, "16-byte aligned buffers");
+  static_assert(C::BM == 128 && C::BN == 128 && C::THREADS == 256, "thread mapping below");
+  static_assert((C::BK * C::BM / 2) % C::THREADS == 0 && (C::BK * C::BN) % C::THREADS == 0, "even split");
+};
+
+__device__ __forceinline__ uint32_t pack_pair(int32_t lo, int32_t hi) {
+  return (uint32_t)(lo & 0xffff) | ((uint32_t)hi << 16);
+}
+
+// Converts ring stage (As, Bs) (kc valid k of BK) into PA / PB.  coff: the
+// tile's BN column offsets in shared memory.
+template <class C>
+__device__ __forceinline__ void pack16_convert(const int32_t *As, const int32_t *Bs, uint32_t *PA,
+                                               uint32_t *PB, const int32_t *coff) {
+  using P = Pack16Cfg<C>;
+  const int tid = threadIdx.x;
+  // A: BK x BM/2 pairs; thread -> (k = tid % BK, p = tid / BK + q * THREADS / BK)
+#pragma unroll
+  for (int q = 0; q < (C::BK * C::BM / 2) / C::THREADS; q++) {
+    const int k = tid % C::BK, p = tid / C::BK + q * (C::THREADS / C::BK);
+    const int32_t a0 = min(As[(2 * p) * C::BK + k], kPackCap);
+    const int32_t a1 = min(As[(2 * p + 1) * C::BK + k], kPackCap);
+    PA[k * P::PA_LD + p] = pack_pair(a0, a1);
+  }
+  // B: BK x BN, column fastest
+#pragma unroll
+  for (int q = 0; q < (C::BK * C::BN) / C::THREADS; q++) {
+    const int e = tid + q * C::THREADS;
+    const int c = e % C::BN;
+    const int32_t v = Bs[e] >= kInfI32 ? kPackCap : min(Bs[e] - coff[c], kPackCap);
+    PB[e] = pack_pair(v, v);
+  }
+}
+
+// One converted chunk: per k, the thread's 4 row pairs (two 8-byte loads)
+// and 8 columns (two 16-byte loads), then 32 packed relaxations.
+template <class C>
+__device__ __forceinline__ void pack16_chunk_compute(const uint32_t *PA, const uint32_t *PB,
+                                                     uint32_t (&acc)[4][8], int ty, int tx, int kc) {
+  using P = Pack16Cfg<C>;
+#pragma unroll 4
+  for (int k = 0; k < kc; k++) {
+    uint32_t a[4], b[8];
+#pragma unroll
+    for (int g = 0; g < 2; g++) {
+      const uint2 v = *reinterpret_cast<const uint2 *>(PA + k * P::PA_LD + g * (C::BM / 4) + ty * 2);
+      a[2 * g] = v.x;
+      a[2 * g + 1] = v.y;
+    }
+#pragma unroll
+    for (int g = 0; g < 2; g++) {
+      const uint4 v = *reinterpret_cast<const uint4 *>(PB + k * C::BN + g * (C::BN / 2) + tx * 4);
+      b[4 * g + 0] = v.x; b[4 * g + 1] = v.y; b[4 * g + 2] = v.z; b[4 * g + 3] = v.w;
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+      for (int j = 0; j < 8; j++) acc[i][j] = __viaddmin_s16x2(a[i], b[j], acc[i][j]);
+  }
+}
+
+// The packed form of tma_minplus_tile (same boxes, same bounded waits).
+// pbuf: 2 * BUF_ELEMS words of shared memory; coff: BN column offsets in
+// shared memory, written before the call (the first barrier below orders
+// them before their use).
+template <class C>
+__device__ __forceinline__ bool tma_minplus_tile16(const CUtensorMap *mapA, int ax, int ay, int az,
+                                                   const CUtensorMap *mapB, int bx, int by, int bz,
+                                                   int K, uint32_t (&acc)[4][8], TmaSmem<int32_t, C> &sm,
+                                                   uint32_t *pbuf, const int32_t *coff) {
+  using P = Pack16Cfg<C>;
+  const int tid = threadIdx.x, ty = tid / C::TX, tx = tid % C::TX;
+  const int n = (int)ceil_div(K, C::BK);
+  if (n == 0) return true;
+  auto issue = [&](int c, int s) {
+    int32_t *As = sm.ring + s * C::STAGE_ELEMS;
+    int32_t *Bs = As + C::A_ELEMS;
+    mbar_arrive_expect_tx(&sm.bars[s], C::TX_BYTES);
+    tma_load_3d(As, mapA, ax + c * C::BK, ay, az, &sm.bars[s]);
+    tma_load_3d(Bs, mapB, bx, by + c * C::BK, bz, &sm.bars[s]);
+  };
+  fence_proxy_async_all();
+  __syncthreads();
+  if (tid == 0)
+    for (int c = 0; c < n && c < C::STAGES; c++) issue(c, c);
+  for (int c = 0; c < n; c++) {
+    const int s = c % C::STAGES;
+    const bool got = mbar_wait_bounded(&sm.bars[s], (sm.phase >> s) & 1u);
+    sm.phase ^= 1u << s;
+    uint32_t *PA = pbuf + (c & 1) * P::BUF_ELEMS;
+    uint32_t *PB = PA + P::PA_ELEMS;
+    if (got) {
+      const int32_t *As = sm.ring + s * C::STAGE_ELEMS;
+      pack16_convert<C>(As, As + C::A_ELEMS, PA, PB, coff);
+    }
+    fence_proxy_async_smem();  // this thread's reads of stage s precede its refill
+    // One barrier per chunk: after it the stage may be refilled (every
+    // thread has converted it) and the packed buffer read; the other packed
+    // buffer was last read in the previous chunk, before this barrier.
+    if (__syncthreads_or(!got)) {
+      for (int c2 = c + 1; c2 < n && c2 < c + C::STAGES; c2++) {
+        const int s2 = c2 % C::STAGES;
+        if (tid == 0) mbar_wait_bounded(&sm.bars[s2], (sm.phase >> s2) & 1u);
+        sm.phase ^= 1u << s2;
+      }
+      __syncthreads();
+      return false;
+    }
+    if (tid == 0 && c + C::STAGES < n) issue(c + C::STAGES, s);
+    pack16_chunk_compute<C>(PA, PB, acc, ty, tx, min(C::BK, K - c * C::BK));
+  }
+  return true;
+}
+
 }  // namespace fapb

@@ -514,6 +514,13 @@ class DeviceGraph:
         """1 SSSP, 2 boundary graph, 3 resident cache (see fap_graph_last_stage1)."""
         return int(lib().fap_graph_last_stage1(self._h))
 
+    def pack16_tiles(self):
+        """(min-plus tiles run in the packed 16-bit form, tiles run) over
+        every solve of this graph so far."""
+        a, b = ctypes.c_int64(), ctypes.c_int64()
+        check(lib().fap_graph_pack16_tiles(self._h, ctypes.byref(a), ctypes.byref(b)), "pack16_tiles")
+        return int(a.value), int(b.value)
+
     def stage1_name(self) -> str:
         """How stage 1 of the last solve ran, in words (fap_graph_stage1_name)."""
         return (lib().fap_graph_stage1_name(self._h) or b"").decode()

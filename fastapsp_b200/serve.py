@@ -44,6 +44,12 @@ class ServerStats:
     failed: int
     cache_builds: int
     busy_ms: float
+    # longest single host call of the worker thread by kind, ms (HOST_STEPS)
+    host_max_ms: dict = None
+
+
+# Kinds of worker host calls timed by the server (fap_server_stats 11-18).
+HOST_STEPS = ("launch", "complete", "cache_build", "admission", "reserve", "solve", "rows", "tail")
 
 
 class Request:
@@ -166,10 +172,11 @@ class Server:
         check(lib().fap_server_drain(self._h), "fap_server_drain")
 
     def stats(self) -> ServerStats:
-        v = np.zeros(11, np.float64)
-        check(lib().fap_server_stats(self._h, ptr(v), 11), "fap_server_stats")
+        v = np.zeros(19, np.float64)
+        check(lib().fap_server_stats(self._h, ptr(v), 19), "fap_server_stats")
+        host = dict(zip(HOST_STEPS, (float(x) for x in v[11:19])))
         return ServerStats(int(v[0]), int(v[1]), float(v[2]), float(v[3]), float(v[4]), int(v[5]),
-                           int(v[6]), int(v[7]), int(v[8]), int(v[9]), float(v[10]))
+                           int(v[6]), int(v[7]), int(v[8]), int(v[9]), float(v[10]), host)
 
     def reset_stats(self) -> None:
         check(lib().fap_server_reset_stats(self._h), "fap_server_reset_stats")

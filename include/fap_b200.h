@@ -166,8 +166,19 @@ FAP_API int fap_graph_sssp_rows(fap_dgraph *g, const int32_t *sources, int32_t c
  * checks convergence on the host, so a solve that uses it is not captured
  * in a CUDA graph); "tile_mb" (device memory for the 128-source tiles that
  * the tiled SSSP and the Bellman-Ford closure of the boundary graph run side
- * by side, at most 16 of them, at least one; default 384). */
+ * by side, at most 16 of them, at least one; default 384);
+ * "minplus_pack16" (int32 graphs, default 1: a min-plus tile of a part with
+ * more than 16 boundary vertices runs in packed 16-bit arithmetic, two
+ * relaxations per DPX instruction, when its values provably fit: every
+ * boundary-row column is shifted by its least finite entry and the part's
+ * largest finite inner-to-boundary distance plus the tile's largest shifted
+ * entry is below 16383; other tiles run in int32; the results are the same
+ * int32 values either way; 0: int32 everywhere). */
 FAP_API int fap_graph_set_param(fap_dgraph *g, const char *key, double value);
+
+/* Min-plus tiles run in the packed 16-bit form and in all, counted over
+ * every solve of g so far (see "minplus_pack16").  Synchronous. */
+FAP_API int fap_graph_pack16_tiles(fap_dgraph *g, int64_t *packed, int64_t *total);
 
 /* Tunes the SSSP bucket width: runs the SSSP stage on `sample` boundary
  * sources spread over all parts (0 = one full wave of CTAs) for each of the

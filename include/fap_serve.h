@@ -95,8 +95,15 @@ FAP_API int fap_server_drain(fap_server *s);
  *   3 p99 latency ms       4 mean latency ms       5 peak device bytes held
  *   6 batches launched     7 answered from resident blocks
  *   8 requests failed      9 resident caches built 10 device busy ms (sum of
- *   the finished batches' durations, over all graphs' streams). */
-#define FAP_SERVER_NSTATS 11
+ *   the finished batches' durations, over all graphs' streams)
+ *   11-18 the longest single host call of the worker thread, in ms, by kind
+ *   (one worker serves every graph, so a slow call delays every graph's next
+ *   batch): 11 assembling and queueing one batch (12-18 are parts of it or
+ *   follow it), 12 retiring one finished batch, 13 building a resident cache,
+ *   14 admission / eviction, 15 output buffer growth, 16 queueing a
+ *   sub-graph solve, 17 queueing a distance-row batch, 18 queueing its
+ *   checksums and status. */
+#define FAP_SERVER_NSTATS 19
 FAP_API int fap_server_stats(fap_server *s, double *out, int32_t count);
 FAP_API int fap_server_reset_stats(fap_server *s);
 
