@@ -64,6 +64,10 @@ def parse_args():
                     help="SSSP form of stage 1: 0 automatic, 1 frontier, 2 tiled Bellman-Ford")
     ap.add_argument("--bgraph-form", type=int, default=0, choices=[0, 1, 2],
                     help="boundary-graph closure: 0 by size, 1 Floyd, 2 Bellman-Ford + tiled expansion")
+    ap.add_argument("--no-tune-solve", action="store_true",
+                    help="keep the default min-plus arithmetic and Floyd form (no timing of the candidates)")
+    ap.add_argument("--no-queue", action="store_true",
+                    help="batched Floyd as three launches per pivot block instead of the work queue")
     ap.add_argument("--no-pack16", action="store_true",
                     help="min-plus tiles in int32 only (no packed 16-bit tiles)")
     ap.add_argument("--no-stage-cache", action="store_true",
@@ -603,21 +607,75 @@ def run_cache_only(args, dg, stream, world):
 EXTRA_WORKLOADS = ("grid512", "rmat16")
 
 
-def run_extra(args, name, ctx, relax_peak, hbm_peak, peak_kind):
+def start_extra(args, name):
+    """Loads a further workload on the host and starts the reference binary
+    on its parity sample in the background (the reference's serial min-plus
+    of a grid512 part takes minutes), so that it runs while the GPU is
+    measured.  The sample: the part with the fewest boundary vertices, then
+    the next ones with at least one boundary vertex."""
+    from fastapsp_b200 import workloads
+    from oracle import oracle as O
+    t0 = time.perf_counter()
+    wl = workloads.load(name)
+    bn = wl.bdy_num
+    order = sorted(range(1, wl.K + 1), key=lambda p: (int(bn[p]), p))
+    ppart = order[:1] + [p for p in order[1:] if int(bn[p]) > 0][:max(0, args.extra_parity_parts - 1)]
+    ppart = ppart[:max(0, args.extra_parity_parts)]
+    job = {"wl": wl, "parts": ppart, "procs": [], "tmp": None, "files": {}, "meta": None,
+           "t0": time.perf_counter(), "integral": bool(wl.edges.integral)}
+    if ppart and O.ref_available():
+        job["tmp"] = tempfile.TemporaryDirectory()
+        tmp = job["tmp"].name
+        pfile = os.path.join(tmp, "partition.bin")
+        (np.asarray(wl.graph.getGraphId(), dtype=np.int64) - 1).astype(np.int32).tofile(pfile)
+        job["meta"] = os.path.join(tmp, "meta.bin")
+        env = dict(os.environ, OMP_NUM_THREADS=str(max(1, min(8, (os.cpu_count() or 1) // 4))),
+                   FAP_PARTITION_FILE=pfile)
+        for i, p in enumerate(ppart):
+            f = os.path.join(tmp, f"out_{p}.bin")
+            job["files"][p] = f
+            cmd = [O.REF_BIN, "--dir", wl.root, "-f", wl.name, "-k", str(wl.K),
+                   "-direct", str(int(wl.edges.directed)), "-weight", str(int(wl.edges.weighted)),
+                   "--parts", str(p), "--quiet", "--rowsum" if job["integral"] else "--dist", f]
+            if i == 0:
+                cmd += ["--meta", job["meta"]]
+            job["procs"].append(subprocess.Popen(cmd, stdout=subprocess.DEVNULL, stderr=subprocess.PIPE,
+                                                 text=True, env=env))
+    log(f"{name} loaded in {time.perf_counter() - t0:.1f} s: {wl.describe()}; reference started on "
+        f"parts {ppart}")
+    return job
+
+
+def finish_extra_parity(job, gpu, dtype):
+    """Waits for the reference processes of start_extra and compares."""
+    from oracle import oracle as O
+    if not job["procs"]:
+        return {"unavailable": "reference binary absent"} if job["parts"] else None
+    for pr in job["procs"]:
+        _, err = pr.communicate(timeout=1800)
+        if pr.returncode != 0:
+            return {"unavailable": f"reference process failed: {err[-300:]}"}
+    wl = job["wl"]
+    parity = compare_parity(wl, gpu, job["files"], dtype, wl.graph.getMapping(), O.read_meta(job["meta"]))
+    parity["parts_chosen"] = "fewest boundary vertices (one part, then parts with boundary vertices)"
+    parity["parts_ids"] = job["parts"]
+    parity["reference_s"] = round(time.perf_counter() - job["t0"], 2)
+    job["tmp"].cleanup()
+    return parity
+
+
+def run_extra(args, job, ctx, relax_peak, hbm_peak, peak_kind):
     """A further workload of the same metric on one GPU: batched solves of
     every part (timed with CUDA events on the library's stream, inputs
     resident, L2 flushed between steps), its min-plus as a fraction of the
     measured relaxation peak, and parity of sampled parts against the
-    reference binary under the same partition.  The sampled parts are the
-    ones with the fewest boundary vertices (the reference's serial min-plus
-    and Floyd then finish in seconds); the reference runs them side by side
-    with all host threads split between them."""
+    reference binary under the same partition (started by start_extra)."""
     import torch
 
-    from fastapsp_b200 import FAP_MODE_BATCHED, DeviceGraph, autotune, workloads
+    from fastapsp_b200 import FAP_MODE_BATCHED, DeviceGraph, autotune
     from fastapsp_b200.sharding import group_parts_by_rows, rows_of
-    t0 = time.perf_counter()
-    wl = workloads.load(name)
+    wl = job["wl"]
+    name = wl.name
     n = wl.n
     vn, vo, bn = wl.ver_num, wl.ver_offset, wl.bdy_num
     ro, col, w = wl.csr()
@@ -627,6 +685,7 @@ def run_extra(args, name, ctx, relax_peak, hbm_peak, peak_kind):
     dtype = dg.dtype
     dg.set_parts(wl.K, gid, st2ed, vn, vo, bn)
     dg.set_param("minplus_pack16", 0 if args.no_pack16 else 1)
+    dg.set_param("floyd_queue", 0 if args.no_queue else 1)
     ldD = (n + 127) // 128 * 128
     stream = torch.cuda.current_stream()
     mine = list(range(1, wl.K + 1))
@@ -641,7 +700,7 @@ def run_extra(args, name, ctx, relax_peak, hbm_peak, peak_kind):
     groups = [mine] if all_rows <= budget_rows else group_parts_by_rows(mine, vn, budget_rows)
     dg.reserve(max(rows_of(g, vn) for g in groups) if len(groups) > 1 else 0)
     tuned = autotune.tune_sssp(dg, vn, bn)
-    log(f"{name} loaded in {time.perf_counter() - t0:.1f} s: {wl.describe()}, {len(groups)} group(s)")
+    log(f"{name}: {len(groups)} group(s)")
 
     def step():
         if staged:
@@ -649,65 +708,76 @@ def run_extra(args, name, ctx, relax_peak, hbm_peak, peak_kind):
         for grp in groups:
             dg.solve(grp, FAP_MODE_BATCHED, check_errors=False)
 
+    def timed_first_group():
+        # one stage-1-2 pass (when staged) and the first group: the choices
+        # tuned affect both, and the other groups repeat the first
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        if staged:
+            dg.cache_build(rebuild=True)
+        dg.solve(groups[0], FAP_MODE_BATCHED, check_errors=False)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    solve_tuned = None
+    if not (args.no_pack16 or args.no_queue or args.no_tune_solve):
+        solve_tuned = autotune.tune_solve(dg, vn, bn, timed_first_group, reps=1)
+        dg.check()
+        log(f"{name}: solve form {solve_tuned['params']} ({'cached' if solve_tuned['cached'] else 'tuned'}: "
+            f"{solve_tuned['ms']} ms)")
+
     for _ in range(args.extra_warmup):
         step()
     dg.check()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     torch.cuda.synchronize()
-    ms, mp_ms = [], []
+    ms, mp_ms, fl_ms = [], [], []
     for _ in range(args.extra_steps):
         flush.zero_()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        mp = 0.0
+        mp = fl = 0.0
         if staged:
             dg.cache_build(rebuild=True)
         for grp in groups:
             dg.solve(grp, FAP_MODE_BATCHED, check_errors=False)
             mp += float(dg.last_timing()[3])
+            fl += float(dg.last_timing()[2])
         e1.record(stream)
         e1.synchronize()
         ms.append(e0.elapsed_time(e1))
         mp_ms.append(mp)
+        fl_ms.append(fl)
     dg.check()
     del flush
     ms_step = float(np.mean(ms))
     mp_step = float(np.mean(mp_ms))
     mp_relax = float(sum(float(vn[p] - bn[p]) * float(bn[p]) * n for p in mine))
     mp_bytes = float(sum(4.0 * ((vn[p] - bn[p]) * n + (vn[p] - bn[p]) * bn[p] + bn[p] * n) for p in mine))
+    # With stage 1 by SSSP and int32-only min-plus tiles (float32, or packing
+    # off), the min-plus tiles run inside the Floyd work queue: the stage
+    # timings then hold Floyd and min-plus together.
+    form = solve_tuned["params"] if solve_tuned else {"minplus_pack16": int(not args.no_pack16),
+                                                      "floyd_queue": int(not args.no_queue)}
+    stage1_now = dg.stage1_name()
+    mp_in_queue = (bool(form["floyd_queue"]) and stage1_now.startswith("SSSP")
+                   and (dtype != 0 or not form["minplus_pack16"]))
+    mp_note = None
+    if mp_in_queue:
+        mp_step += float(np.mean(fl_ms))
+        mp_relax += float(sum(float(vn[p]) ** 3 for p in mine))
+        mp_note = ("the min-plus tiles ran inside the Floyd work queue: time and relaxations of "
+                   "Floyd-Warshall and min-plus together")
     a = mp_relax / (mp_step * 1e-3) / 1e9
-    # parity: the parts with the fewest boundary vertices
-    order = sorted(mine, key=lambda p: (int(bn[p]), p))
-    ppart = order[:max(0, args.extra_parity_parts)]
-    parity = None
-    if ppart:
-        gpu = gpu_parity_blocks(dg, groups, ppart, dtype, staged, FAP_MODE_BATCHED)
+    gpu = gpu_parity_blocks(dg, groups, job["parts"], dtype, staged, FAP_MODE_BATCHED) if job["parts"] else {}
     stage1 = dg.stage1_name()
     pk_tiles = dg.pack16_tiles()
     del dg
     torch.cuda.synchronize()
     torch.cuda.empty_cache()
-    if ppart:
-        from oracle import oracle as O
-        threads = max(1, (os.cpu_count() or 1) // len(ppart))
-        with tempfile.TemporaryDirectory() as tmp:
-            pfile = os.path.join(tmp, "partition.bin")
-            (np.asarray(gid, dtype=np.int64) - 1).astype(np.int32).tofile(pfile)
-            meta_f = os.path.join(tmp, "meta.bin")
-            files = {p: os.path.join(tmp, f"out_{p}.bin") for p in ppart}
-            extra = {i: ["--rowsum" if dtype == 0 else "--dist", files[p]] for i, p in enumerate(ppart)}
-            extra[0] = extra[0] + ["--meta", meta_f]
-            if O.ref_available():
-                tr = time.perf_counter()
-                kind, res = run_reference_sample(wl, [[p] for p in ppart], len(ppart), extra=extra,
-                                                 partition_file=pfile, threads=threads)
-                parity = compare_parity(wl, gpu, files, dtype, st2ed, O.read_meta(meta_f))
-                parity["parts_chosen"] = "fewest boundary vertices"
-                parity["reference_s"] = round(time.perf_counter() - tr, 2)
-            else:
-                parity = {"unavailable": "reference binary absent"}
-        del gpu
     out = {
         "value": all_rows * n / (ms_step * 1e-3), "unit": UNIT, "ms_per_step": ms_step,
         "steps": args.extra_steps, "warmup": args.extra_warmup,
@@ -715,17 +785,20 @@ def run_extra(args, name, ctx, relax_peak, hbm_peak, peak_kind):
         "config": {**wl.describe(), "groups": len(groups), "stage_cache": staged, "stage1": stage1,
                    "minplus_packed_tiles": {"packed": pk_tiles[0], "total": pk_tiles[1]},
                    "sssp_delta_factor": tuned["factor"],
+                   "solve_form": (solve_tuned["params"] if solve_tuned else
+                                  {"minplus_pack16": int(not args.no_pack16), "floyd_queue": int(not args.no_queue)}),
                    "l2": "256 MB buffer written between timed steps (outside the events); "
                          f"each step writes {4 * n * all_rows / 1e9:.1f} GB of distances"},
         "minplus": {"ms": mp_step, "relax": mp_relax, "bytes": mp_bytes, "achieved_grelax_s": a,
                     "frac_of_relax_peak": a / (relax_peak / 1e9),
                     "frac_of_hbm": mp_bytes / (mp_step * 1e-3) / 1e9 / hbm_peak,
-                    "peaks": f"relaxation peak measured live (fap_measure_relax_peak); HBM {peak_kind}"},
-        "parity": parity,
+                    "peaks": f"relaxation peak measured live (fap_measure_relax_peak); HBM {peak_kind}",
+                    "note": mp_note},
+        "parity": None,
     }
     log(f"{name}: {ms_step:.1f} ms/step, {out['value']:.4g} entries/s, min-plus {mp_step:.1f} ms "
-        f"({out['minplus']['frac_of_relax_peak']:.2f} of the relaxation peak), parity {parity}")
-    return out
+        f"({out['minplus']['frac_of_relax_peak']:.2f} of the relaxation peak)")
+    return out, gpu, dtype
 
 
 def main_fap(args):
@@ -755,6 +828,17 @@ def main_fap(args):
     def allsum(x):
         return reduce_over_ranks(x, "sum", device="cuda")
 
+    # further workloads: loaded on the host first, so that the reference's
+    # parity runs of their sampled parts proceed while the GPU is measured
+    extra_jobs = {}
+    if rank == 0 and world == 1 and args.extra:
+        for name in [x for x in args.extra.split(",") if x]:
+            try:
+                extra_jobs[name] = start_extra(args, name)
+            except Exception as e:  # noqa: BLE001 - reported in the line, not fatal
+                extra_jobs[name] = e
+                log(f"{name}: {e}")
+
     t_load = time.perf_counter()
     wl = workloads.load(args.workload)
     log(f"workload {wl.name} loaded in {time.perf_counter() - t_load:.1f} s: {wl.describe()}")
@@ -781,6 +865,7 @@ def main_fap(args):
     dg.set_param("sssp_form", args.sssp_form)
     dg.set_param("bgraph_form", args.bgraph_form)
     dg.set_param("minplus_pack16", 0 if args.no_pack16 else 1)
+    dg.set_param("floyd_queue", 0 if args.no_queue else 1)
     if args.cache_only:
         run_cache_only(args, dg, stream, world)
         if world > 1:
@@ -818,6 +903,22 @@ def main_fap(args):
     tuned = autotune.tune_sssp(dg, vn, bn)
     log(f"SSSP delta {tuned['delta']:.6g} ({'cached' if tuned['cached'] else 'tuned'}: "
         f"{tuned['key']}, factor {tuned['factor']})")
+
+    def timed_step():
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        solve_all(FAP_MODE_BATCHED)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    solve_tuned = None
+    if not (args.no_pack16 or args.no_queue or args.no_tune_solve):
+        solve_tuned = autotune.tune_solve(dg, vn, bn, timed_step)
+        dg.check()
+        log(f"solve form {solve_tuned['params']} ({'cached' if solve_tuned['cached'] else 'tuned'}: "
+            f"{solve_tuned['ms']} ms)")
     relax_peak = ctx.relax_peak(dtype)
     hbm_peak, peak_kind = read_peaks()
 
@@ -976,6 +1077,12 @@ def main_fap(args):
     stage_roof["minplus"]["frac_of_relax_peak"] = (stage_roof["minplus"]["achieved_grelax_s"]
                                                    / peak_grelax)
     stage_roof["minplus"]["frac_of_hbm"] = stage_roof["minplus"]["achieved_gbs"] / hbm_peak
+    form_now = (solve_tuned["params"] if solve_tuned else
+                {"minplus_pack16": int(not args.no_pack16), "floyd_queue": int(not args.no_queue)})
+    if (form_now["floyd_queue"] and stage1_used.startswith("SSSP")
+            and (dtype != 0 or not form_now["minplus_pack16"])):
+        stage_roof["minplus"]["note"] = ("the min-plus tiles of parts with more than 16 boundary vertices "
+                                         "ran inside the Floyd work queue: their time is in the floyd stage")
     stage_roof["sssp"]["frac_of_hbm"] = stage_roof["sssp"]["achieved_gbs"] / hbm_peak
 
     # ---- e2e through the public API: host inputs in, every block out ----
@@ -1020,17 +1127,24 @@ def main_fap(args):
         torch.cuda.empty_cache()
         serving = run_serving(args, local)
 
-    # ---- further workloads (rank 0, N=1 only) ----
+    # ---- further workloads (rank 0, N=1 only); their reference parity
+    # processes started before the headline measurement ----
     extras = None
-    if rank == 0 and world == 1 and args.extra:
+    if extra_jobs:
         extras = {}
         torch.cuda.empty_cache()
-        for name in [x for x in args.extra.split(",") if x]:
+        for name, job in extra_jobs.items():
+            gpu = None
             try:
-                extras[name] = run_extra(args, name, ctx, relax_peak, hbm_peak, peak_kind)
+                if isinstance(job, Exception):
+                    raise job
+                extras[name], gpu, xdtype = run_extra(args, job, ctx, relax_peak, hbm_peak, peak_kind)
+                extras[name]["parity"] = finish_extra_parity(job, gpu, xdtype)
+                log(f"{name}: parity {extras[name]['parity']}")
             except Exception as e:  # noqa: BLE001 - reported in the line, not fatal
                 extras[name] = {"unavailable": str(e)[:300]}
                 log(f"{name}: {e}")
+            del gpu
             torch.cuda.empty_cache()
 
     # ---- CPU baseline (rank 0, N=1 only) and parity of the same parts ----
@@ -1086,7 +1200,11 @@ def main_fap(args):
                                                   "SSSP, gather, Floyd, -")}
                                       if staged and cache_phases else None),
                       "sssp_delta": {"value": tuned["delta"], "factor_of_mean_weight": tuned["factor"],
-                                     "bucket": tuned["key"], "from_cache": tuned["cached"]}},
+                                     "bucket": tuned["key"], "from_cache": tuned["cached"]},
+                      "solve_form": ({"params": solve_tuned["params"], "candidates_ms": solve_tuned["ms"],
+                                      "from_cache": solve_tuned["cached"]} if solve_tuned else
+                                     {"params": {"minplus_pack16": int(not args.no_pack16),
+                                                 "floyd_queue": int(not args.no_queue)}})},
             "plain": {"value": plain_value, "ms_per_step": plain_max / max(len(plain_ms), 1),
                       "steps": len(plain_ms)},
             "batched_over_plain": (value / plain_value) if plain_value else None,

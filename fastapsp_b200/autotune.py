@@ -1,5 +1,10 @@
-"""Autotuner for the SSSP bucket width (delta), cached per (part size,
-boundary count) bucket.
+"""Autotuners, cached per (part size, boundary count) bucket:
+
+  tune_sssp   the SSSP bucket width (delta);
+  tune_solve  the min-plus arithmetic of the part tiles (packed 16-bit where
+              the distances provably fit, or int32 throughout) and the form
+              of the batched Floyd (one persistent launch over a work queue,
+              or three launches per pivot block), timed as whole solves.
 
 The best delta depends on the graph: on road-like graphs with deep
 shortest-path trees wide buckets win (few rounds), on small-world graphs
@@ -83,3 +88,46 @@ def tune_sssp(dg, ver_num, bdy_num, *, path: str | None = None, force: bool = Fa
         pass  # a read-only home: the tuned value still applies to dg
     delta = 1e9 if factor is None else factor * mw
     return {**entry, "key": key, "delta": delta, "cached": False}
+
+
+# Candidates of tune_solve: the min-plus arithmetic and the batched Floyd's
+# form.  (The tile shape itself, 128 x 128 outputs per CTA with 8 x 8 per
+# thread and K chunks of 16 through a 4-stage TMA ring, is fixed: it is the
+# largest that keeps two CTAs and 128 registers per thread on an SM.)
+SOLVE_CANDIDATES = tuple({"minplus_pack16": p, "floyd_queue": q} for p in (1, 0) for q in (1, 0))
+
+
+def tune_solve(dg, ver_num, bdy_num, step, *, reps: int = 2, path: str | None = None,
+               force: bool = False) -> dict:
+    """Sets dg's min-plus arithmetic and Floyd form from the cache, or tunes
+    them: for each candidate (float32 graphs: the Floyd form only, packing
+    applies to int32) one untimed and `reps` timed calls of `step()`, which
+    runs one solve step of the job being measured and returns its device
+    time in ms; the fastest candidate is applied and cached under
+    "solve:" + the SSSP bucket key.  Returns the entry plus 'key' and
+    'cached'."""
+    path = path or cache_path()
+    key = "solve:" + bucket_key(ver_num, bdy_num, dg.dtype)
+    cache = _load(path)
+    entry = cache.get(key)
+    if entry is not None and not force:
+        for k, v in entry["params"].items():
+            dg.set_param(k, v)
+        return {**entry, "key": key, "cached": True}
+    cands = [c for c in SOLVE_CANDIDATES if dg.dtype == 0 or c["minplus_pack16"] == 0]
+    ms = []
+    for c in cands:
+        for k, v in c.items():
+            dg.set_param(k, v)
+        step()
+        ms.append(float(np.median([step() for _ in range(max(1, reps))])))
+    best = int(np.argmin(ms))
+    for k, v in cands[best].items():
+        dg.set_param(k, v)
+    entry = {"params": cands[best], "ms": [round(x, 4) for x in ms], "candidates": cands}
+    cache[key] = entry
+    try:
+        _save(path, cache)
+    except OSError:
+        pass  # a read-only home: the tuned choice still applies to dg
+    return {**entry, "key": key, "cached": False}

@@ -161,6 +161,45 @@ struct fap_ctx {
   bool destroy_pending = false;  // fap_ctx_destroy called while graphs were live
 };
 
+// Device copy of a FloydQueue item list (see fap_internal.h) and its
+// counters.  Items: for every pivot block kb, the Floyd-1 items of all parts
+// that have block kb, then their Floyd-2 items, then their Floyd-3 items;
+// after all Floyd items the boundary-row scatter items of every part
+// (nfloyd Floyd items, nitems in all).
+struct QueueBuf {
+  DevBuf items, cnt;
+  int32_t nfloyd = 0, nitems = 0, stride = 2, nparts = 0;
+};
+
+namespace {
+std::vector<QItem> floyd_queue_items(const std::vector<PartDesc> &parts, int32_t *nfloyd, int32_t *max_nb) {
+  std::vector<QItem> it;
+  int mnb = 0;
+  for (const PartDesc &d : parts) mnb = std::max<int>(mnb, (int)ceil_div(std::max(d.s, 1), kFloydTile));
+  for (int kb = 0; kb < mnb; kb++) {
+    for (size_t p = 0; p < parts.size(); p++) {
+      const int nb = (int)ceil_div(parts[p].s, kFloydTile);
+      if (kb < nb) it.push_back(QItem{kQFloyd1, (int32_t)p, kb, 0});
+    }
+    for (size_t p = 0; p < parts.size(); p++) {
+      const int nb = (int)ceil_div(parts[p].s, kFloydTile);
+      if (kb < nb)
+        for (int t = 0; t < 2 * (nb - 1); t++) it.push_back(QItem{kQFloyd2, (int32_t)p, kb, t});
+    }
+    for (size_t p = 0; p < parts.size(); p++) {
+      const int nb = (int)ceil_div(parts[p].s, kFloydTile);
+      if (kb < nb)
+        for (int t = 0; t < (nb - 1) * (nb - 1); t++) it.push_back(QItem{kQFloyd3, (int32_t)p, kb, t});
+    }
+  }
+  *nfloyd = (int32_t)it.size();
+  for (size_t p = 0; p < parts.size(); p++)
+    for (int r = 0; r < parts[p].b; r += kQScatterRows) it.push_back(QItem{kQScatter, (int32_t)p, r, 0});
+  *max_nb = mnb;
+  return it;
+}
+}  // namespace
+
 struct fap_dgraph {
   fap_ctx *ctx = nullptr;
   int32_t n = 0;
@@ -206,11 +245,16 @@ struct fap_dgraph {
   // fit (int32 graphs; Pack16): bounds buffers of the prepared batch.
   bool pack16 = true;
   DevBuf d_pk_off, d_pk_range, d_pk_maxa, d_pk_tiles;
+  // Work queue of the batched Floyd (FloydQueue): the batch's items and
+  // counters, and the resident cache build's (its parts are all parts).
+  bool floyd_queue = true;
+  QueueBuf q, cq;
   Pack16 pk{};
   // CUDA graph of the batched launch sequence (replayed while nothing that
   // it captured changes: batch, buffers, parameters, stream)
   bool use_graph = true;
   uint64_t epoch = 1;
+  uint64_t direct_epoch = 0;  // epoch of the last batched solve launched directly (0: none)
   cudaGraphExec_t gexec = nullptr;
   uint64_t gexec_epoch = 0;
   cudaStream_t gexec_stream = nullptr;
@@ -480,7 +524,7 @@ extern "C" int fap_graph_destroy(fap_dgraph *G) try {
                       &G->d_msbf_items, &G->d_msbf_act, &G->d_msbf_changed, &G->d_bitro, &G->d_bitcol,
                       &G->d_botro, &G->d_botcol, &G->d_bitw, &G->d_bitems, &G->d_bDt, &G->d_bact, &G->d_bpact,
                       &G->d_bgpart, &G->d_bpcolmap, &G->d_grow, &G->d_pk_off, &G->d_pk_range,
-                      &G->d_pk_maxa, &G->d_pk_tiles})
+                      &G->d_pk_maxa, &G->d_pk_tiles, &G->q.items, &G->q.cnt, &G->cq.items, &G->cq.cnt})
       b->release();
     if (G->h_changed) cudaFreeHost(G->h_changed);
     for (cudaEvent_t &ev : G->cev)
@@ -946,7 +990,19 @@ int prepare_batch(fap_dgraph *G, const std::vector<int32_t> &ids, bool cached, b
     G->pk = Pack16{G->d_pk_off.as<int32_t>(), G->d_pk_range.as<int32_t>(), G->d_pk_maxa.as<int32_t>(),
                    (int32_t)ntiles, G->d_pk_tiles.as<unsigned long long>()};
   }
+  std::vector<QItem> qitems;
+  if (!cached) {
+    int32_t mnb = 0;
+    qitems = floyd_queue_items(G->parts, &G->q.nfloyd, &mnb);
+    G->q.nitems = (int32_t)qitems.size();
+    G->q.stride = 2 + 2 * mnb;
+    G->q.nparts = (int32_t)G->parts.size();
+    FAP_TRY(G->q.items.ensure_async(std::max<size_t>(qitems.size(), 1) * sizeof(QItem), st));
+    FAP_TRY(G->q.cnt.ensure_async(((size_t)G->q.nparts * G->q.stride + 2) * 4, st));
+  }
   FAP_CK(cudaStreamSynchronize(st));
+  if (!qitems.empty())
+    FAP_CK(cudaMemcpy(G->q.items.p, qitems.data(), qitems.size() * sizeof(QItem), cudaMemcpyHostToDevice));
   if (bmethod) FAP_TRY(prepare_bgraph(G, G->parts));
   FAP_CK(cudaMemcpy(G->d_parts.p, G->parts.data(), G->parts.size() * sizeof(PartDesc), cudaMemcpyHostToDevice));
   if (!G->work.empty())
@@ -988,6 +1044,21 @@ int launch_paths(fap_dgraph *G, const PartDesc *dp, int np, int max_s, const T *
 }
 
 int ensure_in_edges(fap_dgraph *G);
+
+// Runs a FloydQueue: the Floyd items (and with `scatter` the boundary-row
+// scatter into D, and with mp_work > 0 that many min-plus work items' tiles).
+template <typename T>
+cudaError_t run_floyd_queue(fap_dgraph *G, QueueBuf &qb, const PartDesc *dp, T *F, int64_t ldf, bool scatter,
+                            const MPWork *dw, int mp_work, T *D, int64_t drows, int *status, int64_t *L) {
+  cudaStream_t st = G->ctx->stream;
+  cudaError_t e = cudaMemsetAsync(qb.cnt.p, 0, ((size_t)qb.nparts * qb.stride + 2) * 4, st);
+  if (e != cudaSuccess) return e;
+  FloydQueue q{qb.items.as<const QItem>(), scatter ? qb.nitems : qb.nfloyd, mp_work, qb.cnt.as<int32_t>(),
+               qb.stride, qb.nparts};
+  return launch_floyd_queue<T>(dp, qb.nparts, F, ldf, q, dw, G->n, D, G->ldD, drows, G->d_st2ed.as<const int32_t>(),
+                               G->d_gid.as<const int32_t>(), G->d_ed2st.as<const int32_t>(), status, st, L,
+                               nullptr);
+}
 
 // Bounds buffers of the packed min-plus for the prepared batch, or null.
 const Pack16 *pack16_of(const fap_dgraph *G) { return G->pk.off != nullptr ? &G->pk : nullptr; }
@@ -1088,8 +1159,11 @@ int run_solve(fap_dgraph *G, int mode) {
     FAP_CK(record_event(c->ev[0], st));
     FAP_CK(launch_gather<T>(dp, np, G->max_ldf, ro, col, w, gid, st2ed, ed2st, D, G->ldD, F, st, &L));
     FAP_CK(record_event(c->ev[1], st));
-    FAP_CK(launch_floyd_parts_multi<T>(dp, np, (int)ceil_div(G->max_s, kFloydTile), F, G->max_ldf,
-                                       status, st, &L));
+    if (G->floyd_queue)
+      FAP_CK(run_floyd_queue<T>(G, G->q, dp, F, G->max_ldf, false, nullptr, 0, D, G->max_rows, status, &L));
+    else
+      FAP_CK(launch_floyd_parts_multi<T>(dp, np, (int)ceil_div(G->max_s, kFloydTile), F, G->max_ldf,
+                                         status, st, &L));
     FAP_CK(record_event(c->ev[2], st));
     FAP_TRY(close_bgraph<T>(G, dp, np, G->max_b, F, status, max_rounds, &L));
     FAP_TRY(expand_bgraph<T>(G, dp, np, G->max_s, F, D, G->max_ldf, status, &L));
@@ -1122,8 +1196,15 @@ int run_solve(fap_dgraph *G, int mode) {
     FAP_CK(record_event(c->ev[1], st));
     FAP_CK(launch_gather<T>(dp, np, G->max_ldf, ro, col, w, gid, st2ed, ed2st, D, G->ldD, F, st, &L));
     FAP_CK(record_event(c->ev[2], st));
+    // With the work queue, the min-plus tiles run in the same launch as the
+    // Floyd (each part's as soon as its closure and boundary rows are done)
+    // unless they use the packed form, whose bounds need every boundary row.
+    int mp_in_queue = 0;
     if (G->floyd_per_cta) {
       FAP_CK(launch_floyd_parts<T>(dp, np, F, G->max_ldf, D, G->ldD, st2ed, status, st, &L));
+    } else if (G->floyd_queue) {
+      mp_in_queue = pack16_of(G) == nullptr ? (int)G->work.size() : 0;
+      FAP_CK(run_floyd_queue<T>(G, G->q, dp, F, G->max_ldf, true, dw, mp_in_queue, D, G->max_rows, status, &L));
     } else {
       FAP_CK(launch_floyd_parts_multi<T>(dp, np, (int)ceil_div(G->max_s, kFloydTile), F, G->max_ldf,
                                          status, st, &L));
@@ -1132,8 +1213,9 @@ int run_solve(fap_dgraph *G, int mode) {
     FAP_CK(record_event(c->ev[3], st));
     FAP_CK(launch_minplus_thin<T>(dp, G->d_thin.as<int32_t>(), (int)G->thin.size(), G->max_s, G->n, F, D,
                                   G->ldD, gid, ed2st, st, &L));
-    FAP_CK(launch_minplus_parts<T>(dp, np, dw, (int)G->work.size(), G->n, F, G->max_ldf, D, G->ldD,
-                                   G->max_rows, gid, ed2st, status, st, &L, pack16_of(G)));
+    if (mp_in_queue == 0)
+      FAP_CK(launch_minplus_parts<T>(dp, np, dw, (int)G->work.size(), G->n, F, G->max_ldf, D, G->ldD,
+                                     G->max_rows, gid, ed2st, status, st, &L, pack16_of(G)));
     if (G->paths) FAP_TRY(launch_paths<T>(G, dp, np, G->max_s, F, &L));
     FAP_CK(record_event(c->ev[4], st));
   } else {
@@ -1166,6 +1248,8 @@ int status_code(int h) {
   if (h == kDevSsspRoundLimit)
     return fail(FAP_ERR_NOT_CONVERGED, "SSSP hit its round bound");
   if (h == kDevTmaTimeout) return fail(FAP_ERR_DEVICE, "a TMA tile load did not complete in time");
+  if (h == kDevQueueTimeout)
+    return fail(FAP_ERR_DEVICE, "a work-queue item waited too long for the items it depends on");
   if (h != kDevOk) return fail(FAP_ERR_DEVICE, "device-side error %d", h);
   return FAP_OK;
 }
@@ -1213,8 +1297,13 @@ extern "C" int fap_solve(fap_dgraph *G, const int32_t *parts, int32_t count, int
   // (the tiled SSSP form tests convergence on the host: not capturable)
   const bool host_loop = !cached && (bmethod ? bgraph_bf(G) : use_msbf(G));
   G->stage1_name = cached ? "resident cache (" + G->cache_stage1_name + ")" : stage1_form_name(G, bmethod);
-  if (mode == FAP_MODE_BATCHED && G->use_graph && st != nullptr && !host_loop) {
-    if (!G->gexec || G->gexec_epoch != G->epoch || G->gexec_stream != st) {
+  // A batch is captured the second time it is solved unchanged: a batch
+  // solved once (a server's batches of changing composition) runs its
+  // launches directly instead of paying for a capture and an instantiation.
+  const bool replayable = G->gexec && G->gexec_epoch == G->epoch && G->gexec_stream == st;
+  if (mode == FAP_MODE_BATCHED && G->use_graph && st != nullptr && !host_loop &&
+      (replayable || G->direct_epoch == G->epoch)) {
+    if (!replayable) {
       if (G->gexec) cudaGraphExecDestroy(G->gexec);
       G->gexec = nullptr;
       // Capture the whole batched launch sequence once; replay it while the
@@ -1244,6 +1333,7 @@ extern "C" int fap_solve(fap_dgraph *G, const int32_t *parts, int32_t count, int
   } else {
     rc = (G->dtype == FAP_DTYPE_I32) ? run_solve<int32_t>(G, mode) : run_solve<float>(G, mode);
     if (rc != FAP_OK) return rc;
+    G->direct_epoch = mode == FAP_MODE_BATCHED ? G->epoch : 0;
   }
   for (const PartDesc &d : G->parts) G->row_base[d.part] = d.row_base;
   G->path_ok.assign(G->K + 1, 0);
@@ -1755,6 +1845,10 @@ extern "C" int fap_graph_set_param(fap_dgraph *G, const char *key, double value)
     G->last_ids.clear();
     return FAP_OK;
   }
+  if (std::strcmp(key, "floyd_queue") == 0) {
+    G->floyd_queue = value != 0.0;
+    return FAP_OK;
+  }
   if (std::strcmp(key, "minplus_pack16") == 0) {
     G->pack16 = value != 0.0;
     G->last_ids.clear();
@@ -1987,6 +2081,17 @@ int cache_build_impl(fap_dgraph *G) {
   if (!bm && !use_msbf(G))  // (the tiled form sizes its own tiles)
     FAP_TRY(G->sssp_scratch.ensure(
         (size_t)std::max(sssp_scratch_rows(G->n, (int)src.size()), 1) * (size_t)G->n * 4));
+  {
+    int32_t mnb = 0;
+    const std::vector<QItem> qitems = floyd_queue_items(G->cparts, &G->cq.nfloyd, &mnb);
+    G->cq.nitems = (int32_t)qitems.size();
+    G->cq.stride = 2 + 2 * mnb;
+    G->cq.nparts = (int32_t)G->cparts.size();
+    FAP_TRY(G->cq.items.ensure(std::max<size_t>(qitems.size(), 1) * sizeof(QItem)));
+    FAP_TRY(G->cq.cnt.ensure(((size_t)G->cq.nparts * G->cq.stride + 2) * 4));
+    if (!qitems.empty())
+      FAP_CK(cudaMemcpy(G->cq.items.p, qitems.data(), qitems.size() * sizeof(QItem), cudaMemcpyHostToDevice));
+  }
   FAP_CK(cudaMemcpy(G->d_cparts.p, G->cparts.data(), G->cparts.size() * sizeof(PartDesc),
                     cudaMemcpyHostToDevice));
   if (!src.empty()) {
@@ -2012,7 +2117,10 @@ int cache_build_impl(fap_dgraph *G) {
     FAP_CK(cudaEventRecord(G->cev[0], st));
     FAP_CK(launch_gather<T>(dp, K, cs.ldf, G->ro.as<const int32_t>(), G->col.as<const int32_t>(),
                             G->w.as<const T>(), gid, st2ed, ed2st, Bd, G->ldD, F, st, &L));
-    FAP_CK(launch_floyd_parts_multi<T>(dp, K, (int)ceil_div(cs.max_s, kFloydTile), F, cs.ldf, status, st, &L));
+    if (G->floyd_queue)
+      FAP_CK(run_floyd_queue<T>(G, G->cq, dp, F, cs.ldf, false, nullptr, 0, Bd, 0, status, &L));
+    else
+      FAP_CK(launch_floyd_parts_multi<T>(dp, K, (int)ceil_div(cs.max_s, kFloydTile), F, cs.ldf, status, st, &L));
     FAP_CK(cudaEventRecord(G->cev[1], st));
     FAP_TRY(close_bgraph<T>(G, dp, K, cs.max_b, F, status, rounds, &L));
     FAP_CK(cudaEventRecord(G->cev[2], st));
@@ -2034,6 +2142,8 @@ int cache_build_impl(fap_dgraph *G) {
   G->cache_bmethod = false;
   if (G->floyd_per_cta) {
     FAP_CK(launch_floyd_parts<T>(dp, K, F, cs.ldf, Bd, G->ldD, st2ed, status, st, &L));
+  } else if (G->floyd_queue) {
+    FAP_CK(run_floyd_queue<T>(G, G->cq, dp, F, cs.ldf, true, nullptr, 0, Bd, 0, status, &L));
   } else {
     FAP_CK(launch_floyd_parts_multi<T>(dp, K, (int)ceil_div(cs.max_s, kFloydTile), F, cs.ldf, status,
                                        st, &L));

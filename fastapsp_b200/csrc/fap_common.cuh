@@ -63,6 +63,7 @@ enum DevStatus : int {
   kDevSsspRoundLimit = 1,   // SSSP did not converge within its round bound
   kDevBadIndex = 2,         // an input index was out of range (skipped)
   kDevTmaTimeout = 3,       // a TMA stage never completed (bounded wait gave up)
+  kDevQueueTimeout = 4,     // a work-queue item's dependencies never completed (bounded wait gave up)
 };
 
 __device__ inline void set_status(int *status, int code) {

@@ -715,7 +715,7 @@ __device__ __forceinline__ void minplus_part_epilogue(const PartDesc &pd, const 
         const T *Fr = F + pd.f_off + (int64_t)(pd.b + r) * pd.ldf;
 #pragma unroll
         for (int j = 0; j < C::TN; j++)
-          if (own[j] >= 0) acc[4 * gi + l][j] = Fr[own[j]];
+          if (own[j] >= 0) acc[4 * gi + l][j] = __ldcg(Fr + own[j]);   // (L2: see acc_load)
       }
       T *dst = Cm + (int64_t)r * ldD + n0;
 #pragma unroll
@@ -741,24 +741,25 @@ __device__ __forceinline__ void minplus_part_epilogue(const PartDesc &pd, const 
 // 16-bit engine and shifts its results back by the column offsets; the
 // others run the int32 engine.  Both give the same int32 values.
 // ---------------------------------------------------------------------------
+// One min-plus tile: rows wk.m0 .. +BM of the part's inner block against
+// columns n0 .. +BN.  Block-wide; raw is the CTA's dynamic shared memory
+// (the TMA ring at its start, the packed buffers after it).  Returns false
+// (in every thread) if a TMA stage never completed.
 template <typename T, bool PACK>
-__global__ void __launch_bounds__(MPCfg<T>::THREADS, 2)
-    minplus_part_kernel(const PartDesc *__restrict__ parts, const MPWork *__restrict__ work, int n,
-                        const T *__restrict__ F, T *D, int64_t ldD,
-                        const int32_t *__restrict__ graph_id, const int32_t *__restrict__ ed2st,
-                        const __grid_constant__ CUtensorMap mapF, const __grid_constant__ CUtensorMap mapD,
-                        int *status, Pack16 pk) {
+__device__ __forceinline__ bool minplus_part_tile(const PartDesc &pd, const MPWork &wk, int tile_x, int n,
+                                                  const T *__restrict__ F, T *D, int64_t ldD,
+                                                  const int32_t *__restrict__ graph_id,
+                                                  const int32_t *__restrict__ ed2st, const CUtensorMap *mapF,
+                                                  const CUtensorMap *mapD, const Pack16 &pk,
+                                                  TmaSmem<T, typename FloydCfg<T, kFloydTile>::TC> &sm,
+                                                  unsigned char *raw) {
   using C = MPCfg<T>;
   using TC = typename FloydCfg<T, kFloydTile>::TC;
-  extern __shared__ __align__(128) unsigned char mp_smem_raw[];
-  auto sm = tma_smem_init<T, TC>(mp_smem_raw);
-  const MPWork wk = work[blockIdx.y];
-  const PartDesc pd = parts[wk.pidx];
-  const int n0 = blockIdx.x * C::BN;
+  const int n0 = tile_x * C::BN;
   const int K = pd.b;
   T *Cm = D + (pd.row_base + pd.b) * ldD;
   T acc[C::TM][C::TN];
-  // A = F rows b+m0.. of part wk.pidx (columns 0..b-1); B = D rows
+  // A = F rows b+m0.. of the part (columns 0..b-1); B = D rows
   // row_base..row_base+b-1 (the part's boundary rows).  Rows and columns past
   // the part's extent are never stored; k past b is never read.
   // The part's square in the arena (its index there: a batch index, or the
@@ -766,7 +767,7 @@ __global__ void __launch_bounds__(MPCfg<T>::THREADS, 2)
   const int fz = (int)(pd.f_off / ((int64_t)pd.ldf * pd.ldf));
   bool packed = false;
   if constexpr (PACK) {
-    packed = __ldg(pk.maxA + wk.pidx) + __ldg(pk.range + (int64_t)wk.pidx * pk.ntiles + blockIdx.x) < kPackCap;
+    packed = __ldg(pk.maxA + wk.pidx) + __ldg(pk.range + (int64_t)wk.pidx * pk.ntiles + tile_x) < kPackCap;
     if (threadIdx.x == 0) {
       atomicAdd(pk.tiles + 1, 1ull);
       if (packed) atomicAdd(pk.tiles, 1ull);
@@ -775,7 +776,7 @@ __global__ void __launch_bounds__(MPCfg<T>::THREADS, 2)
   if (packed) {
     if constexpr (PACK) {
       using P = Pack16Cfg<TC>;
-      const uintptr_t base = (reinterpret_cast<uintptr_t>(mp_smem_raw) + 127) & ~uintptr_t(127);
+      const uintptr_t base = (reinterpret_cast<uintptr_t>(raw) + 127) & ~uintptr_t(127);
       uint32_t *pbuf = reinterpret_cast<uint32_t *>(base + P::BUF_OFFSET);
       int32_t *coff = reinterpret_cast<int32_t *>(pbuf + 2 * P::BUF_ELEMS);
       for (int c = threadIdx.x; c < C::BN; c += blockDim.x)
@@ -786,11 +787,9 @@ __global__ void __launch_bounds__(MPCfg<T>::THREADS, 2)
 #pragma unroll
         for (int j = 0; j < 8; j++) a16[i][j] = kPackInit;
       // (the engine's first barrier orders the column offsets before use)
-      if (!tma_minplus_tile16<TC>(&mapF, 0, pd.b + wk.m0, fz, &mapD, n0, (int)pd.row_base, 0, K, a16, sm,
-                                  pbuf, coff)) {
-        if (threadIdx.x == 0) set_status(status, kDevTmaTimeout);
-        return;
-      }
+      if (!tma_minplus_tile16<TC>(mapF, 0, pd.b + wk.m0, fz, mapD, n0, (int)pd.row_base, 0, K, a16, sm, pbuf,
+                                  coff, pd.s - pd.b - wk.m0))
+        return false;
       const int tx = threadIdx.x % C::TX;
 #pragma unroll
       for (int j = 0; j < 8; j++) {
@@ -805,16 +804,48 @@ __global__ void __launch_bounds__(MPCfg<T>::THREADS, 2)
           acc[r0 + 1][j] = hi < kPackCap ? hi + off : Dist<T>::inf();
         }
       }
+      // every thread has read its offsets before the buffers are reused
+      __syncthreads();
     }
   } else {
     acc_fill<T, C>(acc, Dist<T>::inf());
-    if (!tma_minplus_tile<T, TC>(&mapF, 0, pd.b + wk.m0, fz, &mapD, n0, (int)pd.row_base, 0, K, acc,
-                                 sm)) {
-      if (threadIdx.x == 0) set_status(status, kDevTmaTimeout);
-      return;
-    }
+    // (rows past the part's inner block are never stored: their warps skip
+    // the relaxations)
+    if (!tma_minplus_tile<T, TC, true>(mapF, 0, pd.b + wk.m0, fz, mapD, n0, (int)pd.row_base, 0, K, acc, sm,
+                                       pd.s - pd.b - wk.m0, C::BN))
+      return false;
   }
   minplus_part_epilogue<T, C>(pd, wk, n0, n, F, Cm, ldD, graph_id, ed2st, acc);
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// Stage 3: min-plus merge with the fused decode of own-part columns.
+// grid (ldD / BN, nwork): CTA (x, y) computes rows work[y].m0 .. +BM of the
+// part's inner block against columns x*BN .. +BN.
+//   R[i][j] = min(INF, min_{k<b} F[b+i][k] + S[k][j])   (S = the part's
+//   boundary rows of D), then for own-part columns j the closed Floyd value
+//   F[b+i][ed2st[j]-start] replaces it, as the reference's decode does.
+// PACK (int32): a tile whose entries provably fit (Pack16) runs the packed
+// 16-bit engine and shifts its results back by the column offsets; the
+// others run the int32 engine.  Both give the same int32 values.
+// ---------------------------------------------------------------------------
+template <typename T, bool PACK>
+__global__ void __launch_bounds__(MPCfg<T>::THREADS, 2)
+    minplus_part_kernel(const PartDesc *__restrict__ parts, const MPWork *__restrict__ work, int n,
+                        const T *__restrict__ F, T *D, int64_t ldD,
+                        const int32_t *__restrict__ graph_id, const int32_t *__restrict__ ed2st,
+                        const __grid_constant__ CUtensorMap mapF, const __grid_constant__ CUtensorMap mapD,
+                        int *status, Pack16 pk) {
+  using TC = typename FloydCfg<T, kFloydTile>::TC;
+  extern __shared__ __align__(128) unsigned char mp_smem_raw[];
+  auto sm = tma_smem_init<T, TC>(mp_smem_raw);
+  const MPWork wk = work[blockIdx.y];
+  const PartDesc pd = parts[wk.pidx];
+  if (!minplus_part_tile<T, PACK>(pd, wk, blockIdx.x, n, F, D, ldD, graph_id, ed2st, &mapF, &mapD, pk, sm,
+                                  mp_smem_raw) &&
+      threadIdx.x == 0)
+    set_status(status, kDevTmaTimeout);
 }
 
 // Packed-form bounds of a batch (see Pack16): one CTA per (column tile, work
@@ -893,6 +924,209 @@ __global__ void __launch_bounds__(256)
     for (int w = 0; w < 8; w++) x = max(x, red[w]);
     pk.maxA[wk.pidx] = x;
   }
+}
+
+// ---------------------------------------------------------------------------
+// Work-queue form of the batched Floyd-Warshall (FloydQueue).  One
+// persistent launch: each CTA claims the next item of the list, waits for
+// the per-part counters of the items it depends on, runs it, and counts it
+// done.  Items are claimed in list order and every dependency of an item
+// comes earlier in the list, so every awaited item has been claimed by a
+// running CTA and finishes: the waits end (they are bounded all the same;
+// on a timeout the CTA records kDevQueueTimeout and raises the abort flag,
+// which ends every other wait).  Dependencies of part p:
+//   Floyd-1 (pivot block kb)   every Floyd-3 item of block kb-1
+//   Floyd-2 (block kb)         Floyd-1 of block kb
+//   Floyd-3 (block kb)         every Floyd-2 item of block kb
+//   scatter                    the last block's Floyd-3 items (Floyd-1 when
+//                              the part is one tile)
+//   min-plus tile              every scatter item of the part
+// A finished item's global writes are made visible to the TMA (async proxy)
+// and to other CTAs (fence, then the counter increment); a waiting CTA reads
+// the counter with acquire semantics before it loads anything.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int ld_acquire_gpu(const int32_t *p) {
+  int32_t v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+constexpr uint32_t kQueuePollLimit = 1u << 24;   // x ~150 ns: a few seconds
+
+__device__ bool queue_wait(const int32_t *ctr, int need, const int32_t *abort) {
+  for (uint32_t i = 0; i < kQueuePollLimit; i++) {
+    if (ld_acquire_gpu(ctr) >= need) return true;
+    if (ld_acquire_gpu(abort) != 0) return false;
+    __nanosleep(128);
+  }
+  return false;
+}
+
+// Claimed item, decoded by thread 0 into shared memory (so that nothing of
+// the dispatch stays live in registers across an item's body).
+struct QClaim {
+  int kind;     // kQFloyd1..3, kQScatter; 0 = min-plus tile; -1 = stop
+  int pidx, kb, t, m0;
+};
+
+template <typename T, bool WITH_MP>
+__global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS, 2)
+    floyd_queue_kernel(const PartDesc *__restrict__ parts, T *F, FloydQueue q,
+                       const MPWork *__restrict__ work, int n, T *D, int64_t ldD,
+                       const int32_t *__restrict__ st2ed, const int32_t *__restrict__ graph_id,
+                       const int32_t *__restrict__ ed2st, const __grid_constant__ CUtensorMap mapA,
+                       const __grid_constant__ CUtensorMap mapB, const __grid_constant__ CUtensorMap mapD,
+                       int *status, Pack16 pk) {
+  using TC = typename FloydCfg<T, kFloydTile>::TC;
+  extern __shared__ __align__(128) unsigned char fq_smem_raw[];
+  auto sm = tma_smem_init<T, TC>(fq_smem_raw);
+  __shared__ QClaim cl;
+  const int tid = threadIdx.x;
+  for (;;) {
+    if (tid == 0) {
+      int32_t *abort = q.cnt + (int64_t)q.nparts * q.stride;
+      const int64_t ntiles = ldD / kMinplusBN;
+      const int64_t total = q.nitems + (int64_t)q.mp_work * ntiles;
+      const int64_t it = atomicAdd(abort + 1, 1);
+      QClaim c{-1, 0, 0, 0, 0};
+      if (it < total) {
+        if (it < q.nitems) {
+          const QItem qi = q.items[it];
+          c = QClaim{qi.kind, qi.pidx, qi.kb, qi.t, 0};
+        } else {
+          const int64_t m = it - q.nitems;
+          const MPWork wk = work[m / ntiles];
+          c = QClaim{0, wk.pidx, 0, (int)(m % ntiles), wk.m0};
+        }
+        const PartDesc pd = parts[c.pidx];
+        const int nb = (int)ceil_div(pd.s, kFloydTile);
+        const int32_t *cn = q.cnt + (int64_t)c.pidx * q.stride;
+        const int32_t *p2 = cn + 2, *p3 = cn + 2 + (q.stride - 2) / 2;
+        bool ok = true;
+        if (c.kind == kQFloyd1) {
+          if (c.kb > 0) ok = queue_wait(p3 + c.kb - 1, (nb - 1) * (nb - 1), abort);
+        } else if (c.kind == kQFloyd2) {
+          ok = queue_wait(cn, c.kb + 1, abort);
+        } else if (c.kind == kQFloyd3) {
+          ok = queue_wait(p2 + c.kb, 2 * (nb - 1), abort);
+        } else if (c.kind == kQScatter) {
+          ok = nb == 1 ? queue_wait(cn, 1, abort) : queue_wait(p3 + nb - 1, (nb - 1) * (nb - 1), abort);
+        } else {
+          ok = queue_wait(cn + 1, (int)ceil_div(pd.b, kQScatterRows), abort);
+        }
+        if (!ok) {
+          set_status(status, kDevQueueTimeout);
+          atomicExch(abort, 1);
+          c.kind = -1;
+        }
+        // the items waited for wrote with generic stores; this CTA reads
+        // them with the TMA too
+        fence_proxy_async_all();
+      }
+      cl = c;
+    }
+    __syncthreads();
+    const int kind = cl.kind;
+    if (kind < 0) break;
+    bool ok = true;
+    if (kind == kQFloyd1) {
+      const PartDesc pd = parts[cl.pidx];
+      const int kb = cl.kb;
+      floyd_diag_close<T, kFloydTile>(F + pd.f_off, pd.ldf, kb * kFloydTile, sm.ring,
+                                      min(kFloydTile, pd.s - kb * kFloydTile));
+    } else if (kind == kQFloyd2 || kind == kQFloyd3) {
+      const PartDesc pd = parts[cl.pidx];
+      const int kb = cl.kb, t = cl.t;
+      const int nb = (int)ceil_div(pd.s, kFloydTile);
+      int i, j;
+      if (kind == kQFloyd3) {
+        i = t / (nb - 1);
+        j = t % (nb - 1);
+        i = i < kb ? i : i + 1;
+        j = j < kb ? j : j + 1;
+      } else if (t < nb - 1) {
+        i = kb;
+        j = t < kb ? t : t + 1;
+      } else {
+        const int t2 = t - (nb - 1);
+        i = t2 < kb ? t2 : t2 + 1;
+        j = kb;
+      }
+      const int z = (int)(pd.f_off / ((int64_t)pd.ldf * pd.ldf));
+      ok = floyd_tile_update<T, kFloydTile>(&mapA, &mapB, z, F + pd.f_off, pd.ldf, i, j, kb, sm,
+                                            min(kFloydTile, pd.s - kb * kFloydTile),
+                                            min(kFloydTile, pd.s - i * kFloydTile),
+                                            min(kFloydTile, pd.s - j * kFloydTile));
+    } else if (kind == kQScatter) {
+      // boundary rows kb .. kb + kQScatterRows of the closed matrix into D
+      // (the reference's decode of rows < b, util_Myalgorithm.h:75-86)
+      const PartDesc pd = parts[cl.pidx];
+      const int r0 = cl.kb, r1 = min(pd.b, r0 + kQScatterRows);
+      const T *mat = F + pd.f_off;
+      const int64_t cnt = (int64_t)(r1 - r0) * pd.s;
+      for (int64_t e = tid; e < cnt; e += blockDim.x) {
+        const int i = r0 + (int)(e / pd.s), j = (int)(e % pd.s);
+        D[(pd.row_base + i) * ldD + st2ed[pd.start + j]] = __ldcg(mat + (int64_t)i * pd.ldf + j);
+      }
+    } else if constexpr (WITH_MP) {
+      const PartDesc pd = parts[cl.pidx];
+      const MPWork wk{cl.pidx, cl.m0};
+      ok = minplus_part_tile<T, false>(pd, wk, cl.t, n, F, D, ldD, graph_id, ed2st, &mapA, &mapD, pk, sm,
+                                       fq_smem_raw);
+    }
+    // this item's writes: visible to the async proxy, then to other CTAs,
+    // before it counts as done
+    fence_proxy_async_all();
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) {
+        set_status(status, kDevTmaTimeout);
+        atomicExch(q.cnt + (int64_t)q.nparts * q.stride, 1);
+      }
+      break;
+    }
+    if (tid == 0 && kind > 0) {
+      int32_t *cn = q.cnt + (int64_t)cl.pidx * q.stride;
+      const int half = (q.stride - 2) / 2;
+      int32_t *done = kind == kQFloyd1 ? cn : kind == kQFloyd2 ? cn + 2 + cl.kb
+                    : kind == kQFloyd3 ? cn + 2 + half + cl.kb : cn + 1;
+      __threadfence();
+      atomicAdd(done, 1);
+    }
+  }
+}
+
+template <typename T>
+cudaError_t launch_floyd_queue(const PartDesc *parts, int nparts, T *F, int64_t ldf, const FloydQueue &q,
+                               const MPWork *work, int n, T *D, int64_t ldD, int64_t drows,
+                               const int32_t *st2ed, const int32_t *graph_id, const int32_t *ed2st,
+                               int *status, cudaStream_t stream, int64_t *launches, const Pack16 *pk) {
+  if (nparts <= 0 || (q.nitems <= 0 && q.mp_work <= 0)) return cudaSuccess;
+  using FC = FloydCfg<T, kFloydTile>;
+  CUtensorMap mapA, mapB, mapD;
+  cudaError_t e = make_arena_tmaps<T>(F, ldf, nparts, &mapA, &mapB);
+  if (e == cudaSuccess)
+    e = make_tmap_3d(&mapD, D, Dist<T>::kDtype == FAP_DTYPE_F32, ldD, std::max<int64_t>(drows, 1), 1,
+                     FC::TC::BN, FC::TC::BK);
+  if (e != cudaSuccess) return e;
+  // (min-plus tiles in the queue run in int32: the packed form needs bounds
+  // over the boundary rows that the queue itself scatters, so a batch that
+  // uses the packed form keeps its min-plus in launch_minplus_parts)
+  (void)pk;
+  auto kern = q.mp_work > 0 ? floyd_queue_kernel<T, true> : floyd_queue_kernel<T, false>;
+  const size_t smem = FC::SMEM_BYTES;
+  e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, FC::THREADS, smem);
+  if (e != cudaSuccess) return e;
+  const int64_t total = q.nitems + (int64_t)q.mp_work * (ldD / kMinplusBN);
+  const int grid =
+      (int)std::max<int64_t>(1, std::min<int64_t>(total, (int64_t)std::max(per_sm, 1) * device_sm_count()));
+  Pack16 none{};
+  kern<<<grid, FC::THREADS, smem, stream>>>(parts, F, q, work, n, D, ldD, st2ed, graph_id, ed2st, mapA, mapB, mapD,
+                                            status, none);
+  *launches += 1;
+  return cudaGetLastError();
 }
 
 // Thin-K variant (b <= kThinK): the product is store-bound, not
@@ -2415,6 +2649,10 @@ cudaError_t launch_relax_peak(T *sink, int blocks, int iters, cudaStream_t strea
   template cudaError_t launch_floyd_matrix<T>(T *, int64_t, int, int *, cudaStream_t, int64_t *, int); \
   template cudaError_t launch_floyd_parts_multi<T>(const PartDesc *, int, int, T *, int64_t, int *, \
                                                    cudaStream_t, int64_t *);                      \
+  template cudaError_t launch_floyd_queue<T>(const PartDesc *, int, T *, int64_t, const FloydQueue &, \
+                                             const MPWork *, int, T *, int64_t, int64_t,          \
+                                             const int32_t *, const int32_t *, const int32_t *,    \
+                                             int *, cudaStream_t, int64_t *, const Pack16 *);     \
   template cudaError_t launch_bdy_scatter<T>(const PartDesc *, int, const T *, T *, int64_t,      \
                                              const int32_t *, int, int, cudaStream_t, int64_t *); \
   template cudaError_t launch_minplus_parts<T>(const PartDesc *, int, const MPWork *, int, int,   \

@@ -66,6 +66,32 @@ struct Pack16 {
   unsigned long long *tiles;  // [2]: tiles run packed, tiles run (cumulative)
 };
 
+// Work queue of the batched Floyd-Warshall in one persistent launch: items
+// 0..nitems-1 are listed (kind, batch index, pivot block, tile) so that
+// every item's dependencies come earlier in the list, and CTAs claim them in
+// list order from a counter; a CTA waits (bounded) for the per-part
+// counters its item depends on.  When the batch's min-plus merge follows the
+// Floyd directly (stage 1 by SSSP), the boundary-row scatter of each part and
+// the min-plus tiles (mp_work x column tiles, after the listed items) are in
+// the same launch, each part's starting as soon as its own closure is done.
+struct QItem {
+  int32_t kind;  // kQFloyd1..3, kQScatter
+  int32_t pidx;  // batch index of the part
+  int32_t kb;    // pivot block (Floyd) / first boundary row / kQScatterRows (scatter)
+  int32_t t;     // tile index within the phase
+};
+constexpr int32_t kQFloyd1 = 1, kQFloyd2 = 2, kQFloyd3 = 3, kQScatter = 4;
+constexpr int kQScatterRows = 8;
+struct FloydQueue {
+  const QItem *items;
+  int32_t nitems;
+  int32_t mp_work;   // min-plus work items (MPWork) appended after the list (0: none)
+  int32_t *cnt;      // per batch part `stride` counters, then the abort flag and the claim counter
+  int32_t stride;    // 2 + 2 * max_nb: Floyd-1 rounds done, scatter items done, then per pivot
+                     // block the Floyd-2 and the Floyd-3 items done
+  int32_t nparts;
+};
+
 constexpr int kFloydTile = 128;
 constexpr int kMinplusBM = 128;
 constexpr int kMinplusBN = 128;
@@ -147,6 +173,17 @@ template <typename T>
 cudaError_t launch_bdy_scatter(const PartDesc *parts, int nparts, const T *F, T *D, int64_t ldD,
                                const int32_t *st2ed, int max_b, int max_s, cudaStream_t stream,
                                int64_t *launches);
+
+// The batched Floyd-Warshall of every part as one persistent launch over a
+// work queue (FloydQueue); with q.mp_work > 0 also the boundary-row scatter
+// into D (as launch_bdy_scatter) and the min-plus tiles (as
+// launch_minplus_parts, pk as there).  q.cnt must be zero (nparts * stride
+// + 2 ints) when the launch starts.
+template <typename T>
+cudaError_t launch_floyd_queue(const PartDesc *parts, int nparts, T *F, int64_t ldf, const FloydQueue &q,
+                               const MPWork *work, int n, T *D, int64_t ldD, int64_t drows,
+                               const int32_t *st2ed, const int32_t *graph_id, const int32_t *ed2st,
+                               int *status, cudaStream_t stream, int64_t *launches, const Pack16 *pk);
 
 // Min-plus merge of the inner rows of the batch's parts, with the own-part
 // columns taken from the closed Floyd matrices (fused decode).

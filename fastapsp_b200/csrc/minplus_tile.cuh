@@ -207,7 +207,10 @@ __device__ __forceinline__ void acc_load(T (&acc)[C::TM][C::TN], const T *P, int
       for (int gj = 0; gj < C::GN; gj++) {
         const int c0 = n0 + tile_col<C>(tx, gj, 0);
         if (FULL) {
-          V v = *reinterpret_cast<const V *>(P + (int64_t)r * ld + c0);
+          // L2 only (ld.global.cg): the tile may have been written by another
+          // SM earlier in the same launch (the Floyd work queue), and this
+          // SM's L1 could still hold an older copy of it
+          V v = __ldcg(reinterpret_cast<const V *>(P + (int64_t)r * ld + c0));
           acc[4 * gi + l][4 * gj + 0] = v.x;
           acc[4 * gi + l][4 * gj + 1] = v.y;
           acc[4 * gi + l][4 * gj + 2] = v.z;
@@ -216,7 +219,7 @@ __device__ __forceinline__ void acc_load(T (&acc)[C::TM][C::TN], const T *P, int
 #pragma unroll
           for (int q = 0; q < 4; q++)
             acc[4 * gi + l][4 * gj + q] =
-                (r < M && c0 + q < N) ? P[(int64_t)r * ld + c0 + q] : Dist<T>::inf();
+                (r < M && c0 + q < N) ? __ldcg(P + (int64_t)r * ld + c0 + q) : Dist<T>::inf();
         }
       }
     }

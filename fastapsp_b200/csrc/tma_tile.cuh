@@ -103,8 +103,14 @@ __device__ __forceinline__ bool tma_minplus_tile(const CUtensorMap *mapA, int ax
                                                  const CUtensorMap *mapB, int bx, int by, int bz,
                                                  int K, T (&acc)[8][8], TmaSmem<T, C> &sm,
                                                  int mvalid = C::BM, int nvalid = C::BN) {
-  const bool rhi = !PAD || mvalid > C::BM / 2, chi = !PAD || nvalid > C::BN / 2;
   const int tid = threadIdx.x, ty = tid / C::TX, tx = tid % C::TX;
+  // Rows are skipped per warp: a warp holds rows 8w..8w+7 of each row group
+  // (two values of ty), so whether any of them is real is warp-uniform.
+  // Columns span every warp, so they are skipped per tile half only.
+  static_assert(C::TX == 16, "a warp holds two row quads of each group");
+  const int w8 = (tid / 32) * 8;
+  const bool rlo = !PAD || w8 < mvalid, rhi = !PAD || C::BM / 2 + w8 < mvalid;
+  const bool chi = !PAD || nvalid > C::BN / 2;
   const int n = (int)ceil_div(K, C::BK);
   if (n == 0) return true;
   auto issue = [&](int c, int s) {
@@ -129,8 +135,8 @@ __device__ __forceinline__ bool tma_minplus_tile(const CUtensorMap *mapA, int ax
       const int kc = min(C::BK, K - c * C::BK);
       if (!PAD || (rhi && chi)) tma_chunk_compute<T, C, 2, 2>(As, As + C::A_ELEMS, acc, ty, tx, kc);
       else if (rhi) tma_chunk_compute<T, C, 2, 1>(As, As + C::A_ELEMS, acc, ty, tx, kc);
-      else if (chi) tma_chunk_compute<T, C, 1, 2>(As, As + C::A_ELEMS, acc, ty, tx, kc);
-      else tma_chunk_compute<T, C, 1, 1>(As, As + C::A_ELEMS, acc, ty, tx, kc);
+      else if (rlo && chi) tma_chunk_compute<T, C, 1, 2>(As, As + C::A_ELEMS, acc, ty, tx, kc);
+      else if (rlo) tma_chunk_compute<T, C, 1, 1>(As, As + C::A_ELEMS, acc, ty, tx, kc);
     }
     fence_proxy_async_smem();  // this thread's reads of stage s precede its refill
     if (__syncthreads_or(!got)) {
@@ -213,7 +219,7 @@ __device__ __forceinline__ void pack16_convert(const int32_t *As, const int32_t 
 
 // One converted chunk: per k, the thread's 4 row pairs (two 8-byte loads)
 // and 8 columns (two 16-byte loads), then 32 packed relaxations.
-template <class C>
+template <class C, int GI = 2>
 __device__ __forceinline__ void pack16_chunk_compute(const uint32_t *PA, const uint32_t *PB,
                                                      uint32_t (&acc)[4][8], int ty, int tx, int kc) {
   using P = Pack16Cfg<C>;
@@ -221,7 +227,7 @@ __device__ __forceinline__ void pack16_chunk_compute(const uint32_t *PA, const u
   for (int k = 0; k < kc; k++) {
     uint32_t a[4], b[8];
 #pragma unroll
-    for (int g = 0; g < 2; g++) {
+    for (int g = 0; g < GI; g++) {
       const uint2 v = *reinterpret_cast<const uint2 *>(PA + k * P::PA_LD + g * (C::BM / 4) + ty * 2);
       a[2 * g] = v.x;
       a[2 * g + 1] = v.y;
@@ -232,7 +238,7 @@ __device__ __forceinline__ void pack16_chunk_compute(const uint32_t *PA, const u
       b[4 * g + 0] = v.x; b[4 * g + 1] = v.y; b[4 * g + 2] = v.z; b[4 * g + 3] = v.w;
     }
 #pragma unroll
-    for (int i = 0; i < 4; i++)
+    for (int i = 0; i < 2 * GI; i++)
 #pragma unroll
       for (int j = 0; j < 8; j++) acc[i][j] = __viaddmin_s16x2(a[i], b[j], acc[i][j]);
   }
@@ -246,9 +252,13 @@ template <class C>
 __device__ __forceinline__ bool tma_minplus_tile16(const CUtensorMap *mapA, int ax, int ay, int az,
                                                    const CUtensorMap *mapB, int bx, int by, int bz,
                                                    int K, uint32_t (&acc)[4][8], TmaSmem<int32_t, C> &sm,
-                                                   uint32_t *pbuf, const int32_t *coff) {
+                                                   uint32_t *pbuf, const int32_t *coff, int mvalid = C::BM) {
   using P = Pack16Cfg<C>;
   const int tid = threadIdx.x, ty = tid / C::TX, tx = tid % C::TX;
+  // rows skipped per warp as in tma_minplus_tile (row pairs of a warp lie
+  // in its rows 8w..8w+7 of each group)
+  const int w8 = (tid / 32) * 8;
+  const bool rlo = w8 < mvalid, rhi = C::BM / 2 + w8 < mvalid;
   const int n = (int)ceil_div(K, C::BK);
   if (n == 0) return true;
   auto issue = [&](int c, int s) {
@@ -286,7 +296,8 @@ __device__ __forceinline__ bool tma_minplus_tile16(const CUtensorMap *mapA, int 
       return false;
     }
     if (tid == 0 && c + C::STAGES < n) issue(c + C::STAGES, s);
-    pack16_chunk_compute<C>(PA, PB, acc, ty, tx, min(C::BK, K - c * C::BK));
+    if (rhi) pack16_chunk_compute<C, 2>(PA, PB, acc, ty, tx, min(C::BK, K - c * C::BK));
+    else if (rlo) pack16_chunk_compute<C, 1>(PA, PB, acc, ty, tx, min(C::BK, K - c * C::BK));
   }
   return true;
 }

@@ -75,3 +75,35 @@ def test_tuning_keeps_results_bit_exact(cuda_ok, tmp_path):
     dg.solve(mode=FAP_MODE_BATCHED)
     cs = np.concatenate([dg.block_checksums(p) for p in range(1, case["K"] + 1)])
     np.testing.assert_array_equal(cs, case["row_checksums"])
+
+
+class FakeSolveGraph:
+    """Stand-in device graph whose step time depends on the parameters."""
+
+    def __init__(self, dtype, best):
+        self.dtype = dtype
+        self.best = best
+        self.params = {}
+
+    def set_param(self, k, v):
+        self.params[k] = v
+
+    def step(self):
+        cur = {k: self.params.get(k) for k in self.best}
+        return 1.0 if cur == self.best else 5.0
+
+
+@pytest.mark.parametrize("dtype,best", [(0, {"minplus_pack16": 1, "floyd_queue": 0}),
+                                        (1, {"minplus_pack16": 0, "floyd_queue": 1})])
+def test_tune_solve_picks_the_fastest_and_caches_it(tmp_path, dtype, best):
+    path = str(tmp_path / "tune.json")
+    vn, bn = [0, 1000, 1024], [0, 170, 160]
+    g = FakeSolveGraph(dtype, best)
+    out = autotune.tune_solve(g, vn, bn, g.step, path=path)
+    assert out["params"] == best and not out["cached"]
+    assert g.params == best
+    # float32 graphs only time the Floyd form (packing applies to int32)
+    assert len(out["candidates"]) == (4 if dtype == 0 else 2)
+    g2 = FakeSolveGraph(dtype, best)
+    out2 = autotune.tune_solve(g2, vn, bn, lambda: pytest.fail("timed again"), path=path)
+    assert out2["cached"] and g2.params == best
