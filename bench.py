@@ -775,6 +775,7 @@ def run_extra(args, job, ctx, relax_peak, hbm_peak, peak_kind):
     gpu = gpu_parity_blocks(dg, groups, job["parts"], dtype, staged, FAP_MODE_BATCHED) if job["parts"] else {}
     stage1 = dg.stage1_name()
     pk_tiles = dg.pack16_tiles()
+    xk_tiles = dg.expand16_tiles()
     del dg
     torch.cuda.synchronize()
     torch.cuda.empty_cache()
@@ -784,6 +785,7 @@ def run_extra(args, job, ctx, relax_peak, hbm_peak, peak_kind):
         "dtype": "int32" if dtype == 0 else "f32", "data": wl.data_description(),
         "config": {**wl.describe(), "groups": len(groups), "stage_cache": staged, "stage1": stage1,
                    "minplus_packed_tiles": {"packed": pk_tiles[0], "total": pk_tiles[1]},
+                   "expansion_packed_tiles": {"packed": xk_tiles[0], "total": xk_tiles[1]},
                    "sssp_delta_factor": tuned["factor"],
                    "solve_form": (solve_tuned["params"] if solve_tuned else
                                   {"minplus_pack16": int(not args.no_pack16), "floyd_queue": int(not args.no_queue)}),

@@ -169,10 +169,16 @@ struct fap_ctx {
 struct QueueBuf {
   DevBuf items, cnt;
   int32_t nfloyd = 0, nitems = 0, stride = 2, nparts = 0;
+  bool sym = false;
 };
 
 namespace {
-std::vector<QItem> floyd_queue_items(const std::vector<PartDesc> &parts, int32_t *nfloyd, int32_t *max_nb) {
+// sym: the matrices are symmetric; the panel items are the row panel's
+// tiles only (each also stores its transpose into the column panel) and the
+// remainder items the tiles (i, j) with i <= j (each off-diagonal one also
+// stores its transpose into (j, i)); t holds i << 16 | j for those.
+std::vector<QItem> floyd_queue_items(const std::vector<PartDesc> &parts, bool sym, int32_t *nfloyd,
+                                     int32_t *max_nb) {
   std::vector<QItem> it;
   int mnb = 0;
   for (const PartDesc &d : parts) mnb = std::max<int>(mnb, (int)ceil_div(std::max(d.s, 1), kFloydTile));
@@ -183,13 +189,24 @@ std::vector<QItem> floyd_queue_items(const std::vector<PartDesc> &parts, int32_t
     }
     for (size_t p = 0; p < parts.size(); p++) {
       const int nb = (int)ceil_div(parts[p].s, kFloydTile);
-      if (kb < nb)
+      if (kb >= nb) continue;
+      if (sym) {
+        for (int j = 0; j < nb; j++)
+          if (j != kb) it.push_back(QItem{kQFloyd2S, (int32_t)p, kb, (kb << 16) | j});
+      } else {
         for (int t = 0; t < 2 * (nb - 1); t++) it.push_back(QItem{kQFloyd2, (int32_t)p, kb, t});
+      }
     }
     for (size_t p = 0; p < parts.size(); p++) {
       const int nb = (int)ceil_div(parts[p].s, kFloydTile);
-      if (kb < nb)
+      if (kb >= nb) continue;
+      if (sym) {
+        for (int i = 0; i < nb; i++)
+          for (int j = i; j < nb; j++)
+            if (i != kb && j != kb) it.push_back(QItem{kQFloyd3S, (int32_t)p, kb, (i << 16) | j});
+      } else {
         for (int t = 0; t < (nb - 1) * (nb - 1); t++) it.push_back(QItem{kQFloyd3, (int32_t)p, kb, t});
+      }
     }
   }
   *nfloyd = (int32_t)it.size();
@@ -245,9 +262,13 @@ struct fap_dgraph {
   // fit (int32 graphs; Pack16): bounds buffers of the prepared batch.
   bool pack16 = true;
   DevBuf d_pk_off, d_pk_range, d_pk_maxa, d_pk_tiles;
+  // the same for the tiled expansion of the boundary graph (Expand16), sized
+  // for the launch's part list
+  DevBuf d_xk_off, d_xk_range, d_xk_maxb, d_xk_tiles;
   // Work queue of the batched Floyd (FloydQueue): the batch's items and
   // counters, and the resident cache build's (its parts are all parts).
   bool floyd_queue = true;
+  bool floyd_sym = true;  // use sym_local in the queue (parameter "floyd_symmetric")
   QueueBuf q, cq;
   Pack16 pk{};
   // CUDA graph of the batched launch sequence (replayed while nothing that
@@ -270,6 +291,11 @@ struct fap_dgraph {
   // would not reproduce); boff = prefix sums of the boundary counts.
   int stage1 = 0;  // 0 auto, 1 SSSP, 2 boundary graph whenever applicable
   bool bnd_dupfree = false;
+  // Every arc inside a part has its reverse with the same weight (and no
+  // duplicates): each part's local closure is a symmetric matrix, so the
+  // Floyd work queue computes only the tiles on and above the diagonal and
+  // stores each one's transpose (floyd_queue_items, sym).
+  bool sym_local = false;
   int64_t total_b = 0;
   std::vector<int32_t> boff;
   std::vector<int32_t> bpcol;  // boundary columns of dB padded per part to multiples of 4 (prefix sums)
@@ -524,7 +550,8 @@ extern "C" int fap_graph_destroy(fap_dgraph *G) try {
                       &G->d_msbf_items, &G->d_msbf_act, &G->d_msbf_changed, &G->d_bitro, &G->d_bitcol,
                       &G->d_botro, &G->d_botcol, &G->d_bitw, &G->d_bitems, &G->d_bDt, &G->d_bact, &G->d_bpact,
                       &G->d_bgpart, &G->d_bpcolmap, &G->d_grow, &G->d_pk_off, &G->d_pk_range,
-                      &G->d_pk_maxa, &G->d_pk_tiles, &G->q.items, &G->q.cnt, &G->cq.items, &G->cq.cnt})
+                      &G->d_pk_maxa, &G->d_pk_tiles, &G->q.items, &G->q.cnt, &G->cq.items, &G->cq.cnt,
+                      &G->d_xk_off, &G->d_xk_range, &G->d_xk_maxb, &G->d_xk_tiles})
       b->release();
     if (G->h_changed) cudaFreeHost(G->h_changed);
     for (cudaEvent_t &ev : G->cev)
@@ -608,6 +635,27 @@ extern "C" int fap_graph_set_parts(fap_dgraph *G, int32_t K, const int32_t *grap
         }
         seen[v] = u;
       }
+  }
+  {
+    // symmetric parts: sort the intra-part arcs and look each reverse up
+    G->sym_local = false;
+    if (G->bnd_dupfree) {
+      std::vector<std::pair<uint64_t, uint32_t>> arcs;
+      for (int32_t u = 0; u < n; u++)
+        for (int32_t e = G->h_ro[u]; e < G->h_ro[u + 1]; e++) {
+          const int32_t v = G->h_col[e];
+          if (graph_id[v] == graph_id[u] && v != u)
+            arcs.emplace_back(((uint64_t)(uint32_t)u << 32) | (uint32_t)v, G->h_w[e]);
+        }
+      std::sort(arcs.begin(), arcs.end());
+      bool sym = true;
+      for (size_t i = 0; i < arcs.size() && sym; i++) {
+        const uint64_t rev = (arcs[i].first << 32) | (arcs[i].first >> 32);
+        const auto it = std::lower_bound(arcs.begin(), arcs.end(), std::make_pair(rev, (uint32_t)0));
+        sym = it != arcs.end() && it->first == rev && it->second == arcs[i].second;
+      }
+      G->sym_local = sym;
+    }
   }
   {
     // edges of the boundary graph
@@ -869,9 +917,24 @@ int expand_bgraph(fap_dgraph *G, const PartDesc *dp, int np, int max_s, const T 
                   int *status, int64_t *L) {
   cudaStream_t st = G->ctx->stream;
   if (bgraph_bf(G)) {  // padded dB columns: TMA-fed tiles (F: np squares of side ldFB)
+    // packed 16-bit tiles where they provably fit (int32, "minplus_pack16")
+    Expand16 xk{};
+    const bool pack = G->pack16 && G->dtype == FAP_DTYPE_I32;
+    if (pack) {
+      const int64_t nrt = ceil_div(G->total_b, 128);
+      FAP_TRY(G->d_xk_off.ensure_async((size_t)np * G->total_b * 4, st));
+      FAP_TRY(G->d_xk_range.ensure_async((size_t)np * nrt * 4, st));
+      FAP_TRY(G->d_xk_maxb.ensure_async((size_t)np * 4, st));
+      if (!G->d_xk_tiles.p) {
+        FAP_TRY(G->d_xk_tiles.ensure_async(2 * sizeof(unsigned long long), st));
+        FAP_CK(cudaMemsetAsync(G->d_xk_tiles.p, 0, 2 * sizeof(unsigned long long), st));
+      }
+      xk = Expand16{G->d_xk_off.as<int32_t>(), G->d_xk_range.as<int32_t>(), G->d_xk_maxb.as<int32_t>(),
+                    (int32_t)nrt, G->d_xk_tiles.as<unsigned long long>()};
+    }
     FAP_CK(launch_bdy_expand_tma<T>(dp, np, max_s, (int)G->total_b, G->d_grow.as<const int64_t>(),
                                     G->d_st2ed.as<const int32_t>(), G->d_dB.as<const T>(), G->ldB, F, ldFB, np,
-                                    Dout, G->ldD, G->d_FB.as<T>(), ldFB, status, st, L));
+                                    Dout, G->ldD, G->d_FB.as<T>(), ldFB, status, st, L, pack ? &xk : nullptr));
     return FAP_OK;
   }
   if (!bgraph_tiled_expand(G)) {
@@ -993,7 +1056,10 @@ int prepare_batch(fap_dgraph *G, const std::vector<int32_t> &ids, bool cached, b
   std::vector<QItem> qitems;
   if (!cached) {
     int32_t mnb = 0;
-    qitems = floyd_queue_items(G->parts, &G->q.nfloyd, &mnb);
+    // (the local closures of the boundary-graph form are symmetric when the
+    // parts are; the SSSP form's matrices hold boundary rows and are not)
+    G->q.sym = bmethod && G->sym_local && G->floyd_sym;
+    qitems = floyd_queue_items(G->parts, G->q.sym, &G->q.nfloyd, &mnb);
     G->q.nitems = (int32_t)qitems.size();
     G->q.stride = 2 + 2 * mnb;
     G->q.nparts = (int32_t)G->parts.size();
@@ -1054,7 +1120,7 @@ cudaError_t run_floyd_queue(fap_dgraph *G, QueueBuf &qb, const PartDesc *dp, T *
   cudaError_t e = cudaMemsetAsync(qb.cnt.p, 0, ((size_t)qb.nparts * qb.stride + 2) * 4, st);
   if (e != cudaSuccess) return e;
   FloydQueue q{qb.items.as<const QItem>(), scatter ? qb.nitems : qb.nfloyd, mp_work, qb.cnt.as<int32_t>(),
-               qb.stride, qb.nparts};
+               qb.stride, qb.nparts, qb.sym ? 1 : 0};
   return launch_floyd_queue<T>(dp, qb.nparts, F, ldf, q, dw, G->n, D, G->ldD, drows, G->d_st2ed.as<const int32_t>(),
                                G->d_gid.as<const int32_t>(), G->d_ed2st.as<const int32_t>(), status, st, L,
                                nullptr);
@@ -1849,6 +1915,11 @@ extern "C" int fap_graph_set_param(fap_dgraph *G, const char *key, double value)
     G->floyd_queue = value != 0.0;
     return FAP_OK;
   }
+  if (std::strcmp(key, "floyd_symmetric") == 0) {
+    G->floyd_sym = value != 0.0;
+    G->last_ids.clear();
+    return FAP_OK;
+  }
   if (std::strcmp(key, "minplus_pack16") == 0) {
     G->pack16 = value != 0.0;
     G->last_ids.clear();
@@ -1956,6 +2027,21 @@ extern "C" int fap_graph_pack16_tiles(fap_dgraph *G, int64_t *packed, int64_t *t
   DeviceGuard g(G->ctx->device);
   unsigned long long h[2] = {0, 0};
   FAP_CK(cudaMemcpyAsync(h, G->d_pk_tiles.p, sizeof(h), cudaMemcpyDeviceToHost, G->ctx->stream));
+  FAP_CK(cudaStreamSynchronize(G->ctx->stream));
+  *packed = (int64_t)h[0];
+  *total = (int64_t)h[1];
+  return FAP_OK;
+} catch (...) {
+  return fail_exception();
+}
+
+extern "C" int fap_graph_expand16_tiles(fap_dgraph *G, int64_t *packed, int64_t *total) try {
+  if (!G || !packed || !total) return fail(FAP_ERR_INVALID, "NULL argument");
+  *packed = *total = 0;
+  if (!G->d_xk_tiles.p) return FAP_OK;
+  DeviceGuard g(G->ctx->device);
+  unsigned long long h[2] = {0, 0};
+  FAP_CK(cudaMemcpyAsync(h, G->d_xk_tiles.p, sizeof(h), cudaMemcpyDeviceToHost, G->ctx->stream));
   FAP_CK(cudaStreamSynchronize(G->ctx->stream));
   *packed = (int64_t)h[0];
   *total = (int64_t)h[1];
@@ -2083,7 +2169,8 @@ int cache_build_impl(fap_dgraph *G) {
         (size_t)std::max(sssp_scratch_rows(G->n, (int)src.size()), 1) * (size_t)G->n * 4));
   {
     int32_t mnb = 0;
-    const std::vector<QItem> qitems = floyd_queue_items(G->cparts, &G->cq.nfloyd, &mnb);
+    G->cq.sym = bm && G->sym_local && G->floyd_sym;
+    const std::vector<QItem> qitems = floyd_queue_items(G->cparts, G->cq.sym, &G->cq.nfloyd, &mnb);
     G->cq.nitems = (int32_t)qitems.size();
     G->cq.stride = 2 + 2 * mnb;
     G->cq.nparts = (int32_t)G->cparts.size();

@@ -788,7 +788,7 @@ __device__ __forceinline__ bool minplus_part_tile(const PartDesc &pd, const MPWo
         for (int j = 0; j < 8; j++) a16[i][j] = kPackInit;
       // (the engine's first barrier orders the column offsets before use)
       if (!tma_minplus_tile16<TC>(mapF, 0, pd.b + wk.m0, fz, mapD, n0, (int)pd.row_base, 0, K, a16, sm, pbuf,
-                                  coff, pd.s - pd.b - wk.m0))
+                                  nullptr, coff, pd.s - pd.b - wk.m0))
         return false;
       const int tx = threadIdx.x % C::TX;
 #pragma unroll
@@ -1002,15 +1002,19 @@ __global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS, 2)
         const int nb = (int)ceil_div(pd.s, kFloydTile);
         const int32_t *cn = q.cnt + (int64_t)c.pidx * q.stride;
         const int32_t *p2 = cn + 2, *p3 = cn + 2 + (q.stride - 2) / 2;
+        // items per pivot block (symmetric: the row panel, the tiles on and
+        // above the diagonal)
+        const int n2 = q.sym ? nb - 1 : 2 * (nb - 1);
+        const int n3 = q.sym ? (nb - 1) * nb / 2 : (nb - 1) * (nb - 1);
         bool ok = true;
         if (c.kind == kQFloyd1) {
-          if (c.kb > 0) ok = queue_wait(p3 + c.kb - 1, (nb - 1) * (nb - 1), abort);
-        } else if (c.kind == kQFloyd2) {
+          if (c.kb > 0) ok = queue_wait(p3 + c.kb - 1, n3, abort);
+        } else if (c.kind == kQFloyd2 || c.kind == kQFloyd2S) {
           ok = queue_wait(cn, c.kb + 1, abort);
-        } else if (c.kind == kQFloyd3) {
-          ok = queue_wait(p2 + c.kb, 2 * (nb - 1), abort);
+        } else if (c.kind == kQFloyd3 || c.kind == kQFloyd3S) {
+          ok = queue_wait(p2 + c.kb, n2, abort);
         } else if (c.kind == kQScatter) {
-          ok = nb == 1 ? queue_wait(cn, 1, abort) : queue_wait(p3 + nb - 1, (nb - 1) * (nb - 1), abort);
+          ok = nb == 1 ? queue_wait(cn, 1, abort) : queue_wait(p3 + nb - 1, n3, abort);
         } else {
           ok = queue_wait(cn + 1, (int)ceil_div(pd.b, kQScatterRows), abort);
         }
@@ -1034,12 +1038,15 @@ __global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS, 2)
       const int kb = cl.kb;
       floyd_diag_close<T, kFloydTile>(F + pd.f_off, pd.ldf, kb * kFloydTile, sm.ring,
                                       min(kFloydTile, pd.s - kb * kFloydTile));
-    } else if (kind == kQFloyd2 || kind == kQFloyd3) {
+    } else if (kind == kQFloyd2 || kind == kQFloyd3 || kind == kQFloyd2S || kind == kQFloyd3S) {
       const PartDesc pd = parts[cl.pidx];
       const int kb = cl.kb, t = cl.t;
       const int nb = (int)ceil_div(pd.s, kFloydTile);
       int i, j;
-      if (kind == kQFloyd3) {
+      if (kind == kQFloyd2S || kind == kQFloyd3S) {
+        i = t >> 16;
+        j = t & 0xffff;
+      } else if (kind == kQFloyd3) {
         i = t / (nb - 1);
         j = t % (nb - 1);
         i = i < kb ? i : i + 1;
@@ -1053,10 +1060,11 @@ __global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS, 2)
         j = kb;
       }
       const int z = (int)(pd.f_off / ((int64_t)pd.ldf * pd.ldf));
-      ok = floyd_tile_update<T, kFloydTile>(&mapA, &mapB, z, F + pd.f_off, pd.ldf, i, j, kb, sm,
-                                            min(kFloydTile, pd.s - kb * kFloydTile),
-                                            min(kFloydTile, pd.s - i * kFloydTile),
-                                            min(kFloydTile, pd.s - j * kFloydTile));
+      ok = floyd_tile_update_sym<T, kFloydTile>(&mapA, &mapB, z, F + pd.f_off, pd.ldf, i, j, kb, sm,
+                                                min(kFloydTile, pd.s - kb * kFloydTile),
+                                                min(kFloydTile, pd.s - i * kFloydTile),
+                                                min(kFloydTile, pd.s - j * kFloydTile),
+                                                kind == kQFloyd2S || kind == kQFloyd3S);
     } else if (kind == kQScatter) {
       // boundary rows kb .. kb + kQScatterRows of the closed matrix into D
       // (the reference's decode of rows < b, util_Myalgorithm.h:75-86)
@@ -1087,8 +1095,10 @@ __global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS, 2)
     if (tid == 0 && kind > 0) {
       int32_t *cn = q.cnt + (int64_t)cl.pidx * q.stride;
       const int half = (q.stride - 2) / 2;
-      int32_t *done = kind == kQFloyd1 ? cn : kind == kQFloyd2 ? cn + 2 + cl.kb
-                    : kind == kQFloyd3 ? cn + 2 + half + cl.kb : cn + 1;
+      int32_t *done = kind == kQFloyd1                           ? cn
+                      : (kind == kQFloyd2 || kind == kQFloyd2S) ? cn + 2 + cl.kb
+                      : (kind == kQFloyd3 || kind == kQFloyd3S) ? cn + 2 + half + cl.kb
+                                                                : cn + 1;
       __threadfence();
       atomicAdd(done, 1);
     }
@@ -2083,12 +2093,81 @@ cudaError_t launch_bgraph_bf(const PartDesc *parts, int nparts, int max_b, const
 // boundary columns (bd_col.., a 16-byte start), B = q's local rows
 // F_q[0..b_q) over columns n0.. (the arena map), K = b_q; the stores go to
 // the columns' original ids (st2ed), own-part values also to FB.
-template <typename T>
+// Packed-form bounds of the expansion (Expand16): grid (128-row tiles of dB,
+// parts), warp w takes rows m0 + w, m0 + w + 8, ...; its lanes read the
+// row's b_q entries of part q's boundary columns (coalesced).
+__global__ void __launch_bounds__(256)
+    expand16_rows_kernel(const PartDesc *__restrict__ parts, int nbB, const int32_t *__restrict__ dB,
+                         int64_t ldB, Expand16 xk) {
+  const PartDesc pd = parts[blockIdx.y];
+  const int m0 = blockIdx.x * 128, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int32_t tile_range = 0;
+  for (int r = warp; r < 128; r += 8) {
+    const int g = m0 + r;
+    if (g >= nbB) break;
+    const int32_t *row = dB + (int64_t)g * ldB + pd.bd_col;
+    int32_t lo = INT32_MAX, hi = 0;
+    for (int k = lane; k < pd.b; k += 32) {
+      const int32_t v = __ldg(row + k);
+      if (v < kInfI32) {
+        lo = min(lo, v);
+        hi = max(hi, v);
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+      hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    if (lane == 0) {
+      xk.off[(int64_t)blockIdx.y * nbB + g] = lo == INT32_MAX ? 0 : lo;
+      tile_range = max(tile_range, lo == INT32_MAX ? 0 : hi - lo);
+    }
+  }
+  __shared__ int32_t red[8];
+  if (lane == 0) red[warp] = tile_range;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int32_t m = 0;
+    for (int w = 0; w < 8; w++) m = max(m, red[w]);
+    xk.range[(int64_t)blockIdx.y * xk.nrt + blockIdx.x] = m;
+  }
+}
+
+// Largest finite F_q[b'][v] (b' < b_q, v < s_q) of every part (one CTA per
+// part); a negative entry (never produced from non-negative weights) makes
+// the part's tiles run in int32.
+__global__ void __launch_bounds__(256)
+    expand16_maxb_kernel(const PartDesc *__restrict__ parts, const int32_t *__restrict__ F, Expand16 xk) {
+  const PartDesc pd = parts[blockIdx.x];
+  const int64_t cnt = (int64_t)pd.b * pd.s;
+  int32_t m = 0;
+  for (int64_t e = threadIdx.x; e < cnt; e += blockDim.x) {
+    const int32_t v = __ldg(F + pd.f_off + (e / pd.s) * pd.ldf + e % pd.s);
+    if (v < 0) m = kPackCap;
+    else if (v < kInfI32) m = max(m, v);
+  }
+  __shared__ int32_t red[8];
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x / 32] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int32_t x = 0;
+    for (int w = 0; w < 8; w++) x = max(x, red[w]);
+    xk.maxB[blockIdx.x] = x;
+  }
+}
+
+// Tiled expansion (any boundary count): grid (column tiles, 128-row tiles of
+// dB, parts); a CTA is a min-plus tile dB[g][b'_q] (x) F_q[b'][j] written
+// to D rows grow[g], columns st2ed[start_q + j] (and, for g of part q itself,
+// to FB).  PACK (int32): a tile whose values provably fit (Expand16) runs
+// the packed 16-bit engine with its rows shifted by their offsets.
+template <typename T, bool PACK>
 __global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS, 2)
     bdy_expand_tma_kernel(const PartDesc *__restrict__ parts, int nbB, const int64_t *__restrict__ grow,
                           const int32_t *__restrict__ st2ed, T *D, int64_t ldD, T *FB, int64_t ldFB,
                           const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
-                          int *status) {
+                          int *status, Expand16 xk) {
   using TC = typename FloydCfg<T, kFloydTile>::TC;
   extern __shared__ __align__(128) unsigned char bxt_smem_raw[];
   const PartDesc pd = parts[blockIdx.z];
@@ -2098,14 +2177,59 @@ __global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS, 2)
   if (n0 >= pd.s) return;
   auto sm = tma_smem_init<T, TC>(bxt_smem_raw);
   T acc[8][8];
-#pragma unroll
-  for (int i = 0; i < 8; i++)
-#pragma unroll
-    for (int j = 0; j < 8; j++) acc[i][j] = Dist<T>::inf();
   const int fz = (int)(pd.f_off / ((int64_t)pd.ldf * pd.ldf));
-  if (!tma_minplus_tile<T, TC>(&mapA, pd.bd_col, m0, 0, &mapB, n0, 0, fz, pd.b, acc, sm)) {
-    if (threadIdx.x == 0) set_status(status, kDevTmaTimeout);
-    return;
+  bool packed = false;
+  if constexpr (PACK) {
+    packed = __ldg(xk.range + (int64_t)blockIdx.z * xk.nrt + blockIdx.y) + __ldg(xk.maxB + blockIdx.z) < kPackCap;
+    if (threadIdx.x == 0) {
+      atomicAdd(xk.tiles + 1, 1ull);
+      if (packed) atomicAdd(xk.tiles, 1ull);
+    }
+  }
+  if (packed) {
+    if constexpr (PACK) {
+      using P = Pack16Cfg<TC>;
+      const uintptr_t base = (reinterpret_cast<uintptr_t>(bxt_smem_raw) + 127) & ~uintptr_t(127);
+      uint32_t *pbuf = reinterpret_cast<uint32_t *>(base + P::BUF_OFFSET);
+      int32_t *roff = reinterpret_cast<int32_t *>(pbuf + 2 * P::BUF_ELEMS) + TC::BN;
+      for (int r = threadIdx.x; r < TC::BM; r += blockDim.x)
+        roff[r] = m0 + r < nbB ? __ldg(xk.off + (int64_t)blockIdx.z * nbB + m0 + r) : 0;
+      uint32_t a16[4][8];
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 8; j++) a16[i][j] = kPackInit;
+      // (the engine's first barrier orders the row offsets before use)
+      if (!tma_minplus_tile16<TC>(&mapA, pd.bd_col, m0, 0, &mapB, n0, 0, fz, pd.b, a16, sm, pbuf, roff, nullptr,
+                                  nbB - m0)) {
+        if (threadIdx.x == 0) set_status(status, kDevTmaTimeout);
+        return;
+      }
+      const int ty = threadIdx.x / TC::TX;
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        // pair i = 2g + h holds rows 4g + 2h and 4g + 2h + 1 of the thread
+        const int r0 = 4 * (i / 2) + 2 * (i % 2);
+        const int tr = (i / 2) * (TC::BM / 2) + ty * 4 + 2 * (i % 2);   // tile row of the pair's first
+        const int32_t o0 = roff[tr], o1 = roff[tr + 1];
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+          const int32_t lo = (int32_t)(int16_t)(a16[i][j] & 0xffffu);
+          const int32_t hi = (int32_t)(int16_t)(a16[i][j] >> 16);
+          acc[r0][j] = lo < kPackCap ? lo + o0 : Dist<T>::inf();
+          acc[r0 + 1][j] = hi < kPackCap ? hi + o1 : Dist<T>::inf();
+        }
+      }
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+#pragma unroll
+      for (int j = 0; j < 8; j++) acc[i][j] = Dist<T>::inf();
+    if (!tma_minplus_tile<T, TC>(&mapA, pd.bd_col, m0, 0, &mapB, n0, 0, fz, pd.b, acc, sm)) {
+      if (threadIdx.x == 0) set_status(status, kDevTmaTimeout);
+      return;
+    }
   }
   const int tid = threadIdx.x, ty = tid / TC::TX, tx = tid % TC::TX;
   int col[8];
@@ -2142,7 +2266,7 @@ template <typename T>
 cudaError_t launch_bdy_expand_tma(const PartDesc *parts, int nparts, int max_s, int nbB, const int64_t *grow,
                                   const int32_t *st2ed, const T *dB, int64_t ldB, const T *F, int64_t ldf,
                                   int nparts_f, T *D, int64_t ldD, T *FB, int64_t ldFB, int *status,
-                                  cudaStream_t stream, int64_t *launches) {
+                                  cudaStream_t stream, int64_t *launches, const Expand16 *xk) {
   using TC = typename FloydCfg<T, kFloydTile>::TC;
   if (nparts <= 0 || max_s <= 0 || nbB <= 0) return cudaSuccess;
   if (nparts > 65535 || ceil_div(nbB, TC::BM) > 65535) return cudaErrorInvalidConfiguration;
@@ -2150,12 +2274,30 @@ cudaError_t launch_bdy_expand_tma(const PartDesc *parts, int nparts, int max_s, 
   cudaError_t e = make_tmap_3d(&mapA, dB, Dist<T>::kDtype == FAP_DTYPE_F32, ldB, nbB, 1, TC::BK, TC::BM);
   if (e == cudaSuccess) e = make_arena_tmaps<T>(F, ldf, nparts_f, &unused, &mapB);
   if (e != cudaSuccess) return e;
+  const dim3 grid((unsigned)ceil_div(max_s, TC::BN), (unsigned)ceil_div(nbB, TC::BM), nparts);
+  Expand16 none{};
+  if constexpr (std::is_same<T, int32_t>::value) {
+    if (xk != nullptr) {
+      if (xk->nrt < (int)ceil_div(nbB, TC::BM)) return cudaErrorInvalidValue;
+      expand16_rows_kernel<<<dim3((unsigned)ceil_div(nbB, 128), (unsigned)nparts), 256, 0, stream>>>(
+          parts, nbB, dB, ldB, *xk);
+      expand16_maxb_kernel<<<(unsigned)nparts, 256, 0, stream>>>(parts, F, *xk);
+      *launches += 2;
+      const size_t smem = Pack16Cfg<TC>::SMEM_BYTES;
+      auto kern = bdy_expand_tma_kernel<T, true>;
+      e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+      kern<<<grid, TC::THREADS, smem, stream>>>(parts, nbB, grow, st2ed, D, ldD, FB, ldFB, mapA, mapB, status,
+                                                *xk);
+      *launches += 1;
+      return cudaGetLastError();
+    }
+  }
   const size_t smem = TC::SMEM_BYTES;
-  auto kern = bdy_expand_tma_kernel<T>;
+  auto kern = bdy_expand_tma_kernel<T, false>;
   e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  kern<<<dim3((unsigned)ceil_div(max_s, TC::BN), (unsigned)ceil_div(nbB, TC::BM), nparts), TC::THREADS, smem,
-         stream>>>(parts, nbB, grow, st2ed, D, ldD, FB, ldFB, mapA, mapB, status);
+  kern<<<grid, TC::THREADS, smem, stream>>>(parts, nbB, grow, st2ed, D, ldD, FB, ldFB, mapA, mapB, status, none);
   *launches += 1;
   return cudaGetLastError();
 }
@@ -2683,7 +2825,7 @@ cudaError_t launch_relax_peak(T *sink, int blocks, int iters, cudaStream_t strea
   template cudaError_t launch_bdy_expand_tma<T>(const PartDesc *, int, int, int, const int64_t *,  \
                                                 const int32_t *, const T *, int64_t, const T *,    \
                                                 int64_t, int, T *, int64_t, T *, int64_t, int *,   \
-                                                cudaStream_t, int64_t *);                          \
+                                                cudaStream_t, int64_t *, const Expand16 *);                          \
   template cudaError_t launch_bdy_expand_tiled<T>(const PartDesc *, int, int, int, const int64_t *, \
                                                   const int32_t *, const T *, int64_t, const T *,  \
                                                   T *, int64_t, T *, int64_t, cudaStream_t,        \

@@ -66,6 +66,20 @@ struct Pack16 {
   unsigned long long *tiles;  // [2]: tiles run packed, tiles run (cumulative)
 };
 
+// Packed 16-bit form of the tiled expansion of the boundary graph (int32):
+// per part q (index in the launch's part list) and boundary index g, off =
+// the least finite dB[g][b'] over q's boundary columns b'; per (q, 128-row
+// tile of dB) the largest finite dB[g][b'] - off (range); per part the
+// largest finite F_q[b'][v], b' < b_q, v < s_q (maxB).  A tile runs packed
+// when range + maxB < kPackCap (rows shifted by off, see tma_minplus_tile16).
+struct Expand16 {
+  int32_t *off;     // [nparts][nbB]
+  int32_t *range;   // [nparts][nrt]
+  int32_t *maxB;    // [nparts]
+  int32_t nrt;      // 128-row tiles of dB
+  unsigned long long *tiles;  // [2]: tiles run packed, tiles run (cumulative)
+};
+
 // Work queue of the batched Floyd-Warshall in one persistent launch: items
 // 0..nitems-1 are listed (kind, batch index, pivot block, tile) so that
 // every item's dependencies come earlier in the list, and CTAs claim them in
@@ -81,6 +95,9 @@ struct QItem {
   int32_t t;     // tile index within the phase
 };
 constexpr int32_t kQFloyd1 = 1, kQFloyd2 = 2, kQFloyd3 = 3, kQScatter = 4;
+// Symmetric matrices: the row-panel tile (kb, j) and the remainder tile
+// (i, j), i <= j, each also storing its transpose; t = i << 16 | j.
+constexpr int32_t kQFloyd2S = 5, kQFloyd3S = 6;
 constexpr int kQScatterRows = 8;
 struct FloydQueue {
   const QItem *items;
@@ -90,6 +107,7 @@ struct FloydQueue {
   int32_t stride;    // 2 + 2 * max_nb: Floyd-1 rounds done, scatter items done, then per pivot
                      // block the Floyd-2 and the Floyd-3 items done
   int32_t nparts;
+  int32_t sym;       // the Floyd items are the symmetric kinds
 };
 
 constexpr int kFloydTile = 128;
@@ -278,7 +296,7 @@ template <typename T>
 cudaError_t launch_bdy_expand_tma(const PartDesc *parts, int nparts, int max_s, int nbB, const int64_t *grow,
                                   const int32_t *st2ed, const T *dB, int64_t ldB, const T *F, int64_t ldf,
                                   int nparts_f, T *D, int64_t ldD, T *FB, int64_t ldFB, int *status,
-                                  cudaStream_t stream, int64_t *launches);
+                                  cudaStream_t stream, int64_t *launches, const Expand16 *xk = nullptr);
 // Tiled expansion (any boundary count): grid (boundary-index tiles, column
 // tiles, parts); a CTA is a min-plus tile dB[g][b'_q] (x) F_q[b'][j] written
 // to D[grow[g]][st2ed[start_q + j]] (and FB[g][j] for g of part q).

@@ -125,6 +125,47 @@ __device__ __forceinline__ bool floyd_tile_update(const CUtensorMap *mapA, const
   return ok;
 }
 
+// floyd_tile_update, and for a symmetric matrix (transpose, ti != tj) also
+// the transpose of the updated tile stored into (tj, ti), which then needs no
+// update of its own.  Each thread's 4 consecutive rows of a column
+// are 4 consecutive columns of the transposed tile: one 16-byte store, and
+// the two row quads of a warp fill whole 32-byte sectors.
+template <typename T, int TILE>
+__device__ __forceinline__ bool floyd_tile_update_sym(const CUtensorMap *mapA, const CUtensorMap *mapB,
+                                                      int z, T *mat, int64_t ld, int ti, int tj, int tk,
+                                                      TmaSmem<T, typename FloydCfg<T, TILE>::TC> &sm,
+                                                      int kvalid, int mvalid, int nvalid, bool transpose) {
+  using C = typename FloydCfg<T, TILE>::C;
+  using TC = typename FloydCfg<T, TILE>::TC;
+  using V = typename Vec4<T>::type;
+  T acc[C::TM][C::TN];
+  const int64_t r0 = (int64_t)ti * TILE, c0 = (int64_t)tj * TILE;
+  acc_load<T, C, true>(acc, mat + r0 * ld + c0, ld, 0, 0, 0, 0);
+  const bool ok = tma_minplus_tile<T, TC, true>(mapA, tk * TILE, ti * TILE, z, mapB, tj * TILE, tk * TILE,
+                                                z, kvalid, acc, sm, mvalid, nvalid);
+  if (!ok) return false;
+  acc_store<T, C, true>(acc, mat + r0 * ld + c0, ld, 0, 0, 0, 0);
+  if (transpose && ti != tj) {
+    const int tid = threadIdx.x, ty = tid / C::TX, tx = tid % C::TX;
+#pragma unroll
+    for (int gj = 0; gj < C::GN; gj++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int c = tile_col<C>(tx, gj, q);   // row of the transposed tile
+#pragma unroll
+        for (int gi = 0; gi < C::GM; gi++) {
+          V v;
+          v.x = acc[4 * gi + 0][4 * gj + q];
+          v.y = acc[4 * gi + 1][4 * gj + q];
+          v.z = acc[4 * gi + 2][4 * gj + q];
+          v.w = acc[4 * gi + 3][4 * gj + q];
+          *reinterpret_cast<V *>(mat + (c0 + c) * ld + r0 + tile_row<C>(ty, gi, 0)) = v;
+        }
+      }
+  }
+  return true;
+}
+
 // Closes one padded matrix (nb x nb tiles, s real rows) of part z with the
 // calling CTA.
 template <typename T, int TILE>

@@ -179,9 +179,9 @@ struct Pack16Cfg {
   static constexpr int PB_ELEMS = C::BK * C::BN;
   static constexpr int BUF_ELEMS = PA_ELEMS + PB_ELEMS;   // one buffer (two are used)
   // after the ring (128-byte aligned) and its mbarriers (64 bytes): the two
-  // packed buffers, then the tile's column offsets
+  // packed buffers, then the tile's column offsets, then its row offsets
   static constexpr int BUF_OFFSET = C::RING_BYTES + 64;
-  static constexpr int SMEM_BYTES = 128 + BUF_OFFSET + 2 * BUF_ELEMS * 4 + C::BN * 4;
+  static constexpr int SMEM_BYTES = 128 + BUF_OFFSET + 2 * BUF_ELEMS * 4 + C::BN * 4 + C::BM * 4;
   static_assert(C::STAGES * 8 <= 64, "mbarriers fit before the packed buffers");
   static_assert((PA_ELEMS * 4) % 16 == 0 && (BUF_ELEMS * 4) % 16 == 0, "16-byte aligned buffers");
   static_assert(C::BM == 128 && C::BN == 128 && C::THREADS == 256, "thread mapping below");
@@ -192,27 +192,33 @@ __device__ __forceinline__ uint32_t pack_pair(int32_t lo, int32_t hi) {
   return (uint32_t)(lo & 0xffff) | ((uint32_t)hi << 16);
 }
 
-// Converts ring stage (As, Bs) (kc valid k of BK) into PA / PB.  coff: the
-// tile's BN column offsets in shared memory.
+// An entry shifted by its offset and clamped: the sentinel (and anything at
+// least kPackCap above the offset) becomes kPackCap.
+__device__ __forceinline__ int32_t pack_clamp(int32_t v, int32_t off) {
+  return v >= kInfI32 ? kPackCap : min(v - off, kPackCap);
+}
+
+// Converts ring stage (As, Bs) (kc valid k of BK) into PA / PB.  roff: the
+// tile's BM row offsets of A, coff: its BN column offsets of B, in shared
+// memory (either may be null: no shift).
 template <class C>
 __device__ __forceinline__ void pack16_convert(const int32_t *As, const int32_t *Bs, uint32_t *PA,
-                                               uint32_t *PB, const int32_t *coff) {
+                                               uint32_t *PB, const int32_t *roff, const int32_t *coff) {
   using P = Pack16Cfg<C>;
   const int tid = threadIdx.x;
   // A: BK x BM/2 pairs; thread -> (k = tid % BK, p = tid / BK + q * THREADS / BK)
 #pragma unroll
   for (int q = 0; q < (C::BK * C::BM / 2) / C::THREADS; q++) {
     const int k = tid % C::BK, p = tid / C::BK + q * (C::THREADS / C::BK);
-    const int32_t a0 = min(As[(2 * p) * C::BK + k], kPackCap);
-    const int32_t a1 = min(As[(2 * p + 1) * C::BK + k], kPackCap);
+    const int32_t a0 = pack_clamp(As[(2 * p) * C::BK + k], roff ? roff[2 * p] : 0);
+    const int32_t a1 = pack_clamp(As[(2 * p + 1) * C::BK + k], roff ? roff[2 * p + 1] : 0);
     PA[k * P::PA_LD + p] = pack_pair(a0, a1);
   }
   // B: BK x BN, column fastest
 #pragma unroll
   for (int q = 0; q < (C::BK * C::BN) / C::THREADS; q++) {
     const int e = tid + q * C::THREADS;
-    const int c = e % C::BN;
-    const int32_t v = Bs[e] >= kInfI32 ? kPackCap : min(Bs[e] - coff[c], kPackCap);
+    const int32_t v = pack_clamp(Bs[e], coff ? coff[e % C::BN] : 0);
     PB[e] = pack_pair(v, v);
   }
 }
@@ -245,14 +251,15 @@ __device__ __forceinline__ void pack16_chunk_compute(const uint32_t *PA, const u
 }
 
 // The packed form of tma_minplus_tile (same boxes, same bounded waits).
-// pbuf: 2 * BUF_ELEMS words of shared memory; coff: BN column offsets in
-// shared memory, written before the call (the first barrier below orders
-// them before their use).
+// pbuf: 2 * BUF_ELEMS words of shared memory; roff / coff: BM row offsets of
+// A / BN column offsets of B in shared memory (null: no shift), written
+// before the call (the first barrier below orders them before their use).
 template <class C>
 __device__ __forceinline__ bool tma_minplus_tile16(const CUtensorMap *mapA, int ax, int ay, int az,
                                                    const CUtensorMap *mapB, int bx, int by, int bz,
                                                    int K, uint32_t (&acc)[4][8], TmaSmem<int32_t, C> &sm,
-                                                   uint32_t *pbuf, const int32_t *coff, int mvalid = C::BM) {
+                                                   uint32_t *pbuf, const int32_t *roff, const int32_t *coff,
+                                                   int mvalid = C::BM) {
   using P = Pack16Cfg<C>;
   const int tid = threadIdx.x, ty = tid / C::TX, tx = tid % C::TX;
   // rows skipped per warp as in tma_minplus_tile (row pairs of a warp lie
@@ -280,7 +287,7 @@ __device__ __forceinline__ bool tma_minplus_tile16(const CUtensorMap *mapA, int 
     uint32_t *PB = PA + P::PA_ELEMS;
     if (got) {
       const int32_t *As = sm.ring + s * C::STAGE_ELEMS;
-      pack16_convert<C>(As, As + C::A_ELEMS, PA, PB, coff);
+      pack16_convert<C>(As, As + C::A_ELEMS, PA, PB, roff, coff);
     }
     fence_proxy_async_smem();  // this thread's reads of stage s precede its refill
     // One barrier per chunk: after it the stage may be refilled (every

@@ -521,6 +521,13 @@ class DeviceGraph:
         check(lib().fap_graph_pack16_tiles(self._h, ctypes.byref(a), ctypes.byref(b)), "pack16_tiles")
         return int(a.value), int(b.value)
 
+    def expand16_tiles(self):
+        """(tiles of the boundary graph's tiled expansion run in the packed
+        16-bit form, tiles run) over every solve and cache build so far."""
+        a, b = ctypes.c_int64(), ctypes.c_int64()
+        check(lib().fap_graph_expand16_tiles(self._h, ctypes.byref(a), ctypes.byref(b)), "expand16_tiles")
+        return int(a.value), int(b.value)
+
     def stage1_name(self) -> str:
         """How stage 1 of the last solve ran, in words (fap_graph_stage1_name)."""
         return (lib().fap_graph_stage1_name(self._h) or b"").decode()

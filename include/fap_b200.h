@@ -179,6 +179,12 @@ FAP_API int fap_graph_set_param(fap_dgraph *g, const char *key, double value);
 /* Min-plus tiles run in the packed 16-bit form and in all, counted over
  * every solve of g so far (see "minplus_pack16").  Synchronous. */
 FAP_API int fap_graph_pack16_tiles(fap_dgraph *g, int64_t *packed, int64_t *total);
+/* The same for the tiles of the boundary graph's tiled expansion (int32,
+ * Bellman-Ford closure of the boundary graph): rows of the closed boundary
+ * graph are shifted by their least finite entry per part, and a tile runs
+ * packed when that part's largest finite boundary-row distance plus the
+ * tile's largest shifted entry is below 16383. */
+FAP_API int fap_graph_expand16_tiles(fap_dgraph *g, int64_t *packed, int64_t *total);
 
 /* Tunes the SSSP bucket width: runs the SSSP stage on `sample` boundary
  * sources spread over all parts (0 = one full wave of CTAs) for each of the

@@ -77,3 +77,24 @@ def test_packed_tiles_from_the_resident_cache(cuda_ok, tmp_path):
     for p in (2, 5, 9):
         assert np.array_equal(dg.copy_block(p), ref[p - 1]), f"part {p}"
     assert dg.pack16_tiles()[0] > 0
+
+
+def test_packed_expansion_tiles_equal_int32(cuda_ok):
+    """The tiled expansion of the boundary graph (Bellman-Ford closure, forced
+    on a small grid) in packed 16-bit tiles gives the int32 tiles' blocks."""
+    el = _grid(96, 200000, 13)
+    import tempfile
+    with tempfile.TemporaryDirectory() as tmp:
+        dg, vn, bn = _device_graph(el, 12, tmp, "pkx")
+    dg.set_param("bgraph_form", 2)
+    dg.set_param("minplus_pack16", 0)
+    dg.solve(None, FAP_MODE_BATCHED)
+    assert "Bellman-Ford" in dg.stage1_name()
+    ref = _blocks(dg, range(1, 13))
+    assert dg.expand16_tiles() == (0, 0)
+    dg.set_param("minplus_pack16", 1)
+    dg.solve(None, FAP_MODE_BATCHED)
+    for p in range(1, 13):
+        assert np.array_equal(dg.copy_block(p), ref[p - 1]), f"part {p}"
+    packed, total = dg.expand16_tiles()
+    assert 0 < packed <= total

@@ -2,7 +2,10 @@
 (parameter "floyd_queue", the default) against the three-launches-per-pivot
 form: the same tile updates run in the same dependency order, so the blocks
 are bit-identical (float32 too), in each form the queue takes:
-  boundary-graph stage 1        Floyd items only (local closures)
+  boundary-graph stage 1        Floyd items only (local closures); on
+                                undirected graphs only the tiles on and
+                                above the diagonal, each storing its
+                                transpose (parameter "floyd_symmetric")
   SSSP stage 1, packed min-plus Floyd + boundary-row scatter items
   SSSP stage 1, int32 / float32 Floyd + scatter + min-plus tiles, one launch
   resident cache build          Floyd (+ scatter) items of every part"""
@@ -56,3 +59,15 @@ def test_queue_in_the_cache_build(cuda_ok, name):
     dg.solve(parts, FAP_MODE_BATCHED)
     for p in parts:
         assert np.array_equal(dg.copy_block(p).view(np.int32), want[p - 1].view(np.int32)), f"part {p}"
+
+
+@pytest.mark.parametrize("name", ["grid128", "road20k"])
+def test_symmetric_queue_equals_full_queue(cuda_ok, name):
+    """Undirected parts: the local closures are symmetric, and computing the
+    upper tiles with their transposes gives the full computation's blocks."""
+    wl, dg = _dg(name)
+    want = _solve_all(dg, wl.K, True, floyd_symmetric=0)
+    got = _solve_all(dg, wl.K, True, floyd_symmetric=1)
+    assert "boundary graph" in dg.stage1_name()
+    for p, (a, b) in enumerate(zip(got, want), 1):
+        assert np.array_equal(a, b), f"part {p}"
