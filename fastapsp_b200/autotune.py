@@ -2,9 +2,11 @@
 
   tune_sssp   the SSSP bucket width (delta);
   tune_solve  the min-plus arithmetic of the part tiles (packed 16-bit where
-              the distances provably fit, or int32 throughout) and the form
-              of the batched Floyd (one persistent launch over a work queue,
-              or three launches per pivot block), timed as whole solves.
+              the distances provably fit, or int32 throughout), the form of
+              the batched Floyd (one persistent launch over a work queue, or
+              three launches per pivot block) and the boundary count up to
+              which parts take the thin min-plus kernel, timed as whole
+              solves.
 
 The best delta depends on the graph: on road-like graphs with deep
 shortest-path trees wide buckets win (few rounds), on small-world graphs
@@ -95,6 +97,11 @@ def tune_sssp(dg, ver_num, bdy_num, *, path: str | None = None, force: bool = Fa
 # thread and K chunks of 16 through a 4-stage TMA ring, is fixed: it is the
 # largest that keeps two CTAs and 128 registers per thread on an SM.)
 SOLVE_CANDIDATES = tuple({"minplus_pack16": p, "floyd_queue": q} for p in (1, 0) for q in (1, 0))
+# Second pass, from the best of the first: the boundary count up to which a
+# part takes the store-shaped thin min-plus kernel rather than the
+# register-tiled one (only when some part has 5..16 boundary vertices, where
+# the choice can matter).
+THIN_CANDIDATES = (16, 8, 4)
 
 
 def tune_solve(dg, ver_num, bdy_num, step, *, reps: int = 2, path: str | None = None,
@@ -114,17 +121,28 @@ def tune_solve(dg, ver_num, bdy_num, step, *, reps: int = 2, path: str | None = 
         for k, v in entry["params"].items():
             dg.set_param(k, v)
         return {**entry, "key": key, "cached": True}
-    cands = [c for c in SOLVE_CANDIDATES if dg.dtype == 0 or c["minplus_pack16"] == 0]
-    ms = []
-    for c in cands:
+    def timed(c):
         for k, v in c.items():
             dg.set_param(k, v)
         step()
-        ms.append(float(np.median([step() for _ in range(max(1, reps))])))
-    best = int(np.argmin(ms))
-    for k, v in cands[best].items():
+        return float(np.median([step() for _ in range(max(1, reps))]))
+
+    cands = [dict(c) for c in SOLVE_CANDIDATES if dg.dtype == 0 or c["minplus_pack16"] == 0]
+    ms = [timed(c) for c in cands]
+    best = cands[int(np.argmin(ms))]
+    bn = np.asarray(bdy_num)[1:]
+    if np.any((bn > min(THIN_CANDIDATES)) & (bn <= max(THIN_CANDIDATES))):
+        for t in THIN_CANDIDATES[1:]:
+            c = {**best, "thin_max_b": t}
+            cands.append(c)
+            ms.append(timed(c))
+        best = {**best, "thin_max_b": THIN_CANDIDATES[0]}
+        i = int(np.argmin(ms))
+        if "thin_max_b" in cands[i]:
+            best = cands[i]
+    for k, v in best.items():
         dg.set_param(k, v)
-    entry = {"params": cands[best], "ms": [round(x, 4) for x in ms], "candidates": cands}
+    entry = {"params": best, "ms": [round(x, 4) for x in ms], "candidates": cands}
     cache[key] = entry
     try:
         _save(path, cache)

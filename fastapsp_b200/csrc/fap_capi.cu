@@ -267,6 +267,10 @@ struct fap_dgraph {
   DevBuf d_xk_off, d_xk_range, d_xk_maxb, d_xk_tiles;
   // Work queue of the batched Floyd (FloydQueue): the batch's items and
   // counters, and the resident cache build's (its parts are all parts).
+  // Parts with at most this many boundary vertices (<= kThinBoundary) take
+  // the store-shaped thin min-plus kernel, the others the register-tiled
+  // one (parameter "thin_max_b", tuned with the solve form).
+  int thin_max_b = kThinBoundary;
   bool floyd_queue = true;
   bool floyd_sym = true;  // use sym_local in the queue (parameter "floyd_symmetric")
   QueueBuf q, cq;
@@ -1015,7 +1019,7 @@ int prepare_batch(fap_dgraph *G, const std::vector<int32_t> &ids, bool cached, b
     }
     G->part_src_off.push_back((int32_t)G->src.size());
     G->part_work_begin.push_back((int32_t)G->work.size());
-    if (d.b <= kThinBoundary) {
+    if (d.b <= G->thin_max_b) {
       G->thin_pos.push_back((int32_t)G->thin.size());
       G->thin.push_back((int32_t)i);
     } else {
@@ -1913,6 +1917,13 @@ extern "C" int fap_graph_set_param(fap_dgraph *G, const char *key, double value)
   }
   if (std::strcmp(key, "floyd_queue") == 0) {
     G->floyd_queue = value != 0.0;
+    return FAP_OK;
+  }
+  if (std::strcmp(key, "thin_max_b") == 0) {
+    if (!(value >= 0.0) || value > kThinBoundary)
+      return fail(FAP_ERR_INVALID, "thin_max_b is in [0, %d]", kThinBoundary);
+    G->thin_max_b = (int)value;
+    G->last_ids.clear();
     return FAP_OK;
   }
   if (std::strcmp(key, "floyd_symmetric") == 0) {

@@ -173,7 +173,14 @@ FAP_API int fap_graph_sssp_rows(fap_dgraph *g, const int32_t *sources, int32_t c
  * boundary-row column is shifted by its least finite entry and the part's
  * largest finite inner-to-boundary distance plus the tile's largest shifted
  * entry is below 16383; other tiles run in int32; the results are the same
- * int32 values either way; 0: int32 everywhere). */
+ * int32 values either way; 0: int32 everywhere); "floyd_queue" (default 1:
+ * the batched Floyd-Warshall as one persistent launch over a device work
+ * queue; 0: three launches per pivot block); "floyd_symmetric" (default 1:
+ * on parts whose arcs all have reverses of equal weight, the queue computes
+ * the local closures' tiles on and above the diagonal and stores their
+ * transposes); "thin_max_b" (0..16, default 16: parts with at most this many
+ * boundary vertices take the store-shaped thin min-plus kernel, the others
+ * the register-tiled one). */
 FAP_API int fap_graph_set_param(fap_dgraph *g, const char *key, double value);
 
 /* Min-plus tiles run in the packed 16-bit form and in all, counted over

@@ -90,7 +90,8 @@ class FakeSolveGraph:
 
     def step(self):
         cur = {k: self.params.get(k) for k in self.best}
-        return 1.0 if cur == self.best else 5.0
+        thin_penalty = 0.5 if self.params.get("thin_max_b", 16) != self.best.get("thin_max_b", 16) else 0.0
+        return (1.0 if cur == self.best else 5.0) + thin_penalty
 
 
 @pytest.mark.parametrize("dtype,best", [(0, {"minplus_pack16": 1, "floyd_queue": 0}),
@@ -107,3 +108,15 @@ def test_tune_solve_picks_the_fastest_and_caches_it(tmp_path, dtype, best):
     g2 = FakeSolveGraph(dtype, best)
     out2 = autotune.tune_solve(g2, vn, bn, lambda: pytest.fail("timed again"), path=path)
     assert out2["cached"] and g2.params == best
+
+
+def test_tune_solve_thin_threshold_second_pass(tmp_path):
+    """Parts with 5..16 boundary vertices: the thin-kernel threshold is tuned
+    after the arithmetic and Floyd form, from the best of those."""
+    path = str(tmp_path / "tune.json")
+    vn, bn = [0, 900, 910, 905], [0, 6, 9, 12]
+    best = {"minplus_pack16": 1, "floyd_queue": 1, "thin_max_b": 8}
+    g = FakeSolveGraph(0, best)
+    out = autotune.tune_solve(g, vn, bn, g.step, path=path)
+    assert out["params"] == best and g.params["thin_max_b"] == 8
+    assert len(out["candidates"]) == 4 + 2

@@ -98,3 +98,22 @@ def test_packed_expansion_tiles_equal_int32(cuda_ok):
         assert np.array_equal(dg.copy_block(p), ref[p - 1]), f"part {p}"
     packed, total = dg.expand16_tiles()
     assert 0 < packed <= total
+
+
+@pytest.mark.parametrize("thin_max_b", [0, 4, 8])
+def test_thin_threshold_changes_no_value(cuda_ok, thin_max_b):
+    """Parts with few boundary vertices in the register-tiled (packed) min-plus
+    instead of the thin kernel give the same blocks (the autotuner's third
+    choice)."""
+    from fastapsp_b200 import workloads
+    wl = workloads.load("road20k")
+    ro, col, w = wl.csr()
+    dg = DeviceGraph(Context(0), ro, col, w)
+    dg.set_parts(wl.K, wl.graph.getGraphId(), wl.graph.getMapping(), wl.ver_num, wl.ver_offset, wl.bdy_num)
+    dg.solve(None, FAP_MODE_BATCHED)
+    want = _blocks(dg, range(1, wl.K + 1))
+    dg.set_param("thin_max_b", thin_max_b)
+    for mode in (FAP_MODE_BATCHED, FAP_MODE_PLAIN):
+        dg.solve(None, mode)
+        for p in range(1, wl.K + 1):
+            assert np.array_equal(dg.copy_block(p), want[p - 1]), f"part {p} mode {mode}"
