@@ -1119,13 +1119,15 @@ int ensure_in_edges(fap_dgraph *G);
 // scatter into D, and with mp_work > 0 that many min-plus work items' tiles).
 template <typename T>
 cudaError_t run_floyd_queue(fap_dgraph *G, QueueBuf &qb, const PartDesc *dp, T *F, int64_t ldf, bool scatter,
-                            const MPWork *dw, int mp_work, T *D, int64_t drows, int *status, int64_t *L) {
+                            const MPWork *dw, int mp_work, T *D, int64_t drows, int *status, int64_t *L,
+                            int arena_parts = -1) {
   cudaStream_t st = G->ctx->stream;
   cudaError_t e = cudaMemsetAsync(qb.cnt.p, 0, ((size_t)qb.nparts * qb.stride + 2) * 4, st);
   if (e != cudaSuccess) return e;
   FloydQueue q{qb.items.as<const QItem>(), scatter ? qb.nitems : qb.nfloyd, mp_work, qb.cnt.as<int32_t>(),
                qb.stride, qb.nparts, qb.sym ? 1 : 0};
-  return launch_floyd_queue<T>(dp, qb.nparts, F, ldf, q, dw, G->n, D, G->ldD, drows, G->d_st2ed.as<const int32_t>(),
+  return launch_floyd_queue<T>(dp, arena_parts > 0 ? arena_parts : qb.nparts, F, ldf, q, dw, G->n, D, G->ldD,
+                               drows, G->d_st2ed.as<const int32_t>(),
                                G->d_gid.as<const int32_t>(), G->d_ed2st.as<const int32_t>(), status, st, L,
                                nullptr);
 }

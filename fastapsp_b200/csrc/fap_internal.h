@@ -193,7 +193,8 @@ cudaError_t launch_bdy_scatter(const PartDesc *parts, int nparts, const T *F, T 
                                int64_t *launches);
 
 // The batched Floyd-Warshall of every part as one persistent launch over a
-// work queue (FloydQueue); with q.mp_work > 0 also the boundary-row scatter
+// work queue (FloydQueue; nparts = the squares in the arena F, which the
+// queue's parts index by f_off); with q.mp_work > 0 also the boundary-row scatter
 // into D (as launch_bdy_scatter) and the min-plus tiles (as
 // launch_minplus_parts, pk as there).  q.cnt must be zero (nparts * stride
 // + 2 ints) when the launch starts.
