@@ -896,7 +896,34 @@ def main_fap(args):
         dg.reserve(max(rows_of(g, vn) for g in groups))
     log(f"{len(groups)} group(s) of parts; rows budget {budget_rows}")
 
+    # N > 1: the sharded boundary-graph form when the graph takes it (each
+    # rank closes its own parts locally, an NCCL all-gather exchanges their
+    # boundary rows, each rank closes the boundary graph and merges its own
+    # parts); otherwise each rank's partial batch takes stage 1 by SSSP
+    shard = None
+    if world > 1 and args.stage1 != 1 and not staged:
+        from fastapsp_b200 import FapError
+        from fastapsp_b200.sharding import shard_layout
+        owner, elems, stride, _ = shard_layout(vn, bn, shard_parts(vn, bn, n, world))
+        tdt = torch.int32 if dtype == 0 else torch.float32
+        send = torch.zeros(max(stride, 1), dtype=tdt, device="cuda")
+        recv = torch.zeros(world * max(stride, 1), dtype=tdt, device="cuda")
+        try:
+            dg.shard_begin(mine, send.data_ptr(), stride)
+            shard = (owner, stride, send, recv)
+        except FapError as e:
+            log(f"sharded boundary-graph form not available ({e}); partial batches per rank")
+        barrier()
+
     def solve_all(mode):
+        if shard is not None and mode == FAP_MODE_BATCHED:
+            owner_, stride_, send_, recv_ = shard
+            dg.shard_begin(mine, send_.data_ptr(), stride_)
+            dist.all_gather_into_tensor(recv_, send_)
+            dg.shard_finish(recv_.data_ptr(), world, owner_, stride_)
+            for grp in groups:
+                dg.solve(grp, mode, check_errors=False)
+            return
         if staged and mode == FAP_MODE_BATCHED:
             dg.cache_build(rebuild=True)
         for grp in groups:
@@ -916,7 +943,7 @@ def main_fap(args):
         return e0.elapsed_time(e1)
 
     solve_tuned = None
-    if not (args.no_pack16 or args.no_queue or args.no_tune_solve):
+    if not (args.no_pack16 or args.no_queue or args.no_tune_solve or shard is not None):
         solve_tuned = autotune.tune_solve(dg, vn, bn, timed_step)
         dg.check()
         log(f"solve form {solve_tuned['params']} ({'cached' if solve_tuned['cached'] else 'tuned'}: "
@@ -950,6 +977,13 @@ def main_fap(args):
             dg.cache_build(rebuild=True)
             launches += dg.last_launches()
             ec.record(stream)
+        if shard is not None:
+            owner_, stride_, send_, recv_ = shard
+            dg.shard_begin(mine, send_.data_ptr(), stride_)
+            launches += dg.last_launches()
+            dist.all_gather_into_tensor(recv_, send_)
+            dg.shard_finish(recv_.data_ptr(), world, owner_, stride_)
+            launches += dg.last_launches()
         for grp in groups:
             dg.solve(grp, FAP_MODE_BATCHED, check_errors=False)
             if len(groups) > 1:
@@ -998,7 +1032,7 @@ def main_fap(args):
 
     # ---- batched with predecessor matrices (optional) ----
     paths = None
-    if args.paths:
+    if args.paths and shard is None:
         try:
             dg.set_param("paths", 1)
             dg.solve(groups[0], FAP_MODE_BATCHED, check_errors=True)   # allocates P
@@ -1110,6 +1144,11 @@ def main_fap(args):
         g2.reserve(max(rows_of(g, vn) for g in groups))
         if staged:
             g2.cache_build()
+        if shard is not None:
+            owner_, stride_, send_, recv_ = shard
+            g2.shard_begin(mine, send_.data_ptr(), stride_)
+            dist.all_gather_into_tensor(recv_, send_)
+            g2.shard_finish(recv_.data_ptr(), world, owner_, stride_)
         for grp in groups:
             g2.solve(grp, FAP_MODE_BATCHED)
             for p in grp:

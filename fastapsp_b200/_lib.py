@@ -120,6 +120,8 @@ _SIGS = {
     "fap_floyd_noalloc_status": (INT, []),
     "fap_graph_pack16_tiles": (INT, [P, ctypes.POINTER(I64), ctypes.POINTER(I64)]),
     "fap_graph_expand16_tiles": (INT, [P, ctypes.POINTER(I64), ctypes.POINTER(I64)]),
+    "fap_graph_shard_begin": (INT, [P, P, I32, P, I64, ctypes.POINTER(I64)]),
+    "fap_graph_shard_finish": (INT, [P, P, I32, P, I64]),
     "fap_legacy_last_status": (INT, []),
     "fap_host_last_error": (ctypes.c_char_p, []),
     "fap_host_from_mtx": (INT, [ctypes.c_char_p, INT, INT, INT, PP]),

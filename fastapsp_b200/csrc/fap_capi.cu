@@ -289,6 +289,12 @@ struct fap_dgraph {
   // (cF, equal padded squares of side cache_ldf, part p at (p - 1)).
   bool cache_ready = false;
   bool use_cache = true;
+  // Sharded boundary-graph form (fap_graph_shard_*): the rank's own parts
+  // (ascending) and which cache slots hold finished parts (empty: all).
+  std::vector<int32_t> shard_own;
+  bool shard_begun = false;
+  std::vector<char> cache_valid;
+  DevBuf d_cown;
   // Boundary-graph form of stage 1 (see launch_bgraph): applicable when no
   // two arcs join the same ordered pair inside a part (the reference's
   // matrix build keeps the last of such duplicates, which the local closure
@@ -533,6 +539,8 @@ void cache_drop(fap_dgraph *G) {
                     &G->d_rowidx})
     b->release();
   G->cache_ready = false;
+  G->cache_valid.clear();
+  G->shard_begun = false;
   G->cb_off.clear();
   G->cparts.clear();
   G->last_ids.clear();
@@ -918,7 +926,7 @@ int close_bgraph(fap_dgraph *G, const PartDesc *dp, int np, int max_b, const T *
 // expansion for small boundary sets, the tiled one otherwise.  Also FB.
 template <typename T>
 int expand_bgraph(fap_dgraph *G, const PartDesc *dp, int np, int max_s, const T *F, T *Dout, int64_t ldFB,
-                  int *status, int64_t *L) {
+                  int *status, int64_t *L, int64_t nrows = -1) {
   cudaStream_t st = G->ctx->stream;
   if (bgraph_bf(G)) {  // padded dB columns: TMA-fed tiles (F: np squares of side ldFB)
     // packed 16-bit tiles where they provably fit (int32, "minplus_pack16")
@@ -942,7 +950,9 @@ int expand_bgraph(fap_dgraph *G, const PartDesc *dp, int np, int max_s, const T 
     return FAP_OK;
   }
   if (!bgraph_tiled_expand(G)) {
-    FAP_CK(launch_bdy_expand<T>(G->d_brows.as<const int64_t>(), (int)G->total_b, G->d_bpart.as<const BPart>(),
+    // (rows: the first nrows (boundary index, output row) pairs of d_brows)
+    FAP_CK(launch_bdy_expand<T>(G->d_brows.as<const int64_t>(), nrows >= 0 ? (int)nrows : (int)G->total_b,
+                                G->d_bpart.as<const BPart>(),
                                 G->d_gid.as<const int32_t>(), G->d_ed2st.as<const int32_t>(), G->n,
                                 G->d_dB.as<const T>(), G->ldB, (int)G->total_b, F, Dout, G->ldD, G->d_FB.as<T>(),
                                 ldFB, st, L));
@@ -1362,6 +1372,10 @@ extern "C" int fap_solve(fap_dgraph *G, const int32_t *parts, int32_t count, int
     G->epoch++;
   }
   const bool cached = mode == FAP_MODE_BATCHED && G->cache_ready && G->use_cache;
+  if (cached && !G->cache_valid.empty())
+    for (const int32_t p : ids)
+      if (!G->cache_valid[p])
+        return fail(FAP_ERR_STATE, "part %d is another rank's: the sharded cache holds this rank's parts only", p);
   const bool bmethod = !cached && mode == FAP_MODE_BATCHED && (int32_t)ids.size() == G->K && bmethod_ok(G);
   FAP_TRY(prepare_batch(G, ids, cached, bmethod));
   int rc = FAP_OK;
@@ -2256,6 +2270,7 @@ int cache_build_impl(fap_dgraph *G) {
   G->cache_max_b = cs.max_b;
   G->cache_max_s = cs.max_s;
   G->cache_ready = true;
+  G->cache_valid.clear();  // every part
   G->launches = L;
   c->launches += L;
   // The SSSP scratch (up to one row of n per resident CTA) is not needed by
@@ -2360,6 +2375,219 @@ extern "C" int fap_graph_cache_rebuild(fap_dgraph *G) try {
   return rc;
 } catch (...) {
   if (G) cache_drop(G);  // a half-built cache is not kept
+  return fail_exception();
+}
+
+// ---------------------------------------------------------------------------
+// Sharded boundary-graph form: parts split over ranks (one process per GPU).
+// Each rank closes its own parts locally, the ranks all-gather the boundary
+// rows of those local closures, and each rank then closes the boundary graph
+// itself (the same work on every rank), expands the boundary rows of its own
+// parts and makes their closures exact, leaving them in the resident cache
+// for fap_solve.  The layout of a rank's send buffer: its own parts in
+// ascending order, each part's rows 0..b-1, columns 0..s-1 of its local
+// closure, row-major.
+// ---------------------------------------------------------------------------
+namespace {
+template <typename T>
+int shard_begin_impl(fap_dgraph *G, void *send, int64_t send_cap, int64_t *send_elems) {
+  fap_ctx *c = G->ctx;
+  cudaStream_t st = c->stream;
+  const int32_t K = G->K;
+  const CacheShape cs = cache_shape(G);
+  if (cs.total_b > INT32_MAX) return fail(FAP_ERR_RANGE, "too many boundary vertices for the cache");
+  int64_t need = 0;
+  for (const int32_t p : G->shard_own) need += (int64_t)G->bnum[p] * G->vnum[p];
+  *send_elems = need;
+  if (need > send_cap) return fail(FAP_ERR_INVALID, "send buffer holds %lld elements, %lld needed",
+                                   (long long)send_cap, (long long)need);
+  FAP_CK(cudaStreamSynchronize(st));
+  FAP_TRY(G->cBd.ensure((size_t)std::max<int64_t>(cs.total_b, 1) * G->ldD * 4));
+  FAP_TRY(G->cF.ensure((size_t)K * cs.ldf * cs.ldf * 4));
+  G->cb_off.assign(K + 2, 0);
+  for (int32_t p = 1; p <= K; p++) G->cb_off[p + 1] = G->cb_off[p] + G->bnum[p];
+  G->cparts.clear();
+  std::vector<PartDesc> own;
+  for (int32_t p = 1; p <= K; p++) {
+    PartDesc d{};
+    d.part = p;
+    d.start = G->voff[p];
+    d.s = G->vnum[p];
+    d.b = G->bnum[p];
+    d.row_base = G->cb_off[p];
+    d.ldf = cs.ldf;
+    d.f_off = (int64_t)(p - 1) * cs.ldf * cs.ldf;
+    d.bd_row = (int32_t)G->cb_off[p];
+    d.flags = kPartLocal;
+    d.bd_col = G->bpcol[p];
+    G->cparts.push_back(d);
+  }
+  for (const int32_t p : G->shard_own) own.push_back(G->cparts[p - 1]);
+  FAP_TRY(G->d_cparts.ensure(G->cparts.size() * sizeof(PartDesc)));
+  FAP_TRY(G->d_cown.ensure(std::max<size_t>(own.size(), 1) * sizeof(PartDesc)));
+  {
+    int32_t mnb = 0;
+    G->cq.sym = G->sym_local && G->floyd_sym;
+    const std::vector<QItem> qitems = floyd_queue_items(own, G->cq.sym, &G->cq.nfloyd, &mnb);
+    G->cq.nitems = (int32_t)qitems.size();
+    G->cq.stride = 2 + 2 * mnb;
+    G->cq.nparts = (int32_t)own.size();
+    FAP_TRY(G->cq.items.ensure(std::max<size_t>(qitems.size(), 1) * sizeof(QItem)));
+    FAP_TRY(G->cq.cnt.ensure(((size_t)G->cq.nparts * G->cq.stride + 2) * 4));
+    if (!qitems.empty())
+      FAP_CK(cudaMemcpy(G->cq.items.p, qitems.data(), qitems.size() * sizeof(QItem), cudaMemcpyHostToDevice));
+  }
+  FAP_CK(cudaMemcpy(G->d_cparts.p, G->cparts.data(), G->cparts.size() * sizeof(PartDesc), cudaMemcpyHostToDevice));
+  if (!own.empty())
+    FAP_CK(cudaMemcpy(G->d_cown.p, own.data(), own.size() * sizeof(PartDesc), cudaMemcpyHostToDevice));
+  G->last_ids.clear();
+  G->epoch++;
+  T *F = G->cF.as<T>();
+  int *status = G->d_status.as<int>();
+  int64_t L = 0;
+  FAP_CK(cudaMemsetAsync(status, 0, sizeof(int), st));
+  if (!own.empty()) {
+    // local closures of the own parts (their slots of the cache's arena)
+    FAP_CK(launch_gather<T>(G->d_cown.as<const PartDesc>(), (int)own.size(), cs.ldf, G->ro.as<const int32_t>(),
+                            G->col.as<const int32_t>(), G->w.as<const T>(), G->d_gid.as<const int32_t>(),
+                            G->d_st2ed.as<const int32_t>(), G->d_ed2st.as<const int32_t>(), G->cBd.as<T>(),
+                            G->ldD, F, st, &L));
+    FAP_CK(run_floyd_queue<T>(G, G->cq, G->d_cown.as<const PartDesc>(), F, cs.ldf, false, nullptr, 0,
+                              G->cBd.as<T>(), 0, status, &L, (int)K));
+    // their boundary rows, packed
+    int64_t off = 0;
+    for (const PartDesc &d : own) {
+      if (d.b > 0)
+        FAP_CK(cudaMemcpy2DAsync(static_cast<T *>(send) + off, (size_t)d.s * 4, F + d.f_off, (size_t)cs.ldf * 4,
+                                 (size_t)d.s * 4, (size_t)d.b, cudaMemcpyDeviceToDevice, st));
+      off += (int64_t)d.b * d.s;
+    }
+  }
+  G->launches = L;
+  c->launches += L;
+  FAP_TRY(read_status(G));
+  G->cache_ldf = cs.ldf;
+  G->cache_max_b = cs.max_b;
+  G->cache_max_s = cs.max_s;
+  G->shard_begun = true;
+  return FAP_OK;
+}
+
+template <typename T>
+int shard_finish_impl(fap_dgraph *G, const void *recv, int32_t world, const int32_t *owner, int64_t stride) {
+  fap_ctx *c = G->ctx;
+  cudaStream_t st = c->stream;
+  const int32_t K = G->K;
+  const int64_t ldf = G->cache_ldf;
+  T *F = G->cF.as<T>();
+  const T *R = static_cast<const T *>(recv);
+  std::vector<char> mine((size_t)K + 1, 0);
+  for (const int32_t p : G->shard_own) mine[p] = 1;
+  // other ranks' boundary rows into their parts' slots
+  std::vector<int64_t> off((size_t)world, 0);
+  for (int32_t p = 1; p <= K; p++) {
+    const int32_t r = owner[p];
+    const PartDesc &d = G->cparts[p - 1];
+    const int64_t elems = (int64_t)d.b * d.s;
+    if (off[r] + elems > stride) return fail(FAP_ERR_INVALID, "rank %d's parts exceed the stride", r);
+    if (!mine[p] && d.b > 0)
+      FAP_CK(cudaMemcpy2DAsync(F + d.f_off, (size_t)ldf * 4, R + (int64_t)r * stride + off[r], (size_t)d.s * 4,
+                               (size_t)d.s * 4, (size_t)d.b, cudaMemcpyDeviceToDevice, st));
+    off[r] += elems;
+  }
+  FAP_CK(cudaStreamSynchronize(st));
+  FAP_TRY(prepare_bgraph(G, G->cparts));
+  // the staged expansion writes only the listed rows: the own parts' first
+  int64_t nrows = -1;
+  if (!bgraph_bf(G) && !bgraph_tiled_expand(G)) {
+    std::vector<int64_t> rows;
+    for (const int32_t p : G->shard_own) {
+      const PartDesc &d = G->cparts[p - 1];
+      for (int32_t k = 0; k < d.b; k++) {
+        rows.push_back(G->boff[p] + k);
+        rows.push_back(d.row_base + k);
+      }
+    }
+    nrows = (int64_t)rows.size() / 2;
+    if (!rows.empty())
+      FAP_CK(cudaMemcpy(G->d_brows.p, rows.data(), rows.size() * 8, cudaMemcpyHostToDevice));
+  }
+  const PartDesc *dp = G->d_cparts.as<const PartDesc>();
+  T *Bd = G->cBd.as<T>();
+  int *status = G->d_status.as<int>();
+  const int64_t rounds = G->sssp_max_rounds > 0 ? G->sssp_max_rounds : 8 * (int64_t)G->n + 1024;
+  int64_t L = 0;
+  FAP_CK(cudaMemsetAsync(status, 0, sizeof(int), st));
+  FAP_TRY(close_bgraph<T>(G, dp, K, G->cache_max_b, F, status, rounds, &L));
+  FAP_TRY(expand_bgraph<T>(G, dp, K, G->cache_max_s, F, Bd, ldf, status, &L, nrows));
+  if (!G->shard_own.empty())
+    FAP_CK(launch_local_fixup<T>(G->d_cown.as<const PartDesc>(), (int)G->shard_own.size(), G->cache_max_s, F,
+                                 G->d_FB.as<const T>(), ldf, st, &L));
+  G->launches = L;
+  c->launches += L;
+  FAP_TRY(read_status(G));
+  G->cache_bmethod = true;
+  G->cache_stage1_name = std::string("sharded ") + stage1_form_name(G, true);
+  G->cache_ready = true;
+  G->cache_valid = mine;
+  G->last_ids.clear();
+  G->epoch++;
+  return FAP_OK;
+}
+}  // namespace
+
+extern "C" int fap_graph_shard_begin(fap_dgraph *G, const int32_t *own_parts, int32_t count, void *send,
+                                     int64_t send_cap, int64_t *send_elems) try {
+  if (!G || !send_elems || (count > 0 && (!own_parts || !send))) return fail(FAP_ERR_INVALID, "NULL argument");
+  if (G->K == 0) return fail(FAP_ERR_STATE, "fap_graph_shard_begin before fap_graph_set_parts");
+  if (!bmethod_ok(G) || !G->floyd_queue)
+    return fail(FAP_ERR_STATE, "the sharded form needs the boundary-graph form of stage 1 (an int32 graph "
+                               "without duplicate arcs inside a part) and the Floyd work queue");
+  std::vector<char> seen((size_t)G->K + 1, 0);
+  std::vector<int32_t> own;
+  for (int32_t i = 0; i < count; i++) {
+    const int32_t p = own_parts[i];
+    if (p < 1 || p > G->K || seen[p]) return fail(FAP_ERR_INVALID, "bad or repeated part id %d", p);
+    seen[p] = 1;
+    own.push_back(p);
+  }
+  std::sort(own.begin(), own.end());
+  DeviceGuard g(G->ctx->device);
+  cache_drop(G);
+  G->shard_own = own;
+  const int rc = G->dtype == FAP_DTYPE_I32 ? shard_begin_impl<int32_t>(G, send, send_cap, send_elems)
+                                           : shard_begin_impl<float>(G, send, send_cap, send_elems);
+  if (rc != FAP_OK) cache_drop(G);
+  return rc;
+} catch (...) {
+  if (G) cache_drop(G);
+  return fail_exception();
+}
+
+extern "C" int fap_graph_shard_finish(fap_dgraph *G, const void *recv, int32_t world, const int32_t *owner,
+                                      int64_t stride) try {
+  if (!G || !recv || !owner) return fail(FAP_ERR_INVALID, "NULL argument");
+  if (!G->shard_begun) return fail(FAP_ERR_STATE, "fap_graph_shard_finish before fap_graph_shard_begin");
+  if (world < 1 || stride < 0) return fail(FAP_ERR_INVALID, "bad world or stride");
+  for (int32_t p = 1; p <= G->K; p++)
+    if (owner[p] < 0 || owner[p] >= world) return fail(FAP_ERR_INVALID, "part %d: owner %d outside 0..%d", p,
+                                                       owner[p], world - 1);
+  // this rank's parts are exactly the parts of one owner rank
+  if (!G->shard_own.empty()) {
+    const int32_t r0 = owner[G->shard_own[0]];
+    std::vector<char> mine((size_t)G->K + 1, 0);
+    for (const int32_t p : G->shard_own) mine[p] = 1;
+    for (int32_t p = 1; p <= G->K; p++)
+      if ((owner[p] == r0) != (mine[p] != 0))
+        return fail(FAP_ERR_INVALID, "owner[] does not give this rank's parts (part %d)", p);
+  }
+  DeviceGuard g(G->ctx->device);
+  const int rc = G->dtype == FAP_DTYPE_I32 ? shard_finish_impl<int32_t>(G, recv, world, owner, stride)
+                                           : shard_finish_impl<float>(G, recv, world, owner, stride);
+  if (rc != FAP_OK) cache_drop(G);
+  return rc;
+} catch (...) {
+  if (G) cache_drop(G);
   return fail_exception();
 }
 

@@ -521,6 +521,25 @@ class DeviceGraph:
         check(lib().fap_graph_pack16_tiles(self._h, ctypes.byref(a), ctypes.byref(b)), "pack16_tiles")
         return int(a.value), int(b.value)
 
+    def shard_begin(self, own_parts, send_ptr: int, send_cap: int) -> int:
+        """Sharded boundary-graph form, step 1 (fap_graph_shard_begin): local
+        closures of this rank's parts; their boundary rows packed into the
+        device buffer at send_ptr (send_cap elements of the graph's dtype).
+        Returns the element count written."""
+        ids = _i32(list(own_parts))
+        out = ctypes.c_int64()
+        check(lib().fap_graph_shard_begin(self._h, ptr(ids), int(ids.shape[0]), ctypes.c_void_p(send_ptr),
+                                          int(send_cap), ctypes.byref(out)), "fap_graph_shard_begin")
+        return int(out.value)
+
+    def shard_finish(self, recv_ptr: int, world: int, owner, stride: int) -> None:
+        """Step 2 (fap_graph_shard_finish): every rank's packed rows at
+        recv_ptr (rank r's at r * stride elements), owner[p] = rank of part p
+        (index 0 unused).  Leaves this rank's parts in the resident cache."""
+        own = _i32(owner)
+        check(lib().fap_graph_shard_finish(self._h, ctypes.c_void_p(recv_ptr), int(world), ptr(own),
+                                           int(stride)), "fap_graph_shard_finish")
+
     def expand16_tiles(self):
         """(tiles of the boundary graph's tiled expansion run in the packed
         16-bit form, tiles run) over every solve and cache build so far."""

@@ -75,3 +75,24 @@ def group_parts_by_rows(parts: Sequence[int], ver_num: Sequence[int], max_rows: 
     if cur:
         groups.append(cur)
     return groups
+
+
+def shard_layout(ver_num: Sequence[int], bdy_num: Sequence[int], shards: Sequence[Sequence[int]]):
+    """Layout of the boundary-row exchange of the sharded boundary-graph form
+    (fap_graph_shard_begin / _finish): owner[p] = rank of part p (index 0
+    unused), elems[r] = elements rank r sends (its parts ascending, b_p x s_p
+    each), stride = the largest of them (every rank's send buffer is padded
+    to it for the all-gather), offset[p] = where part p's rows start inside
+    its owner's segment."""
+    K = len(ver_num) - 1
+    owner = [0] * (K + 1)
+    for r, parts in enumerate(shards):
+        for p in parts:
+            owner[p] = r
+    elems = [0] * len(shards)
+    offset = [0] * (K + 1)
+    for p in range(1, K + 1):
+        r = owner[p]
+        offset[p] = elems[r]
+        elems[r] += int(bdy_num[p]) * int(ver_num[p])
+    return owner, elems, max(elems) if elems else 0, offset

@@ -204,6 +204,28 @@ FAP_API int fap_graph_tune_sssp(fap_dgraph *g, const double *deltas, int32_t cou
 /* Mean edge weight of the graph (the scale SSSP bucket widths are tuned in). */
 FAP_API double fap_graph_mean_weight(const fap_dgraph *g);
 
+/* ---- sharded boundary-graph form (parts split over ranks, one process
+ * per GPU; the multi-GPU form of fap/fap_more_task_mpi.cpp:34-80) ----
+ * fap_graph_shard_begin closes this rank's own parts locally (the
+ * boundary-graph form's local closures, in the resident cache's Floyd
+ * arena) and packs their boundary rows into `send` (device memory of the
+ * graph's dtype, send_cap elements): the own parts in ascending order, each
+ * part's rows 0..b-1, columns 0..s-1, row-major; *send_elems receives the
+ * count.  The caller then gathers every rank's send buffer into one device
+ * buffer, rank r's at r * stride (e.g. an NCCL all-gather of buffers padded
+ * to `stride` elements).  fap_graph_shard_finish takes that buffer and
+ * owner[p] (the rank of part p, p = 1..K; index 0 unused), closes the
+ * boundary graph (the same work on every rank), expands the boundary rows of
+ * the own parts and makes their closures exact: the resident cache then
+ * holds the own parts, and fap_solve(g, own parts, FAP_MODE_BATCHED) runs
+ * their min-plus merge (other parts are refused with FAP_ERR_STATE until
+ * the cache is built or dropped again).  Needs the boundary-graph form
+ * (int32 graph without duplicate arcs inside a part) and "floyd_queue". */
+FAP_API int fap_graph_shard_begin(fap_dgraph *g, const int32_t *own_parts, int32_t count, void *send,
+                                  int64_t send_cap, int64_t *send_elems);
+FAP_API int fap_graph_shard_finish(fap_dgraph *g, const void *recv, int32_t world, const int32_t *owner,
+                                   int64_t stride);
+
 /* Frees the output matrix, Floyd arena and scratch of g (the CSR, the
  * partition and the resident cache stay); no block stays resident
  * afterwards. */

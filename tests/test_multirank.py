@@ -90,3 +90,74 @@ def test_failing_rank_does_not_hang_the_other():
     kinds = {r[1]: r[0] for r in res}
     assert kinds[1] == "err"
     assert kinds[0] == "err"   # its collective ends with an error (peer gone / timeout)
+
+
+def _exchange_worker(rank, world, port, vn, bn, out_q):
+    """One gloo rank of the boundary-row exchange: pack its parts' rows at
+    the layout's offsets, all-gather, and read every other rank's parts back
+    the way fap_graph_shard_finish does (owner segment + offset)."""
+    import torch
+    import torch.distributed as dist
+
+    from fastapsp_b200.sharding import shard_layout
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=20))
+    try:
+        shards = shard_parts(vn, bn, 1000, world)
+        owner, elems, stride, offset = shard_layout(vn, bn, shards)
+
+        def block(p):
+            r = np.arange(int(bn[p]))[:, None]
+            c = np.arange(int(vn[p]))[None, :]
+            return (p * 1000000 + r * 1000 + c).astype(np.int32)
+
+        send = np.full(stride, -1, np.int32)
+        pos = 0
+        for p in sorted(shards[rank]):          # the library's packing order
+            assert offset[p] == pos
+            blk = block(p).ravel()
+            send[pos:pos + blk.size] = blk
+            pos += blk.size
+        assert pos == elems[rank]
+        got = [torch.empty(stride, dtype=torch.int32) for _ in range(world)]
+        dist.all_gather(got, torch.from_numpy(send))
+        recv = torch.cat(got).numpy()
+        bad = []
+        for p in range(1, len(vn)):
+            n_el = int(bn[p]) * int(vn[p])
+            seg = recv[owner[p] * stride + offset[p]: owner[p] * stride + offset[p] + n_el]
+            if not np.array_equal(seg.reshape(int(bn[p]), int(vn[p])), block(p)):
+                bad.append(p)
+        out_q.put(("ok", rank, bad, elems, stride))
+    except Exception as e:  # reported to the parent
+        out_q.put(("err", rank, repr(e)))
+    finally:
+        try:
+            dist.destroy_process_group()
+        except Exception:
+            pass
+
+
+def test_boundary_row_exchange_layout_over_two_gloo_ranks():
+    """The sharded boundary-graph form's exchange: every rank packs its own
+    parts' boundary rows (ascending, b x s each) at the offsets of
+    shard_layout, and after an all-gather every rank finds every part's rows
+    at owner * stride + offset."""
+    rng = np.random.default_rng(5)
+    K = 11
+    vn = np.concatenate([[0], rng.integers(20, 40, K)]).astype(np.int64)
+    bn = np.concatenate([[0], rng.integers(0, 6, K)]).astype(np.int64)
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_exchange_worker, args=(r, 2, port, vn, bn, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    res = [q.get(timeout=120) for _ in range(2)]
+    for p in ps:
+        p.join(timeout=60)
+    assert all(r[0] == "ok" for r in res), res
+    assert all(r[2] == [] for r in res), res
+    elems, stride = res[0][3], res[0][4]
+    assert stride == max(elems) and sum(elems) == int((vn * bn).sum())
