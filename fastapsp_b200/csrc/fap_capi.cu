@@ -313,6 +313,11 @@ struct fap_dgraph {
   bool cache_bmethod = false;  // the resident cache was built with it
   int64_t ldB = 0;
   DevBuf d_dB, d_bpart, d_brows, d_FB;
+  // Column table of the staged expansion (launch_bdy_expand): max_b x ldD
+  // values for the prepared part list, when that is at most kColTableBytes
+  // (empty: the expansion gathers from F).
+  DevBuf d_bTc;
+  int bTc_maxb = 0;
   // Large boundary sets: dB closed by Bellman-Ford in alternating local
   // (min-plus with the parts' local closures) and cross steps (the in-arc
   // CSR of the cross-part arcs over boundary indices, built once per
@@ -563,7 +568,7 @@ extern "C" int fap_graph_destroy(fap_dgraph *G) try {
                       &G->d_botro, &G->d_botcol, &G->d_bitw, &G->d_bitems, &G->d_bDt, &G->d_bact, &G->d_bpact,
                       &G->d_bgpart, &G->d_bpcolmap, &G->d_grow, &G->d_pk_off, &G->d_pk_range,
                       &G->d_pk_maxa, &G->d_pk_tiles, &G->q.items, &G->q.cnt, &G->cq.items, &G->cq.cnt,
-                      &G->d_xk_off, &G->d_xk_range, &G->d_xk_maxb, &G->d_xk_tiles})
+                      &G->d_xk_off, &G->d_xk_range, &G->d_xk_maxb, &G->d_xk_tiles, &G->d_bTc})
       b->release();
     if (G->h_changed) cudaFreeHost(G->h_changed);
     for (cudaEvent_t &ev : G->cev)
@@ -748,6 +753,8 @@ namespace {
 constexpr int64_t kBgraphFloydMax = 8192;
 // The staged expansion keeps kExpandRows rows of dB in shared memory.
 constexpr int64_t kBgraphStagedMax = 4096;
+// Largest column table of the staged expansion (max_b x ldD values).
+constexpr size_t kColTableBytes = size_t(256) << 20;
 // Automatic Bellman-Ford closure only while the boundary graph has at most
 // this many edges per edge of the graph (its cliques grow as b_p^2) and dB
 // stays within 64 Ki boundary vertices (17 GB).
@@ -891,6 +898,16 @@ int prepare_bgraph(fap_dgraph *G, const std::vector<PartDesc> &parts) {
     FAP_CK(cudaMemcpy(G->d_grow.p, grow.data(), grow.size() * 8, cudaMemcpyHostToDevice));
   }
   if (bgraph_bf(G)) FAP_TRY(build_bgraph_csr(G));
+  G->bTc_maxb = 0;
+  if (!bgraph_bf(G) && !bgraph_tiled_expand(G)) {
+    int maxb = 0;
+    for (const PartDesc &d : parts) maxb = std::max(maxb, d.b);
+    const size_t bytes = (size_t)maxb * G->ldD * 4;
+    if (maxb > 0 && bytes <= kColTableBytes) {
+      FAP_TRY(G->d_bTc.ensure(bytes));
+      G->bTc_maxb = maxb;
+    }
+  }
   return FAP_OK;
 }
 
@@ -955,7 +972,7 @@ int expand_bgraph(fap_dgraph *G, const PartDesc *dp, int np, int max_s, const T 
                                 G->d_bpart.as<const BPart>(),
                                 G->d_gid.as<const int32_t>(), G->d_ed2st.as<const int32_t>(), G->n,
                                 G->d_dB.as<const T>(), G->ldB, (int)G->total_b, F, Dout, G->ldD, G->d_FB.as<T>(),
-                                ldFB, st, L));
+                                ldFB, G->bTc_maxb > 0 ? G->d_bTc.as<T>() : nullptr, G->bTc_maxb, st, L));
   } else {
     FAP_CK(launch_bdy_expand_tiled<T>(dp, np, max_s, (int)G->total_b, G->d_grow.as<const int64_t>(),
                                       G->d_st2ed.as<const int32_t>(), G->d_dB.as<const T>(), G->ldB, F, Dout,
@@ -2089,6 +2106,8 @@ extern "C" int fap_graph_release(fap_dgraph *G) try {
   G->P.release();
   G->d_dB.release();
   G->d_FB.release();
+  G->d_bTc.release();
+  G->bTc_maxb = 0;
   G->d_pk_off.release();
   G->d_pk_range.release();
   G->d_pk_maxa.release();
@@ -2111,7 +2130,8 @@ extern "C" int fap_graph_device_bytes(const fap_dgraph *G, int64_t *bytes) try {
                           &G->d_rowidx, &G->P, &G->d_tro, &G->d_tcol, &G->d_tw, &G->d_dB,
                           &G->d_bpart, &G->d_brows, &G->d_FB, &G->d_msbf_items, &G->d_msbf_act,
                           &G->d_msbf_changed, &G->d_bitro, &G->d_bitcol, &G->d_botro, &G->d_botcol, &G->d_bitw, &G->d_bitems,
-                          &G->d_bDt, &G->d_bact, &G->d_bpact, &G->d_bgpart, &G->d_bpcolmap, &G->d_grow})
+                          &G->d_bDt, &G->d_bact, &G->d_bpact, &G->d_bgpart, &G->d_bpcolmap, &G->d_grow,
+                          &G->d_bTc})
     t += (int64_t)b->bytes;
   *bytes = t;
   return FAP_OK;
@@ -2618,7 +2638,7 @@ extern "C" int fap_graph_cache_bytes(const fap_dgraph *G, int64_t *bytes, int *b
     *bytes = (int64_t)(G->cBd.bytes + G->cF.bytes + G->d_cparts.bytes);
     if (G->cache_bmethod)  // the boundary graph's buffers stay for rebuilds
       for (const DevBuf *b : {&G->d_dB, &G->d_FB, &G->d_bitro, &G->d_bitcol, &G->d_botro, &G->d_botcol, &G->d_bitw, &G->d_bitems, &G->d_bDt,
-                              &G->d_bact, &G->d_bpact, &G->d_bgpart, &G->d_bpcolmap, &G->d_grow})
+                              &G->d_bact, &G->d_bpact, &G->d_bgpart, &G->d_bpcolmap, &G->d_grow, &G->d_bTc})
         *bytes += (int64_t)b->bytes;
   } else {
     // plus what the build needs while it runs: the SSSP scratch, or the
@@ -2632,6 +2652,9 @@ extern "C" int fap_graph_cache_bytes(const fap_dgraph *G, int64_t *bytes, int *b
                (int64_t)alloc_size((size_t)(G->K + 1) * sizeof(BPart)) +
                (int64_t)alloc_size((size_t)std::max<int64_t>(2 * G->total_b, 2) * 8);
       if (bgraph_tiled_expand(G)) *bytes += (int64_t)alloc_size((size_t)G->total_b * 8);
+      if (!bgraph_bf(G) && !bgraph_tiled_expand(G) && cs.max_b > 0 &&
+          (size_t)cs.max_b * G->ldD * 4 <= kColTableBytes)  // the expansion's column table
+        *bytes += (int64_t)alloc_size((size_t)cs.max_b * G->ldD * 4);
       if (bgraph_bf(G)) {  // cross-arc CSR, work lists, tiles, stamps, part table
         const int64_t xe = std::max<int64_t>(G->bgraph_cross, 1);
         *bytes += 3 * (int64_t)alloc_size((size_t)(G->total_b + 1) * 4) + 3 * (int64_t)alloc_size((size_t)xe * 4) +

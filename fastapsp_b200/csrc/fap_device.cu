@@ -1679,10 +1679,35 @@ cudaError_t launch_bgraph(const PartDesc *parts, int nparts, int max_b, const T 
   return cudaGetLastError();
 }
 
+// Column table of the expansion: Tc[k][v] = F_q[k][j] for the column's part
+// q (local index j) and k < b_q, the sentinel for b_q <= k < maxb, so that
+// the expansion reads a column's boundary entries with coalesced loads (the
+// F arena itself is ordered by part, the output by original vertex id).
+// One read of every part's boundary rows per solve.
+template <typename T>
+__global__ void bdy_coltable_kernel(const BPart *__restrict__ bpart, const int32_t *__restrict__ graph_id,
+                                    const int32_t *__restrict__ ed2st, int n, const T *__restrict__ F, int maxb,
+                                    T *Tc, int64_t ldT) {
+  const T inf = Dist<T>::inf();
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < ldT; v += (int64_t)gridDim.x * blockDim.x) {
+    int qb = 0;
+    const T *Fq = nullptr;
+    int64_t ldq = 0;
+    if (v < n) {
+      const BPart Q = bpart[__ldg(graph_id + v)];
+      qb = Q.b;
+      Fq = F + Q.f_off + (__ldg(ed2st + v) - Q.voff);
+      ldq = Q.ldf;
+    }
+    for (int k = 0; k < maxb; k++) Tc[k * ldT + v] = k < qb ? __ldg(Fq + k * ldq) : inf;
+  }
+}
+
 // grid (column chunks, groups of kExpandRows listed rows); the rows' dB
 // entries sit in shared memory; a thread computes whole output columns
 // (coalesced stores in original column order) from the boundary rows of the
-// column's part, read once for all of the CTA's rows.  Own-part entries are
+// column's part, read once for all of the CTA's rows (from the column table
+// Tc when it is given, else from the F arena).  Own-part entries are
 // also written to FB[g][j] (the exact distances from boundary vertex g to
 // its part's vertices, for the local-closure fix-up).  RG rows per CTA:
 // 32 where their dB entries fit in shared memory (each scattered F load
@@ -1695,9 +1720,14 @@ __global__ void __launch_bounds__(256)
     bdy_expand_kernel(const int64_t *__restrict__ rows, int nrows, const BPart *__restrict__ bpart,
                       const int32_t *__restrict__ graph_id, const int32_t *__restrict__ ed2st, int n,
                       const T *__restrict__ dB, int64_t ldB, int nbB, const T *__restrict__ F, T *D,
-                      int64_t ldD, T *FB, int64_t ldFB) {
-  extern __shared__ unsigned char bx_smem_raw[];
-  T *drow = reinterpret_cast<T *>(bx_smem_raw);  // RG x nbB
+                      int64_t ldD, T *FB, int64_t ldFB, const T *__restrict__ Tc) {
+  extern __shared__ __align__(16) unsigned char bx_smem_raw[];
+  // rows of RG x nbB dB entries, each padded to a multiple of 4 so that they
+  // are staged with 16-byte loads, eight in flight per thread (dB rows start
+  // on 512-byte boundaries and hold ldB >= that many entries)
+  using V = typename Vec4<T>::type;
+  const int nbs = (nbB + 3) & ~3, nvr = nbs / 4;
+  T *drow = reinterpret_cast<T *>(bx_smem_raw);  // RG x nbs
   const int r0 = blockIdx.y * RG;
   const int nr = min(RG, nrows - r0);
   int64_t g[RG], dr[RG];
@@ -1706,29 +1736,49 @@ __global__ void __launch_bounds__(256)
     g[q] = q < nr ? rows[2 * (r0 + q)] : 0;
     dr[q] = q < nr ? rows[2 * (r0 + q) + 1] : 0;
   }
-  for (int t = threadIdx.x; t < nr * nbB; t += blockDim.x) {
-    const int q = t / nbB, k = t % nbB;
-    drow[t] = dB[rows[2 * (r0 + q)] * ldB + k];
+  for (int t0 = threadIdx.x; t0 < nr * nvr; t0 += 8 * blockDim.x) {
+    V tmp[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int t = t0 + u * blockDim.x;
+      if (t < nr * nvr)
+        tmp[u] = __ldg(reinterpret_cast<const V *>(dB + rows[2 * (r0 + t / nvr)] * ldB) + t % nvr);
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int t = t0 + u * blockDim.x;
+      if (t < nr * nvr) reinterpret_cast<V *>(drow)[t] = tmp[u];
+    }
   }
   __syncthreads();
   const T inf = Dist<T>::inf();
-  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < ldD; v += (int64_t)gridDim.x * blockDim.x) {
+  // (the next column's part and local index are loaded while this one's
+  // minima run)
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  int gv = v < n ? __ldg(graph_id + v) : 0, ev = v < n ? __ldg(ed2st + v) : 0;
+  for (; v < ldD; v += stride) {
+    const int64_t vn = v + stride;
+    const int gn = vn < n ? __ldg(graph_id + vn) : 0, en = vn < n ? __ldg(ed2st + vn) : 0;
     T acc[RG];
 #pragma unroll
     for (int q = 0; q < RG; q++) acc[q] = inf;
     int j = -1, qb = 0, qoff = 0;
     if (v < n) {
-      const BPart Q = bpart[__ldg(graph_id + v)];
-      j = __ldg(ed2st + v) - Q.voff;
+      const BPart Q = bpart[gv];
+      j = ev - Q.voff;
       qb = Q.b;
       qoff = Q.boff;
-      const T *Fq = F + Q.f_off + j;
+      const T *Fq = Tc ? Tc + v : F + Q.f_off + j;
+      const int64_t ldq = Tc ? ldD : Q.ldf;
       for (int k = 0; k < Q.b; k++) {
-        const T f = __ldg(Fq + (int64_t)k * Q.ldf);
+        const T f = __ldg(Fq + (int64_t)k * ldq);
 #pragma unroll
-        for (int q = 0; q < RG; q++) acc[q] = Dist<T>::relax(drow[q * nbB + Q.boff + k], f, acc[q]);
+        for (int q = 0; q < RG; q++) acc[q] = Dist<T>::relax(drow[q * nbs + Q.boff + k], f, acc[q]);
       }
     }
+    gv = gn;
+    ev = en;
 #pragma unroll
     for (int q = 0; q < RG; q++) {
       if (q >= nr) break;
@@ -1741,8 +1791,10 @@ __global__ void __launch_bounds__(256)
 template <typename T, int RG>
 cudaError_t launch_bdy_expand_rg(const int64_t *rows, int nrows, const BPart *bpart, const int32_t *graph_id,
                                  const int32_t *ed2st, int n, const T *dB, int64_t ldB, int nbB, const T *F,
-                                 T *D, int64_t ldD, T *FB, int64_t ldFB, cudaStream_t stream, int64_t *launches) {
-  const size_t smem = (size_t)RG * std::max(nbB, 1) * sizeof(T);
+                                 T *D, int64_t ldD, T *FB, int64_t ldFB, const T *Tc, cudaStream_t stream,
+                                 int64_t *launches) {
+  const size_t smem = (size_t)RG * round_up(std::max(nbB, 1), 4) * sizeof(T);
+  if (ldB < round_up(std::max(nbB, 1), 4) || ldB % 4 != 0) return cudaErrorInvalidValue;
   auto kern = bdy_expand_kernel<T, RG>;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -1753,7 +1805,7 @@ cudaError_t launch_bdy_expand_rg(const int64_t *rows, int nrows, const BPart *bp
   const int64_t ny = ceil_div(nrows, RG);
   const int bx = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(ldD, 256), ceil_div((int64_t)device_sm_count() * 16, ny)));
   kern<<<dim3(bx, (unsigned)ny), 256, smem, stream>>>(
-      rows, nrows, bpart, graph_id, ed2st, n, dB, ldB, nbB, F, D, ldD, FB, ldFB);
+      rows, nrows, bpart, graph_id, ed2st, n, dB, ldB, nbB, F, D, ldD, FB, ldFB, Tc);
   *launches += 1;
   return cudaGetLastError();
 }
@@ -1761,13 +1813,21 @@ cudaError_t launch_bdy_expand_rg(const int64_t *rows, int nrows, const BPart *bp
 template <typename T>
 cudaError_t launch_bdy_expand(const int64_t *rows, int nrows, const BPart *bpart, const int32_t *graph_id,
                               const int32_t *ed2st, int n, const T *dB, int64_t ldB, int nbB, const T *F,
-                              T *D, int64_t ldD, T *FB, int64_t ldFB, cudaStream_t stream, int64_t *launches) {
+                              T *D, int64_t ldD, T *FB, int64_t ldFB, T *Tc, int maxb, cudaStream_t stream,
+                              int64_t *launches) {
   if (nrows <= 0) return cudaSuccess;
-  if ((size_t)kExpandRowsWide * std::max(nbB, 1) * sizeof(T) <= 160 * 1024)
+  if (Tc) {
+    const int blocks = (int)std::min<int64_t>(ceil_div(ldD, 256), (int64_t)device_sm_count() * 8);
+    bdy_coltable_kernel<T><<<blocks, 256, 0, stream>>>(bpart, graph_id, ed2st, n, F, maxb, Tc, ldD);
+    *launches += 1;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  if ((size_t)kExpandRowsWide * round_up(std::max(nbB, 1), 4) * sizeof(T) <= 160 * 1024)
     return launch_bdy_expand_rg<T, kExpandRowsWide>(rows, nrows, bpart, graph_id, ed2st, n, dB, ldB, nbB, F, D,
-                                                     ldD, FB, ldFB, stream, launches);
+                                                     ldD, FB, ldFB, Tc, stream, launches);
   return launch_bdy_expand_rg<T, kExpandRows>(rows, nrows, bpart, graph_id, ed2st, n, dB, ldB, nbB, F, D, ldD,
-                                              FB, ldFB, stream, launches);
+                                              FB, ldFB, Tc, stream, launches);
 }
 
 // Boundary graph closed by Bellman-Ford in alternating steps (large
@@ -2813,8 +2873,8 @@ cudaError_t launch_relax_peak(T *sink, int blocks, int iters, cudaStream_t strea
                                         cudaStream_t, int64_t *);                                  \
   template cudaError_t launch_bdy_expand<T>(const int64_t *, int, const BPart *, const int32_t *,  \
                                             const int32_t *, int, const T *, int64_t, int,         \
-                                            const T *, T *, int64_t, T *, int64_t, cudaStream_t,   \
-                                            int64_t *);                                            \
+                                            const T *, T *, int64_t, T *, int64_t, T *, int,       \
+                                            cudaStream_t, int64_t *);                              \
   template cudaError_t launch_local_fixup<T>(const PartDesc *, int, int, T *, const T *, int64_t,  \
                                              cudaStream_t, int64_t *);                             \
   template cudaError_t launch_bgraph_bf<T>(const PartDesc *, int, int, const T *, const int32_t *,  \

@@ -266,10 +266,15 @@ cudaError_t launch_bgraph(const PartDesc *parts, int nparts, int max_b, const T 
 //     exact closure (inner rows: min over leaving through a boundary vertex;
 //     boundary rows: FB), so that the min-plus merge and its decode run as in
 //     the SSSP form.
+//     With Tc (maxb x ldD values, may be null) the launch first writes the
+//     column table Tc[k][v] = F_q[k][j(v)] (k < b_q, the sentinel up to
+//     maxb, maxb >= every b_q), so that the expansion reads it with
+//     coalesced loads instead of gathering from F.
 template <typename T>
 cudaError_t launch_bdy_expand(const int64_t *rows, int nrows, const BPart *bpart, const int32_t *graph_id,
                               const int32_t *ed2st, int n, const T *dB, int64_t ldB, int nbB, const T *F,
-                              T *D, int64_t ldD, T *FB, int64_t ldFB, cudaStream_t stream, int64_t *launches);
+                              T *D, int64_t ldD, T *FB, int64_t ldFB, T *Tc, int maxb, cudaStream_t stream,
+                              int64_t *launches);
 // Boundary graph closed by Bellman-Ford (large boundary sets), ztiles tiles
 // of kMsbfS sources side by side, alternating a local step (per part whose
 // rows changed: min-plus of the tile's rows with the part's local closure
