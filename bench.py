@@ -79,6 +79,8 @@ def parse_args():
     ap.add_argument("--extra", default=",".join(EXTRA_WORKLOADS),
                     help="further workloads timed after the headline one (comma list, '' for none)")
     ap.add_argument("--extra-steps", type=int, default=2)
+    ap.add_argument("--extra-plain-steps", type=int, default=1,
+                    help="plain-form steps (one launch sequence per part) timed for each further workload")
     ap.add_argument("--extra-warmup", type=int, default=3)
     ap.add_argument("--extra-parity-parts", type=int, default=2,
                     help="parts of each further workload checked against the reference binary")
@@ -672,7 +674,7 @@ def run_extra(args, job, ctx, relax_peak, hbm_peak, peak_kind):
     reference binary under the same partition (started by start_extra)."""
     import torch
 
-    from fastapsp_b200 import FAP_MODE_BATCHED, DeviceGraph, autotune
+    from fastapsp_b200 import FAP_MODE_BATCHED, FAP_MODE_PLAIN, DeviceGraph, autotune
     from fastapsp_b200.sharding import group_parts_by_rows, rows_of
     wl = job["wl"]
     name = wl.name
@@ -752,6 +754,20 @@ def run_extra(args, job, ctx, relax_peak, hbm_peak, peak_kind):
         mp_ms.append(mp)
         fl_ms.append(fl)
     dg.check()
+    # the plain form of the same job: one launch sequence per part (stage 1
+    # by SSSP from that part's boundary vertices), the groups as above
+    plain_ms = []
+    for _ in range(max(0, args.extra_plain_steps)):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for grp in groups:
+            dg.solve(grp, FAP_MODE_PLAIN, check_errors=False)
+        e1.record(stream)
+        e1.synchronize()
+        plain_ms.append(e0.elapsed_time(e1))
+    dg.check()
     del flush
     ms_step = float(np.mean(ms))
     mp_step = float(np.mean(mp_ms))
@@ -798,8 +814,13 @@ def run_extra(args, job, ctx, relax_peak, hbm_peak, peak_kind):
                     "note": mp_note},
         "parity": None,
     }
+    if plain_ms:
+        pm = float(np.mean(plain_ms))
+        out["plain"] = {"value": all_rows * n / (pm * 1e-3), "ms_per_step": pm, "steps": len(plain_ms)}
+        out["batched_over_plain"] = pm / ms_step
     log(f"{name}: {ms_step:.1f} ms/step, {out['value']:.4g} entries/s, min-plus {mp_step:.1f} ms "
-        f"({out['minplus']['frac_of_relax_peak']:.2f} of the relaxation peak)")
+        f"({out['minplus']['frac_of_relax_peak']:.2f} of the relaxation peak)"
+        + (f"; plain {float(np.mean(plain_ms)):.1f} ms/step" if plain_ms else ""))
     return out, gpu, dtype
 
 
