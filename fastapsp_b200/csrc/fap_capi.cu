@@ -314,8 +314,9 @@ struct fap_dgraph {
   int64_t ldB = 0;
   DevBuf d_dB, d_bpart, d_brows, d_FB;
   // Column table of the staged expansion (launch_bdy_expand): max_b x ldD
-  // values for the prepared part list, when that is at most kColTableBytes
-  // (empty: the expansion gathers from F).
+  // values for a prepared batch of all parts, when that is at most
+  // kColTableBytes (resident-cache builds and larger tables: the expansion
+  // gathers from F, so that a server's resident graphs hold no table).
   DevBuf d_bTc;
   int bTc_maxb = 0;
   // Large boundary sets: dB closed by Bellman-Ford in alternating local
@@ -864,7 +865,7 @@ int build_bgraph_csr(fap_dgraph *G) {
 
 // Per-part table, output-row list and dB for a batch of all parts in the
 // boundary-graph form (descriptors built, F offsets final).
-int prepare_bgraph(fap_dgraph *G, const std::vector<PartDesc> &parts) {
+int prepare_bgraph(fap_dgraph *G, const std::vector<PartDesc> &parts, bool col_table = false) {
   const int32_t K = G->K;
   std::vector<BPart> bp((size_t)K + 1);
   std::vector<int64_t> rows;
@@ -899,7 +900,7 @@ int prepare_bgraph(fap_dgraph *G, const std::vector<PartDesc> &parts) {
   }
   if (bgraph_bf(G)) FAP_TRY(build_bgraph_csr(G));
   G->bTc_maxb = 0;
-  if (!bgraph_bf(G) && !bgraph_tiled_expand(G)) {
+  if (col_table && !bgraph_bf(G) && !bgraph_tiled_expand(G)) {
     int maxb = 0;
     for (const PartDesc &d : parts) maxb = std::max(maxb, d.b);
     const size_t bytes = (size_t)maxb * G->ldD * 4;
@@ -1100,7 +1101,7 @@ int prepare_batch(fap_dgraph *G, const std::vector<int32_t> &ids, bool cached, b
   FAP_CK(cudaStreamSynchronize(st));
   if (!qitems.empty())
     FAP_CK(cudaMemcpy(G->q.items.p, qitems.data(), qitems.size() * sizeof(QItem), cudaMemcpyHostToDevice));
-  if (bmethod) FAP_TRY(prepare_bgraph(G, G->parts));
+  if (bmethod) FAP_TRY(prepare_bgraph(G, G->parts, true));
   FAP_CK(cudaMemcpy(G->d_parts.p, G->parts.data(), G->parts.size() * sizeof(PartDesc), cudaMemcpyHostToDevice));
   if (!G->work.empty())
     FAP_CK(cudaMemcpy(G->d_work.p, G->work.data(), G->work.size() * sizeof(MPWork), cudaMemcpyHostToDevice));
@@ -2638,7 +2639,7 @@ extern "C" int fap_graph_cache_bytes(const fap_dgraph *G, int64_t *bytes, int *b
     *bytes = (int64_t)(G->cBd.bytes + G->cF.bytes + G->d_cparts.bytes);
     if (G->cache_bmethod)  // the boundary graph's buffers stay for rebuilds
       for (const DevBuf *b : {&G->d_dB, &G->d_FB, &G->d_bitro, &G->d_bitcol, &G->d_botro, &G->d_botcol, &G->d_bitw, &G->d_bitems, &G->d_bDt,
-                              &G->d_bact, &G->d_bpact, &G->d_bgpart, &G->d_bpcolmap, &G->d_grow, &G->d_bTc})
+                              &G->d_bact, &G->d_bpact, &G->d_bgpart, &G->d_bpcolmap, &G->d_grow})
         *bytes += (int64_t)b->bytes;
   } else {
     // plus what the build needs while it runs: the SSSP scratch, or the
@@ -2652,9 +2653,6 @@ extern "C" int fap_graph_cache_bytes(const fap_dgraph *G, int64_t *bytes, int *b
                (int64_t)alloc_size((size_t)(G->K + 1) * sizeof(BPart)) +
                (int64_t)alloc_size((size_t)std::max<int64_t>(2 * G->total_b, 2) * 8);
       if (bgraph_tiled_expand(G)) *bytes += (int64_t)alloc_size((size_t)G->total_b * 8);
-      if (!bgraph_bf(G) && !bgraph_tiled_expand(G) && cs.max_b > 0 &&
-          (size_t)cs.max_b * G->ldD * 4 <= kColTableBytes)  // the expansion's column table
-        *bytes += (int64_t)alloc_size((size_t)cs.max_b * G->ldD * 4);
       if (bgraph_bf(G)) {  // cross-arc CSR, work lists, tiles, stamps, part table
         const int64_t xe = std::max<int64_t>(G->bgraph_cross, 1);
         *bytes += 3 * (int64_t)alloc_size((size_t)(G->total_b + 1) * 4) + 3 * (int64_t)alloc_size((size_t)xe * 4) +
