@@ -1148,8 +1148,11 @@ def main_fap(args):
     if args.e2e_steps > 0 and world == 1 and len(groups) > 1:
         log("e2e with grouped output")
     max_rows = int(max(vn[p] for p in mine))
-    host_buf = torch.empty((max_rows, n), dtype=torch.float32, pin_memory=True)
-    hb = host_buf.numpy()
+    # two pinned host buffers: each block's copy is queued on one of the
+    # library's two copy slots, so that the next block's conversion to
+    # float32 overlaps this block's device-to-host copy
+    host_bufs = [torch.empty((max_rows, n), dtype=torch.float32, pin_memory=True) for _ in range(2)]
+    hbs = [b.numpy() for b in host_bufs]
     pin = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory().numpy()
            for k, v in dict(ro=ro, col=col, w=w.astype(np.float32), gid=gid, st2ed=st2ed,
                             vn=vn, vo=vo, bn=bn).items()}
@@ -1170,10 +1173,14 @@ def main_fap(args):
             g2.shard_begin(mine, send_.data_ptr(), stride_)
             dist.all_gather_into_tensor(recv_, send_)
             g2.shard_finish(recv_.data_ptr(), world, owner_, stride_)
+        k = 0
         for grp in groups:
             g2.solve(grp, FAP_MODE_BATCHED)
             for p in grp:
-                g2.copy_block(p, out_dtype=FAP_DTYPE_F32, out=hb[:int(vn[p])])
+                g2.copy_block_async(p, hbs[k % 2][:int(vn[p])], k % 2, out_dtype=FAP_DTYPE_F32)
+                k += 1
+            for slot in range(2):   # the group's blocks are out before its rows are reused
+                g2.copy_wait(slot)
         t1 = time.perf_counter()
         del g2
         if i > 0:
@@ -1185,7 +1192,7 @@ def main_fap(args):
     # ---- serving stream (rank 0, N=1 only) ----
     serving = None
     if rank == 0 and world == 1 and not args.no_serve:
-        del host_buf, hb
+        del host_bufs, hbs
         torch.cuda.empty_cache()
         serving = run_serving(args, local)
 

@@ -76,6 +76,8 @@ _SIGS = {
     "fap_graph_check": (INT, [P]),
     "fap_graph_block": (INT, [P, I32, PP, ctypes.POINTER(I64), ctypes.POINTER(I64)]),
     "fap_graph_copy_block": (INT, [P, I32, P, INT]),
+    "fap_graph_copy_block_async": (INT, [P, I32, P, INT, I32]),
+    "fap_graph_copy_wait": (INT, [P, I32]),
     "fap_graph_block_checksums": (INT, [P, I32, P]),
     "fap_graph_path_block": (INT, [P, I32, PP, ctypes.POINTER(I64), ctypes.POINTER(I64)]),
     "fap_graph_copy_path_block": (INT, [P, I32, P]),

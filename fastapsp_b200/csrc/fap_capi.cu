@@ -239,6 +239,17 @@ struct fap_dgraph {
   std::vector<int64_t> row_base;  // per part (1..K), -1 = not resident
   // batch state
   DevBuf F, d_parts, d_work, d_src, d_srcrows, d_status, d_checks, staging;
+  // Asynchronous block copies (fap_graph_copy_block_async): per slot a
+  // float32 staging buffer, the stream its device-to-host copy runs on and
+  // the events that order it (conversion done on the context stream, copy
+  // done), so that the next block's conversion overlaps this one's copy.
+  struct CopySlot {
+    DevBuf staging;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t converted = nullptr, done = nullptr;
+    bool busy = false;
+  };
+  CopySlot cslot[FAP_COPY_SLOTS];
   std::vector<PartDesc> parts;
   std::vector<MPWork> work;
   std::vector<int32_t> src;
@@ -572,6 +583,13 @@ extern "C" int fap_graph_destroy(fap_dgraph *G) try {
                       &G->d_xk_off, &G->d_xk_range, &G->d_xk_maxb, &G->d_xk_tiles, &G->d_bTc})
       b->release();
     if (G->h_changed) cudaFreeHost(G->h_changed);
+    for (auto &cs : G->cslot) {
+      if (cs.stream) cudaStreamSynchronize(cs.stream);
+      cs.staging.release();
+      if (cs.converted) cudaEventDestroy(cs.converted);
+      if (cs.done) cudaEventDestroy(cs.done);
+      if (cs.stream) cudaStreamDestroy(cs.stream);
+    }
     for (cudaEvent_t &ev : G->cev)
       if (ev) cudaEventDestroy(ev);
     cache_drop(G);
@@ -655,23 +673,37 @@ extern "C" int fap_graph_set_parts(fap_dgraph *G, int32_t K, const int32_t *grap
       }
   }
   {
-    // symmetric parts: sort the intra-part arcs and look each reverse up
+    // symmetric parts: the intra-part arcs of every row sorted by head, and
+    // each arc's reverse looked up in its head's row (no two intra-part arcs
+    // join the same ordered pair, so the reverse is unique)
     G->sym_local = false;
     if (G->bnd_dupfree) {
-      std::vector<std::pair<uint64_t, uint32_t>> arcs;
-      for (int32_t u = 0; u < n; u++)
+      std::vector<int64_t> sro((size_t)n + 1, 0);
+      for (int32_t u = 0; u < n; u++) {
+        int64_t c = 0;
         for (int32_t e = G->h_ro[u]; e < G->h_ro[u + 1]; e++) {
           const int32_t v = G->h_col[e];
-          if (graph_id[v] == graph_id[u] && v != u)
-            arcs.emplace_back(((uint64_t)(uint32_t)u << 32) | (uint32_t)v, G->h_w[e]);
+          c += graph_id[v] == graph_id[u] && v != u;
         }
-      std::sort(arcs.begin(), arcs.end());
-      bool sym = true;
-      for (size_t i = 0; i < arcs.size() && sym; i++) {
-        const uint64_t rev = (arcs[i].first << 32) | (arcs[i].first >> 32);
-        const auto it = std::lower_bound(arcs.begin(), arcs.end(), std::make_pair(rev, (uint32_t)0));
-        sym = it != arcs.end() && it->first == rev && it->second == arcs[i].second;
+        sro[u + 1] = sro[u] + c;
       }
+      std::vector<std::pair<int32_t, uint32_t>> arcs((size_t)sro[n]);
+      for (int32_t u = 0; u < n; u++) {
+        int64_t pos = sro[u];
+        for (int32_t e = G->h_ro[u]; e < G->h_ro[u + 1]; e++) {
+          const int32_t v = G->h_col[e];
+          if (graph_id[v] == graph_id[u] && v != u) arcs[(size_t)pos++] = {v, G->h_w[e]};
+        }
+        std::sort(arcs.begin() + sro[u], arcs.begin() + sro[u + 1]);
+      }
+      bool sym = true;
+      for (int32_t u = 0; u < n && sym; u++)
+        for (int64_t i = sro[u]; i < sro[u + 1] && sym; i++) {
+          const int32_t v = arcs[(size_t)i].first;
+          const auto b = arcs.begin() + sro[v], e = arcs.begin() + sro[v + 1];
+          const auto it = std::lower_bound(b, e, std::make_pair(u, (uint32_t)0));
+          sym = it != e && it->first == u && it->second == arcs[(size_t)i].second;
+        }
       G->sym_local = sym;
     }
   }
@@ -1557,6 +1589,71 @@ extern "C" int fap_graph_copy_block(fap_dgraph *G, int32_t part, void *host, int
   return fail_exception();
 }
 
+extern "C" int fap_graph_copy_block_async(fap_dgraph *G, int32_t part, void *host, int out_dtype,
+                                          int32_t slot) try {
+  if (!G || !host) return fail(FAP_ERR_INVALID, "NULL argument");
+  if (slot < 0 || slot >= FAP_COPY_SLOTS) return fail(FAP_ERR_INVALID, "slot %d outside 0..%d", slot, FAP_COPY_SLOTS - 1);
+  if (out_dtype != G->dtype && !(G->dtype == FAP_DTYPE_I32 && out_dtype == FAP_DTYPE_F32))
+    return fail(FAP_ERR_INVALID, "cannot copy %s distances as int32", G->dtype == FAP_DTYPE_F32 ? "float" : "?");
+  void *dp;
+  int64_t rows, ld;
+  FAP_TRY(fap_graph_block(G, part, &dp, &rows, &ld));
+  DeviceGuard g(G->ctx->device);
+  cudaStream_t st = G->ctx->stream;
+  const int64_t n = G->n;
+  auto &cs = G->cslot[slot];
+  // the slot's previous copy has finished reading its staging buffer and
+  // writing its host memory
+  if (cs.busy) FAP_CK(cudaEventSynchronize(cs.done));
+  cs.busy = false;
+  if (rows == 0) return FAP_OK;
+  if (out_dtype == G->dtype) {
+    // no conversion: the copy reads the block itself, so it runs on the
+    // context stream, in order with the solves that may reuse the rows
+    FAP_CK(cudaMemcpy2DAsync(host, (size_t)n * 4, dp, (size_t)ld * 4, (size_t)n * 4, (size_t)rows,
+                             cudaMemcpyDeviceToHost, st));
+    if (!cs.done) FAP_CK(cudaEventCreateWithFlags(&cs.done, cudaEventDisableTiming));
+    FAP_CK(cudaEventRecord(cs.done, st));
+    cs.busy = true;
+    return FAP_OK;
+  }
+  if (!cs.stream) FAP_CK(cudaStreamCreateWithFlags(&cs.stream, cudaStreamNonBlocking));
+  if (!cs.converted) FAP_CK(cudaEventCreateWithFlags(&cs.converted, cudaEventDisableTiming));
+  if (!cs.done) FAP_CK(cudaEventCreateWithFlags(&cs.done, cudaEventDisableTiming));
+  // (sized once for the largest part: growing it would free the buffer,
+  // and a cudaFree waits for the other slot's copy)
+  if (cs.staging.bytes < (size_t)rows * n * 4) {
+    int32_t most = 0;
+    for (int32_t q = 1; q <= G->K; q++) most = std::max(most, G->vnum[q]);
+    FAP_TRY(cs.staging.ensure((size_t)std::max<int64_t>(most, rows) * n * 4));
+  }
+  int64_t L = 0;
+  // the conversion on the context stream (after the solve that made the
+  // block), the copy of the converted rows on the slot's stream
+  FAP_CK(launch_i32_to_f32(reinterpret_cast<const int32_t *>(dp), rows, n, ld, cs.staging.as<float>(), st, &L));
+  FAP_CK(cudaEventRecord(cs.converted, st));
+  FAP_CK(cudaStreamWaitEvent(cs.stream, cs.converted, 0));
+  FAP_CK(cudaMemcpyAsync(host, cs.staging.p, (size_t)rows * n * 4, cudaMemcpyDeviceToHost, cs.stream));
+  FAP_CK(cudaEventRecord(cs.done, cs.stream));
+  cs.busy = true;
+  return FAP_OK;
+} catch (...) {
+  return fail_exception();
+}
+
+extern "C" int fap_graph_copy_wait(fap_dgraph *G, int32_t slot) try {
+  if (!G) return fail(FAP_ERR_INVALID, "NULL graph");
+  if (slot < 0 || slot >= FAP_COPY_SLOTS) return fail(FAP_ERR_INVALID, "slot %d outside 0..%d", slot, FAP_COPY_SLOTS - 1);
+  DeviceGuard g(G->ctx->device);
+  auto &cs = G->cslot[slot];
+  if (cs.busy) FAP_CK(cudaEventSynchronize(cs.done));
+  cs.busy = false;
+  FAP_TRY(read_status(G));
+  return FAP_OK;
+} catch (...) {
+  return fail_exception();
+}
+
 extern "C" int fap_graph_path_block(fap_dgraph *G, int32_t part, void **dev_ptr, int64_t *rows,
                                     int64_t *ld) try {
   if (!G || !dev_ptr || !rows || !ld) return fail(FAP_ERR_INVALID, "NULL argument");
@@ -2112,6 +2209,11 @@ extern "C" int fap_graph_release(fap_dgraph *G) try {
   G->d_pk_off.release();
   G->d_pk_range.release();
   G->d_pk_maxa.release();
+  for (auto &cs : G->cslot) {
+    if (cs.stream) FAP_CK(cudaStreamSynchronize(cs.stream));
+    cs.busy = false;
+    cs.staging.release();
+  }
   G->max_rows = 0;
   std::fill(G->row_base.begin(), G->row_base.end(), -1);
   G->last_ids.clear();

@@ -441,6 +441,22 @@ class DeviceGraph:
               "fap_graph_copy_block")
         return out
 
+    def copy_block_async(self, part: int, out, slot: int, out_dtype: Optional[int] = None) -> None:
+        """Queues the copy of part's block into `out` (rows x n, contiguous;
+        pinned for the full rate) on copy slot 0 or 1 without waiting for
+        it; `out` must stay alive until copy_wait(slot) or the slot's next
+        copy (fap_graph_copy_block_async)."""
+        dt = self.dtype if out_dtype is None else out_dtype
+        _, rows, _ = self.block_info(part)
+        want = np.int32 if dt == L.FAP_DTYPE_I32 else np.float32
+        if out.dtype != want or out.shape != (rows, self.n) or not out.flags.c_contiguous:
+            raise ValueError(f"out must be a contiguous {rows} x {self.n} {np.dtype(want).name} array")
+        check(lib().fap_graph_copy_block_async(self._h, int(part), ptr(out), int(dt), int(slot)),
+              "fap_graph_copy_block_async")
+
+    def copy_wait(self, slot: int) -> None:
+        check(lib().fap_graph_copy_wait(self._h, int(slot)), "fap_graph_copy_wait")
+
     def copy_path_block(self, part: int) -> np.ndarray:
         """rows x n int32 predecessors of a part solved with set_param("paths", 1)."""
         _, rows, _ = self.block_info(part)

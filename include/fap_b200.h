@@ -129,6 +129,23 @@ FAP_API int fap_graph_block(fap_dgraph *g, int32_t part, void **dev_ptr, int64_t
  * the int32 path).  Synchronous. */
 FAP_API int fap_graph_copy_block(fap_dgraph *g, int32_t part, void *host, int out_dtype);
 
+/* The same copy queued without waiting for it (no counterpart in the
+ * reference: its getters return host matrices).  slot (0 or 1) names one of
+ * two copies in flight: from int32 to FAP_DTYPE_F32 the conversion runs on
+ * the context stream into the slot's own staging buffer and the
+ * device-to-host copy on the slot's stream, so that the next block's
+ * conversion overlaps this block's copy.  A call on a slot first waits for
+ * that slot's previous copy, which frees its host memory for reuse; the
+ * staging buffer of a slot is allocated on its first use (cudaMalloc).
+ * `host` must stay valid until fap_graph_copy_wait(slot) or the slot's next
+ * call returns, and pinned host memory gives the full copy rate.  A copy
+ * without conversion runs on the context stream. */
+FAP_API int fap_graph_copy_block_async(fap_dgraph *g, int32_t part, void *host, int out_dtype, int32_t slot);
+/* Waits for the slot's copy; then FAP_OK or the device-side error of the
+ * last solve. */
+FAP_API int fap_graph_copy_wait(fap_dgraph *g, int32_t slot);
+#define FAP_COPY_SLOTS 2
+
 /* Per-row checksums of part p's block (int32 path only):
  * sum_j uint32(d[r][j]) * (2j+1) mod 2^64, j < n.  host_out[rows]. */
 FAP_API int fap_graph_block_checksums(fap_dgraph *g, int32_t part, uint64_t *host_out);

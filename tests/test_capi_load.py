@@ -105,6 +105,8 @@ def test_entry_points_refuse_null_handles_without_a_gpu():
         lambda: lib.fap_graph_last_launches(None, None),
         lambda: lib.fap_graph_block(None, 1, None, None, None),
         lambda: lib.fap_graph_copy_block(None, 1, None, 0),
+        lambda: lib.fap_graph_copy_block_async(None, 1, None, 0, 0),
+        lambda: lib.fap_graph_copy_wait(None, 0),
         lambda: lib.fap_graph_path_block(None, 1, None, None, None),
         lambda: lib.fap_graph_copy_path_block(None, 1, None),
         lambda: lib.fap_graph_block_checksums(None, 1, None),

@@ -431,3 +431,31 @@ def test_legacy_abi_blocked_floyd_entry_points(cuda_ok):
 def test_relax_peak_is_positive(cuda_ok):
     ctx = Context(0)
     assert ctx.relax_peak(FAP_DTYPE_I32) > 1e12
+
+
+@pytest.mark.parametrize("name", ["grid64_k8", "rmat8_f32_k4", "road300_k6"])
+def test_async_block_copies_equal_the_synchronous_ones(cuda_ok, name):
+    """fap_graph_copy_block_async on the two copy slots (float32 output, and
+    the graph's own dtype without conversion) gives the bytes
+    fap_graph_copy_block gives; a slot reused waits for its previous copy."""
+    case = load_golden(name)
+    K = int(case["K"])
+    ctx = Context(0)
+    ro, col, w = case["row_offset"], case["col_val"], case["weight"]
+    dg = DeviceGraph(ctx, ro, col[:ro[-1]], w[:ro[-1]])
+    dg.set_parts(K, case["graph_id"], case["st2ed"], case["ver_num"], case["ver_offset"], case["bdy_num"])
+    dg.solve(mode=FAP_MODE_BATCHED)
+    dg.check()
+    vn, n = case["ver_num"], int(case["n"])
+    for dt in sorted({FAP_DTYPE_F32, dg.dtype}):
+        want = {p: dg.copy_block(p, out_dtype=dt) for p in range(1, K + 1)}
+        npdt = np.float32 if dt == FAP_DTYPE_F32 else np.int32
+        outs = {p: np.full((int(vn[p]), n), -7, npdt) for p in range(1, K + 1)}
+        for k, p in enumerate(range(1, K + 1)):
+            dg.copy_block_async(p, outs[p], k % 2, out_dtype=dt)
+        dg.copy_wait(0)
+        dg.copy_wait(1)
+        for p in range(1, K + 1):
+            assert np.array_equal(outs[p].view(np.int32), want[p].view(np.int32)), (dt, p)
+    with pytest.raises(FapError):  # (the last loop's buffers are float32)
+        dg.copy_block_async(1, outs[1], 2, out_dtype=FAP_DTYPE_F32)
