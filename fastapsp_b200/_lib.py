@@ -134,6 +134,7 @@ _SIGS = {
     "fap_host_destroy": (INT, [P]),
     "fap_host_set_partition": (INT, [P, P]),
     "fap_host_set_options": (INT, [P, INT, INT, INT]),
+    "fap_host_set_max_resident_rows": (INT, [P, I64]),
     "fap_host_precondition": (INT, [P]),
     "fap_host_is_split": (INT, [P]),
     "fap_host_dtype": (INT, [P]),

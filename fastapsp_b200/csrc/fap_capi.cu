@@ -235,6 +235,7 @@ struct fap_dgraph {
   // output
   int64_t ldD = 0;
   int64_t max_rows = 0;
+  int64_t row_limit = 0;  // "max_resident_rows": bound on max_rows, 0 = none
   DevBuf D;
   std::vector<int64_t> row_base;  // per part (1..K), -1 = not resident
   // batch state
@@ -754,7 +755,11 @@ extern "C" int fap_graph_set_parts(fap_dgraph *G, int32_t K, const int32_t *grap
 
 extern "C" int fap_graph_reserve(fap_dgraph *G, int64_t max_rows) try {
   if (!G) return fail(FAP_ERR_INVALID, "NULL graph");
+  if (G->row_limit > 0 && max_rows > G->row_limit)
+    return fail(FAP_ERR_NOMEM, "%lld rows asked, at most %lld may be resident (\"max_resident_rows\")",
+                (long long)max_rows, (long long)G->row_limit);
   if (max_rows <= 0 || max_rows > G->n) max_rows = G->n;
+  if (G->row_limit > 0) max_rows = std::min(max_rows, G->row_limit);
   DeviceGuard g(G->ctx->device);
   cudaStreamSynchronize(G->ctx->stream);
   const size_t bytes = (size_t)max_rows * (size_t)G->ldD * 4;
@@ -2073,6 +2078,12 @@ extern "C" int fap_graph_set_param(fap_dgraph *G, const char *key, double value)
   }
   if (std::strcmp(key, "sssp_max_rounds") == 0) {
     G->sssp_max_rounds = value >= 1 ? (int64_t)value : -1;
+    return FAP_OK;
+  }
+  if (std::strcmp(key, "max_resident_rows") == 0) {
+    G->row_limit = value >= 1 ? (int64_t)value : 0;
+    // Blocks reserved beyond the new bound are given back at once.
+    if (G->row_limit > 0 && G->max_rows > G->row_limit) return fap_graph_release(G);
     return FAP_OK;
   }
   return fail(FAP_ERR_INVALID, "unknown parameter '%s'", key);

@@ -372,6 +372,10 @@ fapGraph::fapGraph(LoadedTag, int32_t n, int64_t m, std::vector<int32_t> ro, std
 void fapGraph::setDevice(int device) { device_ = device; }
 void fapGraph::setDtype(int dtype) { dtype_ = dtype; }
 void fapGraph::setMode(SolveMode mode) { mode_ = mode; }
+void fapGraph::setMaxResidentRows(int64_t rows) {
+  row_limit_ = std::max<int64_t>(rows, 0);
+  if (dg_) check(fap_graph_set_param(dg_, "max_resident_rows", (double)row_limit_), "max_resident_rows");
+}
 
 int fapGraph::getDtype() {
   ensure_device();
@@ -418,6 +422,7 @@ void fapGraph::preCondition() {
   }
   is_split = (num_vertexs > max_vertexs_num_limit);
   prepared_ = true;
+  cache_tried_ = false;
   if (dg_) {
     check(fap_graph_set_parts(dg_, K, graph_id.data(), st2ed.data(), C_BlockVer_num.data(),
                               C_BlockVer_offset.data(), C_BlockBdy_num.data()),
@@ -441,12 +446,61 @@ void fapGraph::ensure_device() {
       check(fap_graph_set_parts(dg_, K, graph_id.data(), st2ed.data(), C_BlockVer_num.data(),
                                 C_BlockVer_offset.data(), C_BlockBdy_num.data()),
             "fap_graph_set_parts");
+    if (row_limit_ > 0)
+      check(fap_graph_set_param(dg_, "max_resident_rows", (double)row_limit_), "max_resident_rows");
   }
 }
 
 void fapGraph::run_parts(const std::vector<int32_t> &ids) {
   check(fap_solve(dg_, ids.data(), (int32_t)ids.size(), static_cast<int>(mode_)), "fap_solve");
   check(fap_graph_check(dg_), "fap_graph_check");
+}
+
+// Output rows for solving the parts in groups, when the device holds fewer
+// than n of them: as many as setMaxResidentRows allows, else room for
+// `need` rows (the largest part to be solved; fewer allowed rows than that
+// raise FAP_ERR_NOMEM).  In
+// the batched form every part's stage-1 rows and local closure are also
+// kept resident once, when they fit (fap_graph_cache_build), so that each
+// group runs only its parts' min-plus merge; without room for them each
+// group runs its own stage 1.
+int64_t fapGraph::reserve_group_rows(int64_t need) {
+  need = std::max<int64_t>(need, 1);
+  int64_t rows = need;
+  if (row_limit_ >= need && fap_graph_reserve(dg_, row_limit_) == FAP_OK) {
+    rows = row_limit_;
+  } else {
+    check(fap_graph_reserve(dg_, need), "fap_graph_reserve");
+  }
+  if (mode_ == SolveMode::Batched && !cache_tried_) {
+    cache_tried_ = true;
+    (void)fap_graph_cache_build(dg_);  // FAP_ERR_NOMEM: groups run stage 1 themselves
+  }
+  return rows;
+}
+
+// Solves every part into all n output rows, reserving them again when an
+// earlier grouped solve left fewer; FAP_ERR_NOMEM when they do not fit.
+int fapGraph::solve_all(int mode) {
+  std::vector<int32_t> all;
+  for (int32_t p = 1; p <= K; p++) all.push_back(p);
+  int rc = fap_solve(dg_, all.data(), K, mode);
+  if (rc == FAP_ERR_NOMEM && fap_graph_reserve(dg_, 0) == FAP_OK) rc = fap_solve(dg_, all.data(), K, mode);
+  return rc;
+}
+
+// Solves parts first, first + 1, ... while their rows fit in `rows`; returns
+// the first part not solved.
+int32_t fapGraph::run_group(int32_t first, int64_t rows) {
+  std::vector<int32_t> ids;
+  int64_t used = 0;
+  for (int32_t p = first; p <= K; p++) {
+    if (!ids.empty() && used + C_BlockVer_num[p] > rows) break;
+    ids.push_back(p);
+    used += C_BlockVer_num[p];
+  }
+  run_parts(ids);
+  return first + (int32_t)ids.size();
 }
 
 void fapGraph::copy_block(int32_t id, float *dst) {
@@ -470,12 +524,25 @@ int32_t fapGraph::solve(bool path_needed) {
   dist.assign((size_t)(n * n), 0.0f);
   path.assign((size_t)(n * n), -1);
   path_ready_ = false;
-  std::vector<int32_t> all;
-  for (int32_t p = 1; p <= K; p++) all.push_back(p);
-  run_parts(all);
-  for (int32_t p = 1; p <= K; p++) {
-    copy_block(p, dist.data() + (size_t)C_BlockVer_offset[p] * n);
-    if (path_needed) copy_path_block(p, path.data() + (size_t)C_BlockVer_offset[p] * n);
+  const int rc = solve_all(static_cast<int>(mode_));
+  if (rc == FAP_OK) {
+    check(fap_graph_check(dg_), "fap_graph_check");
+    for (int32_t p = 1; p <= K; p++) {
+      copy_block(p, dist.data() + (size_t)C_BlockVer_offset[p] * n);
+      if (path_needed) copy_path_block(p, path.data() + (size_t)C_BlockVer_offset[p] * n);
+    }
+  } else if (rc == FAP_ERR_NOMEM) {
+    // Fewer than n rows fit on the device: solve and copy group by group.
+    const int64_t rows = reserve_group_rows(max_subgraph_vertexs);
+    for (int32_t p = 1; p <= K;) {
+      const int32_t next = run_group(p, rows);
+      for (; p < next; p++) {
+        copy_block(p, dist.data() + (size_t)C_BlockVer_offset[p] * n);
+        if (path_needed) copy_path_block(p, path.data() + (size_t)C_BlockVer_offset[p] * n);
+      }
+    }
+  } else {
+    check(rc, "fap_solve");
   }
   path_ready_ = path_needed;
   return 0;
@@ -492,17 +559,27 @@ int32_t fapGraph::solveSubGraph(int32_t id, bool path_needed) {
   int64_t rows, ld;
   if (mode_ == SolveMode::Plain) {
     // Plain form: every call solves its part with its own launch sequence.
-    run_parts({id});
+    const int rc = fap_solve(dg_, &id, 1, FAP_MODE_PLAIN);
+    if (rc == FAP_ERR_NOMEM) {
+      reserve_group_rows(C_BlockVer_num[id]);
+      run_parts({id});
+    } else {
+      check(rc, "fap_solve");
+      check(fap_graph_check(dg_), "fap_graph_check");
+    }
   } else if (fap_graph_block(dg_, id, &dp, &rows, &ld) != FAP_OK ||
              (path_needed && fap_graph_path_block(dg_, id, &dp, &rows, &ld) != FAP_OK)) {
     // Batched form: solve every part once (blocks stay resident in HBM);
-    // later calls only copy.  Without room for every block, solve this part.
-    std::vector<int32_t> all;
-    for (int32_t p = 1; p <= K; p++) all.push_back(p);
-    if (fap_solve(dg_, all.data(), (int32_t)all.size(), FAP_MODE_BATCHED) != FAP_OK) {
-      run_parts({id});
-    } else {
+    // later calls only copy.  Without room for every block, solve this part
+    // and the ones after it that fit (the reference's callers visit the
+    // parts in order), from the resident cache when it fits.
+    const int rc = solve_all(FAP_MODE_BATCHED);
+    if (rc == FAP_OK) {
       check(fap_graph_check(dg_), "fap_graph_check");
+    } else if (rc == FAP_ERR_NOMEM) {
+      run_group(id, reserve_group_rows(C_BlockVer_num[id]));
+    } else {
+      check(rc, "fap_solve");
     }
   }
   subgraph_dist.resize((size_t)C_BlockVer_num[id] * n);
@@ -719,6 +796,11 @@ int fap_host_set_options(fap::fapGraph *g, int device, int dtype, int mode) {
     g->setDtype(dtype);
     g->setMode(mode == 0 ? fap::SolveMode::Plain : fap::SolveMode::Batched);
   })
+}
+
+int fap_host_set_max_resident_rows(fap::fapGraph *g, int64_t rows) {
+  FAPH_NEED(g);
+  FAPH_BODY(g->setMaxResidentRows(rows))
 }
 
 int fap_host_precondition(fap::fapGraph *g) {

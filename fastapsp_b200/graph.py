@@ -133,6 +133,12 @@ class fapGraph:
     def setMode(self, mode: str) -> None:
         self.setOptions(mode=L.FAP_MODE_PLAIN if mode == "plain" else L.FAP_MODE_BATCHED)
 
+    def setMaxResidentRows(self, rows: int) -> None:
+        """At most `rows` output rows on the device (0 = no bound): solve and
+        solveSubGraph then run the parts in groups whose rows fit, as they do
+        when HBM cannot hold all n rows."""
+        check(lib().fap_host_set_max_resident_rows(self._h, int(rows)), "setMaxResidentRows")
+
     # ---- sizes / CSR ----
     def _sizes(self):
         out = np.zeros(4, np.int64)

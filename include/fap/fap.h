@@ -89,7 +89,13 @@ class __attribute__((visibility("default"))) fapGraph {
   void ensure_device();
   bool path_ready_ = false;  // `path` holds every part's predecessors
 
+  int64_t row_limit_ = 0;     // setMaxResidentRows
+  bool cache_tried_ = false;  // the resident cache was attempted for grouped solves
+
   void run_parts(const std::vector<int32_t> &ids);
+  int solve_all(int mode);
+  int64_t reserve_group_rows(int64_t need);
+  int32_t run_group(int32_t first, int64_t rows);
   void copy_block(int32_t id, float *dst);
   void copy_path_block(int32_t id, int32_t *dst);
   void set_paths(bool on);
@@ -133,6 +139,10 @@ class __attribute__((visibility("default"))) fapGraph {
   void setDtype(int dtype);
   void setMode(SolveMode mode);
   SolveMode getMode() const { return mode_; }
+  // Bounds the output rows held on the device (0 = no bound): solve and
+  // solveSubGraph then run the parts in groups whose rows fit, as they do
+  // when HBM cannot hold all n rows.
+  void setMaxResidentRows(int64_t rows);
   int getDtype();
 
   void preCondition();

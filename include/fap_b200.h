@@ -106,9 +106,10 @@ FAP_API int fap_graph_set_parts(fap_dgraph *g, int32_t K, const int32_t *graph_i
                         const int32_t *st2ed, const int32_t *ver_num,
                         const int32_t *ver_offset, const int32_t *bdy_num);
 
-/* Reserves the output matrix for at most max_rows rows (0 = all n rows).
- * When max_rows < n, each fap_solve call may only request parts whose rows
- * fit; their blocks are packed from row 0 in request order. */
+/* Reserves the output matrix for at most max_rows rows (0 = all n rows, or
+ * as many as "max_resident_rows" allows; more than that bound fails with
+ * FAP_ERR_NOMEM).  When max_rows < n, each fap_solve call may only request
+ * parts whose rows fit; their blocks are packed from row 0 in request order. */
 FAP_API int fap_graph_reserve(fap_dgraph *g, int64_t max_rows);
 
 /* Solves the listed parts (1-based ids; parts == NULL means 1..K) into the
@@ -197,7 +198,10 @@ FAP_API int fap_graph_sssp_rows(fap_dgraph *g, const int32_t *sources, int32_t c
  * the local closures' tiles on and above the diagonal and stores their
  * transposes); "thin_max_b" (0..16, default 16: parts with at most this many
  * boundary vertices take the store-shaped thin min-plus kernel, the others
- * the register-tiled one). */
+ * the register-tiled one); "max_resident_rows" (>= 1: at most this many
+ * output rows are reserved on the device, as when HBM cannot hold all n
+ * rows; blocks already reserved beyond it are released; 0, the default: no
+ * bound). */
 FAP_API int fap_graph_set_param(fap_dgraph *g, const char *key, double value);
 
 /* Min-plus tiles run in the packed 16-bit form and in all, counted over

@@ -51,6 +51,11 @@ FAP_API int fap_host_destroy(fap_host_graph *g);
 FAP_API int fap_host_set_partition(fap_host_graph *g, const int32_t *graph_id);
 /* device ordinal, FAP_DTYPE_*, FAP_MODE_* */
 FAP_API int fap_host_set_options(fap_host_graph *g, int device, int dtype, int mode);
+/* At most `rows` output rows on the device (0 = no bound): solve and
+ * solve_subgraph then run the parts in groups whose rows fit, as they do
+ * when HBM cannot hold all n rows (no counterpart in the reference, whose
+ * split graphs always solve one part per call, fap/fap.cpp:196-208). */
+FAP_API int fap_host_set_max_resident_rows(fap_host_graph *g, int64_t rows);
 FAP_API int fap_host_precondition(fap_host_graph *g);
 FAP_API int fap_host_is_split(fap_host_graph *g);
 FAP_API int fap_host_dtype(fap_host_graph *g);

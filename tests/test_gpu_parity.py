@@ -105,6 +105,38 @@ def test_subgraph_getters_and_self_check(cuda_ok):
             g.getSubGraphDistance(1)  # not the current part
 
 
+@pytest.mark.parametrize("mode", [FAP_MODE_BATCHED, FAP_MODE_PLAIN])
+@pytest.mark.parametrize("name", ["road300_k6", "rmat8_f32_k4", "grid12_k4"])
+def test_bounded_resident_rows_match_reference(cuda_ok, name, mode):
+    """With fewer output rows allowed on the device than the graph has (as
+    when HBM cannot hold all n rows), solveSubGraph and solve run the parts
+    in groups that fit (in the batched form from the resident cache) and
+    give the reference's values; a part with more rows than the bound is
+    refused."""
+    case = load_golden(name)
+    K, vn, vo = case["K"], case["ver_num"], case["ver_offset"]
+    with tempfile.TemporaryDirectory() as tmp:
+        g = build_graph(case, tmp, mode)
+        g.setMaxResidentRows(2 * int(max(vn[1:])))
+        for p in list(range(K, 0, -1)) + [1, 2, 1]:
+            assert g.solveSubGraph(p) == 0
+            assert_dist_equal(g.getSubGraphDistance(p), case["dist"][vo[p]:vo[p] + vn[p]],
+                              case["integral"])
+        if mode == FAP_MODE_BATCHED:
+            assert g.device_graph().last_stage1() == 3  # from the resident cache
+        assert g.solve() == 0
+        assert_dist_equal(g.getAllDistance(), case["dist"], case["integral"])
+        big = int(np.argmax(vn[1:])) + 1
+        g.setMaxResidentRows(int(vn[big]) - 1)
+        with pytest.raises(FapError):
+            g.solveSubGraph(big)
+        with pytest.raises(FapError):
+            g.solve()
+        g.setMaxResidentRows(0)
+        assert g.solve() == 0
+        assert_dist_equal(g.getAllDistance(), case["dist"], case["integral"])
+
+
 @pytest.mark.parametrize("name", ["grid12_k4", "disconnected_k3"])
 def test_check_result_self_check(cuda_ok, name):
     """check_result compares sampled entries with fresh GPU shortest-path rows

@@ -195,6 +195,7 @@ def test_host_wrappers_refuse_null_arguments():
         lambda: lib.fap_host_dtype(None),
         lambda: lib.fap_host_set_partition(None, None),
         lambda: lib.fap_host_set_options(None, 0, 0, 0),
+        lambda: lib.fap_host_set_max_resident_rows(None, 0),
         lambda: lib.fap_host_solve(None, 0),
         lambda: lib.fap_host_solve_subgraph(None, 1, 0),
         lambda: lib.fap_host_current_subgraph(None),
