@@ -70,6 +70,9 @@ def parse_args():
                     help="batched Floyd as three launches per pivot block instead of the work queue")
     ap.add_argument("--no-pack16", action="store_true",
                     help="min-plus tiles in int32 only (no packed 16-bit tiles)")
+    ap.add_argument("--no-prepack", action="store_true",
+                    help="packed min-plus tiles convert their int32 stages in shared memory instead of "
+                         "reading operands packed once per solve")
     ap.add_argument("--no-stage-cache", action="store_true",
                     help="grouped jobs: run stages 1-2 per group instead of once for all parts")
     ap.add_argument("--cache-only", action="store_true",
@@ -687,6 +690,7 @@ def run_extra(args, job, ctx, relax_peak, hbm_peak, peak_kind):
     dtype = dg.dtype
     dg.set_parts(wl.K, gid, st2ed, vn, vo, bn)
     dg.set_param("minplus_pack16", 0 if args.no_pack16 else 1)
+    dg.set_param("minplus_prepack", 0 if args.no_prepack else 1)
     dg.set_param("floyd_queue", 0 if args.no_queue else 1)
     ldD = (n + 127) // 128 * 128
     stream = torch.cuda.current_stream()
@@ -888,6 +892,7 @@ def main_fap(args):
     dg.set_param("sssp_form", args.sssp_form)
     dg.set_param("bgraph_form", args.bgraph_form)
     dg.set_param("minplus_pack16", 0 if args.no_pack16 else 1)
+    dg.set_param("minplus_prepack", 0 if args.no_prepack else 1)
     dg.set_param("floyd_queue", 0 if args.no_queue else 1)
     if args.cache_only:
         run_cache_only(args, dg, stream, world)

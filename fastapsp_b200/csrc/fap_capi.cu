@@ -274,6 +274,12 @@ struct fap_dgraph {
   // fit (int32 graphs; Pack16): bounds buffers of the prepared batch.
   bool pack16 = true;
   DevBuf d_pk_off, d_pk_range, d_pk_maxa, d_pk_tiles;
+  // ... with the operands packed beforehand (Pack16::s16 / at) when they fit
+  // in kPrepackBytes and a quarter of the free device memory (parameter
+  // "minplus_prepack"); pk_krow: their first row per batch part
+  bool prepack = true;
+  DevBuf d_pk_s16, d_pk_at, d_pk_krow;
+  std::vector<int32_t> pk_krow;
   // the same for the tiled expansion of the boundary graph (Expand16), sized
   // for the launch's part list
   DevBuf d_xk_off, d_xk_range, d_xk_maxb, d_xk_tiles;
@@ -580,7 +586,7 @@ extern "C" int fap_graph_destroy(fap_dgraph *G) try {
                       &G->d_msbf_items, &G->d_msbf_act, &G->d_msbf_changed, &G->d_bitro, &G->d_bitcol,
                       &G->d_botro, &G->d_botcol, &G->d_bitw, &G->d_bitems, &G->d_bDt, &G->d_bact, &G->d_bpact,
                       &G->d_bgpart, &G->d_bpcolmap, &G->d_grow, &G->d_pk_off, &G->d_pk_range,
-                      &G->d_pk_maxa, &G->d_pk_tiles, &G->q.items, &G->q.cnt, &G->cq.items, &G->cq.cnt,
+                      &G->d_pk_s16, &G->d_pk_at, &G->d_pk_krow, &G->d_pk_maxa, &G->d_pk_tiles, &G->q.items, &G->q.cnt, &G->cq.items, &G->cq.cnt,
                       &G->d_xk_off, &G->d_xk_range, &G->d_xk_maxb, &G->d_xk_tiles, &G->d_bTc})
       b->release();
     if (G->h_changed) cudaFreeHost(G->h_changed);
@@ -793,6 +799,7 @@ constexpr int64_t kBgraphFloydMax = 8192;
 constexpr int64_t kBgraphStagedMax = 4096;
 // Largest column table of the staged expansion (max_b x ldD values).
 constexpr size_t kColTableBytes = size_t(256) << 20;
+constexpr size_t kPrepackBytes = size_t(8) << 30;
 // Automatic Bellman-Ford closure only while the boundary graph has at most
 // this many edges per edge of the graph (its cliques grow as b_p^2) and dB
 // stays within 64 Ki boundary vertices (17 GB).
@@ -1121,6 +1128,37 @@ int prepare_batch(fap_dgraph *G, const std::vector<int32_t> &ids, bool cached, b
     }
     G->pk = Pack16{G->d_pk_off.as<int32_t>(), G->d_pk_range.as<int32_t>(), G->d_pk_maxa.as<int32_t>(),
                    (int32_t)ntiles, G->d_pk_tiles.as<unsigned long long>()};
+    // Operands packed beforehand for the parts with tile work: rows of the
+    // parts' boundary vertices in batch order.
+    G->pk_krow.assign(np, -1);
+    int64_t prows = 0;
+    int32_t at_ld = 0, max_b = 0;
+    for (const MPWork &w : G->work) {
+      const PartDesc &d = G->parts[w.pidx];
+      if (G->pk_krow[w.pidx] >= 0) continue;
+      G->pk_krow[w.pidx] = (int32_t)prows;
+      prows += d.b;
+      at_ld = std::max(at_ld, d.s - d.b);
+      max_b = std::max(max_b, d.b);
+    }
+    at_ld = (int32_t)round_up((int64_t)std::max(at_ld, 1), 4);
+    const size_t pbytes = (size_t)prows * ((size_t)G->ldD * 2 + (size_t)at_ld * 4);
+    size_t free_b = 0, total_b = 0;
+    if (G->prepack && prows > 0 && prows < INT32_MAX && pbytes <= kPrepackBytes &&
+        cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && pbytes <= free_b / 4 &&
+        G->d_pk_s16.ensure_async((size_t)prows * G->ldD * 2, st) == FAP_OK &&
+        G->d_pk_at.ensure_async((size_t)prows * at_ld * 4, st) == FAP_OK &&
+        G->d_pk_krow.ensure_async(np * 4, st) == FAP_OK) {
+      G->pk.s16 = G->d_pk_s16.as<uint16_t>();
+      G->pk.at = G->d_pk_at.as<uint32_t>();
+      G->pk.krow = G->d_pk_krow.as<const int32_t>();
+      G->pk.at_ld = at_ld;
+      G->pk.max_b = max_b;
+      G->pk.prows = prows;
+    } else {
+      cudaGetLastError();  // (a failed cudaMemGetInfo or allocation: tiles convert their stages)
+      G->pk_krow.clear();
+    }
   }
   std::vector<QItem> qitems;
   if (!cached) {
@@ -1144,6 +1182,8 @@ int prepare_batch(fap_dgraph *G, const std::vector<int32_t> &ids, bool cached, b
     FAP_CK(cudaMemcpy(G->d_work.p, G->work.data(), G->work.size() * sizeof(MPWork), cudaMemcpyHostToDevice));
   if (!G->thin.empty())
     FAP_CK(cudaMemcpy(G->d_thin.p, G->thin.data(), G->thin.size() * 4, cudaMemcpyHostToDevice));
+  if (G->pk.s16 != nullptr)
+    FAP_CK(cudaMemcpy(G->d_pk_krow.p, G->pk_krow.data(), G->pk_krow.size() * 4, cudaMemcpyHostToDevice));
   if (!G->src.empty()) {
     FAP_CK(cudaMemcpy(G->d_src.p, G->src.data(), G->src.size() * 4, cudaMemcpyHostToDevice));
     FAP_CK(cudaMemcpy(G->d_srcrows.p, G->srcrows.data(), G->srcrows.size() * 8, cudaMemcpyHostToDevice));
@@ -2072,6 +2112,11 @@ extern "C" int fap_graph_set_param(fap_dgraph *G, const char *key, double value)
     G->last_ids.clear();
     return FAP_OK;
   }
+  if (std::strcmp(key, "minplus_prepack") == 0) {
+    G->prepack = value != 0.0;
+    G->last_ids.clear();
+    return FAP_OK;
+  }
   if (std::strcmp(key, "floyd_per_cta") == 0) {
     G->floyd_per_cta = value != 0.0;
     return FAP_OK;
@@ -2220,6 +2265,9 @@ extern "C" int fap_graph_release(fap_dgraph *G) try {
   G->d_pk_off.release();
   G->d_pk_range.release();
   G->d_pk_maxa.release();
+  G->d_pk_s16.release();
+  G->d_pk_at.release();
+  G->d_pk_krow.release();
   for (auto &cs : G->cslot) {
     if (cs.stream) FAP_CK(cudaStreamSynchronize(cs.stream));
     cs.busy = false;
@@ -2245,7 +2293,8 @@ extern "C" int fap_graph_device_bytes(const fap_dgraph *G, int64_t *bytes) try {
                           &G->d_bpart, &G->d_brows, &G->d_FB, &G->d_msbf_items, &G->d_msbf_act,
                           &G->d_msbf_changed, &G->d_bitro, &G->d_bitcol, &G->d_botro, &G->d_botcol, &G->d_bitw, &G->d_bitems,
                           &G->d_bDt, &G->d_bact, &G->d_bpact, &G->d_bgpart, &G->d_bpcolmap, &G->d_grow,
-                          &G->d_bTc})
+                          &G->d_bTc, &G->d_pk_off, &G->d_pk_range, &G->d_pk_maxa, &G->d_pk_tiles, &G->d_pk_s16,
+                          &G->d_pk_at, &G->d_pk_krow, &G->d_xk_off, &G->d_xk_range, &G->d_xk_maxb, &G->d_xk_tiles})
     t += (int64_t)b->bytes;
   *bytes = t;
   return FAP_OK;

@@ -81,19 +81,25 @@ PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
 }
 }  // namespace
 
-cudaError_t make_tmap_3d(CUtensorMap *map, const void *base, bool is_float, uint64_t d0, uint64_t d1,
-                         uint64_t d2, uint32_t box0, uint32_t box1) {
+// (elements of `esize` bytes of type dt; d0 x esize must be a multiple of 16)
+cudaError_t make_tmap_3d_dt(CUtensorMap *map, const void *base, CUtensorMapDataType dt, uint64_t esize,
+                            uint64_t d0, uint64_t d1, uint64_t d2, uint32_t box0, uint32_t box1) {
   auto enc = tmap_encoder();
   if (!enc) return cudaErrorNotSupported;
   const cuuint64_t dims[3] = {d0, d1, d2};
-  const cuuint64_t strides[2] = {d0 * 4, d0 * d1 * 4};
+  const cuuint64_t strides[2] = {d0 * esize, d0 * d1 * esize};
   const cuuint32_t box[3] = {box0, box1, 1};
   const cuuint32_t estr[3] = {1, 1, 1};
-  const CUresult r = enc(map, is_float ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_INT32, 3,
-                         const_cast<void *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  const CUresult r = enc(map, dt, 3, const_cast<void *>(base), dims, strides, box, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+cudaError_t make_tmap_3d(CUtensorMap *map, const void *base, bool is_float, uint64_t d0, uint64_t d1,
+                         uint64_t d2, uint32_t box0, uint32_t box1) {
+  return make_tmap_3d_dt(map, base, is_float ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_INT32,
+                         4, d0, d1, d2, box0, box1);
 }
 
 template <typename T>
@@ -739,20 +745,23 @@ __device__ __forceinline__ void minplus_part_epilogue(const PartDesc &pd, const 
 //   F[b+i][ed2st[j]-start] replaces it, as the reference's decode does.
 // PACK (int32): a tile whose entries provably fit (Pack16) runs the packed
 // 16-bit engine and shifts its results back by the column offsets; the
-// others run the int32 engine.  Both give the same int32 values.
+// others run the int32 engine.  Both give the same int32 values.  PACK 1
+// converts the int32 stages in shared memory, PACK 2 reads the operands
+// packed beforehand (Pack16::s16 / at, tensor maps mapAT / mapS).
 // ---------------------------------------------------------------------------
 // One min-plus tile: rows wk.m0 .. +BM of the part's inner block against
 // columns n0 .. +BN.  Block-wide; raw is the CTA's dynamic shared memory
 // (the TMA ring at its start, the packed buffers after it).  Returns false
 // (in every thread) if a TMA stage never completed.
-template <typename T, bool PACK>
+template <typename T, int PACK>
 __device__ __forceinline__ bool minplus_part_tile(const PartDesc &pd, const MPWork &wk, int tile_x, int n,
                                                   const T *__restrict__ F, T *D, int64_t ldD,
                                                   const int32_t *__restrict__ graph_id,
                                                   const int32_t *__restrict__ ed2st, const CUtensorMap *mapF,
                                                   const CUtensorMap *mapD, const Pack16 &pk,
                                                   TmaSmem<T, typename FloydCfg<T, kFloydTile>::TC> &sm,
-                                                  unsigned char *raw) {
+                                                  unsigned char *raw, const CUtensorMap *mapAT = nullptr,
+                                                  const CUtensorMap *mapS = nullptr) {
   using C = MPCfg<T>;
   using TC = typename FloydCfg<T, kFloydTile>::TC;
   const int n0 = tile_x * C::BN;
@@ -766,18 +775,48 @@ __device__ __forceinline__ bool minplus_part_tile(const PartDesc &pd, const MPWo
   // part's slot in the resident cache).
   const int fz = (int)(pd.f_off / ((int64_t)pd.ldf * pd.ldf));
   bool packed = false;
-  if constexpr (PACK) {
+  if constexpr (PACK != 0) {
     packed = __ldg(pk.maxA + wk.pidx) + __ldg(pk.range + (int64_t)wk.pidx * pk.ntiles + tile_x) < kPackCap;
     if (threadIdx.x == 0) {
       atomicAdd(pk.tiles + 1, 1ull);
       if (packed) atomicAdd(pk.tiles, 1ull);
     }
   }
-  if (packed) {
-    if constexpr (PACK) {
+  if (packed && PACK == 2) {
+    if constexpr (PACK == 2) {
+      // column offsets after the ring's memory (unused by the packed ring)
+      int32_t *coff = reinterpret_cast<int32_t *>(reinterpret_cast<unsigned char *>(sm.ring) +
+                                                  Pack16pCfg<TC>::STAGE_WORDS * 4 * TC::STAGES);
+      for (int c = threadIdx.x; c < C::BN; c += blockDim.x)
+        coff[c] = __ldg(pk.off + (int64_t)wk.pidx * ldD + n0 + c);
+      uint32_t a16[8][4];
+#pragma unroll
+      for (int i = 0; i < 8; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) a16[i][j] = kPackInit;
+      // (the engine's first barrier orders the column offsets before use)
+      if (!tma_minplus_tile16p<TC>(mapAT, wk.m0, mapS, n0, __ldg(pk.krow + wk.pidx), K, a16, sm,
+                                   pd.s - pd.b - wk.m0))
+        return false;
+      const int tx = threadIdx.x % C::TX;
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        // acc16[.][p] holds columns tile_col(tx, p / 2, 2 (p % 2)) and the next
+        const int32_t off = coff[tile_col<C>(tx, j / 4, j % 4)];
+        const int p = j / 2;
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+          const int32_t v = (j % 2) ? (int32_t)(int16_t)(a16[i][p] >> 16) : (int32_t)(int16_t)(a16[i][p] & 0xffffu);
+          acc[i][j] = v < kPackCap ? v + off : Dist<T>::inf();
+        }
+      }
+      // every thread has read its offsets before the shared memory is reused
+      __syncthreads();
+    }
+  } else if (packed) {
+    if constexpr (PACK == 1) {
       using P = Pack16Cfg<TC>;
-      const uintptr_t base = (reinterpret_cast<uintptr_t>(raw) + 127) & ~uintptr_t(127);
-      uint32_t *pbuf = reinterpret_cast<uint32_t *>(base + P::BUF_OFFSET);
+      uint32_t *pbuf = reinterpret_cast<uint32_t *>(smem_align128(raw) + P::BUF_OFFSET);
       int32_t *coff = reinterpret_cast<int32_t *>(pbuf + 2 * P::BUF_ELEMS);
       for (int c = threadIdx.x; c < C::BN; c += blockDim.x)
         coff[c] = __ldg(pk.off + (int64_t)wk.pidx * ldD + n0 + c);
@@ -830,12 +869,13 @@ __device__ __forceinline__ bool minplus_part_tile(const PartDesc &pd, const MPWo
 // 16-bit engine and shifts its results back by the column offsets; the
 // others run the int32 engine.  Both give the same int32 values.
 // ---------------------------------------------------------------------------
-template <typename T, bool PACK>
+template <typename T, int PACK>
 __global__ void __launch_bounds__(MPCfg<T>::THREADS, 2)
     minplus_part_kernel(const PartDesc *__restrict__ parts, const MPWork *__restrict__ work, int n,
                         const T *__restrict__ F, T *D, int64_t ldD,
                         const int32_t *__restrict__ graph_id, const int32_t *__restrict__ ed2st,
                         const __grid_constant__ CUtensorMap mapF, const __grid_constant__ CUtensorMap mapD,
+                        const __grid_constant__ CUtensorMap mapAT, const __grid_constant__ CUtensorMap mapS,
                         int *status, Pack16 pk) {
   using TC = typename FloydCfg<T, kFloydTile>::TC;
   extern __shared__ __align__(128) unsigned char mp_smem_raw[];
@@ -843,7 +883,7 @@ __global__ void __launch_bounds__(MPCfg<T>::THREADS, 2)
   const MPWork wk = work[blockIdx.y];
   const PartDesc pd = parts[wk.pidx];
   if (!minplus_part_tile<T, PACK>(pd, wk, blockIdx.x, n, F, D, ldD, graph_id, ed2st, &mapF, &mapD, pk, sm,
-                                  mp_smem_raw) &&
+                                  mp_smem_raw, &mapAT, &mapS) &&
       threadIdx.x == 0)
     set_status(status, kDevTmaTimeout);
 }
@@ -886,6 +926,13 @@ __global__ void __launch_bounds__(kMinplusBN)
   if (lo == INT32_MAX) lo = 0;
   else range = hi - lo;
   pk.off[(int64_t)wk.pidx * ldD + j] = lo;
+  if (pk.s16 != nullptr) {
+    // the pre-packed boundary rows (columns past n: no finite entry)
+    uint16_t *dst = pk.s16 + (int64_t)pk.krow[wk.pidx] * ldD + j;
+    const int32_t *col = D + pd.row_base * ldD + j;
+    for (int k = 0; k < pd.b; k++)
+      dst[(int64_t)k * ldD] = (uint16_t)(j < n ? pack_clamp(__ldg(col + (int64_t)k * ldD), lo) : kPackCap);
+  }
   // the tile's largest range
   __shared__ int32_t red[kMinplusBN / 32];
   for (int o = 16; o > 0; o >>= 1) range = max(range, __shfl_xor_sync(0xffffffffu, range, o));
@@ -923,6 +970,39 @@ __global__ void __launch_bounds__(256)
     int32_t x = 0;
     for (int w = 0; w < 8; w++) x = max(x, red[w]);
     pk.maxA[wk.pidx] = x;
+  }
+}
+
+// Pre-packed A operand of the packed tiles (Pack16::at): CTA (x, y) moves
+// boundary indices 32x .. 32x+31 of work item y's 128 inner rows through a
+// shared-memory transpose, reading F[b+m0+r][k] along k and writing
+// at[krow + k][m0 + r] along r, clamped at kPackCap in both halves.  Rows
+// past the part's inner block (up to at_ld) read as having no finite entry.
+__global__ void __launch_bounds__(256)
+    pack16_at_kernel(const PartDesc *__restrict__ parts, const MPWork *__restrict__ work,
+                     const int32_t *__restrict__ F, Pack16 pk) {
+  const MPWork wk = work[blockIdx.y];
+  const PartDesc pd = parts[wk.pidx];
+  const int k0 = blockIdx.x * 32;
+  if (k0 >= pd.b) return;
+  const int M = pd.s - pd.b;
+  __shared__ uint32_t t[kMinplusBM][33];
+  const int tid = threadIdx.x;
+#pragma unroll 4
+  for (int q = 0; q < kMinplusBM / 8; q++) {
+    const int r = tid / 32 + 8 * q, c = tid % 32;
+    const int i = wk.m0 + r, k = k0 + c;
+    int32_t v = kPackCap;
+    if (i < M && k < pd.b) v = pack_clamp(__ldg(F + pd.f_off + (int64_t)(pd.b + i) * pd.ldf + k), 0);
+    t[r][c] = pack_pair(v, v);
+  }
+  __syncthreads();
+  uint32_t *at = pk.at + (int64_t)pk.krow[wk.pidx] * pk.at_ld;
+#pragma unroll 4
+  for (int q = 0; q < 16; q++) {
+    const int r = tid % kMinplusBM, c = tid / kMinplusBM + 2 * q;
+    const int k = k0 + c, i = wk.m0 + r;
+    if (k < pd.b && i < pk.at_ld) at[(int64_t)k * pk.at_ld + i] = t[r][c];
   }
 }
 
@@ -1079,7 +1159,7 @@ __global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS, 2)
     } else if constexpr (WITH_MP) {
       const PartDesc pd = parts[cl.pidx];
       const MPWork wk{cl.pidx, cl.m0};
-      ok = minplus_part_tile<T, false>(pd, wk, cl.t, n, F, D, ldD, graph_id, ed2st, &mapA, &mapD, pk, sm,
+      ok = minplus_part_tile<T, 0>(pd, wk, cl.t, n, F, D, ldD, graph_id, ed2st, &mapA, &mapD, pk, sm,
                                        fq_smem_raw);
     }
     // this item's writes: visible to the async proxy, then to other CTAs,
@@ -1341,23 +1421,46 @@ cudaError_t launch_minplus_parts(const PartDesc *parts, int nparts, const MPWork
       pack16_cols_kernel<<<grid, kMinplusBN, 0, stream>>>(parts, work, n, D, ldD, *pk);
       pack16_maxa_kernel<<<(unsigned)nwork, 256, 0, stream>>>(parts, work, F, *pk);
       *launches += 2;
-      using P = Pack16Cfg<TC>;
-      const size_t smem = P::SMEM_BYTES;
-      auto kern = minplus_part_kernel<T, true>;
-      e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess) return e;
-      kern<<<grid, C::THREADS, smem, stream>>>(parts, work, n, F, D, ldD, graph_id, ed2st, mapF, mapD, status,
-                                               *pk);
+      if (pk->s16 != nullptr) {
+        // operands packed beforehand: the boundary rows (above) and the
+        // inner-to-boundary distances, then tiles without conversion
+        if (pk->at == nullptr || pk->krow == nullptr || pk->at_ld % 4 != 0 || pk->prows <= 0 || pk->max_b <= 0)
+          return cudaErrorInvalidValue;
+        CUtensorMap mapAT, mapS;
+        e = make_tmap_3d_dt(&mapAT, pk->at, CU_TENSOR_MAP_DATA_TYPE_UINT32, 4, pk->at_ld, pk->prows, 1, TC::BM,
+                            TC::BK);
+        if (e == cudaSuccess)
+          e = make_tmap_3d_dt(&mapS, pk->s16, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, ldD, pk->prows, 1, TC::BN,
+                              TC::BK);
+        if (e != cudaSuccess) return e;
+        pack16_at_kernel<<<dim3((unsigned)ceil_div(pk->max_b, 32), (unsigned)nwork), 256, 0, stream>>>(parts, work,
+                                                                                                     F, *pk);
+        *launches += 1;
+        const size_t smem = TC::SMEM_BYTES;
+        auto kern = minplus_part_kernel<T, 2>;
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        kern<<<grid, C::THREADS, smem, stream>>>(parts, work, n, F, D, ldD, graph_id, ed2st, mapF, mapD, mapAT,
+                                                 mapS, status, *pk);
+      } else {
+        using P = Pack16Cfg<TC>;
+        const size_t smem = P::SMEM_BYTES;
+        auto kern = minplus_part_kernel<T, 1>;
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        kern<<<grid, C::THREADS, smem, stream>>>(parts, work, n, F, D, ldD, graph_id, ed2st, mapF, mapD, mapF,
+                                                 mapD, status, *pk);
+      }
       done = true;
     }
   }
   if (!done) {
     const size_t smem = TC::SMEM_BYTES;
-    auto kern = minplus_part_kernel<T, false>;
+    auto kern = minplus_part_kernel<T, 0>;
     e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    kern<<<grid, C::THREADS, smem, stream>>>(parts, work, n, F, D, ldD, graph_id, ed2st, mapF, mapD, status,
-                                             none);
+    kern<<<grid, C::THREADS, smem, stream>>>(parts, work, n, F, D, ldD, graph_id, ed2st, mapF, mapD, mapF, mapD,
+                                             status, none);
   }
   *launches += 1;
   return cudaGetLastError();
@@ -2249,8 +2352,7 @@ __global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS, 2)
   if (packed) {
     if constexpr (PACK) {
       using P = Pack16Cfg<TC>;
-      const uintptr_t base = (reinterpret_cast<uintptr_t>(bxt_smem_raw) + 127) & ~uintptr_t(127);
-      uint32_t *pbuf = reinterpret_cast<uint32_t *>(base + P::BUF_OFFSET);
+      uint32_t *pbuf = reinterpret_cast<uint32_t *>(smem_align128(bxt_smem_raw) + P::BUF_OFFSET);
       int32_t *roff = reinterpret_cast<int32_t *>(pbuf + 2 * P::BUF_ELEMS) + TC::BN;
       for (int r = threadIdx.x; r < TC::BM; r += blockDim.x)
         roff[r] = m0 + r < nbB ? __ldg(xk.off + (int64_t)blockIdx.z * nbB + m0 + r) : 0;

@@ -58,12 +58,24 @@ struct MPWork {
 // its column's off (range); per part the largest finite A = F[b+i][k]
 // (maxA).  A tile runs packed when maxA + range < kPackCap, otherwise in
 // int32.  Buffers: off [nparts][ldD], range [nparts][ntiles], maxA [nparts].
+// Optional pre-packed operands (s16 null: every packed tile converts its
+// stages in shared memory): s16 [rows][ldD] uint16 holds the boundary rows
+// of D shifted by off and clamped at kPackCap, at [rows][at_ld] uint32 the
+// inner-to-boundary distances F[b+i][k] clamped at kPackCap in both halves,
+// k-major (column i); part pidx's boundary vertex k is row krow[pidx] + k of
+// both (krow < 0: the part has no work).
 struct Pack16 {
   int32_t *off;
   int32_t *range;
   int32_t *maxA;
   int32_t ntiles;
   unsigned long long *tiles;  // [2]: tiles run packed, tiles run (cumulative)
+  uint16_t *s16;
+  uint32_t *at;
+  const int32_t *krow;
+  int32_t at_ld;
+  int32_t max_b;              // largest boundary count of the work's parts
+  int64_t prows;              // rows of s16 and at
 };
 
 // Packed 16-bit form of the tiled expansion of the boundary graph (int32):

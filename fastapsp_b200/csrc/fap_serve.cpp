@@ -718,6 +718,8 @@ int fap_server_add_graph(fap_server *s, int32_t n, int64_t m, const int32_t *row
   // Batches change from one launch to the next: launch the stages directly
   // instead of capturing a CUDA graph per batch.
   fap_graph_set_param(g->dg, "cuda_graph", 0);
+  // (the admission footprint does not count pre-packed min-plus operands)
+  fap_graph_set_param(g->dg, "minplus_prepack", 0);
   fap_graph_device_bytes(g->dg, &g->base_bytes);
   void *stream = nullptr;
   fap_ctx_get_stream(g->ctx, &stream);

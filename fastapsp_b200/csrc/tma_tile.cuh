@@ -37,6 +37,14 @@ struct TmaTileCfg {
   static_assert((A_ELEMS * sizeof(T)) % 128 == 0 && (B_ELEMS * sizeof(T)) % 128 == 0, "aligned boxes");
 };
 
+// The first 128-byte boundary at or after raw (dynamic shared memory).  The
+// pointer is formed by arithmetic on raw itself, not through an integer, so
+// that the compiler still knows it points to shared memory and accesses
+// through it become shared-memory loads and stores with immediate offsets.
+__device__ __forceinline__ unsigned char *smem_align128(unsigned char *raw) {
+  return raw + ((128u - (smem_u32(raw) & 127u)) & 127u);
+}
+
 // Carved dynamic shared memory of a TMA tile CTA.
 template <typename T, class C>
 struct TmaSmem {
@@ -48,7 +56,7 @@ struct TmaSmem {
 template <typename T, class C>
 __device__ __forceinline__ TmaSmem<T, C> tma_smem_init(unsigned char *raw) {
   TmaSmem<T, C> s;
-  const uintptr_t a = (reinterpret_cast<uintptr_t>(raw) + 127) & ~uintptr_t(127);
+  unsigned char *a = smem_align128(raw);
   s.ring = reinterpret_cast<T *>(a);
   s.bars = reinterpret_cast<uint64_t *>(a + C::RING_BYTES);
   s.phase = 0;
@@ -305,6 +313,107 @@ __device__ __forceinline__ bool tma_minplus_tile16(const CUtensorMap *mapA, int 
     if (tid == 0 && c + C::STAGES < n) issue(c + C::STAGES, s);
     if (rhi) pack16_chunk_compute<C, 2>(PA, PB, acc, ty, tx, min(C::BK, K - c * C::BK));
     else if (rlo) pack16_chunk_compute<C, 1>(PA, PB, acc, ty, tx, min(C::BK, K - c * C::BK));
+  }
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// Packed 16-bit form on operands packed in global memory beforehand, so that
+// the stages arrive ready for the relaxations (no conversion, no second
+// barrier per chunk).  One __viaddmin_s16x2 relaxes one row against two
+// adjacent columns:
+//   AT[k][i] = (A'[i][k], A'[i][k])     uint32, k-major (i fastest)
+//   S[k][c]  = B'[k][c]                 uint16, so a uint32 holds columns
+//                                       (c, c+1) of row k
+// with the clamping and bounds of the in-kernel form above (the caller
+// packs both arrays; A' = min(A, kPackCap), B' = min(B - off[c], kPackCap)).
+// A stage is the AT box (x = rows ax.., y = k) and the S box (x = columns
+// bx.., y = k), both at y = ky + c * BK.  acc[i][p]: row tile_row(i), columns
+// tile_col(2p mod 4 ..) as in Pack16pCfg below.
+// ---------------------------------------------------------------------------
+template <class C>
+struct Pack16pCfg {
+  static constexpr int A_WORDS = C::BK * C::BM;        // AT box: BK rows of BM uint32
+  static constexpr int B_WORDS = C::BK * C::BN / 2;    // S box: BK rows of BN uint16
+  static constexpr int STAGE_WORDS = A_WORDS + B_WORDS;
+  static constexpr uint32_t TX_BYTES = STAGE_WORDS * 4;
+  static_assert(C::STAGES * STAGE_WORDS * 4 <= C::RING_BYTES, "the packed ring fits in the int32 ring");
+  static_assert((A_WORDS * 4) % 128 == 0 && (STAGE_WORDS * 4) % 128 == 0, "128-byte aligned boxes");
+  static_assert(C::BM == 128 && C::BN == 128 && C::THREADS == 256 && C::TX == 16, "thread mapping below");
+};
+
+// One chunk: per k, the thread's 8 rows (two 16-byte loads: rows ty*4..+3 of
+// each row group, duplicated halves) and 4 column pairs (two 8-byte loads:
+// columns tx*4..+3 of each column group), then 32 packed relaxations.
+template <class C, int GI = 2>
+__device__ __forceinline__ void pack16p_chunk_compute(const uint32_t *As, const uint32_t *Bs,
+                                                      uint32_t (&acc)[8][4], int ty, int tx, int kc) {
+#pragma unroll 4
+  for (int k = 0; k < kc; k++) {
+    uint32_t a[8], b[4];
+#pragma unroll
+    for (int g = 0; g < GI; g++) {
+      const uint4 v = *reinterpret_cast<const uint4 *>(As + k * C::BM + g * (C::BM / 2) + ty * 4);
+      a[4 * g + 0] = v.x; a[4 * g + 1] = v.y; a[4 * g + 2] = v.z; a[4 * g + 3] = v.w;
+    }
+#pragma unroll
+    for (int g = 0; g < 2; g++) {
+      const uint2 v = *reinterpret_cast<const uint2 *>(Bs + k * (C::BN / 2) + g * (C::BN / 4) + tx * 2);
+      b[2 * g + 0] = v.x; b[2 * g + 1] = v.y;
+    }
+#pragma unroll
+    for (int i = 0; i < 4 * GI; i++)
+#pragma unroll
+      for (int p = 0; p < 4; p++) acc[i][p] = __viaddmin_s16x2(a[i], b[p], acc[i][p]);
+  }
+}
+
+// The pre-packed form of tma_minplus_tile16: the same ring protocol as
+// tma_minplus_tile (one barrier per chunk, bounded waits, drain on a
+// timeout) over the int32 ring's memory and mbarriers.  mvalid: rows of the
+// tile that are not padding (warps holding none of them skip the work).
+template <class C>
+__device__ __forceinline__ bool tma_minplus_tile16p(const CUtensorMap *mapA, int ax, const CUtensorMap *mapB,
+                                                    int bx, int ky, int K, uint32_t (&acc)[8][4],
+                                                    TmaSmem<int32_t, C> &sm, int mvalid = C::BM) {
+  using P = Pack16pCfg<C>;
+  const int tid = threadIdx.x, ty = tid / C::TX, tx = tid % C::TX;
+  const int w8 = (tid / 32) * 8;
+  const bool rlo = w8 < mvalid, rhi = C::BM / 2 + w8 < mvalid;
+  const int n = (int)ceil_div(K, C::BK);
+  if (n == 0) return true;
+  uint32_t *ring = reinterpret_cast<uint32_t *>(sm.ring);
+  auto issue = [&](int c, int s) {
+    uint32_t *As = ring + s * P::STAGE_WORDS;
+    mbar_arrive_expect_tx(&sm.bars[s], P::TX_BYTES);
+    tma_load_3d(As, mapA, ax, ky + c * C::BK, 0, &sm.bars[s]);
+    tma_load_3d(As + P::A_WORDS, mapB, bx, ky + c * C::BK, 0, &sm.bars[s]);
+  };
+  fence_proxy_async_all();
+  __syncthreads();
+  if (tid == 0)
+    for (int c = 0; c < n && c < C::STAGES; c++) issue(c, c);
+  for (int c = 0; c < n; c++) {
+    const int s = c % C::STAGES;
+    const bool got = mbar_wait_bounded(&sm.bars[s], (sm.phase >> s) & 1u);
+    sm.phase ^= 1u << s;
+    if (got) {
+      const uint32_t *As = ring + s * P::STAGE_WORDS;
+      const int kc = min(C::BK, K - c * C::BK);
+      if (rhi) pack16p_chunk_compute<C, 2>(As, As + P::A_WORDS, acc, ty, tx, kc);
+      else if (rlo) pack16p_chunk_compute<C, 1>(As, As + P::A_WORDS, acc, ty, tx, kc);
+    }
+    fence_proxy_async_smem();  // this thread's reads of stage s precede its refill
+    if (__syncthreads_or(!got)) {
+      for (int c2 = c + 1; c2 < n && c2 < c + C::STAGES; c2++) {
+        const int s2 = c2 % C::STAGES;
+        if (tid == 0) mbar_wait_bounded(&sm.bars[s2], (sm.phase >> s2) & 1u);
+        sm.phase ^= 1u << s2;
+      }
+      __syncthreads();
+      return false;
+    }
+    if (tid == 0 && c + C::STAGES < n) issue(c + C::STAGES, s);
   }
   return true;
 }

@@ -191,7 +191,12 @@ FAP_API int fap_graph_sssp_rows(fap_dgraph *g, const int32_t *sources, int32_t c
  * boundary-row column is shifted by its least finite entry and the part's
  * largest finite inner-to-boundary distance plus the tile's largest shifted
  * entry is below 16383; other tiles run in int32; the results are the same
- * int32 values either way; 0: int32 everywhere); "floyd_queue" (default 1:
+ * int32 values either way; 0: int32 everywhere); "minplus_prepack" (default
+ * 1: the packed tiles read operands packed once per solve, the boundary rows
+ * as 16-bit columns and the inner-to-boundary distances with both halves
+ * equal, when those arrays fit in 8 GiB and a quarter of the free device
+ * memory; 0, or when they do not fit: each tile converts its int32 stages
+ * in shared memory; the same values either way); "floyd_queue" (default 1:
  * the batched Floyd-Warshall as one persistent launch over a device work
  * queue; 0: three launches per pivot block); "floyd_symmetric" (default 1:
  * on parts whose arcs all have reverses of equal weight, the queue computes

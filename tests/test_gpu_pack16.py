@@ -1,7 +1,8 @@
 """The packed 16-bit min-plus tiles (int32 graphs, parts with more than 16
 boundary vertices) give the same int32 blocks as the int32 tiles, whether
-all, some or none of the tiles fit the packed form, and in the plain, the
-batched and the cached solves."""
+all, some or none of the tiles fit the packed form, in the plain, the
+batched and the cached solves, and with the operands packed beforehand
+("minplus_prepack" 1, the default) or stage by stage in shared memory (0)."""
 import numpy as np
 import pytest
 
@@ -38,10 +39,12 @@ def _grid(heavy_rows, heavy_wmax, seed):
     return el
 
 
+@pytest.mark.parametrize("prepack", [1, 0])
 @pytest.mark.parametrize("heavy_rows,expect", [(96, "all"), (48, "some"), (0, "none")])
-def test_packed_tiles_equal_int32_tiles(cuda_ok, tmp_path, heavy_rows, expect):
+def test_packed_tiles_equal_int32_tiles(cuda_ok, tmp_path, heavy_rows, expect, prepack):
     el = _grid(heavy_rows, 200000, 11)
     dg, vn, bn = _device_graph(el, 12, tmp_path, f"pk{heavy_rows}")
+    dg.set_param("minplus_prepack", prepack)
     parts = list(range(1, 13))
     assert int(bn[1:].min()) > 16          # every part runs the min-plus tile kernel
     dg.set_param("minplus_pack16", 0)
@@ -64,9 +67,11 @@ def test_packed_tiles_equal_int32_tiles(cuda_ok, tmp_path, heavy_rows, expect):
         assert 0 < packed < total, (packed, total)
 
 
-def test_packed_tiles_from_the_resident_cache(cuda_ok, tmp_path):
+@pytest.mark.parametrize("prepack", [1, 0])
+def test_packed_tiles_from_the_resident_cache(cuda_ok, tmp_path, prepack):
     el = G.grid_graph(96, 96, extra_frac=0.01, wmin=1, wmax=100, seed=12)
     dg, vn, bn = _device_graph(el, 12, tmp_path, "pkc")
+    dg.set_param("minplus_prepack", prepack)
     dg.set_param("minplus_pack16", 0)
     dg.solve(None, FAP_MODE_BATCHED)
     ref = _blocks(dg, range(1, 13))

@@ -11,8 +11,8 @@ preprocessing (METIS k-way, boundary detection, sort_and_encode); every case
 is then solved with stage 1 by the frontier and the tiled SSSP, by the
 boundary graph closed by Floyd and by Bellman-Ford, with the Floyd as the
 work queue and as per-phase launches, symmetric and not, with thin and tile
-min-plus kernels, packed and int32 tiles, in the plain form, and from the
-resident cache."""
+min-plus kernels, packed (operands packed beforehand or per stage) and int32
+tiles, in the plain form, and from the resident cache."""
 import numpy as np
 import pytest
 
@@ -41,6 +41,7 @@ FORMS = [
     {"floyd_symmetric": 0},                        # full Floyd items
     {"thin_max_b": 0},                             # register-tiled min-plus for every part
     {"thin_max_b": 0, "minplus_pack16": 0},        # ... in int32 only
+    {"thin_max_b": 0, "minplus_prepack": 0},       # ... packed stage by stage in shared memory
 ]
 
 
