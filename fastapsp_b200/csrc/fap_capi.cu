@@ -1143,9 +1143,11 @@ int prepare_batch(fap_dgraph *G, const std::vector<int32_t> &ids, bool cached, b
     }
     at_ld = (int32_t)round_up((int64_t)std::max(at_ld, 1), 4);
     const size_t pbytes = (size_t)prows * ((size_t)G->ldD * 2 + (size_t)at_ld * 4);
+    // (the free memory is asked for only when the buffers have to grow)
+    const bool grow = G->d_pk_s16.bytes < (size_t)prows * G->ldD * 2 || G->d_pk_at.bytes < (size_t)prows * at_ld * 4;
     size_t free_b = 0, total_b = 0;
     if (G->prepack && prows > 0 && prows < INT32_MAX && pbytes <= kPrepackBytes &&
-        cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && pbytes <= free_b / 4 &&
+        (!grow || (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && pbytes <= free_b / 4)) &&
         G->d_pk_s16.ensure_async((size_t)prows * G->ldD * 2, st) == FAP_OK &&
         G->d_pk_at.ensure_async((size_t)prows * at_ld * 4, st) == FAP_OK &&
         G->d_pk_krow.ensure_async(np * 4, st) == FAP_OK) {

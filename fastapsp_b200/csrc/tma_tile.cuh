@@ -74,27 +74,37 @@ __device__ __forceinline__ TmaSmem<T, C> tma_smem_init(unsigned char *raw) {
 // loads, then 64 relaxations.  GI / GJ: the thread's row / column groups
 // computed (1 skips the second group, rows or columns BM/2.. or BN/2..,
 // when they are all padding).
+template <typename T, class C, int GI, int GJ>
+__device__ __forceinline__ void tma_k_step(const T *Arow, const T *Bs, T (&acc)[8][8], int tx, int k) {
+  using V = typename Vec4<T>::type;
+  T a[8], b[8];
+#pragma unroll
+  for (int g = 0; g < GI; g++)
+#pragma unroll
+    for (int l = 0; l < 4; l++) a[4 * g + l] = Arow[(g * (C::BM / 2) + l) * C::BK + k];
+#pragma unroll
+  for (int g = 0; g < GJ; g++) {
+    const V v = *reinterpret_cast<const V *>(Bs + k * C::BN + g * (C::BN / 2) + tx * 4);
+    b[4 * g + 0] = v.x; b[4 * g + 1] = v.y; b[4 * g + 2] = v.z; b[4 * g + 3] = v.w;
+  }
+#pragma unroll
+  for (int i = 0; i < 4 * GI; i++)
+#pragma unroll
+    for (int j = 0; j < 4 * GJ; j++) acc[i][j] = Dist<T>::relax(a[i], b[j], acc[i][j]);
+}
+
+// (a full chunk runs with k unrolled: constant shared-memory offsets and no
+// loop counter; a partial last chunk runs the rolled loop)
 template <typename T, class C, int GI = 2, int GJ = 2>
 __device__ __forceinline__ void tma_chunk_compute(const T *As, const T *Bs, T (&acc)[8][8], int ty,
                                                   int tx, int kc) {
-  using V = typename Vec4<T>::type;
   const T *Arow = As + (ty * 4) * C::BK;
-#pragma unroll 4
-  for (int k = 0; k < kc; k++) {
-    T a[8], b[8];
+  if (kc == C::BK) {
 #pragma unroll
-    for (int g = 0; g < GI; g++)
-#pragma unroll
-      for (int l = 0; l < 4; l++) a[4 * g + l] = Arow[(g * (C::BM / 2) + l) * C::BK + k];
-#pragma unroll
-    for (int g = 0; g < GJ; g++) {
-      const V v = *reinterpret_cast<const V *>(Bs + k * C::BN + g * (C::BN / 2) + tx * 4);
-      b[4 * g + 0] = v.x; b[4 * g + 1] = v.y; b[4 * g + 2] = v.z; b[4 * g + 3] = v.w;
-    }
-#pragma unroll
-    for (int i = 0; i < 4 * GI; i++)
-#pragma unroll
-      for (int j = 0; j < 4 * GJ; j++) acc[i][j] = Dist<T>::relax(a[i], b[j], acc[i][j]);
+    for (int k = 0; k < C::BK; k++) tma_k_step<T, C, GI, GJ>(Arow, Bs, acc, tx, k);
+  } else {
+#pragma unroll 1
+    for (int k = 0; k < kc; k++) tma_k_step<T, C, GI, GJ>(Arow, Bs, acc, tx, k);
   }
 }
 
@@ -233,28 +243,37 @@ __device__ __forceinline__ void pack16_convert(const int32_t *As, const int32_t 
 
 // One converted chunk: per k, the thread's 4 row pairs (two 8-byte loads)
 // and 8 columns (two 16-byte loads), then 32 packed relaxations.
+template <class C, int GI>
+__device__ __forceinline__ void pack16_k_step(const uint32_t *PA, const uint32_t *PB, uint32_t (&acc)[4][8],
+                                              int ty, int tx, int k) {
+  using P = Pack16Cfg<C>;
+  uint32_t a[4], b[8];
+#pragma unroll
+  for (int g = 0; g < GI; g++) {
+    const uint2 v = *reinterpret_cast<const uint2 *>(PA + k * P::PA_LD + g * (C::BM / 4) + ty * 2);
+    a[2 * g] = v.x;
+    a[2 * g + 1] = v.y;
+  }
+#pragma unroll
+  for (int g = 0; g < 2; g++) {
+    const uint4 v = *reinterpret_cast<const uint4 *>(PB + k * C::BN + g * (C::BN / 2) + tx * 4);
+    b[4 * g + 0] = v.x; b[4 * g + 1] = v.y; b[4 * g + 2] = v.z; b[4 * g + 3] = v.w;
+  }
+#pragma unroll
+  for (int i = 0; i < 2 * GI; i++)
+#pragma unroll
+    for (int j = 0; j < 8; j++) acc[i][j] = __viaddmin_s16x2(a[i], b[j], acc[i][j]);
+}
+
 template <class C, int GI = 2>
 __device__ __forceinline__ void pack16_chunk_compute(const uint32_t *PA, const uint32_t *PB,
                                                      uint32_t (&acc)[4][8], int ty, int tx, int kc) {
-  using P = Pack16Cfg<C>;
-#pragma unroll 4
-  for (int k = 0; k < kc; k++) {
-    uint32_t a[4], b[8];
+  if (kc == C::BK) {
 #pragma unroll
-    for (int g = 0; g < GI; g++) {
-      const uint2 v = *reinterpret_cast<const uint2 *>(PA + k * P::PA_LD + g * (C::BM / 4) + ty * 2);
-      a[2 * g] = v.x;
-      a[2 * g + 1] = v.y;
-    }
-#pragma unroll
-    for (int g = 0; g < 2; g++) {
-      const uint4 v = *reinterpret_cast<const uint4 *>(PB + k * C::BN + g * (C::BN / 2) + tx * 4);
-      b[4 * g + 0] = v.x; b[4 * g + 1] = v.y; b[4 * g + 2] = v.z; b[4 * g + 3] = v.w;
-    }
-#pragma unroll
-    for (int i = 0; i < 2 * GI; i++)
-#pragma unroll
-      for (int j = 0; j < 8; j++) acc[i][j] = __viaddmin_s16x2(a[i], b[j], acc[i][j]);
+    for (int k = 0; k < C::BK; k++) pack16_k_step<C, GI>(PA, PB, acc, ty, tx, k);
+  } else {
+#pragma unroll 1
+    for (int k = 0; k < kc; k++) pack16_k_step<C, GI>(PA, PB, acc, ty, tx, k);
   }
 }
 
@@ -345,26 +364,35 @@ struct Pack16pCfg {
 // One chunk: per k, the thread's 8 rows (two 16-byte loads: rows ty*4..+3 of
 // each row group, duplicated halves) and 4 column pairs (two 8-byte loads:
 // columns tx*4..+3 of each column group), then 32 packed relaxations.
+template <class C, int GI>
+__device__ __forceinline__ void pack16p_k_step(const uint32_t *As, const uint32_t *Bs, uint32_t (&acc)[8][4],
+                                               int ty, int tx, int k) {
+  uint32_t a[8], b[4];
+#pragma unroll
+  for (int g = 0; g < GI; g++) {
+    const uint4 v = *reinterpret_cast<const uint4 *>(As + k * C::BM + g * (C::BM / 2) + ty * 4);
+    a[4 * g + 0] = v.x; a[4 * g + 1] = v.y; a[4 * g + 2] = v.z; a[4 * g + 3] = v.w;
+  }
+#pragma unroll
+  for (int g = 0; g < 2; g++) {
+    const uint2 v = *reinterpret_cast<const uint2 *>(Bs + k * (C::BN / 2) + g * (C::BN / 4) + tx * 2);
+    b[2 * g + 0] = v.x; b[2 * g + 1] = v.y;
+  }
+#pragma unroll
+  for (int i = 0; i < 4 * GI; i++)
+#pragma unroll
+    for (int p = 0; p < 4; p++) acc[i][p] = __viaddmin_s16x2(a[i], b[p], acc[i][p]);
+}
+
 template <class C, int GI = 2>
 __device__ __forceinline__ void pack16p_chunk_compute(const uint32_t *As, const uint32_t *Bs,
                                                       uint32_t (&acc)[8][4], int ty, int tx, int kc) {
-#pragma unroll 4
-  for (int k = 0; k < kc; k++) {
-    uint32_t a[8], b[4];
+  if (kc == C::BK) {
 #pragma unroll
-    for (int g = 0; g < GI; g++) {
-      const uint4 v = *reinterpret_cast<const uint4 *>(As + k * C::BM + g * (C::BM / 2) + ty * 4);
-      a[4 * g + 0] = v.x; a[4 * g + 1] = v.y; a[4 * g + 2] = v.z; a[4 * g + 3] = v.w;
-    }
-#pragma unroll
-    for (int g = 0; g < 2; g++) {
-      const uint2 v = *reinterpret_cast<const uint2 *>(Bs + k * (C::BN / 2) + g * (C::BN / 4) + tx * 2);
-      b[2 * g + 0] = v.x; b[2 * g + 1] = v.y;
-    }
-#pragma unroll
-    for (int i = 0; i < 4 * GI; i++)
-#pragma unroll
-      for (int p = 0; p < 4; p++) acc[i][p] = __viaddmin_s16x2(a[i], b[p], acc[i][p]);
+    for (int k = 0; k < C::BK; k++) pack16p_k_step<C, GI>(As, Bs, acc, ty, tx, k);
+  } else {
+#pragma unroll 1
+    for (int k = 0; k < kc; k++) pack16p_k_step<C, GI>(As, Bs, acc, ty, tx, k);
   }
 }
 
