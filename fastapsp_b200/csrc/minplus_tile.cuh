@@ -129,28 +129,39 @@ struct Vec4<int32_t> { using type = int4; };
 template <>
 struct Vec4<float> { using type = float4; };
 
-// acc <- min(acc, As (x) Bs) over kcount k's of one staged chunk.
+// One k of a staged chunk (acc <- min(acc, As[k][.] + Bs[k][.])).
+template <typename T, class C>
+__device__ __forceinline__ void mma_k_step(const T *As, const T *Bs, T (&acc)[C::TM][C::TN], int ty, int tx,
+                                           int k) {
+  using V = typename Vec4<T>::type;
+  T a[C::TM], b[C::TN];
+#pragma unroll
+  for (int g = 0; g < C::GM; g++) {
+    V v = *reinterpret_cast<const V *>(As + k * C::AP + g * (C::BM / C::GM) + ty * 4);
+    a[4 * g + 0] = v.x; a[4 * g + 1] = v.y; a[4 * g + 2] = v.z; a[4 * g + 3] = v.w;
+  }
+#pragma unroll
+  for (int g = 0; g < C::GN; g++) {
+    V v = *reinterpret_cast<const V *>(Bs + k * C::BN + g * (C::BN / C::GN) + tx * 4);
+    b[4 * g + 0] = v.x; b[4 * g + 1] = v.y; b[4 * g + 2] = v.z; b[4 * g + 3] = v.w;
+  }
+#pragma unroll
+  for (int i = 0; i < C::TM; i++)
+#pragma unroll
+    for (int j = 0; j < C::TN; j++) acc[i][j] = Dist<T>::relax(a[i], b[j], acc[i][j]);
+}
+
+// acc <- min(acc, As (x) Bs) over kcount k's of one staged chunk (a full
+// chunk runs with k unrolled, a partial one with the rolled loop).
 template <typename T, class C>
 __device__ __forceinline__ void mma_chunk(const T *As, const T *Bs, T (&acc)[C::TM][C::TN],
                                           int ty, int tx, int kcount) {
-  using V = typename Vec4<T>::type;
-#pragma unroll 4
-  for (int k = 0; k < kcount; k++) {
-    T a[C::TM], b[C::TN];
+  if (kcount == C::BK) {
 #pragma unroll
-    for (int g = 0; g < C::GM; g++) {
-      V v = *reinterpret_cast<const V *>(As + k * C::AP + g * (C::BM / C::GM) + ty * 4);
-      a[4 * g + 0] = v.x; a[4 * g + 1] = v.y; a[4 * g + 2] = v.z; a[4 * g + 3] = v.w;
-    }
-#pragma unroll
-    for (int g = 0; g < C::GN; g++) {
-      V v = *reinterpret_cast<const V *>(Bs + k * C::BN + g * (C::BN / C::GN) + tx * 4);
-      b[4 * g + 0] = v.x; b[4 * g + 1] = v.y; b[4 * g + 2] = v.z; b[4 * g + 3] = v.w;
-    }
-#pragma unroll
-    for (int i = 0; i < C::TM; i++)
-#pragma unroll
-      for (int j = 0; j < C::TN; j++) acc[i][j] = Dist<T>::relax(a[i], b[j], acc[i][j]);
+    for (int k = 0; k < C::BK; k++) mma_k_step<T, C>(As, Bs, acc, ty, tx, k);
+  } else {
+#pragma unroll 1
+    for (int k = 0; k < kcount; k++) mma_k_step<T, C>(As, Bs, acc, ty, tx, k);
   }
 }
 
