@@ -21,6 +21,7 @@
 #include "tma.cuh"
 #include "tma_tile.cuh"
 
+#include <cooperative_groups.h>
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -31,6 +32,8 @@
 #include <utility>
 
 namespace fapb {
+
+namespace cg = cooperative_groups;
 
 // ---------------------------------------------------------------------------
 // Launch shapes: grid sizes are multiples of the current device's SM count,
@@ -1969,6 +1972,16 @@ constexpr int kLStepList = 2048;  // changed rows listed per part (larger parts 
 // Several tiles run side by side (blockIdx.z / the item range): tile z has
 // its own Dt, xact, lact (nb each) and pact (K + 1) at offset z; its sources
 // are s0 + z * kMsbfS + s for s < kMsbfS and below nb.
+// Reserves one slot of a work list whose length is *count: the lanes of a
+// warp that call it together share one atomicAdd (a busy iteration appends
+// hundreds of thousands of heads to the same counter).
+__device__ __forceinline__ int wl_append(int *count) {
+  const cg::coalesced_group g = cg::coalesced_threads();
+  int base = 0;
+  if (g.thread_rank() == 0) base = atomicAdd(count, (int)g.size());
+  return g.shfl(base, 0) + (int)g.thread_rank();
+}
+
 // Row g of tile z changed: the heads of g's cross-part out-arcs join the
 // work list of iteration `stamp` (each row's heads once per list, each head
 // once per list).  cact/hact point at tile z's stamps.
@@ -1980,7 +1993,7 @@ __device__ __forceinline__ void bgraph_mark_heads(int g, int64_t znb, int *cact,
   for (int e = __ldg(otro + g); e < e1; e++) {
     const int h = __ldg(otcol + e);
     if (atomicExch(hact + h, stamp) != stamp)
-      wl[(stamp & 1) * (int64_t)wl_count[2] + atomicAdd(wl_count + (stamp & 1), 1)] = (int)(znb + h);
+      wl[(stamp & 1) * (int64_t)wl_count[2] + wl_append(wl_count + (stamp & 1))] = (int)(znb + h);
   }
 }
 
@@ -2120,6 +2133,7 @@ __global__ void __launch_bounds__(256)
   const int count = __ldcg(wl_count + (stamp & 1));
   const int *list = wl + (stamp & 1) * (int64_t)wl_count[2];
   const int t1 = stamp + 1;
+  bool any_change = false;
   for (int base = 2 * (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)); base < count; base += 2 * nwarps) {
     const int it = base + half;
     const bool live = it < count;
@@ -2176,15 +2190,17 @@ __global__ void __launch_bounds__(256)
       for (int e = __ldg(otro + v) + hl; e < f1; e += 16) {
         const int h = __ldg(otcol + e);
         if (atomicExch(hact + z * nb + h, t1) != t1)
-          wl[(t1 & 1) * (int64_t)wl_count[2] + atomicAdd(wl_count + (t1 & 1), 1)] = (int)(z * nb + h);
+          wl[(t1 & 1) * (int64_t)wl_count[2] + wl_append(wl_count + (t1 & 1))] = (int)(z * nb + h);
       }
       if (hl == 0) {
         lact[z * nb + v] = t1;
         pact[z * K1 + __ldg(gpart + v)] = t1;
-        *changed = 1;
       }
+      any_change = true;
     }
   }
+  // one store per warp that changed a row (the loop is warp-uniform)
+  if (__any_sync(0xffffffffu, any_change) && lane == 0) *changed = 1;
 }
 
 template <typename T>
