@@ -813,8 +813,15 @@ def run_extra(args, job, ctx, relax_peak, hbm_peak, peak_kind):
                          f"each step writes {4 * n * all_rows / 1e9:.1f} GB of distances"},
         "minplus": {"ms": mp_step, "relax": mp_relax, "bytes": mp_bytes, "achieved_grelax_s": a,
                     "frac_of_relax_peak": a / (relax_peak / 1e9),
+                    # a packed tile relaxes two entries per instruction: with a
+                    # share f of the tiles (and so of the relaxations) packed,
+                    # the instructions are R (1 - f / 2)
+                    "packed_tile_share": (pk_tiles[0] / pk_tiles[1]) if pk_tiles[1] else 0.0,
+                    "frac_of_instruction_peak": a / (relax_peak / 1e9)
+                    * (1.0 - 0.5 * ((pk_tiles[0] / pk_tiles[1]) if pk_tiles[1] else 0.0)),
                     "frac_of_hbm": mp_bytes / (mp_step * 1e-3) / 1e9 / hbm_peak,
-                    "peaks": f"relaxation peak measured live (fap_measure_relax_peak); HBM {peak_kind}",
+                    "peaks": f"relaxation peak measured live (fap_measure_relax_peak, one relaxation per "
+                             f"32-bit DPX instruction); HBM {peak_kind}",
                     "note": mp_note},
         "parity": None,
     }
