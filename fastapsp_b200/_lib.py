@@ -82,6 +82,7 @@ _SIGS = {
     "fap_graph_path_block": (INT, [P, I32, PP, ctypes.POINTER(I64), ctypes.POINTER(I64)]),
     "fap_graph_copy_path_block": (INT, [P, I32, P]),
     "fap_graph_sssp_rows": (INT, [P, P, I32, P]),
+    "fap_queue_order_check": (INT, [P, I32, INT]),
     "fap_graph_set_param": (INT, [P, ctypes.c_char_p, DBL]),
     "fap_graph_last_timing": (INT, [P, P]),
     "fap_graph_last_launches": (INT, [P, ctypes.POINTER(I64)]),

@@ -173,10 +173,16 @@ struct QueueBuf {
 };
 
 namespace {
-// sym: the matrices are symmetric; the panel items are the row panel's
-// tiles only (each also stores its transpose into the column panel) and the
-// remainder items the tiles (i, j) with i <= j (each off-diagonal one also
-// stores its transpose into (j, i)); t holds i << 16 | j for those.
+// Items of the Floyd work queue.  sym: the matrices are symmetric; the panel
+// items are the row panel's tiles only (each also stores its transpose into
+// the column panel) and the remainder items the tiles (i, j) with i <= j
+// (each off-diagonal one also stores its transpose into (j, i)); t holds
+// i << 16 | j for those.  Per pivot block: every part's diagonal item, then
+// every part's panel items, then every part's remainder items, so every
+// dependency of an item (per part: Floyd-1 of block kb after every Floyd-3
+// item of block kb - 1, Floyd-2 after Floyd-1, Floyd-3 after every Floyd-2
+// of the block) comes earlier in the list.  The boundary-row scatter items
+// follow all Floyd items.
 std::vector<QItem> floyd_queue_items(const std::vector<PartDesc> &parts, bool sym, int32_t *nfloyd,
                                      int32_t *max_nb) {
   std::vector<QItem> it;
@@ -215,6 +221,53 @@ std::vector<QItem> floyd_queue_items(const std::vector<PartDesc> &parts, bool sy
   *max_nb = mnb;
   return it;
 }
+
+// Whether every item's dependencies come before it in `it` and every Floyd
+// item of the parts appears exactly once (the queue's waits end only then).
+bool queue_order_ok(const std::vector<PartDesc> &parts, bool sym, const std::vector<QItem> &it, int32_t nfloyd) {
+  const int np = (int)parts.size();
+  std::vector<std::vector<int>> c1(np), c2(np), c3(np);
+  std::vector<int> nbs(np);
+  size_t want = 0;
+  for (int p = 0; p < np; p++) {
+    const int nb = parts[p].s > 0 ? (int)ceil_div(parts[p].s, kFloydTile) : 0;
+    nbs[p] = nb;
+    c1[p].assign(nb, 0);
+    c2[p].assign(nb, 0);
+    c3[p].assign(nb, 0);
+    want += nb * (1 + (sym ? nb - 1 : 2 * (nb - 1)) + (sym ? (size_t)(nb - 1) * nb / 2 : (size_t)(nb - 1) * (nb - 1)));
+  }
+  if ((size_t)nfloyd != want) return false;
+  std::vector<uint64_t> keys;
+  keys.reserve(nfloyd);
+  for (int32_t x = 0; x < nfloyd; x++) {
+    const QItem &q = it[x];
+    if (q.pidx < 0 || q.pidx >= np || q.kb < 0 || q.kb >= nbs[q.pidx]) return false;
+    const int p = q.pidx, nb = nbs[p], kb = q.kb;
+    const int n2 = sym ? nb - 1 : 2 * (nb - 1), n3 = sym ? (nb - 1) * nb / 2 : (nb - 1) * (nb - 1);
+    int ph;
+    if (q.kind == kQFloyd1) {
+      if (kb > 0 && c3[p][kb - 1] != n3) return false;
+      ph = 0;
+      c1[p][kb]++;
+    } else if (q.kind == (sym ? kQFloyd2S : kQFloyd2)) {
+      if (c1[p][kb] != 1) return false;
+      ph = 1;
+      c2[p][kb]++;
+    } else if (q.kind == (sym ? kQFloyd3S : kQFloyd3)) {
+      if (c2[p][kb] != n2) return false;
+      ph = 2;
+      c3[p][kb]++;
+    } else {
+      return false;
+    }
+    if (q.t < 0) return false;
+    keys.push_back(((((uint64_t)p << 8 | (uint64_t)kb) * 3 + ph) << 32) | (uint32_t)q.t);
+  }
+  std::sort(keys.begin(), keys.end());
+  return std::adjacent_find(keys.begin(), keys.end()) == keys.end();
+}
+
 }  // namespace
 
 struct fap_dgraph {
@@ -2035,6 +2088,21 @@ int ensure_in_edges(fap_dgraph *G) {
   return FAP_OK;
 }
 }  // namespace
+
+extern "C" int fap_queue_order_check(const int32_t *part_sizes, int32_t nparts, int sym) try {
+  if (!part_sizes || nparts < 0) return fail(FAP_ERR_INVALID, "NULL or negative argument");
+  std::vector<PartDesc> parts((size_t)nparts);
+  for (int32_t p = 0; p < nparts; p++) {
+    if (part_sizes[p] < 0 || part_sizes[p] > 255 * kFloydTile) return fail(FAP_ERR_INVALID, "part size %d", part_sizes[p]);
+    parts[p].s = part_sizes[p];
+  }
+  int32_t nfloyd = 0, mnb = 0;
+  const std::vector<QItem> it = floyd_queue_items(parts, sym != 0, &nfloyd, &mnb);
+  if (!queue_order_ok(parts, sym != 0, it, nfloyd)) return fail(FAP_ERR_STATE, "queue order breaks a dependency");
+  return FAP_OK;
+} catch (...) {
+  return fail_exception();
+}
 
 extern "C" int fap_graph_set_param(fap_dgraph *G, const char *key, double value) try {
   if (!G || !key) return fail(FAP_ERR_INVALID, "NULL argument");

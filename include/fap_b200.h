@@ -209,6 +209,13 @@ FAP_API int fap_graph_sssp_rows(fap_dgraph *g, const int32_t *sources, int32_t c
  * bound). */
 FAP_API int fap_graph_set_param(fap_dgraph *g, const char *key, double value);
 
+/* Diagnostics (no GPU work): builds the Floyd work queue's item list for
+ * parts of the given sizes (sym: the symmetric items) and checks that every
+ * item's dependencies come earlier in the list and that every item appears
+ * once (the persistent launch's waits end only then); FAP_OK when they do,
+ * FAP_ERR_STATE otherwise. */
+FAP_API int fap_queue_order_check(const int32_t *part_sizes, int32_t nparts, int sym);
+
 /* Min-plus tiles run in the packed 16-bit form and in all, counted over
  * every solve of g so far (see "minplus_pack16").  Synchronous. */
 FAP_API int fap_graph_pack16_tiles(fap_dgraph *g, int64_t *packed, int64_t *total);
