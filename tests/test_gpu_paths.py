@@ -156,3 +156,27 @@ def test_fapgraph_path_getters(cuda_ok, name):
                 assert ws, f"{x} -> {y} is not an edge"
                 total += min(ws)
             assert abs(total - d) <= (0 if case["integral"] else 1e-4 * max(d, 1.0))
+
+
+@pytest.mark.parametrize("name", ["grid12_k4", "rgg300_f32_k4"])
+def test_fapgraph_paths_with_bounded_resident_rows(cuda_ok, name):
+    """With fewer output rows allowed on the device than the graph has, the
+    parts solved in groups (from the resident cache) give the same
+    predecessor rows as one solve of every part."""
+    case = load_golden(name)
+    n, K = int(case["n"]), int(case["K"])
+    with tempfile.TemporaryDirectory() as tmp:
+        write_golden_mtx(case, tmp)
+        g = fapGraph(case["name"], bool(case["directed"]), bool(case["weighted"]), K, root=tmp)
+        if case["injected_partition"]:
+            gid0 = (np.arange(n, dtype=np.int64) * K // n).astype(np.int32)
+            g.setPartition(gid0 + 1)
+        g.preCondition()
+        assert g.solve(is_path_needed=True) == 0
+        D, P = g.getAllDistance(), g.getAllPath()
+        g.setMaxResidentRows(int(max(case["ver_num"][1:])))
+        for p in range(K, 0, -1):
+            g.solveSubGraph(p, is_path_needed=True)
+            off, rows = int(case["ver_offset"][p]), int(case["ver_num"][p])
+            np.testing.assert_array_equal(g.getSubGraphPath(p), P[off:off + rows])
+            np.testing.assert_array_equal(g.getSubGraphDistance(p), D[off:off + rows])
