@@ -335,7 +335,7 @@ struct fap_dgraph {
   std::vector<int32_t> pk_krow;
   // the same for the tiled expansion of the boundary graph (Expand16), sized
   // for the launch's part list
-  DevBuf d_xk_off, d_xk_range, d_xk_maxb, d_xk_tiles;
+  DevBuf d_xk_off, d_xk_range, d_xk_maxb, d_xk_tiles, d_xk_ap, d_xk_bd;
   // Work queue of the batched Floyd (FloydQueue): the batch's items and
   // counters, and the resident cache build's (its parts are all parts).
   // Parts with at most this many boundary vertices (<= kThinBoundary) take
@@ -640,7 +640,8 @@ extern "C" int fap_graph_destroy(fap_dgraph *G) try {
                       &G->d_botro, &G->d_botcol, &G->d_bitw, &G->d_bitems, &G->d_bDt, &G->d_bact, &G->d_bpact,
                       &G->d_bgpart, &G->d_bpcolmap, &G->d_grow, &G->d_pk_off, &G->d_pk_range,
                       &G->d_pk_s16, &G->d_pk_at, &G->d_pk_krow, &G->d_pk_maxa, &G->d_pk_tiles, &G->q.items, &G->q.cnt, &G->cq.items, &G->cq.cnt,
-                      &G->d_xk_off, &G->d_xk_range, &G->d_xk_maxb, &G->d_xk_tiles, &G->d_bTc})
+                      &G->d_xk_off, &G->d_xk_range, &G->d_xk_maxb, &G->d_xk_tiles, &G->d_bTc,
+                      &G->d_xk_ap, &G->d_xk_bd})
       b->release();
     if (G->h_changed) cudaFreeHost(G->h_changed);
     for (auto &cs : G->cslot) {
@@ -1058,6 +1059,25 @@ int expand_bgraph(fap_dgraph *G, const PartDesc *dp, int np, int max_s, const T 
       }
       xk = Expand16{G->d_xk_off.as<int32_t>(), G->d_xk_range.as<int32_t>(), G->d_xk_maxb.as<int32_t>(),
                     (int32_t)nrt, G->d_xk_tiles.as<unsigned long long>()};
+      // operands packed beforehand ("minplus_prepack"), when they fit
+      int32_t max_b = 0;
+      for (int32_t q = 1; q <= G->K; q++) max_b = std::max(max_b, G->bnum[q]);
+      const int64_t ap_ld = round_up(ceil_div(G->total_b, 2), 4);
+      const size_t ap_bytes = (size_t)G->total_b * ap_ld * 4, bd_bytes = (size_t)G->total_b * ldFB * 4;
+      const bool grow = G->d_xk_ap.bytes < ap_bytes || G->d_xk_bd.bytes < bd_bytes;
+      size_t free_b = 0, total_mem = 0;
+      if (G->prepack && max_b > 0 && ldFB % 4 == 0 && ap_bytes + bd_bytes <= kPrepackBytes &&
+          (!grow || (cudaMemGetInfo(&free_b, &total_mem) == cudaSuccess && ap_bytes + bd_bytes <= free_b / 4)) &&
+          G->d_xk_ap.ensure_async(ap_bytes, st) == FAP_OK && G->d_xk_bd.ensure_async(bd_bytes, st) == FAP_OK) {
+        xk.ap = G->d_xk_ap.as<uint32_t>();
+        xk.bd = G->d_xk_bd.as<uint32_t>();
+        xk.ap_ld = (int32_t)ap_ld;
+        xk.bd_ld = (int32_t)ldFB;
+        xk.max_b = max_b;
+        xk.rows = G->total_b;
+      } else {
+        cudaGetLastError();  // (a failed cudaMemGetInfo or allocation: tiles convert their stages)
+      }
     }
     FAP_CK(launch_bdy_expand_tma<T>(dp, np, max_s, (int)G->total_b, G->d_grow.as<const int64_t>(),
                                     G->d_st2ed.as<const int32_t>(), G->d_dB.as<const T>(), G->ldB, F, ldFB, np,
@@ -2338,6 +2358,8 @@ extern "C" int fap_graph_release(fap_dgraph *G) try {
   G->d_pk_s16.release();
   G->d_pk_at.release();
   G->d_pk_krow.release();
+  G->d_xk_ap.release();
+  G->d_xk_bd.release();
   for (auto &cs : G->cslot) {
     if (cs.stream) FAP_CK(cudaStreamSynchronize(cs.stream));
     cs.busy = false;
@@ -2364,7 +2386,8 @@ extern "C" int fap_graph_device_bytes(const fap_dgraph *G, int64_t *bytes) try {
                           &G->d_msbf_changed, &G->d_bitro, &G->d_bitcol, &G->d_botro, &G->d_botcol, &G->d_bitw, &G->d_bitems,
                           &G->d_bDt, &G->d_bact, &G->d_bpact, &G->d_bgpart, &G->d_bpcolmap, &G->d_grow,
                           &G->d_bTc, &G->d_pk_off, &G->d_pk_range, &G->d_pk_maxa, &G->d_pk_tiles, &G->d_pk_s16,
-                          &G->d_pk_at, &G->d_pk_krow, &G->d_xk_off, &G->d_xk_range, &G->d_xk_maxb, &G->d_xk_tiles})
+                          &G->d_pk_at, &G->d_pk_krow, &G->d_xk_off, &G->d_xk_range, &G->d_xk_maxb, &G->d_xk_tiles,
+                          &G->d_xk_ap, &G->d_xk_bd})
     t += (int64_t)b->bytes;
   *bytes = t;
   return FAP_OK;

@@ -2341,12 +2341,13 @@ __global__ void __launch_bounds__(256)
 // to D rows grow[g], columns st2ed[start_q + j] (and, for g of part q itself,
 // to FB).  PACK (int32): a tile whose values provably fit (Expand16) runs
 // the packed 16-bit engine with its rows shifted by their offsets.
-template <typename T, bool PACK>
+template <typename T, int PACK>
 __global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS, 2)
     bdy_expand_tma_kernel(const PartDesc *__restrict__ parts, int nbB, const int64_t *__restrict__ grow,
                           const int32_t *__restrict__ st2ed, T *D, int64_t ldD, T *FB, int64_t ldFB,
                           const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
-                          int *status, Expand16 xk) {
+                          int *status, Expand16 xk, const __grid_constant__ CUtensorMap mapAP,
+                          const __grid_constant__ CUtensorMap mapBD) {
   using TC = typename FloydCfg<T, kFloydTile>::TC;
   extern __shared__ __align__(128) unsigned char bxt_smem_raw[];
   const PartDesc pd = parts[blockIdx.z];
@@ -2358,7 +2359,7 @@ __global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS, 2)
   T acc[8][8];
   const int fz = (int)(pd.f_off / ((int64_t)pd.ldf * pd.ldf));
   bool packed = false;
-  if constexpr (PACK) {
+  if constexpr (PACK != 0) {
     packed = __ldg(xk.range + (int64_t)blockIdx.z * xk.nrt + blockIdx.y) + __ldg(xk.maxB + blockIdx.z) < kPackCap;
     if (threadIdx.x == 0) {
       atomicAdd(xk.tiles + 1, 1ull);
@@ -2366,10 +2367,17 @@ __global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS, 2)
     }
   }
   if (packed) {
-    if constexpr (PACK) {
+    if constexpr (PACK != 0) {
       using P = Pack16Cfg<TC>;
-      uint32_t *pbuf = reinterpret_cast<uint32_t *>(smem_align128(bxt_smem_raw) + P::BUF_OFFSET);
-      int32_t *roff = reinterpret_cast<int32_t *>(pbuf + 2 * P::BUF_ELEMS) + TC::BN;
+      // row offsets: after the packed buffers (PACK 1), after the packed
+      // ring in the int32 ring's memory (PACK 2)
+      int32_t *roff =
+          PACK == 1 ? reinterpret_cast<int32_t *>(reinterpret_cast<uint32_t *>(smem_align128(bxt_smem_raw) +
+                                                                               P::BUF_OFFSET) +
+                                                  2 * P::BUF_ELEMS) +
+                          TC::BN
+                    : reinterpret_cast<int32_t *>(reinterpret_cast<unsigned char *>(sm.ring) +
+                                                  Pack16qCfg<TC>::STAGE_WORDS * 4 * TC::STAGES);
       for (int r = threadIdx.x; r < TC::BM; r += blockDim.x)
         roff[r] = m0 + r < nbB ? __ldg(xk.off + (int64_t)blockIdx.z * nbB + m0 + r) : 0;
       uint32_t a16[4][8];
@@ -2378,8 +2386,15 @@ __global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS, 2)
 #pragma unroll
         for (int j = 0; j < 8; j++) a16[i][j] = kPackInit;
       // (the engine's first barrier orders the row offsets before use)
-      if (!tma_minplus_tile16<TC>(&mapA, pd.bd_col, m0, 0, &mapB, n0, 0, fz, pd.b, a16, sm, pbuf, roff, nullptr,
-                                  nbB - m0)) {
+      bool ok;
+      if constexpr (PACK == 1) {
+        uint32_t *pbuf = reinterpret_cast<uint32_t *>(smem_align128(bxt_smem_raw) + P::BUF_OFFSET);
+        ok = tma_minplus_tile16<TC>(&mapA, pd.bd_col, m0, 0, &mapB, n0, 0, fz, pd.b, a16, sm, pbuf, roff, nullptr,
+                                    nbB - m0);
+      } else {
+        ok = tma_minplus_tile16q<TC>(&mapAP, m0 / 2, &mapBD, n0, pd.bd_row, pd.b, a16, sm, nbB - m0);
+      }
+      if (!ok) {
         if (threadIdx.x == 0) set_status(status, kDevTmaTimeout);
         return;
       }
@@ -2440,6 +2455,50 @@ __global__ void __launch_bounds__(FloydCfg<T, kFloydTile>::THREADS, 2)
     }
 }
 
+// Pre-packed A operand of the packed expansion tiles (Expand16::ap): CTA
+// (x, y, q) packs dB rows 128x .. 128x+127 at part q's boundary columns
+// bd_col + 32y .. +31 through a shared-memory transpose: reads along k,
+// writes along the row pairs.  Rows past nbB read as having no finite entry.
+__global__ void __launch_bounds__(256)
+    expand16_pack_a_kernel(const PartDesc *__restrict__ parts, int nbB, const int32_t *__restrict__ dB,
+                           int64_t ldB, Expand16 xk) {
+  const PartDesc pd = parts[blockIdx.z];
+  const int g0 = blockIdx.x * 128, k0 = blockIdx.y * 32;
+  if (k0 >= pd.b) return;
+  __shared__ uint16_t t[32][130];
+  const int tid = threadIdx.x;
+  const int32_t *off = xk.off + (int64_t)blockIdx.z * nbB;
+#pragma unroll 4
+  for (int q = 0; q < 16; q++) {
+    const int r = tid / 32 + 8 * q, k = tid % 32;
+    const int g = g0 + r;
+    int32_t v = kPackCap;
+    if (g < nbB && k0 + k < pd.b) v = pack_clamp(__ldg(dB + (int64_t)g * ldB + pd.bd_col + k0 + k), __ldg(off + g));
+    t[k][r] = (uint16_t)v;
+  }
+  __syncthreads();
+#pragma unroll 4
+  for (int q = 0; q < 8; q++) {
+    const int p = tid % 64, k = tid / 64 + 4 * q;
+    const int gp = g0 / 2 + p;
+    if (k0 + k < pd.b && gp < xk.ap_ld)
+      xk.ap[(int64_t)(pd.bd_row + k0 + k) * xk.ap_ld + gp] = (uint32_t)t[k][2 * p] | ((uint32_t)t[k][2 * p + 1] << 16);
+  }
+}
+
+// Pre-packed B operand (Expand16::bd): row bd_row + k of part q holds
+// F_q[k][v] clamped at kPackCap in both halves (kPackCap past s_q).
+__global__ void __launch_bounds__(256)
+    expand16_pack_b_kernel(const PartDesc *__restrict__ parts, const int32_t *__restrict__ F, Expand16 xk) {
+  const PartDesc pd = parts[blockIdx.z];
+  const int k = blockIdx.y;
+  if (k >= pd.b) return;
+  const int v = blockIdx.x * 256 + threadIdx.x;
+  if (v >= xk.bd_ld) return;
+  const int32_t x = v < pd.s ? min(__ldg(F + pd.f_off + (int64_t)k * pd.ldf + v), kPackCap) : kPackCap;
+  xk.bd[(int64_t)(pd.bd_row + k) * xk.bd_ld + v] = pack_pair(x, x);
+}
+
 template <typename T>
 cudaError_t launch_bdy_expand_tma(const PartDesc *parts, int nparts, int max_s, int nbB, const int64_t *grow,
                                   const int32_t *st2ed, const T *dB, int64_t ldB, const T *F, int64_t ldf,
@@ -2461,21 +2520,49 @@ cudaError_t launch_bdy_expand_tma(const PartDesc *parts, int nparts, int max_s, 
           parts, nbB, dB, ldB, *xk);
       expand16_maxb_kernel<<<(unsigned)nparts, 256, 0, stream>>>(parts, F, *xk);
       *launches += 2;
+      if (xk->ap != nullptr) {
+        // operands packed beforehand, then tiles without conversion
+        if (xk->bd == nullptr || xk->ap_ld % 4 != 0 || xk->bd_ld % 4 != 0 || xk->rows <= 0 || xk->max_b <= 0 ||
+            xk->ap_ld < (int)ceil_div(nbB, 2) || xk->bd_ld < max_s)
+          return cudaErrorInvalidValue;
+        CUtensorMap mapAP, mapBD;
+        e = make_tmap_3d_dt(&mapAP, xk->ap, CU_TENSOR_MAP_DATA_TYPE_UINT32, 4, xk->ap_ld, xk->rows, 1, TC::BM / 2,
+                            TC::BK);
+        if (e == cudaSuccess)
+          e = make_tmap_3d_dt(&mapBD, xk->bd, CU_TENSOR_MAP_DATA_TYPE_UINT32, 4, xk->bd_ld, xk->rows, 1, TC::BN,
+                              TC::BK);
+        if (e != cudaSuccess) return e;
+        expand16_pack_a_kernel<<<dim3((unsigned)ceil_div(nbB, 128), (unsigned)ceil_div(xk->max_b, 32),
+                                      (unsigned)nparts),
+                                 256, 0, stream>>>(parts, nbB, dB, ldB, *xk);
+        expand16_pack_b_kernel<<<dim3((unsigned)ceil_div(xk->bd_ld, 256), (unsigned)xk->max_b, (unsigned)nparts),
+                                 256, 0, stream>>>(parts, F, *xk);
+        *launches += 2;
+        const size_t smem = TC::SMEM_BYTES;
+        auto kern = bdy_expand_tma_kernel<T, 2>;
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        kern<<<grid, TC::THREADS, smem, stream>>>(parts, nbB, grow, st2ed, D, ldD, FB, ldFB, mapA, mapB, status,
+                                                  *xk, mapAP, mapBD);
+        *launches += 1;
+        return cudaGetLastError();
+      }
       const size_t smem = Pack16Cfg<TC>::SMEM_BYTES;
-      auto kern = bdy_expand_tma_kernel<T, true>;
+      auto kern = bdy_expand_tma_kernel<T, 1>;
       e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       if (e != cudaSuccess) return e;
       kern<<<grid, TC::THREADS, smem, stream>>>(parts, nbB, grow, st2ed, D, ldD, FB, ldFB, mapA, mapB, status,
-                                                *xk);
+                                                *xk, mapA, mapB);
       *launches += 1;
       return cudaGetLastError();
     }
   }
   const size_t smem = TC::SMEM_BYTES;
-  auto kern = bdy_expand_tma_kernel<T, false>;
+  auto kern = bdy_expand_tma_kernel<T, 0>;
   e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  kern<<<grid, TC::THREADS, smem, stream>>>(parts, nbB, grow, st2ed, D, ldD, FB, ldFB, mapA, mapB, status, none);
+  kern<<<grid, TC::THREADS, smem, stream>>>(parts, nbB, grow, st2ed, D, ldD, FB, ldFB, mapA, mapB, status, none,
+                                            mapA, mapB);
   *launches += 1;
   return cudaGetLastError();
 }

@@ -90,6 +90,16 @@ struct Expand16 {
   int32_t *maxB;    // [nparts]
   int32_t nrt;      // 128-row tiles of dB
   unsigned long long *tiles;  // [2]: tiles run packed, tiles run (cumulative)
+  // Optional operands packed beforehand (ap null: every packed tile converts
+  // its stages in shared memory).  ap [rows][ap_ld] words: the dB rows at
+  // part q's boundary columns, shifted by off and clamped at kPackCap, two
+  // rows a word (row 2p in the low half), k-major: word p of row bd_row + k.
+  // bd [rows][bd_ld] words: F_q[k][v] clamped at kPackCap in both halves,
+  // row bd_row + k, column v (kPackCap past the part's s columns).
+  uint32_t *ap;
+  uint32_t *bd;
+  int32_t ap_ld, bd_ld, max_b;
+  int64_t rows;
 };
 
 // Work queue of the batched Floyd-Warshall in one persistent launch: items

@@ -446,4 +446,105 @@ __device__ __forceinline__ bool tma_minplus_tile16p(const CUtensorMap *mapA, int
   return true;
 }
 
+// ---------------------------------------------------------------------------
+// Packed 16-bit form on row pairs packed beforehand: the A box holds BK rows
+// (k) of BM/2 words, each word two rows of A (row 2p in the low half), and
+// the B box BK rows of BN words with both halves equal; one
+// __viaddmin_s16x2 relaxes two rows against one column, as in
+// tma_minplus_tile16 (acc[i][j]: pair i = 2g + h, rows 4g + 2h and the next
+// of the thread, column j), without the conversion.
+// ---------------------------------------------------------------------------
+template <class C>
+struct Pack16qCfg {
+  static constexpr int A_WORDS = C::BK * C::BM / 2;
+  static constexpr int B_WORDS = C::BK * C::BN;
+  static constexpr int STAGE_WORDS = A_WORDS + B_WORDS;
+  static constexpr uint32_t TX_BYTES = STAGE_WORDS * 4;
+  static_assert(C::STAGES * STAGE_WORDS * 4 <= C::RING_BYTES, "the packed ring fits in the int32 ring");
+  static_assert((A_WORDS * 4) % 128 == 0 && (STAGE_WORDS * 4) % 128 == 0, "128-byte aligned boxes");
+  static_assert(C::BM == 128 && C::BN == 128 && C::THREADS == 256 && C::TX == 16, "thread mapping below");
+};
+
+template <class C, int GI>
+__device__ __forceinline__ void pack16q_k_step(const uint32_t *PA, const uint32_t *PB, uint32_t (&acc)[4][8],
+                                               int ty, int tx, int k) {
+  uint32_t a[4], b[8];
+#pragma unroll
+  for (int g = 0; g < GI; g++) {
+    const uint2 v = *reinterpret_cast<const uint2 *>(PA + k * (C::BM / 2) + g * (C::BM / 4) + ty * 2);
+    a[2 * g] = v.x;
+    a[2 * g + 1] = v.y;
+  }
+#pragma unroll
+  for (int g = 0; g < 2; g++) {
+    const uint4 v = *reinterpret_cast<const uint4 *>(PB + k * C::BN + g * (C::BN / 2) + tx * 4);
+    b[4 * g + 0] = v.x; b[4 * g + 1] = v.y; b[4 * g + 2] = v.z; b[4 * g + 3] = v.w;
+  }
+#pragma unroll
+  for (int i = 0; i < 2 * GI; i++)
+#pragma unroll
+    for (int j = 0; j < 8; j++) acc[i][j] = __viaddmin_s16x2(a[i], b[j], acc[i][j]);
+}
+
+template <class C, int GI>
+__device__ __forceinline__ void pack16q_chunk_compute(const uint32_t *PA, const uint32_t *PB,
+                                                      uint32_t (&acc)[4][8], int ty, int tx, int kc) {
+  if (kc == C::BK) {
+#pragma unroll
+    for (int k = 0; k < C::BK; k++) pack16q_k_step<C, GI>(PA, PB, acc, ty, tx, k);
+  } else {
+#pragma unroll 1
+    for (int k = 0; k < kc; k++) pack16q_k_step<C, GI>(PA, PB, acc, ty, tx, k);
+  }
+}
+
+// A boxes at (ax, ky + c*BK) of mapA (ax: the tile's first row pair), B
+// boxes at (bx, ky + c*BK) of mapB; the same ring protocol as
+// tma_minplus_tile.  mvalid: rows of the tile that are not padding.
+template <class C>
+__device__ __forceinline__ bool tma_minplus_tile16q(const CUtensorMap *mapA, int ax, const CUtensorMap *mapB,
+                                                    int bx, int ky, int K, uint32_t (&acc)[4][8],
+                                                    TmaSmem<int32_t, C> &sm, int mvalid = C::BM) {
+  using P = Pack16qCfg<C>;
+  const int tid = threadIdx.x, ty = tid / C::TX, tx = tid % C::TX;
+  const int w8 = (tid / 32) * 8;
+  const bool rlo = w8 < mvalid, rhi = C::BM / 2 + w8 < mvalid;
+  const int n = (int)ceil_div(K, C::BK);
+  if (n == 0) return true;
+  uint32_t *ring = reinterpret_cast<uint32_t *>(sm.ring);
+  auto issue = [&](int c, int s) {
+    uint32_t *As = ring + s * P::STAGE_WORDS;
+    mbar_arrive_expect_tx(&sm.bars[s], P::TX_BYTES);
+    tma_load_3d(As, mapA, ax, ky + c * C::BK, 0, &sm.bars[s]);
+    tma_load_3d(As + P::A_WORDS, mapB, bx, ky + c * C::BK, 0, &sm.bars[s]);
+  };
+  fence_proxy_async_all();
+  __syncthreads();
+  if (tid == 0)
+    for (int c = 0; c < n && c < C::STAGES; c++) issue(c, c);
+  for (int c = 0; c < n; c++) {
+    const int s = c % C::STAGES;
+    const bool got = mbar_wait_bounded(&sm.bars[s], (sm.phase >> s) & 1u);
+    sm.phase ^= 1u << s;
+    if (got) {
+      const uint32_t *As = ring + s * P::STAGE_WORDS;
+      const int kc = min(C::BK, K - c * C::BK);
+      if (rhi) pack16q_chunk_compute<C, 2>(As, As + P::A_WORDS, acc, ty, tx, kc);
+      else if (rlo) pack16q_chunk_compute<C, 1>(As, As + P::A_WORDS, acc, ty, tx, kc);
+    }
+    fence_proxy_async_smem();  // this thread's reads of stage s precede its refill
+    if (__syncthreads_or(!got)) {
+      for (int c2 = c + 1; c2 < n && c2 < c + C::STAGES; c2++) {
+        const int s2 = c2 % C::STAGES;
+        if (tid == 0) mbar_wait_bounded(&sm.bars[s2], (sm.phase >> s2) & 1u);
+        sm.phase ^= 1u << s2;
+      }
+      __syncthreads();
+      return false;
+    }
+    if (tid == 0 && c + C::STAGES < n) issue(c + C::STAGES, s);
+  }
+  return true;
+}
+
 }  // namespace fapb

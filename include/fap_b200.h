@@ -194,6 +194,8 @@ FAP_API int fap_graph_sssp_rows(fap_dgraph *g, const int32_t *sources, int32_t c
  * int32 values either way; 0: int32 everywhere); "minplus_prepack" (default
  * 1: the packed tiles read operands packed once per solve, the boundary rows
  * as 16-bit columns and the inner-to-boundary distances with both halves
+ * equal, and the packed tiles of the boundary graph's tiled expansion read
+ * the dB rows as row pairs and the parts' boundary rows with both halves
  * equal, when those arrays fit in 8 GiB and a quarter of the free device
  * memory; 0, or when they do not fit: each tile converts its int32 stages
  * in shared memory; the same values either way); "floyd_queue" (default 1:

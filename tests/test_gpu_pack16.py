@@ -84,13 +84,18 @@ def test_packed_tiles_from_the_resident_cache(cuda_ok, tmp_path, prepack):
     assert dg.pack16_tiles()[0] > 0
 
 
-def test_packed_expansion_tiles_equal_int32(cuda_ok):
+@pytest.mark.parametrize("prepack", [1, 0])
+@pytest.mark.parametrize("heavy_rows", [96, 48])
+def test_packed_expansion_tiles_equal_int32(cuda_ok, prepack, heavy_rows):
     """The tiled expansion of the boundary graph (Bellman-Ford closure, forced
-    on a small grid) in packed 16-bit tiles gives the int32 tiles' blocks."""
-    el = _grid(96, 200000, 13)
+    on a small grid) in packed 16-bit tiles gives the int32 tiles' blocks,
+    with the operands packed beforehand or stage by stage, whether every or
+    only some of the tiles fit."""
+    el = _grid(heavy_rows, 200000, 13)
     import tempfile
     with tempfile.TemporaryDirectory() as tmp:
         dg, vn, bn = _device_graph(el, 12, tmp, "pkx")
+    dg.set_param("minplus_prepack", prepack)
     dg.set_param("bgraph_form", 2)
     dg.set_param("minplus_pack16", 0)
     dg.solve(None, FAP_MODE_BATCHED)
@@ -103,6 +108,10 @@ def test_packed_expansion_tiles_equal_int32(cuda_ok):
         assert np.array_equal(dg.copy_block(p), ref[p - 1]), f"part {p}"
     packed, total = dg.expand16_tiles()
     assert 0 < packed <= total
+    dg.cache_build()                  # the cache build's expansion
+    dg.solve(None, FAP_MODE_BATCHED)
+    for p in range(1, 13):
+        assert np.array_equal(dg.copy_block(p), ref[p - 1]), f"part {p} (cache)"
 
 
 @pytest.mark.parametrize("thin_max_b", [0, 4, 8])
