@@ -1057,8 +1057,11 @@ int expand_bgraph(fap_dgraph *G, const PartDesc *dp, int np, int max_s, const T 
         FAP_TRY(G->d_xk_tiles.ensure_async(2 * sizeof(unsigned long long), st));
         FAP_CK(cudaMemsetAsync(G->d_xk_tiles.p, 0, 2 * sizeof(unsigned long long), st));
       }
-      xk = Expand16{G->d_xk_off.as<int32_t>(), G->d_xk_range.as<int32_t>(), G->d_xk_maxb.as<int32_t>(),
-                    (int32_t)nrt, G->d_xk_tiles.as<unsigned long long>()};
+      xk.off = G->d_xk_off.as<int32_t>();
+      xk.range = G->d_xk_range.as<int32_t>();
+      xk.maxB = G->d_xk_maxb.as<int32_t>();
+      xk.nrt = (int32_t)nrt;
+      xk.tiles = G->d_xk_tiles.as<unsigned long long>();
       // operands packed beforehand ("minplus_prepack"), when they fit
       int32_t max_b = 0;
       for (int32_t q = 1; q <= G->K; q++) max_b = std::max(max_b, G->bnum[q]);
@@ -1199,8 +1202,12 @@ int prepare_batch(fap_dgraph *G, const std::vector<int32_t> &ids, bool cached, b
       FAP_TRY(G->d_pk_tiles.ensure_async(2 * sizeof(unsigned long long), st));
       FAP_CK(cudaMemsetAsync(G->d_pk_tiles.p, 0, 2 * sizeof(unsigned long long), st));
     }
-    G->pk = Pack16{G->d_pk_off.as<int32_t>(), G->d_pk_range.as<int32_t>(), G->d_pk_maxa.as<int32_t>(),
-                   (int32_t)ntiles, G->d_pk_tiles.as<unsigned long long>()};
+    G->pk = Pack16{};
+    G->pk.off = G->d_pk_off.as<int32_t>();
+    G->pk.range = G->d_pk_range.as<int32_t>();
+    G->pk.maxA = G->d_pk_maxa.as<int32_t>();
+    G->pk.ntiles = (int32_t)ntiles;
+    G->pk.tiles = G->d_pk_tiles.as<unsigned long long>();
     // Operands packed beforehand for the parts with tile work: rows of the
     // parts' boundary vertices in batch order.
     G->pk_krow.assign(np, -1);
